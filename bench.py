@@ -1,0 +1,353 @@
+#!/usr/bin/env python
+"""SMAC pressure-projection throughput on B200.
+
+Metric: 256^3 pressure solves/s to a 1e-8 FP64 true relative residual,
+mixed precision (headline `value`) beside plain FP64, plus the HBM fraction
+of the dominant kernel.  A step is one projection of the 256^3 single-phase
+workload: divergence of a seeded U[-1,1) face field -> MG-PCG solve to
+1e-8 -> velocity correction.
+
+    python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+
+One process per GPU (torchrun for N>1); every rank projects its own replica
+(the path does not shard: "replicas only"), value = all ranks' solves / the
+slowest rank's time.  --impl reference times the reference algorithm's CPU
+restatement (oracle, all host threads) on the same workload (rank 0 only).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "256^3 pressure solves/s to 1e-8 FP64 resid (mixed; FP64 plain alongside)"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=30)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--n", type=int, default=256)
+    ap.add_argument("--workload", choices=["plain", "vof", "ibm"], default="plain")
+    ap.add_argument("--tol", type=float, default=1e-8)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--cpu-budget", type=float, default=25.0, help="seconds of oracle work for cpu_baseline")
+    return ap.parse_args()
+
+
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    """NVML clock / throttle-reason sampling on a thread during the timed region."""
+
+    REASONS = {
+        "hw_slowdown": 0x0000000000000008,
+        "sw_power_cap": 0x0000000000000004,
+        "hw_thermal_slowdown": 0x0000000000000040,
+        "sw_thermal_slowdown": 0x0000000000000020,
+        "hw_power_brake_slowdown": 0x0000000000000080,
+    }
+
+    def __init__(self, index):
+        self.samples = []
+        self.reasons = set()
+        self._stop = threading.Event()
+        self.ok = False
+        try:
+            import pynvml
+            pynvml.nvmlInit()
+            self.nv = pynvml
+            self.h = pynvml.nvmlDeviceGetHandleByIndex(index)
+            self.max_mhz = pynvml.nvmlDeviceGetMaxClockInfo(self.h, pynvml.NVML_CLOCK_SM)
+            self.ok = True
+        except Exception as e:  # noqa: BLE001
+            self.err = str(e)
+
+    def _run(self):
+        nv = self.nv
+        while not self._stop.is_set():
+            try:
+                self.samples.append(nv.nvmlDeviceGetClockInfo(self.h, nv.NVML_CLOCK_SM))
+                r = nv.nvmlDeviceGetCurrentClocksEventReasons(self.h)
+                for k, bit in self.REASONS.items():
+                    if r & bit:
+                        self.reasons.add(k)
+            except Exception:  # noqa: BLE001
+                pass
+            time.sleep(0.002)
+
+    def __enter__(self):
+        if self.ok:
+            self.t = threading.Thread(target=self._run, daemon=True)
+            self.t.start()
+        return self
+
+    def __exit__(self, *a):
+        if self.ok:
+            self._stop.set()
+            self.t.join()
+
+    def summary(self):
+        if not self.ok:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0, "error": getattr(self, "err", "")}
+        med = statistics.median(self.samples) if self.samples else None
+        return {"sm_mhz": med, "sm_max_mhz": self.max_mhz, "reasons": sorted(self.reasons),
+                "samples": len(self.samples)}
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def ncu_traffic():
+    """Per-launch DRAM bytes of the dominant kernel from the committed ncu summary."""
+    p = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            return json.load(f)
+    return {}
+
+
+# ---------------------------------------------------------------------------
+def build_case(args, solid_fraction=None):
+    from mydemcfd_b200 import workloads as W
+    if args.workload == "plain":
+        return W.plain_case(args.n, seed=2)
+    if args.workload == "vof":
+        return W.vof_case(args.n, seed=3, ratio=1000.0)
+    return W.ibm_case(args.n, seed=4, nsph=200, solid_fraction=solid_fraction)
+
+
+def cpu_baseline(args, case, budget):
+    """The reference algorithm (oracle restatement of solve_pureneumann_gmgpcg,
+    Jacobi V-cycle) on all host threads, a bounded sample of the same solve."""
+    from oracle import oracle as O
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from _cases import ref_grid
+    g = ref_grid(case)
+    cores = O.num_threads()
+    t0 = time.perf_counter()
+    _, _, s1 = O.solve(g, tol=args.tol, stop_rule=O.STOP_REL_RECURSIVE, max_iter=1)
+    t1 = time.perf_counter()
+    _, _, s3 = O.solve(g, tol=args.tol, stop_rule=O.STOP_REL_RECURSIVE, max_iter=3)
+    t3 = time.perf_counter()
+    t_it = max((t3 - t1) - (t1 - t0), 1e-9) / 2.0
+    t_setup = max((t1 - t0) - t_it, 0.0)
+    m = int(max(3, min(2000, (budget - (t3 - t0)) / max(t_it, 1e-9))))
+    ts = time.perf_counter()
+    _, _, sm = O.solve(g, tol=args.tol, stop_rule=O.STOP_REL_RECURSIVE, max_iter=m)
+    te = time.perf_counter()
+    if sm["converged"]:
+        t_solve = te - ts
+        iters = sm["iterations"]
+        how = f"full solve: {iters} PCG iterations to ||r||/||b|| < {args.tol:g} (recursive, checked every 5)"
+    else:
+        rate = sm["res_rel"] ** (1.0 / sm["iterations"])
+        iters = int(math.ceil(math.log(args.tol) / math.log(rate)))
+        t_solve = t_setup + iters * t_it
+        how = (f"{sm['iterations']} PCG iterations timed ({te - ts:.1f} s, {t_it * 1e3:.0f} ms/iteration), "
+               f"residual rate {rate:.3f}/iteration -> {iters} iterations to {args.tol:g} extrapolated")
+    return {
+        "value": 1.0 / t_solve, "unit": "solves/s", "cores": cores, "kind": "port",
+        "sample": f"oracle Jacobi-MG-PCG (reference algorithm) on the {case.N[0]}^3 {args.workload} workload; " + how,
+        "seconds_per_solve": t_solve, "iterations": iters,
+    }
+
+
+def run_reference(args, rank):
+    if rank != 0:
+        return
+    from oracle import oracle as O
+    from mydemcfd_b200 import workloads as W
+    case = build_case(args, solid_fraction=lambda N, h, o, s: O.solid_fraction_spheres(N, h, o, s))
+    # each step is a bounded sample of the solve; the first step sizes it
+    budget = max(2.0, 150.0 / max(1, args.steps + args.warmup))
+    vals = []
+    for i in range(args.warmup + args.steps):
+        cb = cpu_baseline(args, case, budget)
+        if i >= args.warmup:
+            vals.append(cb["seconds_per_solve"])
+    sec = statistics.mean(vals)
+    v = 1.0 / sec
+    out = {
+        "metric": METRIC, "value": v, "unit": "solves/s", "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": sec * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded SplitMix64)",
+        "config": {"workload": f"{args.workload} {args.n}^3 projection, tol {args.tol:g}", "grid": args.n},
+        "impl": "reference",
+        "cpu_baseline": {"value": v, "unit": "solves/s", "cores": cb["cores"], "kind": "port",
+                         "sample": cb["sample"]},
+        "e2e": {"value": v, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(out), flush=True)
+
+
+# ---------------------------------------------------------------------------
+def run_ours(args, rank, world, local_rank):
+    import torch
+    import torch.distributed as dist
+
+    from mydemcfd_b200 import _native as nat
+    from mydemcfd_b200 import workloads as W
+    from mydemcfd_b200.solver import B200PressureSolver, DeviceGrid, ibm_solid_fraction_device
+
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
+
+    case = build_case(args, solid_fraction=lambda N, h, o, s: ibm_solid_fraction_device(N, h, o, s).cpu().numpy())
+    g = DeviceGrid.from_case(case, device=dev)
+    sh = W.shapes(case.N)
+    stream = torch.cuda.current_stream()
+
+    def solver(precision):
+        s = B200PressureSolver(case.N, case.h, precision=precision, tol=args.tol)
+        s.set_coefficients(g)
+        return s
+
+    s_mixed = solver(nat.PRECISION_MIXED)
+    s_plain = solver(nat.PRECISION_FP64)
+    out_v = [torch.zeros(sh[k], dtype=torch.float64, device=dev) for k in "xyz"]
+    pd = torch.zeros(sh["cell"], dtype=torch.float64, device=dev)
+
+    def step(s):
+        return s.project(g.f_vx_star_, g.f_vy_star_, g.f_vz_star_, case.dt, pd, *out_v)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def max_over_ranks(x):
+        if world > 1:
+            t = torch.tensor([x], dtype=torch.float64, device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            return float(t.item())
+        return x
+
+    def timed(fn, k):
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        barrier()
+        torch.cuda.synchronize()
+        ev0.record(stream)
+        stats = [fn() for _ in range(k)]
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        barrier()
+        return max_over_ranks(ev0.elapsed_time(ev1)), stats
+
+    for _ in range(args.warmup):
+        step(s_mixed)
+        step(s_plain)
+    torch.cuda.synchronize()
+
+    with ClockSampler(torch.cuda.current_device()) as clk:
+        ms_mixed, st_mixed = timed(lambda: step(s_mixed), args.steps)
+    ms_plain, st_plain = timed(lambda: step(s_plain), args.steps)
+    sps_mixed = world * args.steps / (ms_mixed / 1e3)
+    sps_plain = world * args.steps / (ms_plain / 1e3)
+
+    # end to end through the C ABI with host buffers: pinned u* in, u and p_delta out
+    e2e = None
+    if not args.no_e2e:
+        host_in = [torch.from_numpy(np.ascontiguousarray(a)).pin_memory() for a in (case.vxs, case.vys, case.vzs)]
+        host_out = [torch.empty(sh[k], dtype=torch.float64).pin_memory() for k in "xyz"] + \
+                   [torch.empty(sh["cell"], dtype=torch.float64).pin_memory()]
+        dev_in = [torch.empty_like(t, device=dev) for t in host_in]
+
+        def e2e_step():
+            for d, h in zip(dev_in, host_in):
+                d.copy_(h, non_blocking=True)
+            st = s_mixed.project(*dev_in, case.dt, pd, *out_v)
+            for h, d in zip(host_out, out_v + [pd]):
+                h.copy_(d, non_blocking=True)
+            return st
+
+        for _ in range(max(1, args.warmup // 2)):
+            e2e_step()
+        ms_e2e, _ = timed(e2e_step, args.steps)
+        e2e = {"value": world * args.steps / (ms_e2e / 1e3), "unit": "solves/s",
+               "h2d_bytes_per_step": int(sum(t.numel() * 8 for t in host_in)),
+               "d2h_bytes_per_step": int(sum(t.numel() * 8 for t in host_out))}
+
+    # roofline of the dominant kernel (fine-grid FP32 red-black Gauss-Seidel sweep
+    # in the mixed solve), timed with CUDA events on the solver's stream
+    peak, peak_kind = measured_peaks()
+    step(s_mixed)
+    ms_k, bytes_k = s_mixed.time_kernel(3, reps=20)
+    achieved = bytes_k / (ms_k / 1e3) / 1e9
+    traffic = ncu_traffic().get("rbgs_f32_sweep_256")
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "traffic": traffic, "kernel": "k_rbgs<float,float> red+black sweep, 256^3 fine grid",
+                "peak_kind": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else peak_kind,
+                "alg_bytes_per_launch": bytes_k / 2, "ms_per_launch": ms_k / 2}
+    kernel_table = {}
+    for kid, name in ((0, "matvec_f64"), (1, "matvec_f32"), (2, "rbgs_sweep_f64"), (3, "rbgs_sweep_f32"),
+                      (4, "true_residual_f64")):
+        ms, b = s_mixed.time_kernel(kid, reps=10)
+        kernel_table[name] = {"ms": ms, "GB/s": b / (ms / 1e3) / 1e9}
+
+    launches = int(sum(s["kernel_launches"] for s in st_mixed))
+    res = {
+        "metric": METRIC, "value": sps_mixed, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_mixed / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32+f64 (mixed)", "data": "synthetic (seeded SplitMix64 U[-1,1) faces)",
+        "config": {"workload": f"{args.workload} {args.n}^3 projection (divergence + MG-PCG to {args.tol:g} + "
+                               f"correction), replicas per GPU", "grid": args.n, "tol": args.tol,
+                   "l2": "working set > L2 (coefficients alone 3x139 MB at 256^3)", "parallelism": f"replicas x{world}"},
+        "plain_fp64": {"value": sps_plain, "ms_per_step": ms_plain / args.steps,
+                       "iterations": st_plain[-1]["iterations"], "rel_residual": st_plain[-1]["rel_residual"]},
+        "mixed": {"iterations": st_mixed[-1]["iterations"], "reliable_updates": st_mixed[-1]["reliable_updates"],
+                  "rel_residual": st_mixed[-1]["rel_residual"], "levels": st_mixed[-1]["num_levels"],
+                  "alg_bytes_per_solve": st_mixed[-1]["alg_bytes"],
+                  "alg_GBps": st_mixed[-1]["alg_bytes"] * args.steps / (ms_mixed / 1e3) / 1e9},
+        "speedup_mixed_vs_plain": sps_mixed / sps_plain,
+        "e2e": e2e,
+        "gpu_launches": launches,
+        "roofline": roofline,
+        "kernels": kernel_table,
+        "clocks": clk.summary(),
+    }
+    if rank == 0 and world == 1 and not args.no_cpu:
+        res["cpu_baseline"] = cpu_baseline(args, case, args.cpu_budget)
+        res["cpu_baseline"].pop("seconds_per_solve", None)
+    if rank == 0:
+        print(json.dumps(res), flush=True)
+    s_mixed.close()
+    s_plain.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank)
+        return
+    run_ours(args, rank, world, local_rank)
+
+
+if __name__ == "__main__":
+    main()

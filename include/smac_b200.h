@@ -1,0 +1,225 @@
+/*
+ * smac_b200.h -- C ABI of the B200-native SMAC pressure projection.
+ *
+ * A drop-in for the reference's pressure-solver seam
+ *   struct G_PressureSolverBase { virtual void solve(G_SMACSolver&) = 0; ... }
+ *   (CFD/pressure_solver/G_PressureSolverBase.h:24-42)
+ * and for the calls on either side of it: the Poisson right-hand side
+ * (G_PressureSolverBase.cu:49-118), the velocity correction
+ * (CFD/G_SMACSolver.cu:1072-1142,1269-1275), the VoF face-coefficient update
+ * (CFD/G_SMACSolver_VoF.cu:1374-1535) and the IBM solid mask
+ * (CFD/G_SMACSolver_IBM.cu:94-147,763-792).
+ *
+ * Conventions
+ *  - Every array argument is a DEVICE pointer in the reference layout
+ *    (MyArray<T,3>, x fastest, index (z*sy + y)*sx + x, CFD/MyArray.h:43-51):
+ *      cells   (Nx+2)(Ny+2)(Nz+2)   x-faces (Nx+3)(Ny+2)(Nz+2)
+ *      y-faces (Nx+2)(Ny+3)(Nz+2)   z-faces (Nx+2)(Ny+2)(Nz+3)
+ *    (CFD/memberList/gridMembers.def), doubles and unsigned chars exactly as
+ *    G_StaggeredGrid holds them.  Type codes are CFD/Enums.h:3-23.
+ *  - Every call returns an smac_status; 0 is success.  Nothing aborts.
+ *    smac_last_error_string() describes the last failure of this thread.
+ *  - A handle owns its stream (given at creation), its multigrid hierarchy,
+ *    its coefficients and all scratch; caller arrays are only borrowed for
+ *    the duration of a call.  One handle must not be used from two threads
+ *    at once.  Calls are asynchronous on the handle's stream except where a
+ *    smac_stats is requested, which ends with one stream synchronisation.
+ */
+#ifndef SMAC_B200_H
+#define SMAC_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct smac_handle smac_handle;
+
+typedef enum {
+  SMAC_OK = 0,
+  SMAC_NOT_CONVERGED = 1, /* tolerance not met within max_iter (reference: silent stop, G_PCGSolver.cu:788) */
+  SMAC_BREAKDOWN = 2,     /* p.Ap <= 0 or r.z <= 0 inside PCG */
+  SMAC_NAN = 3,           /* a non-finite value reached a reduction */
+  SMAC_BAD_ARG = 4,       /* null pointer, bad option value */
+  SMAC_BAD_SHAPE = 5,     /* grid sizes the hierarchy cannot use (reference: abort(), G_GMGSolver.cu:38-51) */
+  SMAC_CUDA_ERROR = 6,    /* a CUDA runtime call failed */
+  SMAC_NO_DEVICE = 7      /* no usable sm_100 device */
+} smac_status;
+
+/* Solver variants: the same four the reference selects with
+ * G_PCGSolver::set_solver(PCG_TYPES) (G_PCGSolver.cu:592-613, CFD/Enums.h:25-30). */
+typedef enum {
+  SMAC_STANDARD_PCG = 0,             /* Jacobi-preconditioned CG                (solve_pcg :448-586) */
+  SMAC_PURENEUMANN_STANDARD_PCG = 1, /* ... with zero-mean projection          (solve_pureneumann_pcg :307-445) */
+  SMAC_GMG_PCG = 2,                  /* multigrid-preconditioned CG            (solve_gmgpcg :619-770) */
+  SMAC_PURENEUMANN_GMG_PCG = 3       /* ... with zero-mean projection          (solve_pureneumann_gmgpcg :772-922) */
+} smac_solver_type;
+
+typedef enum {
+  SMAC_PRECISION_FP64 = 0,  /* every vector, coefficient and reduction in FP64 */
+  SMAC_PRECISION_MIXED = 1  /* FP32 Krylov vectors, matvec and V-cycle (BF16 coefficients on the
+                               coarsest grids), FP64 true residual, solution, reductions,
+                               zero-mean projection and coefficient assembly */
+} smac_precision;
+
+typedef enum {
+  SMAC_STOP_RELATIVE = 0,  /* ||b - A x||_2 / ||b||_2 < tol (b de-meaned for pure Neumann) */
+  SMAC_STOP_REFERENCE = 1  /* max|b - A x| * dt < tol: the reference's test (G_PCGSolver.cu:884-903),
+                              dt being the one passed to smac_divergence */
+} smac_stop_rule;
+
+typedef struct {
+  int nx, ny, nz;     /* interior cells: G_StaggeredGrid::Nx_, Ny_, Nz_ */
+  double dx, dy, dz;  /* spacing: G_StaggeredGrid::dx_, dy_, dz_ */
+} smac_grid_desc;
+
+typedef struct {
+  int solver_type;        /* smac_solver_type, default SMAC_PURENEUMANN_GMG_PCG */
+  int precision;          /* smac_precision, default SMAC_PRECISION_FP64 */
+  int stop_rule;          /* smac_stop_rule, default SMAC_STOP_RELATIVE */
+  double tol;             /* default 1e-8; the reference's tol_ (G_PressureSolverBase.h:40) */
+  int max_iter;           /* PCG iteration cap, default 2000 (G_PCGSolver.cu:788) */
+  int min_coarse;         /* a direction is halved while the result stays >= min_coarse and even
+                             (default 8; the reference's min_size_ is 6, G_GMGSolver.h:22) */
+  int max_levels;         /* grids in the hierarchy including the finest, default 16 (MAX_LEVELS) */
+  int nu1, nu2;           /* red-black Gauss-Seidel pre/post sweeps per level, default 2/2 */
+  int coarse_sweeps;      /* symmetric sweep pairs on the coarsest grid, default 24 */
+  int check_every;        /* residual tests every check_every iterations (device side), default 1 */
+  double reliable_delta;  /* MIXED: recompute the FP64 true residual when the FP32 residual has
+                             fallen by this factor since the last recomputation, default 1e-2 */
+  int bf16_coarse_cells;  /* MIXED: grids with at most this many cells store BF16 coefficients
+                             (default 4096, i.e. 16^3 and below); 0 disables BF16 */
+} smac_options;
+
+typedef struct {
+  int status;              /* smac_status of the solve */
+  int iterations;          /* PCG iterations (preconditioner applications) */
+  int reliable_updates;    /* MIXED: FP64 true-residual recomputations */
+  int num_levels;          /* grids in the multigrid hierarchy */
+  double norm_b;           /* ||b||_2 after the zero-mean projection */
+  double rel_residual;     /* ||b - A x||_2 / ||b||_2 at exit, FP64 operator */
+  double max_residual;     /* max |b - A x| at exit */
+  double alg_bytes;        /* algorithmic HBM bytes of the kernels launched (byte model) */
+  int kernel_launches;     /* kernels launched by the call */
+} smac_stats;
+
+/* ---- lifetime ----------------------------------------------------------- */
+
+/* Fill *opts with the defaults listed above. */
+smac_status smac_default_options(smac_options* opts);
+
+/* Allocate a solver for the grid on the current CUDA device.  stream may be
+ * NULL (legacy default stream).  Replaces the set-up in CFD/main.cu:225-243
+ * (G_PCGSolver + G_GMGSolver::initialize, G_GMGSolver.cu:10-147). */
+smac_status smac_create(const smac_grid_desc* desc, const smac_options* opts, void* cuda_stream,
+                        smac_handle** out);
+smac_status smac_destroy(smac_handle* h);
+/* Change solver options between solves (hierarchy options are fixed at creation). */
+smac_status smac_set_options(smac_handle* h, const smac_options* opts);
+const char* smac_last_error_string(void);
+/* Number of grids in the hierarchy and the interior size of grid `level`. */
+smac_status smac_level_shape(const smac_handle* h, int level, int* nx, int* ny, int* nz, int* num_levels);
+
+/* ---- coefficients --------------------------------------------------------- */
+
+/* Import the Poisson face coefficients f_b and the cell/face types.
+ * Replaces k_build_vof_poisson_A (G_PCGSolver.cu:126-212) and
+ * G_GMGSolver::create_coeffs (G_GMGSolver.cu:913-922): the fine operator is
+ * A_c = sum_faces f_b/h^2 (diagonal) minus f_b/h^2 per F_INTERIOR face; rows of
+ * cells that are not C_INTERIOR are zero; coarse grids are built in FP64.
+ * fbx/fby/fbz: x/y/z-face doubles; celltype: cell bytes; fxt/fyt/fzt: face bytes. */
+smac_status smac_set_coefficients(smac_handle* h, const double* fbx, const double* fby, const double* fbz,
+                                  const uint8_t* celltype, const uint8_t* fxt, const uint8_t* fyt,
+                                  const uint8_t* fzt);
+
+/* Cell and face types of an all-wall box: SMACSolver::set_face_type and
+ * set_cell_type (CFD/SMACSolver.cpp:104-248). */
+smac_status smac_box_types(const smac_grid_desc* desc, uint8_t* celltype, uint8_t* fxt, uint8_t* fyt,
+                           uint8_t* fzt, void* cuda_stream);
+
+/* VoF density and face coefficients from the volume fraction alpha:
+ * k_update_cell_properties_by_alpha + k_update_{x,y,z}_face_properties_by_alpha
+ * (CFD/G_SMACSolver_VoF.cu:1374-1535), FP64.  rho: cells (written on
+ * C_INTERIOR / C_NEAR_BOUNDARY cells); fb*: f_b; fir*: f_inv_rho (may be NULL). */
+smac_status smac_assemble_vof(const smac_grid_desc* desc, const double* alpha, double rho0, double rho1,
+                              const uint8_t* celltype, const uint8_t* fxt, const uint8_t* fyt,
+                              const uint8_t* fzt, double* rho, double* fbx, double* fby, double* fbz,
+                              double* firx, double* firy, double* firz, void* cuda_stream);
+
+/* IBM solid fraction of cells 1..N+1 by 8^3 sub-sampling
+ * (k_get_solid_fraction, CFD/G_SMACSolver_IBM.cu:94-147, clip >= 0.99 -> 1)
+ * for a union of non-overlapping spheres (x, y, z, r per sphere, HOST array
+ * of 4*num_spheres doubles) in place of the reference's cylinder. */
+smac_status smac_ibm_solid_fraction_spheres(const smac_grid_desc* desc, const double origin[3],
+                                            const double* spheres_host, int num_spheres, double* solid_fraction,
+                                            void* cuda_stream);
+/* k_set_solid_cell_from_ibm (CFD/G_SMACSolver_IBM.cu:763-792): cells with
+ * solid fraction > 1-1e-12 become C_SOLID and their six faces F_BOUNDARY. */
+smac_status smac_ibm_set_solid_cells(const smac_grid_desc* desc, const double* solid_fraction, uint8_t* celltype,
+                                     uint8_t* fxt, uint8_t* fyt, uint8_t* fzt, void* cuda_stream);
+
+/* ---- the projection ------------------------------------------------------- */
+
+/* Right-hand side, base_k_make_poisson_rhs (G_PressureSolverBase.cu:49-118):
+ *   rhs = -(1/dt) div(eps u*) - (eps - eps_old)/dt^2 - div(f_b f_s)   on C_INTERIOR cells, 0 elsewhere.
+ * eps/eps_old NULL means eps == 1 (so the second term vanishes); fsx/fsy/fsz
+ * NULL means no surface-tension force.  Uses the coefficients of the last
+ * smac_set_coefficients.  rhs_out (cells, may be NULL) receives the RHS in the
+ * reference layout (interior entries).  dt is also the dt of SMAC_STOP_REFERENCE. */
+smac_status smac_divergence(smac_handle* h, const double* vxs, const double* vys, const double* vzs,
+                            const double* eps, const double* eps_old, const double* fsx, const double* fsy,
+                            const double* fsz, double dt, double* rhs_out);
+
+/* Solve A p_delta = rhs for the RHS of the last smac_divergence (or
+ * smac_set_rhs).  Replaces G_PressureSolverBase::solve -> G_PCGSolver::solve
+ * (G_SMACSolver.cu:1499-1501, G_PCGSolver.cu:615-617).  Pure-Neumann variants
+ * project b and the result onto zero mean over the fluid (C_INTERIOR) cells.
+ * p_delta: cells, interior entries written (ghosts untouched).  stats may be
+ * NULL (then the call does not synchronise). */
+smac_status smac_solve(smac_handle* h, double* p_delta, smac_stats* stats);
+
+/* Supply the RHS directly (cells, reference layout, interior entries read). */
+smac_status smac_set_rhs(smac_handle* h, const double* rhs);
+
+/* Velocity correction, k_correct_vof_velocity + correct_vof_velocity
+ * (G_SMACSolver.cu:1072-1142,1269-1275): on F_INTERIOR faces
+ *   u = u* + f_inv_rho dt (f_s - grad p_delta),
+ * p += p_delta on C_INTERIOR cells (p may be NULL), then p_delta is zeroed
+ * when zero_p_delta != 0 (the reference always zeroes it).  Faces that are
+ * not F_INTERIOR are not written.  fs* may be NULL; fir* NULL means use f_b. */
+smac_status smac_correct(smac_handle* h, double* p_delta, double* p, const double* vxs, const double* vys,
+                         const double* vzs, const double* firx, const double* firy, const double* firz,
+                         const double* fsx, const double* fsy, const double* fsz, double dt, double* vx,
+                         double* vy, double* vz, int zero_p_delta);
+
+/* divergence -> solve -> correction in one call (eps == 1, no f_s, f_inv_rho = f_b).
+ * p_delta receives the pressure increment (not zeroed); faces that are not
+ * F_INTERIOR receive u* so that (vx,vy,vz) is the projected field everywhere. */
+smac_status smac_project(smac_handle* h, const double* vxs, const double* vys, const double* vzs, double dt,
+                         double* p_delta, double* vx, double* vy, double* vz, smac_stats* stats);
+
+/* Adjoint of smac_project with respect to u*: given g = dL/du (faces) returns
+ * dL/du* = g + G A^+ D(B g) on F_INTERIOR faces (g elsewhere), one more MG-PCG
+ * solve with the same operator (A is symmetric).  phi (cells, may be NULL)
+ * receives the adjoint pressure. */
+smac_status smac_project_adjoint(smac_handle* h, const double* gvx, const double* gvy, const double* gvz,
+                                 double* gvxs, double* gvys, double* gvzs, double* phi, smac_stats* stats);
+
+/* y = A x with the FP64 fine operator (cells, reference layout, interior
+ * entries); the reference's k_build_vof_poisson_Ap (G_PCGSolver.cu:214-245). */
+smac_status smac_apply_A(smac_handle* h, const double* x, double* y);
+
+/* Time `reps` launches of one kernel of the solve on the handle's stream with
+ * CUDA events (kernel ids: 0 FP64 matvec+dot, 1 FP32 matvec+dot, 2 FP64 RB-GS
+ * sweep, 3 FP32 RB-GS sweep, 4 FP64 true residual, 5 divergence, 6 correction)
+ * on the finest grid.  Writes the mean milliseconds per launch and the
+ * algorithmic bytes of one launch. */
+smac_status smac_time_kernel(smac_handle* h, int kernel_id, int reps, float* ms_per_launch,
+                             double* alg_bytes_per_launch);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SMAC_B200_H */

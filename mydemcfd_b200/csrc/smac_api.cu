@@ -1,0 +1,1043 @@
+// smac_api.cu -- host side of the B200-native SMAC pressure projection:
+// handle, multigrid hierarchy, CUDA-graph PCG iterations and the C ABI
+// declared in include/smac_b200.h.
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <vector>
+
+#include "smac_b200.h"
+#include "smac_kernels.cuh"
+
+using namespace smac;
+
+namespace {
+
+thread_local char g_err[512] = "";
+
+void set_err(const char* fmt, ...) {
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(g_err, sizeof(g_err), fmt, ap);
+  va_end(ap);
+}
+
+#define CK(call)                                                                          \
+  do {                                                                                    \
+    cudaError_t e_ = (call);                                                              \
+    if (e_ != cudaSuccess) {                                                              \
+      set_err("%s:%d: %s: %s", __FILE__, __LINE__, #call, cudaGetErrorString(e_));        \
+      return SMAC_CUDA_ERROR;                                                             \
+    }                                                                                     \
+  } while (0)
+
+#define CKL()                                                                             \
+  do {                                                                                    \
+    cudaError_t e_ = cudaGetLastError();                                                  \
+    if (e_ != cudaSuccess) {                                                              \
+      set_err("%s:%d: kernel launch: %s", __FILE__, __LINE__, cudaGetErrorString(e_));    \
+      return SMAC_CUDA_ERROR;                                                             \
+    }                                                                                     \
+  } while (0)
+
+#define TRY(expr)                       \
+  do {                                  \
+    smac_status st_ = (expr);           \
+    if (st_ != SMAC_OK) return st_;     \
+  } while (0)
+
+constexpr int MAXL = 16;
+constexpr int COARSE_CELLS = 4096;  // grids at or below this size run in the single-CTA kernel
+
+enum CoefType { CT_F64 = 0, CT_F32 = 1, CT_BF16 = 2 };
+
+struct Level {
+  Geom g{};
+  int cx = 0, cy = 0, cz = 0;  // coarsened from the grid above
+  double *bx64 = nullptr, *by64 = nullptr, *bz64 = nullptr;
+  double *x64 = nullptr, *rhs64 = nullptr;  // levels >= 1
+  void *bxm = nullptr, *bym = nullptr, *bzm = nullptr;  // mixed-precision coefficients
+  int ctm = CT_F32;
+  float *x32 = nullptr, *rhs32 = nullptr;   // levels >= 1
+};
+
+}  // namespace
+
+struct smac_handle {
+  smac_grid_desc desc{};
+  smac_options opts{};
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  RefDims R{};
+  int nlev = 0;
+  int lc = 0;  // first grid of the single-CTA coarse set
+  Level lv[MAXL];
+  uint8_t* fluid = nullptr;   // padded cell bits: 1 C_INTERIOR, 2 fluid unknown
+  double nfluid = 0.0;
+  // copies of the reference-layout types (the correction and the adjoint read them)
+  uint8_t *ct = nullptr, *fxt = nullptr, *fyt = nullptr, *fzt = nullptr;
+  // fine FP64 vectors
+  double *b64 = nullptr, *x64a = nullptr, *x64b = nullptr, *r64 = nullptr, *z64 = nullptr, *d64 = nullptr,
+         *q64 = nullptr, *tmp64 = nullptr;
+  // fine FP32 vectors (mixed)
+  float *r32 = nullptr, *z32 = nullptr, *d32 = nullptr, *q32 = nullptr, *e32 = nullptr;
+  RedBuf red{};
+  Scalars* s = nullptr;    // device
+  Scalars* hs = nullptr;   // pinned host mirror
+  cudaGraphExec_t graph[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};  // [precision][gmg]
+  bool have_coeffs = false, have_rhs = false;
+  double dt = 1.0;
+  double alg_bytes = 0.0;
+  int launches = 0;
+  std::vector<void*> allocs;
+};
+
+namespace {
+
+template <class T>
+smac_status dalloc(smac_handle* h, T** p, long long n) {
+  void* q = nullptr;
+  CK(cudaMalloc(&q, sizeof(T) * (size_t)n));
+  CK(cudaMemsetAsync(q, 0, sizeof(T) * (size_t)n, h->stream));
+  h->allocs.push_back(q);
+  *p = (T*)q;
+  return SMAC_OK;
+}
+
+// Padded array: returns the pointer to idx(0,0,0) (guard zeros in front).
+template <class T>
+smac_status palloc(smac_handle* h, const Geom& g, T** p) {
+  T* base = nullptr;
+  TRY(dalloc(h, &base, g.alloc));
+  *p = base + g.guard;
+  return SMAC_OK;
+}
+
+template <class T>
+T* base_of(const Geom& g, T* p) {
+  return p - g.guard;
+}
+
+inline int kz_for(const Geom& g) { return g.nz >= 64 ? 16 : (g.nz >= 16 ? 8 : 4); }
+inline dim3 grid_cells(const Geom& g, int kz) {
+  return dim3((g.nx + TBX - 1) / TBX, (g.ny + TBY - 1) / TBY, (g.nz + kz - 1) / kz);
+}
+inline dim3 grid_pairs(const Geom& g, int kz) {
+  return dim3(((g.nx + 1) / 2 + TBX - 1) / TBX, (g.ny + TBY - 1) / TBY, (g.nz + kz - 1) / kz);
+}
+inline dim3 grid_planes(int nx, int ny, int nz) { return dim3((nx + TBX - 1) / TBX, (ny + TBY - 1) / TBY, nz); }
+const dim3 kBlock(TBX, TBY, 1);
+
+template <class T, class C>
+Stencil<T, C> stencil(const Geom& g, const void* bx, const void* by, const void* bz) {
+  typedef acc_t<T> A;
+  return Stencil<T, C>{(const C*)bx, (const C*)by, (const C*)bz, (A)g.ihx2, (A)g.ihy2, (A)g.ihz2};
+}
+
+smac_status validate_options(const smac_options* o) {
+  if (!o) { set_err("options: null"); return SMAC_BAD_ARG; }
+  if (o->solver_type < 0 || o->solver_type > 3) { set_err("options: solver_type %d", o->solver_type); return SMAC_BAD_ARG; }
+  if (o->precision < 0 || o->precision > 1) { set_err("options: precision %d", o->precision); return SMAC_BAD_ARG; }
+  if (o->stop_rule < 0 || o->stop_rule > 1) { set_err("options: stop_rule %d", o->stop_rule); return SMAC_BAD_ARG; }
+  if (!(o->tol > 0.0) || !std::isfinite(o->tol)) { set_err("options: tol must be > 0"); return SMAC_BAD_ARG; }
+  if (o->max_iter < 1) { set_err("options: max_iter must be >= 1"); return SMAC_BAD_ARG; }
+  if (o->min_coarse < 2) { set_err("options: min_coarse must be >= 2"); return SMAC_BAD_ARG; }
+  if (o->max_levels < 1 || o->max_levels > MAXL) { set_err("options: max_levels in [1,16]"); return SMAC_BAD_ARG; }
+  if (o->nu1 < 1 || o->nu2 < 1 || o->nu1 > 16 || o->nu2 > 16) { set_err("options: nu1, nu2 in [1,16]"); return SMAC_BAD_ARG; }
+  if (o->coarse_sweeps < 1 || o->coarse_sweeps > 1024) { set_err("options: coarse_sweeps in [1,1024]"); return SMAC_BAD_ARG; }
+  if (o->check_every < 1) { set_err("options: check_every >= 1"); return SMAC_BAD_ARG; }
+  if (!(o->reliable_delta > 0.0 && o->reliable_delta < 1.0)) { set_err("options: reliable_delta in (0,1)"); return SMAC_BAD_ARG; }
+  return SMAC_OK;
+}
+
+bool is_gmg(const smac_options& o) { return o.solver_type == SMAC_GMG_PCG || o.solver_type == SMAC_PURENEUMANN_GMG_PCG; }
+bool is_pure(const smac_options& o) {
+  return o.solver_type == SMAC_PURENEUMANN_GMG_PCG || o.solver_type == SMAC_PURENEUMANN_STANDARD_PCG;
+}
+
+// BF16 coefficients on the single-CTA grids when they are small enough and
+// do not include the finest grid (whose mixed copy is FP32).
+bool use_bf16(const smac_handle* h, const smac_options& o) {
+  return h->lc >= 1 && o.bf16_coarse_cells > 0 && h->lv[h->lc].g.cells() <= o.bf16_coarse_cells;
+}
+
+void account(smac_handle* h, const Geom& g, double bytes_per_cell, int n = 1) {
+  h->alg_bytes += bytes_per_cell * (double)g.cells() * n;
+  h->launches += n;
+}
+
+// ---------------------------------------------------------------------------
+// V-cycle launch sequence.  T: vector type, CS: coefficient type of the
+// separately launched grids, CC: coefficient type of the single-CTA set.
+template <class T, class CS, class CC>
+smac_status launch_vcycle(smac_handle* h, T* r0, T* z0, bool mixed) {
+  const smac_options& o = h->opts;
+  const int lc = h->lc;
+  const double* shift0 = &h->s->rshift;
+  const double s = sizeof(T);
+  const double sc = mixed ? (double)sizeof(CS) : 8.0;
+  auto X = [&](int l) -> T* { return l == 0 ? z0 : (mixed ? (T*)h->lv[l].x32 : (T*)h->lv[l].x64); };
+  auto B = [&](int l) -> T* { return l == 0 ? r0 : (mixed ? (T*)h->lv[l].rhs32 : (T*)h->lv[l].rhs64); };
+  auto CF = [&](int l, int which) -> const void* {
+    const Level& L = h->lv[l];
+    if (!mixed) return which == 0 ? (const void*)L.bx64 : which == 1 ? (const void*)L.by64 : (const void*)L.bz64;
+    return which == 0 ? L.bxm : which == 1 ? L.bym : L.bzm;
+  };
+  for (int l = 0; l < lc; ++l) {
+    const Level& L = h->lv[l];
+    const Geom& g = L.g;
+    const int kz = kz_for(g);
+    auto S = stencil<T, CS>(g, CF(l, 0), CF(l, 1), CF(l, 2));
+    const double* sh = (l == 0) ? shift0 : nullptr;
+    for (int it = 0; it < o.nu1; ++it) {
+      k_rbgs<T, CS><<<grid_pairs(g, kz), kBlock, 0, h->stream>>>(g, X(l), B(l), sh, S, 0, it == 0, (const T*)nullptr,
+                                                                  g, 0, 0, 0, h->s, kz);
+      k_rbgs<T, CS><<<grid_pairs(g, kz), kBlock, 0, h->stream>>>(g, X(l), B(l), sh, S, 1, 0, (const T*)nullptr, g, 0,
+                                                                  0, 0, h->s, kz);
+      account(h, g, (it == 0 ? 4.0 : 6.0) * s + 6 * sc, 2);
+    }
+    CKL();
+    const Level& Lc = h->lv[l + 1];
+    k_resid_restrict<T, CS><<<grid_planes(Lc.g.nx, Lc.g.ny, Lc.g.nz), kBlock, 0, h->stream>>>(
+        g, X(l), B(l), sh, S, Lc.g, Lc.cx, Lc.cy, Lc.cz, B(l + 1), h->s);
+    account(h, g, 2 * s + 3 * sc + s / 8, 1);
+    CKL();
+  }
+  // single-CTA coarse set
+  {
+    CoarseSet set{};
+    set.n = h->nlev - lc;
+    for (int q = 0; q < set.n; ++q) {
+      const int l = lc + q;
+      CoarseLevel& C = set.L[q];
+      C.g = h->lv[l].g;
+      C.cx = h->lv[l].cx; C.cy = h->lv[l].cy; C.cz = h->lv[l].cz;
+      C.bx = CF(l, 0); C.by = CF(l, 1); C.bz = CF(l, 2);
+      C.x = X(l);
+      C.rhs = B(l);
+    }
+    k_coarse_vcycle<T, CC><<<1, 1024, 0, h->stream>>>(set, o.nu1, o.nu2, o.coarse_sweeps, lc == 0 ? shift0 : nullptr,
+                                                       h->s);
+    h->launches += 1;
+    CKL();
+  }
+  for (int l = lc - 1; l >= 0; --l) {
+    const Level& L = h->lv[l];
+    const Geom& g = L.g;
+    const int kz = kz_for(g);
+    auto S = stencil<T, CS>(g, CF(l, 0), CF(l, 1), CF(l, 2));
+    const double* sh = (l == 0) ? shift0 : nullptr;
+    const Level& Lc = h->lv[l + 1];
+    for (int it = 0; it < o.nu2; ++it) {
+      k_rbgs<T, CS><<<grid_pairs(g, kz), kBlock, 0, h->stream>>>(g, X(l), B(l), sh, S, 1, 0,
+                                                                  it == 0 ? (const T*)X(l + 1) : (const T*)nullptr,
+                                                                  Lc.g, Lc.cx, Lc.cy, Lc.cz, h->s, kz);
+      k_rbgs<T, CS><<<grid_pairs(g, kz), kBlock, 0, h->stream>>>(g, X(l), B(l), sh, S, 0, 0, (const T*)nullptr, g, 0,
+                                                                  0, 0, h->s, kz);
+      account(h, g, 6.0 * s + 6 * sc + (it == 0 ? s / 8 : 0.0), 2);
+    }
+    CKL();
+  }
+  return SMAC_OK;
+}
+
+// One PCG iteration: preconditioner, r.z and beta, direction, matvec and
+// alpha, update (+ FP64 residual recomputation in mixed precision).
+smac_status launch_iteration(smac_handle* h, bool mixed, bool gmg) {
+  const Geom& g = h->lv[0].g;
+  const int kz = kz_for(g);
+  const dim3 gr = grid_cells(g, kz);
+  if (!mixed) {
+    if (gmg) {
+      TRY((launch_vcycle<double, double, double>(h, h->r64, h->z64, false)));
+    } else {
+      auto S = stencil<double, double>(g, h->lv[0].bx64, h->lv[0].by64, h->lv[0].bz64);
+      k_jacobi_precond<double, double><<<gr, kBlock, 0, h->stream>>>(g, h->r64, &h->s->rshift, S, h->z64, h->s, kz);
+      account(h, g, 2 * 8 + 3 * 8);
+    }
+    k_dot_rz<double><<<gr, kBlock, 0, h->stream>>>(g, h->r64, h->z64, h->red, h->s, kz);
+    k_dir<double><<<gr, kBlock, 0, h->stream>>>(g, h->z64, h->d64, h->s, kz);
+    auto S = stencil<double, double>(g, h->lv[0].bx64, h->lv[0].by64, h->lv[0].bz64);
+    k_matvec_pap<double, double><<<gr, kBlock, 0, h->stream>>>(g, h->d64, S, h->q64, h->red, h->s, kz);
+    k_update<double, double><<<gr, kBlock, 0, h->stream>>>(g, h->x64a, h->d64, h->r64, h->q64, h->red, h->s, kz);
+    account(h, g, 16, 1);
+    account(h, g, 24, 1);
+    account(h, g, 5 * 8, 1);
+    account(h, g, 6 * 8, 1);
+    CKL();
+  } else {
+    const bool bf16 = use_bf16(h, h->opts);
+    if (gmg) {
+      if (bf16) {
+        TRY((launch_vcycle<float, float, __nv_bfloat16>(h, h->r32, h->z32, true)));
+      } else {
+        TRY((launch_vcycle<float, float, float>(h, h->r32, h->z32, true)));
+      }
+    } else {
+      auto S = stencil<float, float>(g, h->lv[0].bxm, h->lv[0].bym, h->lv[0].bzm);
+      k_jacobi_precond<float, float><<<gr, kBlock, 0, h->stream>>>(g, h->r32, &h->s->rshift, S, h->z32, h->s, kz);
+      account(h, g, 2 * 4 + 3 * 4);
+    }
+    k_dot_rz<float><<<gr, kBlock, 0, h->stream>>>(g, h->r32, h->z32, h->red, h->s, kz);
+    k_dir<float><<<gr, kBlock, 0, h->stream>>>(g, h->z32, h->d32, h->s, kz);
+    auto S = stencil<float, float>(g, h->lv[0].bxm, h->lv[0].bym, h->lv[0].bzm);
+    k_matvec_pap<float, float><<<gr, kBlock, 0, h->stream>>>(g, h->d32, S, h->q32, h->red, h->s, kz);
+    k_update<float, float><<<gr, kBlock, 0, h->stream>>>(g, h->e32, h->d32, h->r32, h->q32, h->red, h->s, kz);
+    auto S64 = stencil<double, double>(g, h->lv[0].bx64, h->lv[0].by64, h->lv[0].bz64);
+    k_reliable<float><<<gr, kBlock, 0, h->stream>>>(g, h->x64a, h->x64b, h->e32, h->b64, S64, h->r32, h->red, h->s, kz);
+    account(h, g, 8, 1);
+    account(h, g, 12, 1);
+    account(h, g, 5 * 4, 1);
+    account(h, g, 6 * 4, 1);
+    h->launches += 1;  // the FP64 residual kernel (its bytes are counted when it runs)
+    CKL();
+  }
+  return SMAC_OK;
+}
+
+smac_status get_graph(smac_handle* h, bool mixed, bool gmg, cudaGraphExec_t* out) {
+  cudaGraphExec_t& ex = h->graph[mixed ? 1 : 0][gmg ? 1 : 0];
+  if (!ex) {
+    cudaGraph_t graph = nullptr;
+    const double saved_bytes = h->alg_bytes;
+    const int saved_launches = h->launches;
+    CK(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+    smac_status st = launch_iteration(h, mixed, gmg);
+    cudaError_t ec = cudaStreamEndCapture(h->stream, &graph);
+    h->alg_bytes = saved_bytes;
+    h->launches = saved_launches;
+    if (st != SMAC_OK) {
+      if (graph) cudaGraphDestroy(graph);
+      return st;
+    }
+    if (ec != cudaSuccess) {
+      set_err("stream capture: %s", cudaGetErrorString(ec));
+      return SMAC_CUDA_ERROR;
+    }
+    cudaError_t ei = cudaGraphInstantiate(&ex, graph, 0);
+    cudaGraphDestroy(graph);
+    if (ei != cudaSuccess) {
+      ex = nullptr;
+      set_err("graph instantiate: %s", cudaGetErrorString(ei));
+      return SMAC_CUDA_ERROR;
+    }
+  }
+  *out = ex;
+  return SMAC_OK;
+}
+
+void drop_graphs(smac_handle* h) {
+  for (auto& a : h->graph)
+    for (auto& e : a)
+      if (e) { cudaGraphExecDestroy(e); e = nullptr; }
+}
+
+// Per-iteration accounting (bytes of one iteration), measured once by a dry
+// accounting pass.
+double iteration_bytes(smac_handle* h, bool mixed, bool gmg, int* launches) {
+  const double b0 = h->alg_bytes;
+  const int l0 = h->launches;
+  // count without launching: replicate the accounting of launch_iteration
+  const Geom& g = h->lv[0].g;
+  double bytes = 0.0;
+  int n = 0;
+  const double s = mixed ? 4.0 : 8.0, sc = mixed ? 4.0 : 8.0;
+  if (gmg) {
+    for (int l = 0; l < h->lc; ++l) {
+      const double cells = (double)h->lv[l].g.cells();
+      const double scl = (l == 0 || !mixed) ? sc : 4.0;
+      for (int it = 0; it < h->opts.nu1; ++it) { bytes += ((it == 0 ? 4.0 : 6.0) * s + 6 * scl) * cells; n += 2; }
+      bytes += (2 * s + 3 * scl + s / 8) * cells; n += 1;
+      for (int it = 0; it < h->opts.nu2; ++it) { bytes += (6.0 * s + 6 * scl + (it == 0 ? s / 8 : 0.0)) * cells; n += 2; }
+    }
+    n += 1;
+  } else {
+    bytes += (2 * s + 3 * sc) * (double)g.cells();
+    n += 1;
+  }
+  bytes += (2 * s + 3 * s + 5 * s + 6 * s) * (double)g.cells();
+  n += 4;
+  if (mixed) n += 1;
+  h->alg_bytes = b0;
+  h->launches = l0;
+  if (launches) *launches = n;
+  return bytes;
+}
+
+}  // namespace
+
+// ===========================================================================
+extern "C" {
+
+const char* smac_last_error_string(void) { return g_err; }
+
+smac_status smac_default_options(smac_options* o) {
+  if (!o) { set_err("null options"); return SMAC_BAD_ARG; }
+  o->solver_type = SMAC_PURENEUMANN_GMG_PCG;
+  o->precision = SMAC_PRECISION_FP64;
+  o->stop_rule = SMAC_STOP_RELATIVE;
+  o->tol = 1e-8;
+  o->max_iter = 2000;
+  o->min_coarse = 8;
+  o->max_levels = 16;
+  o->nu1 = 2;
+  o->nu2 = 2;
+  o->coarse_sweeps = 24;
+  o->check_every = 1;
+  o->reliable_delta = 1e-2;
+  o->bf16_coarse_cells = COARSE_CELLS;
+  return SMAC_OK;
+}
+
+smac_status smac_create(const smac_grid_desc* desc, const smac_options* opts, void* cuda_stream, smac_handle** out) {
+  if (!desc || !out) { set_err("smac_create: null argument"); return SMAC_BAD_ARG; }
+  *out = nullptr;
+  smac_options o;
+  if (opts) o = *opts; else smac_default_options(&o);
+  TRY(validate_options(&o));
+  if (desc->nx < 2 || desc->ny < 2 || desc->nz < 2 || !(desc->dx > 0) || !(desc->dy > 0) || !(desc->dz > 0)) {
+    set_err("smac_create: grid %dx%dx%d, spacing must be > 0", desc->nx, desc->ny, desc->nz);
+    return SMAC_BAD_SHAPE;
+  }
+  int dev = -1;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) { set_err("smac_create: no CUDA device: %s", cudaGetErrorString(e)); return SMAC_NO_DEVICE; }
+  cudaDeviceProp prop;
+  CK(cudaGetDeviceProperties(&prop, dev));
+  if (prop.major != 10) {
+    set_err("smac_create: device %s is sm_%d%d; this library is built for sm_100a", prop.name, prop.major, prop.minor);
+    return SMAC_NO_DEVICE;
+  }
+  smac_handle* h = new (std::nothrow) smac_handle();
+  if (!h) { set_err("smac_create: out of host memory"); return SMAC_BAD_ARG; }
+  h->desc = *desc;
+  h->opts = o;
+  h->R = RefDims{desc->nx, desc->ny, desc->nz};
+  if (cuda_stream) {
+    h->stream = (cudaStream_t)cuda_stream;
+  } else {
+    // a blocking stream: ordered with work on the legacy default stream, and capturable
+    cudaError_t es = cudaStreamCreate(&h->stream);
+    if (es != cudaSuccess) { set_err("cudaStreamCreate: %s", cudaGetErrorString(es)); delete h; return SMAC_CUDA_ERROR; }
+    h->own_stream = true;
+  }
+  auto fail = [&](smac_status st) {
+    char keep[512];
+    memcpy(keep, g_err, sizeof(keep));
+    smac_destroy(h);
+    memcpy(g_err, keep, sizeof(keep));
+    return st;
+  };
+  // hierarchy: halve a direction while it stays even and >= min_coarse
+  {
+    int nx = desc->nx, ny = desc->ny, nz = desc->nz;
+    double ix2 = 1.0 / (desc->dx * desc->dx), iy2 = 1.0 / (desc->dy * desc->dy), iz2 = 1.0 / (desc->dz * desc->dz);
+    h->lv[0].g = make_geom(nx, ny, nz, ix2, iy2, iz2);
+    h->nlev = 1;
+    while (h->nlev < o.max_levels && is_gmg(o)) {
+      const int cx = (nx % 2 == 0 && nx / 2 >= o.min_coarse), cy = (ny % 2 == 0 && ny / 2 >= o.min_coarse),
+                cz = (nz % 2 == 0 && nz / 2 >= o.min_coarse);
+      if (!cx && !cy && !cz) break;
+      if (cx) { nx /= 2; ix2 *= 0.25; }
+      if (cy) { ny /= 2; iy2 *= 0.25; }
+      if (cz) { nz /= 2; iz2 *= 0.25; }
+      Level& L = h->lv[h->nlev];
+      L.g = make_geom(nx, ny, nz, ix2, iy2, iz2);
+      L.cx = cx; L.cy = cy; L.cz = cz;
+      h->nlev += 1;
+    }
+    h->lc = h->nlev - 1;
+    for (int l = 0; l < h->nlev; ++l)
+      if (h->lv[l].g.cells() <= COARSE_CELLS) { h->lc = l; break; }
+    if (h->lv[0].g.alloc >= (1LL << 31)) { set_err("smac_create: grid too large for 32-bit indexing"); return fail(SMAC_BAD_SHAPE); }
+  }
+  // storage
+  const Geom& g0 = h->lv[0].g;
+  smac_status st;
+#define PA(ptr) do { st = palloc(h, g0, &(ptr)); if (st != SMAC_OK) return fail(st); } while (0)
+  PA(h->lv[0].bx64); PA(h->lv[0].by64); PA(h->lv[0].bz64);
+  PA(h->b64); PA(h->x64a); PA(h->x64b); PA(h->r64); PA(h->z64); PA(h->d64); PA(h->q64); PA(h->tmp64);
+  {
+    float* p;
+    st = palloc(h, g0, &p); if (st != SMAC_OK) return fail(st); h->lv[0].bxm = p;
+    st = palloc(h, g0, &p); if (st != SMAC_OK) return fail(st); h->lv[0].bym = p;
+    st = palloc(h, g0, &p); if (st != SMAC_OK) return fail(st); h->lv[0].bzm = p;
+    h->lv[0].ctm = CT_F32;
+  }
+  PA(h->r32); PA(h->z32); PA(h->d32); PA(h->q32); PA(h->e32);
+  PA(h->fluid);
+#undef PA
+  {
+    const long long nc = (long long)(desc->nx + 2) * (desc->ny + 2) * (desc->nz + 2);
+    const long long nxf = (long long)(desc->nx + 3) * (desc->ny + 2) * (desc->nz + 2);
+    const long long nyf = (long long)(desc->nx + 2) * (desc->ny + 3) * (desc->nz + 2);
+    const long long nzf = (long long)(desc->nx + 2) * (desc->ny + 2) * (desc->nz + 3);
+    if ((st = dalloc(h, &h->ct, nc)) || (st = dalloc(h, &h->fxt, nxf)) || (st = dalloc(h, &h->fyt, nyf)) ||
+        (st = dalloc(h, &h->fzt, nzf)))
+      return fail(st);
+  }
+  for (int l = 1; l < h->nlev; ++l) {
+    Level& L = h->lv[l];
+    const Geom& g = L.g;
+    if ((st = palloc(h, g, &L.bx64)) || (st = palloc(h, g, &L.by64)) || (st = palloc(h, g, &L.bz64)) ||
+        (st = palloc(h, g, &L.x64)) || (st = palloc(h, g, &L.rhs64)) || (st = palloc(h, g, &L.x32)) ||
+        (st = palloc(h, g, &L.rhs32)))
+      return fail(st);
+    const bool bf16 = use_bf16(h, o) && l >= h->lc;
+    if (bf16) {
+      __nv_bfloat16* p;
+      if ((st = palloc(h, g, &p))) return fail(st); L.bxm = p;
+      if ((st = palloc(h, g, &p))) return fail(st); L.bym = p;
+      if ((st = palloc(h, g, &p))) return fail(st); L.bzm = p;
+      L.ctm = CT_BF16;
+    } else {
+      float* p;
+      if ((st = palloc(h, g, &p))) return fail(st); L.bxm = p;
+      if ((st = palloc(h, g, &p))) return fail(st); L.bym = p;
+      if ((st = palloc(h, g, &p))) return fail(st); L.bzm = p;
+      L.ctm = CT_F32;
+    }
+  }
+  // reductions: the largest reducing launch is a fine-grid cell launch
+  {
+    long long maxb = 0;
+    for (int l = 0; l < h->nlev; ++l) {
+      const dim3 gr = grid_cells(h->lv[l].g, kz_for(h->lv[l].g));
+      maxb = std::max(maxb, (long long)gr.x * gr.y * gr.z);
+      const dim3 gp = grid_planes(h->lv[l].g.nx, h->lv[l].g.ny, h->lv[l].g.nz);
+      maxb = std::max(maxb, (long long)gp.x * gp.y * gp.z);
+    }
+    if ((st = dalloc(h, &h->red.partials, maxb * 4 + 64))) return fail(st);
+    if ((st = dalloc(h, &h->red.ticket, 64))) return fail(st);
+  }
+  if ((st = dalloc(h, &h->s, 1))) return fail(st);
+  {
+    cudaError_t eh = cudaMallocHost((void**)&h->hs, sizeof(Scalars));
+    if (eh != cudaSuccess) { set_err("cudaMallocHost: %s", cudaGetErrorString(eh)); return fail(SMAC_CUDA_ERROR); }
+    memset(h->hs, 0, sizeof(Scalars));
+  }
+  cudaError_t es = cudaStreamSynchronize(h->stream);
+  if (es != cudaSuccess) { set_err("smac_create: %s", cudaGetErrorString(es)); return fail(SMAC_CUDA_ERROR); }
+  *out = h;
+  return SMAC_OK;
+}
+
+smac_status smac_destroy(smac_handle* h) {
+  if (!h) return SMAC_OK;
+  if (h->stream) cudaStreamSynchronize(h->stream);
+  drop_graphs(h);
+  for (void* p : h->allocs) cudaFree(p);
+  if (h->hs) cudaFreeHost(h->hs);
+  if (h->own_stream && h->stream) cudaStreamDestroy(h->stream);
+  delete h;
+  return SMAC_OK;
+}
+
+smac_status smac_set_options(smac_handle* h, const smac_options* opts) {
+  if (!h || !opts) { set_err("smac_set_options: null argument"); return SMAC_BAD_ARG; }
+  TRY(validate_options(opts));
+  if (opts->min_coarse != h->opts.min_coarse || opts->max_levels != h->opts.max_levels ||
+      opts->bf16_coarse_cells != h->opts.bf16_coarse_cells || is_gmg(*opts) != is_gmg(h->opts)) {
+    set_err("smac_set_options: min_coarse, max_levels, bf16_coarse_cells and the GMG/Jacobi choice are fixed at creation");
+    return SMAC_BAD_ARG;
+  }
+  if (opts->nu1 != h->opts.nu1 || opts->nu2 != h->opts.nu2 || opts->coarse_sweeps != h->opts.coarse_sweeps) drop_graphs(h);
+  h->opts = *opts;
+  return SMAC_OK;
+}
+
+smac_status smac_level_shape(const smac_handle* h, int level, int* nx, int* ny, int* nz, int* num_levels) {
+  if (!h) { set_err("null handle"); return SMAC_BAD_ARG; }
+  if (num_levels) *num_levels = h->nlev;
+  if (level < 0 || level >= h->nlev) { set_err("level %d out of range", level); return SMAC_BAD_ARG; }
+  if (nx) *nx = h->lv[level].g.nx;
+  if (ny) *ny = h->lv[level].g.ny;
+  if (nz) *nz = h->lv[level].g.nz;
+  return SMAC_OK;
+}
+
+smac_status smac_set_coefficients(smac_handle* h, const double* fbx, const double* fby, const double* fbz,
+                                  const uint8_t* ct, const uint8_t* fxt, const uint8_t* fyt, const uint8_t* fzt) {
+  if (!h || !fbx || !fby || !fbz || !ct || !fxt || !fyt || !fzt) {
+    set_err("smac_set_coefficients: null argument");
+    return SMAC_BAD_ARG;
+  }
+  const Geom& g = h->lv[0].g;
+  {
+    const RefDims& R = h->R;
+    const size_t nc = (size_t)(R.Nx + 2) * (R.Ny + 2) * (R.Nz + 2);
+    const size_t nxf = (size_t)(R.Nx + 3) * (R.Ny + 2) * (R.Nz + 2);
+    const size_t nyf = (size_t)(R.Nx + 2) * (R.Ny + 3) * (R.Nz + 2);
+    const size_t nzf = (size_t)(R.Nx + 2) * (R.Ny + 2) * (R.Nz + 3);
+    CK(cudaMemcpyAsync(h->ct, ct, nc, cudaMemcpyDeviceToDevice, h->stream));
+    CK(cudaMemcpyAsync(h->fxt, fxt, nxf, cudaMemcpyDeviceToDevice, h->stream));
+    CK(cudaMemcpyAsync(h->fyt, fyt, nyf, cudaMemcpyDeviceToDevice, h->stream));
+    CK(cudaMemcpyAsync(h->fzt, fzt, nzf, cudaMemcpyDeviceToDevice, h->stream));
+  }
+  k_import_coeffs<<<grid_planes(g.nx + 1, g.ny + 1, g.nz + 1), kBlock, 0, h->stream>>>(
+      g, h->R, fbx, fby, fbz, ct, fxt, fyt, fzt, h->lv[0].bx64, h->lv[0].by64, h->lv[0].bz64, h->fluid);
+  CKL();
+  k_fluid_finalize<<<grid_planes(g.nx, g.ny, g.nz), kBlock, 0, h->stream>>>(g, h->lv[0].bx64, h->lv[0].by64,
+                                                                            h->lv[0].bz64, h->fluid, h->red, h->s);
+  CKL();
+  // FP32 fine copy for the mixed-precision Krylov operator
+  {
+    const long long n = g.alloc;
+    k_convert<float><<<1184, 256, 0, h->stream>>>(base_of(g, h->lv[0].bx64), base_of(g, (float*)h->lv[0].bxm), n);
+    k_convert<float><<<1184, 256, 0, h->stream>>>(base_of(g, h->lv[0].by64), base_of(g, (float*)h->lv[0].bym), n);
+    k_convert<float><<<1184, 256, 0, h->stream>>>(base_of(g, h->lv[0].bz64), base_of(g, (float*)h->lv[0].bzm), n);
+    CKL();
+  }
+  for (int l = 1; l < h->nlev; ++l) {
+    Level& F = h->lv[l - 1];
+    Level& L = h->lv[l];
+    const dim3 gr = grid_planes(L.g.nx + 1, L.g.ny + 1, L.g.nz + 1);
+    k_coarsen_coeffs<double><<<gr, kBlock, 0, h->stream>>>(F.g, L.g, L.cx, L.cy, L.cz, F.bx64, F.by64, F.bz64, L.bx64,
+                                                           L.by64, L.bz64, nullptr, nullptr, nullptr);
+    CKL();
+    const long long n = L.g.alloc;
+    if (L.ctm == CT_BF16) {
+      k_convert<__nv_bfloat16><<<256, 256, 0, h->stream>>>(base_of(L.g, L.bx64), base_of(L.g, (__nv_bfloat16*)L.bxm), n);
+      k_convert<__nv_bfloat16><<<256, 256, 0, h->stream>>>(base_of(L.g, L.by64), base_of(L.g, (__nv_bfloat16*)L.bym), n);
+      k_convert<__nv_bfloat16><<<256, 256, 0, h->stream>>>(base_of(L.g, L.bz64), base_of(L.g, (__nv_bfloat16*)L.bzm), n);
+    } else {
+      k_convert<float><<<256, 256, 0, h->stream>>>(base_of(L.g, L.bx64), base_of(L.g, (float*)L.bxm), n);
+      k_convert<float><<<256, 256, 0, h->stream>>>(base_of(L.g, L.by64), base_of(L.g, (float*)L.bym), n);
+      k_convert<float><<<256, 256, 0, h->stream>>>(base_of(L.g, L.bz64), base_of(L.g, (float*)L.bzm), n);
+    }
+    CKL();
+  }
+  CK(cudaMemcpyAsync(h->hs, h->s, sizeof(Scalars), cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  h->nfluid = h->hs->sum_tmp;
+  h->have_coeffs = true;
+  return SMAC_OK;
+}
+
+smac_status smac_box_types(const smac_grid_desc* d, uint8_t* ct, uint8_t* fxt, uint8_t* fyt, uint8_t* fzt,
+                           void* stream) {
+  if (!d || !ct || !fxt || !fyt || !fzt) { set_err("smac_box_types: null argument"); return SMAC_BAD_ARG; }
+  RefDims R{d->nx, d->ny, d->nz};
+  k_box_types<<<grid_planes(d->nx + 3, d->ny + 3, d->nz + 3), kBlock, 0, (cudaStream_t)stream>>>(R, ct, fxt, fyt, fzt);
+  CKL();
+  return SMAC_OK;
+}
+
+smac_status smac_assemble_vof(const smac_grid_desc* d, const double* alpha, double rho0, double rho1, const uint8_t* ct,
+                              const uint8_t* fxt, const uint8_t* fyt, const uint8_t* fzt, double* rho, double* fbx,
+                              double* fby, double* fbz, double* firx, double* firy, double* firz, void* stream) {
+  if (!d || !alpha || !ct || !fxt || !fyt || !fzt || !rho || !fbx || !fby || !fbz) {
+    set_err("smac_assemble_vof: null argument");
+    return SMAC_BAD_ARG;
+  }
+  RefDims R{d->nx, d->ny, d->nz};
+  cudaStream_t s = (cudaStream_t)stream;
+  k_vof_rho<<<grid_planes(d->nx + 1, d->ny + 1, d->nz + 1), kBlock, 0, s>>>(R, alpha, rho0, rho1, ct, rho);
+  CKL();
+  k_vof_faces<<<grid_planes(d->nx + 2, d->ny + 2, d->nz + 2), kBlock, 0, s>>>(R, rho, fxt, fyt, fzt, fbx, fby, fbz,
+                                                                                firx, firy, firz);
+  CKL();
+  return SMAC_OK;
+}
+
+smac_status smac_ibm_solid_fraction_spheres(const smac_grid_desc* d, const double origin[3], const double* spheres,
+                                            int nsph, double* sf, void* stream) {
+  if (!d || !origin || (!spheres && nsph > 0) || nsph < 0 || !sf) {
+    set_err("smac_ibm_solid_fraction_spheres: bad argument");
+    return SMAC_BAD_ARG;
+  }
+  RefDims R{d->nx, d->ny, d->nz};
+  cudaStream_t s = (cudaStream_t)stream;
+  double* dsph = nullptr;
+  if (nsph > 0) {
+    CK(cudaMallocAsync((void**)&dsph, sizeof(double) * 4 * nsph, s));
+    CK(cudaMemcpyAsync(dsph, spheres, sizeof(double) * 4 * nsph, cudaMemcpyHostToDevice, s));
+  }
+  k_ibm_spheres<<<grid_planes(d->nx + 1, d->ny + 1, d->nz + 1), kBlock, 0, s>>>(R, d->dx, d->dy, d->dz, origin[0],
+                                                                                  origin[1], origin[2], dsph, nsph, sf);
+  CKL();
+  if (dsph) CK(cudaFreeAsync(dsph, s));
+  CK(cudaStreamSynchronize(s));
+  return SMAC_OK;
+}
+
+smac_status smac_ibm_set_solid_cells(const smac_grid_desc* d, const double* sf, uint8_t* ct, uint8_t* fxt, uint8_t* fyt,
+                                     uint8_t* fzt, void* stream) {
+  if (!d || !sf || !ct || !fxt || !fyt || !fzt) { set_err("smac_ibm_set_solid_cells: null argument"); return SMAC_BAD_ARG; }
+  RefDims R{d->nx, d->ny, d->nz};
+  k_ibm_set_solid<<<grid_planes(d->nx + 1, d->ny + 1, d->nz + 1), kBlock, 0, (cudaStream_t)stream>>>(R, sf, ct, fxt, fyt,
+                                                                                                       fzt);
+  CKL();
+  return SMAC_OK;
+}
+
+smac_status smac_divergence(smac_handle* h, const double* vxs, const double* vys, const double* vzs, const double* eps,
+                            const double* eps_old, const double* fsx, const double* fsy, const double* fsz, double dt,
+                            double* rhs_out) {
+  if (!h || !vxs || !vys || !vzs) { set_err("smac_divergence: null argument"); return SMAC_BAD_ARG; }
+  if (!h->have_coeffs) { set_err("smac_divergence: call smac_set_coefficients first"); return SMAC_BAD_ARG; }
+  if ((eps == nullptr) != (eps_old == nullptr)) { set_err("smac_divergence: eps and eps_old go together"); return SMAC_BAD_ARG; }
+  if (!((fsx && fsy && fsz) || (!fsx && !fsy && !fsz))) { set_err("smac_divergence: fsx/fsy/fsz go together"); return SMAC_BAD_ARG; }
+  if (!(dt > 0) || !std::isfinite(dt)) { set_err("smac_divergence: dt must be > 0"); return SMAC_BAD_ARG; }
+  const Geom& g = h->lv[0].g;
+  k_divergence<<<grid_planes(g.nx, g.ny, g.nz), kBlock, 0, h->stream>>>(
+      g, h->R, 1.0 / h->desc.dx, 1.0 / h->desc.dy, 1.0 / h->desc.dz, 1.0 / dt, vxs, vys, vzs, eps, eps_old,
+      h->lv[0].bx64, h->lv[0].by64, h->lv[0].bz64, fsx, fsy, fsz, h->fluid, h->b64, rhs_out);
+  CKL();
+  h->dt = dt;
+  h->have_rhs = true;
+  return SMAC_OK;
+}
+
+smac_status smac_set_rhs(smac_handle* h, const double* rhs) {
+  if (!h || !rhs) { set_err("smac_set_rhs: null argument"); return SMAC_BAD_ARG; }
+  const Geom& g = h->lv[0].g;
+  k_import_cells<double><<<grid_planes(g.nx, g.ny, g.nz), kBlock, 0, h->stream>>>(g, h->R, rhs, h->b64);
+  CKL();
+  h->have_rhs = true;
+  return SMAC_OK;
+}
+
+namespace {
+
+// Solve A x = b for the padded b64; leaves the solution (not yet de-meaned)
+// in *xout and the scalars on the host mirror.
+smac_status run_solve(smac_handle* h, const double** xout) {
+  const smac_options& o = h->opts;
+  const bool mixed = o.precision == SMAC_PRECISION_MIXED;
+  const bool gmg = is_gmg(o);
+  const bool pure = is_pure(o);
+  const Geom& g = h->lv[0].g;
+  const int kz = kz_for(g);
+  const size_t bytes = sizeof(double) * (size_t)g.alloc;
+  h->alg_bytes = 0.0;
+  h->launches = 0;
+  // device scalars that the set-up kernel does not write
+  Scalars init{};
+  init.max_iter = o.max_iter;
+  init.stop_rule = o.stop_rule;
+  init.tol_max = o.tol / h->dt;
+  init.reliable_delta2 = o.reliable_delta * o.reliable_delta;
+  init.inv_nfluid = (pure && h->nfluid > 0) ? 1.0 / h->nfluid : 0.0;
+  init.mixed = mixed ? 1 : 0;
+  *h->hs = init;
+  CK(cudaMemcpyAsync(h->s, h->hs, sizeof(Scalars), cudaMemcpyHostToDevice, h->stream));
+  CK(cudaMemsetAsync(base_of(g, h->x64a), 0, bytes, h->stream));
+  if (mixed) {
+    CK(cudaMemsetAsync(base_of(g, h->x64b), 0, bytes, h->stream));
+    CK(cudaMemsetAsync(base_of(g, h->d32), 0, sizeof(float) * (size_t)g.alloc, h->stream));
+    CK(cudaMemsetAsync(base_of(g, h->e32), 0, sizeof(float) * (size_t)g.alloc, h->stream));
+  } else {
+    CK(cudaMemsetAsync(base_of(g, h->d64), 0, bytes, h->stream));
+  }
+  const dim3 gp = grid_planes(g.nx, g.ny, g.nz);
+  k_setup_sum<double><<<gp, kBlock, 0, h->stream>>>(g, h->b64, h->red, h->s);
+  if (mixed)
+    k_setup_project<float><<<gp, kBlock, 0, h->stream>>>(g, h->b64, h->fluid, h->r32, h->red, h->s, o.tol);
+  else
+    k_setup_project<double><<<gp, kBlock, 0, h->stream>>>(g, h->b64, h->fluid, h->r64, h->red, h->s, o.tol);
+  CKL();
+  account(h, g, 8, 1);
+  account(h, g, 8 + 8 + (mixed ? 4 : 8) + 1, 1);
+  cudaGraphExec_t ex = nullptr;
+  TRY(get_graph(h, mixed, gmg, &ex));
+  int per_launch = 0;
+  const double per_bytes = iteration_bytes(h, mixed, gmg, &per_launch);
+  int restarts = 0;
+  int launched = 0;
+  const int max_launches = o.max_iter + 8;
+  for (;;) {
+    if (launched > max_launches) {  // the device sets done by max_iter; this is a second bound
+      set_err("run_solve: iteration bound exceeded without a device decision");
+      return SMAC_NOT_CONVERGED;
+    }
+    // launch a batch of iterations; kernels after convergence return at once
+    int batch = 2;
+    for (int q = 0; q < batch; ++q) CK(cudaGraphLaunch(ex, h->stream));
+    launched += batch;
+    CK(cudaMemcpyAsync(h->hs, h->s, sizeof(Scalars), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    if (h->hs->done) {
+      if (!mixed && h->hs->status == 0) {
+        // verify the recursive residual with the FP64 true residual
+        auto S = stencil<double, double>(g, h->lv[0].bx64, h->lv[0].by64, h->lv[0].bz64);
+        k_true_residual<<<grid_cells(g, kz), kBlock, 0, h->stream>>>(g, h->x64a, h->b64, S, h->r64, 0, h->red, h->s, kz);
+        CKL();
+        account(h, g, 5 * 8, 1);
+        CK(cudaMemcpyAsync(h->hs, h->s, sizeof(Scalars), cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+        const Scalars& hs = *h->hs;
+        const bool ok = (o.stop_rule == 1) ? (hs.true_rmax < hs.tol_max) : (hs.true_rr <= hs.tol2bb);
+        if (!ok && hs.iter < o.max_iter && restarts < 3) {
+          // restart PCG from the true residual
+          ++restarts;
+          k_true_residual<<<grid_cells(g, kz), kBlock, 0, h->stream>>>(g, h->x64a, h->b64, S, h->r64, 1, h->red, h->s,
+                                                                        kz);
+          CKL();
+          account(h, g, 6 * 8, 1);
+          CK(cudaMemsetAsync(base_of(g, h->d64), 0, bytes, h->stream));
+          CK(cudaMemcpyAsync(h->hs, h->s, sizeof(Scalars), cudaMemcpyDeviceToHost, h->stream));
+          CK(cudaStreamSynchronize(h->stream));
+          h->hs->done = 0;
+          h->hs->first = 1;
+          h->hs->status = 0;
+          CK(cudaMemcpyAsync(h->s, h->hs, sizeof(Scalars), cudaMemcpyHostToDevice, h->stream));
+          continue;
+        }
+      }
+      break;
+    }
+  }
+  // accounting: iterations actually executed (early-exited launches move no data)
+  {
+    const int it = h->hs->iter;
+    h->alg_bytes += per_bytes * it;
+    h->launches += per_launch * launched;
+    if (mixed) {
+      h->alg_bytes += (double)h->hs->reliable_count * (8 + 4 + 3 * 8 + 8 + 8 + 4) * (double)g.cells();
+    }
+  }
+  if (!mixed) {
+    *xout = h->x64a;
+  } else {
+    *xout = h->hs->xbuf ? h->x64b : h->x64a;
+  }
+  if (mixed || h->hs->status != 0) {
+    // true residual of the final iterate (mixed: already computed unless
+    // the solve stopped without a final recomputation)
+    auto S = stencil<double, double>(g, h->lv[0].bx64, h->lv[0].by64, h->lv[0].bz64);
+    k_true_residual<<<grid_cells(g, kz), kBlock, 0, h->stream>>>(g, *xout, h->b64, S, h->r64, 0, h->red, h->s, kz);
+    CKL();
+    account(h, g, 5 * 8, 1);
+    CK(cudaMemcpyAsync(h->hs, h->s, sizeof(Scalars), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+  }
+  return SMAC_OK;
+}
+
+void fill_stats(smac_handle* h, smac_stats* st) {
+  if (!st) return;
+  const Scalars& hs = *h->hs;
+  st->status = hs.status;
+  st->iterations = hs.iter;
+  st->reliable_updates = hs.reliable_count;
+  st->num_levels = is_gmg(h->opts) ? h->nlev : 0;
+  st->norm_b = std::sqrt(hs.bb);
+  st->rel_residual = hs.bb > 0 ? std::sqrt(hs.true_rr / hs.bb) : 0.0;
+  st->max_residual = hs.true_rmax;
+  st->alg_bytes = h->alg_bytes;
+  st->kernel_launches = h->launches;
+}
+
+// x -> reference-layout p_delta, zero-mean over fluid cells for pure Neumann.
+smac_status export_solution(smac_handle* h, const double* x, double* p_delta) {
+  const Geom& g = h->lv[0].g;
+  const dim3 gp = grid_planes(g.nx, g.ny, g.nz);
+  const bool pure = is_pure(h->opts);
+  if (pure) {
+    k_sum_fluid<<<gp, kBlock, 0, h->stream>>>(g, x, h->fluid, h->red, h->s);
+    CKL();
+  }
+  k_export_cells<<<gp, kBlock, 0, h->stream>>>(g, h->R, x, h->fluid, pure ? &h->s->sum_tmp : nullptr, p_delta);
+  CKL();
+  account(h, g, pure ? 8 + 1 + 8 + 1 + 8 : 16, pure ? 2 : 1);
+  return SMAC_OK;
+}
+
+}  // namespace
+
+smac_status smac_solve(smac_handle* h, double* p_delta, smac_stats* stats) {
+  if (!h || !p_delta) { set_err("smac_solve: null argument"); return SMAC_BAD_ARG; }
+  if (!h->have_coeffs || !h->have_rhs) { set_err("smac_solve: coefficients and rhs are required first"); return SMAC_BAD_ARG; }
+  const double* x = nullptr;
+  TRY(run_solve(h, &x));
+  TRY(export_solution(h, x, p_delta));
+  if (stats) {
+    CK(cudaMemcpyAsync(h->hs, h->s, sizeof(Scalars), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    fill_stats(h, stats);
+  }
+  const int status = h->hs->status;
+  if (status != 0) {
+    set_err("smac_solve: %s after %d iterations (relative residual %.3e)",
+            status == 1 ? "not converged" : status == 2 ? "breakdown" : "non-finite value", h->hs->iter,
+            h->hs->bb > 0 ? std::sqrt(h->hs->true_rr / h->hs->bb) : 0.0);
+  }
+  return (smac_status)status;
+}
+
+smac_status smac_correct(smac_handle* h, double* p_delta, double* p, const double* vxs, const double* vys,
+                         const double* vzs, const double* firx, const double* firy, const double* firz,
+                         const double* fsx, const double* fsy, const double* fsz, double dt, double* vx, double* vy,
+                         double* vz, int zero_p_delta) {
+  if (!h || !p_delta || !vxs || !vys || !vzs || !vx || !vy || !vz) { set_err("smac_correct: null argument"); return SMAC_BAD_ARG; }
+  if (!h->have_coeffs) { set_err("smac_correct: coefficients required"); return SMAC_BAD_ARG; }
+  if (!((firx && firy && firz) || (!firx && !firy && !firz))) { set_err("smac_correct: fir* go together"); return SMAC_BAD_ARG; }
+  if (!((fsx && fsy && fsz) || (!fsx && !fsy && !fsz))) { set_err("smac_correct: fs* go together"); return SMAC_BAD_ARG; }
+  const Geom& g = h->lv[0].g;
+  const RefDims& R = h->R;
+  k_correct<<<grid_planes(R.Nx + 2, R.Ny + 2, R.Nz + 2), kBlock, 0, h->stream>>>(
+      R, g, 1.0 / h->desc.dx, 1.0 / h->desc.dy, 1.0 / h->desc.dz, dt, h->ct, h->fxt, h->fyt, h->fzt, p_delta, p, vxs,
+      vys, vzs, firx, firy, firz, h->lv[0].bx64, h->lv[0].by64, h->lv[0].bz64, fsx, fsy, fsz, vx, vy, vz, 0);
+  CKL();
+  account(h, g, 3 * 8 + 8 + 3 * 8 + 3 * 8 + 3, 1);
+  if (zero_p_delta) {
+    const long long n = (long long)(R.Nx + 2) * (R.Ny + 2) * (R.Nz + 2);
+    CK(cudaMemsetAsync(p_delta, 0, sizeof(double) * (size_t)n, h->stream));
+  }
+  return SMAC_OK;
+}
+
+
+smac_status smac_project(smac_handle* h, const double* vxs, const double* vys, const double* vzs, double dt,
+                         double* p_delta, double* vx, double* vy, double* vz, smac_stats* stats) {
+  if (!h || !vxs || !vys || !vzs || !p_delta || !vx || !vy || !vz) { set_err("smac_project: null argument"); return SMAC_BAD_ARG; }
+  TRY(smac_divergence(h, vxs, vys, vzs, nullptr, nullptr, nullptr, nullptr, nullptr, dt, nullptr));
+  const double* x = nullptr;
+  TRY(run_solve(h, &x));
+  TRY(export_solution(h, x, p_delta));
+  const Geom& g = h->lv[0].g;
+  const RefDims& R = h->R;
+  k_correct<<<grid_planes(R.Nx + 2, R.Ny + 2, R.Nz + 2), kBlock, 0, h->stream>>>(
+      R, g, 1.0 / h->desc.dx, 1.0 / h->desc.dy, 1.0 / h->desc.dz, dt, h->ct, h->fxt, h->fyt, h->fzt, p_delta, nullptr,
+      vxs, vys, vzs, nullptr, nullptr, nullptr, h->lv[0].bx64, h->lv[0].by64, h->lv[0].bz64, nullptr, nullptr, nullptr,
+      vx, vy, vz, 1);
+  CKL();
+  account(h, g, 3 * 8 + 8 + 3 * 8 + 3 * 8 + 3, 1);
+  if (stats) {
+    CK(cudaStreamSynchronize(h->stream));
+    fill_stats(h, stats);
+  }
+  const int status = h->hs->status;
+  if (status != 0) set_err("smac_project: solve status %d after %d iterations", status, h->hs->iter);
+  return (smac_status)status;
+}
+
+smac_status smac_project_adjoint(smac_handle* h, const double* gvx, const double* gvy, const double* gvz, double* gvxs,
+                                 double* gvys, double* gvzs, double* phi, smac_stats* stats) {
+  if (!h || !gvx || !gvy || !gvz || !gvxs || !gvys || !gvzs) { set_err("smac_project_adjoint: null argument"); return SMAC_BAD_ARG; }
+  if (!h->have_coeffs) { set_err("smac_project_adjoint: coefficients required"); return SMAC_BAD_ARG; }
+  const Geom& g = h->lv[0].g;
+  const RefDims& R = h->R;
+  k_adj_divergence<<<grid_planes(g.nx, g.ny, g.nz), kBlock, 0, h->stream>>>(
+      g, R, 1.0 / h->desc.dx, 1.0 / h->desc.dy, 1.0 / h->desc.dz, gvx, gvy, gvz, h->lv[0].bx64, h->lv[0].by64,
+      h->lv[0].bz64, h->fluid, h->b64);
+  CKL();
+  h->have_rhs = true;
+  const double* x = nullptr;
+  TRY(run_solve(h, &x));
+  account(h, g, 3 * 8 + 3 * 8 + 1 + 8, 1);
+  const dim3 gp = grid_planes(g.nx, g.ny, g.nz);
+  k_sum_fluid<<<gp, kBlock, 0, h->stream>>>(g, x, h->fluid, h->red, h->s);
+  CKL();
+  if (!is_pure(h->opts)) {
+    // no null space: psi is the solution itself
+    CK(cudaMemsetAsync(&h->s->sum_tmp, 0, sizeof(double), h->stream));
+  }
+  k_adj_gradient<<<grid_planes(R.Nx + 3, R.Ny + 3, R.Nz + 3), kBlock, 0, h->stream>>>(
+      g, R, 1.0 / h->desc.dx, 1.0 / h->desc.dy, 1.0 / h->desc.dz, x, h->fluid, &h->s->sum_tmp, gvx, gvy, gvz, gvxs,
+      gvys, gvzs);
+  CKL();
+  account(h, g, 8 + 1 + 6 * 8, 2);
+  if (phi) {
+    k_export_cells<<<gp, kBlock, 0, h->stream>>>(g, R, x, h->fluid, is_pure(h->opts) ? &h->s->sum_tmp : nullptr, phi);
+    CKL();
+  }
+  if (stats) {
+    CK(cudaStreamSynchronize(h->stream));
+    fill_stats(h, stats);
+  }
+  const int status = h->hs->status;
+  if (status != 0) set_err("smac_project_adjoint: solve status %d after %d iterations", status, h->hs->iter);
+  return (smac_status)status;
+}
+
+smac_status smac_apply_A(smac_handle* h, const double* x, double* y) {
+  if (!h || !x || !y) { set_err("smac_apply_A: null argument"); return SMAC_BAD_ARG; }
+  if (!h->have_coeffs) { set_err("smac_apply_A: coefficients required"); return SMAC_BAD_ARG; }
+  const Geom& g = h->lv[0].g;
+  const dim3 gp = grid_planes(g.nx, g.ny, g.nz);
+  k_import_cells<double><<<gp, kBlock, 0, h->stream>>>(g, h->R, x, h->tmp64);
+  auto S = stencil<double, double>(g, h->lv[0].bx64, h->lv[0].by64, h->lv[0].bz64);
+  k_apply<<<gp, kBlock, 0, h->stream>>>(g, h->tmp64, S, h->q64);
+  k_export_cells<<<gp, kBlock, 0, h->stream>>>(g, h->R, h->q64, h->fluid, nullptr, y);
+  CKL();
+  return SMAC_OK;
+}
+
+smac_status smac_time_kernel(smac_handle* h, int kernel_id, int reps, float* ms, double* bytes) {
+  if (!h || !ms || !bytes || reps < 1) { set_err("smac_time_kernel: bad argument"); return SMAC_BAD_ARG; }
+  if (!h->have_coeffs) { set_err("smac_time_kernel: coefficients required"); return SMAC_BAD_ARG; }
+  const Geom& g = h->lv[0].g;
+  const int kz = kz_for(g);
+  // a state in which no kernel early-exits and the updates are no-ops
+  Scalars st{};
+  st.max_iter = 1 << 30;
+  st.inv_nfluid = 0.0;
+  st.rz = 1.0;
+  st.alpha = 0.0;
+  st.beta = 0.0;
+  *h->hs = st;
+  CK(cudaMemcpyAsync(h->s, h->hs, sizeof(Scalars), cudaMemcpyHostToDevice, h->stream));
+  cudaEvent_t e0, e1;
+  CK(cudaEventCreate(&e0));
+  CK(cudaEventCreate(&e1));
+  double per = 0.0;
+  auto launch = [&]() -> smac_status {
+    switch (kernel_id) {
+      case 0: {
+        auto S = stencil<double, double>(g, h->lv[0].bx64, h->lv[0].by64, h->lv[0].bz64);
+        k_matvec_pap<double, double><<<grid_cells(g, kz), kBlock, 0, h->stream>>>(g, h->d64, S, h->q64, h->red, h->s, kz);
+        per = 5 * 8.0;
+        break;
+      }
+      case 1: {
+        auto S = stencil<float, float>(g, h->lv[0].bxm, h->lv[0].bym, h->lv[0].bzm);
+        k_matvec_pap<float, float><<<grid_cells(g, kz), kBlock, 0, h->stream>>>(g, h->d32, S, h->q32, h->red, h->s, kz);
+        per = 5 * 4.0;
+        break;
+      }
+      case 2: {
+        auto S = stencil<double, double>(g, h->lv[0].bx64, h->lv[0].by64, h->lv[0].bz64);
+        k_rbgs<double, double><<<grid_pairs(g, kz), kBlock, 0, h->stream>>>(g, h->z64, h->r64, nullptr, S, 0, 0, nullptr, g, 0, 0, 0, h->s, kz);
+        k_rbgs<double, double><<<grid_pairs(g, kz), kBlock, 0, h->stream>>>(g, h->z64, h->r64, nullptr, S, 1, 0, nullptr, g, 0, 0, 0, h->s, kz);
+        per = 6 * 8.0;
+        break;
+      }
+      case 3: {
+        auto S = stencil<float, float>(g, h->lv[0].bxm, h->lv[0].bym, h->lv[0].bzm);
+        k_rbgs<float, float><<<grid_pairs(g, kz), kBlock, 0, h->stream>>>(g, h->z32, h->r32, nullptr, S, 0, 0, nullptr, g, 0, 0, 0, h->s, kz);
+        k_rbgs<float, float><<<grid_pairs(g, kz), kBlock, 0, h->stream>>>(g, h->z32, h->r32, nullptr, S, 1, 0, nullptr, g, 0, 0, 0, h->s, kz);
+        per = 6 * 4.0;
+        break;
+      }
+      case 4: {
+        auto S = stencil<double, double>(g, h->lv[0].bx64, h->lv[0].by64, h->lv[0].bz64);
+        k_true_residual<<<grid_cells(g, kz), kBlock, 0, h->stream>>>(g, h->x64a, h->b64, S, h->r64, 0, h->red, h->s, kz);
+        per = 5 * 8.0;
+        break;
+      }
+      default:
+        set_err("smac_time_kernel: unknown kernel id %d", kernel_id);
+        return SMAC_BAD_ARG;
+    }
+    CKL();
+    return SMAC_OK;
+  };
+  TRY(launch());  // warm-up
+  CK(cudaEventRecord(e0, h->stream));
+  for (int q = 0; q < reps; ++q) TRY(launch());
+  CK(cudaEventRecord(e1, h->stream));
+  CK(cudaEventSynchronize(e1));
+  float tot = 0.f;
+  CK(cudaEventElapsedTime(&tot, e0, e1));
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  *ms = tot / reps;
+  *bytes = per * (double)g.cells();
+  return SMAC_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,1161 @@
+// smac_kernels.cuh -- sm_100a kernels of the SMAC pressure projection.
+//
+// Operator.  For cell c with face coefficients b (x: bx[c] low, bx[c+1] high;
+// y: by[c], by[c+px]; z: bz[c], bz[c+ps]) and h-scales ih2:
+//   diag = sum of the six b*ih2,  off = sum of b*ih2*x_nb,  (A x)_c = diag x_c - off
+// which is the reference's k_build_vof_poisson_A / k_build_vof_poisson_Ap
+// (CFD/pressure_solver/G_PCGSolver.cu:126-245) without the seven stored
+// stencil arrays: the diagonal is recomputed from the three face arrays.
+//
+// Parity-critical element-wise kernels (divergence, correction, VoF and IBM
+// set-up) use __dadd_rn/__dmul_rn so that no multiply-add is contracted and
+// each result rounds exactly like the reference built with -fmad=false.
+#pragma once
+
+#include "smac_common.cuh"
+
+namespace smac {
+
+constexpr int TBX = 32;   // threads along x
+constexpr int TBY = 4;    // threads along y
+constexpr int TNT = TBX * TBY;
+
+template <class T> struct Acc { typedef T type; };
+template <class T> using acc_t = typename Acc<T>::type;
+
+#define DADD __dadd_rn
+#define DMUL __dmul_rn
+#define DDIV __ddiv_rn
+
+// ------------------------------------------------------------------------
+// Reference-layout index helpers (MyArray<T,3>: (z*sy + y)*sx + x).
+struct RefDims {
+  int Nx, Ny, Nz;
+  __host__ __device__ __forceinline__ long long cell(int x, int y, int z) const {
+    return ((long long)z * (Ny + 2) + y) * (Nx + 2) + x;
+  }
+  __host__ __device__ __forceinline__ long long xf(int x, int y, int z) const {
+    return ((long long)z * (Ny + 2) + y) * (Nx + 3) + x;
+  }
+  __host__ __device__ __forceinline__ long long yf(int x, int y, int z) const {
+    return ((long long)z * (Ny + 3) + y) * (Nx + 2) + x;
+  }
+  __host__ __device__ __forceinline__ long long zf(int x, int y, int z) const {
+    return ((long long)z * (Ny + 2) + y) * (Nx + 2) + x;
+  }
+};
+
+// ------------------------------------------------------------------------
+// Stencil pieces.
+template <class T, class C>
+struct Stencil {
+  typedef acc_t<T> A;
+  const C* __restrict__ bx;
+  const C* __restrict__ by;
+  const C* __restrict__ bz;
+  A ihx2, ihy2, ihz2;
+  __device__ __forceinline__ void coeffs(int c, int px, int ps, A& wxm, A& wxp, A& wym, A& wyp, A& wzm,
+                                         A& wzp) const {
+    wxm = (A)CoefLoad<C>::get(bx, c) * ihx2;
+    wxp = (A)CoefLoad<C>::get(bx, c + 1) * ihx2;
+    wym = (A)CoefLoad<C>::get(by, c) * ihy2;
+    wyp = (A)CoefLoad<C>::get(by, c + px) * ihy2;
+    wzm = (A)CoefLoad<C>::get(bz, c) * ihz2;
+    wzp = (A)CoefLoad<C>::get(bz, c + ps) * ihz2;
+  }
+};
+
+// ------------------------------------------------------------------------
+// Import of the reference-layout f_b into the padded fine arrays (FP64).
+// Face between cells a (low) and b (high): coefficient = f_b unless an
+// in-domain neighbour cell is not C_INTERIOR (the reference zeroes such rows,
+// G_PCGSolver.cu:156-166) or the face lies inside the domain and is not
+// F_INTERIOR (the reference's f_b is 0 there, CFD/G_SMACSolver_VoF.cu:1432-1436).
+// Domain-boundary faces keep f_b: with the zero ghost it enters only the
+// diagonal, as the reference's Adiag does (G_PCGSolver.cu:168-175).
+__global__ void k_import_coeffs(Geom g, RefDims R, const double* __restrict__ fbx, const double* __restrict__ fby,
+                                const double* __restrict__ fbz, const uint8_t* __restrict__ ct,
+                                const uint8_t* __restrict__ fxt, const uint8_t* __restrict__ fyt,
+                                const uint8_t* __restrict__ fzt, double* bx, double* by, double* bz,
+                                uint8_t* fluid) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int k = blockIdx.z;
+  if (i > g.nx || j > g.ny || k > g.nz) return;
+  const int c = g.idx(i, j, k);
+  auto interior_cell = [&](int ii, int jj, int kk) -> int {  // 1 C_INTERIOR, 0 other, -1 outside
+    if (ii < 0 || jj < 0 || kk < 0 || ii >= g.nx || jj >= g.ny || kk >= g.nz) return -1;
+    return ct[R.cell(ii + 1, jj + 1, kk + 1)] == C_INTERIOR ? 1 : 0;
+  };
+  // x-face i between cells i-1 and i
+  if (i <= g.nx && j < g.ny && k < g.nz) {
+    const int a = interior_cell(i - 1, j, k), b = interior_cell(i, j, k);
+    double v = fbx[R.xf(i + 1, j + 1, k + 1)];
+    if (a == 0 || b == 0) v = 0.0;
+    if (a == 1 && b == 1 && fxt[R.xf(i + 1, j + 1, k + 1)] != F_INTERIOR) v = 0.0;
+    bx[c] = v;
+  }
+  if (i < g.nx && j <= g.ny && k < g.nz) {
+    const int a = interior_cell(i, j - 1, k), b = interior_cell(i, j, k);
+    double v = fby[R.yf(i + 1, j + 1, k + 1)];
+    if (a == 0 || b == 0) v = 0.0;
+    if (a == 1 && b == 1 && fyt[R.yf(i + 1, j + 1, k + 1)] != F_INTERIOR) v = 0.0;
+    by[c] = v;
+  }
+  if (i < g.nx && j < g.ny && k <= g.nz) {
+    const int a = interior_cell(i, j, k - 1), b = interior_cell(i, j, k);
+    double v = fbz[R.zf(i + 1, j + 1, k + 1)];
+    if (a == 0 || b == 0) v = 0.0;
+    if (a == 1 && b == 1 && fzt[R.zf(i + 1, j + 1, k + 1)] != F_INTERIOR) v = 0.0;
+    bz[c] = v;
+  }
+  if (i < g.nx && j < g.ny && k < g.nz) fluid[c] = (interior_cell(i, j, k) == 1) ? 1 : 0;
+}
+
+// Cell bits: bit 0 C_INTERIOR, bit 1 fluid (C_INTERIOR with a non-zero
+// diagonal: the cells that carry unknowns).  Counts the fluid cells.
+
+__global__ void k_fluid_finalize(Geom g, const double* __restrict__ bx, const double* __restrict__ by,
+                                 const double* __restrict__ bz, uint8_t* fluid, RedBuf red, Scalars* s) {
+  const int i = blockIdx.x * TBX + threadIdx.x;
+  const int j = blockIdx.y * TBY + threadIdx.y;
+  const int k = blockIdx.z;
+  double v[1] = {0.0};
+  if (i < g.nx && j < g.ny && k < g.nz) {
+    const int c = g.idx(i, j, k);
+    const double d = bx[c] + bx[c + 1] + by[c] + by[c + g.px] + bz[c] + bz[c + g.ps];
+    const uint8_t in = fluid[c] & 1;
+    const uint8_t f = (in && d > 0.0) ? 1 : 0;
+    fluid[c] = (uint8_t)(in | (f << 1));
+    v[0] = f;
+  }
+  const Op ops[1] = {Op::Sum};
+  double out[1];
+  if (grid_reduce<1, TNT>(v, ops, red, 0, out)) {
+    if (threadIdx.x == 0 && threadIdx.y == 0) s->sum_tmp = out[0];
+  }
+}
+
+// Coarse face coefficients: mean of the fine faces that tile the coarse face
+// (2x2 in 3-D), computed in FP64 and stored as C.  The coarse operator uses
+// 1/H^2 = (1/h^2)/4 per coarsened direction, like G_GMGSolver::initialize
+// (G_GMGSolver.cu:71-73,135-137).
+template <class C>
+__global__ void k_coarsen_coeffs(Geom gf, Geom gc, int cx, int cy, int cz, const double* __restrict__ fbx,
+                                 const double* __restrict__ fby, const double* __restrict__ fbz, C* bx, C* by,
+                                 C* bz, double* bx64, double* by64, double* bz64) {
+  const int I = blockIdx.x * blockDim.x + threadIdx.x;
+  const int J = blockIdx.y * blockDim.y + threadIdx.y;
+  const int K = blockIdx.z;
+  if (I > gc.nx || J > gc.ny || K > gc.nz) return;
+  const int c = gc.idx(I, J, K);
+  const int ry = cy ? 2 : 1, rz = cz ? 2 : 1, rx = cx ? 2 : 1;
+  if (J < gc.ny && K < gc.nz) {  // x-face I
+    const int i = cx ? 2 * I : I;
+    double s = 0.0;
+    for (int dk = 0; dk < rz; ++dk)
+      for (int dj = 0; dj < ry; ++dj) s += fbx[gf.idx(i, (cy ? 2 * J : J) + dj, (cz ? 2 * K : K) + dk)];
+    s /= (double)(ry * rz);
+    bx[c] = coef_from_double<C>(s);
+    if (bx64) bx64[c] = s;
+  }
+  if (I < gc.nx && K < gc.nz) {  // y-face J
+    const int jj = cy ? 2 * J : J;
+    double s = 0.0;
+    for (int dk = 0; dk < rz; ++dk)
+      for (int di = 0; di < rx; ++di) s += fby[gf.idx((cx ? 2 * I : I) + di, jj, (cz ? 2 * K : K) + dk)];
+    s /= (double)(rx * rz);
+    by[c] = coef_from_double<C>(s);
+    if (by64) by64[c] = s;
+  }
+  if (I < gc.nx && J < gc.ny) {  // z-face K
+    const int kk = cz ? 2 * K : K;
+    double s = 0.0;
+    for (int dj = 0; dj < ry; ++dj)
+      for (int di = 0; di < rx; ++di) s += fbz[gf.idx((cx ? 2 * I : I) + di, (cy ? 2 * J : J) + dj, kk)];
+    s /= (double)(rx * ry);
+    bz[c] = coef_from_double<C>(s);
+    if (bz64) bz64[c] = s;
+  }
+}
+
+// FP64 -> C copy of a whole padded array (fine-level FP32 / BF16 coefficients).
+template <class C>
+__global__ void k_convert(const double* __restrict__ a, C* b, long long n) {
+  long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  for (; t < n; t += (long long)gridDim.x * blockDim.x) b[t] = coef_from_double<C>(a[t]);
+}
+
+// ------------------------------------------------------------------------
+// Right-hand side: base_k_make_poisson_rhs (G_PressureSolverBase.cu:49-118),
+// same operation order; eps == nullptr means eps == 1, fs == nullptr means
+// f_s == 0.  The f_b of the surface-tension term is read from the padded
+// coefficients (equal to the reference's f_b on every face of a C_INTERIOR
+// cell: the masked faces carry f_b = 0 in the reference as well).
+// `cellbits` bit 0 marks C_INTERIOR cells.  Writes the padded rhs and
+// optionally the reference-layout rhs.
+__global__ void k_divergence(Geom g, RefDims R, double inv_dx, double inv_dy, double inv_dz, double inv_dt,
+                             const double* __restrict__ vx, const double* __restrict__ vy,
+                             const double* __restrict__ vz, const double* __restrict__ eps,
+                             const double* __restrict__ eps_old, const double* __restrict__ bx,
+                             const double* __restrict__ by, const double* __restrict__ bz,
+                             const double* __restrict__ fsx, const double* __restrict__ fsy,
+                             const double* __restrict__ fsz, const uint8_t* __restrict__ cellbits, double* rhs,
+                             double* rhs_ref) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int k = blockIdx.z;
+  if (i >= g.nx || j >= g.ny || k >= g.nz) return;
+  const int ix = i + 1, iy = j + 1, iz = k + 1;
+  const int c = g.idx(i, j, k);
+  double out = 0.0;
+  if (cellbits[c] & 1) {
+    double exp_ = 1.0, exm = 1.0, eyp = 1.0, eym = 1.0, ezp = 1.0, ezm = 1.0, deps = 0.0;
+    if (eps) {
+      const double e0 = eps[R.cell(ix, iy, iz)];
+      exp_ = DMUL(0.5, DADD(e0, eps[R.cell(ix + 1, iy, iz)]));
+      exm = DMUL(0.5, DADD(eps[R.cell(ix - 1, iy, iz)], e0));
+      eyp = DMUL(0.5, DADD(e0, eps[R.cell(ix, iy + 1, iz)]));
+      eym = DMUL(0.5, DADD(eps[R.cell(ix, iy - 1, iz)], e0));
+      ezp = DMUL(0.5, DADD(e0, eps[R.cell(ix, iy, iz + 1)]));
+      ezm = DMUL(0.5, DADD(eps[R.cell(ix, iy, iz - 1)], e0));
+      deps = DADD(e0, -eps_old[R.cell(ix, iy, iz)]);
+    }
+    const double tx = DMUL(DADD(DMUL(exp_, vx[R.xf(ix + 1, iy, iz)]), -DMUL(exm, vx[R.xf(ix, iy, iz)])), inv_dx);
+    const double ty = DMUL(DADD(DMUL(eyp, vy[R.yf(ix, iy + 1, iz)]), -DMUL(eym, vy[R.yf(ix, iy, iz)])), inv_dy);
+    const double tz = DMUL(DADD(DMUL(ezp, vz[R.zf(ix, iy, iz + 1)]), -DMUL(ezm, vz[R.zf(ix, iy, iz)])), inv_dz);
+    const double div_eps = DADD(DADD(tx, ty), tz);
+    double f_st = 0.0;
+    if (fsx) {
+      const double sx = DMUL(DADD(DMUL(bx[c + 1], fsx[R.xf(ix + 1, iy, iz)]), -DMUL(bx[c], fsx[R.xf(ix, iy, iz)])), inv_dx);
+      const double sy = DMUL(DADD(DMUL(by[c + g.px], fsy[R.yf(ix, iy + 1, iz)]), -DMUL(by[c], fsy[R.yf(ix, iy, iz)])), inv_dy);
+      const double sz = DMUL(DADD(DMUL(bz[c + g.ps], fsz[R.zf(ix, iy, iz + 1)]), -DMUL(bz[c], fsz[R.zf(ix, iy, iz)])), inv_dz);
+      f_st = DADD(DADD(sx, sy), sz);
+    }
+    out = DADD(DADD(DMUL(-inv_dt, div_eps), -DMUL(DMUL(deps, inv_dt), inv_dt)), -f_st);
+  }
+  rhs[c] = out;
+  if (rhs_ref) rhs_ref[R.cell(ix, iy, iz)] = out;
+}
+
+// Reference-layout cell array (interior) -> padded array.
+template <class T>
+__global__ void k_import_cells(Geom g, RefDims R, const double* __restrict__ src, T* dst) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int k = blockIdx.z;
+  if (i >= g.nx || j >= g.ny || k >= g.nz) return;
+  dst[g.idx(i, j, k)] = (T)src[R.cell(i + 1, j + 1, k + 1)];
+}
+
+// Padded FP64 array -> reference-layout interior, minus `shift` on fluid cells
+// (the zero-mean projection of the solution).
+__global__ void k_export_cells(Geom g, RefDims R, const double* __restrict__ src, const uint8_t* __restrict__ fluid,
+                               const double* shift, double* dst) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int k = blockIdx.z;
+  if (i >= g.nx || j >= g.ny || k >= g.nz) return;
+  const int c = g.idx(i, j, k);
+  double v = src[c];
+  if (shift && (fluid[c] & 2)) v -= *shift;
+  dst[R.cell(i + 1, j + 1, k + 1)] = v;
+}
+
+// ------------------------------------------------------------------------
+// Set-up of a solve: b -= mean_fluid(b) (pure Neumann), r = b (FP64 or
+// FP32), x = 0, ||b||^2.  Two passes: sum, then project + norm.
+template <class TR>
+__global__ void k_setup_sum(Geom g, const double* __restrict__ b, RedBuf red, Scalars* s) {
+  const int i = blockIdx.x * TBX + threadIdx.x;
+  const int j = blockIdx.y * TBY + threadIdx.y;
+  const int k = blockIdx.z;
+  double v[1] = {0.0};
+  if (i < g.nx && j < g.ny && k < g.nz) v[0] = b[g.idx(i, j, k)];
+  const Op ops[1] = {Op::Sum};
+  double out[1];
+  if (grid_reduce<1, TNT>(v, ops, red, 0, out))
+    if (threadIdx.x == 0 && threadIdx.y == 0) s->sum_tmp = out[0] * s->inv_nfluid;
+}
+
+template <class TR>
+__global__ void k_setup_project(Geom g, double* b, const uint8_t* __restrict__ fluid, TR* r, RedBuf red,
+                                Scalars* s, double tol) {
+  const int i = blockIdx.x * TBX + threadIdx.x;
+  const int j = blockIdx.y * TBY + threadIdx.y;
+  const int k = blockIdx.z;
+  double v[2] = {0.0, 0.0};
+  if (i < g.nx && j < g.ny && k < g.nz) {
+    const int c = g.idx(i, j, k);
+    double bv = b[c];
+    if (fluid[c] & 2) bv -= s->sum_tmp;
+    else bv = 0.0;
+    b[c] = bv;
+    r[c] = (TR)bv;
+    v[0] = bv * bv;
+    v[1] = fabs(bv);
+  }
+  const Op ops[2] = {Op::Sum, Op::Max};
+  double out[2];
+  if (grid_reduce<2, TNT>(v, ops, red, 0, out)) {
+    if (threadIdx.x == 0 && threadIdx.y == 0) {
+      s->bb = out[0];
+      s->tol2bb = tol * tol * out[0];
+      s->rr = out[0];
+      s->rr_anchor = out[0];
+      s->rmax = out[1];
+      s->rshift = 0.0;
+      s->true_rr = out[0];
+      s->true_rmax = out[1];
+      s->iter = 0;
+      s->first = 1;
+      s->e_reset = s->mixed;
+      s->xbuf = 0;
+      s->reliable_count = 0;
+      s->do_reliable = 0;
+      s->status = 0;
+      s->done = 0;
+      if (!isfinite(out[0])) { s->status = 3; s->done = 1; }
+      else if (out[0] == 0.0) { s->done = 1; }  // b == 0: x = 0 is exact
+      else if (s->stop_rule == 1 && out[1] < s->tol_max) { s->done = 1; }
+    }
+  }
+}
+
+// ------------------------------------------------------------------------
+// PCG: q = A d, pAp = d.q, alpha = rz/pAp.
+template <class T, class C>
+__global__ void __launch_bounds__(TNT) k_matvec_pap(Geom g, const T* __restrict__ d, Stencil<T, C> S, T* q,
+                                                    RedBuf red, Scalars* s, int kz) {
+  if (s->done) return;
+  typedef acc_t<T> A;
+  const int i = blockIdx.x * TBX + threadIdx.x;
+  const int j = blockIdx.y * TBY + threadIdx.y;
+  const int k0 = blockIdx.z * kz;
+  double v[1] = {0.0};
+  if (i < g.nx && j < g.ny) {
+    const int k1 = min(k0 + kz, g.nz);
+    int c = g.idx(i, j, k0);
+    A xm = (A)d[c - g.ps], xc = (A)d[c];
+    for (int k = k0; k < k1; ++k, c += g.ps) {
+      const A xp = (A)d[c + g.ps];
+      A wxm, wxp, wym, wyp, wzm, wzp;
+      S.coeffs(c, g.px, g.ps, wxm, wxp, wym, wyp, wzm, wzp);
+      const A diag = (wxm + wxp) + (wym + wyp) + (wzm + wzp);
+      const A off = (wxm * (A)d[c - 1] + wxp * (A)d[c + 1]) + (wym * (A)d[c - g.px] + wyp * (A)d[c + g.px]) +
+                    (wzm * xm + wzp * xp);
+      const A y = diag * xc - off;
+      q[c] = (T)y;
+      v[0] += (double)xc * (double)y;
+      xm = xc;
+      xc = xp;
+    }
+  }
+  const Op ops[1] = {Op::Sum};
+  double out[1];
+  if (grid_reduce<1, TNT>(v, ops, red, 0, out)) {
+    if (threadIdx.x == 0 && threadIdx.y == 0) {
+      const double pAp = out[0];
+      s->pAp = pAp;
+      if (!isfinite(pAp)) { s->status = 3; s->done = 1; }
+      else if (!(pAp > 0.0)) { s->status = 2; s->done = 1; }
+      else s->alpha = s->rz / pAp;
+    }
+  }
+}
+
+// PCG: x += alpha d, r -= alpha q, recursive residual statistics and the
+// stopping test.  In mixed precision x is the FP32 increment since the last
+// FP64 recomputation (reset to alpha d after one) and a small enough
+// residual requests an FP64 recomputation instead of stopping.
+template <class T, class TX>
+__global__ void __launch_bounds__(TNT) k_update(Geom g, TX* x, const T* __restrict__ d, T* r, const T* __restrict__ q,
+                                                RedBuf red, Scalars* s, int kz) {
+  if (s->done) return;
+  const int i = blockIdx.x * TBX + threadIdx.x;
+  const int j = blockIdx.y * TBY + threadIdx.y;
+  const int k0 = blockIdx.z * kz;
+  const double alpha_d = s->alpha;
+  const T alpha = (T)alpha_d;
+  const bool reset = s->e_reset;
+  double v[3] = {0.0, 0.0, 0.0};
+  if (i < g.nx && j < g.ny) {
+    const int k1 = min(k0 + kz, g.nz);
+    int c = g.idx(i, j, k0);
+    for (int k = k0; k < k1; ++k, c += g.ps) {
+      const T dv = d[c];
+      if (reset) x[c] = (TX)(alpha * dv);
+      else x[c] = x[c] + (TX)(alpha * dv);
+      const T rn = r[c] - alpha * q[c];
+      r[c] = rn;
+      v[0] += (double)rn;
+      v[1] += (double)rn * (double)rn;
+      v[2] = fmax(v[2], fabs((double)rn));
+    }
+  }
+  const Op ops[3] = {Op::Sum, Op::Sum, Op::Max};
+  double out[3];
+  if (grid_reduce<3, TNT>(v, ops, red, 0, out)) {
+    if (threadIdx.x == 0 && threadIdx.y == 0) {
+      s->iter += 1;
+      s->e_reset = 0;
+      const double m = out[0] * s->inv_nfluid;
+      s->rshift = m;
+      const double rr = fmax(out[1] - out[0] * m, 0.0);
+      s->rr = rr;
+      s->rmax = out[2];
+      if (!isfinite(out[1])) { s->status = 3; s->done = 1; return; }
+      const bool small = (s->stop_rule == 1) ? (out[2] < s->tol_max) : (rr <= s->tol2bb);
+      if (s->mixed) {
+        if (small || rr < s->reliable_delta2 * s->rr_anchor || s->iter >= s->max_iter) s->do_reliable = 1;
+      } else if (small) {
+        s->status = 0; s->done = 1;
+      } else if (s->iter >= s->max_iter) {
+        s->status = 1; s->done = 1;
+      }
+    }
+  }
+}
+
+// Mixed precision: FP64 true residual.  x_new = x64[xbuf] + e (FP64 sum at
+// every stencil point), r = b - A64 x_new written as FP32, x_new stored in
+// the other FP64 buffer; the stopping test runs on this true residual.
+template <class T>
+__global__ void __launch_bounds__(TNT) k_reliable(Geom g, double* x64a, double* x64b, const T* __restrict__ e,
+                                                  const double* __restrict__ b, Stencil<double, double> S, T* r,
+                                                  RedBuf red, Scalars* s, int kz) {
+  if (s->done || !s->do_reliable) return;
+  const int i = blockIdx.x * TBX + threadIdx.x;
+  const int j = blockIdx.y * TBY + threadIdx.y;
+  const int k0 = blockIdx.z * kz;
+  const double* __restrict__ xs = s->xbuf ? x64b : x64a;
+  double* xd = s->xbuf ? x64a : x64b;
+  double v[3] = {0.0, 0.0, 0.0};
+  if (i < g.nx && j < g.ny) {
+    const int k1 = min(k0 + kz, g.nz);
+    int c = g.idx(i, j, k0);
+    auto X = [&](int cc) { return xs[cc] + (double)e[cc]; };
+    double xm = X(c - g.ps), xc = X(c);
+    for (int k = k0; k < k1; ++k, c += g.ps) {
+      const double xp = X(c + g.ps);
+      double wxm, wxp, wym, wyp, wzm, wzp;
+      S.coeffs(c, g.px, g.ps, wxm, wxp, wym, wyp, wzm, wzp);
+      const double diag = (wxm + wxp) + (wym + wyp) + (wzm + wzp);
+      const double off = (wxm * X(c - 1) + wxp * X(c + 1)) + (wym * X(c - g.px) + wyp * X(c + g.px)) +
+                         (wzm * xm + wzp * xp);
+      const double rv = b[c] - (diag * xc - off);
+      xd[c] = xc;
+      r[c] = (T)rv;
+      v[0] += rv;
+      v[1] += rv * rv;
+      v[2] = fmax(v[2], fabs(rv));
+      xm = xc;
+      xc = xp;
+    }
+  }
+  const Op ops[3] = {Op::Sum, Op::Sum, Op::Max};
+  double out[3];
+  if (grid_reduce<3, TNT>(v, ops, red, 0, out)) {
+    if (threadIdx.x == 0 && threadIdx.y == 0) {
+      s->xbuf ^= 1;
+      s->e_reset = 1;
+      s->do_reliable = 0;
+      s->reliable_count += 1;
+      const double m = out[0] * s->inv_nfluid;
+      s->rshift = m;
+      const double rr = fmax(out[1] - out[0] * m, 0.0);
+      s->rr = rr;
+      s->rr_anchor = rr;
+      s->rmax = out[2];
+      s->true_rr = rr;
+      s->true_rmax = out[2];
+      if (!isfinite(out[1])) { s->status = 3; s->done = 1; return; }
+      const bool ok = (s->stop_rule == 1) ? (out[2] < s->tol_max) : (rr <= s->tol2bb);
+      if (ok) { s->status = 0; s->done = 1; }
+      else if (s->iter >= s->max_iter) { s->status = 1; s->done = 1; }
+    }
+  }
+}
+
+// rz_new = (r - shift).z over all cells (z is 0 where the diagonal is 0, so
+// the shift needs no mask), beta = rz_new / rz.
+template <class T>
+__global__ void __launch_bounds__(TNT) k_dot_rz(Geom g, const T* __restrict__ r, const T* __restrict__ z, RedBuf red,
+                                                Scalars* s, int kz) {
+  if (s->done) return;
+  const int i = blockIdx.x * TBX + threadIdx.x;
+  const int j = blockIdx.y * TBY + threadIdx.y;
+  const int k0 = blockIdx.z * kz;
+  double v[2] = {0.0, 0.0};
+  if (i < g.nx && j < g.ny) {
+    const int k1 = min(k0 + kz, g.nz);
+    int c = g.idx(i, j, k0);
+    for (int k = k0; k < k1; ++k, c += g.ps) {
+      const double zv = (double)z[c];
+      v[0] += (double)r[c] * zv;
+      v[1] += zv;
+    }
+  }
+  const Op ops[2] = {Op::Sum, Op::Sum};
+  double out[2];
+  if (grid_reduce<2, TNT>(v, ops, red, 0, out)) {
+    if (threadIdx.x == 0 && threadIdx.y == 0) {
+      const double rz_new = out[0] - s->rshift * out[1];
+      if (!isfinite(rz_new)) { s->status = 3; s->done = 1; return; }
+      if (!(rz_new > 0.0)) {
+        // r.z <= 0 with r != 0 means the preconditioner lost definiteness
+        s->status = 2; s->done = 1; return;
+      }
+      s->beta = s->first ? 0.0 : rz_new / s->rz;
+      s->rz = rz_new;
+      s->first = 0;
+    }
+  }
+}
+
+// d = z + beta d
+template <class T>
+__global__ void __launch_bounds__(TNT) k_dir(Geom g, const T* __restrict__ z, T* d, const Scalars* s, int kz) {
+  if (s->done) return;
+  const int i = blockIdx.x * TBX + threadIdx.x;
+  const int j = blockIdx.y * TBY + threadIdx.y;
+  const int k0 = blockIdx.z * kz;
+  const T beta = (T)s->beta;
+  if (i < g.nx && j < g.ny) {
+    const int k1 = min(k0 + kz, g.nz);
+    int c = g.idx(i, j, k0);
+    for (int k = k0; k < k1; ++k, c += g.ps) d[c] = z[c] + beta * d[c];
+  }
+}
+
+// FP64 true residual r = b - A x with statistics (final check, plain mode).
+// When `restart` is set and the test fails, r is overwritten with the true
+// residual and PCG restarts from it.
+__global__ void __launch_bounds__(TNT) k_true_residual(Geom g, const double* __restrict__ x, const double* __restrict__ b,
+                                                       Stencil<double, double> S, double* r, int write_r, RedBuf red,
+                                                       Scalars* s, int kz) {
+  const int i = blockIdx.x * TBX + threadIdx.x;
+  const int j = blockIdx.y * TBY + threadIdx.y;
+  const int k0 = blockIdx.z * kz;
+  double v[3] = {0.0, 0.0, 0.0};
+  if (i < g.nx && j < g.ny) {
+    const int k1 = min(k0 + kz, g.nz);
+    int c = g.idx(i, j, k0);
+    double xm = x[c - g.ps], xc = x[c];
+    for (int k = k0; k < k1; ++k, c += g.ps) {
+      const double xp = x[c + g.ps];
+      double wxm, wxp, wym, wyp, wzm, wzp;
+      S.coeffs(c, g.px, g.ps, wxm, wxp, wym, wyp, wzm, wzp);
+      const double diag = (wxm + wxp) + (wym + wyp) + (wzm + wzp);
+      const double off = (wxm * x[c - 1] + wxp * x[c + 1]) + (wym * x[c - g.px] + wyp * x[c + g.px]) +
+                         (wzm * xm + wzp * xp);
+      const double rv = b[c] - (diag * xc - off);
+      if (write_r) r[c] = rv;
+      v[0] += rv;
+      v[1] += rv * rv;
+      v[2] = fmax(v[2], fabs(rv));
+      xm = xc;
+      xc = xp;
+    }
+  }
+  const Op ops[3] = {Op::Sum, Op::Sum, Op::Max};
+  double out[3];
+  if (grid_reduce<3, TNT>(v, ops, red, 0, out)) {
+    if (threadIdx.x == 0 && threadIdx.y == 0) {
+      const double m = out[0] * s->inv_nfluid;
+      s->true_rr = fmax(out[1] - out[0] * m, 0.0);
+      s->true_rmax = out[2];
+      if (write_r) { s->rshift = m; s->rr = s->true_rr; s->rmax = out[2]; }
+    }
+  }
+}
+
+// y = A x (FP64), plain operator application for testing.
+__global__ void k_apply(Geom g, const double* __restrict__ x, Stencil<double, double> S, double* y) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int k = blockIdx.z;
+  if (i >= g.nx || j >= g.ny || k >= g.nz) return;
+  const int c = g.idx(i, j, k);
+  double wxm, wxp, wym, wyp, wzm, wzp;
+  S.coeffs(c, g.px, g.ps, wxm, wxp, wym, wyp, wzm, wzp);
+  const double diag = (wxm + wxp) + (wym + wyp) + (wzm + wzp);
+  const double off = (wxm * x[c - 1] + wxp * x[c + 1]) + (wym * x[c - g.px] + wyp * x[c + g.px]) +
+                     (wzm * x[c - g.ps] + wzp * x[c + g.ps]);
+  y[c] = diag * x[c] - off;
+}
+
+// Sum of x over fluid cells (the zero-mean projection of the solution).
+__global__ void k_sum_fluid(Geom g, const double* __restrict__ x, const uint8_t* __restrict__ fluid, RedBuf red,
+                            Scalars* s) {
+  const int i = blockIdx.x * TBX + threadIdx.x;
+  const int j = blockIdx.y * TBY + threadIdx.y;
+  const int k = blockIdx.z;
+  double v[1] = {0.0};
+  if (i < g.nx && j < g.ny && k < g.nz) {
+    const int c = g.idx(i, j, k);
+    if (fluid[c] & 2) v[0] = x[c];
+  }
+  const Op ops[1] = {Op::Sum};
+  double out[1];
+  if (grid_reduce<1, TNT>(v, ops, red, 0, out))
+    if (threadIdx.x == 0 && threadIdx.y == 0) s->sum_tmp = out[0] * s->inv_nfluid;
+}
+
+// ------------------------------------------------------------------------
+// Multigrid V-cycle pieces (red-black Gauss-Seidel).  Colour of (i,j,k) is
+// (i+j+k)&1.  A thread owns the x-pair (2t, 2t+1) of a row and updates the
+// member of the requested colour in every plane of its z-chunk.
+//   rhs_eff = rhs - shift on cells with a non-zero diagonal (shift: the
+//             running mean of the PCG residual, fine grid only)
+//   zero_init: the iterate is 0 before this half-sweep (first pre-smoothing
+//             sweep): neighbours are not read.
+//   xc != nullptr: add the coarse-grid correction xc[parent] to every
+//             neighbour read (prolongation fused into the first
+//             post-smoothing half-sweep; the updated cell needs no old value).
+template <class T, class C>
+__global__ void __launch_bounds__(TNT) k_rbgs(Geom g, T* x, const T* __restrict__ rhs, const double* shift,
+                                              Stencil<T, C> S, int colour, int zero_init, const T* __restrict__ xc,
+                                              Geom gc, int cx, int cy, int cz, const Scalars* s, int kz) {
+  if (s && s->done) return;
+  typedef acc_t<T> A;
+  const int t = blockIdx.x * TBX + threadIdx.x;
+  const int j = blockIdx.y * TBY + threadIdx.y;
+  const int k0 = blockIdx.z * kz;
+  const int i0 = 2 * t;
+  if (i0 >= g.nx || j >= g.ny) return;
+  const A sh = shift ? (A)(*shift) : (A)0;
+  const int k1 = min(k0 + kz, g.nz);
+  for (int k = k0; k < k1; ++k) {
+    const int i = i0 + ((i0 + j + k + colour) & 1);
+    if (i >= g.nx) continue;
+    const int c = g.idx(i, j, k);
+    A wxm, wxp, wym, wyp, wzm, wzp;
+    S.coeffs(c, g.px, g.ps, wxm, wxp, wym, wyp, wzm, wzp);
+    const A diag = (wxm + wxp) + (wym + wyp) + (wzm + wzp);
+    A out = (A)0;
+    if (diag > (A)0) {
+      A bv = (A)rhs[c] - sh;
+      if (!zero_init) {
+        A n[6] = {(A)x[c - 1], (A)x[c + 1], (A)x[c - g.px], (A)x[c + g.px], (A)x[c - g.ps], (A)x[c + g.ps]};
+        if (xc) {
+          const int ci[6][3] = {{i - 1, j, k}, {i + 1, j, k}, {i, j - 1, k}, {i, j + 1, k}, {i, j, k - 1}, {i, j, k + 1}};
+#pragma unroll
+          for (int q = 0; q < 6; ++q) {
+            const int a = ci[q][0], b = ci[q][1], d = ci[q][2];
+            if (a >= 0 && b >= 0 && d >= 0 && a < g.nx && b < g.ny && d < g.nz)
+              n[q] += (A)xc[gc.idx(cx ? a >> 1 : a, cy ? b >> 1 : b, cz ? d >> 1 : d)];
+          }
+        }
+        bv += (wxm * n[0] + wxp * n[1]) + (wym * n[2] + wyp * n[3]) + (wzm * n[4] + wzp * n[5]);
+      }
+      out = bv / diag;
+    }
+    x[c] = (T)out;
+  }
+}
+
+// Residual of the fine grid restricted to the coarse grid:
+// rhs_c = mean over the children of (rhs_eff - A x)  (the reference's
+// k_get_res_* followed by k_restrict_* averaging, G_GMGSolver.cu:152-226,416-493).
+template <class T, class C>
+__global__ void __launch_bounds__(TNT) k_resid_restrict(Geom g, const T* __restrict__ x, const T* __restrict__ rhs,
+                                                        const double* shift, Stencil<T, C> S, Geom gc, int cx, int cy,
+                                                        int cz, T* rhs_c, const Scalars* s) {
+  if (s && s->done) return;
+  typedef acc_t<T> A;
+  const int I = blockIdx.x * TBX + threadIdx.x;
+  const int J = blockIdx.y * TBY + threadIdx.y;
+  const int K = blockIdx.z;
+  if (I >= gc.nx || J >= gc.ny || K >= gc.nz) return;
+  const A sh = shift ? (A)(*shift) : (A)0;
+  A acc = (A)0;
+  const int rx = cx ? 2 : 1, ry = cy ? 2 : 1, rz = cz ? 2 : 1;
+  for (int dk = 0; dk < rz; ++dk)
+    for (int dj = 0; dj < ry; ++dj)
+      for (int di = 0; di < rx; ++di) {
+        const int i = (cx ? 2 * I : I) + di, j = (cy ? 2 * J : J) + dj, k = (cz ? 2 * K : K) + dk;
+        const int c = g.idx(i, j, k);
+        A wxm, wxp, wym, wyp, wzm, wzp;
+        S.coeffs(c, g.px, g.ps, wxm, wxp, wym, wyp, wzm, wzp);
+        const A diag = (wxm + wxp) + (wym + wyp) + (wzm + wzp);
+        const A off = (wxm * (A)x[c - 1] + wxp * (A)x[c + 1]) + (wym * (A)x[c - g.px] + wyp * (A)x[c + g.px]) +
+                      (wzm * (A)x[c - g.ps] + wzp * (A)x[c + g.ps]);
+        A bv = (A)rhs[c];
+        if (diag > (A)0) bv -= sh;
+        acc += bv - (diag * (A)x[c] - off);
+      }
+  rhs_c[gc.idx(I, J, K)] = (T)(acc / (A)(rx * ry * rz));
+}
+
+// ------------------------------------------------------------------------
+// Coarse grids in one persistent single-CTA kernel: pre-smoothing,
+// residual/restriction, the coarsest solve (symmetric sweep pairs),
+// prolongation and post-smoothing of every grid at or below the first
+// grid with <= 4096 cells, with __syncthreads between the steps.
+struct CoarseLevel {
+  Geom g;
+  int cx, cy, cz;          // how this grid was coarsened from the one above
+  const void* bx;
+  const void* by;
+  const void* bz;
+  void* x;
+  void* rhs;
+};
+constexpr int MAX_COARSE = 8;
+struct CoarseSet {
+  CoarseLevel L[MAX_COARSE];
+  int n;  // grids in the set; L[0] receives rhs and returns x
+};
+
+template <class T, class C>
+__device__ __forceinline__ void cta_half_sweep(const CoarseLevel& L, int colour, bool zero_init, const T* xc,
+                                               const CoarseLevel* Lc, const double* shift) {
+  typedef acc_t<T> A;
+  const Geom& g = L.g;
+  T* x = (T*)L.x;
+  const T* rhs = (const T*)L.rhs;
+  Stencil<T, C> S{(const C*)L.bx, (const C*)L.by, (const C*)L.bz, (A)g.ihx2, (A)g.ihy2, (A)g.ihz2};
+  const A sh = shift ? (A)(*shift) : (A)0;
+  const int half = (g.nx + 1) / 2;
+  const int total = half * g.ny * g.nz;
+  for (int t = threadIdx.x; t < total; t += blockDim.x) {
+    const int tx = t % half;
+    const int j = (t / half) % g.ny;
+    const int k = t / (half * g.ny);
+    const int i0 = 2 * tx;
+    const int i = i0 + ((i0 + j + k + colour) & 1);
+    if (i >= g.nx) continue;
+    const int c = g.idx(i, j, k);
+    A wxm, wxp, wym, wyp, wzm, wzp;
+    S.coeffs(c, g.px, g.ps, wxm, wxp, wym, wyp, wzm, wzp);
+    const A diag = (wxm + wxp) + (wym + wyp) + (wzm + wzp);
+    A out = (A)0;
+    if (diag > (A)0) {
+      A bv = (A)rhs[c] - sh;
+      if (!zero_init) {
+        A n[6] = {(A)x[c - 1], (A)x[c + 1], (A)x[c - g.px], (A)x[c + g.px], (A)x[c - g.ps], (A)x[c + g.ps]};
+        if (xc) {
+          const Geom& gc = Lc->g;
+          const int ci[6][3] = {{i - 1, j, k}, {i + 1, j, k}, {i, j - 1, k}, {i, j + 1, k}, {i, j, k - 1}, {i, j, k + 1}};
+#pragma unroll
+          for (int q = 0; q < 6; ++q) {
+            const int a = ci[q][0], b = ci[q][1], d = ci[q][2];
+            if (a >= 0 && b >= 0 && d >= 0 && a < g.nx && b < g.ny && d < g.nz)
+              n[q] += (A)xc[gc.idx(Lc->cx ? a >> 1 : a, Lc->cy ? b >> 1 : b, Lc->cz ? d >> 1 : d)];
+          }
+        }
+        bv += (wxm * n[0] + wxp * n[1]) + (wym * n[2] + wyp * n[3]) + (wzm * n[4] + wzp * n[5]);
+      }
+      out = bv / diag;
+    }
+    x[c] = (T)out;
+  }
+}
+
+template <class T, class C>
+__device__ __forceinline__ void cta_resid_restrict(const CoarseLevel& L, const CoarseLevel& Lc, const double* shift) {
+  typedef acc_t<T> A;
+  const Geom& g = L.g;
+  const Geom& gc = Lc.g;
+  const T* x = (const T*)L.x;
+  const T* rhs = (const T*)L.rhs;
+  T* rhs_c = (T*)Lc.rhs;
+  Stencil<T, C> S{(const C*)L.bx, (const C*)L.by, (const C*)L.bz, (A)g.ihx2, (A)g.ihy2, (A)g.ihz2};
+  const A sh = shift ? (A)(*shift) : (A)0;
+  const int total = gc.nx * gc.ny * gc.nz;
+  const int rx = Lc.cx ? 2 : 1, ry = Lc.cy ? 2 : 1, rz = Lc.cz ? 2 : 1;
+  for (int t = threadIdx.x; t < total; t += blockDim.x) {
+    const int I = t % gc.nx, J = (t / gc.nx) % gc.ny, K = t / (gc.nx * gc.ny);
+    A acc = (A)0;
+    for (int dk = 0; dk < rz; ++dk)
+      for (int dj = 0; dj < ry; ++dj)
+        for (int di = 0; di < rx; ++di) {
+          const int i = (Lc.cx ? 2 * I : I) + di, j = (Lc.cy ? 2 * J : J) + dj, k = (Lc.cz ? 2 * K : K) + dk;
+          const int c = g.idx(i, j, k);
+          A wxm, wxp, wym, wyp, wzm, wzp;
+          S.coeffs(c, g.px, g.ps, wxm, wxp, wym, wyp, wzm, wzp);
+          const A diag = (wxm + wxp) + (wym + wyp) + (wzm + wzp);
+          const A off = (wxm * (A)x[c - 1] + wxp * (A)x[c + 1]) + (wym * (A)x[c - g.px] + wyp * (A)x[c + g.px]) +
+                        (wzm * (A)x[c - g.ps] + wzp * (A)x[c + g.ps]);
+          A bv = (A)rhs[c];
+          if (diag > (A)0) bv -= sh;
+          acc += bv - (diag * (A)x[c] - off);
+        }
+    rhs_c[gc.idx(I, J, K)] = (T)(acc / (A)(rx * ry * rz));
+  }
+}
+
+// x (this grid) += coarse x at the parent, for the coarsest hand-off where the
+// next step is the symmetric sweep (no fused half-sweep available).
+template <class T>
+__device__ __forceinline__ void cta_prolong(const CoarseLevel& L, const CoarseLevel& Lc) {
+  const Geom& g = L.g;
+  const Geom& gc = Lc.g;
+  T* x = (T*)L.x;
+  const T* xc = (const T*)Lc.x;
+  const int total = g.nx * g.ny * g.nz;
+  for (int t = threadIdx.x; t < total; t += blockDim.x) {
+    const int i = t % g.nx, j = (t / g.nx) % g.ny, k = t / (g.nx * g.ny);
+    x[g.idx(i, j, k)] += xc[gc.idx(Lc.cx ? i >> 1 : i, Lc.cy ? j >> 1 : j, Lc.cz ? k >> 1 : k)];
+  }
+}
+
+template <class T, class C>
+__global__ void __launch_bounds__(1024) k_coarse_vcycle(CoarseSet set, int nu1, int nu2, int coarse_pairs,
+                                                        const double* shift0, const Scalars* s) {
+  if (s && s->done) return;
+  const int n = set.n;
+  // down
+  for (int l = 0; l < n - 1; ++l) {
+    const double* sh = (l == 0) ? shift0 : nullptr;
+    for (int it = 0; it < nu1; ++it) {
+      cta_half_sweep<T, C>(set.L[l], 0, it == 0, nullptr, nullptr, sh);
+      __syncthreads();
+      cta_half_sweep<T, C>(set.L[l], 1, false, nullptr, nullptr, sh);
+      __syncthreads();
+    }
+    cta_resid_restrict<T, C>(set.L[l], set.L[l + 1], sh);
+    __syncthreads();
+  }
+  // coarsest: symmetric sweep pairs from zero
+  {
+    const CoarseLevel& L = set.L[n - 1];
+    const double* sh = (n == 1) ? shift0 : nullptr;
+    for (int it = 0; it < coarse_pairs; ++it) {
+      cta_half_sweep<T, C>(L, 0, it == 0, nullptr, nullptr, sh);
+      __syncthreads();
+      cta_half_sweep<T, C>(L, 1, false, nullptr, nullptr, sh);
+      __syncthreads();
+    }
+    for (int it = 0; it < coarse_pairs; ++it) {
+      cta_half_sweep<T, C>(L, 1, false, nullptr, nullptr, sh);
+      __syncthreads();
+      cta_half_sweep<T, C>(L, 0, false, nullptr, nullptr, sh);
+      __syncthreads();
+    }
+  }
+  // up
+  for (int l = n - 2; l >= 0; --l) {
+    const double* sh = (l == 0) ? shift0 : nullptr;
+    for (int it = 0; it < nu2; ++it) {
+      const bool fuse = (it == 0);
+      cta_half_sweep<T, C>(set.L[l], 1, false, fuse ? (const T*)set.L[l + 1].x : nullptr, &set.L[l + 1], sh);
+      __syncthreads();
+      cta_half_sweep<T, C>(set.L[l], 0, false, nullptr, nullptr, sh);
+      __syncthreads();
+    }
+  }
+}
+
+// ------------------------------------------------------------------------
+// Velocity correction: k_correct_vof_velocity (CFD/G_SMACSolver.cu:1072-1142),
+// same thread ranges and operation order.  fs == nullptr: f_s = 0;
+// fir == nullptr: f_inv_rho taken from the padded f_b.  write_all: faces that
+// are not F_INTERIOR receive u* (used by smac_project).
+__global__ void k_correct(RefDims R, Geom g, double inv_dx, double inv_dy, double inv_dz, double dt,
+                          const uint8_t* __restrict__ ct, const uint8_t* __restrict__ fxt,
+                          const uint8_t* __restrict__ fyt, const uint8_t* __restrict__ fzt,
+                          const double* __restrict__ pd, double* p, const double* __restrict__ vxs,
+                          const double* __restrict__ vys, const double* __restrict__ vzs,
+                          const double* __restrict__ firx, const double* __restrict__ firy,
+                          const double* __restrict__ firz, const double* __restrict__ fbx,
+                          const double* __restrict__ fby, const double* __restrict__ fbz,
+                          const double* __restrict__ fsx, const double* __restrict__ fsy,
+                          const double* __restrict__ fsz, double* vx, double* vy, double* vz, int write_all) {
+  const int ix = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  const int iy = blockIdx.y * blockDim.y + threadIdx.y + 1;
+  const int iz = blockIdx.z + 1;
+  const int Nx = R.Nx, Ny = R.Ny, Nz = R.Nz;
+  // padded f_b of the face, used when f_inv_rho is not supplied
+  auto padded = [&](const double* b, int i, int j, int k) -> double {
+    if (i < 0 || j < 0 || k < 0 || i > g.nx || j > g.ny || k > g.nz) return 0.0;
+    return b[g.idx(i, j, k)];
+  };
+  // a face is corrected only when both of its cells exist (F_INTERIOR faces
+  // always satisfy this; the bound keeps mislabelled ghost faces harmless)
+  if (!(iy >= Ny + 2 || ix >= Nx + 3 || iz >= Nz + 2)) {
+    const long long f = R.xf(ix, iy, iz);
+    if (fxt[f] == F_INTERIOR && ix <= Nx + 1) {
+      const double ir = firx ? firx[f] : padded(fbx, ix - 1, iy - 1, iz - 1);
+      const double fs = fsx ? fsx[f] : 0.0;
+      const double gp = DMUL(DADD(pd[R.cell(ix, iy, iz)], -pd[R.cell(ix - 1, iy, iz)]), inv_dx);
+      vx[f] = DADD(vxs[f], DMUL(DMUL(ir, dt), DADD(fs, -gp)));
+    } else if (write_all) {
+      vx[f] = vxs[f];
+    }
+  }
+  if (!(iy >= Ny + 3 || ix >= Nx + 2 || iz >= Nz + 2)) {
+    const long long f = R.yf(ix, iy, iz);
+    if (fyt[f] == F_INTERIOR && iy <= Ny + 1) {
+      const double ir = firy ? firy[f] : padded(fby, ix - 1, iy - 1, iz - 1);
+      const double fs = fsy ? fsy[f] : 0.0;
+      const double gp = DMUL(DADD(pd[R.cell(ix, iy, iz)], -pd[R.cell(ix, iy - 1, iz)]), inv_dy);
+      vy[f] = DADD(vys[f], DMUL(DMUL(ir, dt), DADD(fs, -gp)));
+    } else if (write_all) {
+      vy[f] = vys[f];
+    }
+  }
+  if (!(iy >= Ny + 2 || ix >= Nx + 2 || iz >= Nz + 3)) {
+    const long long f = R.zf(ix, iy, iz);
+    if (fzt[f] == F_INTERIOR && iz <= Nz + 1) {
+      const double ir = firz ? firz[f] : padded(fbz, ix - 1, iy - 1, iz - 1);
+      const double fs = fsz ? fsz[f] : 0.0;
+      const double gp = DMUL(DADD(pd[R.cell(ix, iy, iz)], -pd[R.cell(ix, iy, iz - 1)]), inv_dz);
+      vz[f] = DADD(vzs[f], DMUL(DMUL(ir, dt), DADD(fs, -gp)));
+    } else if (write_all) {
+      vz[f] = vzs[f];
+    }
+  }
+  if (p && ix < Nx + 1 && iy < Ny + 1 && iz < Nz + 1) {
+    if (ct[R.cell(ix, iy, iz)] == C_INTERIOR) p[R.cell(ix, iy, iz)] = DADD(p[R.cell(ix, iy, iz)], pd[R.cell(ix, iy, iz)]);
+  }
+}
+
+// Zero the entries of the reference-layout write-only faces' ghosts are left
+// alone; zero a reference-layout cell array's interior (p_delta reset,
+// G_SMACSolver.cu:1273 zeroes the whole array).
+__global__ void k_fill(double* a, long long n, double v) {
+  long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  for (; t < n; t += (long long)gridDim.x * blockDim.x) a[t] = v;
+}
+
+// ------------------------------------------------------------------------
+// Adjoint pieces.  The projection on F_INTERIOR faces is
+//   u = u* + B G A^+ D u*     (B = diag f_b, G = face gradient, D = divergence)
+// with the zero-mean projection Pi of the pure-Neumann solve, so
+//   dL/du* = g + D^T Pi A^+ G^T B g = g + G psi,  psi = Pi A^+ D_int(B g)
+// using D^T = -G and G^T = -D_int (D_int: divergence over F_INTERIOR faces).
+// rhs_adj = D_int(B g) on fluid cells, written to the padded rhs.
+__global__ void k_adj_divergence(Geom g, RefDims R, double inv_dx, double inv_dy, double inv_dz,
+                                 const double* __restrict__ gx, const double* __restrict__ gy,
+                                 const double* __restrict__ gz, const double* __restrict__ bx,
+                                 const double* __restrict__ by, const double* __restrict__ bz,
+                                 const uint8_t* __restrict__ fluid, double* rhs) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int k = blockIdx.z;
+  if (i >= g.nx || j >= g.ny || k >= g.nz) return;
+  const int c = g.idx(i, j, k);
+  double out = 0.0;
+  if (fluid[c] & 2) {
+    // only faces between two cells carry the projection; wall faces have
+    // f_b = 0 for pure Neumann walls and are excluded explicitly otherwise
+    const double wxm = (i > 0) ? bx[c] : 0.0, wxp = (i < g.nx - 1) ? bx[c + 1] : 0.0;
+    const double wym = (j > 0) ? by[c] : 0.0, wyp = (j < g.ny - 1) ? by[c + g.px] : 0.0;
+    const double wzm = (k > 0) ? bz[c] : 0.0, wzp = (k < g.nz - 1) ? bz[c + g.ps] : 0.0;
+    const int ix = i + 1, iy = j + 1, iz = k + 1;
+    out = (wxp * gx[R.xf(ix + 1, iy, iz)] - wxm * gx[R.xf(ix, iy, iz)]) * inv_dx +
+          (wyp * gy[R.yf(ix, iy + 1, iz)] - wym * gy[R.yf(ix, iy, iz)]) * inv_dy +
+          (wzp * gz[R.zf(ix, iy, iz + 1)] - wzm * gz[R.zf(ix, iy, iz)]) * inv_dz;
+  }
+  rhs[c] = out;
+}
+
+// dL/du* = g + G psi on every face, psi = A^+ D_int(B g) on fluid cells and 0
+// elsewhere (also beyond the walls).  The forward map reads u* on every face
+// of a fluid cell through the divergence, wall faces included, so the
+// gradient term reaches those faces too.  psi = x - shift on fluid cells
+// (shift: the fluid mean of the solve's solution).
+__global__ void k_adj_gradient(Geom g, RefDims R, double inv_dx, double inv_dy, double inv_dz,
+                               const double* __restrict__ x, const uint8_t* __restrict__ fluid, const double* shift,
+                               const double* __restrict__ gx, const double* __restrict__ gy,
+                               const double* __restrict__ gz, double* ox, double* oy, double* oz) {
+  const int ix = blockIdx.x * blockDim.x + threadIdx.x;
+  const int iy = blockIdx.y * blockDim.y + threadIdx.y;
+  const int iz = blockIdx.z;
+  const int Nx = R.Nx, Ny = R.Ny, Nz = R.Nz;
+  const double sh = *shift;
+  // psi at reference cell (cx, cy, cz)
+  auto P = [&](int cx, int cy, int cz) -> double {
+    const int i = cx - 1, j = cy - 1, k = cz - 1;
+    if (i < 0 || j < 0 || k < 0 || i >= g.nx || j >= g.ny || k >= g.nz) return 0.0;
+    const int c = g.idx(i, j, k);
+    return (fluid[c] & 2) ? x[c] - sh : 0.0;
+  };
+  if (ix < Nx + 3 && iy < Ny + 2 && iz < Nz + 2) {
+    const long long f = R.xf(ix, iy, iz);
+    double v = gx[f];
+    if (ix >= 1 && ix <= Nx + 1) v += (P(ix, iy, iz) - P(ix - 1, iy, iz)) * inv_dx;
+    ox[f] = v;
+  }
+  if (ix < Nx + 2 && iy < Ny + 3 && iz < Nz + 2) {
+    const long long f = R.yf(ix, iy, iz);
+    double v = gy[f];
+    if (iy >= 1 && iy <= Ny + 1) v += (P(ix, iy, iz) - P(ix, iy - 1, iz)) * inv_dy;
+    oy[f] = v;
+  }
+  if (ix < Nx + 2 && iy < Ny + 2 && iz < Nz + 3) {
+    const long long f = R.zf(ix, iy, iz);
+    double v = gz[f];
+    if (iz >= 1 && iz <= Nz + 1) v += (P(ix, iy, iz) - P(ix, iy, iz - 1)) * inv_dz;
+    oz[f] = v;
+  }
+}
+
+// Jacobi preconditioner z = (r - shift)/diag on cells with a non-zero
+// diagonal (the reference's z = invAdiag r, G_PCGSolver.cu:248-273).
+template <class T, class C>
+__global__ void __launch_bounds__(TNT) k_jacobi_precond(Geom g, const T* __restrict__ r, const double* shift,
+                                                        Stencil<T, C> S, T* z, const Scalars* s, int kz) {
+  if (s->done) return;
+  typedef acc_t<T> A;
+  const int i = blockIdx.x * TBX + threadIdx.x;
+  const int j = blockIdx.y * TBY + threadIdx.y;
+  const int k0 = blockIdx.z * kz;
+  if (i >= g.nx || j >= g.ny) return;
+  const A sh = shift ? (A)(*shift) : (A)0;
+  const int k1 = min(k0 + kz, g.nz);
+  int c = g.idx(i, j, k0);
+  for (int k = k0; k < k1; ++k, c += g.ps) {
+    A wxm, wxp, wym, wyp, wzm, wzp;
+    S.coeffs(c, g.px, g.ps, wxm, wxp, wym, wyp, wzm, wzp);
+    const A diag = (wxm + wxp) + (wym + wyp) + (wzm + wzp);
+    z[c] = (T)((diag > (A)0) ? ((A)r[c] - sh) / diag : (A)0);
+  }
+}
+
+// ------------------------------------------------------------------------
+// Set-up kernels in the reference layout.
+// SMACSolver::set_face_type / set_cell_type (CFD/SMACSolver.cpp:104-248).
+__global__ void k_box_types(RefDims R, uint8_t* ct, uint8_t* fxt, uint8_t* fyt, uint8_t* fzt) {
+  const int ix = blockIdx.x * blockDim.x + threadIdx.x;
+  const int iy = blockIdx.y * blockDim.y + threadIdx.y;
+  const int iz = blockIdx.z;
+  const int Nx = R.Nx, Ny = R.Ny, Nz = R.Nz;
+  if (ix < Nx + 3 && iy < Ny + 2 && iz < Nz + 2) {
+    uint8_t t = F_GHOST;
+    if (iz >= 1 && iz <= Nz && iy >= 1 && iy <= Ny && ix >= 1 && ix <= Nx + 1)
+      t = (ix == 1 || ix == Nx + 1) ? F_BOUNDARY : F_INTERIOR;
+    fxt[R.xf(ix, iy, iz)] = t;
+  }
+  if (ix < Nx + 2 && iy < Ny + 3 && iz < Nz + 2) {
+    uint8_t t = F_GHOST;
+    if (iz >= 1 && iz <= Nz && iy >= 1 && iy <= Ny + 1 && ix >= 1 && ix <= Nx)
+      t = (iy == 1 || iy == Ny + 1) ? F_BOUNDARY : F_INTERIOR;
+    fyt[R.yf(ix, iy, iz)] = t;
+  }
+  if (ix < Nx + 2 && iy < Ny + 2 && iz < Nz + 3) {
+    uint8_t t = F_GHOST;
+    if (iz >= 1 && iz <= Nz + 1 && iy >= 1 && iy <= Ny && ix >= 1 && ix <= Nx)
+      t = (iz == 1 || iz == Nz + 1) ? F_BOUNDARY : F_INTERIOR;
+    fzt[R.zf(ix, iy, iz)] = t;
+  }
+  if (ix < Nx + 2 && iy < Ny + 2 && iz < Nz + 2) {
+    const bool in = ix >= 1 && ix <= Nx && iy >= 1 && iy <= Ny && iz >= 1 && iz <= Nz;
+    ct[R.cell(ix, iy, iz)] = in ? C_INTERIOR : C_GHOST;
+  }
+}
+
+// k_update_cell_properties_by_alpha (CFD/G_SMACSolver_VoF.cu:1374-1407)
+__global__ void k_vof_rho(RefDims R, const double* __restrict__ alpha, double rho0, double rho1,
+                          const uint8_t* __restrict__ ct, double* rho) {
+  const int ix = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  const int iy = blockIdx.y * blockDim.y + threadIdx.y + 1;
+  const int iz = blockIdx.z + 1;
+  if (ix >= R.Nx + 2 || iy >= R.Ny + 2 || iz >= R.Nz + 2) return;
+  const long long c = R.cell(ix, iy, iz);
+  const uint8_t t = ct[c];
+  if (t == C_INTERIOR || t == C_NEAR_BOUNDARY) {
+    const double a = alpha[c];
+    rho[c] = DADD(DMUL(DADD(1., -a), rho0), DMUL(a, rho1));
+  }
+}
+
+// k_update_{x,y,z}_face_properties_by_alpha (CFD/G_SMACSolver_VoF.cu:1409-1535)
+__global__ void k_vof_faces(RefDims R, const double* __restrict__ rho, const uint8_t* __restrict__ fxt,
+                            const uint8_t* __restrict__ fyt, const uint8_t* __restrict__ fzt, double* fbx, double* fby,
+                            double* fbz, double* firx, double* firy, double* firz) {
+  const int ix = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  const int iy = blockIdx.y * blockDim.y + threadIdx.y + 1;
+  const int iz = blockIdx.z + 1;
+  const int Nx = R.Nx, Ny = R.Ny, Nz = R.Nz;
+  if (!(ix >= Nx + 3 || iy >= Ny + 2 || iz >= Nz + 2)) {
+    const long long f = R.xf(ix, iy, iz);
+    double b = 0.0;
+    if (fxt[f] == F_INTERIOR && ix <= Nx + 1) b = DDIV(1., DMUL(0.5, DADD(rho[R.cell(ix, iy, iz)], rho[R.cell(ix - 1, iy, iz)])));
+    fbx[f] = b;
+    if (firx) firx[f] = b;
+  }
+  if (!(ix >= Nx + 2 || iy >= Ny + 3 || iz >= Nz + 2)) {
+    const long long f = R.yf(ix, iy, iz);
+    double b = 0.0;
+    if (fyt[f] == F_INTERIOR && iy <= Ny + 1) b = DDIV(1., DMUL(0.5, DADD(rho[R.cell(ix, iy, iz)], rho[R.cell(ix, iy - 1, iz)])));
+    fby[f] = b;
+    if (firy) firy[f] = b;
+  }
+  if (!(ix >= Nx + 2 || iy >= Ny + 2 || iz >= Nz + 3)) {
+    const long long f = R.zf(ix, iy, iz);
+    double b = 0.0;
+    if (fzt[f] == F_INTERIOR && iz <= Nz + 1) b = DDIV(1., DMUL(0.5, DADD(rho[R.cell(ix, iy, iz)], rho[R.cell(ix, iy, iz - 1)])));
+    fbz[f] = b;
+    if (firz) firz[f] = b;
+  }
+}
+
+// Solid fraction by 8^3 sub-sampling (k_get_solid_fraction,
+// CFD/G_SMACSolver_IBM.cu:94-147) for a union of non-overlapping spheres.
+// Cells entirely inside or outside a sphere by a margin far above the
+// rounding of the sample coordinates skip the sampling; the count is the same.
+__global__ void k_ibm_spheres(RefDims R, double dx, double dy, double dz, double ox, double oy, double oz,
+                              const double* __restrict__ sph, int nsph, double* sf) {
+  const int ix = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  const int iy = blockIdx.y * blockDim.y + threadIdx.y + 1;
+  const int iz = blockIdx.z + 1;
+  if (ix >= R.Nx + 2 || iy >= R.Ny + 2 || iz >= R.Nz + 2) return;
+  const double xc = DADD(DADD(DMUL(dx, (double)ix), -DMUL(0.5, dx)), ox);
+  const double yc = DADD(DADD(DMUL(dy, (double)iy), -DMUL(0.5, dy)), oy);
+  const double zc = DADD(DADD(DMUL(dz, (double)iz), -DMUL(0.5, dz)), oz);
+  const double xini = DADD(xc, -DMUL(dx, 0.5)), yini = DADD(yc, -DMUL(dy, 0.5)), zini = DADD(zc, -DMUL(dz, 0.5));
+  const double fact = 1. / 8.;
+  const double sdx = DMUL(dx, fact), sdy = DMUL(dy, fact), sdz = DMUL(dz, fact);
+  const double margin = DMUL(1e-6, DADD(DADD(DMUL(dx, dx), DMUL(dy, dy)), DMUL(dz, dz)));
+  int numpts = 0;
+  for (int s = 0; s < nsph; ++s) {
+    const double cx = sph[4 * s], cy = sph[4 * s + 1], cz = sph[4 * s + 2], r = sph[4 * s + 3];
+    const double rsq = DMUL(r, r);
+    const double lx = xini, hx = DADD(xini, dx), ly = yini, hy = DADD(yini, dy), lz = zini, hz = DADD(zini, dz);
+    const double nx_ = fmax(0.0, fmax(DADD(lx, -cx), DADD(cx, -hx)));
+    const double ny_ = fmax(0.0, fmax(DADD(ly, -cy), DADD(cy, -hy)));
+    const double nz_ = fmax(0.0, fmax(DADD(lz, -cz), DADD(cz, -hz)));
+    const double fx = fmax(fabs(DADD(lx, -cx)), fabs(DADD(hx, -cx)));
+    const double fy = fmax(fabs(DADD(ly, -cy)), fabs(DADD(hy, -cy)));
+    const double fz = fmax(fabs(DADD(lz, -cz)), fabs(DADD(hz, -cz)));
+    const double near2 = DADD(DADD(DMUL(nx_, nx_), DMUL(ny_, ny_)), DMUL(nz_, nz_));
+    const double far2 = DADD(DADD(DMUL(fx, fx), DMUL(fy, fy)), DMUL(fz, fz));
+    if (near2 > DADD(rsq, margin)) continue;
+    if (far2 < DADD(rsq, -margin)) { numpts += 512; continue; }
+    for (int kz = 0; kz < 8; ++kz)
+      for (int ky = 0; ky < 8; ++ky)
+        for (int kx = 0; kx < 8; ++kx) {
+          const double x_pt = DADD(xini, DMUL(sdx, kx + 0.5));
+          const double y_pt = DADD(yini, DMUL(sdy, ky + 0.5));
+          const double z_pt = DADD(zini, DMUL(sdz, kz + 0.5));
+          const double ddx = DADD(x_pt, -cx), ddy = DADD(y_pt, -cy), ddz = DADD(z_pt, -cz);
+          if (DADD(DADD(DMUL(ddx, ddx), DMUL(ddy, ddy)), DMUL(ddz, ddz)) <= rsq) numpts += 1;
+        }
+  }
+  double frac = DMUL((double)numpts, 1. / 512.);
+  if (frac > 1. - 1.e-2) frac = 1.0;
+  sf[R.cell(ix, iy, iz)] = frac;
+}
+
+// k_set_solid_cell_from_ibm (CFD/G_SMACSolver_IBM.cu:763-792)
+__global__ void k_ibm_set_solid(RefDims R, const double* __restrict__ sf, uint8_t* ct, uint8_t* fxt, uint8_t* fyt,
+                                uint8_t* fzt) {
+  const int ix = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  const int iy = blockIdx.y * blockDim.y + threadIdx.y + 1;
+  const int iz = blockIdx.z + 1;
+  if (ix >= R.Nx + 2 || iy >= R.Ny + 2 || iz >= R.Nz + 2) return;
+  if (sf[R.cell(ix, iy, iz)] > 1. - 1.e-12) {
+    ct[R.cell(ix, iy, iz)] = C_SOLID;
+    fxt[R.xf(ix, iy, iz)] = F_BOUNDARY;
+    fxt[R.xf(ix + 1, iy, iz)] = F_BOUNDARY;
+    fyt[R.yf(ix, iy, iz)] = F_BOUNDARY;
+    fyt[R.yf(ix, iy + 1, iz)] = F_BOUNDARY;
+    fzt[R.zf(ix, iy, iz)] = F_BOUNDARY;
+    fzt[R.zf(ix, iy, iz + 1)] = F_BOUNDARY;
+  }
+}
+
+}  // namespace smac

@@ -1,0 +1,295 @@
+"""Host-side mirror of the reference's pressure-solver seam over the C ABI.
+
+Reference interface (CFD/pressure_solver/G_PressureSolverBase.h:24-42,
+CFD/pressure_solver/G_PCGSolver.h:17-38, CFD/G_SMACSolver.h:9-125):
+
+    struct G_PressureSolverBase { virtual void solve(G_SMACSolver&) = 0; double tol_; ... };
+    struct G_PCGSolver : G_PressureSolverBase { void set_solver(PCG_TYPES); ... };
+    G_SMACSolver::solve_poisson()          -> pressure_solver_->solve(*this)   (G_SMACSolver.cu:1499-1501)
+    G_SMACSolver::correct_vof_velocity()   -> k_correct_vof_velocity; p_delta_ = 0 (G_SMACSolver.cu:1269-1275)
+
+Here `DeviceGrid` holds the G_StaggeredGrid members the path reads or writes
+as CUDA tensors in the reference layout, `B200PressureSolver` is the
+G_PressureSolverBase replacement (same `tol_`, `set_solver`, `solve`), and
+`SMACStep` carries the two G_SMACSolver calls.  All compute goes through
+libsmac_b200.so; there is no Python or CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass
+
+import numpy as np
+import torch
+
+from . import _native as nat
+from .workloads import Case, shapes
+
+
+def _ptr(t):
+    if t is None:
+        return None
+    assert t.is_cuda and t.is_contiguous(), "device tensors must be contiguous CUDA tensors"
+    return ctypes.c_void_p(t.data_ptr())
+
+
+def _dev(a, dtype, device):
+    if isinstance(a, torch.Tensor):
+        return a.to(device=device, dtype=dtype).contiguous()
+    return torch.from_numpy(np.ascontiguousarray(a)).to(device=device, dtype=dtype)
+
+
+@dataclass
+class DeviceGrid:
+    """The G_StaggeredGrid members of the projection (CFD/memberList/gridMembers.def)."""
+    Nx_: int
+    Ny_: int
+    Nz_: int
+    dx_: float
+    dy_: float
+    dz_: float
+    f_vx_star_: torch.Tensor
+    f_vy_star_: torch.Tensor
+    f_vz_star_: torch.Tensor
+    f_bx_: torch.Tensor
+    f_by_: torch.Tensor
+    f_bz_: torch.Tensor
+    f_inv_rhox_: torch.Tensor
+    f_inv_rhoy_: torch.Tensor
+    f_inv_rhoz_: torch.Tensor
+    celltype_: torch.Tensor
+    f_xtype_: torch.Tensor
+    f_ytype_: torch.Tensor
+    f_ztype_: torch.Tensor
+    p_: torch.Tensor
+    p_delta_: torch.Tensor
+    rhs_: torch.Tensor
+    f_vx_: torch.Tensor
+    f_vy_: torch.Tensor
+    f_vz_: torch.Tensor
+    void_fraction_: torch.Tensor | None = None
+    void_fraction_old_: torch.Tensor | None = None
+    f_sx_: torch.Tensor | None = None
+    f_sy_: torch.Tensor | None = None
+    f_sz_: torch.Tensor | None = None
+
+    @property
+    def N(self):
+        return (self.Nx_, self.Ny_, self.Nz_)
+
+    @staticmethod
+    def from_case(case: Case, device="cuda") -> "DeviceGrid":
+        sh = shapes(case.N)
+        f64, u8 = torch.float64, torch.uint8
+        z = lambda k: torch.zeros(sh[k], dtype=f64, device=device)  # noqa: E731
+        return DeviceGrid(
+            *case.N, *case.h,
+            f_vx_star_=_dev(case.vxs, f64, device), f_vy_star_=_dev(case.vys, f64, device),
+            f_vz_star_=_dev(case.vzs, f64, device),
+            f_bx_=_dev(case.fbx, f64, device), f_by_=_dev(case.fby, f64, device), f_bz_=_dev(case.fbz, f64, device),
+            f_inv_rhox_=_dev(case.fbx, f64, device), f_inv_rhoy_=_dev(case.fby, f64, device),
+            f_inv_rhoz_=_dev(case.fbz, f64, device),
+            celltype_=_dev(case.ct, u8, device), f_xtype_=_dev(case.fxt, u8, device),
+            f_ytype_=_dev(case.fyt, u8, device), f_ztype_=_dev(case.fzt, u8, device),
+            p_=z("cell"), p_delta_=z("cell"), rhs_=z("cell"), f_vx_=z("x"), f_vy_=z("y"), f_vz_=z("z"),
+        )
+
+
+class B200PressureSolver:
+    """Drop-in for G_PressureSolverBase / G_PCGSolver over libsmac_b200.so.
+
+    `tol_` has the meaning of the chosen stop rule: by default the relative
+    FP64 true residual ||b - A x|| / ||b||; with stop_rule=STOP_REFERENCE the
+    reference's test max|r| * dt < tol_ (G_PCGSolver.cu:884-903).
+    """
+
+    def __init__(self, N, h, precision=nat.PRECISION_FP64, tol=1e-8, stream=None, **options):
+        self._lib = nat.load()
+        self.N = tuple(N)
+        self.h = tuple(h)
+        self.opts = nat.default_options(precision=precision, tol=tol, **options)
+        self.desc = nat.GridDesc(*self.N, *self.h)
+        self._stream = stream if stream is not None else torch.cuda.current_stream()
+        handle = ctypes.c_void_p()
+        nat.check(self._lib.smac_create(ctypes.byref(self.desc), ctypes.byref(self.opts),
+                                        ctypes.c_void_p(self._stream.cuda_stream), ctypes.byref(handle)))
+        self._h = handle
+        self.last_stats: dict | None = None
+
+    # -- G_PressureSolverBase surface -------------------------------------
+    @property
+    def tol_(self) -> float:
+        return self.opts.tol
+
+    @tol_.setter
+    def tol_(self, v: float):
+        self.opts.tol = float(v)
+        self._apply()
+
+    def set_solver(self, pcg_type: int):
+        """G_PCGSolver::set_solver(PCG_TYPES) (G_PCGSolver.cu:592-613)."""
+        self.opts.solver_type = int(pcg_type)
+        self._apply()
+
+    def set_options(self, **kw):
+        for k, v in kw.items():
+            setattr(self.opts, k, v)
+        self._apply()
+
+    def _apply(self):
+        if getattr(self, "_h", None):
+            nat.check(self._lib.smac_set_options(self._h, ctypes.byref(self.opts)))
+
+    def solve(self, solv: "SMACStep", raise_on_fail=True) -> dict:
+        """G_PressureSolverBase::solve(G_SMACSolver&): RHS from the grid, then
+        the Poisson solve into grid.p_delta_."""
+        g = solv.grid_
+        self.set_coefficients(g)
+        self.divergence(g, solv.dt_)
+        return self.solve_rhs(g.p_delta_, raise_on_fail=raise_on_fail)
+
+    # -- finer-grained calls ----------------------------------------------
+    def set_coefficients(self, g: DeviceGrid):
+        nat.check(self._lib.smac_set_coefficients(
+            self._h, _ptr(g.f_bx_), _ptr(g.f_by_), _ptr(g.f_bz_), _ptr(g.celltype_), _ptr(g.f_xtype_),
+            _ptr(g.f_ytype_), _ptr(g.f_ztype_)))
+
+    def divergence(self, g: DeviceGrid, dt: float):
+        nat.check(self._lib.smac_divergence(
+            self._h, _ptr(g.f_vx_star_), _ptr(g.f_vy_star_), _ptr(g.f_vz_star_), _ptr(g.void_fraction_),
+            _ptr(g.void_fraction_old_), _ptr(g.f_sx_), _ptr(g.f_sy_), _ptr(g.f_sz_), ctypes.c_double(dt),
+            _ptr(g.rhs_)))
+
+    def set_rhs(self, rhs: torch.Tensor):
+        nat.check(self._lib.smac_set_rhs(self._h, _ptr(rhs)))
+
+    def solve_rhs(self, p_delta: torch.Tensor, raise_on_fail=True) -> dict:
+        st = nat.Stats()
+        rc = self._lib.smac_solve(self._h, _ptr(p_delta), ctypes.byref(st))
+        self.last_stats = st.as_dict()
+        if raise_on_fail:
+            nat.check(rc)
+        elif rc not in (nat.OK, nat.NOT_CONVERGED, nat.BREAKDOWN, nat.NAN):
+            nat.check(rc)
+        return self.last_stats
+
+    def correct(self, g: DeviceGrid, dt: float, zero_p_delta=True):
+        nat.check(self._lib.smac_correct(
+            self._h, _ptr(g.p_delta_), _ptr(g.p_), _ptr(g.f_vx_star_), _ptr(g.f_vy_star_), _ptr(g.f_vz_star_),
+            _ptr(g.f_inv_rhox_), _ptr(g.f_inv_rhoy_), _ptr(g.f_inv_rhoz_), _ptr(g.f_sx_), _ptr(g.f_sy_),
+            _ptr(g.f_sz_), ctypes.c_double(dt), _ptr(g.f_vx_), _ptr(g.f_vy_), _ptr(g.f_vz_),
+            ctypes.c_int(1 if zero_p_delta else 0)))
+
+    def project(self, vxs, vys, vzs, dt, p_delta, vx, vy, vz, raise_on_fail=True) -> dict:
+        st = nat.Stats()
+        rc = self._lib.smac_project(self._h, _ptr(vxs), _ptr(vys), _ptr(vzs), ctypes.c_double(dt), _ptr(p_delta),
+                                    _ptr(vx), _ptr(vy), _ptr(vz), ctypes.byref(st))
+        self.last_stats = st.as_dict()
+        if raise_on_fail:
+            nat.check(rc)
+        return self.last_stats
+
+    def project_adjoint(self, gvx, gvy, gvz, ox, oy, oz, phi=None, raise_on_fail=True) -> dict:
+        st = nat.Stats()
+        rc = self._lib.smac_project_adjoint(self._h, _ptr(gvx), _ptr(gvy), _ptr(gvz), _ptr(ox), _ptr(oy), _ptr(oz),
+                                            _ptr(phi), ctypes.byref(st))
+        self.last_stats = st.as_dict()
+        if raise_on_fail:
+            nat.check(rc)
+        return self.last_stats
+
+    def apply_A(self, x: torch.Tensor, y: torch.Tensor):
+        nat.check(self._lib.smac_apply_A(self._h, _ptr(x), _ptr(y)))
+
+    def time_kernel(self, kernel_id: int, reps: int = 20):
+        ms = ctypes.c_float()
+        b = ctypes.c_double()
+        nat.check(self._lib.smac_time_kernel(self._h, kernel_id, reps, ctypes.byref(ms), ctypes.byref(b)))
+        return ms.value, b.value
+
+    def num_levels(self) -> int:
+        n = ctypes.c_int()
+        nat.check(self._lib.smac_level_shape(self._h, 0, None, None, None, ctypes.byref(n)))
+        return n.value
+
+    def level_shape(self, level: int):
+        a, b, c, n = ctypes.c_int(), ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        nat.check(self._lib.smac_level_shape(self._h, level, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c),
+                                             ctypes.byref(n)))
+        return (a.value, b.value, c.value)
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.smac_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class SMACStep:
+    """The G_SMACSolver calls around the seam, in the reference's order
+    (CFD/main.cu:313-315): solve_poisson(), then correct_vof_velocity()."""
+
+    def __init__(self, grid: DeviceGrid, dt: float = 1.0):
+        self.grid_ = grid
+        self.dt_ = float(dt)
+        self.inv_dt_ = 1.0 / self.dt_
+        self.pressure_solver_: B200PressureSolver | None = None
+
+    def solve_poisson(self):
+        return self.pressure_solver_.solve(self)
+
+    def correct_vof_velocity(self):
+        self.pressure_solver_.correct(self.grid_, self.dt_, zero_p_delta=True)
+
+
+# -- set-up helpers on the device (reference layout) --------------------------
+def box_types_device(N, device="cuda"):
+    sh = shapes(N)
+    ct = torch.empty(sh["cell"], dtype=torch.uint8, device=device)
+    fxt = torch.empty(sh["x"], dtype=torch.uint8, device=device)
+    fyt = torch.empty(sh["y"], dtype=torch.uint8, device=device)
+    fzt = torch.empty(sh["z"], dtype=torch.uint8, device=device)
+    d = nat.GridDesc(*N, 1.0, 1.0, 1.0)
+    s = torch.cuda.current_stream().cuda_stream
+    nat.check(nat.load().smac_box_types(ctypes.byref(d), _ptr(ct), _ptr(fxt), _ptr(fyt), _ptr(fzt),
+                                        ctypes.c_void_p(s)))
+    return ct, fxt, fyt, fzt
+
+
+def assemble_vof_device(N, h, alpha, rho0, rho1, ct, fxt, fyt, fzt):
+    sh = shapes(N)
+    dev = alpha.device
+    rho = torch.ones(sh["cell"], dtype=torch.float64, device=dev)
+    fb = [torch.zeros(sh[k], dtype=torch.float64, device=dev) for k in "xyz"]
+    fir = [torch.zeros(sh[k], dtype=torch.float64, device=dev) for k in "xyz"]
+    d = nat.GridDesc(*N, *h)
+    s = torch.cuda.current_stream().cuda_stream
+    nat.check(nat.load().smac_assemble_vof(ctypes.byref(d), _ptr(alpha), ctypes.c_double(rho0), ctypes.c_double(rho1),
+                                           _ptr(ct), _ptr(fxt), _ptr(fyt), _ptr(fzt), _ptr(rho), *map(_ptr, fb),
+                                           *map(_ptr, fir), ctypes.c_void_p(s)))
+    return rho, fb, fir
+
+
+def ibm_solid_fraction_device(N, h, origin, spheres, device="cuda"):
+    sh = shapes(N)
+    sf = torch.zeros(sh["cell"], dtype=torch.float64, device=device)
+    sph = np.ascontiguousarray(np.asarray(spheres, np.float64).reshape(-1))
+    org = (ctypes.c_double * 3)(*origin)
+    d = nat.GridDesc(*N, *h)
+    s = torch.cuda.current_stream().cuda_stream
+    nat.check(nat.load().smac_ibm_solid_fraction_spheres(
+        ctypes.byref(d), org, sph.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), ctypes.c_int(len(sph) // 4),
+        _ptr(sf), ctypes.c_void_p(s)))
+    return sf
+
+
+def ibm_set_solid_device(N, sf, ct, fxt, fyt, fzt):
+    d = nat.GridDesc(*N, 1.0, 1.0, 1.0)
+    s = torch.cuda.current_stream().cuda_stream
+    nat.check(nat.load().smac_ibm_set_solid_cells(ctypes.byref(d), _ptr(sf), _ptr(ct), _ptr(fxt), _ptr(fyt),
+                                                  _ptr(fzt), ctypes.c_void_p(s)))

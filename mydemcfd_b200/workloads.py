@@ -1,0 +1,270 @@
+"""Seeded synthetic inputs for the projection, in the reference layout.
+
+Arrays are numpy, shape (sz, sy, sx), x fastest (CFD/MyArray.h:43-51);
+cells (N+2)^3, x-faces (Nx+3)(Ny+2)(Nz+2) and so on (gridMembers.def).
+
+Random numbers: SplitMix64(seed) -> u = (bits >> 11) * 2^-53 -> 2u - 1,
+uniform in [-1, 1); the i-th draw of a stream depends only on (seed, i), so
+the same arrays come out on any host.
+
+Workloads (BASELINE configurations; seeded synthetic fields with the stated
+shapes stand in for simulation state):
+  plain   - single phase, rho = 1 (f_b = 1 on interior faces), dt = 1,
+            u* i.i.d. U[-1,1) on F_INTERIOR faces, 0 on the others
+  vof     - a sphere of radius 0.25 L centred U[0.3,0.7]^3, alpha ramped
+            linearly over 1.5 cells across the interface, density ratio
+            rho1/rho0 (alpha = 1 inside), f_b = 1/(0.5(rho_L+rho_R))
+  ibm     - `nsph` non-overlapping spheres, radii U[4,12] cells, centres
+            uniform in the interior with rejection sampling; cells >= 99%
+            solid (8^3 sub-samples) become C_SOLID with zero-flux faces
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass, field
+
+import numpy as np
+
+F_INTERIOR, F_BOUNDARY, F_GHOST = 0, 1, 2
+C_INTERIOR, C_GHOST, C_SOLID = 0, 2, 3
+
+_GOLDEN = np.uint64(0x9E3779B97F4A7C15)
+_M1 = np.uint64(0xBF58476D1CE4E5B9)
+_M2 = np.uint64(0x94D049BB133111EB)
+
+
+def splitmix64(seed: int, n: int, offset: int = 0) -> np.ndarray:
+    """Draws offset+1 .. offset+n of SplitMix64 seeded with `seed`."""
+    i = np.arange(offset + 1, offset + n + 1, dtype=np.uint64)
+    with np.errstate(over="ignore"):
+        z = np.uint64(seed & 0xFFFFFFFFFFFFFFFF) + i * _GOLDEN
+        z = (z ^ (z >> np.uint64(30))) * _M1
+        z = (z ^ (z >> np.uint64(27))) * _M2
+        z = z ^ (z >> np.uint64(31))
+    return z
+
+
+def uniform01(seed: int, n: int, offset: int = 0) -> np.ndarray:
+    return (splitmix64(seed, n, offset) >> np.uint64(11)).astype(np.float64) * (2.0 ** -53)
+
+
+def uniform_pm1(seed: int, n: int, offset: int = 0) -> np.ndarray:
+    return 2.0 * uniform01(seed, n, offset) - 1.0
+
+
+def substream(seed: int, tag: int) -> int:
+    """Seed of an independent stream derived from (seed, tag)."""
+    return int(splitmix64((seed * 0x100000001B3 + tag) & 0xFFFFFFFFFFFFFFFF, 1)[0])
+
+
+# ---------------------------------------------------------------------------
+def shapes(N):
+    nx, ny, nz = N
+    return {
+        "cell": (nz + 2, ny + 2, nx + 2),
+        "x": (nz + 2, ny + 2, nx + 3),
+        "y": (nz + 2, ny + 3, nx + 2),
+        "z": (nz + 3, ny + 2, nx + 2),
+    }
+
+
+def box_types(N):
+    """SMACSolver::set_face_type / set_cell_type (CFD/SMACSolver.cpp:104-248)."""
+    nx, ny, nz = N
+    sh = shapes(N)
+    fxt = np.full(sh["x"], F_GHOST, np.uint8)
+    fyt = np.full(sh["y"], F_GHOST, np.uint8)
+    fzt = np.full(sh["z"], F_GHOST, np.uint8)
+    fxt[1:nz + 1, 1:ny + 1, 1:nx + 2] = F_INTERIOR
+    fxt[1:nz + 1, 1:ny + 1, 1] = F_BOUNDARY
+    fxt[1:nz + 1, 1:ny + 1, nx + 1] = F_BOUNDARY
+    fyt[1:nz + 1, 1:ny + 2, 1:nx + 1] = F_INTERIOR
+    fyt[1:nz + 1, 1, 1:nx + 1] = F_BOUNDARY
+    fyt[1:nz + 1, ny + 1, 1:nx + 1] = F_BOUNDARY
+    fzt[1:nz + 2, 1:ny + 1, 1:nx + 1] = F_INTERIOR
+    fzt[1, 1:ny + 1, 1:nx + 1] = F_BOUNDARY
+    fzt[nz + 1, 1:ny + 1, 1:nx + 1] = F_BOUNDARY
+    ct = np.full(sh["cell"], C_GHOST, np.uint8)
+    ct[1:nz + 1, 1:ny + 1, 1:nx + 1] = C_INTERIOR
+    return ct, fxt, fyt, fzt
+
+
+def set_solid_cells(sf, ct, fxt, fyt, fzt):
+    """k_set_solid_cell_from_ibm (CFD/G_SMACSolver_IBM.cu:763-792), in place."""
+    solid = np.zeros(sf.shape, bool)
+    solid[1:, 1:, 1:] = sf[1:, 1:, 1:] > 1.0 - 1e-12
+    ct[solid] = C_SOLID
+    z, y, x = np.nonzero(solid)
+    fxt[z, y, x] = F_BOUNDARY
+    fxt[z, y, x + 1] = F_BOUNDARY
+    fyt[z, y, x] = F_BOUNDARY
+    fyt[z, y + 1, x] = F_BOUNDARY
+    fzt[z, y, x] = F_BOUNDARY
+    fzt[z + 1, y, x] = F_BOUNDARY
+
+
+def seeded_faces(N, seed, fxt, fyt, fzt):
+    """Face field i.i.d. U[-1,1) on F_INTERIOR faces and 0 elsewhere (the
+    wall rule of G_BoundaryFunctions.h:388-389: no-slip u* = 0)."""
+    sh = shapes(N)
+    out = []
+    for tag, (key, t) in enumerate((("x", fxt), ("y", fyt), ("z", fzt))):
+        n = int(np.prod(sh[key]))
+        v = uniform_pm1(substream(seed, tag + 1), n).reshape(sh[key])
+        v[t != F_INTERIOR] = 0.0
+        out.append(np.ascontiguousarray(v))
+    return tuple(out)
+
+
+def face_coeffs_vof(N, alpha, rho0, rho1, ct, fxt, fyt, fzt):
+    """k_update_cell_properties_by_alpha + k_update_*_face_properties_by_alpha
+    (CFD/G_SMACSolver_VoF.cu:1374-1535) in numpy: same operations."""
+    nx, ny, nz = N
+    sh = shapes(N)
+    rho = np.ones(sh["cell"])
+    fluid = (ct == C_INTERIOR) | (ct == 1)
+    fluid[0, :, :] = False
+    fluid[:, 0, :] = False
+    fluid[:, :, 0] = False
+    rho[fluid] = (1.0 - alpha[fluid]) * rho0 + alpha[fluid] * rho1
+    fbx = np.zeros(sh["x"])
+    fby = np.zeros(sh["y"])
+    fbz = np.zeros(sh["z"])
+    m = fxt[:, :, 1:nx + 2] == F_INTERIOR
+    fr = 0.5 * (rho[:, :, 1:nx + 2] + rho[:, :, 0:nx + 1])
+    fbx[:, :, 1:nx + 2] = np.where(m, 1.0 / np.where(m, fr, 1.0), 0.0)
+    m = fyt[:, 1:ny + 2, :] == F_INTERIOR
+    fr = 0.5 * (rho[:, 1:ny + 2, :] + rho[:, 0:ny + 1, :])
+    fby[:, 1:ny + 2, :] = np.where(m, 1.0 / np.where(m, fr, 1.0), 0.0)
+    m = fzt[1:nz + 2, :, :] == F_INTERIOR
+    fr = 0.5 * (rho[1:nz + 2, :, :] + rho[0:nz + 1, :, :])
+    fbz[1:nz + 2, :, :] = np.where(m, 1.0 / np.where(m, fr, 1.0), 0.0)
+    return rho, (fbx, fby, fbz)
+
+
+def constant_coeffs(N, fxt, fyt, fzt, value=1.0):
+    """rho = 1 everywhere: f_b = 1 on F_INTERIOR faces, 0 on the others."""
+    return tuple(np.where(t == F_INTERIOR, value, 0.0) for t in (fxt, fyt, fzt))
+
+
+def cell_centres(N, h, origin=(0.0, 0.0, 0.0)):
+    """StaggeredGrid::get_cell_coord (CFD/StaggeredGrid.h:121-142)."""
+    nx, ny, nz = N
+    x = h[0] * np.arange(nx + 2) - 0.5 * h[0] + origin[0]
+    y = h[1] * np.arange(ny + 2) - 0.5 * h[1] + origin[1]
+    z = h[2] * np.arange(nz + 2) - 0.5 * h[2] + origin[2]
+    return x, y, z
+
+
+def sphere_alpha(N, h, centre, radius, width_cells=1.5):
+    """Volume fraction of a sphere: 1 inside, 0 outside, linear across a band
+    of width_cells cells centred on the interface."""
+    x, y, z = cell_centres(N, h)
+    Z, Y, X = np.meshgrid(z, y, x, indexing="ij")
+    r = np.sqrt((X - centre[0]) ** 2 + (Y - centre[1]) ** 2 + (Z - centre[2]) ** 2)
+    w = width_cells * min(h)
+    return np.clip(0.5 - (r - radius) / w, 0.0, 1.0)
+
+
+def random_spheres(N, h, seed, nsph=200, rmin_cells=4.0, rmax_cells=12.0, gap_cells=2.0, margin_cells=2.0,
+                   max_tries=200000):
+    """Non-overlapping spheres (x, y, z, r) in physical units, rejection sampled."""
+    nx, ny, nz = N
+    hmin = min(h)
+    L = np.array([nx * h[0], ny * h[1], nz * h[2]])
+    st = substream(seed, 77)
+    spheres = []
+    k = 0
+    tries = 0
+    while len(spheres) < nsph and tries < max_tries:
+        u = uniform01(st, 4, offset=4 * k)
+        k += 1
+        tries += 1
+        r = (rmin_cells + (rmax_cells - rmin_cells) * u[3]) * hmin
+        lo = r + margin_cells * hmin
+        c = lo + (L - 2 * lo) * u[:3]
+        if np.any(L - 2 * lo <= 0):
+            continue
+        ok = True
+        for s in spheres:
+            if np.linalg.norm(c - s[:3]) < r + s[3] + gap_cells * hmin:
+                ok = False
+                break
+        if ok:
+            spheres.append(np.array([c[0], c[1], c[2], r]))
+    return np.array(spheres).reshape(-1, 4)
+
+
+@dataclass
+class Case:
+    """Inputs of one projection in the reference layout (host numpy)."""
+    name: str
+    N: tuple
+    h: tuple
+    dt: float
+    vxs: np.ndarray
+    vys: np.ndarray
+    vzs: np.ndarray
+    fbx: np.ndarray
+    fby: np.ndarray
+    fbz: np.ndarray
+    ct: np.ndarray
+    fxt: np.ndarray
+    fyt: np.ndarray
+    fzt: np.ndarray
+    meta: dict = field(default_factory=dict)
+
+    @property
+    def fir(self):
+        return (self.fbx, self.fby, self.fbz)
+
+
+def plain_case(n=64, seed=1, dt=1.0, N=None):
+    N = tuple(N) if N is not None else (n, n, n)
+    h = tuple(1.0 / N[0] for _ in range(3))
+    ct, fxt, fyt, fzt = box_types(N)
+    vxs, vys, vzs = seeded_faces(N, seed, fxt, fyt, fzt)
+    fbx, fby, fbz = constant_coeffs(N, fxt, fyt, fzt)
+    return Case(f"plain{N[0]}", N, h, dt, vxs, vys, vzs, fbx, fby, fbz, ct, fxt, fyt, fzt,
+                {"seed": seed})
+
+
+def vof_case(n=192, seed=3, ratio=1000.0, dt=1.0, width_cells=1.5):
+    N = (n, n, n)
+    h = (1.0 / n,) * 3
+    ct, fxt, fyt, fzt = box_types(N)
+    u = uniform01(substream(seed, 11), 3)
+    centre = 0.3 + 0.4 * u
+    alpha = sphere_alpha(N, h, centre, 0.25, width_cells)
+    rho, (fbx, fby, fbz) = face_coeffs_vof(N, alpha, 1.0, ratio, ct, fxt, fyt, fzt)
+    vxs, vys, vzs = seeded_faces(N, seed, fxt, fyt, fzt)
+    return Case(f"vof{n}", N, h, dt, vxs, vys, vzs, fbx, fby, fbz, ct, fxt, fyt, fzt,
+                {"seed": seed, "alpha": alpha, "rho": rho, "centre": centre, "ratio": ratio})
+
+
+def ibm_case(n=256, seed=4, nsph=200, dt=1.0, solid_fraction=None, rmin_cells=4.0, rmax_cells=12.0):
+    """`solid_fraction(N, h, origin, spheres)` computes the 8^3-sampled solid
+    fraction (the GPU kernel or the oracle); it is required."""
+    N = (n, n, n)
+    h = (1.0 / n,) * 3
+    spheres = random_spheres(N, h, seed, nsph=nsph, rmin_cells=rmin_cells, rmax_cells=rmax_cells)
+    sf = solid_fraction(N, h, (0.0, 0.0, 0.0), spheres)
+    ct, fxt, fyt, fzt = box_types(N)
+    set_solid_cells(sf, ct, fxt, fyt, fzt)
+    fbx, fby, fbz = constant_coeffs(N, fxt, fyt, fzt)
+    vxs, vys, vzs = seeded_faces(N, seed, fxt, fyt, fzt)
+    return Case(f"ibm{n}", N, h, dt, vxs, vys, vzs, fbx, fby, fbz, ct, fxt, fyt, fzt,
+                {"seed": seed, "spheres": spheres, "sf": sf, "solid_cells": int((ct == C_SOLID).sum())})
+
+
+def interior(a):
+    """Interior block of a reference-layout cell array."""
+    return a[1:-1, 1:-1, 1:-1]
+
+
+def demean_fluid(p, ct):
+    """p minus its mean over C_INTERIOR cells (interior block returned)."""
+    pi = interior(p).copy()
+    m = interior(ct) == C_INTERIOR
+    pi[m] -= pi[m].mean()
+    pi[~m] = 0.0
+    return pi

@@ -1,0 +1,251 @@
+"""ctypes binding of ``libsmac_oracle.so`` (see ``smac_oracle.cpp``).
+
+TEST INFRASTRUCTURE ONLY -- the checker for the CUDA path, never the product.
+All arrays are numpy arrays in the reference layout: shape (sz, sy, sx),
+C order, so that flat index = (z*sy + y)*sx + x (CFD/MyArray.h:43-51).
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+from dataclasses import dataclass
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "libsmac_oracle.so")
+_lib = None
+
+# CFD/Enums.h:25-30
+STANDARD_PCG = 0
+PURENEUMANN_STANDARD_PCG = 1
+GMG_PCG = 2
+PURENEUMANN_GMG_PCG = 3
+
+STOP_REFERENCE = 0      # max|r|*dt < tol every check_freq iterations (G_PCGSolver.cu:884-903)
+STOP_REL_RECURSIVE = 1  # ||r||/||b|| < tol on the recursive residual, same frequency
+STOP_REL_TRUE = 2       # ||b - A p||/||b|| < tol, every iteration
+
+
+class OrcStats(ctypes.Structure):
+    _fields_ = [
+        ("iterations", ctypes.c_int),
+        ("converged", ctypes.c_int),
+        ("norm_b", ctypes.c_double),
+        ("res_max", ctypes.c_double),
+        ("res_rel", ctypes.c_double),
+        ("true_res_rel", ctypes.c_double),
+        ("num_levels", ctypes.c_int),
+        ("status", ctypes.c_int),
+    ]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+_dp = ctypes.POINTER(ctypes.c_double)
+_u8p = ctypes.POINTER(ctypes.c_uint8)
+
+
+class OrcProblem(ctypes.Structure):
+    _fields_ = [
+        ("Nx", ctypes.c_int), ("Ny", ctypes.c_int), ("Nz", ctypes.c_int),
+        ("dx", ctypes.c_double), ("dy", ctypes.c_double), ("dz", ctypes.c_double), ("dt", ctypes.c_double),
+        ("vxs", _dp), ("vys", _dp), ("vzs", _dp),
+        ("eps", _dp), ("eps_old", _dp),
+        ("fbx", _dp), ("fby", _dp), ("fbz", _dp),
+        ("fsx", _dp), ("fsy", _dp), ("fsz", _dp),
+        ("ct", _u8p), ("fxt", _u8p), ("fyt", _u8p), ("fzt", _u8p),
+    ]
+
+
+def build(force: bool = False) -> str:
+    """Compile libsmac_oracle.so with the Makefile beside this file."""
+    if force or not os.path.exists(_LIB_PATH) or (
+        os.path.getmtime(_LIB_PATH) < os.path.getmtime(os.path.join(_HERE, "smac_oracle.cpp"))
+    ):
+        subprocess.run(["make", "-C", _HERE, "libsmac_oracle.so"], check=True,
+                       stdout=subprocess.DEVNULL)
+    return _LIB_PATH
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        build()
+        _lib = ctypes.CDLL(_LIB_PATH)
+        _lib.orc_solve.restype = ctypes.c_int
+        _lib.orc_num_threads.restype = ctypes.c_int
+    return _lib
+
+
+def _p(a, ctype=ctypes.c_double):
+    if a is None:
+        return None
+    assert a.flags["C_CONTIGUOUS"], "oracle arrays must be C contiguous"
+    return a.ctypes.data_as(ctypes.POINTER(ctype))
+
+
+def _u8(a):
+    return _p(a, ctypes.c_uint8)
+
+
+def num_threads() -> int:
+    return lib().orc_num_threads()
+
+
+def set_num_threads(n: int) -> None:
+    lib().orc_set_num_threads(int(n))
+
+
+# ---------------------------------------------------------------------------
+# shapes (CFD/memberList/gridMembers.def)
+def cell_shape(N):
+    nx, ny, nz = N
+    return (nz + 2, ny + 2, nx + 2)
+
+
+def xface_shape(N):
+    nx, ny, nz = N
+    return (nz + 2, ny + 2, nx + 3)
+
+
+def yface_shape(N):
+    nx, ny, nz = N
+    return (nz + 2, ny + 3, nx + 2)
+
+
+def zface_shape(N):
+    nx, ny, nz = N
+    return (nz + 3, ny + 2, nx + 2)
+
+
+def set_face_type(N):
+    fxt = np.empty(xface_shape(N), np.uint8)
+    fyt = np.empty(yface_shape(N), np.uint8)
+    fzt = np.empty(zface_shape(N), np.uint8)
+    lib().orc_set_face_type(*N, _u8(fxt), _u8(fyt), _u8(fzt))
+    return fxt, fyt, fzt
+
+
+def set_cell_type(N):
+    ct = np.empty(cell_shape(N), np.uint8)
+    lib().orc_set_cell_type(*N, _u8(ct))
+    return ct
+
+
+def solid_fraction_spheres(N, h, origin, spheres):
+    sf = np.zeros(cell_shape(N), np.float64)
+    sph = np.ascontiguousarray(np.asarray(spheres, np.float64).reshape(-1, 4))
+    c = ctypes.c_double
+    lib().orc_solid_fraction_spheres(*N, c(h[0]), c(h[1]), c(h[2]), c(origin[0]), c(origin[1]), c(origin[2]),
+                                     _p(sph), ctypes.c_int(sph.shape[0]), _p(sf))
+    return sf
+
+
+def set_solid_cells(N, sf, ct, fxt, fyt, fzt):
+    lib().orc_set_solid_cells(*N, _p(sf), _u8(ct), _u8(fxt), _u8(fyt), _u8(fzt))
+
+
+def face_coeffs_vof(N, alpha, rho0, rho1, ct, fxt, fyt, fzt):
+    rho = np.ones(cell_shape(N), np.float64)
+    fbx = np.zeros(xface_shape(N)); fby = np.zeros(yface_shape(N)); fbz = np.zeros(zface_shape(N))
+    irx = np.zeros(xface_shape(N)); iry = np.zeros(yface_shape(N)); irz = np.zeros(zface_shape(N))
+    c = ctypes.c_double
+    lib().orc_face_coeffs_vof(*N, _p(alpha), c(rho0), c(rho1), _u8(ct), _u8(fxt), _u8(fyt), _u8(fzt), _p(rho),
+                              _p(fbx), _p(fby), _p(fbz), _p(irx), _p(iry), _p(irz))
+    return rho, (fbx, fby, fbz), (irx, iry, irz)
+
+
+def make_rhs(g: "RefGrid"):
+    rhs = np.zeros(cell_shape(g.N))
+    c = ctypes.c_double
+    lib().orc_make_rhs(*g.N, c(1.0 / g.h[0]), c(1.0 / g.h[1]), c(1.0 / g.h[2]), c(1.0 / g.dt),
+                       _p(g.vxs), _p(g.vys), _p(g.vzs), _p(g.eps), _p(g.eps_old),
+                       _p(g.fbx), _p(g.fby), _p(g.fbz), _p(g.fsx), _p(g.fsy), _p(g.fsz), _u8(g.ct), _p(rhs))
+    return rhs
+
+
+def build_A(g: "RefGrid"):
+    """The 8 stencil arrays of k_build_vof_poisson_A, shape (8,)+cell_shape."""
+    A = np.zeros((8,) + cell_shape(g.N))
+    c = ctypes.c_double
+    lib().orc_build_A(*g.N, c(1.0 / g.h[0] ** 2), c(1.0 / g.h[1] ** 2), c(1.0 / g.h[2] ** 2),
+                      _p(g.fbx), _p(g.fby), _p(g.fbz), _u8(g.ct), _u8(g.fxt), _u8(g.fyt), _u8(g.fzt), _p(A))
+    return A
+
+
+def apply_A(N, A, p):
+    out = np.zeros(cell_shape(N))
+    lib().orc_apply_A(*N, _p(np.ascontiguousarray(A)), _p(np.ascontiguousarray(p)), _p(out))
+    return out
+
+
+def solve(g: "RefGrid", solver_type=PURENEUMANN_GMG_PCG, tol=1e-11, levels=4, max_iter=0,
+          stop_rule=STOP_REFERENCE, check_freq=0, p_delta=None):
+    """Run the reference PCG solver restatement; returns (p_delta, rhs, stats dict)."""
+    pd = np.zeros(cell_shape(g.N)) if p_delta is None else np.ascontiguousarray(p_delta).copy()
+    rhs = np.zeros(cell_shape(g.N))
+    prob = g.problem()
+    st = OrcStats()
+    rc = lib().orc_solve(ctypes.byref(prob), ctypes.c_int(solver_type), ctypes.c_double(tol),
+                         ctypes.c_int(levels), ctypes.c_int(max_iter), ctypes.c_int(stop_rule),
+                         ctypes.c_int(check_freq), _p(pd), _p(rhs), ctypes.byref(st))
+    d = st.as_dict()
+    d["rc"] = rc
+    return pd, rhs, d
+
+
+def correct(g: "RefGrid", p_delta, p=None, v=None):
+    """k_correct_vof_velocity: returns (vx, vy, vz, p) after the correction."""
+    N = g.N
+    p = np.zeros(cell_shape(N)) if p is None else p.copy()
+    if v is None:
+        vx, vy, vz = np.zeros(xface_shape(N)), np.zeros(yface_shape(N)), np.zeros(zface_shape(N))
+    else:
+        vx, vy, vz = (a.copy() for a in v)
+    c = ctypes.c_double
+    lib().orc_correct(*N, c(1.0 / g.h[0]), c(1.0 / g.h[1]), c(1.0 / g.h[2]), c(g.dt),
+                      _u8(g.ct), _u8(g.fxt), _u8(g.fyt), _u8(g.fzt), _p(np.ascontiguousarray(p_delta)), _p(p),
+                      _p(g.vxs), _p(g.vys), _p(g.vzs), _p(g.firx), _p(g.firy), _p(g.firz),
+                      _p(g.fsx), _p(g.fsy), _p(g.fsz), _p(vx), _p(vy), _p(vz))
+    return vx, vy, vz, p
+
+
+@dataclass
+class RefGrid:
+    """The grid fields the pressure path reads, in the reference layout."""
+    N: tuple
+    h: tuple
+    dt: float
+    vxs: np.ndarray
+    vys: np.ndarray
+    vzs: np.ndarray
+    eps: np.ndarray
+    eps_old: np.ndarray
+    fbx: np.ndarray
+    fby: np.ndarray
+    fbz: np.ndarray
+    fsx: np.ndarray
+    fsy: np.ndarray
+    fsz: np.ndarray
+    firx: np.ndarray
+    firy: np.ndarray
+    firz: np.ndarray
+    ct: np.ndarray
+    fxt: np.ndarray
+    fyt: np.ndarray
+    fzt: np.ndarray
+
+    def problem(self) -> OrcProblem:
+        pr = OrcProblem()
+        pr.Nx, pr.Ny, pr.Nz = self.N
+        pr.dx, pr.dy, pr.dz = self.h
+        pr.dt = self.dt
+        for name in ("vxs", "vys", "vzs", "eps", "eps_old", "fbx", "fby", "fbz", "fsx", "fsy", "fsz"):
+            setattr(pr, name, _p(getattr(self, name)))
+        for name in ("ct", "fxt", "fyt", "fzt"):
+            setattr(pr, name, _u8(getattr(self, name)))
+        self._keep = pr  # arrays are owned by self
+        return pr

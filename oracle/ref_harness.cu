@@ -1,0 +1,176 @@
+// ref_harness.cu -- a small driver of ours that runs the REFERENCE's own GPU
+// pressure path, compiled unmodified from its sources (oracle/Makefile, target
+// `ref`), on host arrays.  TEST INFRASTRUCTURE ONLY: it pins the CPU oracle
+// (oracle/smac_oracle.cpp) to the reference and produces the golden vectors in
+// tests/golden/.  The product never links it.
+//
+// It follows the reference driver's set-up (CFD/main.cu:183-243): a host
+// SMACSolver with calloc'ed members, G_SMACSolver::solver_malloc + cpuTogpu,
+// G_PCGSolver + G_GMGSolver::initialize, set_solver, tol_, then
+// G_SMACSolver::solve_poisson() and correct_vof_velocity().
+//
+// Two things the reference leaves to chance are pinned here: every multigrid
+// level array is zeroed after G_GMGSolver::initialize (the reference reads
+// never-written ghost entries of q_tmp_ and of the coarse f_b arrays), and
+// shapes for which the reference would abort() or index levels_[-1] are
+// refused before any reference code runs.
+#include <cstdint>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <unistd.h>
+
+#include "G_SMACSolver.h"
+#include "SMACSolver.h"
+#include "pressure_solver/G_GMGSolver.h"
+#include "pressure_solver/G_PCGSolver.h"
+
+namespace {
+
+// G_GMGSolver::initialize's level count and abort conditions
+// (CFD/pressure_solver/G_GMGSolver.cu:10-147), evaluated without running it.
+int count_levels(int Nx, int Ny, int Nz, int levels, int min_size) {
+  bool cx = Nx / 2 >= min_size, cy = Ny / 2 >= min_size, cz = Nz / 2 >= min_size;
+  if ((Nx % 2 == 1 && cx) || (Ny % 2 == 1 && cy) || (Nz % 2 == 1 && cz)) return -1;
+  int sx = cx ? Nx / 2 : Nx, sy = cy ? Ny / 2 : Ny, sz = cz ? Nz / 2 : Nz;
+  int n = 1;
+  for (int i = 1; i < levels; ++i) {
+    cx = sx / 2 >= min_size; cy = sy / 2 >= min_size; cz = sz / 2 >= min_size;
+    if (!cx && !cy && !cz) break;
+    if ((sx % 2 == 1 && cx) || (sy % 2 == 1 && cy) || (sz % 2 == 1 && cz)) return -1;
+    if (cx) sx /= 2;
+    if (cy) sy /= 2;
+    if (cz) sz /= 2;
+    ++n;
+  }
+  return n;
+}
+
+template <class T>
+void put(MyArray<T, 3>& a, const T* src) {
+  if (src) std::memcpy(a.data_, src, sizeof(T) * (size_t)a.size_);
+}
+template <class T>
+void get(const MyArray<T, 3>& a, T* dst) {
+  if (dst) std::memcpy(dst, a.data_, sizeof(T) * (size_t)a.size_);
+}
+
+}  // namespace
+
+extern "C" {
+
+struct ref_inputs {
+  int Nx, Ny, Nz;
+  double Lx, Ly, Lz, dt;
+  int solver_type;   // PCG_TYPES
+  double tol;        // tol_ (max|r|*dt)
+  int levels;        // gmg_levels
+  int do_correct;
+  const double *vxs, *vys, *vzs, *eps, *eps_old, *fbx, *fby, *fbz, *fsx, *fsy, *fsz, *firx, *firy, *firz;
+  const uint8_t *ct, *fxt, *fyt, *fzt;
+};
+
+struct ref_outputs {
+  double *p_delta, *rhs, *vx, *vy, *vz, *p;
+  int iterations;     // parsed from the reference's "PCG iter = %d" line
+  int num_levels;
+};
+
+// Returns 0 on success, -1 refused shape, -2 CUDA error.
+int ref_solve(const ref_inputs* in, ref_outputs* out) {
+  const int Nx = in->Nx, Ny = in->Ny, Nz = in->Nz;
+  const bool gmg = in->solver_type == GMG_PCG || in->solver_type == PURENEUMANN_GMG_PCG;
+  if (gmg) {
+    const int nl = count_levels(Nx, Ny, Nz, in->levels, 6);
+    if (nl < 2) return -1;
+    out->num_levels = nl;
+  }
+  SMACSolver solv;
+  solv.set_calc_properties(0., 0., 0., in->Lx, in->Ly, in->Lz, Nx, Ny, Nz);
+  solv.grid_.bc_.num_boundary_id_ = 1;
+  solv.solver_malloc();
+  StaggeredGrid& hg = solv.grid_;
+  put(hg.f_vx_star_, in->vxs); put(hg.f_vy_star_, in->vys); put(hg.f_vz_star_, in->vzs);
+  put(hg.void_fraction_, in->eps); put(hg.void_fraction_old_, in->eps_old);
+  put(hg.f_bx_, in->fbx); put(hg.f_by_, in->fby); put(hg.f_bz_, in->fbz);
+  put(hg.f_sx_, in->fsx); put(hg.f_sy_, in->fsy); put(hg.f_sz_, in->fsz);
+  put(hg.f_inv_rhox_, in->firx); put(hg.f_inv_rhoy_, in->firy); put(hg.f_inv_rhoz_, in->firz);
+  put(hg.celltype_, in->ct); put(hg.f_xtype_, in->fxt); put(hg.f_ytype_, in->fyt); put(hg.f_ztype_, in->fzt);
+  solv.dt_ = in->dt;
+  solv.inv_dt_ = 1. / in->dt;
+
+  G_SMACSolver g;
+  g.set_calc_properties(0., 0., 0., in->Lx, in->Ly, in->Lz, Nx, Ny, Nz);
+  g.grid_.bc_.num_boundary_id_ = 1;
+  g.solver_malloc();
+  g.cpuTogpu(solv.grid_);
+  g.set_block_grid(Nx, Ny, Nz);
+  g.dt_ = in->dt;
+  g.inv_dt_ = 1. / in->dt;
+
+  G_PCGSolver pcg;
+  pcg.copyData(g);
+  g.pressure_solver_ = &pcg;
+  G_GMGSolver gmgs;
+  if (gmg) {
+    gmgs.initialize(g, in->levels);
+    gmgs.copyData(g);
+    for (int i = 0; i < gmgs.num_levels_; ++i) {
+#define MEMBER(type, name, xs, ys, zs, save) \
+      cudaMemset(gmgs.levels_[i].name.data_, 0, sizeof(type) * (size_t)gmgs.levels_[i].name.size_);
+#include "memberList/levelMembers.def"
+#undef MEMBER
+    }
+    pcg.set_gmg(gmgs);
+  }
+  pcg.set_solver((PCG_TYPES)in->solver_type);
+  pcg.tol_ = in->tol;
+  cudaDeviceSynchronize();
+
+  // capture the reference's stdout to read its iteration count
+  fflush(stdout);
+  char path[] = "/tmp/ref_harness_XXXXXX";
+  const int fd = mkstemp(path);
+  const int saved = dup(1);
+  if (fd >= 0) dup2(fd, 1);
+  g.solve_poisson();
+  cudaDeviceSynchronize();
+  fflush(stdout);
+  if (fd >= 0) {
+    dup2(saved, 1);
+    close(saved);
+    FILE* f = fopen(path, "r");
+    char line[512];
+    out->iterations = -1;
+    while (f && fgets(line, sizeof(line), f)) {
+      int it;
+      if (sscanf(line, "PCG iter = %d", &it) == 1) out->iterations = it;
+    }
+    if (f) fclose(f);
+    close(fd);
+    unlink(path);
+  }
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) {
+    fprintf(stderr, "ref_solve: %s\n", cudaGetErrorString(e));
+    return -2;
+  }
+  g.gpuTocpu(solv.grid_);
+  get(hg.p_delta_, out->p_delta);
+  get(hg.rhs_, out->rhs);
+  if (in->do_correct) {
+    g.correct_vof_velocity(solv);
+    cudaDeviceSynchronize();
+    g.gpuTocpu(solv.grid_);
+    get(hg.f_vx_, out->vx); get(hg.f_vy_, out->vy); get(hg.f_vz_, out->vz);
+    get(hg.p_, out->p);
+  }
+  e = cudaGetLastError();
+  if (gmg) gmgs.free_levels();
+  g.solver_free();
+  solv.solver_free();
+  return e == cudaSuccess ? 0 : -2;
+}
+
+}  // extern "C"

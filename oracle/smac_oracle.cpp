@@ -1,0 +1,950 @@
+// smac_oracle.cpp -- CPU restatement of the reference SMAC pressure projection.
+//
+// TEST INFRASTRUCTURE ONLY.  This file is the parity checker for the CUDA
+// path in mydemcfd_b200/csrc; only tests/, __graft_entry__.smoke() and the
+// cpu_baseline / --impl reference legs of bench.py may load it.  The product
+// never links it and never falls back to it.
+//
+// It restates, operation for operation, the reference's GPU algorithm for the
+// pressure path (the reference has no CPU pressure solve: CFD/main.cu:60-69
+// refuses to run on the CPU and CFD/SMACSolver.cpp declares but never defines
+// solve_poisson).  Arrays use the reference layout: MyArray<T,3> with x
+// fastest, index (z*sy + y)*sx + x (CFD/MyArray.h:43-51); cells are
+// (Nx+2)(Ny+2)(Nz+2), x-faces (Nx+3)(Ny+2)(Nz+2), y-faces (Nx+2)(Ny+3)(Nz+2),
+// z-faces (Nx+2)(Ny+2)(Nz+3) (CFD/memberList/gridMembers.def).
+//
+// Build with -ffp-contract=off: the reference is compiled with -fmad=false
+// (makefile_CFD:5), so every elementwise kernel here rounds exactly like the
+// reference's.  Reductions (the reference calls cub::DeviceReduce::Sum/Max)
+// use a fixed-chunk pairwise order that does not depend on the thread count.
+//
+// Memory the reference reads without ever writing (the ghost entries of the
+// multigrid q_tmp_ buffers and of the coarse-level face coefficients,
+// CFD/pressure_solver/G_GMGSolver.cu:499-644,692-717) is taken to be zero.
+
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstdio>
+#include <cstring>
+#include <vector>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+namespace {
+
+// CFD/Enums.h:3-23
+enum : uint8_t { F_INTERIOR = 0, F_BOUNDARY = 1, F_GHOST = 2, F_NEAR_BOUNDARY = 3 };
+enum : uint8_t { C_INTERIOR = 0, C_NEAR_BOUNDARY = 1, C_GHOST = 2, C_SOLID = 3 };
+// CFD/Enums.h:25-30
+enum : int { STANDARD_PCG = 0, PURENEUMANN_STANDARD_PCG = 1, GMG_PCG = 2, PURENEUMANN_GMG_PCG = 3 };
+
+constexpr double kEPS = 1.e-12;  // CFD/hardCodedParameters.h:7
+
+struct Arr {
+  double* d = nullptr;
+  int sx = 0, sy = 0, sz = 0;
+  inline double& operator()(int x, int y, int z) const {
+    return d[((size_t)z * sy + y) * sx + x];
+  }
+  size_t size() const { return (size_t)sx * sy * sz; }
+};
+
+struct Buf {
+  std::vector<double> v;
+  Arr a;
+  void alloc(int sx, int sy, int sz) {
+    v.assign((size_t)sx * sy * sz, 0.0);
+    a.d = v.data();
+    a.sx = sx; a.sy = sy; a.sz = sz;
+  }
+};
+
+template <class T>
+struct View {
+  T* d = nullptr;
+  int sx = 0, sy = 0, sz = 0;
+  inline T& operator()(int x, int y, int z) const {
+    return d[((size_t)z * sy + y) * sx + x];
+  }
+};
+
+// Deterministic sum: fixed chunks of whole (y,z) rows, each chunk summed
+// sequentially, chunk partials combined pairwise.  Independent of threads.
+template <class F>
+double det_sum_rows(int nrows, F&& rowsum) {
+  const int chunk = 16;
+  const int nchunks = (nrows + chunk - 1) / chunk;
+  std::vector<double> part(nchunks, 0.0);
+#pragma omp parallel for schedule(static)
+  for (int c = 0; c < nchunks; ++c) {
+    double s = 0.0;
+    const int r1 = std::min(nrows, (c + 1) * chunk);
+    for (int r = c * chunk; r < r1; ++r) s += rowsum(r);
+    part[c] = s;
+  }
+  // pairwise combine
+  int n = nchunks;
+  while (n > 1) {
+    const int h = n / 2;
+    for (int i = 0; i < h; ++i) part[i] = part[2 * i] + part[2 * i + 1];
+    if (n & 1) part[h] = part[n - 1];
+    n = h + (n & 1);
+  }
+  return nchunks ? part[0] : 0.0;
+}
+
+template <class F>
+double det_max_rows(int nrows, F&& rowmax) {
+  double m = 0.0;
+#pragma omp parallel for reduction(max : m) schedule(static)
+  for (int r = 0; r < nrows; ++r) m = std::max(m, rowmax(r));
+  return m;
+}
+
+// ---------------------------------------------------------------------------
+// Grid state for one solve (the subset of G_StaggeredGrid the path touches).
+struct Grid {
+  int Nx, Ny, Nz;
+  double inv_dx, inv_dy, inv_dz, inv_dx2, inv_dy2, inv_dz2;
+  View<const uint8_t> ct, fxt, fyt, fzt;
+  Arr fbx, fby, fbz;            // face coefficients (inputs, read only)
+  Buf rhs, r, z, dir, Ap, ptmp, res; // cell work arrays, (N+2)^3
+  Buf Axp, Axm, Ayp, Aym, Azp, Azm, Adiag, invAdiag;
+  Arr pd;                       // p_delta_ (caller owned, in/out)
+};
+
+// ---------------------------------------------------------------------------
+// Multigrid hierarchy: CFD/pressure_solver/G_GMGSolver.{h,cu}, G_Levels.h,
+// CFD/memberList/levelMembers.def.
+struct Level {
+  bool cx = true, cy = true, cz = true;
+  double idx2, idy2, idz2;
+  Buf q, qtmp, fbx, fby, fbz, rhs, res, Axp, Axm, Ayp, Aym, Azp, Azm, invAdiag, Adiag;
+  int sx() const { return q.a.sx; }
+  int sy() const { return q.a.sy; }
+  int sz() const { return q.a.sz; }
+};
+
+struct GMG {
+  int num_levels = 0;
+  int min_size = 6;         // G_GMGSolver.h:22
+  int num_iter_coarse = 30; // G_GMGSolver.h:23
+  int num_iter_fine = 4;    // G_GMGSolver.h:24
+  double omega = 0.6;       // G_GMGSolver.cu:697,724
+  std::vector<Level> lv;
+};
+
+// G_GMGSolver::initialize (G_GMGSolver.cu:10-147).  Returns 0, or -1 where
+// the reference would abort() (odd size in a direction that coarsens).
+int gmg_initialize(GMG& g, const Grid& grid, int num_levels) {
+  if (num_levels > 16 || num_levels < 1) return -1;
+  g.lv.clear();
+  g.lv.reserve(num_levels);
+  g.num_levels = 0;
+  const int Nx = grid.Nx, Ny = grid.Ny, Nz = grid.Nz;
+  {
+    Level L;
+    if (Nx / 2 < g.min_size) L.cx = false;
+    if (Ny / 2 < g.min_size) L.cy = false;
+    if (Nz / 2 < g.min_size) L.cz = false;
+    if ((Nx % 2 == 1 && L.cx) || (Ny % 2 == 1 && L.cy) || (Nz % 2 == 1 && L.cz)) return -1;
+    const int nx = L.cx ? Nx / 2 : Nx, ny = L.cy ? Ny / 2 : Ny, nz = L.cz ? Nz / 2 : Nz;
+    for (Buf* b : {&L.q, &L.qtmp, &L.rhs, &L.res, &L.Axp, &L.Axm, &L.Ayp, &L.Aym, &L.Azp, &L.Azm,
+                   &L.invAdiag, &L.Adiag})
+      b->alloc(nx + 2, ny + 2, nz + 2);
+    L.fbx.alloc(nx + 3, ny + 2, nz + 2);
+    L.fby.alloc(nx + 2, ny + 3, nz + 2);
+    L.fbz.alloc(nx + 2, ny + 2, nz + 3);
+    L.idx2 = L.cx ? grid.inv_dx2 * 0.25 : grid.inv_dx2;
+    L.idy2 = L.cy ? grid.inv_dy2 * 0.25 : grid.inv_dy2;
+    L.idz2 = L.cz ? grid.inv_dz2 * 0.25 : grid.inv_dz2;
+    g.lv.push_back(std::move(L));
+    g.num_levels = 1;
+  }
+  for (int i = 1; i < num_levels; ++i) {
+    const Level& O = g.lv[i - 1];
+    Level L;
+    if ((O.sx() - 2) / 2 < g.min_size) L.cx = false;
+    if ((O.sy() - 2) / 2 < g.min_size) L.cy = false;
+    if ((O.sz() - 2) / 2 < g.min_size) L.cz = false;
+    if (!L.cx && !L.cy && !L.cz) break;
+    if (((O.sx() - 2) % 2 == 1 && L.cx) || ((O.sy() - 2) % 2 == 1 && L.cy) ||
+        ((O.sz() - 2) % 2 == 1 && L.cz))
+      return -1;
+    const int nx = L.cx ? (O.sx() - 2) / 2 : O.sx() - 2;
+    const int ny = L.cy ? (O.sy() - 2) / 2 : O.sy() - 2;
+    const int nz = L.cz ? (O.sz() - 2) / 2 : O.sz() - 2;
+    for (Buf* b : {&L.q, &L.qtmp, &L.rhs, &L.res, &L.Axp, &L.Axm, &L.Ayp, &L.Aym, &L.Azp, &L.Azm,
+                   &L.invAdiag, &L.Adiag})
+      b->alloc(nx + 2, ny + 2, nz + 2);
+    L.fbx.alloc(nx + 3, ny + 2, nz + 2);
+    L.fby.alloc(nx + 2, ny + 3, nz + 2);
+    L.fbz.alloc(nx + 2, ny + 2, nz + 3);
+    L.idx2 = L.cx ? O.idx2 * 0.25 : O.idx2;
+    L.idy2 = L.cy ? O.idy2 * 0.25 : O.idy2;
+    L.idz2 = L.cz ? O.idz2 * 0.25 : O.idz2;
+    g.lv.push_back(std::move(L));
+    g.num_levels += 1;
+  }
+  // With a single level the reference's v_cycle_as_preconditioner launches
+  // k_propagate_level_to_level on levels_[num_levels-2] = levels_[-1]
+  // (G_GMGSolver.cu:977): undefined behaviour, so such shapes are refused.
+  if (g.num_levels < 2) return -2;
+  return 0;
+}
+
+// k_create_level0_coeffs / k_create_level_coeffs (G_GMGSolver.cu:499-644):
+// coarse f_b(ix,iy,iz) = mean over the fine faces (2ix-1..2ix) x (2iy-1..2iy)
+// x (2iz-1..2iz) of a coarsened direction (quirk: includes the mid-cell face).
+void coarsen_face(const Arr& fine, Arr& coarse, bool cx, bool cy, bool cz) {
+  const int rx = cx ? 2 : 1, ry = cy ? 2 : 1, rz = cz ? 2 : 1;
+#pragma omp parallel for collapse(2) schedule(static)
+  for (int iz = 1; iz < coarse.sz - 1; ++iz)
+    for (int iy = 1; iy < coarse.sy - 1; ++iy)
+      for (int ix = 1; ix < coarse.sx - 1; ++ix) {
+        const int IX = cx ? 2 * ix - 1 : ix, IY = cy ? 2 * iy - 1 : iy, IZ = cz ? 2 * iz - 1 : iz;
+        double count = 0., tmp = 0.;
+        for (int kz = 0; kz < rz; ++kz)
+          for (int ky = 0; ky < ry; ++ky)
+            for (int kx = 0; kx < rx; ++kx) {
+              tmp += fine(IX + kx, IY + ky, IZ + kz);
+              count += 1.0;
+            }
+        coarse(ix, iy, iz) = tmp / count;
+      }
+}
+
+// k_create_level_A (G_GMGSolver.cu:646-685)
+void level_build_A(Level& L) {
+  const Arr &fbx = L.fbx.a, &fby = L.fby.a, &fbz = L.fbz.a;
+#pragma omp parallel for collapse(2) schedule(static)
+  for (int iz = 1; iz < L.sz() - 1; ++iz)
+    for (int iy = 1; iy < L.sy() - 1; ++iy)
+      for (int ix = 1; ix < L.sx() - 1; ++ix) {
+        const double axp = fbx(ix + 1, iy, iz) * L.idx2;
+        const double axm = fbx(ix, iy, iz) * L.idx2;
+        const double ayp = fby(ix, iy + 1, iz) * L.idy2;
+        const double aym = fby(ix, iy, iz) * L.idy2;
+        const double azp = fbz(ix, iy, iz + 1) * L.idz2;
+        const double azm = fbz(ix, iy, iz) * L.idz2;
+        L.Axp.a(ix, iy, iz) = axp; L.Axm.a(ix, iy, iz) = axm;
+        L.Ayp.a(ix, iy, iz) = ayp; L.Aym.a(ix, iy, iz) = aym;
+        L.Azp.a(ix, iy, iz) = azp; L.Azm.a(ix, iy, iz) = azm;
+        const double ad = (axp + axm + ayp + aym + azp + azm);
+        L.Adiag.a(ix, iy, iz) = ad;
+        L.invAdiag.a(ix, iy, iz) = (std::fabs(ad) < kEPS) ? 0. : 1. / ad;
+      }
+}
+
+// G_GMGSolver::create_coeffs (G_GMGSolver.cu:913-922)
+void gmg_create_coeffs(GMG& g, const Grid& grid) {
+  Level& L0 = g.lv[0];
+  coarsen_face(grid.fbx, L0.fbx.a, L0.cx, L0.cy, L0.cz);
+  coarsen_face(grid.fby, L0.fby.a, L0.cx, L0.cy, L0.cz);
+  coarsen_face(grid.fbz, L0.fbz.a, L0.cx, L0.cy, L0.cz);
+  level_build_A(L0);
+  for (int l = 1; l < g.num_levels; ++l) {
+    Level& L = g.lv[l];
+    coarsen_face(g.lv[l - 1].fbx.a, L.fbx.a, L.cx, L.cy, L.cz);
+    coarsen_face(g.lv[l - 1].fby.a, L.fby.a, L.cx, L.cy, L.cz);
+    coarsen_face(g.lv[l - 1].fbz.a, L.fbz.a, L.cx, L.cy, L.cz);
+    level_build_A(L);
+  }
+}
+
+// One omega-Jacobi sweep over the interior of an (sx,sy,sz) array
+// (k_jacobi_iteration_general / k_jacobi_level_iteration, G_GMGSolver.cu:692-746).
+void jacobi_sweep(const Arr& Axp, const Arr& Axm, const Arr& Ayp, const Arr& Aym, const Arr& Azp,
+                  const Arr& Azm, const Arr& invAdiag, const Arr& p, const Arr& rhs, Arr& ptmp,
+                  double omega) {
+#pragma omp parallel for collapse(2) schedule(static)
+  for (int iz = 1; iz < p.sz - 1; ++iz)
+    for (int iy = 1; iy < p.sy - 1; ++iy)
+      for (int ix = 1; ix < p.sx - 1; ++ix) {
+        const double tmp_p = Axp(ix, iy, iz) * p(ix + 1, iy, iz) + Axm(ix, iy, iz) * p(ix - 1, iy, iz) +
+                             Ayp(ix, iy, iz) * p(ix, iy + 1, iz) + Aym(ix, iy, iz) * p(ix, iy - 1, iz) +
+                             Azp(ix, iy, iz) * p(ix, iy, iz + 1) + Azm(ix, iy, iz) * p(ix, iy, iz - 1);
+        ptmp(ix, iy, iz) = (1.0 - omega) * p(ix, iy, iz) + omega * (tmp_p + rhs(ix, iy, iz)) * invAdiag(ix, iy, iz);
+      }
+}
+
+// residue = rhs - A q on the interior (k_get_res_general / k_get_res_levels,
+// G_GMGSolver.cu:152-226)
+void residual(const Arr& Axp, const Arr& Axm, const Arr& Ayp, const Arr& Aym, const Arr& Azp,
+              const Arr& Azm, const Arr& Adiag, const Arr& q, const Arr& rhs, Arr& res) {
+#pragma omp parallel for collapse(2) schedule(static)
+  for (int iz = 1; iz < q.sz - 1; ++iz)
+    for (int iy = 1; iy < q.sy - 1; ++iy)
+      for (int ix = 1; ix < q.sx - 1; ++ix) {
+        const double Ap = q(ix, iy, iz) * Adiag(ix, iy, iz) -
+                          (Axp(ix, iy, iz) * q(ix + 1, iy, iz) + Axm(ix, iy, iz) * q(ix - 1, iy, iz) +
+                           Ayp(ix, iy, iz) * q(ix, iy + 1, iz) + Aym(ix, iy, iz) * q(ix, iy - 1, iz) +
+                           Azp(ix, iy, iz) * q(ix, iy, iz + 1) + Azm(ix, iy, iz) * q(ix, iy, iz - 1));
+        res(ix, iy, iz) = rhs(ix, iy, iz) - Ap;
+      }
+}
+
+// coarse_rhs = mean of children (k_restrict_grid_to_level0 /
+// k_restrict_level_to_level, G_GMGSolver.cu:416-493)
+void restrict_avg(const Arr& res, Arr& crhs, bool cx, bool cy, bool cz) {
+  const int rx = cx ? 2 : 1, ry = cy ? 2 : 1, rz = cz ? 2 : 1;
+#pragma omp parallel for collapse(2) schedule(static)
+  for (int iz = 1; iz < crhs.sz - 1; ++iz)
+    for (int iy = 1; iy < crhs.sy - 1; ++iy)
+      for (int ix = 1; ix < crhs.sx - 1; ++ix) {
+        const int IX = cx ? 2 * ix - 1 : ix, IY = cy ? 2 * iy - 1 : iy, IZ = cz ? 2 * iz - 1 : iz;
+        double count = 0., tmp = 0.;
+        for (int kz = 0; kz < rz; ++kz)
+          for (int ky = 0; ky < ry; ++ky)
+            for (int kx = 0; kx < rx; ++kx) {
+              tmp += res(IX + kx, IY + ky, IZ + kz);
+              count += 1.0;
+            }
+        crhs(ix, iy, iz) = tmp / count;
+      }
+}
+
+// fine += coarse on the children (k_propagate_*, G_GMGSolver.cu:285-389)
+void prolong_inject(const Arr& cq, Arr& fq, bool cx, bool cy, bool cz) {
+  const int rx = cx ? 2 : 1, ry = cy ? 2 : 1, rz = cz ? 2 : 1;
+#pragma omp parallel for collapse(2) schedule(static)
+  for (int iz = 1; iz < cq.sz - 1; ++iz)
+    for (int iy = 1; iy < cq.sy - 1; ++iy)
+      for (int ix = 1; ix < cq.sx - 1; ++ix) {
+        const int IX = cx ? 2 * ix - 1 : ix, IY = cy ? 2 * iy - 1 : iy, IZ = cz ? 2 * iz - 1 : iz;
+        const double prop = cq(ix, iy, iz);
+        for (int kz = 0; kz < rz; ++kz)
+          for (int ky = 0; ky < ry; ++ky)
+            for (int kx = 0; kx < rx; ++kx) fq(IX + kx, IY + ky, IZ + kz) += prop;
+      }
+}
+
+void zero(Arr& a) { std::fill(a.d, a.d + a.size(), 0.0); }
+
+// G_GMGSolver::v_cycle_as_preconditioner (G_GMGSolver.cu:925-998).
+// q is overwritten with V(rhs), x0 = 0.  The host-side pointer swaps of the
+// reference are reproduced with local buffer swaps (even sweep counts).
+void gmg_vcycle(GMG& g, Grid& grid, Arr& q, const Arr& rhs) {
+  const int nf = g.num_iter_fine, nc = g.num_iter_coarse, NL = g.num_levels;
+  zero(q);
+  for (int l = 0; l < NL; ++l) zero(g.lv[l].q.a);
+  Arr a = q, b = grid.ptmp.a;  // ptmp ghosts stay 0
+  for (int it = 0; it < nf; ++it) {
+    jacobi_sweep(grid.Axp.a, grid.Axm.a, grid.Ayp.a, grid.Aym.a, grid.Azp.a, grid.Azm.a, grid.invAdiag.a,
+                 a, rhs, b, g.omega);
+    std::swap(a, b);
+  }
+  // after an even number of sweeps the current iterate lives in q again;
+  // grid.res plays the role of grid.residue_
+  residual(grid.Axp.a, grid.Axm.a, grid.Ayp.a, grid.Aym.a, grid.Azp.a, grid.Azm.a, grid.Adiag.a, a, rhs,
+           grid.res.a);
+  restrict_avg(grid.res.a, g.lv[0].rhs.a, g.lv[0].cx, g.lv[0].cy, g.lv[0].cz);
+
+  auto level_sweeps = [&](Level& L, int n) {
+    Arr x = L.q.a, y = L.qtmp.a;
+    for (int it = 0; it < n; ++it) {
+      jacobi_sweep(L.Axp.a, L.Axm.a, L.Ayp.a, L.Aym.a, L.Azp.a, L.Azm.a, L.invAdiag.a, x, L.rhs.a, y, g.omega);
+      std::swap(x, y);
+    }
+    if (n % 2) {  // keep the iterate in L.q (reference sweep counts are even)
+      std::swap(L.q.v, L.qtmp.v);
+      L.q.a.d = L.q.v.data();
+      L.qtmp.a.d = L.qtmp.v.data();
+    }
+  };
+
+  for (int l = 0; l < NL - 1; ++l) {
+    Level& L = g.lv[l];
+    level_sweeps(L, nf);
+    residual(L.Axp.a, L.Axm.a, L.Ayp.a, L.Aym.a, L.Azp.a, L.Azm.a, L.Adiag.a, L.q.a, L.rhs.a, L.res.a);
+    Level& C = g.lv[l + 1];
+    restrict_avg(L.res.a, C.rhs.a, C.cx, C.cy, C.cz);
+  }
+  level_sweeps(g.lv[NL - 1], nc);
+  if (NL >= 2) {
+    Level& C = g.lv[NL - 1];
+    prolong_inject(C.q.a, g.lv[NL - 2].q.a, C.cx, C.cy, C.cz);
+  }
+  for (int l = NL - 2; l >= 0; --l) {
+    Level& L = g.lv[l];
+    level_sweeps(L, nf);
+    if (l != 0) {
+      prolong_inject(L.q.a, g.lv[l - 1].q.a, L.cx, L.cy, L.cz);
+    } else {
+      prolong_inject(L.q.a, a, L.cx, L.cy, L.cz);
+    }
+  }
+  for (int it = 0; it < nf; ++it) {
+    jacobi_sweep(grid.Axp.a, grid.Axm.a, grid.Ayp.a, grid.Aym.a, grid.Azp.a, grid.Azm.a, grid.invAdiag.a,
+                 a, rhs, b, g.omega);
+    std::swap(a, b);
+  }
+  if (a.d != q.d) std::memcpy(q.d, a.d, q.size() * sizeof(double));
+}
+
+// ---------------------------------------------------------------------------
+// Interior reductions over a cell array: the reference copies the N^3
+// interior to pcg_tmp_ and calls cub::DeviceReduce::Sum / Max.
+double interior_sum(const Grid& g, const Arr& a) {
+  const int Ny = g.Ny, Nz = g.Nz, Nx = g.Nx;
+  return det_sum_rows(Ny * Nz, [&](int r) {
+    const int iy = r % Ny + 1, iz = r / Ny + 1;
+    double s = 0.0;
+    for (int ix = 1; ix <= Nx; ++ix) s += a(ix, iy, iz);
+    return s;
+  });
+}
+double interior_dot(const Grid& g, const Arr& a, const Arr& b) {
+  const int Ny = g.Ny, Nz = g.Nz, Nx = g.Nx;
+  return det_sum_rows(Ny * Nz, [&](int r) {
+    const int iy = r % Ny + 1, iz = r / Ny + 1;
+    double s = 0.0;
+    for (int ix = 1; ix <= Nx; ++ix) s += a(ix, iy, iz) * b(ix, iy, iz);
+    return s;
+  });
+}
+double interior_maxabs(const Grid& g, const Arr& a) {
+  const int Ny = g.Ny, Nz = g.Nz, Nx = g.Nx;
+  return det_max_rows(Ny * Nz, [&](int r) {
+    const int iy = r % Ny + 1, iz = r / Ny + 1;
+    double m = 0.0;
+    for (int ix = 1; ix <= Nx; ++ix) m = std::max(m, std::fabs(a(ix, iy, iz)));
+    return m;
+  });
+}
+
+// G_PressureSolverBase::subtract_cell_mean (G_PressureSolverBase.cu:142-155):
+// mean over the N^3 interior, subtracted from every (N+2)^3 entry.
+void subtract_cell_mean(const Grid& g, Arr& p) {
+  const double sum = interior_sum(g, p);
+  const double size_inv = 1. / (double)((size_t)g.Nx * g.Ny * g.Nz);
+  const double a = -1. * size_inv;
+  const size_t n = p.size();
+#pragma omp parallel for schedule(static)
+  for (size_t i = 0; i < n; ++i) p.d[i] += a * sum;
+}
+
+// k_build_vof_poisson_A (G_PCGSolver.cu:126-212)
+void build_A(Grid& g) {
+#pragma omp parallel for collapse(2) schedule(static)
+  for (int iz = 1; iz <= g.Nz; ++iz)
+    for (int iy = 1; iy <= g.Ny; ++iy)
+      for (int ix = 1; ix <= g.Nx; ++ix) {
+        if (g.ct(ix, iy, iz) != C_INTERIOR) {
+          g.Axp.a(ix, iy, iz) = 0.; g.Axm.a(ix, iy, iz) = 0.;
+          g.Ayp.a(ix, iy, iz) = 0.; g.Aym.a(ix, iy, iz) = 0.;
+          g.Azp.a(ix, iy, iz) = 0.; g.Azm.a(ix, iy, iz) = 0.;
+          g.Adiag.a(ix, iy, iz) = 0.; g.invAdiag.a(ix, iy, iz) = 0.;
+          continue;
+        }
+        double axp = g.fbx(ix + 1, iy, iz) * g.inv_dx2;
+        double axm = g.fbx(ix, iy, iz) * g.inv_dx2;
+        double ayp = g.fby(ix, iy + 1, iz) * g.inv_dy2;
+        double aym = g.fby(ix, iy, iz) * g.inv_dy2;
+        double azp = g.fbz(ix, iy, iz + 1) * g.inv_dz2;
+        double azm = g.fbz(ix, iy, iz) * g.inv_dz2;
+        const double ad = (axp + axm + ayp + aym + azp + azm);
+        g.Adiag.a(ix, iy, iz) = ad;
+        g.invAdiag.a(ix, iy, iz) = 1. / ad;
+        if (g.fxt(ix + 1, iy, iz) == F_BOUNDARY) axp = 0.;
+        if (g.fxt(ix, iy, iz) == F_BOUNDARY) axm = 0.;
+        if (g.fyt(ix, iy + 1, iz) == F_BOUNDARY) ayp = 0.;
+        if (g.fyt(ix, iy, iz) == F_BOUNDARY) aym = 0.;
+        if (g.fzt(ix, iy, iz + 1) == F_BOUNDARY) azp = 0.;
+        if (g.fzt(ix, iy, iz) == F_BOUNDARY) azm = 0.;
+        g.Axp.a(ix, iy, iz) = axp; g.Axm.a(ix, iy, iz) = axm;
+        g.Ayp.a(ix, iy, iz) = ayp; g.Aym.a(ix, iy, iz) = aym;
+        g.Azp.a(ix, iy, iz) = azp; g.Azm.a(ix, iy, iz) = azm;
+      }
+}
+
+// Ap = A p on the interior (k_build_vof_poisson_Ap, G_PCGSolver.cu:214-245;
+// the same expression as k_make_pAp :87-124).
+void apply_A(const Grid& g, const Arr& p, Arr& out) {
+#pragma omp parallel for collapse(2) schedule(static)
+  for (int iz = 1; iz <= g.Nz; ++iz)
+    for (int iy = 1; iy <= g.Ny; ++iy)
+      for (int ix = 1; ix <= g.Nx; ++ix) {
+        out(ix, iy, iz) =
+            g.Adiag.a(ix, iy, iz) * p(ix, iy, iz) -
+            (g.Axp.a(ix, iy, iz) * p(ix + 1, iy, iz) + g.Axm.a(ix, iy, iz) * p(ix - 1, iy, iz) +
+             g.Ayp.a(ix, iy, iz) * p(ix, iy + 1, iz) + g.Aym.a(ix, iy, iz) * p(ix, iy - 1, iz) +
+             g.Azp.a(ix, iy, iz) * p(ix, iy, iz + 1) + g.Azm.a(ix, iy, iz) * p(ix, iy, iz - 1));
+      }
+}
+
+}  // namespace
+
+// ===========================================================================
+// C ABI (ctypes).  All arrays are in the reference layout described above.
+extern "C" {
+
+struct orc_stats {
+  int iterations;        // PCG iterations, counted like the reference's print (G_PCGSolver.cu:921)
+  int converged;         // 1 if the stopping test passed before max_iter
+  double norm_b;         // sqrt(sum b^2) of the de-meaned rhs (guarded like :814-817)
+  double res_max;        // max |r| (recursive residual) at exit
+  double res_rel;        // ||r||_2 / norm_b (recursive) at exit
+  double true_res_rel;   // ||b - A p||_2 / norm_b at exit (b de-meaned for pure Neumann)
+  int num_levels;        // multigrid levels built (0 for Jacobi PCG)
+  int status;            // 0 ok, -1 odd size (reference abort()), -2 single level (reference UB)
+};
+
+int orc_num_threads(void) {
+#ifdef _OPENMP
+  return omp_get_max_threads();
+#else
+  return 1;
+#endif
+}
+
+void orc_set_num_threads(int n) {
+#ifdef _OPENMP
+  if (n > 0) omp_set_num_threads(n);
+#else
+  (void)n;
+#endif
+}
+
+// SMACSolver::set_face_type (CFD/SMACSolver.cpp:104-202): all-wall box.
+void orc_set_face_type(int Nx, int Ny, int Nz, uint8_t* fxt, uint8_t* fyt, uint8_t* fzt) {
+  View<uint8_t> X{fxt, Nx + 3, Ny + 2, Nz + 2}, Y{fyt, Nx + 2, Ny + 3, Nz + 2}, Z{fzt, Nx + 2, Ny + 2, Nz + 3};
+  std::memset(fxt, F_GHOST, (size_t)(Nx + 3) * (Ny + 2) * (Nz + 2));
+  std::memset(fyt, F_GHOST, (size_t)(Nx + 2) * (Ny + 3) * (Nz + 2));
+  std::memset(fzt, F_GHOST, (size_t)(Nx + 2) * (Ny + 2) * (Nz + 3));
+  for (int iz = 1; iz <= Nz; ++iz)
+    for (int iy = 1; iy <= Ny; ++iy)
+      for (int ix = 1; ix <= Nx + 1; ++ix) X(ix, iy, iz) = F_INTERIOR;
+  for (int iz = 1; iz <= Nz; ++iz)
+    for (int iy = 1; iy <= Ny; ++iy) { X(1, iy, iz) = F_BOUNDARY; X(Nx + 1, iy, iz) = F_BOUNDARY; }
+  for (int iz = 1; iz <= Nz; ++iz)
+    for (int iy = 1; iy <= Ny + 1; ++iy)
+      for (int ix = 1; ix <= Nx; ++ix) Y(ix, iy, iz) = F_INTERIOR;
+  for (int iz = 1; iz <= Nz; ++iz)
+    for (int ix = 1; ix <= Nx; ++ix) { Y(ix, 1, iz) = F_BOUNDARY; Y(ix, Ny + 1, iz) = F_BOUNDARY; }
+  for (int iz = 1; iz <= Nz + 1; ++iz)
+    for (int iy = 1; iy <= Ny; ++iy)
+      for (int ix = 1; ix <= Nx; ++ix) Z(ix, iy, iz) = F_INTERIOR;
+  for (int iy = 1; iy <= Ny; ++iy)
+    for (int ix = 1; ix <= Nx; ++ix) { Z(ix, iy, 1) = F_BOUNDARY; Z(ix, iy, Nz + 1) = F_BOUNDARY; }
+}
+
+// SMACSolver::set_cell_type (CFD/SMACSolver.cpp:206-248): ghosts C_GHOST,
+// every real cell C_INTERIOR (the near-boundary tag is disabled at :240-241).
+void orc_set_cell_type(int Nx, int Ny, int Nz, uint8_t* ct) {
+  View<uint8_t> C{ct, Nx + 2, Ny + 2, Nz + 2};
+  std::memset(ct, C_GHOST, (size_t)(Nx + 2) * (Ny + 2) * (Nz + 2));
+  for (int iz = 1; iz <= Nz; ++iz)
+    for (int iy = 1; iy <= Ny; ++iy)
+      for (int ix = 1; ix <= Nx; ++ix) C(ix, iy, iz) = C_INTERIOR;
+}
+
+// Solid fraction by 8^3 sub-sampling (k_get_solid_fraction,
+// CFD/G_SMACSolver_IBM.cu:94-147, constants :13-17) with a sphere predicate in
+// place of the reference's z-aligned cylinder (:28-37).  spheres: n x 4
+// (xc, yc, zc, r).  Cells ix,iy,iz in 1..N+1 like the reference kernel.
+// Cells entirely inside or outside every sphere (by a margin far above the
+// rounding of the sample coordinates) are classified without sampling; all
+// others are sampled exactly as the reference does.
+void orc_solid_fraction_spheres(int Nx, int Ny, int Nz, double dx, double dy, double dz, double ox,
+                                double oy, double oz, const double* sph, int nsph, double* sf) {
+  Arr S{sf, Nx + 2, Ny + 2, Nz + 2};
+  const int N8 = 8;
+  const double fact = 1. / (double)N8;
+  const double inv_total = 1. / (double)(N8 * N8 * N8);
+#pragma omp parallel for collapse(2) schedule(dynamic, 4)
+  for (int iz = 1; iz < Nz + 2; ++iz)
+    for (int iy = 1; iy < Ny + 2; ++iy)
+      for (int ix = 1; ix < Nx + 2; ++ix) {
+        const double xc = dx * (double)(ix)-0.5 * dx + ox;  // StaggeredGrid::get_cell_coord :136-138
+        const double yc = dy * (double)(iy)-0.5 * dy + oy;
+        const double zc = dz * (double)(iz)-0.5 * dz + oz;
+        const double xini = xc - dx * 0.5, yini = yc - dy * 0.5, zini = zc - dz * 0.5;
+        const double sdx = dx * fact, sdy = dy * fact, sdz = dz * fact;
+        int numpts = 0;
+        for (int s = 0; s < nsph; ++s) {
+          const double cx = sph[4 * s], cy = sph[4 * s + 1], cz = sph[4 * s + 2], r = sph[4 * s + 3];
+          const double rsq = r * r;
+          // nearest / farthest distance from the sphere centre to the cell box
+          const double lx = xini, hx = xini + dx, ly = yini, hy = yini + dy, lz = zini, hz = zini + dz;
+          const double nx_ = std::max(0.0, std::max(lx - cx, cx - hx));
+          const double ny_ = std::max(0.0, std::max(ly - cy, cy - hy));
+          const double nz_ = std::max(0.0, std::max(lz - cz, cz - hz));
+          const double fx = std::max(std::fabs(lx - cx), std::fabs(hx - cx));
+          const double fy = std::max(std::fabs(ly - cy), std::fabs(hy - cy));
+          const double fz = std::max(std::fabs(lz - cz), std::fabs(hz - cz));
+          const double near2 = nx_ * nx_ + ny_ * ny_ + nz_ * nz_;
+          const double far2 = fx * fx + fy * fy + fz * fz;
+          const double margin = 1e-6 * (dx * dx + dy * dy + dz * dz);
+          if (near2 > rsq + margin) continue;
+          if (far2 < rsq - margin) { numpts += N8 * N8 * N8; continue; }
+          for (int kz = 0; kz < N8; ++kz)
+            for (int ky = 0; ky < N8; ++ky)
+              for (int kx = 0; kx < N8; ++kx) {
+                const double x_pt = xini + sdx * (kx + 0.5);
+                const double y_pt = yini + sdy * (ky + 0.5);
+                const double z_pt = zini + sdz * (kz + 0.5);
+                const double ddx = x_pt - cx, ddy = y_pt - cy, ddz = z_pt - cz;
+                if (ddx * ddx + ddy * ddy + ddz * ddz <= rsq) numpts += 1;
+              }
+        }
+        double solidfraction = (double)numpts * inv_total;
+        if (solidfraction > 1. - 1.e-2) solidfraction = 1.0;  // clip, :137-139
+        S(ix, iy, iz) = solidfraction;
+      }
+}
+
+// k_set_solid_cell_from_ibm (CFD/G_SMACSolver_IBM.cu:763-792).
+void orc_set_solid_cells(int Nx, int Ny, int Nz, const double* sf, uint8_t* ct, uint8_t* fxt, uint8_t* fyt,
+                         uint8_t* fzt) {
+  View<const double> S{sf, Nx + 2, Ny + 2, Nz + 2};
+  View<uint8_t> C{ct, Nx + 2, Ny + 2, Nz + 2};
+  View<uint8_t> X{fxt, Nx + 3, Ny + 2, Nz + 2}, Y{fyt, Nx + 2, Ny + 3, Nz + 2}, Z{fzt, Nx + 2, Ny + 2, Nz + 3};
+  for (int iz = 1; iz < Nz + 2; ++iz)
+    for (int iy = 1; iy < Ny + 2; ++iy)
+      for (int ix = 1; ix < Nx + 2; ++ix)
+        if (S(ix, iy, iz) > 1. - kEPS) {
+          C(ix, iy, iz) = C_SOLID;
+          X(ix, iy, iz) = F_BOUNDARY; X(ix + 1, iy, iz) = F_BOUNDARY;
+          Y(ix, iy, iz) = F_BOUNDARY; Y(ix, iy + 1, iz) = F_BOUNDARY;
+          Z(ix, iy, iz) = F_BOUNDARY; Z(ix, iy, iz + 1) = F_BOUNDARY;
+        }
+}
+
+// Face coefficients from the volume fraction:
+// k_update_cell_properties_by_alpha (CFD/G_SMACSolver_VoF.cu:1374-1407) then
+// k_update_{x,y,z}_face_properties_by_alpha (:1409-1535):
+// rho = (1-a) rho0 + a rho1 on C_INTERIOR/C_NEAR_BOUNDARY cells;
+// f_b = f_inv_rho = 1/(0.5(rho_L+rho_R)) on F_INTERIOR faces, 0 elsewhere.
+// rho must hold valid values on non-fluid cells on entry (only F_INTERIOR
+// faces read it, and those touch fluid cells only).
+void orc_face_coeffs_vof(int Nx, int Ny, int Nz, const double* alpha, double rho0, double rho1,
+                         const uint8_t* ct, const uint8_t* fxt, const uint8_t* fyt, const uint8_t* fzt,
+                         double* rho, double* fbx, double* fby, double* fbz, double* firx, double* firy,
+                         double* firz) {
+  View<const double> A{alpha, Nx + 2, Ny + 2, Nz + 2};
+  View<const uint8_t> C{ct, Nx + 2, Ny + 2, Nz + 2};
+  View<const uint8_t> X{fxt, Nx + 3, Ny + 2, Nz + 2}, Y{fyt, Nx + 2, Ny + 3, Nz + 2}, Z{fzt, Nx + 2, Ny + 2, Nz + 3};
+  Arr R{rho, Nx + 2, Ny + 2, Nz + 2};
+  Arr BX{fbx, Nx + 3, Ny + 2, Nz + 2}, BY{fby, Nx + 2, Ny + 3, Nz + 2}, BZ{fbz, Nx + 2, Ny + 2, Nz + 3};
+  Arr IX{firx, Nx + 3, Ny + 2, Nz + 2}, IY{firy, Nx + 2, Ny + 3, Nz + 2}, IZ{firz, Nx + 2, Ny + 2, Nz + 3};
+#pragma omp parallel for collapse(2) schedule(static)
+  for (int iz = 1; iz < Nz + 2; ++iz)
+    for (int iy = 1; iy < Ny + 2; ++iy)
+      for (int ix = 1; ix < Nx + 2; ++ix) {
+        const uint8_t c = C(ix, iy, iz);
+        if (c == C_INTERIOR || c == C_NEAR_BOUNDARY) {
+          const double a = A(ix, iy, iz);
+          R(ix, iy, iz) = (1. - a) * rho0 + a * rho1;
+        }
+      }
+#pragma omp parallel for collapse(2) schedule(static)
+  for (int iz = 1; iz < Nz + 2; ++iz)
+    for (int iy = 1; iy < Ny + 2; ++iy) {
+      for (int ix = 1; ix < Nx + 3; ++ix) {
+        if (X(ix, iy, iz) != F_INTERIOR) { BX(ix, iy, iz) = 0.; IX(ix, iy, iz) = 0.; continue; }
+        const double fr = 0.5 * (R(ix, iy, iz) + R(ix - 1, iy, iz));
+        BX(ix, iy, iz) = 1. / fr; IX(ix, iy, iz) = BX(ix, iy, iz);
+      }
+    }
+#pragma omp parallel for collapse(2) schedule(static)
+  for (int iz = 1; iz < Nz + 2; ++iz)
+    for (int iy = 1; iy < Ny + 3; ++iy) {
+      for (int ix = 1; ix < Nx + 2; ++ix) {
+        if (Y(ix, iy, iz) != F_INTERIOR) { BY(ix, iy, iz) = 0.; IY(ix, iy, iz) = 0.; continue; }
+        const double fr = 0.5 * (R(ix, iy, iz) + R(ix, iy - 1, iz));
+        BY(ix, iy, iz) = 1. / fr; IY(ix, iy, iz) = BY(ix, iy, iz);
+      }
+    }
+#pragma omp parallel for collapse(2) schedule(static)
+  for (int iz = 1; iz < Nz + 3; ++iz)
+    for (int iy = 1; iy < Ny + 2; ++iy) {
+      for (int ix = 1; ix < Nx + 2; ++ix) {
+        if (Z(ix, iy, iz) != F_INTERIOR) { BZ(ix, iy, iz) = 0.; IZ(ix, iy, iz) = 0.; continue; }
+        const double fr = 0.5 * (R(ix, iy, iz) + R(ix, iy, iz - 1));
+        BZ(ix, iy, iz) = 1. / fr; IZ(ix, iy, iz) = BZ(ix, iy, iz);
+      }
+    }
+}
+
+// base_k_make_poisson_rhs (CFD/pressure_solver/G_PressureSolverBase.cu:49-118)
+void orc_make_rhs(int Nx, int Ny, int Nz, double inv_dx, double inv_dy, double inv_dz, double inv_dt,
+                  const double* vxs, const double* vys, const double* vzs, const double* eps,
+                  const double* eps_old, const double* fbx, const double* fby, const double* fbz,
+                  const double* fsx, const double* fsy, const double* fsz, const uint8_t* ct, double* rhs) {
+  View<const double> VX{vxs, Nx + 3, Ny + 2, Nz + 2}, VY{vys, Nx + 2, Ny + 3, Nz + 2}, VZ{vzs, Nx + 2, Ny + 2, Nz + 3};
+  View<const double> E{eps, Nx + 2, Ny + 2, Nz + 2}, EO{eps_old, Nx + 2, Ny + 2, Nz + 2};
+  View<const double> BX{fbx, Nx + 3, Ny + 2, Nz + 2}, BY{fby, Nx + 2, Ny + 3, Nz + 2}, BZ{fbz, Nx + 2, Ny + 2, Nz + 3};
+  View<const double> SX{fsx, Nx + 3, Ny + 2, Nz + 2}, SY{fsy, Nx + 2, Ny + 3, Nz + 2}, SZ{fsz, Nx + 2, Ny + 2, Nz + 3};
+  View<const uint8_t> C{ct, Nx + 2, Ny + 2, Nz + 2};
+  Arr R{rhs, Nx + 2, Ny + 2, Nz + 2};
+#pragma omp parallel for collapse(2) schedule(static)
+  for (int iz = 1; iz <= Nz; ++iz)
+    for (int iy = 1; iy <= Ny; ++iy)
+      for (int ix = 1; ix <= Nx; ++ix) {
+        if (C(ix, iy, iz) != C_INTERIOR) { R(ix, iy, iz) = 0.0; continue; }
+        const double exp_ = 0.5 * (E(ix, iy, iz) + E(ix + 1, iy, iz));
+        const double exm = 0.5 * (E(ix - 1, iy, iz) + E(ix, iy, iz));
+        const double eyp = 0.5 * (E(ix, iy, iz) + E(ix, iy + 1, iz));
+        const double eym = 0.5 * (E(ix, iy - 1, iz) + E(ix, iy, iz));
+        const double ezp = 0.5 * (E(ix, iy, iz) + E(ix, iy, iz + 1));
+        const double ezm = 0.5 * (E(ix, iy, iz - 1) + E(ix, iy, iz));
+        const double div_eps = (exp_ * VX(ix + 1, iy, iz) - exm * VX(ix, iy, iz)) * inv_dx +
+                               (eyp * VY(ix, iy + 1, iz) - eym * VY(ix, iy, iz)) * inv_dy +
+                               (ezp * VZ(ix, iy, iz + 1) - ezm * VZ(ix, iy, iz)) * inv_dz;
+        const double deps = E(ix, iy, iz) - EO(ix, iy, iz);
+        const double f_st = (BX(ix + 1, iy, iz) * SX(ix + 1, iy, iz) - BX(ix, iy, iz) * SX(ix, iy, iz)) * inv_dx +
+                            (BY(ix, iy + 1, iz) * SY(ix, iy + 1, iz) - BY(ix, iy, iz) * SY(ix, iy, iz)) * inv_dy +
+                            (BZ(ix, iy, iz + 1) * SZ(ix, iy, iz + 1) - BZ(ix, iy, iz) * SZ(ix, iy, iz)) * inv_dz;
+        R(ix, iy, iz) = -inv_dt * div_eps - deps * inv_dt * inv_dt - f_st;
+      }
+}
+
+// k_build_vof_poisson_A exported for kernel-level parity: writes the 8
+// stencil arrays (Axp,Axm,Ayp,Aym,Azp,Azm,Adiag,invAdiag), each (N+2)^3,
+// interior only (entries outside the interior are left untouched).
+void orc_build_A(int Nx, int Ny, int Nz, double inv_dx2, double inv_dy2, double inv_dz2, const double* fbx,
+                 const double* fby, const double* fbz, const uint8_t* ct, const uint8_t* fxt, const uint8_t* fyt,
+                 const uint8_t* fzt, double* A8) {
+  Grid g;
+  g.Nx = Nx; g.Ny = Ny; g.Nz = Nz;
+  g.inv_dx2 = inv_dx2; g.inv_dy2 = inv_dy2; g.inv_dz2 = inv_dz2;
+  g.ct = {ct, Nx + 2, Ny + 2, Nz + 2};
+  g.fxt = {fxt, Nx + 3, Ny + 2, Nz + 2}; g.fyt = {fyt, Nx + 2, Ny + 3, Nz + 2}; g.fzt = {fzt, Nx + 2, Ny + 2, Nz + 3};
+  g.fbx = {const_cast<double*>(fbx), Nx + 3, Ny + 2, Nz + 2};
+  g.fby = {const_cast<double*>(fby), Nx + 2, Ny + 3, Nz + 2};
+  g.fbz = {const_cast<double*>(fbz), Nx + 2, Ny + 2, Nz + 3};
+  const size_t nc = (size_t)(Nx + 2) * (Ny + 2) * (Nz + 2);
+  Buf* bufs[8] = {&g.Axp, &g.Axm, &g.Ayp, &g.Aym, &g.Azp, &g.Azm, &g.Adiag, &g.invAdiag};
+  for (int k = 0; k < 8; ++k) {
+    bufs[k]->a = {A8 + k * nc, Nx + 2, Ny + 2, Nz + 2};
+  }
+  build_A(g);
+}
+
+// (A p) on the interior from the 7 stencil arrays written by orc_build_A.
+void orc_apply_A(int Nx, int Ny, int Nz, const double* A8, const double* p, double* out) {
+  Grid g;
+  g.Nx = Nx; g.Ny = Ny; g.Nz = Nz;
+  const size_t nc = (size_t)(Nx + 2) * (Ny + 2) * (Nz + 2);
+  Buf* bufs[8] = {&g.Axp, &g.Axm, &g.Ayp, &g.Aym, &g.Azp, &g.Azm, &g.Adiag, &g.invAdiag};
+  for (int k = 0; k < 8; ++k) bufs[k]->a = {const_cast<double*>(A8) + k * nc, Nx + 2, Ny + 2, Nz + 2};
+  Arr P{const_cast<double*>(p), Nx + 2, Ny + 2, Nz + 2}, O{out, Nx + 2, Ny + 2, Nz + 2};
+  apply_A(g, P, O);
+}
+
+// The PCG solvers of CFD/pressure_solver/G_PCGSolver.cu, selected like
+// G_PCGSolver::set_solver (:592-613):
+//   PURENEUMANN_GMG_PCG  solve_pureneumann_gmgpcg  :772-922
+//   GMG_PCG              solve_gmgpcg              :619-770
+//   PURENEUMANN_STANDARD_PCG solve_pureneumann_pcg :307-445
+//   STANDARD_PCG         solve_pcg                 :448-586
+// The solve builds its own RHS (base_k_make_poisson_rhs) and operator from the
+// grid fields, exactly like the reference, and updates p_delta in place.
+//
+// stop_rule 0: the reference's test, max|r|*dt < tol every check_freq
+//              iterations (:884-903); check_freq <= 0 selects the reference's
+//              frequency (5 for GMG, 10 for Jacobi PCG).
+// stop_rule 1: ||r||_2 / norm_b < tol on the recursive residual, same
+//              checking frequency (a relative-residual form of the same loop).
+// stop_rule 2: true residual ||b - A p||_2 / norm_b < tol, every iteration.
+// max_iter <= 0 selects the reference's 2000.
+struct orc_problem {
+  int Nx, Ny, Nz;
+  double dx, dy, dz, dt;
+  const double *vxs, *vys, *vzs;         // u* faces
+  const double *eps, *eps_old;           // void fraction (new, old) cells
+  const double *fbx, *fby, *fbz;         // face coefficients
+  const double *fsx, *fsy, *fsz;         // surface-tension face force
+  const uint8_t *ct, *fxt, *fyt, *fzt;   // cell and face types
+};
+
+int orc_solve(const orc_problem* P, int solver_type, double tol, int levels, int max_iter, int stop_rule,
+              int check_freq, double* p_delta, double* rhs_out, orc_stats* st) {
+  const int Nx = P->Nx, Ny = P->Ny, Nz = P->Nz;
+  Grid g;
+  g.Nx = Nx; g.Ny = Ny; g.Nz = Nz;
+  g.inv_dx = 1. / P->dx; g.inv_dy = 1. / P->dy; g.inv_dz = 1. / P->dz;
+  g.inv_dx2 = 1. / (P->dx * P->dx); g.inv_dy2 = 1. / (P->dy * P->dy); g.inv_dz2 = 1. / (P->dz * P->dz);
+  g.ct = {P->ct, Nx + 2, Ny + 2, Nz + 2};
+  g.fxt = {P->fxt, Nx + 3, Ny + 2, Nz + 2}; g.fyt = {P->fyt, Nx + 2, Ny + 3, Nz + 2}; g.fzt = {P->fzt, Nx + 2, Ny + 2, Nz + 3};
+  g.fbx = {const_cast<double*>(P->fbx), Nx + 3, Ny + 2, Nz + 2};
+  g.fby = {const_cast<double*>(P->fby), Nx + 2, Ny + 3, Nz + 2};
+  g.fbz = {const_cast<double*>(P->fbz), Nx + 2, Ny + 2, Nz + 3};
+  for (Buf* b : {&g.rhs, &g.r, &g.z, &g.dir, &g.Ap, &g.ptmp, &g.res, &g.Axp, &g.Axm, &g.Ayp, &g.Aym, &g.Azp, &g.Azm,
+                 &g.Adiag, &g.invAdiag})
+    b->alloc(Nx + 2, Ny + 2, Nz + 2);
+  g.pd = {p_delta, Nx + 2, Ny + 2, Nz + 2};
+
+  const bool use_gmg = (solver_type == GMG_PCG || solver_type == PURENEUMANN_GMG_PCG);
+  const bool pure = (solver_type == PURENEUMANN_GMG_PCG || solver_type == PURENEUMANN_STANDARD_PCG);
+  if (check_freq <= 0) check_freq = use_gmg ? 5 : 10;
+  if (max_iter <= 0) max_iter = 2000;
+  const double dt = P->dt;
+
+  std::memset(st, 0, sizeof(*st));
+  GMG gmg;
+  if (use_gmg) {
+    const int rc = gmg_initialize(gmg, g, levels);
+    if (rc != 0) { st->status = rc; return rc; }
+    st->num_levels = gmg.num_levels;
+  }
+
+  orc_make_rhs(Nx, Ny, Nz, g.inv_dx, g.inv_dy, g.inv_dz, 1. / dt, P->vxs, P->vys, P->vzs, P->eps, P->eps_old,
+               P->fbx, P->fby, P->fbz, P->fsx, P->fsy, P->fsz, P->ct, g.rhs.a.d);
+  if (rhs_out) std::memcpy(rhs_out, g.rhs.a.d, g.rhs.a.size() * sizeof(double));
+  build_A(g);
+  apply_A(g, g.pd, g.Ap.a);
+
+  // mean of b over the interior (:800-804), then r = (b - mean) - Ap and the
+  // norm of b (:807-817).  The non-Neumann variants skip the mean (:655).
+  const double mean_b = interior_sum(g, g.rhs.a) / (double)((size_t)Nx * Ny * Nz);
+  Buf bhat;  // b as the loop sees it (de-meaned for pure Neumann)
+  bhat.alloc(Nx + 2, Ny + 2, Nz + 2);
+#pragma omp parallel for collapse(2) schedule(static)
+  for (int iz = 1; iz <= Nz; ++iz)
+    for (int iy = 1; iy <= Ny; ++iy)
+      for (int ix = 1; ix <= Nx; ++ix) {
+        const double b = pure ? g.rhs.a(ix, iy, iz) - mean_b : g.rhs.a(ix, iy, iz);
+        bhat.a(ix, iy, iz) = b;
+        g.r.a(ix, iy, iz) = b - g.Ap.a(ix, iy, iz);
+      }
+  double norm_b = interior_dot(g, bhat.a, bhat.a);
+  if (norm_b < 1.0e-16) norm_b = 1.0;
+  norm_b = std::sqrt(norm_b);
+  st->norm_b = norm_b;
+
+  if (pure) subtract_cell_mean(g, g.r.a);
+
+  if (use_gmg) {
+    gmg_create_coeffs(gmg, g);
+    gmg_vcycle(gmg, g, g.z.a, g.r.a);
+  } else {
+    // z = invAdiag * r over all (N+2)^3 entries (base_k_mult_elementwise_array, :359)
+    const size_t n = g.z.a.size();
+    for (size_t i = 0; i < n; ++i) g.z.a.d[i] = g.invAdiag.a.d[i] * g.r.a.d[i];
+  }
+  if (pure) subtract_cell_mean(g, g.z.a);
+  std::memcpy(g.dir.a.d, g.z.a.d, g.z.a.size() * sizeof(double));
+
+  double rz[2];
+  int rz_old = 0, rz_new = 1;
+  rz[rz_old] = interior_dot(g, g.r.a, g.z.a);
+
+  auto true_rel = [&]() {
+    Buf t;
+    t.alloc(Nx + 2, Ny + 2, Nz + 2);
+    apply_A(g, g.pd, t.a);
+    const double s = det_sum_rows(Ny * Nz, [&](int rr) {
+      const int iy = rr % Ny + 1, iz = rr / Ny + 1;
+      double acc = 0.0;
+      for (int ix = 1; ix <= Nx; ++ix) {
+        const double d = bhat.a(ix, iy, iz) - t.a(ix, iy, iz);
+        acc += d * d;
+      }
+      return acc;
+    });
+    return std::sqrt(s) / norm_b;
+  };
+
+  int iter = 0;
+  bool conv = false;
+  for (iter = 0; iter < max_iter; ++iter) {
+    apply_A(g, g.dir.a, g.Ap.a);  // k_make_pAp
+    const double pAp = interior_dot(g, g.dir.a, g.Ap.a);
+    const double alpha = rz[rz_old] / pAp;
+    if (use_gmg) {
+      // k_update_p_r (:66-85)
+#pragma omp parallel for collapse(2) schedule(static)
+      for (int iz = 1; iz <= Nz; ++iz)
+        for (int iy = 1; iy <= Ny; ++iy)
+          for (int ix = 1; ix <= Nx; ++ix) {
+            g.pd(ix, iy, iz) += alpha * g.dir.a(ix, iy, iz);
+            g.r.a(ix, iy, iz) -= alpha * g.Ap.a(ix, iy, iz);
+          }
+      if (pure) subtract_cell_mean(g, g.r.a);
+      gmg_vcycle(gmg, g, g.z.a, g.r.a);
+      rz[rz_new] = interior_dot(g, g.r.a, g.z.a);
+    } else {
+      // k_update_p_r_z_make_rz_tmp (:248-273)
+#pragma omp parallel for collapse(2) schedule(static)
+      for (int iz = 1; iz <= Nz; ++iz)
+        for (int iy = 1; iy <= Ny; ++iy)
+          for (int ix = 1; ix <= Nx; ++ix) {
+            const double r_new = g.r.a(ix, iy, iz) - alpha * g.Ap.a(ix, iy, iz);
+            g.pd(ix, iy, iz) += alpha * g.dir.a(ix, iy, iz);
+            g.r.a(ix, iy, iz) = r_new;
+            g.z.a(ix, iy, iz) = g.invAdiag.a(ix, iy, iz) * r_new;
+          }
+      rz[rz_new] = interior_dot(g, g.r.a, g.z.a);
+    }
+    bool stop = false;
+    if (stop_rule == 2) {
+      stop = true_rel() < tol;
+    } else if (iter % check_freq == 0) {
+      if (stop_rule == 0) {
+        const double max_divu = interior_maxabs(g, g.r.a) * dt;
+        stop = max_divu < tol;
+      } else {
+        stop = std::sqrt(interior_dot(g, g.r.a, g.r.a)) / norm_b < tol;
+      }
+    }
+    if (stop) { iter++; conv = true; break; }
+    // k_update_dir (:276-288)
+    const double beta = rz[rz_new] / rz[rz_old];
+#pragma omp parallel for collapse(2) schedule(static)
+    for (int iz = 1; iz <= Nz; ++iz)
+      for (int iy = 1; iy <= Ny; ++iy)
+        for (int ix = 1; ix <= Nx; ++ix)
+          g.dir.a(ix, iy, iz) = g.z.a(ix, iy, iz) + beta * g.dir.a(ix, iy, iz);
+    std::swap(rz_old, rz_new);
+  }
+  st->iterations = iter;
+  st->converged = conv ? 1 : 0;
+  st->res_max = interior_maxabs(g, g.r.a);
+  st->res_rel = std::sqrt(interior_dot(g, g.r.a, g.r.a)) / norm_b;
+  st->true_res_rel = true_rel();
+  return 0;
+}
+
+// k_correct_vof_velocity (CFD/G_SMACSolver.cu:1072-1142): on F_INTERIOR
+// faces u = u* + f_inv_rho*dt*(f_s - grad p_delta); p += p_delta on
+// C_INTERIOR cells.  Faces of other types are left untouched.
+void orc_correct(int Nx, int Ny, int Nz, double inv_dx, double inv_dy, double inv_dz, double dt,
+                 const uint8_t* ct, const uint8_t* fxt, const uint8_t* fyt, const uint8_t* fzt,
+                 const double* pd, double* p, const double* vxs, const double* vys, const double* vzs,
+                 const double* firx, const double* firy, const double* firz, const double* fsx,
+                 const double* fsy, const double* fsz, double* vx, double* vy, double* vz) {
+  View<const uint8_t> C{ct, Nx + 2, Ny + 2, Nz + 2};
+  View<const uint8_t> X{fxt, Nx + 3, Ny + 2, Nz + 2}, Y{fyt, Nx + 2, Ny + 3, Nz + 2}, Z{fzt, Nx + 2, Ny + 2, Nz + 3};
+  View<const double> PD{pd, Nx + 2, Ny + 2, Nz + 2};
+  Arr PN{p, Nx + 2, Ny + 2, Nz + 2};
+  View<const double> VXS{vxs, Nx + 3, Ny + 2, Nz + 2}, VYS{vys, Nx + 2, Ny + 3, Nz + 2}, VZS{vzs, Nx + 2, Ny + 2, Nz + 3};
+  View<const double> IRX{firx, Nx + 3, Ny + 2, Nz + 2}, IRY{firy, Nx + 2, Ny + 3, Nz + 2}, IRZ{firz, Nx + 2, Ny + 2, Nz + 3};
+  View<const double> SX{fsx, Nx + 3, Ny + 2, Nz + 2}, SY{fsy, Nx + 2, Ny + 3, Nz + 2}, SZ{fsz, Nx + 2, Ny + 2, Nz + 3};
+  Arr VX{vx, Nx + 3, Ny + 2, Nz + 2}, VY{vy, Nx + 2, Ny + 3, Nz + 2}, VZ{vz, Nx + 2, Ny + 2, Nz + 3};
+  // the reference's thread range: ix,iy,iz from 1, bounded per face kind
+#pragma omp parallel for collapse(2) schedule(static)
+  for (int iz = 1; iz < Nz + 3; ++iz)
+    for (int iy = 1; iy < Ny + 3; ++iy)
+      for (int ix = 1; ix < Nx + 3; ++ix) {
+        if (!(iy >= Ny + 2 || ix >= Nx + 3 || iz >= Nz + 2))
+          if (X(ix, iy, iz) == F_INTERIOR)
+            VX(ix, iy, iz) = VXS(ix, iy, iz) + IRX(ix, iy, iz) * dt *
+                                                   (SX(ix, iy, iz) - (PD(ix, iy, iz) - PD(ix - 1, iy, iz)) * inv_dx);
+        if (!(iy >= Ny + 3 || ix >= Nx + 2 || iz >= Nz + 2))
+          if (Y(ix, iy, iz) == F_INTERIOR)
+            VY(ix, iy, iz) = VYS(ix, iy, iz) + IRY(ix, iy, iz) * dt *
+                                                   (SY(ix, iy, iz) - (PD(ix, iy, iz) - PD(ix, iy - 1, iz)) * inv_dy);
+        if (!(iy >= Ny + 2 || ix >= Nx + 2 || iz >= Nz + 3))
+          if (Z(ix, iy, iz) == F_INTERIOR)
+            VZ(ix, iy, iz) = VZS(ix, iy, iz) + IRZ(ix, iy, iz) * dt *
+                                                   (SZ(ix, iy, iz) - (PD(ix, iy, iz) - PD(ix, iy, iz - 1)) * inv_dz);
+        if (ix < Nx + 1 && iy < Ny + 1 && iz < Nz + 1)
+          if (C(ix, iy, iz) == C_INTERIOR) PN(ix, iy, iz) += PD(ix, iy, iz);
+      }
+}
+
+}  // extern "C"

@@ -1,0 +1,65 @@
+"""Shared builders for the tests: workload Case -> oracle RefGrid, golden I/O."""
+from __future__ import annotations
+
+import json
+import os
+
+import numpy as np
+
+from mydemcfd_b200 import workloads as W
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+
+def ref_grid(case, eps=None, eps_old=None, fs=None):
+    from oracle import oracle as O
+    sh = W.shapes(case.N)
+    eps = np.ones(sh["cell"]) if eps is None else eps
+    eps_old = np.ones(sh["cell"]) if eps_old is None else eps_old
+    fsx, fsy, fsz = fs if fs is not None else (np.zeros(sh["x"]), np.zeros(sh["y"]), np.zeros(sh["z"]))
+    return O.RefGrid(case.N, case.h, case.dt, case.vxs, case.vys, case.vzs, eps, eps_old,
+                     case.fbx, case.fby, case.fbz, fsx, fsy, fsz, case.fbx, case.fby, case.fbz,
+                     case.ct, case.fxt, case.fyt, case.fzt)
+
+
+def oracle_solid_fraction(N, h, origin, spheres):
+    from oracle import oracle as O
+    return O.solid_fraction_spheres(N, h, origin, spheres)
+
+
+def build_case(spec):
+    spec = dict(spec)
+    kind = spec.pop("kind")
+    if kind == "plain":
+        if "N" in spec:
+            spec["N"] = tuple(spec["N"])
+        return W.plain_case(**spec)
+    if kind == "vof":
+        return W.vof_case(**spec)
+    if kind == "ibm":
+        return W.ibm_case(solid_fraction=oracle_solid_fraction, rmin_cells=3.0, rmax_cells=6.0, **spec)
+    raise ValueError(kind)
+
+
+def golden_names():
+    if not os.path.isdir(GOLDEN):
+        return []
+    return sorted(f[:-4] for f in os.listdir(GOLDEN) if f.endswith(".npz"))
+
+
+def load_golden(name):
+    d = np.load(os.path.join(GOLDEN, name + ".npz"))
+    meta = json.loads(str(d["meta"]))
+    return meta, {k: d[k] for k in d.files if k != "meta"}
+
+
+def fluid_demeaned(p_interior, ct):
+    m = W.interior(ct) == W.C_INTERIOR
+    out = np.where(m, p_interior, 0.0)
+    out[m] -= out[m].mean()
+    return out
+
+
+def rel_err(a, b):
+    nb = np.linalg.norm(b)
+    return np.linalg.norm(a - b) / (nb if nb > 0 else 1.0)

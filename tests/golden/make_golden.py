@@ -1,0 +1,98 @@
+"""Generate the golden vectors of tests/golden/ by running the REFERENCE's own
+GPU pressure path (oracle/_ref/libref_smac.so, built from the reference
+sources by `make -C oracle ref`) on seeded inputs.
+
+Needs a CUDA device.  Inputs are NOT stored: they are regenerated from the
+seeds by mydemcfd_b200.workloads (SplitMix64), so a fixture holds only the
+reference's outputs and the parameters that produced them.
+
+    python tests/golden/make_golden.py --out tests/golden
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import sys
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+sys.path.insert(0, ROOT)
+
+from mydemcfd_b200 import workloads as W  # noqa: E402
+from oracle import oracle as O  # noqa: E402
+from oracle import ref as REF  # noqa: E402
+
+# (name, builder kwargs, solver_type, tol, levels, store velocities)
+CASES = [
+    ("plain24_s7_gmg", dict(kind="plain", n=24, seed=7), 3, 1e-11, 4, True),
+    ("plain32_s1_gmg", dict(kind="plain", n=32, seed=1), 3, 1e-11, 4, False),
+    ("plain48_s2_gmg", dict(kind="plain", n=48, seed=2), 3, 1e-9, 4, False),
+    ("plain24_s5_jacobi", dict(kind="plain", n=24, seed=5), 1, 1e-10, 4, False),
+    ("plain24_s6_gmg_nomean", dict(kind="plain", n=24, seed=6), 2, 1e-10, 4, False),
+    ("plain32x24x48_s8_gmg", dict(kind="plain", N=(32, 24, 48), seed=8), 3, 1e-10, 4, False),
+    ("vof32_s3_r1000", dict(kind="vof", n=32, seed=3, ratio=1000.0), 3, 1e-9, 4, False),
+    ("ibm48_s4", dict(kind="ibm", n=48, seed=4, nsph=6), 3, 1e-9, 4, False),
+    ("plain64_s1_gmg", dict(kind="plain", n=64, seed=1), 3, 1e-11, 4, False),  # config 1, stored sparsely
+]
+
+
+def oracle_solid_fraction(N, h, origin, spheres):
+    return O.solid_fraction_spheres(N, h, origin, spheres)
+
+
+def build_case(spec):
+    spec = dict(spec)
+    kind = spec.pop("kind")
+    if kind == "plain":
+        return W.plain_case(**spec)
+    if kind == "vof":
+        return W.vof_case(**spec)
+    if kind == "ibm":
+        return W.ibm_case(solid_fraction=oracle_solid_fraction, rmin_cells=3.0, rmax_cells=6.0, **spec)
+    raise ValueError(kind)
+
+
+def sparse_sample(a, stride=97):
+    flat = a.reshape(-1)
+    idx = np.arange(0, flat.size, stride)
+    return idx, flat[idx]
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--out", default=os.path.join(ROOT, "tests", "golden"))
+    args = ap.parse_args()
+    os.makedirs(args.out, exist_ok=True)
+    index = {}
+    for name, spec, st, tol, levels, store_v in CASES:
+        case = build_case(spec)
+        r = REF.solve(case, solver_type=st, tol=tol, levels=levels, do_correct=True)
+        meta = {"spec": spec, "solver_type": st, "tol": tol, "levels": levels, "iterations": r["iterations"],
+                "num_levels": r["num_levels"], "N": list(case.N), "dt": case.dt}
+        pd = W.interior(r["p_delta"])
+        rhs = W.interior(r["rhs"])
+        arrays = {"meta": np.array(json.dumps(meta))}
+        if case.N[0] * case.N[1] * case.N[2] <= 48 ** 3:
+            arrays["p_delta"] = pd
+            arrays["rhs"] = rhs
+        else:
+            idx, val = sparse_sample(pd)
+            arrays["p_delta_idx"], arrays["p_delta_val"] = idx, val
+            idx, val = sparse_sample(rhs)
+            arrays["rhs_idx"], arrays["rhs_val"] = idx, val
+            arrays["p_delta_norm"] = np.array(np.linalg.norm(pd))
+            arrays["p_delta_mean"] = np.array(pd.mean())
+        if store_v:
+            arrays["vx"], arrays["vy"], arrays["vz"] = r["vx"], r["vy"], r["vz"]
+            arrays["p"] = r["p"]
+        np.savez_compressed(os.path.join(args.out, name + ".npz"), **arrays)
+        index[name] = meta
+        print(name, meta, flush=True)
+    with open(os.path.join(args.out, "index.json"), "w") as f:
+        json.dump(index, f, indent=1, sort_keys=True)
+
+
+if __name__ == "__main__":
+    main()
