@@ -45,6 +45,10 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-budget", type=float, default=25.0, help="seconds of oracle work for cpu_baseline")
+    ap.add_argument("--kernel-only", type=int, default=None,
+                    help="set up the workload and launch one kernel (smac_time_kernel id) a few times: a small, "
+                         "self-contained command for ncu captures")
+    ap.add_argument("--reps", type=int, default=3)
     return ap.parse_args()
 
 
@@ -338,8 +342,28 @@ def run_ours(args, rank, world, local_rank):
         dist.destroy_process_group()
 
 
+def run_kernel_only(args):
+    import torch
+
+    from mydemcfd_b200 import _native as nat
+    from mydemcfd_b200.solver import B200PressureSolver, DeviceGrid
+    case = build_case(args)
+    g = DeviceGrid.from_case(case)
+    s = B200PressureSolver(case.N, case.h, precision=nat.PRECISION_MIXED, tol=args.tol)
+    s.set_coefficients(g)
+    s.divergence(g, case.dt)
+    ms, b = s.time_kernel(args.kernel_only, reps=args.reps)
+    torch.cuda.synchronize()
+    print(json.dumps({"kernel_id": args.kernel_only, "n": args.n, "ms_per_launch": ms, "alg_bytes": b,
+                      "GB/s": b / (ms / 1e3) / 1e9}))
+    s.close()
+
+
 def main():
     args = parse()
+    if args.kernel_only is not None:
+        run_kernel_only(args)
+        return
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))

@@ -212,12 +212,23 @@ smac_status smac_project_adjoint(smac_handle* h, const double* gvx, const double
 smac_status smac_apply_A(smac_handle* h, const double* x, double* y);
 
 /* Time `reps` launches of one kernel of the solve on the handle's stream with
- * CUDA events (kernel ids: 0 FP64 matvec+dot, 1 FP32 matvec+dot, 2 FP64 RB-GS
- * sweep, 3 FP32 RB-GS sweep, 4 FP64 true residual, 5 divergence, 6 correction)
- * on the finest grid.  Writes the mean milliseconds per launch and the
- * algorithmic bytes of one launch. */
+ * CUDA events, on the finest grid (kernel ids: 0 FP64 matvec+dot, 1 FP32
+ * matvec+dot, 2 FP64 fused red-black sweep, 3 FP32 fused red-black sweep,
+ * 4 FP64 true residual, 5 FP64 sweep as two half-sweep launches, 6 FP32 sweep
+ * as two half-sweep launches, 7 FP32 direction update + matvec).  Writes the
+ * mean milliseconds per launch (per sweep for 5 and 6) and the algorithmic
+ * bytes of one launch. */
 smac_status smac_time_kernel(smac_handle* h, int kernel_id, int reps, float* ms_per_launch,
                              double* alg_bytes_per_launch);
+
+/* Self-test of the fused red-black sweep: runs one fused out-of-place sweep
+ * (mode 0 plain, 1 from zero, 2 with the coarse-grid correction of grid 1
+ * added to the input) and the same sweep as two in-place half-sweep launches
+ * on the handle's current finest-grid iterate and residual (left by the last
+ * solve; the call overwrites scratch vectors), and writes the number of cells
+ * whose results differ bitwise.  precision: smac_precision of the vectors.
+ * No counterpart in the reference (it has no Gauss-Seidel smoother). */
+smac_status smac_selftest_sweep(smac_handle* h, int precision, int mode, long long* mismatches);
 
 #ifdef __cplusplus
 }

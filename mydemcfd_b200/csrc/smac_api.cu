@@ -10,6 +10,7 @@
 
 #include "smac_b200.h"
 #include "smac_kernels.cuh"
+#include "smac_rbgs.cuh"
 
 using namespace smac;
 
@@ -57,10 +58,10 @@ struct Level {
   Geom g{};
   int cx = 0, cy = 0, cz = 0;  // coarsened from the grid above
   double *bx64 = nullptr, *by64 = nullptr, *bz64 = nullptr;
-  double *x64 = nullptr, *rhs64 = nullptr;  // levels >= 1
+  double *x64 = nullptr, *x64b = nullptr, *rhs64 = nullptr;  // levels >= 1 (two iterates: out-of-place sweeps)
   void *bxm = nullptr, *bym = nullptr, *bzm = nullptr;  // mixed-precision coefficients
   int ctm = CT_F32;
-  float *x32 = nullptr, *rhs32 = nullptr;   // levels >= 1
+  float *x32 = nullptr, *x32b = nullptr, *rhs32 = nullptr;   // levels >= 1
 };
 
 }  // namespace
@@ -79,10 +80,11 @@ struct smac_handle {
   // copies of the reference-layout types (the correction and the adjoint read them)
   uint8_t *ct = nullptr, *fxt = nullptr, *fyt = nullptr, *fzt = nullptr;
   // fine FP64 vectors
-  double *b64 = nullptr, *x64a = nullptr, *x64b = nullptr, *r64 = nullptr, *z64 = nullptr, *d64 = nullptr,
-         *q64 = nullptr, *tmp64 = nullptr;
+  double *b64 = nullptr, *x64a = nullptr, *x64b = nullptr, *r64 = nullptr, *z64 = nullptr, *z64b = nullptr,
+         *d64 = nullptr, *d64b = nullptr, *q64 = nullptr, *tmp64 = nullptr;
   // fine FP32 vectors (mixed)
-  float *r32 = nullptr, *z32 = nullptr, *d32 = nullptr, *q32 = nullptr, *e32 = nullptr;
+  float *r32 = nullptr, *z32 = nullptr, *z32b = nullptr, *d32 = nullptr, *d32b = nullptr, *q32 = nullptr,
+        *e32 = nullptr;
   RedBuf red{};
   Scalars* s = nullptr;    // device
   Scalars* hs = nullptr;   // pinned host mirror
@@ -171,41 +173,81 @@ void account(smac_handle* h, const Geom& g, double bytes_per_cell, int n = 1) {
 // ---------------------------------------------------------------------------
 // V-cycle launch sequence.  T: vector type, CS: coefficient type of the
 // separately launched grids, CC: coefficient type of the single-CTA set.
+// Grids above the single-CTA set use the fused out-of-place sweep
+// (k_rbgs_sweep): pre-smoothing red first from x = 0, residual + restriction,
+// post-smoothing black first with the prolongation fused into its first
+// sweep; `dot` folds r.z into the last sweep of the finest grid.  Returns the
+// buffer that holds z.
+template <class T>
+int sweep_zchunk(const Geom& g) {
+  return g.nz >= 128 ? 16 : (g.nz >= 32 ? 8 : 4);
+}
+template <class T>
+inline dim3 grid_sweep(const Geom& g, int zc) {
+  constexpr int TY = RbTile<T>::TY;
+  return dim3((g.nx + RB_TX - 1) / RB_TX, (g.ny + TY - 1) / TY, (g.nz + zc - 1) / zc);
+}
+
+template <class T, class CS>
+void launch_sweep(smac_handle* h, int l, int mode, bool dot, const T* xin, T* xout, const T* rhs, const double* sh,
+                  const void* bx, const void* by, const void* bz, int c0, const T* xc) {
+  const Level& L = h->lv[l];
+  const Geom& g = L.g;
+  const Level& Lc = h->lv[l + 1 < h->nlev ? l + 1 : l];
+  auto S = stencil<T, CS>(g, bx, by, bz);
+  const int zc = sweep_zchunk<T>(g);
+  const dim3 gr = grid_sweep<T>(g, zc);
+  const dim3 bl(RB_NT, 1, 1);
+#define SW(M, D) k_rbgs_sweep<T, CS, M, D><<<gr, bl, 0, h->stream>>>(g, xin, xout, rhs, sh, S, c0, xc, Lc.g, Lc.cx, \
+                                                                      Lc.cy, Lc.cz, h->s, h->red, zc)
+  if (mode == 0) { if (dot) SW(0, true); else SW(0, false); }
+  else if (mode == 1) { if (dot) SW(1, true); else SW(1, false); }
+  else { if (dot) SW(2, true); else SW(2, false); }
+#undef SW
+}
+
 template <class T, class CS, class CC>
-smac_status launch_vcycle(smac_handle* h, T* r0, T* z0, bool mixed) {
+smac_status launch_vcycle(smac_handle* h, T* r0, T* z0a, T* z0b, bool mixed, bool dot, T** z_out) {
   const smac_options& o = h->opts;
   const int lc = h->lc;
   const double* shift0 = &h->s->rshift;
   const double s = sizeof(T);
   const double sc = mixed ? (double)sizeof(CS) : 8.0;
-  auto X = [&](int l) -> T* { return l == 0 ? z0 : (mixed ? (T*)h->lv[l].x32 : (T*)h->lv[l].x64); };
+  auto XA = [&](int l) -> T* { return l == 0 ? z0a : (mixed ? (T*)h->lv[l].x32 : (T*)h->lv[l].x64); };
+  auto XB = [&](int l) -> T* { return l == 0 ? z0b : (mixed ? (T*)h->lv[l].x32b : (T*)h->lv[l].x64b); };
   auto B = [&](int l) -> T* { return l == 0 ? r0 : (mixed ? (T*)h->lv[l].rhs32 : (T*)h->lv[l].rhs64); };
   auto CF = [&](int l, int which) -> const void* {
     const Level& L = h->lv[l];
     if (!mixed) return which == 0 ? (const void*)L.bx64 : which == 1 ? (const void*)L.by64 : (const void*)L.bz64;
     return which == 0 ? L.bxm : which == 1 ? L.bym : L.bzm;
   };
+  T* cur[MAXL] = {};
+  T* fin[MAXL] = {};
+  auto other = [&](int l, T* p) { return p == XA(l) ? XB(l) : XA(l); };
   for (int l = 0; l < lc; ++l) {
-    const Level& L = h->lv[l];
-    const Geom& g = L.g;
-    const int kz = kz_for(g);
-    auto S = stencil<T, CS>(g, CF(l, 0), CF(l, 1), CF(l, 2));
+    const Geom& g = h->lv[l].g;
     const double* sh = (l == 0) ? shift0 : nullptr;
-    for (int it = 0; it < o.nu1; ++it) {
-      k_rbgs<T, CS><<<grid_pairs(g, kz), kBlock, 0, h->stream>>>(g, X(l), B(l), sh, S, 0, it == 0, (const T*)nullptr,
-                                                                  g, 0, 0, 0, h->s, kz);
-      k_rbgs<T, CS><<<grid_pairs(g, kz), kBlock, 0, h->stream>>>(g, X(l), B(l), sh, S, 1, 0, (const T*)nullptr, g, 0,
-                                                                  0, 0, h->s, kz);
-      account(h, g, (it == 0 ? 4.0 : 6.0) * s + 6 * sc, 2);
+    T* in = nullptr;
+    T* out = XA(l);
+    launch_sweep<T, CS>(h, l, 1, false, in, out, B(l), sh, CF(l, 0), CF(l, 1), CF(l, 2), 0, nullptr);
+    account(h, g, 4.0 * s + 3 * sc, 1);
+    in = out;
+    for (int it = 1; it < o.nu1; ++it) {
+      out = other(l, in);
+      launch_sweep<T, CS>(h, l, 0, false, in, out, B(l), sh, CF(l, 0), CF(l, 1), CF(l, 2), 0, nullptr);
+      account(h, g, 3.0 * s + 3 * sc, 1);
+      in = out;
     }
+    cur[l] = in;
     CKL();
     const Level& Lc = h->lv[l + 1];
+    auto S = stencil<T, CS>(g, CF(l, 0), CF(l, 1), CF(l, 2));
     k_resid_restrict<T, CS><<<grid_planes(Lc.g.nx, Lc.g.ny, Lc.g.nz), kBlock, 0, h->stream>>>(
-        g, X(l), B(l), sh, S, Lc.g, Lc.cx, Lc.cy, Lc.cz, B(l + 1), h->s);
+        g, cur[l], B(l), sh, S, Lc.g, Lc.cx, Lc.cy, Lc.cz, B(l + 1), h->s);
     account(h, g, 2 * s + 3 * sc + s / 8, 1);
     CKL();
   }
-  // single-CTA coarse set
+  // single-CTA coarse set, in place on XA
   {
     CoarseSet set{};
     set.n = h->nlev - lc;
@@ -215,81 +257,90 @@ smac_status launch_vcycle(smac_handle* h, T* r0, T* z0, bool mixed) {
       C.g = h->lv[l].g;
       C.cx = h->lv[l].cx; C.cy = h->lv[l].cy; C.cz = h->lv[l].cz;
       C.bx = CF(l, 0); C.by = CF(l, 1); C.bz = CF(l, 2);
-      C.x = X(l);
+      C.x = XA(l);
       C.rhs = B(l);
     }
     k_coarse_vcycle<T, CC><<<1, 1024, 0, h->stream>>>(set, o.nu1, o.nu2, o.coarse_sweeps, lc == 0 ? shift0 : nullptr,
                                                        h->s);
     h->launches += 1;
     CKL();
+    fin[lc] = XA(lc);
   }
   for (int l = lc - 1; l >= 0; --l) {
-    const Level& L = h->lv[l];
-    const Geom& g = L.g;
-    const int kz = kz_for(g);
-    auto S = stencil<T, CS>(g, CF(l, 0), CF(l, 1), CF(l, 2));
+    const Geom& g = h->lv[l].g;
     const double* sh = (l == 0) ? shift0 : nullptr;
-    const Level& Lc = h->lv[l + 1];
+    T* in = cur[l];
     for (int it = 0; it < o.nu2; ++it) {
-      k_rbgs<T, CS><<<grid_pairs(g, kz), kBlock, 0, h->stream>>>(g, X(l), B(l), sh, S, 1, 0,
-                                                                  it == 0 ? (const T*)X(l + 1) : (const T*)nullptr,
-                                                                  Lc.g, Lc.cx, Lc.cy, Lc.cz, h->s, kz);
-      k_rbgs<T, CS><<<grid_pairs(g, kz), kBlock, 0, h->stream>>>(g, X(l), B(l), sh, S, 0, 0, (const T*)nullptr, g, 0,
-                                                                  0, 0, h->s, kz);
-      account(h, g, 6.0 * s + 6 * sc + (it == 0 ? s / 8 : 0.0), 2);
+      T* out = other(l, in);
+      const bool last_dot = dot && l == 0 && it == o.nu2 - 1;
+      launch_sweep<T, CS>(h, l, it == 0 ? 2 : 0, last_dot, in, out, B(l), sh, CF(l, 0), CF(l, 1), CF(l, 2), 1,
+                          it == 0 ? fin[l + 1] : nullptr);
+      account(h, g, 3.0 * s + 3 * sc + (it == 0 ? s / 8 : 0.0), 1);
+      in = out;
     }
+    fin[l] = in;
     CKL();
   }
+  *z_out = fin[0];
   return SMAC_OK;
 }
 
-// One PCG iteration: preconditioner, r.z and beta, direction, matvec and
-// alpha, update (+ FP64 residual recomputation in mixed precision).
-smac_status launch_iteration(smac_handle* h, bool mixed, bool gmg) {
+// One PCG iteration: preconditioner (+ r.z, beta), direction update fused
+// with the matvec (+ p.Ap, alpha), update of x and r (+ stopping test), and
+// in mixed precision the FP64 residual recomputation when requested.
+// `parity` selects which direction buffer is the old one.
+smac_status launch_iteration(smac_handle* h, bool mixed, bool gmg, int parity) {
   const Geom& g = h->lv[0].g;
   const int kz = kz_for(g);
   const dim3 gr = grid_cells(g, kz);
+  const bool fused_dot = gmg && h->lc > 0;
   if (!mixed) {
+    double* z = h->z64;
     if (gmg) {
-      TRY((launch_vcycle<double, double, double>(h, h->r64, h->z64, false)));
+      TRY((launch_vcycle<double, double, double>(h, h->r64, h->z64, h->z64b, false, fused_dot, &z)));
     } else {
       auto S = stencil<double, double>(g, h->lv[0].bx64, h->lv[0].by64, h->lv[0].bz64);
       k_jacobi_precond<double, double><<<gr, kBlock, 0, h->stream>>>(g, h->r64, &h->s->rshift, S, h->z64, h->s, kz);
       account(h, g, 2 * 8 + 3 * 8);
     }
-    k_dot_rz<double><<<gr, kBlock, 0, h->stream>>>(g, h->r64, h->z64, h->red, h->s, kz);
-    k_dir<double><<<gr, kBlock, 0, h->stream>>>(g, h->z64, h->d64, h->s, kz);
+    if (!fused_dot) {
+      k_dot_rz<double><<<gr, kBlock, 0, h->stream>>>(g, h->r64, z, h->red, h->s, kz);
+      account(h, g, 16, 1);
+    }
+    double* dold = parity ? h->d64b : h->d64;
+    double* dnew = parity ? h->d64 : h->d64b;
     auto S = stencil<double, double>(g, h->lv[0].bx64, h->lv[0].by64, h->lv[0].bz64);
-    k_matvec_pap<double, double><<<gr, kBlock, 0, h->stream>>>(g, h->d64, S, h->q64, h->red, h->s, kz);
-    k_update<double, double><<<gr, kBlock, 0, h->stream>>>(g, h->x64a, h->d64, h->r64, h->q64, h->red, h->s, kz);
-    account(h, g, 16, 1);
-    account(h, g, 24, 1);
-    account(h, g, 5 * 8, 1);
+    k_dir_matvec<double, double><<<gr, kBlock, 0, h->stream>>>(g, z, dold, dnew, S, h->q64, h->red, h->s, kz);
+    k_update<double, double><<<gr, kBlock, 0, h->stream>>>(g, h->x64a, dnew, h->r64, h->q64, h->red, h->s, kz);
+    account(h, g, 7 * 8, 1);
     account(h, g, 6 * 8, 1);
     CKL();
   } else {
     const bool bf16 = use_bf16(h, h->opts);
+    float* z = h->z32;
     if (gmg) {
       if (bf16) {
-        TRY((launch_vcycle<float, float, __nv_bfloat16>(h, h->r32, h->z32, true)));
+        TRY((launch_vcycle<float, float, __nv_bfloat16>(h, h->r32, h->z32, h->z32b, true, fused_dot, &z)));
       } else {
-        TRY((launch_vcycle<float, float, float>(h, h->r32, h->z32, true)));
+        TRY((launch_vcycle<float, float, float>(h, h->r32, h->z32, h->z32b, true, fused_dot, &z)));
       }
     } else {
       auto S = stencil<float, float>(g, h->lv[0].bxm, h->lv[0].bym, h->lv[0].bzm);
       k_jacobi_precond<float, float><<<gr, kBlock, 0, h->stream>>>(g, h->r32, &h->s->rshift, S, h->z32, h->s, kz);
       account(h, g, 2 * 4 + 3 * 4);
     }
-    k_dot_rz<float><<<gr, kBlock, 0, h->stream>>>(g, h->r32, h->z32, h->red, h->s, kz);
-    k_dir<float><<<gr, kBlock, 0, h->stream>>>(g, h->z32, h->d32, h->s, kz);
+    if (!fused_dot) {
+      k_dot_rz<float><<<gr, kBlock, 0, h->stream>>>(g, h->r32, z, h->red, h->s, kz);
+      account(h, g, 8, 1);
+    }
+    float* dold = parity ? h->d32b : h->d32;
+    float* dnew = parity ? h->d32 : h->d32b;
     auto S = stencil<float, float>(g, h->lv[0].bxm, h->lv[0].bym, h->lv[0].bzm);
-    k_matvec_pap<float, float><<<gr, kBlock, 0, h->stream>>>(g, h->d32, S, h->q32, h->red, h->s, kz);
-    k_update<float, float><<<gr, kBlock, 0, h->stream>>>(g, h->e32, h->d32, h->r32, h->q32, h->red, h->s, kz);
+    k_dir_matvec<float, float><<<gr, kBlock, 0, h->stream>>>(g, z, dold, dnew, S, h->q32, h->red, h->s, kz);
+    k_update<float, float><<<gr, kBlock, 0, h->stream>>>(g, h->e32, dnew, h->r32, h->q32, h->red, h->s, kz);
     auto S64 = stencil<double, double>(g, h->lv[0].bx64, h->lv[0].by64, h->lv[0].bz64);
     k_reliable<float><<<gr, kBlock, 0, h->stream>>>(g, h->x64a, h->x64b, h->e32, h->b64, S64, h->r32, h->red, h->s, kz);
-    account(h, g, 8, 1);
-    account(h, g, 12, 1);
-    account(h, g, 5 * 4, 1);
+    account(h, g, 7 * 4, 1);
     account(h, g, 6 * 4, 1);
     h->launches += 1;  // the FP64 residual kernel (its bytes are counted when it runs)
     CKL();
@@ -304,7 +355,8 @@ smac_status get_graph(smac_handle* h, bool mixed, bool gmg, cudaGraphExec_t* out
     const double saved_bytes = h->alg_bytes;
     const int saved_launches = h->launches;
     CK(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
-    smac_status st = launch_iteration(h, mixed, gmg);
+    smac_status st = launch_iteration(h, mixed, gmg, 0);
+    if (st == SMAC_OK) st = launch_iteration(h, mixed, gmg, 1);
     cudaError_t ec = cudaStreamEndCapture(h->stream, &graph);
     h->alg_bytes = saved_bytes;
     h->launches = saved_launches;
@@ -334,34 +386,35 @@ void drop_graphs(smac_handle* h) {
       if (e) { cudaGraphExecDestroy(e); e = nullptr; }
 }
 
-// Per-iteration accounting (bytes of one iteration), measured once by a dry
-// accounting pass.
+// Algorithmic bytes of one PCG iteration (the byte model: every array a
+// kernel must touch, read or written once; s = vector element size, sc =
+// coefficient element size): fused sweeps 5s+... per cell as accounted in
+// launch_vcycle, direction+matvec 7s, update 6s.
 double iteration_bytes(smac_handle* h, bool mixed, bool gmg, int* launches) {
-  const double b0 = h->alg_bytes;
-  const int l0 = h->launches;
-  // count without launching: replicate the accounting of launch_iteration
   const Geom& g = h->lv[0].g;
   double bytes = 0.0;
   int n = 0;
-  const double s = mixed ? 4.0 : 8.0, sc = mixed ? 4.0 : 8.0;
+  const double s = mixed ? 4.0 : 8.0;
   if (gmg) {
     for (int l = 0; l < h->lc; ++l) {
       const double cells = (double)h->lv[l].g.cells();
-      const double scl = (l == 0 || !mixed) ? sc : 4.0;
-      for (int it = 0; it < h->opts.nu1; ++it) { bytes += ((it == 0 ? 4.0 : 6.0) * s + 6 * scl) * cells; n += 2; }
-      bytes += (2 * s + 3 * scl + s / 8) * cells; n += 1;
-      for (int it = 0; it < h->opts.nu2; ++it) { bytes += (6.0 * s + 6 * scl + (it == 0 ? s / 8 : 0.0)) * cells; n += 2; }
+      const double sc = mixed ? 4.0 : 8.0;
+      bytes += (4.0 * s + 3 * sc) * cells;
+      n += 1;
+      for (int it = 1; it < h->opts.nu1; ++it) { bytes += (3.0 * s + 3 * sc) * cells; n += 1; }
+      bytes += (2 * s + 3 * sc + s / 8) * cells;
+      n += 1;
+      for (int it = 0; it < h->opts.nu2; ++it) { bytes += (3.0 * s + 3 * sc + (it == 0 ? s / 8 : 0.0)) * cells; n += 1; }
     }
-    n += 1;
+    n += 1;  // single-CTA coarse grids (their bytes are negligible)
+    if (h->lc == 0) { bytes += 2 * s * (double)g.cells(); n += 1; }
   } else {
-    bytes += (2 * s + 3 * sc) * (double)g.cells();
-    n += 1;
+    bytes += (2 * s + 3 * s) * (double)g.cells() + 2 * s * (double)g.cells();
+    n += 2;
   }
-  bytes += (2 * s + 3 * s + 5 * s + 6 * s) * (double)g.cells();
-  n += 4;
+  bytes += (7 * s + 6 * s) * (double)g.cells();
+  n += 2;
   if (mixed) n += 1;
-  h->alg_bytes = b0;
-  h->launches = l0;
   if (launches) *launches = n;
   return bytes;
 }
@@ -458,7 +511,8 @@ smac_status smac_create(const smac_grid_desc* desc, const smac_options* opts, vo
   smac_status st;
 #define PA(ptr) do { st = palloc(h, g0, &(ptr)); if (st != SMAC_OK) return fail(st); } while (0)
   PA(h->lv[0].bx64); PA(h->lv[0].by64); PA(h->lv[0].bz64);
-  PA(h->b64); PA(h->x64a); PA(h->x64b); PA(h->r64); PA(h->z64); PA(h->d64); PA(h->q64); PA(h->tmp64);
+  PA(h->b64); PA(h->x64a); PA(h->x64b); PA(h->r64); PA(h->z64); PA(h->z64b); PA(h->d64); PA(h->d64b); PA(h->q64);
+  PA(h->tmp64);
   {
     float* p;
     st = palloc(h, g0, &p); if (st != SMAC_OK) return fail(st); h->lv[0].bxm = p;
@@ -466,7 +520,7 @@ smac_status smac_create(const smac_grid_desc* desc, const smac_options* opts, vo
     st = palloc(h, g0, &p); if (st != SMAC_OK) return fail(st); h->lv[0].bzm = p;
     h->lv[0].ctm = CT_F32;
   }
-  PA(h->r32); PA(h->z32); PA(h->d32); PA(h->q32); PA(h->e32);
+  PA(h->r32); PA(h->z32); PA(h->z32b); PA(h->d32); PA(h->d32b); PA(h->q32); PA(h->e32);
   PA(h->fluid);
 #undef PA
   {
@@ -482,8 +536,8 @@ smac_status smac_create(const smac_grid_desc* desc, const smac_options* opts, vo
     Level& L = h->lv[l];
     const Geom& g = L.g;
     if ((st = palloc(h, g, &L.bx64)) || (st = palloc(h, g, &L.by64)) || (st = palloc(h, g, &L.bz64)) ||
-        (st = palloc(h, g, &L.x64)) || (st = palloc(h, g, &L.rhs64)) || (st = palloc(h, g, &L.x32)) ||
-        (st = palloc(h, g, &L.rhs32)))
+        (st = palloc(h, g, &L.x64)) || (st = palloc(h, g, &L.x64b)) || (st = palloc(h, g, &L.rhs64)) ||
+        (st = palloc(h, g, &L.x32)) || (st = palloc(h, g, &L.x32b)) || (st = palloc(h, g, &L.rhs32)))
       return fail(st);
     const bool bf16 = use_bf16(h, o) && l >= h->lc;
     if (bf16) {
@@ -579,8 +633,8 @@ smac_status smac_set_coefficients(smac_handle* h, const double* fbx, const doubl
   k_import_coeffs<<<grid_planes(g.nx + 1, g.ny + 1, g.nz + 1), kBlock, 0, h->stream>>>(
       g, h->R, fbx, fby, fbz, ct, fxt, fyt, fzt, h->lv[0].bx64, h->lv[0].by64, h->lv[0].bz64, h->fluid);
   CKL();
-  k_fluid_finalize<<<grid_planes(g.nx, g.ny, g.nz), kBlock, 0, h->stream>>>(g, h->lv[0].bx64, h->lv[0].by64,
-                                                                            h->lv[0].bz64, h->fluid, h->red, h->s);
+  k_fluid_finalize<<<grid_cells(g, kz_for(g)), kBlock, 0, h->stream>>>(g, h->lv[0].bx64, h->lv[0].by64,
+                                                                       h->lv[0].bz64, h->fluid, h->red, h->s, kz_for(g));
   CKL();
   // FP32 fine copy for the mixed-precision Krylov operator
   {
@@ -732,12 +786,12 @@ smac_status run_solve(smac_handle* h, const double** xout) {
   } else {
     CK(cudaMemsetAsync(base_of(g, h->d64), 0, bytes, h->stream));
   }
-  const dim3 gp = grid_planes(g.nx, g.ny, g.nz);
-  k_setup_sum<double><<<gp, kBlock, 0, h->stream>>>(g, h->b64, h->red, h->s);
+  const dim3 gr = grid_cells(g, kz);
+  k_setup_sum<double><<<gr, kBlock, 0, h->stream>>>(g, h->b64, h->red, h->s, kz);
   if (mixed)
-    k_setup_project<float><<<gp, kBlock, 0, h->stream>>>(g, h->b64, h->fluid, h->r32, h->red, h->s, o.tol);
+    k_setup_project<float><<<gr, kBlock, 0, h->stream>>>(g, h->b64, h->fluid, h->r32, h->red, h->s, o.tol, kz);
   else
-    k_setup_project<double><<<gp, kBlock, 0, h->stream>>>(g, h->b64, h->fluid, h->r64, h->red, h->s, o.tol);
+    k_setup_project<double><<<gr, kBlock, 0, h->stream>>>(g, h->b64, h->fluid, h->r64, h->red, h->s, o.tol, kz);
   CKL();
   account(h, g, 8, 1);
   account(h, g, 8 + 8 + (mixed ? 4 : 8) + 1, 1);
@@ -753,10 +807,11 @@ smac_status run_solve(smac_handle* h, const double** xout) {
       set_err("run_solve: iteration bound exceeded without a device decision");
       return SMAC_NOT_CONVERGED;
     }
-    // launch a batch of iterations; kernels after convergence return at once
-    int batch = 2;
+    // launch a batch of iterations (one graph = two iterations); kernels after
+    // convergence return at once
+    int batch = 1;
     for (int q = 0; q < batch; ++q) CK(cudaGraphLaunch(ex, h->stream));
-    launched += batch;
+    launched += 2 * batch;
     CK(cudaMemcpyAsync(h->hs, h->s, sizeof(Scalars), cudaMemcpyDeviceToHost, h->stream));
     CK(cudaStreamSynchronize(h->stream));
     if (h->hs->done) {
@@ -837,7 +892,7 @@ smac_status export_solution(smac_handle* h, const double* x, double* p_delta) {
   const dim3 gp = grid_planes(g.nx, g.ny, g.nz);
   const bool pure = is_pure(h->opts);
   if (pure) {
-    k_sum_fluid<<<gp, kBlock, 0, h->stream>>>(g, x, h->fluid, h->red, h->s);
+    k_sum_fluid<<<grid_cells(g, kz_for(g)), kBlock, 0, h->stream>>>(g, x, h->fluid, h->red, h->s, kz_for(g));
     CKL();
   }
   k_export_cells<<<gp, kBlock, 0, h->stream>>>(g, h->R, x, h->fluid, pure ? &h->s->sum_tmp : nullptr, p_delta);
@@ -878,7 +933,7 @@ smac_status smac_correct(smac_handle* h, double* p_delta, double* p, const doubl
   if (!((fsx && fsy && fsz) || (!fsx && !fsy && !fsz))) { set_err("smac_correct: fs* go together"); return SMAC_BAD_ARG; }
   const Geom& g = h->lv[0].g;
   const RefDims& R = h->R;
-  k_correct<<<grid_planes(R.Nx + 2, R.Ny + 2, R.Nz + 2), kBlock, 0, h->stream>>>(
+  k_correct<<<grid_planes(R.Nx + 3, R.Ny + 3, R.Nz + 3), kBlock, 0, h->stream>>>(
       R, g, 1.0 / h->desc.dx, 1.0 / h->desc.dy, 1.0 / h->desc.dz, dt, h->ct, h->fxt, h->fyt, h->fzt, p_delta, p, vxs,
       vys, vzs, firx, firy, firz, h->lv[0].bx64, h->lv[0].by64, h->lv[0].bz64, fsx, fsy, fsz, vx, vy, vz, 0);
   CKL();
@@ -900,7 +955,7 @@ smac_status smac_project(smac_handle* h, const double* vxs, const double* vys, c
   TRY(export_solution(h, x, p_delta));
   const Geom& g = h->lv[0].g;
   const RefDims& R = h->R;
-  k_correct<<<grid_planes(R.Nx + 2, R.Ny + 2, R.Nz + 2), kBlock, 0, h->stream>>>(
+  k_correct<<<grid_planes(R.Nx + 3, R.Ny + 3, R.Nz + 3), kBlock, 0, h->stream>>>(
       R, g, 1.0 / h->desc.dx, 1.0 / h->desc.dy, 1.0 / h->desc.dz, dt, h->ct, h->fxt, h->fyt, h->fzt, p_delta, nullptr,
       vxs, vys, vzs, nullptr, nullptr, nullptr, h->lv[0].bx64, h->lv[0].by64, h->lv[0].bz64, nullptr, nullptr, nullptr,
       vx, vy, vz, 1);
@@ -930,7 +985,7 @@ smac_status smac_project_adjoint(smac_handle* h, const double* gvx, const double
   TRY(run_solve(h, &x));
   account(h, g, 3 * 8 + 3 * 8 + 1 + 8, 1);
   const dim3 gp = grid_planes(g.nx, g.ny, g.nz);
-  k_sum_fluid<<<gp, kBlock, 0, h->stream>>>(g, x, h->fluid, h->red, h->s);
+  k_sum_fluid<<<grid_cells(g, kz_for(g)), kBlock, 0, h->stream>>>(g, x, h->fluid, h->red, h->s, kz_for(g));
   CKL();
   if (!is_pure(h->opts)) {
     // no null space: psi is the solution itself
@@ -981,6 +1036,11 @@ smac_status smac_time_kernel(smac_handle* h, int kernel_id, int reps, float* ms,
   st.beta = 0.0;
   *h->hs = st;
   CK(cudaMemcpyAsync(h->s, h->hs, sizeof(Scalars), cudaMemcpyHostToDevice, h->stream));
+  // non-zero operands: d = b (FP64) and d32 = r32, so that p.Ap > 0
+  CK(cudaMemcpyAsync(base_of(g, h->d64), base_of(g, h->b64), sizeof(double) * (size_t)g.alloc, cudaMemcpyDeviceToDevice,
+                     h->stream));
+  k_convert<float><<<1184, 256, 0, h->stream>>>(base_of(g, h->b64), base_of(g, h->d32), g.alloc);
+  k_convert<float><<<1184, 256, 0, h->stream>>>(base_of(g, h->b64), base_of(g, h->r32), g.alloc);
   cudaEvent_t e0, e1;
   CK(cudaEventCreate(&e0));
   CK(cudaEventCreate(&e1));
@@ -1000,17 +1060,35 @@ smac_status smac_time_kernel(smac_handle* h, int kernel_id, int reps, float* ms,
         break;
       }
       case 2: {
+        launch_sweep<double, double>(h, 0, 0, false, h->z64, h->z64b, h->r64, nullptr, h->lv[0].bx64, h->lv[0].by64,
+                                     h->lv[0].bz64, 0, nullptr);
+        per = 6 * 8.0;
+        break;
+      }
+      case 3: {
+        launch_sweep<float, float>(h, 0, 0, false, h->z32, h->z32b, h->r32, nullptr, h->lv[0].bxm, h->lv[0].bym,
+                                   h->lv[0].bzm, 0, nullptr);
+        per = 6 * 4.0;
+        break;
+      }
+      case 5: {
         auto S = stencil<double, double>(g, h->lv[0].bx64, h->lv[0].by64, h->lv[0].bz64);
         k_rbgs<double, double><<<grid_pairs(g, kz), kBlock, 0, h->stream>>>(g, h->z64, h->r64, nullptr, S, 0, 0, nullptr, g, 0, 0, 0, h->s, kz);
         k_rbgs<double, double><<<grid_pairs(g, kz), kBlock, 0, h->stream>>>(g, h->z64, h->r64, nullptr, S, 1, 0, nullptr, g, 0, 0, 0, h->s, kz);
         per = 6 * 8.0;
         break;
       }
-      case 3: {
+      case 6: {
         auto S = stencil<float, float>(g, h->lv[0].bxm, h->lv[0].bym, h->lv[0].bzm);
         k_rbgs<float, float><<<grid_pairs(g, kz), kBlock, 0, h->stream>>>(g, h->z32, h->r32, nullptr, S, 0, 0, nullptr, g, 0, 0, 0, h->s, kz);
         k_rbgs<float, float><<<grid_pairs(g, kz), kBlock, 0, h->stream>>>(g, h->z32, h->r32, nullptr, S, 1, 0, nullptr, g, 0, 0, 0, h->s, kz);
         per = 6 * 4.0;
+        break;
+      }
+      case 7: {
+        auto S = stencil<float, float>(g, h->lv[0].bxm, h->lv[0].bym, h->lv[0].bzm);
+        k_dir_matvec<float, float><<<grid_cells(g, kz), kBlock, 0, h->stream>>>(g, h->z32, h->d32, h->d32b, S, h->q32, h->red, h->s, kz);
+        per = 7 * 4.0;
         break;
       }
       case 4: {
@@ -1038,6 +1116,62 @@ smac_status smac_time_kernel(smac_handle* h, int kernel_id, int reps, float* ms,
   *ms = tot / reps;
   *bytes = per * (double)g.cells();
   return SMAC_OK;
+}
+
+
+}  // extern "C"
+
+namespace {
+template <class T, class C>
+smac_status sweep_selftest(smac_handle* h, int mode, T* x, T* xa, T* xb, T* rhs, const void* bx, const void* by,
+                           const void* bz, const T* xc, long long* mismatches) {
+  const Geom& g = h->lv[0].g;
+  const int kz = kz_for(g);
+  const Level& Lc = h->lv[1];
+  const int c0 = (mode == 2) ? 1 : 0;
+  // reference: two in-place half-sweeps on a copy of x
+  CK(cudaMemcpyAsync(base_of(g, xa), base_of(g, x), sizeof(T) * (size_t)g.alloc, cudaMemcpyDeviceToDevice, h->stream));
+  auto S = stencil<T, C>(g, bx, by, bz);
+  k_rbgs<T, C><<<grid_pairs(g, kz), kBlock, 0, h->stream>>>(g, xa, rhs, &h->s->rshift, S, c0, mode == 1,
+                                                            mode == 2 ? xc : (const T*)nullptr, Lc.g, Lc.cx, Lc.cy,
+                                                            Lc.cz, nullptr, kz);
+  k_rbgs<T, C><<<grid_pairs(g, kz), kBlock, 0, h->stream>>>(g, xa, rhs, &h->s->rshift, S, 1 - c0, 0, (const T*)nullptr,
+                                                            g, 0, 0, 0, nullptr, kz);
+  CKL();
+  // fused sweep, out of place
+  launch_sweep<T, C>(h, 0, mode, false, x, xb, rhs, &h->s->rshift, bx, by, bz, c0, xc);
+  CKL();
+  unsigned long long* cnt = nullptr;
+  CK(cudaMallocAsync((void**)&cnt, sizeof(unsigned long long), h->stream));
+  CK(cudaMemsetAsync(cnt, 0, sizeof(unsigned long long), h->stream));
+  k_count_mismatch<T><<<grid_planes(g.nx, g.ny, g.nz), kBlock, 0, h->stream>>>(g, xa, xb, cnt);
+  CKL();
+  unsigned long long hc = 0;
+  CK(cudaMemcpyAsync(&hc, cnt, sizeof(hc), cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaFreeAsync(cnt, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  *mismatches = (long long)hc;
+  return SMAC_OK;
+}
+}  // namespace
+
+extern "C" {
+
+smac_status smac_selftest_sweep(smac_handle* h, int precision, int mode, long long* mismatches) {
+  if (!h || !mismatches || mode < 0 || mode > 2 || precision < 0 || precision > 1) {
+    set_err("smac_selftest_sweep: bad argument");
+    return SMAC_BAD_ARG;
+  }
+  if (!h->have_coeffs || h->nlev < 2) { set_err("smac_selftest_sweep: needs coefficients and >= 2 grids"); return SMAC_BAD_ARG; }
+  // the V-cycle's shift must be finite; a state with shift 0 is used
+  Scalars st{};
+  *h->hs = st;
+  CK(cudaMemcpyAsync(h->s, h->hs, sizeof(Scalars), cudaMemcpyHostToDevice, h->stream));
+  if (precision == SMAC_PRECISION_FP64)
+    return sweep_selftest<double, double>(h, mode, h->z64, h->tmp64, h->z64b, h->r64, h->lv[0].bx64, h->lv[0].by64,
+                                          h->lv[0].bz64, h->lv[1].x64, mismatches);
+  return sweep_selftest<float, float>(h, mode, h->z32, h->q32, h->z32b, h->r32, h->lv[0].bxm, h->lv[0].bym,
+                                      h->lv[0].bzm, h->lv[1].x32, mismatches);
 }
 
 }  // extern "C"

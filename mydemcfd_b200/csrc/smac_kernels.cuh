@@ -115,19 +115,23 @@ __global__ void k_import_coeffs(Geom g, RefDims R, const double* __restrict__ fb
 // Cell bits: bit 0 C_INTERIOR, bit 1 fluid (C_INTERIOR with a non-zero
 // diagonal: the cells that carry unknowns).  Counts the fluid cells.
 
-__global__ void k_fluid_finalize(Geom g, const double* __restrict__ bx, const double* __restrict__ by,
-                                 const double* __restrict__ bz, uint8_t* fluid, RedBuf red, Scalars* s) {
+__global__ void __launch_bounds__(TNT) k_fluid_finalize(Geom g, const double* __restrict__ bx,
+                                                        const double* __restrict__ by, const double* __restrict__ bz,
+                                                        uint8_t* fluid, RedBuf red, Scalars* s, int kz) {
   const int i = blockIdx.x * TBX + threadIdx.x;
   const int j = blockIdx.y * TBY + threadIdx.y;
-  const int k = blockIdx.z;
+  const int k0 = blockIdx.z * kz;
   double v[1] = {0.0};
-  if (i < g.nx && j < g.ny && k < g.nz) {
-    const int c = g.idx(i, j, k);
-    const double d = bx[c] + bx[c + 1] + by[c] + by[c + g.px] + bz[c] + bz[c + g.ps];
-    const uint8_t in = fluid[c] & 1;
-    const uint8_t f = (in && d > 0.0) ? 1 : 0;
-    fluid[c] = (uint8_t)(in | (f << 1));
-    v[0] = f;
+  if (i < g.nx && j < g.ny) {
+    const int k1 = min(k0 + kz, g.nz);
+    for (int k = k0; k < k1; ++k) {
+      const int c = g.idx(i, j, k);
+      const double d = bx[c] + bx[c + 1] + by[c] + by[c + g.px] + bz[c] + bz[c + g.ps];
+      const uint8_t in = fluid[c] & 1;
+      const uint8_t f = (in && d > 0.0) ? 1 : 0;
+      fluid[c] = (uint8_t)(in | (f << 1));
+      v[0] += f;
+    }
   }
   const Op ops[1] = {Op::Sum};
   double out[1];
@@ -266,12 +270,16 @@ __global__ void k_export_cells(Geom g, RefDims R, const double* __restrict__ src
 // Set-up of a solve: b -= mean_fluid(b) (pure Neumann), r = b (FP64 or
 // FP32), x = 0, ||b||^2.  Two passes: sum, then project + norm.
 template <class TR>
-__global__ void k_setup_sum(Geom g, const double* __restrict__ b, RedBuf red, Scalars* s) {
+__global__ void __launch_bounds__(TNT) k_setup_sum(Geom g, const double* __restrict__ b, RedBuf red, Scalars* s,
+                                                   int kz) {
   const int i = blockIdx.x * TBX + threadIdx.x;
   const int j = blockIdx.y * TBY + threadIdx.y;
-  const int k = blockIdx.z;
+  const int k0 = blockIdx.z * kz;
   double v[1] = {0.0};
-  if (i < g.nx && j < g.ny && k < g.nz) v[0] = b[g.idx(i, j, k)];
+  if (i < g.nx && j < g.ny) {
+    const int k1 = min(k0 + kz, g.nz);
+    for (int k = k0; k < k1; ++k) v[0] += b[g.idx(i, j, k)];
+  }
   const Op ops[1] = {Op::Sum};
   double out[1];
   if (grid_reduce<1, TNT>(v, ops, red, 0, out))
@@ -279,21 +287,25 @@ __global__ void k_setup_sum(Geom g, const double* __restrict__ b, RedBuf red, Sc
 }
 
 template <class TR>
-__global__ void k_setup_project(Geom g, double* b, const uint8_t* __restrict__ fluid, TR* r, RedBuf red,
-                                Scalars* s, double tol) {
+__global__ void __launch_bounds__(TNT) k_setup_project(Geom g, double* b, const uint8_t* __restrict__ fluid, TR* r,
+                                                       RedBuf red, Scalars* s, double tol, int kz) {
   const int i = blockIdx.x * TBX + threadIdx.x;
   const int j = blockIdx.y * TBY + threadIdx.y;
-  const int k = blockIdx.z;
+  const int k0 = blockIdx.z * kz;
   double v[2] = {0.0, 0.0};
-  if (i < g.nx && j < g.ny && k < g.nz) {
-    const int c = g.idx(i, j, k);
-    double bv = b[c];
-    if (fluid[c] & 2) bv -= s->sum_tmp;
-    else bv = 0.0;
-    b[c] = bv;
-    r[c] = (TR)bv;
-    v[0] = bv * bv;
-    v[1] = fabs(bv);
+  const double m = s->sum_tmp;
+  if (i < g.nx && j < g.ny) {
+    const int k1 = min(k0 + kz, g.nz);
+    for (int k = k0; k < k1; ++k) {
+      const int c = g.idx(i, j, k);
+      double bv = b[c];
+      if (fluid[c] & 2) bv -= m;
+      else bv = 0.0;
+      b[c] = bv;
+      r[c] = (TR)bv;
+      v[0] += bv * bv;
+      v[1] = fmax(v[1], fabs(bv));
+    }
   }
   const Op ops[2] = {Op::Sum, Op::Max};
   double out[2];
@@ -586,15 +598,18 @@ __global__ void k_apply(Geom g, const double* __restrict__ x, Stencil<double, do
 }
 
 // Sum of x over fluid cells (the zero-mean projection of the solution).
-__global__ void k_sum_fluid(Geom g, const double* __restrict__ x, const uint8_t* __restrict__ fluid, RedBuf red,
-                            Scalars* s) {
+__global__ void __launch_bounds__(TNT) k_sum_fluid(Geom g, const double* __restrict__ x,
+                                                   const uint8_t* __restrict__ fluid, RedBuf red, Scalars* s, int kz) {
   const int i = blockIdx.x * TBX + threadIdx.x;
   const int j = blockIdx.y * TBY + threadIdx.y;
-  const int k = blockIdx.z;
+  const int k0 = blockIdx.z * kz;
   double v[1] = {0.0};
-  if (i < g.nx && j < g.ny && k < g.nz) {
-    const int c = g.idx(i, j, k);
-    if (fluid[c] & 2) v[0] = x[c];
+  if (i < g.nx && j < g.ny) {
+    const int k1 = min(k0 + kz, g.nz);
+    for (int k = k0; k < k1; ++k) {
+      const int c = g.idx(i, j, k);
+      if (fluid[c] & 2) v[0] += x[c];
+    }
   }
   const Op ops[1] = {Op::Sum};
   double out[1];
@@ -863,9 +878,11 @@ __global__ void k_correct(RefDims R, Geom g, double inv_dx, double inv_dy, doubl
                           const double* __restrict__ fby, const double* __restrict__ fbz,
                           const double* __restrict__ fsx, const double* __restrict__ fsy,
                           const double* __restrict__ fsz, double* vx, double* vy, double* vz, int write_all) {
-  const int ix = blockIdx.x * blockDim.x + threadIdx.x + 1;
-  const int iy = blockIdx.y * blockDim.y + threadIdx.y + 1;
-  const int iz = blockIdx.z + 1;
+  // every face index from 0 (the reference's threads start at 1; index-0
+  // faces are ghost faces that only write_all touches)
+  const int ix = blockIdx.x * blockDim.x + threadIdx.x;
+  const int iy = blockIdx.y * blockDim.y + threadIdx.y;
+  const int iz = blockIdx.z;
   const int Nx = R.Nx, Ny = R.Ny, Nz = R.Nz;
   // padded f_b of the face, used when f_inv_rho is not supplied
   auto padded = [&](const double* b, int i, int j, int k) -> double {
@@ -876,7 +893,7 @@ __global__ void k_correct(RefDims R, Geom g, double inv_dx, double inv_dy, doubl
   // always satisfy this; the bound keeps mislabelled ghost faces harmless)
   if (!(iy >= Ny + 2 || ix >= Nx + 3 || iz >= Nz + 2)) {
     const long long f = R.xf(ix, iy, iz);
-    if (fxt[f] == F_INTERIOR && ix <= Nx + 1) {
+    if (fxt[f] == F_INTERIOR && ix >= 1 && ix <= Nx + 1) {
       const double ir = firx ? firx[f] : padded(fbx, ix - 1, iy - 1, iz - 1);
       const double fs = fsx ? fsx[f] : 0.0;
       const double gp = DMUL(DADD(pd[R.cell(ix, iy, iz)], -pd[R.cell(ix - 1, iy, iz)]), inv_dx);
@@ -887,7 +904,7 @@ __global__ void k_correct(RefDims R, Geom g, double inv_dx, double inv_dy, doubl
   }
   if (!(iy >= Ny + 3 || ix >= Nx + 2 || iz >= Nz + 2)) {
     const long long f = R.yf(ix, iy, iz);
-    if (fyt[f] == F_INTERIOR && iy <= Ny + 1) {
+    if (fyt[f] == F_INTERIOR && iy >= 1 && iy <= Ny + 1) {
       const double ir = firy ? firy[f] : padded(fby, ix - 1, iy - 1, iz - 1);
       const double fs = fsy ? fsy[f] : 0.0;
       const double gp = DMUL(DADD(pd[R.cell(ix, iy, iz)], -pd[R.cell(ix, iy - 1, iz)]), inv_dy);
@@ -898,7 +915,7 @@ __global__ void k_correct(RefDims R, Geom g, double inv_dx, double inv_dy, doubl
   }
   if (!(iy >= Ny + 2 || ix >= Nx + 2 || iz >= Nz + 3)) {
     const long long f = R.zf(ix, iy, iz);
-    if (fzt[f] == F_INTERIOR && iz <= Nz + 1) {
+    if (fzt[f] == F_INTERIOR && iz >= 1 && iz <= Nz + 1) {
       const double ir = firz ? firz[f] : padded(fbz, ix - 1, iy - 1, iz - 1);
       const double fs = fsz ? fsz[f] : 0.0;
       const double gp = DMUL(DADD(pd[R.cell(ix, iy, iz)], -pd[R.cell(ix, iy, iz - 1)]), inv_dz);
@@ -907,7 +924,7 @@ __global__ void k_correct(RefDims R, Geom g, double inv_dx, double inv_dy, doubl
       vz[f] = vzs[f];
     }
   }
-  if (p && ix < Nx + 1 && iy < Ny + 1 && iz < Nz + 1) {
+  if (p && ix >= 1 && iy >= 1 && iz >= 1 && ix < Nx + 1 && iy < Ny + 1 && iz < Nz + 1) {
     if (ct[R.cell(ix, iy, iz)] == C_INTERIOR) p[R.cell(ix, iy, iz)] = DADD(p[R.cell(ix, iy, iz)], pd[R.cell(ix, iy, iz)]);
   }
 }

@@ -1,0 +1,256 @@
+// smac_rbgs.cuh -- fused red-black Gauss-Seidel sweep (both colours in one
+// pass over HBM), out of place: xout = S(xin).
+//
+// S updates colour c0 from xin, then colour c1 = 1 - c0 from the new c0
+// values (pre-smoothing c0 = red, post-smoothing c0 = black, which keeps the
+// V-cycle symmetric).  A CTA owns a TX x TY column of cells and marches z
+// through its chunk [z0, z1):
+//   - plane k+1 of xin (tile + 2-cell ring) is staged in shared memory,
+//   - colour c0 is computed on plane k over the tile + 1-cell ring (the ring
+//     values are recomputed here, so the c1 update at the tile edge never
+//     reads another CTA's output and the result is independent of block
+//     scheduling),
+//   - colour c1 is computed on plane k-1 and the finished row pairs of
+//     plane k-1 are written with one vector store per pair.
+// HBM traffic per cell: xin, rhs and three face coefficients read once and
+// xout written once (6 values), the algorithmic minimum of a full sweep;
+// the ring re-reads hit L2.  Arithmetic is the same expression, in the same
+// order, as the two half-sweep kernels (k_rbgs), so the result is bitwise
+// identical to them.
+//
+// MODE 0: plain sweep.  MODE 1: xin == 0 (first pre-smoothing sweep), not
+// read.  MODE 2: xin + coarse correction xc[parent] (prolongation fused into
+// the first post-smoothing sweep).
+// DOT: also accumulate sum((rhs - shift) * xout) and sum(xout) and finish
+// r.z / beta in the last block (the PCG dot product of the preconditioned
+// residual, fused into the last sweep of the fine grid).
+#pragma once
+
+#include "smac_kernels.cuh"
+
+namespace smac {
+
+constexpr int RB_TX = 64;
+constexpr int RB_NT = 256;
+// tile height: 16 rows for FP32, 8 for FP64 (static shared memory < 48 KB)
+template <class T> struct RbTile { static constexpr int TY = sizeof(T) == 8 ? 8 : 16; };
+
+template <class T> struct Vec2;
+template <> struct Vec2<double> { typedef double2 type; };
+template <> struct Vec2<float> { typedef float2 type; };
+
+template <class T, class C, int MODE, bool DOT>
+__global__ void __launch_bounds__(RB_NT) k_rbgs_sweep(Geom g, const T* __restrict__ xin, T* __restrict__ xout,
+                                                      const T* __restrict__ rhs, const double* shift, Stencil<T, C> S,
+                                                      int c0, const T* __restrict__ xc, Geom gc, int cx, int cy, int cz,
+                                                      Scalars* s, RedBuf red, int zchunk) {
+  typedef acc_t<T> A;
+  constexpr int TX = RB_TX, TY = RbTile<T>::TY;
+  constexpr int XW = TX + 8;  // staged xin columns i0-4 .. i0+TX+3
+  constexpr int XH = TY + 4;  // staged xin rows    j0-2 .. j0+TY+1
+  constexpr int RW = TX + 2;  // c0 region columns  i0-1 .. i0+TX
+  constexpr int RH = TY + 2;  // c0 region rows     j0-1 .. j0+TY
+  __shared__ A Xs[MODE == 1 ? 1 : 3][XH][XW];
+  __shared__ A Rs[3][RH][RW];
+  if (s && s->done) return;
+  const int tid = threadIdx.x;
+  const int i0 = blockIdx.x * TX, j0 = blockIdx.y * TY;
+  const int z0 = blockIdx.z * zchunk;
+  const int z1 = min(z0 + zchunk, g.nz);
+  const A sh = shift ? (A)(*shift) : (A)0;
+  auto slot = [](int k) { return (k + 3) % 3; };
+
+  auto load_plane = [&](int k) {
+    if constexpr (MODE != 1) {
+      const int sl = slot(k);
+      const bool kin = (k >= 0 && k < g.nz);
+      for (int p = tid; p < XH * XW; p += RB_NT) {
+        const int jj = p / XW, ii = p - jj * XW;
+        const int i = i0 - 4 + ii, j = j0 - 2 + jj;
+        A v = (A)0;
+        if (kin && i >= 0 && i < g.nx && j >= 0 && j < g.ny) {
+          v = (A)xin[g.idx(i, j, k)];
+          if constexpr (MODE == 2) v += (A)xc[gc.idx(cx ? i >> 1 : i, cy ? j >> 1 : j, cz ? k >> 1 : k)];
+        }
+        Xs[sl][jj][ii] = v;
+      }
+    }
+  };
+
+  // colour c0 on plane k over the tile and its one-cell ring
+  auto c0_plane = [&](int k) {
+    const int rs = slot(k);
+    const bool kin = (k >= 0 && k < g.nz);
+    for (int q = tid; q < RH * (RW / 2); q += RB_NT) {
+      const int jj = q / (RW / 2), m = q - jj * (RW / 2);
+      const int j = j0 - 1 + jj;
+      const int ibase = i0 - 1;
+      const int ii = ((c0 - j - k - ibase) & 1) + 2 * m;
+      const int i = ibase + ii;
+      A out = (A)0;
+      if (kin && i >= 0 && i < g.nx && j >= 0 && j < g.ny) {
+        const int c = g.idx(i, j, k);
+        A wxm, wxp, wym, wyp, wzm, wzp;
+        S.coeffs(c, g.px, g.ps, wxm, wxp, wym, wyp, wzm, wzp);
+        const A diag = (wxm + wxp) + (wym + wyp) + (wzm + wzp);
+        if (diag > (A)0) {
+          A bv = (A)rhs[c] - sh;
+          if constexpr (MODE != 1) {
+            const int xi = ii + 3, yj = jj + 1;  // position in Xs
+            const A n0 = Xs[rs][yj][xi - 1], n1 = Xs[rs][yj][xi + 1];
+            const A n2 = Xs[rs][yj - 1][xi], n3 = Xs[rs][yj + 1][xi];
+            const A n4 = Xs[slot(k - 1)][yj][xi], n5 = Xs[slot(k + 1)][yj][xi];
+            bv += (wxm * n0 + wxp * n1) + (wym * n2 + wyp * n3) + (wzm * n4 + wzp * n5);
+          }
+          out = bv / diag;
+        }
+      }
+      Rs[rs][jj][ii] = out;
+    }
+  };
+
+  double dv[2] = {0.0, 0.0};
+  // colour c1 on plane k over the tile; store both colours of plane k
+  auto c1_plane = [&](int k) {
+    const int rs = slot(k);
+    for (int q = tid; q < TY * (TX / 2); q += RB_NT) {
+      const int jj = q / (TX / 2), m = q - jj * (TX / 2);
+      const int j = j0 + jj, i = i0 + 2 * m;
+      if (j >= g.ny || i >= g.nx) continue;
+      A val[2];
+#pragma unroll
+      for (int e = 0; e < 2; ++e) {
+        const int ie = i + e;
+        const int ri = ie - (i0 - 1), rj = jj + 1;  // position in Rs
+        if (ie >= g.nx) { val[e] = (A)0; continue; }
+        if (((ie + j + k) & 1) == c0) {
+          val[e] = Rs[rs][rj][ri];
+          continue;
+        }
+        const int c = g.idx(ie, j, k);
+        A wxm, wxp, wym, wyp, wzm, wzp;
+        S.coeffs(c, g.px, g.ps, wxm, wxp, wym, wyp, wzm, wzp);
+        const A diag = (wxm + wxp) + (wym + wyp) + (wzm + wzp);
+        A out = (A)0;
+        if (diag > (A)0) {
+          A bv = (A)rhs[c] - sh;
+          const A n0 = Rs[rs][rj][ri - 1], n1 = Rs[rs][rj][ri + 1];
+          const A n2 = Rs[rs][rj - 1][ri], n3 = Rs[rs][rj + 1][ri];
+          const A n4 = Rs[slot(k - 1)][rj][ri], n5 = Rs[slot(k + 1)][rj][ri];
+          bv += (wxm * n0 + wxp * n1) + (wym * n2 + wyp * n3) + (wzm * n4 + wzp * n5);
+          out = bv / diag;
+        }
+        val[e] = out;
+      }
+      const int c = g.idx(i, j, k);
+      if (i + 1 < g.nx) {
+        typename Vec2<T>::type v2;
+        v2.x = (T)val[0];
+        v2.y = (T)val[1];
+        *reinterpret_cast<typename Vec2<T>::type*>(xout + c) = v2;
+      } else {
+        xout[c] = (T)val[0];
+      }
+      if constexpr (DOT) {
+#pragma unroll
+        for (int e = 0; e < 2; ++e) {
+          if (i + e < g.nx) {
+            const double zv = (double)(T)val[e];
+            dv[0] += (double)rhs[c + e] * zv;
+            dv[1] += zv;
+          }
+        }
+      }
+    }
+  };
+
+  load_plane(z0 - 2);
+  load_plane(z0 - 1);
+  load_plane(z0);
+  __syncthreads();
+  c0_plane(z0 - 1);
+  __syncthreads();  // c0_plane read the slot that load_plane(z0 + 1) refills
+  for (int k = z0; k <= z1; ++k) {
+    load_plane(k + 1);
+    __syncthreads();
+    c0_plane(k);
+    __syncthreads();
+    if (k - 1 >= z0) c1_plane(k - 1);
+  }
+
+  if constexpr (DOT) {
+    const Op ops[2] = {Op::Sum, Op::Sum};
+    double out[2];
+    if (grid_reduce<2, RB_NT>(dv, ops, red, 0, out)) {
+      if (tid == 0) {
+        const double rz_new = out[0] - s->rshift * out[1];
+        if (!isfinite(rz_new)) { s->status = 3; s->done = 1; }
+        else if (!(rz_new > 0.0)) { s->status = 2; s->done = 1; }
+        else {
+          s->beta = s->first ? 0.0 : rz_new / s->rz;
+          s->rz = rz_new;
+          s->first = 0;
+        }
+      }
+    }
+  }
+}
+
+// d = z + beta d fused with q = A d and p.Ap (the direction update of the
+// next iteration is folded into the matvec that needs it): reads z and the
+// old d at the stencil points, writes the new d and q.
+template <class T, class C>
+__global__ void __launch_bounds__(TNT) k_dir_matvec(Geom g, const T* __restrict__ z, T* __restrict__ d_old,
+                                                    T* __restrict__ d_new, Stencil<T, C> S, T* q, RedBuf red,
+                                                    Scalars* s, int kz) {
+  if (s->done) return;
+  typedef acc_t<T> A;
+  const int i = blockIdx.x * TBX + threadIdx.x;
+  const int j = blockIdx.y * TBY + threadIdx.y;
+  const int k0 = blockIdx.z * kz;
+  const A beta = (A)s->beta;
+  double v[1] = {0.0};
+  if (i < g.nx && j < g.ny) {
+    const int k1 = min(k0 + kz, g.nz);
+    int c = g.idx(i, j, k0);
+    auto D = [&](int cc) -> A { return (A)z[cc] + beta * (A)d_old[cc]; };
+    A xm = D(c - g.ps), xc = D(c);
+    for (int k = k0; k < k1; ++k, c += g.ps) {
+      const A xp = D(c + g.ps);
+      A wxm, wxp, wym, wyp, wzm, wzp;
+      S.coeffs(c, g.px, g.ps, wxm, wxp, wym, wyp, wzm, wzp);
+      const A diag = (wxm + wxp) + (wym + wyp) + (wzm + wzp);
+      const A off = (wxm * D(c - 1) + wxp * D(c + 1)) + (wym * D(c - g.px) + wyp * D(c + g.px)) + (wzm * xm + wzp * xp);
+      const A y = diag * xc - off;
+      d_new[c] = (T)xc;
+      q[c] = (T)y;
+      v[0] += (double)(T)xc * (double)(T)y;
+      xm = xc;
+      xc = xp;
+    }
+  }
+  const Op ops[1] = {Op::Sum};
+  double out[1];
+  if (grid_reduce<1, TNT>(v, ops, red, 0, out)) {
+    if (threadIdx.x == 0 && threadIdx.y == 0) {
+      const double pAp = out[0];
+      s->pAp = pAp;
+      if (!isfinite(pAp)) { s->status = 3; s->done = 1; }
+      else if (!(pAp > 0.0)) { s->status = 2; s->done = 1; }
+      else s->alpha = s->rz / pAp;
+    }
+  }
+}
+
+// Number of interior cells where a and b differ bitwise (self-test).
+template <class T>
+__global__ void k_count_mismatch(Geom g, const T* __restrict__ a, const T* __restrict__ b, unsigned long long* cnt) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int k = blockIdx.z;
+  if (i >= g.nx || j >= g.ny || k >= g.nz) return;
+  const int c = g.idx(i, j, k);
+  if (!(a[c] == b[c]) && !(a[c] != a[c] && b[c] != b[c])) atomicAdd(cnt, 1ull);
+}
+
+}  // namespace smac

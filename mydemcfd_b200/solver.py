@@ -207,6 +207,11 @@ class B200PressureSolver:
         nat.check(self._lib.smac_time_kernel(self._h, kernel_id, reps, ctypes.byref(ms), ctypes.byref(b)))
         return ms.value, b.value
 
+    def selftest_sweep(self, precision: int, mode: int) -> int:
+        n = ctypes.c_longlong()
+        nat.check(self._lib.smac_selftest_sweep(self._h, precision, mode, ctypes.byref(n)))
+        return n.value
+
     def num_levels(self) -> int:
         n = ctypes.c_int()
         nat.check(self._lib.smac_level_shape(self._h, 0, None, None, None, ctypes.byref(n)))

@@ -74,7 +74,7 @@ def main():
         pd = W.interior(r["p_delta"])
         rhs = W.interior(r["rhs"])
         arrays = {"meta": np.array(json.dumps(meta))}
-        if case.N[0] * case.N[1] * case.N[2] <= 48 ** 3:
+        if case.N[0] * case.N[1] * case.N[2] <= 32 ** 3:
             arrays["p_delta"] = pd
             arrays["rhs"] = rhs
         else:

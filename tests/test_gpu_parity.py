@@ -153,6 +153,16 @@ def test_apply_A_matches_reference_operator(oracle_lib):
     assert np.abs(W.interior(cpu(yd)) - W.interior(y_o)).max() <= 1e-13 * scale
 
 
+@pytest.mark.parametrize("precision", [nat.PRECISION_FP64, nat.PRECISION_MIXED])
+@pytest.mark.parametrize("n", [64, 40])
+def test_fused_sweep_equals_half_sweeps(precision, n):
+    """The fused one-pass red-black sweep is bitwise the two half-sweep launches."""
+    case = W.vof_case(n, seed=3, ratio=1000.0)
+    g, s, st = solve_gpu(case, tol=1e-6, precision=precision)
+    for mode in (0, 1, 2):
+        assert s.selftest_sweep(precision, mode) == 0, (mode, precision)
+
+
 # ---------------------------------------------------------------------------
 # solves
 def test_fp64_solve_matches_oracle_64(oracle_lib):
