@@ -204,19 +204,18 @@ def run_reference(args, rank):
 
 
 # ---------------------------------------------------------------------------
-def run_ours(args, rank, world, local_rank):
+def run_ours(args, ranks):
     import torch
-    import torch.distributed as dist
 
     from mydemcfd_b200 import _native as nat
+    from mydemcfd_b200 import replicas
     from mydemcfd_b200 import workloads as W
     from mydemcfd_b200.solver import B200PressureSolver, DeviceGrid, ibm_solid_fraction_device
 
-    torch.cuda.set_device(local_rank)
-    dev = torch.device("cuda", local_rank)
-    if world > 1:
-        import datetime
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
+    rank, world = ranks.rank, ranks.world
+    torch.cuda.set_device(ranks.local_rank)
+    dev = torch.device("cuda", ranks.local_rank)
+    replicas.init(ranks, "nccl", device=dev)
 
     case = build_case(args, solid_fraction=lambda N, h, o, s: ibm_solid_fraction_device(N, h, o, s).cpu().numpy())
     g = DeviceGrid.from_case(case, device=dev)
@@ -236,27 +235,16 @@ def run_ours(args, rank, world, local_rank):
     def step(s):
         return s.project(g.f_vx_star_, g.f_vy_star_, g.f_vz_star_, case.dt, pd, *out_v)
 
-    def barrier():
-        if world > 1:
-            dist.barrier()
-
-    def max_over_ranks(x):
-        if world > 1:
-            t = torch.tensor([x], dtype=torch.float64, device=dev)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            return float(t.item())
-        return x
-
     def timed(fn, k):
         ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        barrier()
+        replicas.barrier(ranks)
         torch.cuda.synchronize()
         ev0.record(stream)
         stats = [fn() for _ in range(k)]
         ev1.record(stream)
         torch.cuda.synchronize()
-        barrier()
-        return max_over_ranks(ev0.elapsed_time(ev1)), stats
+        replicas.barrier(ranks)
+        return replicas.max_over_ranks(ranks, ev0.elapsed_time(ev1), device=dev), stats
 
     for _ in range(args.warmup):
         step(s_mixed)
@@ -266,8 +254,8 @@ def run_ours(args, rank, world, local_rank):
     with ClockSampler(torch.cuda.current_device()) as clk:
         ms_mixed, st_mixed = timed(lambda: step(s_mixed), args.steps)
     ms_plain, st_plain = timed(lambda: step(s_plain), args.steps)
-    sps_mixed = world * args.steps / (ms_mixed / 1e3)
-    sps_plain = world * args.steps / (ms_plain / 1e3)
+    sps_mixed = replicas.throughput(ranks, args.steps, ms_mixed)
+    sps_plain = replicas.throughput(ranks, args.steps, ms_plain)
 
     # end to end through the C ABI with host buffers: pinned u* in, u and p_delta out
     e2e = None
@@ -288,7 +276,7 @@ def run_ours(args, rank, world, local_rank):
         for _ in range(max(1, args.warmup // 2)):
             e2e_step()
         ms_e2e, _ = timed(e2e_step, args.steps)
-        e2e = {"value": world * args.steps / (ms_e2e / 1e3), "unit": "solves/s",
+        e2e = {"value": replicas.throughput(ranks, args.steps, ms_e2e), "unit": "solves/s",
                "h2d_bytes_per_step": int(sum(t.numel() * 8 for t in host_in)),
                "d2h_bytes_per_step": int(sum(t.numel() * 8 for t in host_out))}
 
@@ -339,9 +327,7 @@ def run_ours(args, rank, world, local_rank):
         print(json.dumps(res), flush=True)
     s_mixed.close()
     s_plain.close()
-    if world > 1:
-        dist.barrier()
-        dist.destroy_process_group()
+    replicas.finish(ranks)
 
 
 def run_kernel_only(args):
@@ -366,13 +352,12 @@ def main():
     if args.kernel_only is not None:
         run_kernel_only(args)
         return
-    rank = int(os.environ.get("RANK", "0"))
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    from mydemcfd_b200 import replicas
+    ranks = replicas.from_env()
     if args.impl == "reference":
-        run_reference(args, rank)
+        run_reference(args, ranks.rank)
         return
-    run_ours(args, rank, world, local_rank)
+    run_ours(args, ranks)
 
 
 if __name__ == "__main__":

@@ -815,6 +815,51 @@ smac_status run_solve(smac_handle* h, const double** xout) {
     CK(cudaMemcpyAsync(h->hs, h->s, sizeof(Scalars), cudaMemcpyDeviceToHost, h->stream));
     CK(cudaStreamSynchronize(h->stream));
     if (h->hs->done) {
+      if (h->hs->status == 2 && restarts < 3) {
+        // Breakdown (p.Ap or r.z <= 0).  Near the rounding floor of a tight
+        // tolerance it means the Krylov space is exhausted, not failure:
+        // judge by the FP64 true residual and restart PCG from it.
+        const Scalars& hs0 = *h->hs;
+        const int it_now = hs0.iter;
+        auto S = stencil<double, double>(g, h->lv[0].bx64, h->lv[0].by64, h->lv[0].bz64);
+        if (mixed) {
+          // fold the FP32 increment into x64 and recompute r (k_reliable
+          // decides convergence on the true residual)
+          h->hs->done = 0;
+          h->hs->status = 0;
+          h->hs->do_reliable = 1;
+          CK(cudaMemcpyAsync(h->s, h->hs, sizeof(Scalars), cudaMemcpyHostToDevice, h->stream));
+          k_reliable<float><<<grid_cells(g, kz), kBlock, 0, h->stream>>>(g, h->x64a, h->x64b, h->e32, h->b64, S,
+                                                                         h->r32, h->red, h->s, kz);
+          CKL();
+        } else {
+          k_true_residual<<<grid_cells(g, kz), kBlock, 0, h->stream>>>(g, h->x64a, h->b64, S, h->r64, 1, h->red,
+                                                                        h->s, kz);
+          CKL();
+        }
+        account(h, g, 6 * 8, 1);
+        CK(cudaMemcpyAsync(h->hs, h->s, sizeof(Scalars), cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+        const Scalars& hs = *h->hs;
+        const bool ok = (o.stop_rule == 1) ? (hs.true_rmax < hs.tol_max) : (hs.true_rr <= hs.tol2bb);
+        if (ok) {
+          h->hs->status = 0;
+          h->hs->done = 1;
+          break;
+        }
+        if (it_now >= o.max_iter) {
+          h->hs->status = 1;
+          break;
+        }
+        ++restarts;
+        CK(cudaMemsetAsync(base_of(g, mixed ? (void*)h->d32 : (void*)h->d64), 0,
+                           (mixed ? sizeof(float) : sizeof(double)) * (size_t)g.alloc, h->stream));
+        h->hs->done = 0;
+        h->hs->first = 1;
+        h->hs->status = 0;
+        CK(cudaMemcpyAsync(h->s, h->hs, sizeof(Scalars), cudaMemcpyHostToDevice, h->stream));
+        continue;
+      }
       if (!mixed && h->hs->status == 0) {
         // verify the recursive residual with the FP64 true residual
         auto S = stencil<double, double>(g, h->lv[0].bx64, h->lv[0].by64, h->lv[0].bz64);

@@ -46,22 +46,67 @@ struct RefDims {
 };
 
 // ------------------------------------------------------------------------
-// Stencil pieces.
+// Stencil pieces.  Every product and sum is an explicit round-to-nearest
+// intrinsic, so the compiler contracts nothing on its own: every kernel that
+// evaluates the same cell update rounds identically (the fused sweep equals
+// the half-sweep kernels bit for bit) whatever the code around it.
+template <class A> struct Ar;
+template <> struct Ar<double> {
+  static __device__ __forceinline__ double mul(double a, double b) { return __dmul_rn(a, b); }
+  static __device__ __forceinline__ double add(double a, double b) { return __dadd_rn(a, b); }
+  static __device__ __forceinline__ double fma(double a, double b, double c) { return __fma_rn(a, b, c); }
+  static __device__ __forceinline__ double div(double a, double b) { return __ddiv_rn(a, b); }
+};
+template <> struct Ar<float> {
+  static __device__ __forceinline__ float mul(float a, float b) { return __fmul_rn(a, b); }
+  static __device__ __forceinline__ float add(float a, float b) { return __fadd_rn(a, b); }
+  static __device__ __forceinline__ float fma(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+  static __device__ __forceinline__ float div(float a, float b) { return __fdiv_rn(a, b); }
+};
+
 template <class T, class C>
 struct Stencil {
   typedef acc_t<T> A;
+  typedef Ar<A> R;
   const C* __restrict__ bx;
   const C* __restrict__ by;
   const C* __restrict__ bz;
   A ihx2, ihy2, ihz2;
+  // face weights of cell c: x-, x+, y-, y+, z-, z+
   __device__ __forceinline__ void coeffs(int c, int px, int ps, A& wxm, A& wxp, A& wym, A& wyp, A& wzm,
                                          A& wzp) const {
-    wxm = (A)CoefLoad<C>::get(bx, c) * ihx2;
-    wxp = (A)CoefLoad<C>::get(bx, c + 1) * ihx2;
-    wym = (A)CoefLoad<C>::get(by, c) * ihy2;
-    wyp = (A)CoefLoad<C>::get(by, c + px) * ihy2;
-    wzm = (A)CoefLoad<C>::get(bz, c) * ihz2;
-    wzp = (A)CoefLoad<C>::get(bz, c + ps) * ihz2;
+    wxm = R::mul((A)CoefLoad<C>::get(bx, c), ihx2);
+    wxp = R::mul((A)CoefLoad<C>::get(bx, c + 1), ihx2);
+    wym = R::mul((A)CoefLoad<C>::get(by, c), ihy2);
+    wyp = R::mul((A)CoefLoad<C>::get(by, c + px), ihy2);
+    wzm = R::mul((A)CoefLoad<C>::get(bz, c), ihz2);
+    wzp = R::mul((A)CoefLoad<C>::get(bz, c + ps), ihz2);
+  }
+  static __device__ __forceinline__ A diag(A wxm, A wxp, A wym, A wyp, A wzm, A wzp) {
+    return R::add(R::add(R::add(wxm, wxp), R::add(wym, wyp)), R::add(wzm, wzp));
+  }
+  // bv + sum w * n (neighbours in the order x-, x+, y-, y+, z-, z+)
+  static __device__ __forceinline__ A offsum(A bv, A wxm, A wxp, A wym, A wyp, A wzm, A wzp, A n0, A n1, A n2,
+                                             A n3, A n4, A n5) {
+    A acc = R::fma(wxm, n0, bv);
+    acc = R::fma(wxp, n1, acc);
+    acc = R::fma(wym, n2, acc);
+    acc = R::fma(wyp, n3, acc);
+    acc = R::fma(wzm, n4, acc);
+    return R::fma(wzp, n5, acc);
+  }
+  // (A x)_c = diag x_c - sum w * n
+  static __device__ __forceinline__ A apply(A xc, A wxm, A wxp, A wym, A wyp, A wzm, A wzp, A n0, A n1, A n2,
+                                            A n3, A n4, A n5) {
+    const A d = diag(wxm, wxp, wym, wyp, wzm, wzp);
+    return offsum(R::mul(d, xc), -wxm, -wxp, -wym, -wyp, -wzm, -wzp, n0, n1, n2, n3, n4, n5);
+  }
+  // Gauss-Seidel value (bv + sum w * n) / diag, 0 where the diagonal is 0
+  static __device__ __forceinline__ A gs(A bv, A wxm, A wxp, A wym, A wyp, A wzm, A wzp, A n0, A n1, A n2, A n3,
+                                         A n4, A n5) {
+    const A d = diag(wxm, wxp, wym, wyp, wzm, wzp);
+    if (!(d > (A)0)) return (A)0;
+    return R::div(offsum(bv, wxm, wxp, wym, wyp, wzm, wzp, n0, n1, n2, n3, n4, n5), d);
   }
 };
 
@@ -353,10 +398,8 @@ __global__ void __launch_bounds__(TNT) k_matvec_pap(Geom g, const T* __restrict_
       const A xp = (A)d[c + g.ps];
       A wxm, wxp, wym, wyp, wzm, wzp;
       S.coeffs(c, g.px, g.ps, wxm, wxp, wym, wyp, wzm, wzp);
-      const A diag = (wxm + wxp) + (wym + wyp) + (wzm + wzp);
-      const A off = (wxm * (A)d[c - 1] + wxp * (A)d[c + 1]) + (wym * (A)d[c - g.px] + wyp * (A)d[c + g.px]) +
-                    (wzm * xm + wzp * xp);
-      const A y = diag * xc - off;
+      const A y = Stencil<T, C>::apply(xc, wxm, wxp, wym, wyp, wzm, wzp, (A)d[c - 1], (A)d[c + 1], (A)d[c - g.px],
+                                       (A)d[c + g.px], xm, xp);
       q[c] = (T)y;
       v[0] += (double)xc * (double)y;
       xm = xc;
@@ -452,10 +495,8 @@ __global__ void __launch_bounds__(TNT) k_reliable(Geom g, double* x64a, double* 
       const double xp = X(c + g.ps);
       double wxm, wxp, wym, wyp, wzm, wzp;
       S.coeffs(c, g.px, g.ps, wxm, wxp, wym, wyp, wzm, wzp);
-      const double diag = (wxm + wxp) + (wym + wyp) + (wzm + wzp);
-      const double off = (wxm * X(c - 1) + wxp * X(c + 1)) + (wym * X(c - g.px) + wyp * X(c + g.px)) +
-                         (wzm * xm + wzp * xp);
-      const double rv = b[c] - (diag * xc - off);
+      const double rv = b[c] - Stencil<double, double>::apply(xc, wxm, wxp, wym, wyp, wzm, wzp, X(c - 1), X(c + 1),
+                                                              X(c - g.px), X(c + g.px), xm, xp);
       xd[c] = xc;
       r[c] = (T)rv;
       v[0] += rv;
@@ -558,10 +599,8 @@ __global__ void __launch_bounds__(TNT) k_true_residual(Geom g, const double* __r
       const double xp = x[c + g.ps];
       double wxm, wxp, wym, wyp, wzm, wzp;
       S.coeffs(c, g.px, g.ps, wxm, wxp, wym, wyp, wzm, wzp);
-      const double diag = (wxm + wxp) + (wym + wyp) + (wzm + wzp);
-      const double off = (wxm * x[c - 1] + wxp * x[c + 1]) + (wym * x[c - g.px] + wyp * x[c + g.px]) +
-                         (wzm * xm + wzp * xp);
-      const double rv = b[c] - (diag * xc - off);
+      const double rv = b[c] - Stencil<double, double>::apply(xc, wxm, wxp, wym, wyp, wzm, wzp, x[c - 1], x[c + 1],
+                                                              x[c - g.px], x[c + g.px], xm, xp);
       if (write_r) r[c] = rv;
       v[0] += rv;
       v[1] += rv * rv;
@@ -591,10 +630,8 @@ __global__ void k_apply(Geom g, const double* __restrict__ x, Stencil<double, do
   const int c = g.idx(i, j, k);
   double wxm, wxp, wym, wyp, wzm, wzp;
   S.coeffs(c, g.px, g.ps, wxm, wxp, wym, wyp, wzm, wzp);
-  const double diag = (wxm + wxp) + (wym + wyp) + (wzm + wzp);
-  const double off = (wxm * x[c - 1] + wxp * x[c + 1]) + (wym * x[c - g.px] + wyp * x[c + g.px]) +
-                     (wzm * x[c - g.ps] + wzp * x[c + g.ps]);
-  y[c] = diag * x[c] - off;
+  y[c] = Stencil<double, double>::apply(x[c], wxm, wxp, wym, wyp, wzm, wzp, x[c - 1], x[c + 1], x[c - g.px],
+                                        x[c + g.px], x[c - g.ps], x[c + g.ps]);
 }
 
 // Sum of x over fluid cells (the zero-mean projection of the solution).
@@ -647,26 +684,22 @@ __global__ void __launch_bounds__(TNT) k_rbgs(Geom g, T* x, const T* __restrict_
     const int c = g.idx(i, j, k);
     A wxm, wxp, wym, wyp, wzm, wzp;
     S.coeffs(c, g.px, g.ps, wxm, wxp, wym, wyp, wzm, wzp);
-    const A diag = (wxm + wxp) + (wym + wyp) + (wzm + wzp);
-    A out = (A)0;
-    if (diag > (A)0) {
-      A bv = (A)rhs[c] - sh;
-      if (!zero_init) {
-        A n[6] = {(A)x[c - 1], (A)x[c + 1], (A)x[c - g.px], (A)x[c + g.px], (A)x[c - g.ps], (A)x[c + g.ps]};
-        if (xc) {
-          const int ci[6][3] = {{i - 1, j, k}, {i + 1, j, k}, {i, j - 1, k}, {i, j + 1, k}, {i, j, k - 1}, {i, j, k + 1}};
+    const A bv = Ar<A>::add((A)rhs[c], -sh);
+    A n[6] = {(A)0, (A)0, (A)0, (A)0, (A)0, (A)0};
+    if (!zero_init) {
+      n[0] = (A)x[c - 1]; n[1] = (A)x[c + 1]; n[2] = (A)x[c - g.px]; n[3] = (A)x[c + g.px];
+      n[4] = (A)x[c - g.ps]; n[5] = (A)x[c + g.ps];
+      if (xc) {
+        const int ci[6][3] = {{i - 1, j, k}, {i + 1, j, k}, {i, j - 1, k}, {i, j + 1, k}, {i, j, k - 1}, {i, j, k + 1}};
 #pragma unroll
-          for (int q = 0; q < 6; ++q) {
-            const int a = ci[q][0], b = ci[q][1], d = ci[q][2];
-            if (a >= 0 && b >= 0 && d >= 0 && a < g.nx && b < g.ny && d < g.nz)
-              n[q] += (A)xc[gc.idx(cx ? a >> 1 : a, cy ? b >> 1 : b, cz ? d >> 1 : d)];
-          }
+        for (int q = 0; q < 6; ++q) {
+          const int a = ci[q][0], b = ci[q][1], d = ci[q][2];
+          if (a >= 0 && b >= 0 && d >= 0 && a < g.nx && b < g.ny && d < g.nz)
+            n[q] = Ar<A>::add(n[q], (A)xc[gc.idx(cx ? a >> 1 : a, cy ? b >> 1 : b, cz ? d >> 1 : d)]);
         }
-        bv += (wxm * n[0] + wxp * n[1]) + (wym * n[2] + wyp * n[3]) + (wzm * n[4] + wzp * n[5]);
       }
-      out = bv / diag;
     }
-    x[c] = (T)out;
+    x[c] = (T)Stencil<T, C>::gs(bv, wxm, wxp, wym, wyp, wzm, wzp, n[0], n[1], n[2], n[3], n[4], n[5]);
   }
 }
 
@@ -693,14 +726,14 @@ __global__ void __launch_bounds__(TNT) k_resid_restrict(Geom g, const T* __restr
         const int c = g.idx(i, j, k);
         A wxm, wxp, wym, wyp, wzm, wzp;
         S.coeffs(c, g.px, g.ps, wxm, wxp, wym, wyp, wzm, wzp);
-        const A diag = (wxm + wxp) + (wym + wyp) + (wzm + wzp);
-        const A off = (wxm * (A)x[c - 1] + wxp * (A)x[c + 1]) + (wym * (A)x[c - g.px] + wyp * (A)x[c + g.px]) +
-                      (wzm * (A)x[c - g.ps] + wzp * (A)x[c + g.ps]);
+        const A diag = Stencil<T, C>::diag(wxm, wxp, wym, wyp, wzm, wzp);
         A bv = (A)rhs[c];
-        if (diag > (A)0) bv -= sh;
-        acc += bv - (diag * (A)x[c] - off);
+        if (diag > (A)0) bv = Ar<A>::add(bv, -sh);
+        const A ax = Stencil<T, C>::apply((A)x[c], wxm, wxp, wym, wyp, wzm, wzp, (A)x[c - 1], (A)x[c + 1],
+                                          (A)x[c - g.px], (A)x[c + g.px], (A)x[c - g.ps], (A)x[c + g.ps]);
+        acc = Ar<A>::add(acc, Ar<A>::add(bv, -ax));
       }
-  rhs_c[gc.idx(I, J, K)] = (T)(acc / (A)(rx * ry * rz));
+  rhs_c[gc.idx(I, J, K)] = (T)Ar<A>::div(acc, (A)(rx * ry * rz));
 }
 
 // ------------------------------------------------------------------------
@@ -744,27 +777,23 @@ __device__ __forceinline__ void cta_half_sweep(const CoarseLevel& L, int colour,
     const int c = g.idx(i, j, k);
     A wxm, wxp, wym, wyp, wzm, wzp;
     S.coeffs(c, g.px, g.ps, wxm, wxp, wym, wyp, wzm, wzp);
-    const A diag = (wxm + wxp) + (wym + wyp) + (wzm + wzp);
-    A out = (A)0;
-    if (diag > (A)0) {
-      A bv = (A)rhs[c] - sh;
-      if (!zero_init) {
-        A n[6] = {(A)x[c - 1], (A)x[c + 1], (A)x[c - g.px], (A)x[c + g.px], (A)x[c - g.ps], (A)x[c + g.ps]};
-        if (xc) {
-          const Geom& gc = Lc->g;
-          const int ci[6][3] = {{i - 1, j, k}, {i + 1, j, k}, {i, j - 1, k}, {i, j + 1, k}, {i, j, k - 1}, {i, j, k + 1}};
+    const A bv = Ar<A>::add((A)rhs[c], -sh);
+    A n[6] = {(A)0, (A)0, (A)0, (A)0, (A)0, (A)0};
+    if (!zero_init) {
+      n[0] = (A)x[c - 1]; n[1] = (A)x[c + 1]; n[2] = (A)x[c - g.px]; n[3] = (A)x[c + g.px];
+      n[4] = (A)x[c - g.ps]; n[5] = (A)x[c + g.ps];
+      if (xc) {
+        const Geom& gc = Lc->g;
+        const int ci[6][3] = {{i - 1, j, k}, {i + 1, j, k}, {i, j - 1, k}, {i, j + 1, k}, {i, j, k - 1}, {i, j, k + 1}};
 #pragma unroll
-          for (int q = 0; q < 6; ++q) {
-            const int a = ci[q][0], b = ci[q][1], d = ci[q][2];
-            if (a >= 0 && b >= 0 && d >= 0 && a < g.nx && b < g.ny && d < g.nz)
-              n[q] += (A)xc[gc.idx(Lc->cx ? a >> 1 : a, Lc->cy ? b >> 1 : b, Lc->cz ? d >> 1 : d)];
-          }
+        for (int q = 0; q < 6; ++q) {
+          const int a = ci[q][0], b = ci[q][1], d = ci[q][2];
+          if (a >= 0 && b >= 0 && d >= 0 && a < g.nx && b < g.ny && d < g.nz)
+            n[q] = Ar<A>::add(n[q], (A)xc[gc.idx(Lc->cx ? a >> 1 : a, Lc->cy ? b >> 1 : b, Lc->cz ? d >> 1 : d)]);
         }
-        bv += (wxm * n[0] + wxp * n[1]) + (wym * n[2] + wyp * n[3]) + (wzm * n[4] + wzp * n[5]);
       }
-      out = bv / diag;
     }
-    x[c] = (T)out;
+    x[c] = (T)Stencil<T, C>::gs(bv, wxm, wxp, wym, wyp, wzm, wzp, n[0], n[1], n[2], n[3], n[4], n[5]);
   }
 }
 
@@ -790,14 +819,14 @@ __device__ __forceinline__ void cta_resid_restrict(const CoarseLevel& L, const C
           const int c = g.idx(i, j, k);
           A wxm, wxp, wym, wyp, wzm, wzp;
           S.coeffs(c, g.px, g.ps, wxm, wxp, wym, wyp, wzm, wzp);
-          const A diag = (wxm + wxp) + (wym + wyp) + (wzm + wzp);
-          const A off = (wxm * (A)x[c - 1] + wxp * (A)x[c + 1]) + (wym * (A)x[c - g.px] + wyp * (A)x[c + g.px]) +
-                        (wzm * (A)x[c - g.ps] + wzp * (A)x[c + g.ps]);
+          const A diag = Stencil<T, C>::diag(wxm, wxp, wym, wyp, wzm, wzp);
           A bv = (A)rhs[c];
-          if (diag > (A)0) bv -= sh;
-          acc += bv - (diag * (A)x[c] - off);
+          if (diag > (A)0) bv = Ar<A>::add(bv, -sh);
+          const A ax = Stencil<T, C>::apply((A)x[c], wxm, wxp, wym, wyp, wzm, wzp, (A)x[c - 1], (A)x[c + 1],
+                                            (A)x[c - g.px], (A)x[c + g.px], (A)x[c - g.ps], (A)x[c + g.ps]);
+          acc = Ar<A>::add(acc, Ar<A>::add(bv, -ax));
         }
-    rhs_c[gc.idx(I, J, K)] = (T)(acc / (A)(rx * ry * rz));
+    rhs_c[gc.idx(I, J, K)] = (T)Ar<A>::div(acc, (A)(rx * ry * rz));
   }
 }
 
@@ -812,7 +841,8 @@ __device__ __forceinline__ void cta_prolong(const CoarseLevel& L, const CoarseLe
   const int total = g.nx * g.ny * g.nz;
   for (int t = threadIdx.x; t < total; t += blockDim.x) {
     const int i = t % g.nx, j = (t / g.nx) % g.ny, k = t / (g.nx * g.ny);
-    x[g.idx(i, j, k)] += xc[gc.idx(Lc.cx ? i >> 1 : i, Lc.cy ? j >> 1 : j, Lc.cz ? k >> 1 : k)];
+    const int c = g.idx(i, j, k);
+    x[c] = x[c] + xc[gc.idx(Lc.cx ? i >> 1 : i, Lc.cy ? j >> 1 : j, Lc.cz ? k >> 1 : k)];
   }
 }
 
@@ -1027,8 +1057,8 @@ __global__ void __launch_bounds__(TNT) k_jacobi_precond(Geom g, const T* __restr
   for (int k = k0; k < k1; ++k, c += g.ps) {
     A wxm, wxp, wym, wyp, wzm, wzp;
     S.coeffs(c, g.px, g.ps, wxm, wxp, wym, wyp, wzm, wzp);
-    const A diag = (wxm + wxp) + (wym + wyp) + (wzm + wzp);
-    z[c] = (T)((diag > (A)0) ? ((A)r[c] - sh) / diag : (A)0);
+    const A diag = Stencil<T, C>::diag(wxm, wxp, wym, wyp, wzm, wzp);
+    z[c] = (T)((diag > (A)0) ? Ar<A>::div(Ar<A>::add((A)r[c], -sh), diag) : (A)0);
   }
 }
 

@@ -70,7 +70,8 @@ __global__ void __launch_bounds__(RB_NT) k_rbgs_sweep(Geom g, const T* __restric
         A v = (A)0;
         if (kin && i >= 0 && i < g.nx && j >= 0 && j < g.ny) {
           v = (A)xin[g.idx(i, j, k)];
-          if constexpr (MODE == 2) v += (A)xc[gc.idx(cx ? i >> 1 : i, cy ? j >> 1 : j, cz ? k >> 1 : k)];
+          if constexpr (MODE == 2)
+            v = Ar<A>::add(v, (A)xc[gc.idx(cx ? i >> 1 : i, cy ? j >> 1 : j, cz ? k >> 1 : k)]);
         }
         Xs[sl][jj][ii] = v;
       }
@@ -92,17 +93,14 @@ __global__ void __launch_bounds__(RB_NT) k_rbgs_sweep(Geom g, const T* __restric
         const int c = g.idx(i, j, k);
         A wxm, wxp, wym, wyp, wzm, wzp;
         S.coeffs(c, g.px, g.ps, wxm, wxp, wym, wyp, wzm, wzp);
-        const A diag = (wxm + wxp) + (wym + wyp) + (wzm + wzp);
-        if (diag > (A)0) {
-          A bv = (A)rhs[c] - sh;
-          if constexpr (MODE != 1) {
-            const int xi = ii + 3, yj = jj + 1;  // position in Xs
-            const A n0 = Xs[rs][yj][xi - 1], n1 = Xs[rs][yj][xi + 1];
-            const A n2 = Xs[rs][yj - 1][xi], n3 = Xs[rs][yj + 1][xi];
-            const A n4 = Xs[slot(k - 1)][yj][xi], n5 = Xs[slot(k + 1)][yj][xi];
-            bv += (wxm * n0 + wxp * n1) + (wym * n2 + wyp * n3) + (wzm * n4 + wzp * n5);
-          }
-          out = bv / diag;
+        const A bv = Ar<A>::add((A)rhs[c], -sh);
+        if constexpr (MODE != 1) {
+          const int xi = ii + 3, yj = jj + 1;  // position in Xs
+          out = Stencil<T, C>::gs(bv, wxm, wxp, wym, wyp, wzm, wzp, Xs[rs][yj][xi - 1], Xs[rs][yj][xi + 1],
+                                  Xs[rs][yj - 1][xi], Xs[rs][yj + 1][xi], Xs[slot(k - 1)][yj][xi],
+                                  Xs[slot(k + 1)][yj][xi]);
+        } else {
+          out = Stencil<T, C>::gs(bv, wxm, wxp, wym, wyp, wzm, wzp, (A)0, (A)0, (A)0, (A)0, (A)0, (A)0);
         }
       }
       Rs[rs][jj][ii] = out;
@@ -130,17 +128,10 @@ __global__ void __launch_bounds__(RB_NT) k_rbgs_sweep(Geom g, const T* __restric
         const int c = g.idx(ie, j, k);
         A wxm, wxp, wym, wyp, wzm, wzp;
         S.coeffs(c, g.px, g.ps, wxm, wxp, wym, wyp, wzm, wzp);
-        const A diag = (wxm + wxp) + (wym + wyp) + (wzm + wzp);
-        A out = (A)0;
-        if (diag > (A)0) {
-          A bv = (A)rhs[c] - sh;
-          const A n0 = Rs[rs][rj][ri - 1], n1 = Rs[rs][rj][ri + 1];
-          const A n2 = Rs[rs][rj - 1][ri], n3 = Rs[rs][rj + 1][ri];
-          const A n4 = Rs[slot(k - 1)][rj][ri], n5 = Rs[slot(k + 1)][rj][ri];
-          bv += (wxm * n0 + wxp * n1) + (wym * n2 + wyp * n3) + (wzm * n4 + wzp * n5);
-          out = bv / diag;
-        }
-        val[e] = out;
+        const A bv = Ar<A>::add((A)rhs[c], -sh);
+        val[e] = Stencil<T, C>::gs(bv, wxm, wxp, wym, wyp, wzm, wzp, Rs[rs][rj][ri - 1], Rs[rs][rj][ri + 1],
+                                   Rs[rs][rj - 1][ri], Rs[rs][rj + 1][ri], Rs[slot(k - 1)][rj][ri],
+                                   Rs[slot(k + 1)][rj][ri]);
       }
       const int c = g.idx(i, j, k);
       if (i + 1 < g.nx) {
@@ -213,15 +204,14 @@ __global__ void __launch_bounds__(TNT) k_dir_matvec(Geom g, const T* __restrict_
   if (i < g.nx && j < g.ny) {
     const int k1 = min(k0 + kz, g.nz);
     int c = g.idx(i, j, k0);
-    auto D = [&](int cc) -> A { return (A)z[cc] + beta * (A)d_old[cc]; };
+    auto D = [&](int cc) -> A { return Ar<A>::fma(beta, (A)d_old[cc], (A)z[cc]); };
     A xm = D(c - g.ps), xc = D(c);
     for (int k = k0; k < k1; ++k, c += g.ps) {
       const A xp = D(c + g.ps);
       A wxm, wxp, wym, wyp, wzm, wzp;
       S.coeffs(c, g.px, g.ps, wxm, wxp, wym, wyp, wzm, wzp);
-      const A diag = (wxm + wxp) + (wym + wyp) + (wzm + wzp);
-      const A off = (wxm * D(c - 1) + wxp * D(c + 1)) + (wym * D(c - g.px) + wyp * D(c + g.px)) + (wzm * xm + wzp * xp);
-      const A y = diag * xc - off;
+      const A y = Stencil<T, C>::apply(xc, wxm, wxp, wym, wyp, wzm, wzp, D(c - 1), D(c + 1), D(c - g.px), D(c + g.px),
+                                       xm, xp);
       d_new[c] = (T)xc;
       q[c] = (T)y;
       v[0] += (double)(T)xc * (double)(T)y;

@@ -355,7 +355,7 @@ def test_adjoint_dot_product():
 def test_autograd_matches_finite_differences():
     from mydemcfd_b200.autograd import StepOperator, unrolled
     case = W.vof_case(24, seed=5, ratio=100.0)
-    s = make_solver(case, tol=1e-13)
+    s = make_solver(case, tol=1e-12)
     ct, fxt, fyt, fzt = (torch.from_numpy(a).cuda() for a in (case.ct, case.fxt, case.fyt, case.fzt))
     ops = []
     for k in range(3):
