@@ -221,6 +221,27 @@ smac_status smac_apply_A(smac_handle* h, const double* x, double* y);
 smac_status smac_time_kernel(smac_handle* h, int kernel_id, int reps, float* ms_per_launch,
                              double* alg_bytes_per_launch);
 
+/* y = A x (interior cells, reference layout) and *xAx = x.Ax (one device
+ * double) with the FP64 operator of smac_set_coefficients, built directly
+ * from the reference-layout f_b and types, WITHOUT a handle and without
+ * allocating any device memory.  No counterpart in the reference.
+ * It is for callers that cannot allocate: a step loop being recorded into a
+ * CUDA graph (cudaMalloc is not allowed while the stream captures) or a host
+ * code whose pool allocator already owns the device memory.  Its scratch (the
+ * reduction's per-block partials and arrival counter) is a static device array
+ * of 64 KB that every GPU loading this library keeps until the process exits;
+ * grids need ceil(nx/32)*ceil(ny/4) <= 8192 (x-y planes up to 1024 x 1024),
+ * larger ones are refused with SMAC_BAD_SHAPE.  The first call on a device
+ * looks up the array's device address (cudaGetSymbolAddress), so make that
+ * first call before any stream capture.  All calls share the one array:
+ * calls that overlap on the GPU (other streams, other threads) race; order
+ * them on one stream.  All pointers are device pointers; x's ghost entries are
+ * not read. */
+smac_status smac_apply_A_dot_noalloc(const smac_grid_desc* desc, const double* fbx, const double* fby,
+                                     const double* fbz, const uint8_t* celltype, const uint8_t* fxt,
+                                     const uint8_t* fyt, const uint8_t* fzt, const double* x, double* y,
+                                     double* xAx, void* cuda_stream);
+
 /* Self-test of the fused red-black sweep: runs one fused out-of-place sweep
  * (mode 0 plain, 1 from zero, 2 with the coarse-grid correction of grid 1
  * added to the input) and the same sweep as two in-place half-sweep launches

@@ -63,7 +63,7 @@ EXPORTS = [
     "smac_level_shape", "smac_set_coefficients", "smac_box_types", "smac_assemble_vof",
     "smac_ibm_solid_fraction_spheres", "smac_ibm_set_solid_cells", "smac_divergence", "smac_solve",
     "smac_set_rhs", "smac_correct", "smac_project", "smac_project_adjoint", "smac_apply_A", "smac_time_kernel",
-    "smac_selftest_sweep",
+    "smac_selftest_sweep", "smac_apply_A_dot_noalloc",
 ]
 
 
@@ -98,6 +98,7 @@ def load(path: str = LIB_PATH):
         "smac_apply_A": [vp, dp, dp],
         "smac_time_kernel": [vp, ip, ip, ctypes.POINTER(ctypes.c_float), ctypes.POINTER(d)],
         "smac_selftest_sweep": [vp, ip, ip, ctypes.POINTER(ctypes.c_longlong)],
+        "smac_apply_A_dot_noalloc": [ctypes.POINTER(GridDesc), dp, dp, dp, u8p, u8p, u8p, u8p, dp, dp, dp, vp],
     }
     for name, args in sig.items():
         fn = getattr(lib, name)

@@ -11,10 +11,11 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 LIB = os.path.join(HERE, "libsmac_b200.so")
-SOURCES = [os.path.join(HERE, "csrc", "smac_api.cu")]
+SOURCES = [os.path.join(HERE, "csrc", "smac_api.cu"), os.path.join(HERE, "csrc", "smac_noalloc.cu")]
 DEPS = SOURCES + [
     os.path.join(HERE, "csrc", "smac_common.cuh"),
     os.path.join(HERE, "csrc", "smac_kernels.cuh"),
+    os.path.join(HERE, "csrc", "smac_rbgs.cuh"),
     os.path.join(ROOT, "include", "smac_b200.h"),
 ]
 NVCC_FLAGS = [

@@ -25,6 +25,20 @@ void set_err(const char* fmt, ...) {
   va_end(ap);
 }
 
+}  // namespace
+
+namespace smac {
+// error text for smac_last_error_string() from the other translation units
+void set_error_text(const char* fmt, ...) {
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(g_err, sizeof(g_err), fmt, ap);
+  va_end(ap);
+}
+}  // namespace smac
+
+namespace {
+
 #define CK(call)                                                                          \
   do {                                                                                    \
     cudaError_t e_ = (call);                                                              \
@@ -852,8 +866,10 @@ smac_status run_solve(smac_handle* h, const double** xout) {
           break;
         }
         ++restarts;
-        CK(cudaMemsetAsync(base_of(g, mixed ? (void*)h->d32 : (void*)h->d64), 0,
-                           (mixed ? sizeof(float) : sizeof(double)) * (size_t)g.alloc, h->stream));
+        if (mixed)
+          CK(cudaMemsetAsync(base_of(g, h->d32), 0, sizeof(float) * (size_t)g.alloc, h->stream));
+        else
+          CK(cudaMemsetAsync(base_of(g, h->d64), 0, sizeof(double) * (size_t)g.alloc, h->stream));
         h->hs->done = 0;
         h->hs->first = 1;
         h->hs->status = 0;

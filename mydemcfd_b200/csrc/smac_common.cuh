@@ -200,4 +200,91 @@ __device__ __forceinline__ bool grid_reduce(double (&v)[NV], const Op (&ops)[NV]
 
 __device__ __forceinline__ bool finite_d(double x) { return isfinite(x); }
 
+template <class T> struct Acc { typedef T type; };
+template <class T> using acc_t = typename Acc<T>::type;
+
+
+// ------------------------------------------------------------------------
+// Reference-layout index helpers (MyArray<T,3>: (z*sy + y)*sx + x).
+struct RefDims {
+  int Nx, Ny, Nz;
+  __host__ __device__ __forceinline__ long long cell(int x, int y, int z) const {
+    return ((long long)z * (Ny + 2) + y) * (Nx + 2) + x;
+  }
+  __host__ __device__ __forceinline__ long long xf(int x, int y, int z) const {
+    return ((long long)z * (Ny + 2) + y) * (Nx + 3) + x;
+  }
+  __host__ __device__ __forceinline__ long long yf(int x, int y, int z) const {
+    return ((long long)z * (Ny + 3) + y) * (Nx + 2) + x;
+  }
+  __host__ __device__ __forceinline__ long long zf(int x, int y, int z) const {
+    return ((long long)z * (Ny + 2) + y) * (Nx + 2) + x;
+  }
+};
+
+// ------------------------------------------------------------------------
+// Stencil pieces.  Every product and sum is an explicit round-to-nearest
+// intrinsic, so the compiler contracts nothing on its own: every kernel that
+// evaluates the same cell update rounds identically (the fused sweep equals
+// the half-sweep kernels bit for bit) whatever the code around it.
+template <class A> struct Ar;
+template <> struct Ar<double> {
+  static __device__ __forceinline__ double mul(double a, double b) { return __dmul_rn(a, b); }
+  static __device__ __forceinline__ double add(double a, double b) { return __dadd_rn(a, b); }
+  static __device__ __forceinline__ double fma(double a, double b, double c) { return __fma_rn(a, b, c); }
+  static __device__ __forceinline__ double div(double a, double b) { return __ddiv_rn(a, b); }
+};
+template <> struct Ar<float> {
+  static __device__ __forceinline__ float mul(float a, float b) { return __fmul_rn(a, b); }
+  static __device__ __forceinline__ float add(float a, float b) { return __fadd_rn(a, b); }
+  static __device__ __forceinline__ float fma(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+  static __device__ __forceinline__ float div(float a, float b) { return __fdiv_rn(a, b); }
+};
+
+template <class T, class C>
+struct Stencil {
+  typedef acc_t<T> A;
+  typedef Ar<A> R;
+  const C* __restrict__ bx;
+  const C* __restrict__ by;
+  const C* __restrict__ bz;
+  A ihx2, ihy2, ihz2;
+  // face weights of cell c: x-, x+, y-, y+, z-, z+
+  __device__ __forceinline__ void coeffs(int c, int px, int ps, A& wxm, A& wxp, A& wym, A& wyp, A& wzm,
+                                         A& wzp) const {
+    wxm = R::mul((A)CoefLoad<C>::get(bx, c), ihx2);
+    wxp = R::mul((A)CoefLoad<C>::get(bx, c + 1), ihx2);
+    wym = R::mul((A)CoefLoad<C>::get(by, c), ihy2);
+    wyp = R::mul((A)CoefLoad<C>::get(by, c + px), ihy2);
+    wzm = R::mul((A)CoefLoad<C>::get(bz, c), ihz2);
+    wzp = R::mul((A)CoefLoad<C>::get(bz, c + ps), ihz2);
+  }
+  static __device__ __forceinline__ A diag(A wxm, A wxp, A wym, A wyp, A wzm, A wzp) {
+    return R::add(R::add(R::add(wxm, wxp), R::add(wym, wyp)), R::add(wzm, wzp));
+  }
+  // bv + sum w * n (neighbours in the order x-, x+, y-, y+, z-, z+)
+  static __device__ __forceinline__ A offsum(A bv, A wxm, A wxp, A wym, A wyp, A wzm, A wzp, A n0, A n1, A n2,
+                                             A n3, A n4, A n5) {
+    A acc = R::fma(wxm, n0, bv);
+    acc = R::fma(wxp, n1, acc);
+    acc = R::fma(wym, n2, acc);
+    acc = R::fma(wyp, n3, acc);
+    acc = R::fma(wzm, n4, acc);
+    return R::fma(wzp, n5, acc);
+  }
+  // (A x)_c = diag x_c - sum w * n
+  static __device__ __forceinline__ A apply(A xc, A wxm, A wxp, A wym, A wyp, A wzm, A wzp, A n0, A n1, A n2,
+                                            A n3, A n4, A n5) {
+    const A d = diag(wxm, wxp, wym, wyp, wzm, wzp);
+    return offsum(R::mul(d, xc), -wxm, -wxp, -wym, -wyp, -wzm, -wzp, n0, n1, n2, n3, n4, n5);
+  }
+  // Gauss-Seidel value (bv + sum w * n) / diag, 0 where the diagonal is 0
+  static __device__ __forceinline__ A gs(A bv, A wxm, A wxp, A wym, A wyp, A wzm, A wzp, A n0, A n1, A n2, A n3,
+                                         A n4, A n5) {
+    const A d = diag(wxm, wxp, wym, wyp, wzm, wzp);
+    if (!(d > (A)0)) return (A)0;
+    return R::div(offsum(bv, wxm, wxp, wym, wyp, wzm, wzp, n0, n1, n2, n3, n4, n5), d);
+  }
+};
+
 }  // namespace smac
