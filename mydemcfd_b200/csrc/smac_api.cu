@@ -324,7 +324,7 @@ smac_status launch_iteration(smac_handle* h, bool mixed, bool gmg, int parity) {
     double* dold = parity ? h->d64b : h->d64;
     double* dnew = parity ? h->d64 : h->d64b;
     auto S = stencil<double, double>(g, h->lv[0].bx64, h->lv[0].by64, h->lv[0].bz64);
-    k_dir_matvec<double, double><<<gr, kBlock, 0, h->stream>>>(g, z, dold, dnew, S, h->q64, h->red, h->s, kz);
+    k_dir_matvec<double, double><<<gr, kBlock, 0, h->stream>>>(g, z, dold, dnew, S, h->q64, h->fluid, h->red, h->s, kz);
     k_update<double, double><<<gr, kBlock, 0, h->stream>>>(g, h->x64a, dnew, h->r64, h->q64, h->red, h->s, kz);
     account(h, g, 7 * 8, 1);
     account(h, g, 6 * 8, 1);
@@ -350,7 +350,7 @@ smac_status launch_iteration(smac_handle* h, bool mixed, bool gmg, int parity) {
     float* dold = parity ? h->d32b : h->d32;
     float* dnew = parity ? h->d32 : h->d32b;
     auto S = stencil<float, float>(g, h->lv[0].bxm, h->lv[0].bym, h->lv[0].bzm);
-    k_dir_matvec<float, float><<<gr, kBlock, 0, h->stream>>>(g, z, dold, dnew, S, h->q32, h->red, h->s, kz);
+    k_dir_matvec<float, float><<<gr, kBlock, 0, h->stream>>>(g, z, dold, dnew, S, h->q32, h->fluid, h->red, h->s, kz);
     k_update<float, float><<<gr, kBlock, 0, h->stream>>>(g, h->e32, dnew, h->r32, h->q32, h->red, h->s, kz);
     auto S64 = stencil<double, double>(g, h->lv[0].bx64, h->lv[0].by64, h->lv[0].bz64);
     k_reliable<float><<<gr, kBlock, 0, h->stream>>>(g, h->x64a, h->x64b, h->e32, h->b64, S64, h->r32, h->red, h->s, kz);
@@ -1148,7 +1148,7 @@ smac_status smac_time_kernel(smac_handle* h, int kernel_id, int reps, float* ms,
       }
       case 7: {
         auto S = stencil<float, float>(g, h->lv[0].bxm, h->lv[0].bym, h->lv[0].bzm);
-        k_dir_matvec<float, float><<<grid_cells(g, kz), kBlock, 0, h->stream>>>(g, h->z32, h->d32, h->d32b, S, h->q32, h->red, h->s, kz);
+        k_dir_matvec<float, float><<<grid_cells(g, kz), kBlock, 0, h->stream>>>(g, h->z32, h->d32, h->d32b, S, h->q32, h->fluid, h->red, h->s, kz);
         per = 7 * 4.0;
         break;
       }

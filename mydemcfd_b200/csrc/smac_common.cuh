@@ -92,6 +92,7 @@ struct Scalars {
   double reliable_delta2;
   double inv_nfluid; // 1 / number of fluid cells (0 when not pure Neumann)
   double sum_tmp;    // scratch for one-off sums
+  double zshift;     // mean of z = M r over fluid cells, removed in the direction update
   int iter;          // matvecs done
   int max_iter;
   int done;          // 1: converged or failed

@@ -475,6 +475,7 @@ __global__ void __launch_bounds__(TNT) k_dot_rz(Geom g, const T* __restrict__ r,
       }
       s->beta = s->first ? 0.0 : rz_new / s->rz;
       s->rz = rz_new;
+      s->zshift = out[1] * s->inv_nfluid;
       s->first = 0;
     }
   }

@@ -180,6 +180,7 @@ __global__ void __launch_bounds__(RB_NT) k_rbgs_sweep(Geom g, const T* __restric
         else {
           s->beta = s->first ? 0.0 : rz_new / s->rz;
           s->rz = rz_new;
+          s->zshift = out[1] * s->inv_nfluid;
           s->first = 0;
         }
       }
@@ -187,27 +188,34 @@ __global__ void __launch_bounds__(RB_NT) k_rbgs_sweep(Geom g, const T* __restric
   }
 }
 
-// d = z + beta d fused with q = A d and p.Ap (the direction update of the
-// next iteration is folded into the matvec that needs it): reads z and the
-// old d at the stencil points, writes the new d and q.
+// d = (z - zshift) + beta d fused with q = A d and p.Ap (the direction
+// update of the next iteration is folded into the matvec that needs it):
+// reads z and the old d at the stencil points, writes the new d and q.
+// zshift (the fluid mean of z) keeps d free of the constant null-space
+// component of the pure-Neumann operator, which would otherwise make p.Ap a
+// cancellation near the rounding floor; cells without unknowns keep d = 0.
 template <class T, class C>
 __global__ void __launch_bounds__(TNT) k_dir_matvec(Geom g, const T* __restrict__ z, T* __restrict__ d_old,
-                                                    T* __restrict__ d_new, Stencil<T, C> S, T* q, RedBuf red,
-                                                    Scalars* s, int kz) {
+                                                    T* __restrict__ d_new, Stencil<T, C> S, T* q,
+                                                    const uint8_t* __restrict__ fluid, RedBuf red, Scalars* s,
+                                                    int kz) {
   if (s->done) return;
   typedef acc_t<T> A;
   const int i = blockIdx.x * TBX + threadIdx.x;
   const int j = blockIdx.y * TBY + threadIdx.y;
   const int k0 = blockIdx.z * kz;
   const A beta = (A)s->beta;
+  const A zs = (A)s->zshift;
   double v[1] = {0.0};
   if (i < g.nx && j < g.ny) {
     const int k1 = min(k0 + kz, g.nz);
     int c = g.idx(i, j, k0);
-    auto D = [&](int cc) -> A { return Ar<A>::fma(beta, (A)d_old[cc], (A)z[cc]); };
+    // neighbours without unknowns enter through zero face weights only
+    auto D = [&](int cc) -> A { return Ar<A>::fma(beta, (A)d_old[cc], Ar<A>::add((A)z[cc], -zs)); };
     A xm = D(c - g.ps), xc = D(c);
     for (int k = k0; k < k1; ++k, c += g.ps) {
       const A xp = D(c + g.ps);
+      if (!(fluid[c] & 2)) xc = (A)0;
       A wxm, wxp, wym, wyp, wzm, wzp;
       S.coeffs(c, g.px, g.ps, wxm, wxp, wym, wyp, wzm, wzp);
       const A y = Stencil<T, C>::apply(xc, wxm, wxp, wym, wyp, wzm, wzp, D(c - 1), D(c + 1), D(c - g.px), D(c + g.px),
