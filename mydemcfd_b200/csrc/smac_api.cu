@@ -11,6 +11,10 @@
 #include "smac_b200.h"
 #include "smac_kernels.cuh"
 #include "smac_rbgs.cuh"
+#include "smac_rbgs_tma.cuh"
+
+#include <cudaTypedefs.h>
+#include <type_traits>
 
 using namespace smac;
 
@@ -76,6 +80,9 @@ struct Level {
   void *bxm = nullptr, *bym = nullptr, *bzm = nullptr;  // mixed-precision coefficients
   int ctm = CT_F32;
   float *x32 = nullptr, *x32b = nullptr, *rhs32 = nullptr;   // levels >= 1
+  // TMA tensor maps of the fused sweep, indexed by the iterate buffer read
+  SweepMaps mp64[2], mp32[2];
+  bool tma64 = false, tma32 = false;
 };
 
 }  // namespace
@@ -100,6 +107,8 @@ struct smac_handle {
   float *r32 = nullptr, *z32 = nullptr, *z32b = nullptr, *d32 = nullptr, *d32b = nullptr, *q32 = nullptr,
         *e32 = nullptr;
   RedBuf red{};
+  int num_sms = 148;
+  bool use_tma = true;     // fused sweeps stage their tiles with the copy engine
   Scalars* s = nullptr;    // device
   Scalars* hs = nullptr;   // pinned host mirror
   cudaGraphExec_t graph[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};  // [precision][gmg]
@@ -202,12 +211,39 @@ inline dim3 grid_sweep(const Geom& g, int zc) {
   return dim3((g.nx + RB_TX - 1) / RB_TX, (g.ny + TY - 1) / TY, (g.nz + zc - 1) / zc);
 }
 
+template <class T, int MODE, bool DOT>
+void launch_tma_sweep(smac_handle* h, int l, const SweepMaps& maps, T* xout, const double* sh, int c0, const T* xc) {
+  typedef TmaTile<T> Lt;
+  const Level& L = h->lv[l];
+  const Geom& g = L.g;
+  const Level& Lc = h->lv[l + 1 < h->nlev ? l + 1 : l];
+  const long long total = (long long)((g.nx + Lt::TX - 1) / Lt::TX) * ((g.ny + Lt::TY - 1) / Lt::TY) * g.nz;
+  const int G = (int)std::max(1LL, std::min((long long)h->num_sms, total / 8));
+  k_rbgs_tma<T, MODE, DOT><<<G, TMA_NT, Lt::SMEM_BYTES, h->stream>>>(maps, g, xout, sh, g.ihx2, g.ihy2, g.ihz2, c0, xc,
+                                                                     Lc.g, Lc.cx, Lc.cy, Lc.cz, h->s, h->red);
+}
+
 template <class T, class CS>
 void launch_sweep(smac_handle* h, int l, int mode, bool dot, const T* xin, T* xout, const T* rhs, const double* sh,
                   const void* bx, const void* by, const void* bz, int c0, const T* xc) {
   const Level& L = h->lv[l];
   const Geom& g = L.g;
   const Level& Lc = h->lv[l + 1 < h->nlev ? l + 1 : l];
+  if constexpr (std::is_same<T, CS>::value) {
+    const bool ok = sizeof(T) == 8 ? L.tma64 : L.tma32;
+    if (h->use_tma && ok) {
+      // the maps bind the level's two iterate buffers, its rhs and coefficients
+      const SweepMaps* mp = sizeof(T) == 8 ? L.mp64 : L.mp32;
+      const void* xb = (l == 0) ? (sizeof(T) == 8 ? (const void*)h->z64b : (const void*)h->z32b)
+                                : (sizeof(T) == 8 ? (const void*)L.x64b : (const void*)L.x32b);
+      const SweepMaps& M = mp[(xin != nullptr && (const void*)xin == xb) ? 1 : 0];
+      if (mode == 0) { if (dot) launch_tma_sweep<T, 0, true>(h, l, M, xout, sh, c0, xc); else launch_tma_sweep<T, 0, false>(h, l, M, xout, sh, c0, xc); }
+      else if (mode == 1) { if (dot) launch_tma_sweep<T, 1, true>(h, l, M, xout, sh, c0, xc); else launch_tma_sweep<T, 1, false>(h, l, M, xout, sh, c0, xc); }
+      else { if (dot) launch_tma_sweep<T, 2, true>(h, l, M, xout, sh, c0, xc); else launch_tma_sweep<T, 2, false>(h, l, M, xout, sh, c0, xc); }
+      (void)rhs; (void)bx; (void)by; (void)bz;
+      return;
+    }
+  }
   auto S = stencil<T, CS>(g, bx, by, bz);
   const int zc = sweep_zchunk<T>(g);
   const dim3 gr = grid_sweep<T>(g, zc);
@@ -433,6 +469,86 @@ double iteration_bytes(smac_handle* h, bool mixed, bool gmg, int* launches) {
   return bytes;
 }
 
+
+// ---------------------------------------------------------------------------
+// TMA tensor maps.  cuTensorMapEncodeTiled is reached through the runtime's
+// driver entry point (no link against libcuda).
+PFN_cuTensorMapEncodeTiled_v12000 g_encode = nullptr;
+
+bool tma_encoder() {
+  if (g_encode) return true;
+  void* fn = nullptr;
+  cudaDriverEntryPointQueryResult q;
+  if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) != cudaSuccess ||
+      q != cudaDriverEntryPointSuccess || !fn)
+    return false;
+  g_encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+  return true;
+}
+
+// 3-D map of a padded array: extents (e0, e1, e2) elements, row/plane strides
+// of the layout, box (b0, b1, 1); out-of-bounds elements read as zero.
+bool encode_map(CUtensorMap* m, const void* base, bool f64, const Geom& g, int e0, int e1, int e2, int b0, int b1) {
+  const size_t es = f64 ? 8 : 4;
+  cuuint64_t dims[3] = {(cuuint64_t)e0, (cuuint64_t)e1, (cuuint64_t)e2};
+  cuuint64_t strides[2] = {(cuuint64_t)g.px * es, (cuuint64_t)g.ps * es};
+  cuuint32_t box[3] = {(cuuint32_t)b0, (cuuint32_t)b1, 1};
+  cuuint32_t estr[3] = {1, 1, 1};
+  const CUresult r = g_encode(m, f64 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3,
+                              const_cast<void*>(base), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                              CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS;
+}
+
+template <class T>
+bool build_level_maps(SweepMaps (&mp)[2], const Geom& g, const void* xa, const void* xb, const void* rhs,
+                      const void* bx, const void* by, const void* bz) {
+  typedef TmaTile<T> Lt;
+  const bool f64 = sizeof(T) == 8;
+  for (int q = 0; q < 2; ++q) {
+    SweepMaps& M = mp[q];
+    if (!encode_map(&M.xin, q == 0 ? xa : xb, f64, g, g.nx, g.ny, g.nz, Lt::XW, Lt::XH)) return false;
+    if (!encode_map(&M.rhs, rhs, f64, g, g.nx, g.ny, g.nz, Lt::XW, Lt::RH)) return false;
+    if (!encode_map(&M.bx, bx, f64, g, g.nx + 1, g.ny, g.nz, Lt::XW, Lt::RH)) return false;
+    if (!encode_map(&M.by, by, f64, g, g.nx, g.ny + 1, g.nz, Lt::XW, Lt::YH)) return false;
+    if (!encode_map(&M.bz, bz, f64, g, g.nx, g.ny, g.nz + 1, Lt::XW, Lt::RH)) return false;
+  }
+  return true;
+}
+
+template <class T, int MODE, bool DOT>
+cudaError_t tma_attr() {
+  return cudaFuncSetAttribute(k_rbgs_tma<T, MODE, DOT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              TmaTile<T>::SMEM_BYTES);
+}
+
+// Tensor maps for every separately launched grid, or use_tma = false.
+void setup_tma(smac_handle* h) {
+  h->use_tma = false;
+  if (!tma_encoder()) return;
+  cudaError_t e = cudaSuccess;
+  cudaError_t es[12] = {tma_attr<double, 0, false>(), tma_attr<double, 0, true>(), tma_attr<double, 1, false>(),
+                        tma_attr<double, 1, true>(),  tma_attr<double, 2, false>(), tma_attr<double, 2, true>(),
+                        tma_attr<float, 0, false>(),  tma_attr<float, 0, true>(),  tma_attr<float, 1, false>(),
+                        tma_attr<float, 1, true>(),   tma_attr<float, 2, false>(), tma_attr<float, 2, true>()};
+  for (cudaError_t x : es)
+    if (x != cudaSuccess) e = x;
+  if (e != cudaSuccess) { cudaGetLastError(); return; }
+  for (int l = 0; l < h->nlev; ++l) {
+    Level& L = h->lv[l];
+    const void* xa64 = l == 0 ? (const void*)h->z64 : (const void*)L.x64;
+    const void* xb64 = l == 0 ? (const void*)h->z64b : (const void*)L.x64b;
+    const void* r64 = l == 0 ? (const void*)h->r64 : (const void*)L.rhs64;
+    const void* xa32 = l == 0 ? (const void*)h->z32 : (const void*)L.x32;
+    const void* xb32 = l == 0 ? (const void*)h->z32b : (const void*)L.x32b;
+    const void* r32 = l == 0 ? (const void*)h->r32 : (const void*)L.rhs32;
+    L.tma64 = build_level_maps<double>(L.mp64, L.g, xa64, xb64, r64, L.bx64, L.by64, L.bz64);
+    L.tma32 = L.ctm == CT_F32 && build_level_maps<float>(L.mp32, L.g, xa32, xb32, r32, L.bxm, L.bym, L.bzm);
+  }
+  h->use_tma = true;
+}
+
 }  // namespace
 
 // ===========================================================================
@@ -586,6 +702,8 @@ smac_status smac_create(const smac_grid_desc* desc, const smac_options* opts, vo
     if (eh != cudaSuccess) { set_err("cudaMallocHost: %s", cudaGetErrorString(eh)); return fail(SMAC_CUDA_ERROR); }
     memset(h->hs, 0, sizeof(Scalars));
   }
+  h->num_sms = prop.multiProcessorCount;
+  setup_tma(h);
   cudaError_t es = cudaStreamSynchronize(h->stream);
   if (es != cudaSuccess) { set_err("smac_create: %s", cudaGetErrorString(es)); return fail(SMAC_CUDA_ERROR); }
   *out = h;

@@ -366,6 +366,7 @@ __global__ void __launch_bounds__(TNT) k_update(Geom g, TX* x, const T* __restri
   double out[3];
   if (grid_reduce<3, TNT>(v, ops, red, 0, out)) {
     if (threadIdx.x == 0 && threadIdx.y == 0) {
+      if (s->status == 6) { s->done = 1; return; }  // a copy-engine wait expired in a sweep
       s->iter += 1;
       s->e_reset = 0;
       const double m = out[0] * s->inv_nfluid;
