@@ -217,10 +217,12 @@ void launch_tma_sweep(smac_handle* h, int l, const SweepMaps& maps, T* xout, con
   const Level& L = h->lv[l];
   const Geom& g = L.g;
   const Level& Lc = h->lv[l + 1 < h->nlev ? l + 1 : l];
-  const long long total = (long long)((g.nx + Lt::TX - 1) / Lt::TX) * ((g.ny + Lt::TY - 1) / Lt::TY) * g.nz;
-  const int G = (int)std::max(1LL, std::min((long long)h->num_sms, total / 8));
+  const int zc = g.nz >= 128 ? 32 : (g.nz >= 32 ? 16 : g.nz);
+  const long long items =
+      (long long)((g.nx + Lt::TX - 1) / Lt::TX) * ((g.ny + Lt::TY - 1) / Lt::TY) * ((g.nz + zc - 1) / zc);
+  const int G = (int)std::max(1LL, std::min(2LL * h->num_sms, items));
   k_rbgs_tma<T, MODE, DOT><<<G, TMA_NT, Lt::SMEM_BYTES, h->stream>>>(maps, g, xout, sh, g.ihx2, g.ihy2, g.ihz2, c0, xc,
-                                                                     Lc.g, Lc.cx, Lc.cy, Lc.cz, h->s, h->red);
+                                                                     Lc.g, Lc.cx, Lc.cy, Lc.cz, h->s, h->red, zc);
 }
 
 template <class T, class CS>

@@ -5,8 +5,8 @@
 // two half-sweep kernels): xout = S(xin), colour c0 from xin, then colour
 // 1-c0 from the new c0 values.  What changes is how the data arrive:
 //
-//   - one persistent CTA per SM walks a contiguous run of (column tile, z-plane)
-//     steps, so the z-march of a column continues without a new prologue;
+//   - persistent CTAs (two per SM) walk (z-chunk, column tile) items in
+//     z-chunk-major order, each item a z-march over its chunk;
 //   - plane p of the five inputs (xin tile + 2-cell ring; rhs, bx, by, bz tiles
 //     + 1-cell ring) forms one stage, loaded by five cp.async.bulk.tensor 3-D
 //     tile copies issued by one thread and completing on one mbarrier;
@@ -63,11 +63,12 @@ __device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, i
       : "memory");
 }
 
-// Tile geometry of one stage for vector type T.
+// Tile geometry of one stage for vector type T: 64 x 8 cells (FP32) or
+// 32 x 8 (FP64), so that a 5-stage ring fits twice in an SM's shared memory.
 template <class T>
 struct TmaTile {
-  static constexpr int TX = RB_TX;                 // 64 cells along x
-  static constexpr int TY = RbTile<T>::TY;         // 16 (FP32) or 8 (FP64) along y
+  static constexpr int TX = sizeof(T) == 8 ? 32 : 64;
+  static constexpr int TY = 8;
   static constexpr int XW = TX + 8;                // box width: columns i0-4 .. i0+TX+3 (16 B aligned start)
   static constexpr int XH = TY + 4;                // xin rows j0-2 .. j0+TY+1
   static constexpr int RH = TY + 2;                // rhs/bx/bz rows j0-1 .. j0+TY
@@ -93,10 +94,10 @@ struct SweepMaps {
 };
 
 template <class T, int MODE, bool DOT>
-__global__ void __launch_bounds__(TMA_NT, 1)
+__global__ void __launch_bounds__(TMA_NT, 2)
     k_rbgs_tma(const __grid_constant__ SweepMaps maps, Geom g, T* __restrict__ xout, const double* shift, double ihx2,
                double ihy2, double ihz2, int c0, const T* __restrict__ xc, Geom gc, int cx, int cy, int cz, Scalars* s,
-               RedBuf red) {
+               RedBuf red, int zchunk) {
   typedef acc_t<T> A;
   typedef TmaTile<T> L;
   constexpr int TX = L::TX, TY = L::TY, XW = L::XW, RW = L::RW, RH = L::RH;
@@ -114,10 +115,14 @@ __global__ void __launch_bounds__(TMA_NT, 1)
   }
   __syncthreads();
 
+  // Work items are (z-chunk, column tile) in z-chunk-major order, taken with
+  // a stride of the grid size: all column tiles of a z-slab are in flight
+  // together, so the ring rows and columns one CTA reads from its
+  // neighbours' tiles come from L2 rather than DRAM.
   const int ncx = (g.nx + TX - 1) / TX, ncy = (g.ny + TY - 1) / TY;
-  const long long total = (long long)ncx * ncy * g.nz;
-  const long long s0 = total * blockIdx.x / gridDim.x;
-  const long long s1 = total * (blockIdx.x + 1) / gridDim.x;
+  const int ncol = ncx * ncy;
+  const int nzc = (g.nz + zchunk - 1) / zchunk;
+  const int items = ncol * nzc;
   long long gstage = 0;  // stages issued by this CTA so far (mbarrier phase bookkeeping)
   bool failed = false;
   double dv[2] = {0.0, 0.0};
@@ -129,12 +134,10 @@ __global__ void __launch_bounds__(TMA_NT, 1)
   auto tileBY = [&](long long gi) { return reinterpret_cast<const T*>(stage_ptr(gi) + L::BY_OFF); };
   auto tileBZ = [&](long long gi) { return reinterpret_cast<const T*>(stage_ptr(gi) + L::BZ_OFF); };
 
-  long long step = s0;
-  while (step < s1 && !failed) {
-    const int col = (int)(step / g.nz);
-    const int kb = (int)(step % g.nz);
-    const int ke = (int)min((long long)g.nz, (long long)kb + (s1 - step));
-    step += ke - kb;
+  for (int item = blockIdx.x; item < items && !failed; item += gridDim.x) {
+    const int col = item % ncol;
+    const int kb = (item / ncol) * zchunk;
+    const int ke = min(g.nz, kb + zchunk);
     const int i0 = (col % ncx) * TX, j0 = (col / ncx) * TY;
     const int pb = kb - 2, pe = ke + 1;  // stages (planes) of this piece
     const long long gbase = gstage;      // global index of stage pb
