@@ -75,9 +75,9 @@ enum CoefType { CT_F64 = 0, CT_F32 = 1, CT_BF16 = 2 };
 struct Level {
   Geom g{};
   int cx = 0, cy = 0, cz = 0;  // coarsened from the grid above
-  double *bx64 = nullptr, *by64 = nullptr, *bz64 = nullptr;
+  double *bx64 = nullptr, *by64 = nullptr, *bz64 = nullptr;  // stencil weights f_b / h^2 of this grid
   double *x64 = nullptr, *x64b = nullptr, *rhs64 = nullptr;  // levels >= 1 (two iterates: out-of-place sweeps)
-  void *bxm = nullptr, *bym = nullptr, *bzm = nullptr;  // mixed-precision coefficients
+  void *bxm = nullptr, *bym = nullptr, *bzm = nullptr;  // mixed-precision weights
   int ctm = CT_F32;
   float *x32 = nullptr, *x32b = nullptr, *rhs32 = nullptr;   // levels >= 1
   // TMA tensor maps of the fused sweep, indexed by the iterate buffer read
@@ -97,6 +97,7 @@ struct smac_handle {
   int lc = 0;  // first grid of the single-CTA coarse set
   Level lv[MAXL];
   uint8_t* fluid = nullptr;   // padded cell bits: 1 C_INTERIOR, 2 fluid unknown
+  double *fbx = nullptr, *fby = nullptr, *fbz = nullptr;  // masked f_b, padded (divergence, correction, adjoint)
   double nfluid = 0.0;
   // copies of the reference-layout types (the correction and the adjoint read them)
   uint8_t *ct = nullptr, *fxt = nullptr, *fyt = nullptr, *fzt = nullptr;
@@ -156,9 +157,8 @@ inline dim3 grid_planes(int nx, int ny, int nz) { return dim3((nx + TBX - 1) / T
 const dim3 kBlock(TBX, TBY, 1);
 
 template <class T, class C>
-Stencil<T, C> stencil(const Geom& g, const void* bx, const void* by, const void* bz) {
-  typedef acc_t<T> A;
-  return Stencil<T, C>{(const C*)bx, (const C*)by, (const C*)bz, (A)g.ihx2, (A)g.ihy2, (A)g.ihz2};
+Stencil<T, C> stencil(const Geom&, const void* bx, const void* by, const void* bz) {
+  return Stencil<T, C>{(const C*)bx, (const C*)by, (const C*)bz};
 }
 
 smac_status validate_options(const smac_options* o) {
@@ -217,12 +217,21 @@ void launch_tma_sweep(smac_handle* h, int l, const SweepMaps& maps, T* xout, con
   const Level& L = h->lv[l];
   const Geom& g = L.g;
   const Level& Lc = h->lv[l + 1 < h->nlev ? l + 1 : l];
-  const int zc = g.nz >= 128 ? 32 : (g.nz >= 32 ? 16 : g.nz);
-  const long long items =
-      (long long)((g.nx + Lt::TX - 1) / Lt::TX) * ((g.ny + Lt::TY - 1) / Lt::TY) * ((g.nz + zc - 1) / zc);
-  const int G = (int)std::max(1LL, std::min(2LL * h->num_sms, items));
-  k_rbgs_tma<T, MODE, DOT><<<G, TMA_NT, Lt::SMEM_BYTES, h->stream>>>(maps, g, xout, sh, g.ihx2, g.ihy2, g.ihz2, c0, xc,
-                                                                     Lc.g, Lc.cx, Lc.cy, Lc.cz, h->s, h->red, zc);
+  // z-chunk: fewest planes per CTA, counting the 4 staged halo planes of each item
+  const long long ncol = (long long)((g.nx + Lt::TX - 1) / Lt::TX) * ((g.ny + Lt::TY - 1) / Lt::TY);
+  const long long slots = 2LL * h->num_sms;
+  int zc = g.nz;
+  long long best = -1;
+  for (int cand : {64, 32, 16, 8}) {
+    const int z = std::min(cand, g.nz);
+    const long long items = ncol * ((g.nz + z - 1) / z);
+    const long long cost = ((items + slots - 1) / slots) * (z + 4);
+    if (best < 0 || cost < best) { best = cost; zc = z; }
+  }
+  const long long items = ncol * ((g.nz + zc - 1) / zc);
+  const int G = (int)std::max(1LL, std::min(slots, items));
+  k_rbgs_tma<T, MODE, DOT><<<G, Lt::NT, Lt::SMEM_BYTES, h->stream>>>(maps, g, xout, sh, c0, xc, Lc.g, Lc.cx, Lc.cy,
+                                                                    Lc.cz, h->s, h->red, zc);
 }
 
 template <class T, class CS>
@@ -643,6 +652,7 @@ smac_status smac_create(const smac_grid_desc* desc, const smac_options* opts, vo
   smac_status st;
 #define PA(ptr) do { st = palloc(h, g0, &(ptr)); if (st != SMAC_OK) return fail(st); } while (0)
   PA(h->lv[0].bx64); PA(h->lv[0].by64); PA(h->lv[0].bz64);
+  PA(h->fbx); PA(h->fby); PA(h->fbz);
   PA(h->b64); PA(h->x64a); PA(h->x64b); PA(h->r64); PA(h->z64); PA(h->z64b); PA(h->d64); PA(h->d64b); PA(h->q64);
   PA(h->tmp64);
   {
@@ -765,10 +775,11 @@ smac_status smac_set_coefficients(smac_handle* h, const double* fbx, const doubl
     CK(cudaMemcpyAsync(h->fzt, fzt, nzf, cudaMemcpyDeviceToDevice, h->stream));
   }
   k_import_coeffs<<<grid_planes(g.nx + 1, g.ny + 1, g.nz + 1), kBlock, 0, h->stream>>>(
-      g, h->R, fbx, fby, fbz, ct, fxt, fyt, fzt, h->lv[0].bx64, h->lv[0].by64, h->lv[0].bz64, h->fluid);
+      g, h->R, fbx, fby, fbz, ct, fxt, fyt, fzt, h->fbx, h->fby, h->fbz, h->lv[0].bx64, h->lv[0].by64,
+      h->lv[0].bz64, h->fluid);
   CKL();
-  k_fluid_finalize<<<grid_cells(g, kz_for(g)), kBlock, 0, h->stream>>>(g, h->lv[0].bx64, h->lv[0].by64,
-                                                                       h->lv[0].bz64, h->fluid, h->red, h->s, kz_for(g));
+  k_fluid_finalize<<<grid_cells(g, kz_for(g)), kBlock, 0, h->stream>>>(g, h->fbx, h->fby, h->fbz, h->fluid, h->red,
+                                                                       h->s, kz_for(g));
   CKL();
   // FP32 fine copy for the mixed-precision Krylov operator
   {
@@ -872,7 +883,7 @@ smac_status smac_divergence(smac_handle* h, const double* vxs, const double* vys
   const Geom& g = h->lv[0].g;
   k_divergence<<<grid_planes(g.nx, g.ny, g.nz), kBlock, 0, h->stream>>>(
       g, h->R, 1.0 / h->desc.dx, 1.0 / h->desc.dy, 1.0 / h->desc.dz, 1.0 / dt, vxs, vys, vzs, eps, eps_old,
-      h->lv[0].bx64, h->lv[0].by64, h->lv[0].bz64, fsx, fsy, fsz, h->fluid, h->b64, rhs_out);
+      h->fbx, h->fby, h->fbz, fsx, fsy, fsz, h->fluid, h->b64, rhs_out);
   CKL();
   h->dt = dt;
   h->have_rhs = true;
@@ -1116,7 +1127,7 @@ smac_status smac_correct(smac_handle* h, double* p_delta, double* p, const doubl
   const RefDims& R = h->R;
   k_correct<<<grid_planes(R.Nx + 3, R.Ny + 3, R.Nz + 3), kBlock, 0, h->stream>>>(
       R, g, 1.0 / h->desc.dx, 1.0 / h->desc.dy, 1.0 / h->desc.dz, dt, h->ct, h->fxt, h->fyt, h->fzt, p_delta, p, vxs,
-      vys, vzs, firx, firy, firz, h->lv[0].bx64, h->lv[0].by64, h->lv[0].bz64, fsx, fsy, fsz, vx, vy, vz, 0);
+      vys, vzs, firx, firy, firz, h->fbx, h->fby, h->fbz, fsx, fsy, fsz, vx, vy, vz, 0);
   CKL();
   account(h, g, 3 * 8 + 8 + 3 * 8 + 3 * 8 + 3, 1);
   if (zero_p_delta) {
@@ -1138,7 +1149,7 @@ smac_status smac_project(smac_handle* h, const double* vxs, const double* vys, c
   const RefDims& R = h->R;
   k_correct<<<grid_planes(R.Nx + 3, R.Ny + 3, R.Nz + 3), kBlock, 0, h->stream>>>(
       R, g, 1.0 / h->desc.dx, 1.0 / h->desc.dy, 1.0 / h->desc.dz, dt, h->ct, h->fxt, h->fyt, h->fzt, p_delta, nullptr,
-      vxs, vys, vzs, nullptr, nullptr, nullptr, h->lv[0].bx64, h->lv[0].by64, h->lv[0].bz64, nullptr, nullptr, nullptr,
+      vxs, vys, vzs, nullptr, nullptr, nullptr, h->fbx, h->fby, h->fbz, nullptr, nullptr, nullptr,
       vx, vy, vz, 1);
   CKL();
   account(h, g, 3 * 8 + 8 + 3 * 8 + 3 * 8 + 3, 1);
@@ -1158,8 +1169,8 @@ smac_status smac_project_adjoint(smac_handle* h, const double* gvx, const double
   const Geom& g = h->lv[0].g;
   const RefDims& R = h->R;
   k_adj_divergence<<<grid_planes(g.nx, g.ny, g.nz), kBlock, 0, h->stream>>>(
-      g, R, 1.0 / h->desc.dx, 1.0 / h->desc.dy, 1.0 / h->desc.dz, gvx, gvy, gvz, h->lv[0].bx64, h->lv[0].by64,
-      h->lv[0].bz64, h->fluid, h->b64);
+      g, R, 1.0 / h->desc.dx, 1.0 / h->desc.dy, 1.0 / h->desc.dz, gvx, gvy, gvz, h->fbx, h->fby, h->fbz,
+      h->fluid, h->b64);
   CKL();
   h->have_rhs = true;
   const double* x = nullptr;
@@ -1217,11 +1228,12 @@ smac_status smac_time_kernel(smac_handle* h, int kernel_id, int reps, float* ms,
   st.beta = 0.0;
   *h->hs = st;
   CK(cudaMemcpyAsync(h->s, h->hs, sizeof(Scalars), cudaMemcpyHostToDevice, h->stream));
-  // non-zero operands: d = b (FP64) and d32 = r32, so that p.Ap > 0
+  // non-zero operands: d = b (FP64), d32 = r32 = z32 = b, so that p.Ap > 0
   CK(cudaMemcpyAsync(base_of(g, h->d64), base_of(g, h->b64), sizeof(double) * (size_t)g.alloc, cudaMemcpyDeviceToDevice,
                      h->stream));
   k_convert<float><<<1184, 256, 0, h->stream>>>(base_of(g, h->b64), base_of(g, h->d32), g.alloc);
   k_convert<float><<<1184, 256, 0, h->stream>>>(base_of(g, h->b64), base_of(g, h->r32), g.alloc);
+  k_convert<float><<<1184, 256, 0, h->stream>>>(base_of(g, h->b64), base_of(g, h->z32), g.alloc);
   cudaEvent_t e0, e1;
   CK(cudaEventCreate(&e0));
   CK(cudaEventCreate(&e1));

@@ -229,19 +229,40 @@ struct RefDims {
 // evaluates the same cell update rounds identically (the fused sweep equals
 // the half-sweep kernels bit for bit) whatever the code around it.
 template <class A> struct Ar;
+// rcp(d): 1/d from the hardware's approximate reciprocal refined by
+// Newton-Raphson steps y <- y + y (1 - d y) (two for FP64, one for FP32),
+// for the Gauss-Seidel update, where a last-bit difference from the IEEE
+// quotient only perturbs the smoother, identically in every kernel.
 template <> struct Ar<double> {
   static __device__ __forceinline__ double mul(double a, double b) { return __dmul_rn(a, b); }
   static __device__ __forceinline__ double add(double a, double b) { return __dadd_rn(a, b); }
   static __device__ __forceinline__ double fma(double a, double b, double c) { return __fma_rn(a, b, c); }
   static __device__ __forceinline__ double div(double a, double b) { return __ddiv_rn(a, b); }
+  static __device__ __forceinline__ double rcp(double d) {
+    double y;
+    asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(d));
+    double e = __fma_rn(-d, y, 1.0);
+    y = __fma_rn(y, e, y);
+    e = __fma_rn(-d, y, 1.0);
+    return __fma_rn(y, e, y);
+  }
 };
 template <> struct Ar<float> {
   static __device__ __forceinline__ float mul(float a, float b) { return __fmul_rn(a, b); }
   static __device__ __forceinline__ float add(float a, float b) { return __fadd_rn(a, b); }
   static __device__ __forceinline__ float fma(float a, float b, float c) { return __fmaf_rn(a, b, c); }
   static __device__ __forceinline__ float div(float a, float b) { return __fdiv_rn(a, b); }
+  static __device__ __forceinline__ float rcp(float d) {
+    float y;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(d));
+    const float e = __fmaf_rn(-d, y, 1.0f);
+    return __fmaf_rn(y, e, y);
+  }
 };
 
+// The coefficient arrays hold the stencil weights w = f_b / h^2 of their
+// grid (the reference's Axp/Axm/... values, G_PCGSolver.cu:168-173), so a
+// cell update only loads them.
 template <class T, class C>
 struct Stencil {
   typedef acc_t<T> A;
@@ -249,16 +270,15 @@ struct Stencil {
   const C* __restrict__ bx;
   const C* __restrict__ by;
   const C* __restrict__ bz;
-  A ihx2, ihy2, ihz2;
   // face weights of cell c: x-, x+, y-, y+, z-, z+
   __device__ __forceinline__ void coeffs(int c, int px, int ps, A& wxm, A& wxp, A& wym, A& wyp, A& wzm,
                                          A& wzp) const {
-    wxm = R::mul((A)CoefLoad<C>::get(bx, c), ihx2);
-    wxp = R::mul((A)CoefLoad<C>::get(bx, c + 1), ihx2);
-    wym = R::mul((A)CoefLoad<C>::get(by, c), ihy2);
-    wyp = R::mul((A)CoefLoad<C>::get(by, c + px), ihy2);
-    wzm = R::mul((A)CoefLoad<C>::get(bz, c), ihz2);
-    wzp = R::mul((A)CoefLoad<C>::get(bz, c + ps), ihz2);
+    wxm = (A)CoefLoad<C>::get(bx, c);
+    wxp = (A)CoefLoad<C>::get(bx, c + 1);
+    wym = (A)CoefLoad<C>::get(by, c);
+    wyp = (A)CoefLoad<C>::get(by, c + px);
+    wzm = (A)CoefLoad<C>::get(bz, c);
+    wzp = (A)CoefLoad<C>::get(bz, c + ps);
   }
   static __device__ __forceinline__ A diag(A wxm, A wxp, A wym, A wyp, A wzm, A wzp) {
     return R::add(R::add(R::add(wxm, wxp), R::add(wym, wyp)), R::add(wzm, wzp));
@@ -284,7 +304,7 @@ struct Stencil {
                                          A n4, A n5) {
     const A d = diag(wxm, wxp, wym, wyp, wzm, wzp);
     if (!(d > (A)0)) return (A)0;
-    return R::div(offsum(bv, wxm, wxp, wym, wyp, wzm, wzp, n0, n1, n2, n3, n4, n5), d);
+    return R::mul(offsum(bv, wxm, wxp, wym, wyp, wzm, wzp, n0, n1, n2, n3, n4, n5), R::rcp(d));
   }
 };
 

@@ -32,11 +32,13 @@ constexpr int TNT = TBX * TBY;
 // F_INTERIOR (the reference's f_b is 0 there, CFD/G_SMACSolver_VoF.cu:1432-1436).
 // Domain-boundary faces keep f_b: with the zero ghost it enters only the
 // diagonal, as the reference's Adiag does (G_PCGSolver.cu:168-175).
+// Writes the masked f_b (b*) and the stencil weights w = f_b / h^2 (w*),
+// rounded as the reference's Axp = f_bx * inv_dx2 (G_PCGSolver.cu:168-173).
 __global__ void k_import_coeffs(Geom g, RefDims R, const double* __restrict__ fbx, const double* __restrict__ fby,
                                 const double* __restrict__ fbz, const uint8_t* __restrict__ ct,
                                 const uint8_t* __restrict__ fxt, const uint8_t* __restrict__ fyt,
                                 const uint8_t* __restrict__ fzt, double* bx, double* by, double* bz,
-                                uint8_t* fluid) {
+                                double* wx, double* wy, double* wz, uint8_t* fluid) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y * blockDim.y + threadIdx.y;
   const int k = blockIdx.z;
@@ -53,6 +55,7 @@ __global__ void k_import_coeffs(Geom g, RefDims R, const double* __restrict__ fb
     if (a == 0 || b == 0) v = 0.0;
     if (a == 1 && b == 1 && fxt[R.xf(i + 1, j + 1, k + 1)] != F_INTERIOR) v = 0.0;
     bx[c] = v;
+    wx[c] = __dmul_rn(v, g.ihx2);
   }
   if (i < g.nx && j <= g.ny && k < g.nz) {
     const int a = interior_cell(i, j - 1, k), b = interior_cell(i, j, k);
@@ -60,6 +63,7 @@ __global__ void k_import_coeffs(Geom g, RefDims R, const double* __restrict__ fb
     if (a == 0 || b == 0) v = 0.0;
     if (a == 1 && b == 1 && fyt[R.yf(i + 1, j + 1, k + 1)] != F_INTERIOR) v = 0.0;
     by[c] = v;
+    wy[c] = __dmul_rn(v, g.ihy2);
   }
   if (i < g.nx && j < g.ny && k <= g.nz) {
     const int a = interior_cell(i, j, k - 1), b = interior_cell(i, j, k);
@@ -67,6 +71,7 @@ __global__ void k_import_coeffs(Geom g, RefDims R, const double* __restrict__ fb
     if (a == 0 || b == 0) v = 0.0;
     if (a == 1 && b == 1 && fzt[R.zf(i + 1, j + 1, k + 1)] != F_INTERIOR) v = 0.0;
     bz[c] = v;
+    wz[c] = __dmul_rn(v, g.ihz2);
   }
   if (i < g.nx && j < g.ny && k < g.nz) fluid[c] = (interior_cell(i, j, k) == 1) ? 1 : 0;
 }
@@ -99,10 +104,10 @@ __global__ void __launch_bounds__(TNT) k_fluid_finalize(Geom g, const double* __
   }
 }
 
-// Coarse face coefficients: mean of the fine faces that tile the coarse face
-// (2x2 in 3-D), computed in FP64 and stored as C.  The coarse operator uses
-// 1/H^2 = (1/h^2)/4 per coarsened direction, like G_GMGSolver::initialize
-// (G_GMGSolver.cu:71-73,135-137).
+// Coarse stencil weights: mean of the fine weights of the faces that tile the
+// coarse face (2x2 in 3-D), times 1/4 when the face-normal direction is
+// coarsened (1/H^2 = (1/h^2)/4, G_GMGSolver.cu:71-73,135-137); computed in
+// FP64 and stored as C.  Both scalings are powers of two, so they are exact.
 template <class C>
 __global__ void k_coarsen_coeffs(Geom gf, Geom gc, int cx, int cy, int cz, const double* __restrict__ fbx,
                                  const double* __restrict__ fby, const double* __restrict__ fbz, C* bx, C* by,
@@ -118,7 +123,7 @@ __global__ void k_coarsen_coeffs(Geom gf, Geom gc, int cx, int cy, int cz, const
     double s = 0.0;
     for (int dk = 0; dk < rz; ++dk)
       for (int dj = 0; dj < ry; ++dj) s += fbx[gf.idx(i, (cy ? 2 * J : J) + dj, (cz ? 2 * K : K) + dk)];
-    s /= (double)(ry * rz);
+    s *= (cx ? 0.25 : 1.0) / (double)(ry * rz);
     bx[c] = coef_from_double<C>(s);
     if (bx64) bx64[c] = s;
   }
@@ -127,7 +132,7 @@ __global__ void k_coarsen_coeffs(Geom gf, Geom gc, int cx, int cy, int cz, const
     double s = 0.0;
     for (int dk = 0; dk < rz; ++dk)
       for (int di = 0; di < rx; ++di) s += fby[gf.idx((cx ? 2 * I : I) + di, jj, (cz ? 2 * K : K) + dk)];
-    s /= (double)(rx * rz);
+    s *= (cy ? 0.25 : 1.0) / (double)(rx * rz);
     by[c] = coef_from_double<C>(s);
     if (by64) by64[c] = s;
   }
@@ -136,7 +141,7 @@ __global__ void k_coarsen_coeffs(Geom gf, Geom gc, int cx, int cy, int cz, const
     double s = 0.0;
     for (int dj = 0; dj < ry; ++dj)
       for (int di = 0; di < rx; ++di) s += fbz[gf.idx((cx ? 2 * I : I) + di, (cy ? 2 * J : J) + dj, kk)];
-    s /= (double)(rx * ry);
+    s *= (cz ? 0.25 : 1.0) / (double)(rx * ry);
     bz[c] = coef_from_double<C>(s);
     if (bz64) bz64[c] = s;
   }
@@ -679,7 +684,7 @@ __device__ __forceinline__ void cta_half_sweep(const CoarseLevel& L, int colour,
   const Geom& g = L.g;
   T* x = (T*)L.x;
   const T* rhs = (const T*)L.rhs;
-  Stencil<T, C> S{(const C*)L.bx, (const C*)L.by, (const C*)L.bz, (A)g.ihx2, (A)g.ihy2, (A)g.ihz2};
+  Stencil<T, C> S{(const C*)L.bx, (const C*)L.by, (const C*)L.bz};
   const A sh = shift ? (A)(*shift) : (A)0;
   const int half = (g.nx + 1) / 2;
   const int total = half * g.ny * g.nz;
@@ -721,7 +726,7 @@ __device__ __forceinline__ void cta_resid_restrict(const CoarseLevel& L, const C
   const T* x = (const T*)L.x;
   const T* rhs = (const T*)L.rhs;
   T* rhs_c = (T*)Lc.rhs;
-  Stencil<T, C> S{(const C*)L.bx, (const C*)L.by, (const C*)L.bz, (A)g.ihx2, (A)g.ihy2, (A)g.ihz2};
+  Stencil<T, C> S{(const C*)L.bx, (const C*)L.by, (const C*)L.bz};
   const A sh = shift ? (A)(*shift) : (A)0;
   const int total = gc.nx * gc.ny * gc.nz;
   const int rx = Lc.cx ? 2 : 1, ry = Lc.cy ? 2 : 1, rz = Lc.cz ? 2 : 1;

@@ -10,9 +10,12 @@
 //   - plane p of the five inputs (xin tile + 2-cell ring; rhs, bx, by, bz tiles
 //     + 1-cell ring) forms one stage, loaded by five cp.async.bulk.tensor 3-D
 //     tile copies issued by one thread and completing on one mbarrier;
-//   - NS stages live in a shared-memory ring: while plane k is computed,
-//     planes k+2 .. k+NS-2 are in flight, which hides the DRAM latency that
-//     bounded the register-staged kernel;
+//   - NS stages live in a shared-memory ring fed as one stream across the
+//     CTA's items: while plane k is computed, planes k+2 and k+3 (or the next
+//     item's first planes) are in flight;
+//   - step k computes colour c0 on plane k (tile + ring, from the staged
+//     xin) and, after the step's one barrier, colour 1-c0 on plane k-1 from
+//     the c0 results of planes k-2 .. k, which stay in shared memory;
 //   - out-of-bounds boxes are zero-filled by the copy engine, which is the
 //     zero ghost of the layout; cells outside the domain are masked to zero.
 // Every mbarrier wait is bounded: on expiry the CTA records SMAC_CUDA_ERROR in
@@ -26,7 +29,6 @@
 namespace smac {
 
 constexpr int TMA_NS = 5;        // stages in the ring
-constexpr int TMA_NT = 256;      // threads per CTA
 constexpr long long TMA_WAIT_CYCLES = 2000000000LL;  // ~1 s of SM clock before a wait gives up
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
@@ -65,10 +67,15 @@ __device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, i
 
 // Tile geometry of one stage for vector type T: 64 x 8 cells (FP32) or
 // 32 x 8 (FP64), so that a 5-stage ring fits twice in an SM's shared memory.
+// One thread per pair of cells (i0+2m, i0+2m+1) of one row: each pair holds
+// one cell of either colour on every plane.
 template <class T>
 struct TmaTile {
   static constexpr int TX = sizeof(T) == 8 ? 32 : 64;
   static constexpr int TY = 8;
+  static constexpr int NT = TX / 2 * TY;           // threads per CTA
+  static constexpr int NRING = TX + 2 + TY;        // colour-c0 cells of the 1-cell ring, per plane
+  static constexpr int NRS = 4;                    // planes of colour-c0 results kept
   static constexpr int XW = TX + 8;                // box width: columns i0-4 .. i0+TX+3 (16 B aligned start)
   static constexpr int XH = TY + 4;                // xin rows j0-2 .. j0+TY+1
   static constexpr int RH = TY + 2;                // rhs/bx/bz rows j0-1 .. j0+TY
@@ -85,7 +92,7 @@ struct TmaTile {
   static constexpr int BZ_OFF = pad128(BY_OFF + Y_BYTES);
   static constexpr int STAGE_BYTES = pad128(BZ_OFF + R_BYTES);
   static constexpr int TX_BYTES = X_BYTES + 3 * R_BYTES + Y_BYTES;  // bytes the copies deliver per stage
-  static constexpr int RS_BYTES = pad128(3 * RH * RW * (int)sizeof(T));
+  static constexpr int RS_BYTES = pad128(NRS * RH * RW * (int)sizeof(T));
   static constexpr int SMEM_BYTES = TMA_NS * STAGE_BYTES + RS_BYTES + 128;  // + mbarriers
 };
 
@@ -94,20 +101,18 @@ struct SweepMaps {
 };
 
 template <class T, int MODE, bool DOT>
-__global__ void __launch_bounds__(TMA_NT, 2)
-    k_rbgs_tma(const __grid_constant__ SweepMaps maps, Geom g, T* __restrict__ xout, const double* shift, double ihx2,
-               double ihy2, double ihz2, int c0, const T* __restrict__ xc, Geom gc, int cx, int cy, int cz, Scalars* s,
-               RedBuf red, int zchunk) {
+__global__ void __launch_bounds__(TmaTile<T>::NT, 2)
+    k_rbgs_tma(const __grid_constant__ SweepMaps maps, Geom g, T* __restrict__ xout, const double* shift, int c0,
+               const T* __restrict__ xc, Geom gc, int cx, int cy, int cz, Scalars* s, RedBuf red, int zchunk) {
   typedef acc_t<T> A;
   typedef TmaTile<T> L;
-  constexpr int TX = L::TX, TY = L::TY, XW = L::XW, RW = L::RW, RH = L::RH;
+  constexpr int TX = L::TX, TY = L::TY, XW = L::XW, RW = L::RW, RH = L::RH, NT = L::NT, HP = TX / 2;
   extern __shared__ __align__(128) unsigned char smem[];
   uint64_t* bars = reinterpret_cast<uint64_t*>(smem + TMA_NS * L::STAGE_BYTES + L::RS_BYTES);
   A (*Rs)[RH][RW] = reinterpret_cast<A (*)[RH][RW]>(smem + TMA_NS * L::STAGE_BYTES);
   if (s && s->done) return;
   const int tid = threadIdx.x;
   const A sh = shift ? (A)(*shift) : (A)0;
-  const A hx = (A)ihx2, hy = (A)ihy2, hz = (A)ihz2;
 
   if (tid == 0) {
     for (int q = 0; q < TMA_NS; ++q) mbar_init(&bars[q], 1);
@@ -121,174 +126,190 @@ __global__ void __launch_bounds__(TMA_NT, 2)
   // neighbours' tiles come from L2 rather than DRAM.
   const int ncx = (g.nx + TX - 1) / TX, ncy = (g.ny + TY - 1) / TY;
   const int ncol = ncx * ncy;
-  const int nzc = (g.nz + zchunk - 1) / zchunk;
-  const int items = ncol * nzc;
-  long long gstage = 0;  // stages issued by this CTA so far (mbarrier phase bookkeeping)
+  const int items = ncol * ((g.nz + zchunk - 1) / zchunk);
+  const int nmine = (int)blockIdx.x < items ? (items - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
+  auto item_of = [&](int n) { return (int)blockIdx.x + n * (int)gridDim.x; };
+  auto first_plane = [&](int n) { return (item_of(n) / ncol) * zchunk - 2; };
+  auto last_plane = [&](int n) { return min(g.nz, (item_of(n) / ncol) * zchunk + zchunk) + 1; };
+
+  // Producer (thread 0): issues the CTA's stage stream in order, one stage
+  // per slot released by the consumers.
+  int pn = 0, pp = nmine > 0 ? first_plane(0) : 0, ppe = nmine > 0 ? last_plane(0) : 0;
+  unsigned pgi = 0;
+  auto issue_next = [&]() {
+    if (pn >= nmine) return;
+    const int col = item_of(pn) % ncol;
+    const int i0 = (col % ncx) * TX, j0 = (col / ncx) * TY;
+    unsigned char* st = smem + (pgi % TMA_NS) * L::STAGE_BYTES;
+    uint64_t* bar = &bars[pgi % TMA_NS];
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    mbar_expect_tx(bar, (uint32_t)(MODE == 1 ? L::TX_BYTES - L::X_BYTES : L::TX_BYTES));
+    if constexpr (MODE != 1) tma_load_3d(st + L::X_OFF, &maps.xin, i0 - 4, j0 - 2, pp, bar);
+    tma_load_3d(st + L::R_OFF, &maps.rhs, i0 - 4, j0 - 1, pp, bar);
+    tma_load_3d(st + L::BX_OFF, &maps.bx, i0 - 4, j0 - 1, pp, bar);
+    tma_load_3d(st + L::BY_OFF, &maps.by, i0 - 4, j0 - 1, pp, bar);
+    tma_load_3d(st + L::BZ_OFF, &maps.bz, i0 - 4, j0 - 1, pp, bar);
+    ++pgi;
+    if (++pp > ppe && ++pn < nmine) { pp = first_plane(pn); ppe = last_plane(pn); }
+  };
+  if (tid == 0)
+    for (int q = 0; q < TMA_NS; ++q) issue_next();
+
+  // this thread's pair: cells (i0 + 2m, i0 + 2m + 1) of row j0 + jr
+  const int m = tid % HP, jr = tid / HP;
+  unsigned cgi = 0;  // consumer: global index of the item's first stage
   bool failed = false;
   double dv[2] = {0.0, 0.0};
 
-  auto stage_ptr = [&](long long gi) { return smem + (gi % TMA_NS) * L::STAGE_BYTES; };
-  auto tileX = [&](long long gi) { return reinterpret_cast<const T*>(stage_ptr(gi) + L::X_OFF); };
-  auto tileR = [&](long long gi) { return reinterpret_cast<const T*>(stage_ptr(gi) + L::R_OFF); };
-  auto tileBX = [&](long long gi) { return reinterpret_cast<const T*>(stage_ptr(gi) + L::BX_OFF); };
-  auto tileBY = [&](long long gi) { return reinterpret_cast<const T*>(stage_ptr(gi) + L::BY_OFF); };
-  auto tileBZ = [&](long long gi) { return reinterpret_cast<const T*>(stage_ptr(gi) + L::BZ_OFF); };
-
-  for (int item = blockIdx.x; item < items && !failed; item += gridDim.x) {
-    const int col = item % ncol;
-    const int kb = (item / ncol) * zchunk;
-    const int ke = min(g.nz, kb + zchunk);
+  for (int n = 0; n < nmine && !failed; ++n) {
+    const int col = item_of(n) % ncol;
     const int i0 = (col % ncx) * TX, j0 = (col / ncx) * TY;
-    const int pb = kb - 2, pe = ke + 1;  // stages (planes) of this piece
-    const long long gbase = gstage;      // global index of stage pb
-    const int nst = pe - pb + 1;
-    gstage += nst;
-    auto gidx = [&](int p) { return gbase + (p - pb); };
-    auto issue = [&](int p) {  // thread 0 only
-      const long long gi = gidx(p);
-      unsigned char* st = stage_ptr(gi);
-      uint64_t* bar = &bars[gi % TMA_NS];
-      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-      mbar_expect_tx(bar, (uint32_t)(MODE == 1 ? L::TX_BYTES - L::X_BYTES : L::TX_BYTES));
-      if constexpr (MODE != 1) tma_load_3d(st + L::X_OFF, &maps.xin, i0 - 4, j0 - 2, p, bar);
-      tma_load_3d(st + L::R_OFF, &maps.rhs, i0 - 4, j0 - 1, p, bar);
-      tma_load_3d(st + L::BX_OFF, &maps.bx, i0 - 4, j0 - 1, p, bar);
-      tma_load_3d(st + L::BY_OFF, &maps.by, i0 - 4, j0 - 1, p, bar);
-      tma_load_3d(st + L::BZ_OFF, &maps.bz, i0 - 4, j0 - 1, p, bar);
-    };
+    const int kb = first_plane(n) + 2, ke = last_plane(n) - 1;
+    const unsigned gbase = cgi;
+    cgi += (unsigned)(ke - kb + 4);
+    auto stage = [&](int p) { return smem + ((gbase + (unsigned)(p - kb + 2)) % TMA_NS) * L::STAGE_BYTES; };
     auto wait = [&](int p) -> bool {
-      const long long gi = gidx(p);
-      return mbar_wait_bounded(&bars[gi % TMA_NS], (uint32_t)((gi / TMA_NS) & 1));
+      const unsigned gi = gbase + (unsigned)(p - kb + 2);
+      return mbar_wait_bounded(&bars[gi % TMA_NS], (gi / TMA_NS) & 1u);
     };
-    if (tid == 0)
-      for (int p = pb; p <= min(pe, pb + TMA_NS - 1); ++p) issue(p);
+    const int j = j0 + jr, ip = i0 + 2 * m;
 
-    // colour c0 on plane k over the tile + ring; stages k-1, k, k+1 resident
-    auto c0_plane = [&](int k) {
-      const int rs = (k + 3) % 3;
-      const bool kin = (k >= 0 && k < g.nz);
-      const T* Xm = tileX(gidx(k - 1));
-      const T* X0 = tileX(gidx(k));
-      const T* Xp = tileX(gidx(k + 1));
-      const T* Rh = tileR(gidx(k));
-      const T* Bx = tileBX(gidx(k));
-      const T* By = tileBY(gidx(k));
-      const T* Bz0 = tileBZ(gidx(k));
-      const T* Bz1 = tileBZ(gidx(k + 1));
-      for (int q = tid; q < RH * (RW / 2); q += TMA_NT) {
-        const int jj = q / (RW / 2), m = q - jj * (RW / 2);
-        const int j = j0 - 1 + jj;
-        const int ibase = i0 - 1;
-        const int ii = ((c0 - j - k - ibase) & 1) + 2 * m;
-        const int i = ibase + ii;
-        A out = (A)0;
-        if (kin && i >= 0 && i < g.nx && j >= 0 && j < g.ny) {
-          const int cr = jj * XW + ii + 3;        // rhs / bx / by / bz position
-          const int cxp = (jj + 1) * XW + ii + 3;  // xin position
-          const A wxm = Ar<A>::mul((A)Bx[cr], hx), wxp = Ar<A>::mul((A)Bx[cr + 1], hx);
-          const A wym = Ar<A>::mul((A)By[cr], hy), wyp = Ar<A>::mul((A)By[cr + XW], hy);
-          const A wzm = Ar<A>::mul((A)Bz0[cr], hz), wzp = Ar<A>::mul((A)Bz1[cr], hz);
-          const A bv = Ar<A>::add((A)Rh[cr], -sh);
-          if constexpr (MODE == 1) {
-            out = Stencil<T, T>::gs(bv, wxm, wxp, wym, wyp, wzm, wzp, (A)0, (A)0, (A)0, (A)0, (A)0, (A)0);
-          } else {
-            auto XV = [&](const T* t, int pos, int ia, int ja, int ka) -> A {
-              A v = (A)t[pos];
-              if constexpr (MODE == 2) {
-                if (ia >= 0 && ia < g.nx && ja >= 0 && ja < g.ny && ka >= 0 && ka < g.nz)
-                  v = Ar<A>::add(v, (A)xc[gc.idx(cx ? ia >> 1 : ia, cy ? ja >> 1 : ja, cz ? ka >> 1 : ka)]);
-              }
-              return v;
-            };
-            out = Stencil<T, T>::gs(bv, wxm, wxp, wym, wyp, wzm, wzp, XV(X0, cxp - 1, i - 1, j, k),
-                                    XV(X0, cxp + 1, i + 1, j, k), XV(X0, cxp - XW, i, j - 1, k),
-                                    XV(X0, cxp + XW, i, j + 1, k), XV(Xm, cxp, i, j, k - 1), XV(Xp, cxp, i, j, k + 1));
-          }
+    // Colour c0 at tile column xcol (xin tile coordinates: cell i = i0 - 4 + xcol)
+    // and tile row jt (cell j = j0 - 1 + jt) of plane k; zero outside the domain.
+    auto red_at = [&](int xcol, int jt, int k, const unsigned char* sm, const unsigned char* s0,
+                      const unsigned char* sp) -> A {
+      const int ia = i0 - 4 + xcol, ja = j0 - 1 + jt;
+      if (ia < 0 || ia >= g.nx || ja < 0 || ja >= g.ny || k < 0 || k >= g.nz) return (A)0;
+      const T* Rh = reinterpret_cast<const T*>(s0 + L::R_OFF);
+      const T* Bx = reinterpret_cast<const T*>(s0 + L::BX_OFF);
+      const T* By = reinterpret_cast<const T*>(s0 + L::BY_OFF);
+      const T* Bz0 = reinterpret_cast<const T*>(s0 + L::BZ_OFF);
+      const T* Bz1 = reinterpret_cast<const T*>(sp + L::BZ_OFF);
+      const int cr = jt * XW + xcol;
+      const A bv = Ar<A>::add((A)Rh[cr], -sh);
+      const A wxm = (A)Bx[cr], wxp = (A)Bx[cr + 1], wym = (A)By[cr], wyp = (A)By[cr + XW];
+      const A wzm = (A)Bz0[cr], wzp = (A)Bz1[cr];
+      if constexpr (MODE == 1) {
+        return Stencil<T, T>::gs(bv, wxm, wxp, wym, wyp, wzm, wzp, (A)0, (A)0, (A)0, (A)0, (A)0, (A)0);
+      } else {
+        const T* Xm = reinterpret_cast<const T*>(sm + L::X_OFF);
+        const T* X0 = reinterpret_cast<const T*>(s0 + L::X_OFF);
+        const T* Xp = reinterpret_cast<const T*>(sp + L::X_OFF);
+        const int cp = cr + XW;  // xin rows start one row lower
+        A n0 = (A)X0[cp - 1], n1 = (A)X0[cp + 1], n2 = (A)X0[cp - XW], n3 = (A)X0[cp + XW];
+        A n4 = (A)Xm[cp], n5 = (A)Xp[cp];
+        if constexpr (MODE == 2) {
+          // prolongation of the coarse correction, added to each neighbour
+          auto P = [&](A v, int ib, int jb, int kc) -> A {
+            if (ib < 0 || ib >= g.nx || jb < 0 || jb >= g.ny || kc < 0 || kc >= g.nz) return v;
+            return Ar<A>::add(v, (A)xc[gc.idx(cx ? ib >> 1 : ib, cy ? jb >> 1 : jb, cz ? kc >> 1 : kc)]);
+          };
+          n0 = P(n0, ia - 1, ja, k); n1 = P(n1, ia + 1, ja, k);
+          n2 = P(n2, ia, ja - 1, k); n3 = P(n3, ia, ja + 1, k);
+          n4 = P(n4, ia, ja, k - 1); n5 = P(n5, ia, ja, k + 1);
         }
-        Rs[rs][jj][ii] = out;
+        return Stencil<T, T>::gs(bv, wxm, wxp, wym, wyp, wzm, wzp, n0, n1, n2, n3, n4, n5);
       }
     };
 
-    // the march: c0 on planes kb-1 .. ke, c1 on kb .. ke-1
-    int kfail = 0;
-    for (int k = kb - 1; k <= ke && !failed; ++k) {
-      // stages k-1, k, k+1 must have landed (k-1 and k were waited before)
-      const int need_lo = (k == kb - 1) ? k - 1 : k + 1;
-      for (int p = need_lo; p <= k + 1; ++p)
-        if (!wait(p)) failed = true;
-      if (failed) { kfail = k; break; }
-      c0_plane(k);
-      __syncthreads();
+    A red_prev = (A)0;
+    for (int k = kb - 1; k <= ke; ++k) {
+      bool ok = true;
+      if (k == kb - 1) ok = wait(k - 1) && wait(k);
+      ok = ok && wait(k + 1);
+      const unsigned char* sm = stage(k - 1);
+      const unsigned char* s0 = stage(k);
+      const unsigned char* sp = stage(k + 1);
+      A (*Rk)[RW] = Rs[(k + 4) & 3];
+      // main: the colour-c0 cell of this thread's pair
+      const int e = (c0 + j + k) & 1;
+      const A rk = red_at(2 * m + e + 4, jr + 1, k, sm, s0, sp);
+      Rk[jr + 1][2 * m + e + 1] = rk;
+      // ring: rows j0-1 and j0+TY (HP+1 cells each), columns i0-1 and i0+TX (TY/2 each)
+      if (tid < L::NRING) {
+        int rc, rr;  // ring cell in result coordinates (column i - (i0-1), row j - (j0-1))
+        if (tid < 2 * (HP + 1)) {
+          rr = tid < HP + 1 ? 0 : TY + 1;
+          const int t = tid < HP + 1 ? tid : tid - (HP + 1);
+          rc = ((c0 + 1 + j0 - 1 + rr + k) & 1) + 2 * t;
+        } else {
+          const int t = tid - 2 * (HP + 1);
+          const bool left = t < TY / 2;
+          rc = left ? 0 : TX + 1;
+          const int tt = left ? t : t - TY / 2;
+          rr = 1 + (((left ? c0 + 1 : c0) + j0 + k) & 1) + 2 * tt;
+        }
+        Rk[rr][rc] = red_at(rc + 3, rr, k, sm, s0, sp);
+      }
+      if (__syncthreads_or(!ok)) { failed = true; break; }
+      if (tid == 0 && k >= kb) issue_next();  // stage k-2 is free
       if (k - 1 >= kb) {
-        // inline c1 (needs the DOT accumulation on rhs values)
+        // colour 1-c0 on plane kk = k-1 for this thread's pair
         const int kk = k - 1;
-        const int rs = (kk + 3) % 3;
-        const T* Rh = tileR(gidx(kk));
-        const T* Bx = tileBX(gidx(kk));
-        const T* By = tileBY(gidx(kk));
-        const T* Bz0 = tileBZ(gidx(kk));
-        const T* Bz1 = tileBZ(gidx(kk + 1));
-        for (int q = tid; q < TY * (TX / 2); q += TMA_NT) {
-          const int jj = q / (TX / 2), m = q - jj * (TX / 2);
-          const int j = j0 + jj, i = i0 + 2 * m;
-          if (j >= g.ny || i >= g.nx) continue;
-          A val[2];
-          A rv[2];
-#pragma unroll
-          for (int e = 0; e < 2; ++e) {
-            const int ie = i + e;
-            const int ri = ie - (i0 - 1), rj = jj + 1;
-            const int cr = rj * XW + (ie - i0) + 4;
-            rv[e] = (A)Rh[cr];
-            if (ie >= g.nx) { val[e] = (A)0; continue; }
-            if (((ie + j + kk) & 1) == c0) { val[e] = Rs[rs][rj][ri]; continue; }
-            const A wxm = Ar<A>::mul((A)Bx[cr], hx), wxp = Ar<A>::mul((A)Bx[cr + 1], hx);
-            const A wym = Ar<A>::mul((A)By[cr], hy), wyp = Ar<A>::mul((A)By[cr + XW], hy);
-            const A wzm = Ar<A>::mul((A)Bz0[cr], hz), wzp = Ar<A>::mul((A)Bz1[cr], hz);
-            const A bv = Ar<A>::add(rv[e], -sh);
-            val[e] = Stencil<T, T>::gs(bv, wxm, wxp, wym, wyp, wzm, wzp, Rs[rs][rj][ri - 1], Rs[rs][rj][ri + 1],
-                                       Rs[rs][rj - 1][ri], Rs[rs][rj + 1][ri], Rs[(kk + 2) % 3][rj][ri],
-                                       Rs[(kk + 4) % 3][rj][ri]);
-          }
-          const int c = g.idx(i, j, kk);
-          if (i + 1 < g.nx) {
+        const int eb = 1 - ((c0 + j + kk) & 1);
+        const int rcb = 2 * m + eb + 1;  // result coordinates of the cell
+        A (*Rm)[RW] = Rs[(kk + 3) & 3];
+        A (*R0)[RW] = Rs[(kk + 4) & 3];
+        const unsigned char* t0 = sm;  // stage kk
+        const T* Rh = reinterpret_cast<const T*>(t0 + L::R_OFF);
+        const T* Bx = reinterpret_cast<const T*>(t0 + L::BX_OFF);
+        const T* By = reinterpret_cast<const T*>(t0 + L::BY_OFF);
+        const T* Bz0 = reinterpret_cast<const T*>(t0 + L::BZ_OFF);
+        const T* Bz1 = reinterpret_cast<const T*>(s0 + L::BZ_OFF);
+        const int cr = (jr + 1) * XW + rcb + 3;
+        A blk = (A)0;
+        if (ip + eb < g.nx && j < g.ny) {
+          const A bv = Ar<A>::add((A)Rh[cr], -sh);
+          blk = Stencil<T, T>::gs(bv, (A)Bx[cr], (A)Bx[cr + 1], (A)By[cr], (A)By[cr + XW], (A)Bz0[cr], (A)Bz1[cr],
+                                  R0[jr + 1][rcb - 1], R0[jr + 1][rcb + 1], R0[jr][rcb], R0[jr + 2][rcb],
+                                  Rm[jr + 1][rcb], Rk[jr + 1][rcb]);
+        }
+        if (j < g.ny && ip < g.nx) {
+          A v0 = eb ? red_prev : blk, v1 = eb ? blk : red_prev;
+          const int c = g.idx(ip, j, kk);
+          if (ip + 1 < g.nx) {
             typename Vec2<T>::type v2;
-            v2.x = (T)val[0];
-            v2.y = (T)val[1];
+            v2.x = (T)v0;
+            v2.y = (T)v1;
             *reinterpret_cast<typename Vec2<T>::type*>(xout + c) = v2;
           } else {
-            xout[c] = (T)val[0];
+            xout[c] = (T)v0;
           }
           if constexpr (DOT) {
-#pragma unroll
-            for (int e = 0; e < 2; ++e) {
-              if (i + e < g.nx) {
-                const double zv = (double)(T)val[e];
-                dv[0] += (double)(T)rv[e] * zv;
-                dv[1] += zv;
-              }
+            const int crp = (jr + 1) * XW + 2 * m + 4;  // cell ip in tile coordinates
+            const double z0 = (double)(T)v0;
+            dv[0] += (double)Rh[crp] * z0;
+            dv[1] += z0;
+            if (ip + 1 < g.nx) {
+              const double z1 = (double)(T)v1;
+              dv[0] += (double)Rh[crp + 1] * z1;
+              dv[1] += z1;
             }
           }
         }
       }
-      __syncthreads();  // every thread is done with stage k-1 (and with Rs of plane k-2)
-      if (tid == 0 && k - 1 >= pb && k - 1 + TMA_NS <= pe) issue(k - 1 + TMA_NS);
+      red_prev = rk;
     }
     if (failed) {
-      // record the failure (the update kernel stops the solve on it; `done` is
+      // Record the failure (the update kernel stops the solve on it; `done` is
       // not set here so that every CTA still joins the reduction below), then
-      // wait, bounded, for this piece's copies in flight
-      if (tid == 0 && s) s->status = 6;
-      // only stages k-1 .. k-2+NS can have been issued and not yet consumed
-      for (int p = max(pb, kfail - 1); p <= min(pe, kfail - 2 + TMA_NS); ++p) (void)wait(p);
+      // wait, bounded, for every copy this CTA has issued and not consumed.
+      if (tid == 0) {
+        if (s) s->status = 6;
+        for (unsigned gi = gbase; gi < pgi; ++gi) (void)mbar_wait_bounded(&bars[gi % TMA_NS], (gi / TMA_NS) & 1u);
+      }
+      __syncthreads();
+      break;
     }
-    __syncthreads();
+    __syncthreads();  // stages ke-1 .. ke+1 and the result planes are free
+    if (tid == 0)
+      for (int q = 0; q < 3; ++q) issue_next();
   }
 
   if constexpr (DOT) {
     const Op ops[2] = {Op::Sum, Op::Sum};
     double out[2];
-    if (grid_reduce<2, TMA_NT>(dv, ops, red, 0, out)) {
+    if (grid_reduce<2, NT>(dv, ops, red, 0, out)) {
       if (tid == 0 && !(s->done)) {
         const double rz_new = out[0] - s->rshift * out[1];
         if (!isfinite(rz_new)) { s->status = 3; s->done = 1; }
