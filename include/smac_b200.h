@@ -82,10 +82,10 @@ typedef struct {
   double tol;             /* default 1e-8; the reference's tol_ (G_PressureSolverBase.h:40) */
   int max_iter;           /* PCG iteration cap, default 2000 (G_PCGSolver.cu:788) */
   int min_coarse;         /* a direction is halved while the result stays >= min_coarse and even
-                             (default 8; the reference's min_size_ is 6, G_GMGSolver.h:22) */
+                             (default 4; the reference's min_size_ is 6, G_GMGSolver.h:22) */
   int max_levels;         /* grids in the hierarchy including the finest, default 16 (MAX_LEVELS) */
   int nu1, nu2;           /* red-black Gauss-Seidel pre/post sweeps per level, default 2/2 */
-  int coarse_sweeps;      /* symmetric sweep pairs on the coarsest grid, default 24 */
+  int coarse_sweeps;      /* symmetric sweep pairs on the coarsest grid, default 8 */
   int check_every;        /* residual tests every check_every iterations (device side), default 1 */
   double reliable_delta;  /* MIXED: recompute the FP64 true residual when the FP32 residual has
                              fallen by this factor since the last recomputation, default 1e-2 */

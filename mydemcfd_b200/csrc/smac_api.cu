@@ -110,6 +110,7 @@ struct smac_handle {
   RedBuf red{};
   int num_sms = 148;
   bool use_tma = true;     // fused sweeps stage their tiles with the copy engine
+  int tma_ctas[2] = {1, 1};  // resident CTAs per SM of the TMA sweep: [0] FP32, [1] FP64
   Scalars* s = nullptr;    // device
   Scalars* hs = nullptr;   // pinned host mirror
   cudaGraphExec_t graph[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};  // [precision][gmg]
@@ -219,14 +220,13 @@ void launch_tma_sweep(smac_handle* h, int l, const SweepMaps& maps, T* xout, con
   const Level& Lc = h->lv[l + 1 < h->nlev ? l + 1 : l];
   // z-chunk: fewest planes per CTA, counting the 4 staged halo planes of each item
   const long long ncol = (long long)((g.nx + Lt::TX - 1) / Lt::TX) * ((g.ny + Lt::TY - 1) / Lt::TY);
-  const long long slots = 2LL * h->num_sms;
+  const long long slots = (long long)h->tma_ctas[sizeof(T) == 8 ? 1 : 0] * h->num_sms;
   int zc = g.nz;
   long long best = -1;
-  for (int cand : {64, 32, 16, 8}) {
-    const int z = std::min(cand, g.nz);
-    const long long items = ncol * ((g.nz + z - 1) / z);
-    const long long cost = ((items + slots - 1) / slots) * (z + 4);
-    if (best < 0 || cost < best) { best = cost; zc = z; }
+  for (int cand = std::min(64, g.nz); cand >= std::min(4, g.nz); --cand) {
+    const long long items = ncol * ((g.nz + cand - 1) / cand);
+    const long long cost = ((items + slots - 1) / slots) * (cand + 4);
+    if (best < 0 || cost < best) { best = cost; zc = cand; }
   }
   const long long items = ncol * ((g.nz + zc - 1) / zc);
   const int G = (int)std::max(1LL, std::min(slots, items));
@@ -546,6 +546,19 @@ void setup_tma(smac_handle* h) {
   for (cudaError_t x : es)
     if (x != cudaSuccess) e = x;
   if (e != cudaSuccess) { cudaGetLastError(); return; }
+  {
+    int n32 = 0, n64 = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n32, k_rbgs_tma<float, 0, true>, TmaTile<float>::NT,
+                                                      TmaTile<float>::SMEM_BYTES) != cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n64, k_rbgs_tma<double, 0, true>, TmaTile<double>::NT,
+                                                      TmaTile<double>::SMEM_BYTES) != cudaSuccess ||
+        n32 < 1 || n64 < 1) {
+      cudaGetLastError();
+      return;
+    }
+    h->tma_ctas[0] = n32;
+    h->tma_ctas[1] = n64;
+  }
   for (int l = 0; l < h->nlev; ++l) {
     Level& L = h->lv[l];
     const void* xa64 = l == 0 ? (const void*)h->z64 : (const void*)L.x64;
@@ -574,11 +587,11 @@ smac_status smac_default_options(smac_options* o) {
   o->stop_rule = SMAC_STOP_RELATIVE;
   o->tol = 1e-8;
   o->max_iter = 2000;
-  o->min_coarse = 8;
+  o->min_coarse = 4;
   o->max_levels = 16;
   o->nu1 = 2;
   o->nu2 = 2;
-  o->coarse_sweeps = 24;
+  o->coarse_sweeps = 8;
   o->check_every = 1;
   o->reliable_delta = 1e-2;
   o->bf16_coarse_cells = COARSE_CELLS;

@@ -460,12 +460,13 @@ __global__ void __launch_bounds__(TNT) k_dot_rz(Geom g, const T* __restrict__ r,
   const int j = blockIdx.y * TBY + threadIdx.y;
   const int k0 = blockIdx.z * kz;
   double v[2] = {0.0, 0.0};
+  const double sh = s->rshift;
   if (i < g.nx && j < g.ny) {
     const int k1 = min(k0 + kz, g.nz);
     int c = g.idx(i, j, k0);
     for (int k = k0; k < k1; ++k, c += g.ps) {
       const double zv = (double)z[c];
-      v[0] += (double)r[c] * zv;
+      v[0] += ((double)r[c] - sh) * zv;  // z is 0 off the fluid cells
       v[1] += zv;
     }
   }
@@ -473,7 +474,7 @@ __global__ void __launch_bounds__(TNT) k_dot_rz(Geom g, const T* __restrict__ r,
   double out[2];
   if (grid_reduce<2, TNT>(v, ops, red, 0, out)) {
     if (threadIdx.x == 0 && threadIdx.y == 0) {
-      const double rz_new = out[0] - s->rshift * out[1];
+      const double rz_new = out[0];
       if (!isfinite(rz_new)) { s->status = 3; s->done = 1; return; }
       if (!(rz_new > 0.0)) {
         // r.z <= 0 with r != 0 means the preconditioner lost definiteness

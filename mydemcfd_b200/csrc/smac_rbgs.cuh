@@ -57,7 +57,8 @@ __global__ void __launch_bounds__(RB_NT) k_rbgs_sweep(Geom g, const T* __restric
   const int i0 = blockIdx.x * TX, j0 = blockIdx.y * TY;
   const int z0 = blockIdx.z * zchunk;
   const int z1 = min(z0 + zchunk, g.nz);
-  const A sh = shift ? (A)(*shift) : (A)0;
+  const double shd = shift ? *shift : 0.0;
+  const A sh = (A)shd;
   auto slot = [](int k) { return (k + 3) % 3; };
 
   auto load_plane = [&](int k) {
@@ -147,7 +148,7 @@ __global__ void __launch_bounds__(RB_NT) k_rbgs_sweep(Geom g, const T* __restric
         for (int e = 0; e < 2; ++e) {
           if (i + e < g.nx) {
             const double zv = (double)(T)val[e];
-            dv[0] += (double)rhs[c + e] * zv;
+            dv[0] += ((double)rhs[c + e] - shd) * zv;
             dv[1] += zv;
           }
         }
@@ -174,7 +175,7 @@ __global__ void __launch_bounds__(RB_NT) k_rbgs_sweep(Geom g, const T* __restric
     double out[2];
     if (grid_reduce<2, RB_NT>(dv, ops, red, 0, out)) {
       if (tid == 0) {
-        const double rz_new = out[0] - s->rshift * out[1];
+        const double rz_new = out[0];
         if (!isfinite(rz_new)) { s->status = 3; s->done = 1; }
         else if (!(rz_new > 0.0)) { s->status = 2; s->done = 1; }
         else {

@@ -112,7 +112,8 @@ __global__ void __launch_bounds__(TmaTile<T>::NT, 2)
   A (*Rs)[RH][RW] = reinterpret_cast<A (*)[RH][RW]>(smem + TMA_NS * L::STAGE_BYTES);
   if (s && s->done) return;
   const int tid = threadIdx.x;
-  const A sh = shift ? (A)(*shift) : (A)0;
+  const double shd = shift ? *shift : 0.0;
+  const A sh = (A)shd;
 
   if (tid == 0) {
     for (int q = 0; q < TMA_NS; ++q) mbar_init(&bars[q], 1);
@@ -278,11 +279,11 @@ __global__ void __launch_bounds__(TmaTile<T>::NT, 2)
           if constexpr (DOT) {
             const int crp = (jr + 1) * XW + 2 * m + 4;  // cell ip in tile coordinates
             const double z0 = (double)(T)v0;
-            dv[0] += (double)Rh[crp] * z0;
+            dv[0] += ((double)Rh[crp] - shd) * z0;
             dv[1] += z0;
             if (ip + 1 < g.nx) {
               const double z1 = (double)(T)v1;
-              dv[0] += (double)Rh[crp + 1] * z1;
+              dv[0] += ((double)Rh[crp + 1] - shd) * z1;
               dv[1] += z1;
             }
           }
@@ -311,7 +312,7 @@ __global__ void __launch_bounds__(TmaTile<T>::NT, 2)
     double out[2];
     if (grid_reduce<2, NT>(dv, ops, red, 0, out)) {
       if (tid == 0 && !(s->done)) {
-        const double rz_new = out[0] - s->rshift * out[1];
+        const double rz_new = out[0];
         if (!isfinite(rz_new)) { s->status = 3; s->done = 1; }
         else if (!(rz_new > 0.0)) { s->status = 2; s->done = 1; }
         else {

@@ -353,9 +353,13 @@ def test_adjoint_dot_product():
 
 
 def test_autograd_matches_finite_differences():
+    # The unrolled projections are linear in u and the loss is quadratic, so a
+    # central difference has no truncation error for any step: a large step
+    # (1e-3 of |u|) keeps the solve tolerance's share of the difference near
+    # 1e-11 / 1e-3 = 1e-8, well inside the 1e-6 check.
     from mydemcfd_b200.autograd import StepOperator, unrolled
     case = W.vof_case(24, seed=5, ratio=100.0)
-    s = make_solver(case, tol=1e-12)
+    s = make_solver(case, tol=1e-11)
     ct, fxt, fyt, fzt = (torch.from_numpy(a).cuda() for a in (case.ct, case.fxt, case.fyt, case.fzt))
     ops = []
     for k in range(3):
@@ -373,10 +377,10 @@ def test_autograd_matches_finite_differences():
     L = loss(u)
     L.backward()
     grads = [t.grad for t in u]
-    for d in range(4):
+    for d in range(16):
         dirs = [torch.from_numpy(W.uniform_pm1(600 + 10 * d + i, int(np.prod(sh[k]))).reshape(sh[k])).cuda()
                 for i, k in enumerate("xyz")]
-        eps = 1e-6 * float(torch.sqrt(sum((t ** 2).sum() for t in u0)))
+        eps = 1e-3 * float(torch.sqrt(sum((t ** 2).sum() for t in u0)) / torch.sqrt(sum((t ** 2).sum() for t in dirs)))
         with torch.no_grad():
             lp = loss([a + eps * b for a, b in zip(u0, dirs)])
             lm = loss([a - eps * b for a, b in zip(u0, dirs)])
