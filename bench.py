@@ -120,13 +120,21 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
-def ncu_traffic():
-    """Per-launch DRAM bytes of the dominant kernel from the committed ncu summary."""
-    p = os.path.join(ROOT, "profiles", "traffic.json")
-    if os.path.exists(p):
-        with open(p) as f:
-            return json.load(f)
-    return {}
+def ncu_traffic(name="k_rbgs_tma_fp32_256.md"):
+    """Per-launch DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of
+    the dominant kernel, from the line `traffic_bytes_per_launch: N` of the
+    committed ncu summary, or None."""
+    p = os.path.join(ROOT, "profiles", name)
+    if not os.path.exists(p):
+        return None
+    with open(p) as f:
+        for line in f:
+            if "traffic_bytes_per_launch:" in line:
+                try:
+                    return float(line.split("traffic_bytes_per_launch:")[1].strip().strip("`").split()[0])
+                except (ValueError, IndexError):
+                    return None
+    return None
 
 
 # ---------------------------------------------------------------------------
@@ -293,15 +301,15 @@ def run_ours(args, ranks):
                "d2h_bytes_per_step": int(sum(t.numel() * 8 for t in host_out))}
 
     # roofline of the dominant kernel: the fused red-black sweep of the fine
-    # grid in FP32 (k_rbgs_sweep<float>), timed with CUDA events on the
+    # grid in FP32 (k_rbgs_tma<float>), timed with CUDA events on the
     # solver's stream right after the timed region
     peak, peak_kind = measured_peaks()
     step(s_mixed)
     ms_k, bytes_k = s_mixed.time_kernel(3, reps=20)
     achieved = bytes_k / (ms_k / 1e3) / 1e9
-    traffic = ncu_traffic().get("k_rbgs_sweep_f32_256")
+    traffic = ncu_traffic()
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                "traffic": traffic, "kernel": "k_rbgs_sweep<float,float,0,false>: fused red-black sweep, 256^3 grid",
+                "traffic": traffic, "kernel": "k_rbgs_tma<float,0,false>: TMA-staged fused red-black sweep, 256^3 grid",
                 "peak_kind": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else peak_kind,
                 "alg_bytes_per_launch": bytes_k, "ms_per_launch": ms_k}
     kernel_table = {}
