@@ -319,6 +319,25 @@ def run_ours(args, ranks):
         ms, b = s_mixed.time_kernel(kid, reps=10)
         kernel_table[name] = {"ms": ms, "GB/s": b / (ms / 1e3) / 1e9}
 
+    # error of each result against an FP64 solve to 1e-12 of the same input
+    # (relative 2-norm over the fluid cells, fluid mean removed)
+    fluid = torch.from_numpy(W.interior(case.ct) == W.C_INTERIOR).to(dev)
+
+    def pressure(s):
+        step(s)
+        torch.cuda.synchronize()
+        return pd[1:-1, 1:-1, 1:-1][fluid].clone()
+
+    p_mixed, p_plain = pressure(s_mixed), pressure(s_plain)
+    s_tight = B200PressureSolver(case.N, case.h, precision=nat.PRECISION_FP64, tol=1e-12)
+    s_tight.set_coefficients(g)
+    p_tight = pressure(s_tight)
+    s_tight.close()
+
+    def err(p):
+        a, b = p - p.mean(), p_tight - p_tight.mean()
+        return float(torch.linalg.norm(a - b) / torch.linalg.norm(b))
+
     launches = int(sum(s["kernel_launches"] for s in st_mixed))
     res = {
         "metric": METRIC, "value": sps_mixed, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
@@ -328,11 +347,13 @@ def run_ours(args, ranks):
                                f"correction), replicas per GPU", "grid": args.n, "tol": args.tol,
                    "l2": "working set > L2 (coefficients alone 3x139 MB at 256^3)", "parallelism": f"replicas x{world}"},
         "plain_fp64": {"value": sps_plain, "ms_per_step": ms_plain / args.steps,
-                       "iterations": st_plain[-1]["iterations"], "rel_residual": st_plain[-1]["rel_residual"]},
+                       "iterations": st_plain[-1]["iterations"], "rel_residual": st_plain[-1]["rel_residual"],
+                       "error_vs_fp64_1e-12": err(p_plain)},
         "mixed": {"iterations": st_mixed[-1]["iterations"], "reliable_updates": st_mixed[-1]["reliable_updates"],
                   "rel_residual": st_mixed[-1]["rel_residual"], "levels": st_mixed[-1]["num_levels"],
                   "alg_bytes_per_solve": st_mixed[-1]["alg_bytes"],
-                  "alg_GBps": st_mixed[-1]["alg_bytes"] * args.steps / (ms_mixed / 1e3) / 1e9},
+                  "alg_GBps": st_mixed[-1]["alg_bytes"] * args.steps / (ms_mixed / 1e3) / 1e9,
+                  "error_vs_fp64_1e-12": err(p_mixed)},
         "speedup_mixed_vs_plain": sps_mixed / sps_plain,
         "e2e": e2e,
         "gpu_launches": launches,

@@ -157,7 +157,13 @@ __global__ void __launch_bounds__(TmaTile<T>::NT, 2)
     for (int q = 0; q < TMA_NS; ++q) issue_next();
 
   // this thread's pair: cells (i0 + 2m, i0 + 2m + 1) of row j0 + jr
-  const int m = tid % HP, jr = tid / HP;
+  // A warp takes 16 pairs of each of two adjacent rows.  The colour-c0 cells
+  // of the two rows sit at opposite parities and every tile row has an even
+  // length, so the two half-warps read disjoint shared-memory banks.
+  static_assert(HP % 16 == 0 && TY % 2 == 0, "tile shape");
+  const int lane = tid & 31, wv = tid >> 5;
+  const int m = (wv % (HP / 16)) * 16 + (lane & 15);
+  const int jr = 2 * (wv / (HP / 16)) + (lane >> 4);
   unsigned cgi = 0;  // consumer: global index of the item's first stage
   bool failed = false;
   double dv[2] = {0.0, 0.0};
