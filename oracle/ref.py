@@ -34,7 +34,8 @@ class RefInputs(ctypes.Structure):
 
 class RefOutputs(ctypes.Structure):
     _fields_ = [("p_delta", _dp), ("rhs", _dp), ("vx", _dp), ("vy", _dp), ("vz", _dp), ("p", _dp),
-                ("iterations", ctypes.c_int), ("num_levels", ctypes.c_int)]
+                ("iterations", ctypes.c_int), ("num_levels", ctypes.c_int),
+                ("solve_ms", ctypes.c_double), ("correct_ms", ctypes.c_double)]
 
 
 def available() -> bool:
@@ -99,4 +100,6 @@ def solve(case, solver_type=3, tol=1e-11, levels=4, do_correct=True, eps=None, e
         raise RuntimeError(f"ref_solve returned {rc}")
     out["iterations"] = o.iterations
     out["num_levels"] = o.num_levels
+    out["solve_ms"] = o.solve_ms
+    out["correct_ms"] = o.correct_ms
     return out

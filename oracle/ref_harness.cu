@@ -75,6 +75,8 @@ struct ref_outputs {
   double *p_delta, *rhs, *vx, *vy, *vz, *p;
   int iterations;     // parsed from the reference's "PCG iter = %d" line
   int num_levels;
+  double solve_ms;    // device time of solve_poisson (CUDA events on the legacy stream)
+  double correct_ms;  // device time of correct_vof_velocity (0 without do_correct)
 };
 
 // Returns 0 on success, -1 refused shape, -2 CUDA error.
@@ -134,8 +136,18 @@ int ref_solve(const ref_inputs* in, ref_outputs* out) {
   const int fd = mkstemp(path);
   const int saved = dup(1);
   if (fd >= 0) dup2(fd, 1);
+  cudaEvent_t ev0, ev1;
+  cudaEventCreate(&ev0);
+  cudaEventCreate(&ev1);
+  cudaEventRecord(ev0, 0);
   g.solve_poisson();
+  cudaEventRecord(ev1, 0);
   cudaDeviceSynchronize();
+  {
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, ev0, ev1);
+    out->solve_ms = ms;
+  }
   fflush(stdout);
   if (fd >= 0) {
     dup2(saved, 1);
@@ -159,14 +171,22 @@ int ref_solve(const ref_inputs* in, ref_outputs* out) {
   g.gpuTocpu(solv.grid_);
   get(hg.p_delta_, out->p_delta);
   get(hg.rhs_, out->rhs);
+  out->correct_ms = 0.0;
   if (in->do_correct) {
+    cudaEventRecord(ev0, 0);
     g.correct_vof_velocity(solv);
+    cudaEventRecord(ev1, 0);
     cudaDeviceSynchronize();
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, ev0, ev1);
+    out->correct_ms = ms;
     g.gpuTocpu(solv.grid_);
     get(hg.f_vx_, out->vx); get(hg.f_vy_, out->vy); get(hg.f_vz_, out->vz);
     get(hg.p_, out->p);
   }
   e = cudaGetLastError();
+  cudaEventDestroy(ev0);
+  cudaEventDestroy(ev1);
   if (gmg) gmgs.free_levels();
   g.solver_free();
   solv.solver_free();
