@@ -315,7 +315,7 @@ def run_ours(args, ranks):
     kernel_table = {}
     for kid, name in ((0, "matvec_f64"), (1, "matvec_f32"), (2, "rbgs_sweep_f64"), (3, "rbgs_sweep_f32"),
                       (4, "true_residual_f64"), (5, "rbgs_halfsweeps_f64"), (6, "rbgs_halfsweeps_f32"),
-                      (7, "dir_matvec_f32")):
+                      (7, "dir_matvec_f32"), (8, "dir_matvec_f64"), (9, "update_f32"), (10, "update_f64")):
         ms, b = s_mixed.time_kernel(kid, reps=10)
         kernel_table[name] = {"ms": ms, "GB/s": b / (ms / 1e3) / 1e9}
 

@@ -215,7 +215,8 @@ smac_status smac_apply_A(smac_handle* h, const double* x, double* y);
  * CUDA events, on the finest grid (kernel ids: 0 FP64 matvec+dot, 1 FP32
  * matvec+dot, 2 FP64 fused red-black sweep, 3 FP32 fused red-black sweep,
  * 4 FP64 true residual, 5 FP64 sweep as two half-sweep launches, 6 FP32 sweep
- * as two half-sweep launches, 7 FP32 direction update + matvec).  Writes the
+ * as two half-sweep launches, 7 FP32 direction update + matvec, 8 FP64
+ * direction update + matvec, 9 FP32 x/r update, 10 FP64 x/r update).  Writes the
  * mean milliseconds per launch (per sweep for 5 and 6) and the algorithmic
  * bytes of one launch. */
 smac_status smac_time_kernel(smac_handle* h, int kernel_id, int reps, float* ms_per_launch,

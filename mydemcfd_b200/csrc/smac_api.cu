@@ -267,6 +267,26 @@ void launch_sweep(smac_handle* h, int l, int mode, bool dot, const T* xin, T* xo
 #undef SW
 }
 
+// d = z - zshift + beta d, q = A d, p.Ap (k_dir_matvec_vec).
+template <class T>
+void launch_dir_matvec(smac_handle* h, const Geom& g, const T* z, const T* dold, T* dnew, const Stencil<T, T>& S,
+                       T* q, int kz) {
+  constexpr int NV = Vec16<T>::n;
+  const dim3 gr((g.nx + DMV_TX * NV - 1) / (DMV_TX * NV), (g.ny + DMV_TY - 1) / DMV_TY, (g.nz + kz - 1) / kz);
+  k_dir_matvec_vec<T><<<gr, dim3(DMV_TX, DMV_TY, 1), 0, h->stream>>>(g, z, dold, dnew, S, q, h->fluid, h->red, h->s,
+                                                                     kz);
+}
+
+// x += alpha d, r -= alpha q over whole padded arrays (k_update_flat).
+template <class T>
+void launch_update(smac_handle* h, const Geom& g, T* x, const T* d, T* r, const T* q) {
+  const long long nvec = g.alloc / Vec16<T>::n;
+  const long long blocks = (nvec + UPD_NT - 1) / UPD_NT;
+  const int G = (int)std::max(1LL, std::min(4LL * h->num_sms, blocks));
+  k_update_flat<T><<<G, UPD_NT, 0, h->stream>>>(base_of(g, x), base_of(g, d), base_of(g, r), base_of(g, q), g.alloc,
+                                                h->red, h->s);
+}
+
 template <class T, class CS, class CC>
 smac_status launch_vcycle(smac_handle* h, T* r0, T* z0a, T* z0b, bool mixed, bool dot, T** z_out) {
   const smac_options& o = h->opts;
@@ -371,8 +391,8 @@ smac_status launch_iteration(smac_handle* h, bool mixed, bool gmg, int parity) {
     double* dold = parity ? h->d64b : h->d64;
     double* dnew = parity ? h->d64 : h->d64b;
     auto S = stencil<double, double>(g, h->lv[0].bx64, h->lv[0].by64, h->lv[0].bz64);
-    k_dir_matvec<double, double><<<gr, kBlock, 0, h->stream>>>(g, z, dold, dnew, S, h->q64, h->fluid, h->red, h->s, kz);
-    k_update<double, double><<<gr, kBlock, 0, h->stream>>>(g, h->x64a, dnew, h->r64, h->q64, h->red, h->s, kz);
+    launch_dir_matvec<double>(h, g, z, dold, dnew, S, h->q64, kz);
+    launch_update<double>(h, g, h->x64a, dnew, h->r64, h->q64);
     account(h, g, 7 * 8, 1);
     account(h, g, 6 * 8, 1);
     CKL();
@@ -397,8 +417,8 @@ smac_status launch_iteration(smac_handle* h, bool mixed, bool gmg, int parity) {
     float* dold = parity ? h->d32b : h->d32;
     float* dnew = parity ? h->d32 : h->d32b;
     auto S = stencil<float, float>(g, h->lv[0].bxm, h->lv[0].bym, h->lv[0].bzm);
-    k_dir_matvec<float, float><<<gr, kBlock, 0, h->stream>>>(g, z, dold, dnew, S, h->q32, h->fluid, h->red, h->s, kz);
-    k_update<float, float><<<gr, kBlock, 0, h->stream>>>(g, h->e32, dnew, h->r32, h->q32, h->red, h->s, kz);
+    launch_dir_matvec<float>(h, g, z, dold, dnew, S, h->q32, kz);
+    launch_update<float>(h, g, h->e32, dnew, h->r32, h->q32);
     auto S64 = stencil<double, double>(g, h->lv[0].bx64, h->lv[0].by64, h->lv[0].bz64);
     k_reliable<float><<<gr, kBlock, 0, h->stream>>>(g, h->x64a, h->x64b, h->e32, h->b64, S64, h->r32, h->red, h->s, kz);
     account(h, g, 7 * 4, 1);
@@ -1239,10 +1259,14 @@ smac_status smac_time_kernel(smac_handle* h, int kernel_id, int reps, float* ms,
   st.rz = 1.0;
   st.alpha = 0.0;
   st.beta = 0.0;
+  st.tol2bb = -1.0;
+  st.tol_max = -1.0;
   *h->hs = st;
   CK(cudaMemcpyAsync(h->s, h->hs, sizeof(Scalars), cudaMemcpyHostToDevice, h->stream));
-  // non-zero operands: d = b (FP64), d32 = r32 = z32 = b, so that p.Ap > 0
+  // non-zero operands: d = z = b (FP64), d32 = r32 = z32 = b, so that p.Ap > 0
   CK(cudaMemcpyAsync(base_of(g, h->d64), base_of(g, h->b64), sizeof(double) * (size_t)g.alloc, cudaMemcpyDeviceToDevice,
+                     h->stream));
+  CK(cudaMemcpyAsync(base_of(g, h->z64), base_of(g, h->b64), sizeof(double) * (size_t)g.alloc, cudaMemcpyDeviceToDevice,
                      h->stream));
   k_convert<float><<<1184, 256, 0, h->stream>>>(base_of(g, h->b64), base_of(g, h->d32), g.alloc);
   k_convert<float><<<1184, 256, 0, h->stream>>>(base_of(g, h->b64), base_of(g, h->r32), g.alloc);
@@ -1293,8 +1317,24 @@ smac_status smac_time_kernel(smac_handle* h, int kernel_id, int reps, float* ms,
       }
       case 7: {
         auto S = stencil<float, float>(g, h->lv[0].bxm, h->lv[0].bym, h->lv[0].bzm);
-        k_dir_matvec<float, float><<<grid_cells(g, kz), kBlock, 0, h->stream>>>(g, h->z32, h->d32, h->d32b, S, h->q32, h->fluid, h->red, h->s, kz);
+        launch_dir_matvec<float>(h, g, h->z32, h->d32, h->d32b, S, h->q32, kz);
         per = 7 * 4.0;
+        break;
+      }
+      case 8: {
+        auto S = stencil<double, double>(g, h->lv[0].bx64, h->lv[0].by64, h->lv[0].bz64);
+        launch_dir_matvec<double>(h, g, h->z64, h->d64, h->d64b, S, h->q64, kz);
+        per = 7 * 8.0;
+        break;
+      }
+      case 9: {
+        launch_update<float>(h, g, h->e32, h->d32, h->r32, h->q32);
+        per = 6 * 4.0;
+        break;
+      }
+      case 10: {
+        launch_update<double>(h, g, h->tmp64, h->d64, h->r64, h->q64);
+        per = 6 * 8.0;
         break;
       }
       case 4: {

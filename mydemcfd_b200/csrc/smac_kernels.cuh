@@ -342,53 +342,82 @@ __global__ void __launch_bounds__(TNT) k_matvec_pap(Geom g, const T* __restrict_
 // stopping test.  In mixed precision x is the FP32 increment since the last
 // FP64 recomputation (reset to alpha d after one) and a small enough
 // residual requests an FP64 recomputation instead of stopping.
-template <class T, class TX>
-__global__ void __launch_bounds__(TNT) k_update(Geom g, TX* x, const T* __restrict__ d, T* r, const T* __restrict__ q,
-                                                RedBuf red, Scalars* s, int kz) {
+// The scalar bookkeeping of the update, run by one thread of the last block:
+// iteration count, the running mean of r (subtracted on the fly by the
+// V-cycle), ||r||^2 of the de-meaned residual, max|r| and the stopping test.
+__device__ __forceinline__ void update_finish(Scalars* s, const double (&out)[3]) {
+  if (s->status == 6) { s->done = 1; return; }  // a copy-engine wait expired in a sweep
+  s->iter += 1;
+  s->e_reset = 0;
+  const double m = out[0] * s->inv_nfluid;
+  s->rshift = m;
+  const double rr = fmax(out[1] - out[0] * m, 0.0);
+  s->rr = rr;
+  s->rmax = out[2];
+  if (!isfinite(out[1])) { s->status = 3; s->done = 1; return; }
+  const bool small = (s->stop_rule == 1) ? (out[2] < s->tol_max) : (rr <= s->tol2bb);
+  if (s->mixed) {
+    if (small || rr < s->reliable_delta2 * s->rr_anchor || s->iter >= s->max_iter) s->do_reliable = 1;
+  } else if (small) {
+    s->status = 0; s->done = 1;
+  } else if (s->iter >= s->max_iter) {
+    s->status = 1; s->done = 1;
+  }
+}
+
+template <class T> struct Vec16;
+template <> struct Vec16<float> { typedef float4 type; static constexpr int n = 4; };
+template <> struct Vec16<double> { typedef double2 type; static constexpr int n = 2; };
+
+// PCG: x += alpha d, r -= alpha q, recursive residual statistics and the
+// stopping test.  In mixed precision x is the FP32 increment since the last
+// FP64 recomputation (reset to alpha d after one) and a small enough
+// residual requests an FP64 recomputation instead of stopping.
+// The update is element-wise, and d, q and r are 0 in every padding cell, so
+// the kernel streams whole padded arrays (`n` elements from the allocation
+// base) as 16-byte vectors, grid-stride, with a fixed grid for a fixed
+// reduction order.
+constexpr int UPD_NT = 256;
+template <class T>
+__global__ void __launch_bounds__(UPD_NT) k_update_flat(T* x, const T* __restrict__ d, T* r,
+                                                        const T* __restrict__ q, long long n, RedBuf red,
+                                                        Scalars* s) {
   if (s->done) return;
-  const int i = blockIdx.x * TBX + threadIdx.x;
-  const int j = blockIdx.y * TBY + threadIdx.y;
-  const int k0 = blockIdx.z * kz;
-  const double alpha_d = s->alpha;
-  const T alpha = (T)alpha_d;
+  typedef typename Vec16<T>::type V;
+  constexpr int NV = Vec16<T>::n;
+  const T alpha = (T)s->alpha;
   const bool reset = s->e_reset;
   double v[3] = {0.0, 0.0, 0.0};
-  if (i < g.nx && j < g.ny) {
-    const int k1 = min(k0 + kz, g.nz);
-    int c = g.idx(i, j, k0);
-    for (int k = k0; k < k1; ++k, c += g.ps) {
-      const T dv = d[c];
-      if (reset) x[c] = (TX)(alpha * dv);
-      else x[c] = x[c] + (TX)(alpha * dv);
-      const T rn = r[c] - alpha * q[c];
-      r[c] = rn;
-      v[0] += (double)rn;
-      v[1] += (double)rn * (double)rn;
-      v[2] = fmax(v[2], fabs((double)rn));
+  const long long nvec = n / NV;
+  const long long stride = (long long)gridDim.x * UPD_NT;
+  V* xv = reinterpret_cast<V*>(x);
+  V* rv = reinterpret_cast<V*>(r);
+  const V* dv = reinterpret_cast<const V*>(d);
+  const V* qv = reinterpret_cast<const V*>(q);
+  for (long long t = blockIdx.x * (long long)UPD_NT + threadIdx.x; t < nvec; t += stride) {
+    const V dd = dv[t], qq = qv[t];
+    V rr = rv[t];
+    V xx;
+    if (!reset) xx = xv[t];
+    T* xs = reinterpret_cast<T*>(&xx);
+    T* rs = reinterpret_cast<T*>(&rr);
+    const T* ds = reinterpret_cast<const T*>(&dd);
+    const T* qs = reinterpret_cast<const T*>(&qq);
+#pragma unroll
+    for (int e = 0; e < NV; ++e) {
+      xs[e] = reset ? alpha * ds[e] : xs[e] + alpha * ds[e];
+      rs[e] = rs[e] - alpha * qs[e];
+      v[0] += (double)rs[e];
+      v[1] += (double)rs[e] * (double)rs[e];
+      v[2] = fmax(v[2], fabs((double)rs[e]));
     }
+    xv[t] = xx;
+    rv[t] = rr;
   }
   const Op ops[3] = {Op::Sum, Op::Sum, Op::Max};
   double out[3];
-  if (grid_reduce<3, TNT>(v, ops, red, 0, out)) {
-    if (threadIdx.x == 0 && threadIdx.y == 0) {
-      if (s->status == 6) { s->done = 1; return; }  // a copy-engine wait expired in a sweep
-      s->iter += 1;
-      s->e_reset = 0;
-      const double m = out[0] * s->inv_nfluid;
-      s->rshift = m;
-      const double rr = fmax(out[1] - out[0] * m, 0.0);
-      s->rr = rr;
-      s->rmax = out[2];
-      if (!isfinite(out[1])) { s->status = 3; s->done = 1; return; }
-      const bool small = (s->stop_rule == 1) ? (out[2] < s->tol_max) : (rr <= s->tol2bb);
-      if (s->mixed) {
-        if (small || rr < s->reliable_delta2 * s->rr_anchor || s->iter >= s->max_iter) s->do_reliable = 1;
-      } else if (small) {
-        s->status = 0; s->done = 1;
-      } else if (s->iter >= s->max_iter) {
-        s->status = 1; s->done = 1;
-      }
-    }
+  if (grid_reduce<3, UPD_NT>(v, ops, red, 0, out)) {
+    if (threadIdx.x == 0) update_finish(s, out);
   }
 }
 

@@ -241,6 +241,124 @@ __global__ void __launch_bounds__(TNT) k_dir_matvec(Geom g, const T* __restrict_
   }
 }
 
+// The same operation with each thread on 16 bytes of consecutive cells of
+// one row (4 FP32 or 2 FP64), marching kz planes: rows and planes move as
+// 16-byte vectors, x-neighbours across the vector edge come from the
+// adjacent lanes (lanes 0 and 31 load them), and the per-cell arithmetic is
+// that of k_dir_matvec.
+constexpr int DMV_TX = 32, DMV_TY = 4;
+template <class T>
+__global__ void __launch_bounds__(DMV_TX * DMV_TY) k_dir_matvec_vec(Geom g, const T* __restrict__ z,
+                                                                    const T* __restrict__ d_old, T* __restrict__ d_new,
+                                                                    Stencil<T, T> S, T* __restrict__ q,
+                                                                    const uint8_t* __restrict__ fluid, RedBuf red,
+                                                                    Scalars* s, int kz) {
+  if (s->done) return;
+  typedef acc_t<T> A;
+  typedef typename Vec16<T>::type V;
+  constexpr int NV = Vec16<T>::n;
+  const int lane = threadIdx.x;
+  const int i0 = (blockIdx.x * DMV_TX + lane) * NV;
+  const int j = blockIdx.y * DMV_TY + threadIdx.y;
+  const int k0 = blockIdx.z * kz;
+  const A beta = (A)s->beta;
+  const A zs = (A)s->zshift;
+  double v[1] = {0.0};
+  // rows of this warp are uniform: the whole warp is in or out of the grid in j
+  const bool row_in = j < g.ny;
+  const bool any_in = i0 < g.nx;
+  if (row_in && __any_sync(0xffffffffu, any_in)) {
+    const int k1 = min(k0 + kz, g.nz);
+    // lanes past the padded row read a valid vector of it and store nothing
+    // (the lane after the last one in the grid still reads its own vector:
+    // its first element is the neighbour of cell nx-1)
+    int c = g.idx(i0 < g.px ? i0 : g.px - NV, j, k0);
+    auto Dv = [&](int cc, A (&o)[NV]) {
+      const V zz = *reinterpret_cast<const V*>(z + cc);
+      const V dd = *reinterpret_cast<const V*>(d_old + cc);
+      const T* zp = reinterpret_cast<const T*>(&zz);
+      const T* dp = reinterpret_cast<const T*>(&dd);
+#pragma unroll
+      for (int e = 0; e < NV; ++e) o[e] = Ar<A>::fma(beta, (A)dp[e], Ar<A>::add((A)zp[e], -zs));
+    };
+    auto Ds = [&](int cc) -> A { return Ar<A>::fma(beta, (A)d_old[cc], Ar<A>::add((A)z[cc], -zs)); };
+    A xm[NV], xc[NV], xp[NV];
+    Dv(c - g.ps, xm);
+    Dv(c, xc);
+    V bzc = *reinterpret_cast<const V*>(S.bz + c);
+    for (int k = k0; k < k1; ++k, c += g.ps) {
+      Dv(c + g.ps, xp);
+      A ym[NV], yp[NV];
+      Dv(c - g.px, ym);
+      Dv(c + g.px, yp);
+      const V bxv = *reinterpret_cast<const V*>(S.bx + c);
+      const V byv = *reinterpret_cast<const V*>(S.by + c);
+      const V byu = *reinterpret_cast<const V*>(S.by + c + g.px);
+      const V bzu = *reinterpret_cast<const V*>(S.bz + c + g.ps);
+      const T* bxs = reinterpret_cast<const T*>(&bxv);
+      const T* bys = reinterpret_cast<const T*>(&byv);
+      const T* byus = reinterpret_cast<const T*>(&byu);
+      const T* bzs = reinterpret_cast<const T*>(&bzc);
+      const T* bzus = reinterpret_cast<const T*>(&bzu);
+      uint8_t fl[NV];
+#pragma unroll
+      for (int e = 0; e < NV; ++e) fl[e] = fluid[c + e];
+      // centre values with the fluid mask applied, as stored in d_new
+      A xcm[NV];
+#pragma unroll
+      for (int e = 0; e < NV; ++e) xcm[e] = (fl[e] & 2) ? xc[e] : (A)0;
+      // x-neighbours across the vector edge (the unmasked D, as k_dir_matvec reads them)
+      A left = __shfl_up_sync(0xffffffffu, xc[NV - 1], 1);
+      A right = __shfl_down_sync(0xffffffffu, xc[0], 1);
+      T bxr = __shfl_down_sync(0xffffffffu, bxs[0], 1);
+      if (lane == 0) left = Ds(c - 1);
+      if (lane == DMV_TX - 1) {
+        right = Ds(c + NV);
+        bxr = S.bx[c + NV];
+      }
+      A y[NV];
+#pragma unroll
+      for (int e = 0; e < NV; ++e) {
+        const A wxm = (A)bxs[e], wxp = (A)(e + 1 < NV ? bxs[e + 1] : bxr);
+        const A nl = e > 0 ? xc[e - 1] : left, nr = e + 1 < NV ? xc[e + 1] : right;
+        y[e] = Stencil<T, T>::apply(xcm[e], wxm, wxp, (A)bys[e], (A)byus[e], (A)bzs[e], (A)bzus[e], nl, nr, ym[e], yp[e],
+                                    xm[e], xp[e]);
+      }
+      if (any_in) {
+        V dn, qn;
+        T* dns = reinterpret_cast<T*>(&dn);
+        T* qns = reinterpret_cast<T*>(&qn);
+#pragma unroll
+        for (int e = 0; e < NV; ++e) {
+          const bool in = i0 + e < g.nx;
+          dns[e] = in ? (T)xcm[e] : (T)0;
+          qns[e] = in ? (T)y[e] : (T)0;
+          if (in) v[0] += (double)dns[e] * (double)qns[e];
+        }
+        *reinterpret_cast<V*>(d_new + c) = dn;
+        *reinterpret_cast<V*>(q + c) = qn;
+      }
+#pragma unroll
+      for (int e = 0; e < NV; ++e) {
+        xm[e] = xcm[e];
+        xc[e] = xp[e];
+      }
+      bzc = bzu;
+    }
+  }
+  const Op ops[1] = {Op::Sum};
+  double out[1];
+  if (grid_reduce<1, DMV_TX * DMV_TY>(v, ops, red, 0, out)) {
+    if (threadIdx.x == 0 && threadIdx.y == 0) {
+      const double pAp = out[0];
+      s->pAp = pAp;
+      if (!isfinite(pAp)) { s->status = 3; s->done = 1; }
+      else if (!(pAp > 0.0)) { s->status = 2; s->done = 1; }
+      else s->alpha = s->rz / pAp;
+    }
+  }
+}
+
 // Number of interior cells where a and b differ bitwise (self-test).
 template <class T>
 __global__ void k_count_mismatch(Geom g, const T* __restrict__ a, const T* __restrict__ b, unsigned long long* cnt) {
