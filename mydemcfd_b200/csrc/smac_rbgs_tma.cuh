@@ -28,7 +28,10 @@
 
 namespace smac {
 
-constexpr int TMA_NS = 5;        // stages in the ring
+#ifndef SMAC_TMA_NS
+#define SMAC_TMA_NS 5
+#endif
+constexpr int TMA_NS = SMAC_TMA_NS;  // stages in the ring
 constexpr long long TMA_WAIT_CYCLES = 2000000000LL;  // ~1 s of SM clock before a wait gives up
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
