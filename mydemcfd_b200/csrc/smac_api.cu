@@ -323,8 +323,12 @@ smac_status launch_vcycle(smac_handle* h, T* r0, T* z0a, T* z0b, bool mixed, boo
     CKL();
     const Level& Lc = h->lv[l + 1];
     auto S = stencil<T, CS>(g, CF(l, 0), CF(l, 1), CF(l, 2));
-    k_resid_restrict<T, CS><<<grid_planes(Lc.g.nx, Lc.g.ny, Lc.g.nz), kBlock, 0, h->stream>>>(
-        g, cur[l], B(l), sh, S, Lc.g, Lc.cx, Lc.cy, Lc.cz, B(l + 1), h->s);
+    if (std::is_same<T, CS>::value && Lc.cx && Lc.cy && Lc.cz)
+      k_resid_restrict2<T><<<grid_planes(Lc.g.nx, Lc.g.ny, Lc.g.nz), kBlock, 0, h->stream>>>(
+          g, cur[l], B(l), sh, stencil<T, T>(g, CF(l, 0), CF(l, 1), CF(l, 2)), Lc.g, B(l + 1), h->s);
+    else
+      k_resid_restrict<T, CS><<<grid_planes(Lc.g.nx, Lc.g.ny, Lc.g.nz), kBlock, 0, h->stream>>>(
+          g, cur[l], B(l), sh, S, Lc.g, Lc.cx, Lc.cy, Lc.cz, B(l + 1), h->s);
     account(h, g, 2 * s + 3 * sc + s / 8, 1);
     CKL();
   }

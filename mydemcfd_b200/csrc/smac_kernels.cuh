@@ -365,6 +365,9 @@ __device__ __forceinline__ void update_finish(Scalars* s, const double (&out)[3]
   }
 }
 
+template <class T> struct Vec2;
+template <> struct Vec2<double> { typedef double2 type; };
+template <> struct Vec2<float> { typedef float2 type; };
 template <class T> struct Vec16;
 template <> struct Vec16<float> { typedef float4 type; static constexpr int n = 4; };
 template <> struct Vec16<double> { typedef double2 type; static constexpr int n = 2; };
@@ -685,6 +688,83 @@ __global__ void __launch_bounds__(TNT) k_resid_restrict(Geom g, const T* __restr
         acc = Ar<A>::add(acc, Ar<A>::add(bv, -ax));
       }
   rhs_c[gc.idx(I, J, K)] = (T)Ar<A>::div(acc, (A)(rx * ry * rz));
+}
+
+// The same for a coarse grid halved in every direction: each thread reads its
+// 2x2x2 block's rows, the rows and planes around it and the faces once, as
+// 2-vectors of cells (i = 2I, 2I+1), and sums the eight residuals in the
+// order of k_resid_restrict.
+template <class T>
+__global__ void __launch_bounds__(TNT) k_resid_restrict2(Geom g, const T* __restrict__ x, const T* __restrict__ rhs,
+                                                         const double* shift, Stencil<T, T> S, Geom gc, T* rhs_c,
+                                                         const Scalars* s) {
+  if (s && s->done) return;
+  typedef acc_t<T> A;
+  typedef typename Vec2<T>::type V2;
+  const int I = blockIdx.x * TBX + threadIdx.x;
+  const int J = blockIdx.y * TBY + threadIdx.y;
+  const int K = blockIdx.z;
+  if (I >= gc.nx || J >= gc.ny || K >= gc.nz) return;
+  const A sh = shift ? (A)(*shift) : (A)0;
+  const int i = 2 * I, j = 2 * J, k = 2 * K;
+  auto ld2 = [&](const T* p, int c, A& a, A& b) {
+    const V2 v = *reinterpret_cast<const V2*>(p + c);
+    a = (A)v.x;
+    b = (A)v.y;
+  };
+  // x: rows j-1 .. j+2 on planes k, k+1; planes k-1, k+2 on rows j, j+1
+  A xr[2][4][2], xz[2][2][2], xl[2][2], xh[2][2];
+#pragma unroll
+  for (int dk = 0; dk < 2; ++dk) {
+#pragma unroll
+    for (int r = 0; r < 4; ++r) ld2(x, g.idx(i, j - 1 + r, k + dk), xr[dk][r][0], xr[dk][r][1]);
+#pragma unroll
+    for (int dj = 0; dj < 2; ++dj) {
+      const int c = g.idx(i, j + dj, k + dk);
+      xl[dk][dj] = (A)x[c - 1];
+      xh[dk][dj] = (A)x[c + 2];
+    }
+  }
+#pragma unroll
+  for (int dj = 0; dj < 2; ++dj) {
+    ld2(x, g.idx(i, j + dj, k - 1), xz[0][dj][0], xz[0][dj][1]);
+    ld2(x, g.idx(i, j + dj, k + 2), xz[1][dj][0], xz[1][dj][1]);
+  }
+  A acc = (A)0;
+#pragma unroll
+  for (int dk = 0; dk < 2; ++dk) {
+#pragma unroll
+    for (int dj = 0; dj < 2; ++dj) {
+      const int c = g.idx(i, j + dj, k + dk);
+      A b0, b1, bx0, bx1, by0, by1, bu0, bu1, bz0, bz1, bw0, bw1;
+      ld2(rhs, c, b0, b1);
+      ld2(S.bx, c, bx0, bx1);
+      const A bx2 = (A)S.bx[c + 2];
+      ld2(S.by, c, by0, by1);
+      ld2(S.by, c + g.px, bu0, bu1);
+      ld2(S.bz, c, bz0, bz1);
+      ld2(S.bz, c + g.ps, bw0, bw1);
+      // z-neighbours of this row: plane below and above
+      const A* zm = dk == 0 ? xz[0][dj] : xr[0][1 + dj];
+      const A* zp = dk == 0 ? xr[1][1 + dj] : xz[1][dj];
+      const A* row = xr[dk][1 + dj];
+#pragma unroll
+      for (int di = 0; di < 2; ++di) {
+        const A wxm = di ? bx1 : bx0, wxp = di ? bx2 : bx1;
+        const A wym = di ? by1 : by0, wyp = di ? bu1 : bu0;
+        const A wzm = di ? bz1 : bz0, wzp = di ? bw1 : bw0;
+        const A diag = Stencil<T, T>::diag(wxm, wxp, wym, wyp, wzm, wzp);
+        A bv = di ? b1 : b0;
+        if (diag > (A)0) bv = Ar<A>::add(bv, -sh);
+        const A xw = di ? row[0] : xl[dk][dj];
+        const A xe = di ? xh[dk][dj] : row[1];
+        const A ax = Stencil<T, T>::apply(row[di], wxm, wxp, wym, wyp, wzm, wzp, xw, xe, xr[dk][dj][di],
+                                          xr[dk][2 + dj][di], zm[di], zp[di]);
+        acc = Ar<A>::add(acc, Ar<A>::add(bv, -ax));
+      }
+    }
+  }
+  rhs_c[gc.idx(I, J, K)] = (T)Ar<A>::div(acc, (A)8);
 }
 
 // ------------------------------------------------------------------------

@@ -35,9 +35,6 @@ constexpr int RB_NT = 256;
 // tile height: 16 rows for FP32, 8 for FP64 (static shared memory < 48 KB)
 template <class T> struct RbTile { static constexpr int TY = sizeof(T) == 8 ? 8 : 16; };
 
-template <class T> struct Vec2;
-template <> struct Vec2<double> { typedef double2 type; };
-template <> struct Vec2<float> { typedef float2 type; };
 
 template <class T, class C, int MODE, bool DOT>
 __global__ void __launch_bounds__(RB_NT) k_rbgs_sweep(Geom g, const T* __restrict__ xin, T* __restrict__ xout,

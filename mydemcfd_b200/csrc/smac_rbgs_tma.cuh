@@ -103,6 +103,14 @@ struct SweepMaps {
   CUtensorMap xin, rhs, bx, by, bz;
 };
 
+// The coarse-grid values the prolongation adds to the six neighbours of one
+// fine cell on a grid halved in every direction: the cell's parent, and the
+// parent's neighbour in x, y and z on the side the cell's parity selects.
+template <class A>
+struct Coarse4 {
+  A c, x, y, z;
+};
+
 template <class T, int MODE, bool DOT>
 __global__ void __launch_bounds__(TmaTile<T>::NT, 2)
     k_rbgs_tma(const __grid_constant__ SweepMaps maps, Geom g, T* __restrict__ xout, const double* shift, int c0,
@@ -187,7 +195,7 @@ __global__ void __launch_bounds__(TmaTile<T>::NT, 2)
     // Colour c0 at tile column xcol (xin tile coordinates: cell i = i0 - 4 + xcol)
     // and tile row jt (cell j = j0 - 1 + jt) of plane k; zero outside the domain.
     auto red_at = [&](int xcol, int jt, int k, const unsigned char* sm, const unsigned char* s0,
-                      const unsigned char* sp) -> A {
+                      const unsigned char* sp, const Coarse4<A>& cv) -> A {
       const int ia = i0 - 4 + xcol, ja = j0 - 1 + jt;
       if (ia < 0 || ia >= g.nx || ja < 0 || ja >= g.ny || k < 0 || k >= g.nz) return (A)0;
       const T* Rh = reinterpret_cast<const T*>(s0 + L::R_OFF);
@@ -210,17 +218,72 @@ __global__ void __launch_bounds__(TmaTile<T>::NT, 2)
         A n4 = (A)Xm[cp], n5 = (A)Xp[cp];
         if constexpr (MODE == 2) {
           // prolongation of the coarse correction, added to each neighbour
-          auto P = [&](A v, int ib, int jb, int kc) -> A {
-            if (ib < 0 || ib >= g.nx || jb < 0 || jb >= g.ny || kc < 0 || kc >= g.nz) return v;
-            return Ar<A>::add(v, (A)xc[gc.idx(cx ? ib >> 1 : ib, cy ? jb >> 1 : jb, cz ? kc >> 1 : kc)]);
-          };
-          n0 = P(n0, ia - 1, ja, k); n1 = P(n1, ia + 1, ja, k);
-          n2 = P(n2, ia, ja - 1, k); n3 = P(n3, ia, ja + 1, k);
-          n4 = P(n4, ia, ja, k - 1); n5 = P(n5, ia, ja, k + 1);
+          if (cx && cy && cz) {
+            // Halved in every direction: three neighbours share the cell's
+            // coarse parent, the other three are the parent's neighbours
+            // on the side the cell's parity selects.  A neighbour outside
+            // the domain maps to a coarse ghost, which holds 0, like the
+            // neighbour itself: no bounds test is needed.
+            // (the values were loaded one step ahead, coarse4 below)
+            const A c0v = cv.c, cxv = cv.x, cyv = cv.y, czv = cv.z;
+            n0 = Ar<A>::add(n0, (ia & 1) ? c0v : cxv);
+            n1 = Ar<A>::add(n1, (ia & 1) ? cxv : c0v);
+            n2 = Ar<A>::add(n2, (ja & 1) ? c0v : cyv);
+            n3 = Ar<A>::add(n3, (ja & 1) ? cyv : c0v);
+            n4 = Ar<A>::add(n4, (k & 1) ? c0v : czv);
+            n5 = Ar<A>::add(n5, (k & 1) ? czv : c0v);
+          } else {
+            auto P = [&](A v, int ib, int jb, int kc) -> A {
+              if (ib < 0 || ib >= g.nx || jb < 0 || jb >= g.ny || kc < 0 || kc >= g.nz) return v;
+              return Ar<A>::add(v, (A)xc[gc.idx(cx ? ib >> 1 : ib, cy ? jb >> 1 : jb, cz ? kc >> 1 : kc)]);
+            };
+            n0 = P(n0, ia - 1, ja, k); n1 = P(n1, ia + 1, ja, k);
+            n2 = P(n2, ia, ja - 1, k); n3 = P(n3, ia, ja + 1, k);
+            n4 = P(n4, ia, ja, k - 1); n5 = P(n5, ia, ja, k + 1);
+          }
         }
         return Stencil<T, T>::gs(bv, wxm, wxp, wym, wyp, wzm, wzp, n0, n1, n2, n3, n4, n5);
       }
     };
+
+    // Coarse values of a fine cell (MODE 2 on a grid halved in every
+    // direction), loaded from L2 one step before the cell's update so that
+    // the loads overlap the barrier and the colour-(1-c0) pass.
+    const bool pro4 = MODE == 2 && cx && cy && cz;
+    auto coarse4 = [&](int ia, int ja, int k) -> Coarse4<A> {
+      Coarse4<A> q{(A)0, (A)0, (A)0, (A)0};
+      if (pro4 && (unsigned)ia < (unsigned)g.nx && (unsigned)ja < (unsigned)g.ny && (unsigned)k < (unsigned)g.nz) {
+        const T* C = xc + gc.idx(ia >> 1, ja >> 1, k >> 1);
+        q.c = (A)C[0];
+        q.x = (A)C[(ia & 1) ? 1 : -1];
+        q.y = (A)C[(ja & 1) ? gc.px : -gc.px];
+        q.z = (A)C[(k & 1) ? gc.ps : -gc.ps];
+      }
+      return q;
+    };
+    // the ring cell (tile coordinates) of this thread on plane k
+    auto ring_cell = [&](int k, int& rc, int& rr) {
+      if (tid < 2 * (HP + 1)) {
+        rr = tid < HP + 1 ? 0 : TY + 1;
+        const int t = tid < HP + 1 ? tid : tid - (HP + 1);
+        rc = ((c0 + 1 + j0 - 1 + rr + k) & 1) + 2 * t;
+      } else {
+        const int t = tid - 2 * (HP + 1);
+        const bool left = t < TY / 2;
+        rc = left ? 0 : TX + 1;
+        const int tt = left ? t : t - TY / 2;
+        rr = 1 + (((left ? c0 + 1 : c0) + j0 + k) & 1) + 2 * tt;
+      }
+    };
+    Coarse4<A> cm{}, cr4{};
+    if (pro4) {
+      cm = coarse4(ip + ((c0 + j + kb - 1) & 1), j, kb - 1);
+      if (tid < L::NRING) {
+        int rc, rr;
+        ring_cell(kb - 1, rc, rr);
+        cr4 = coarse4(i0 - 1 + rc, j0 - 1 + rr, kb - 1);
+      }
+    }
 
     A red_prev = (A)0;
     for (int k = kb - 1; k <= ke; ++k) {
@@ -233,23 +296,21 @@ __global__ void __launch_bounds__(TmaTile<T>::NT, 2)
       A (*Rk)[RW] = Rs[(k + 4) & 3];
       // main: the colour-c0 cell of this thread's pair
       const int e = (c0 + j + k) & 1;
-      const A rk = red_at(2 * m + e + 4, jr + 1, k, sm, s0, sp);
+      const A rk = red_at(2 * m + e + 4, jr + 1, k, sm, s0, sp, cm);
       Rk[jr + 1][2 * m + e + 1] = rk;
       // ring: rows j0-1 and j0+TY (HP+1 cells each), columns i0-1 and i0+TX (TY/2 each)
       if (tid < L::NRING) {
         int rc, rr;  // ring cell in result coordinates (column i - (i0-1), row j - (j0-1))
-        if (tid < 2 * (HP + 1)) {
-          rr = tid < HP + 1 ? 0 : TY + 1;
-          const int t = tid < HP + 1 ? tid : tid - (HP + 1);
-          rc = ((c0 + 1 + j0 - 1 + rr + k) & 1) + 2 * t;
-        } else {
-          const int t = tid - 2 * (HP + 1);
-          const bool left = t < TY / 2;
-          rc = left ? 0 : TX + 1;
-          const int tt = left ? t : t - TY / 2;
-          rr = 1 + (((left ? c0 + 1 : c0) + j0 + k) & 1) + 2 * tt;
+        ring_cell(k, rc, rr);
+        Rk[rr][rc] = red_at(rc + 3, rr, k, sm, s0, sp, cr4);
+      }
+      if (pro4 && k + 1 <= ke) {  // next plane's coarse values
+        cm = coarse4(ip + ((c0 + j + k + 1) & 1), j, k + 1);
+        if (tid < L::NRING) {
+          int rc, rr;
+          ring_cell(k + 1, rc, rr);
+          cr4 = coarse4(i0 - 1 + rc, j0 - 1 + rr, k + 1);
         }
-        Rk[rr][rc] = red_at(rc + 3, rr, k, sm, s0, sp);
       }
       if (__syncthreads_or(!ok)) { failed = true; break; }
       if (tid == 0 && k >= kb) issue_next();  // stage k-2 is free
