@@ -267,6 +267,13 @@ void launch_sweep(smac_handle* h, int l, int mode, bool dot, const T* xin, T* xo
 #undef SW
 }
 
+// Mixed precision: the FP64 true residual and reliable update (k_reliable_vec).
+void launch_reliable(smac_handle* h, const Geom& g, const Stencil<double, double>& S64, int kz) {
+  const dim3 gr((g.nx + 2 * REL_TX - 1) / (2 * REL_TX), (g.ny + REL_TY - 1) / REL_TY, (g.nz + kz - 1) / kz);
+  k_reliable_vec<float><<<gr, dim3(REL_TX, REL_TY, 1), 0, h->stream>>>(g, h->x64a, h->x64b, h->e32, h->b64, S64,
+                                                                       h->r32, h->red, h->s, kz);
+}
+
 // d = z - zshift + beta d, q = A d, p.Ap (k_dir_matvec_vec).
 template <class T>
 void launch_dir_matvec(smac_handle* h, const Geom& g, const T* z, const T* dold, T* dnew, const Stencil<T, T>& S,
@@ -424,7 +431,7 @@ smac_status launch_iteration(smac_handle* h, bool mixed, bool gmg, int parity) {
     launch_dir_matvec<float>(h, g, z, dold, dnew, S, h->q32, kz);
     launch_update<float>(h, g, h->e32, dnew, h->r32, h->q32);
     auto S64 = stencil<double, double>(g, h->lv[0].bx64, h->lv[0].by64, h->lv[0].bz64);
-    k_reliable<float><<<gr, kBlock, 0, h->stream>>>(g, h->x64a, h->x64b, h->e32, h->b64, S64, h->r32, h->red, h->s, kz);
+    launch_reliable(h, g, S64, kz);
     account(h, g, 7 * 4, 1);
     account(h, g, 6 * 4, 1);
     h->launches += 1;  // the FP64 residual kernel (its bytes are counted when it runs)
@@ -1011,8 +1018,7 @@ smac_status run_solve(smac_handle* h, const double** xout) {
           h->hs->status = 0;
           h->hs->do_reliable = 1;
           CK(cudaMemcpyAsync(h->s, h->hs, sizeof(Scalars), cudaMemcpyHostToDevice, h->stream));
-          k_reliable<float><<<grid_cells(g, kz), kBlock, 0, h->stream>>>(g, h->x64a, h->x64b, h->e32, h->b64, S,
-                                                                         h->r32, h->red, h->s, kz);
+          launch_reliable(h, g, S, kz);
           CKL();
         } else {
           k_true_residual<<<grid_cells(g, kz), kBlock, 0, h->stream>>>(g, h->x64a, h->b64, S, h->r64, 1, h->red,

@@ -482,6 +482,114 @@ __global__ void __launch_bounds__(TNT) k_reliable(Geom g, double* x64a, double* 
   }
 }
 
+// The same with each thread on 2 consecutive cells of one row, marching kz
+// planes: FP64 rows as 16-byte vectors, x-neighbours across the pair from
+// the adjacent lanes (lanes 0 and 31 load them), per-cell arithmetic as in
+// k_reliable.
+constexpr int REL_TX = 32, REL_TY = 4;
+template <class T>
+__global__ void __launch_bounds__(REL_TX * REL_TY) k_reliable_vec(Geom g, double* x64a, double* x64b,
+                                                                  const T* __restrict__ e,
+                                                                  const double* __restrict__ b,
+                                                                  Stencil<double, double> S, T* r, RedBuf red,
+                                                                  Scalars* s, int kz) {
+  if (s->done || !s->do_reliable) return;
+  typedef typename Vec2<T>::type ET;
+  const int lane = threadIdx.x;
+  const int i0 = (blockIdx.x * REL_TX + lane) * 2;
+  const int j = blockIdx.y * REL_TY + threadIdx.y;
+  const int k0 = blockIdx.z * kz;
+  const double* __restrict__ xs = s->xbuf ? x64b : x64a;
+  double* xd = s->xbuf ? x64a : x64b;
+  double v[3] = {0.0, 0.0, 0.0};
+  const bool any_in = i0 < g.nx;
+  if (j < g.ny && __any_sync(0xffffffffu, any_in)) {
+    const int k1 = min(k0 + kz, g.nz);
+    // lanes past the padded row read a valid pair of it and store nothing
+    int c = g.idx(i0 < g.px ? i0 : g.px - 2, j, k0);
+    auto X2 = [&](int cc, double& a, double& bb) {
+      const double2 xv = *reinterpret_cast<const double2*>(xs + cc);
+      const ET ev = *reinterpret_cast<const ET*>(e + cc);
+      a = xv.x + (double)ev.x;
+      bb = xv.y + (double)ev.y;
+    };
+    auto X = [&](int cc) { return xs[cc] + (double)e[cc]; };
+    double xm[2], xc[2], xp[2];
+    X2(c - g.ps, xm[0], xm[1]);
+    X2(c, xc[0], xc[1]);
+    double2 bzc = *reinterpret_cast<const double2*>(S.bz + c);
+    for (int k = k0; k < k1; ++k, c += g.ps) {
+      X2(c + g.ps, xp[0], xp[1]);
+      double ym[2], yp[2];
+      X2(c - g.px, ym[0], ym[1]);
+      X2(c + g.px, yp[0], yp[1]);
+      const double2 bxv = *reinterpret_cast<const double2*>(S.bx + c);
+      const double2 byv = *reinterpret_cast<const double2*>(S.by + c);
+      const double2 byu = *reinterpret_cast<const double2*>(S.by + c + g.px);
+      const double2 bzu = *reinterpret_cast<const double2*>(S.bz + c + g.ps);
+      const double2 bv = *reinterpret_cast<const double2*>(b + c);
+      double left = __shfl_up_sync(0xffffffffu, xc[1], 1);
+      double right = __shfl_down_sync(0xffffffffu, xc[0], 1);
+      double bxr = __shfl_down_sync(0xffffffffu, bxv.x, 1);
+      if (lane == 0) left = X(c - 1);
+      if (lane == REL_TX - 1) {
+        right = X(c + 2);
+        bxr = S.bx[c + 2];
+      }
+      const double rv0 = bv.x - Stencil<double, double>::apply(xc[0], bxv.x, bxv.y, byv.x, byu.x, bzc.x, bzu.x, left,
+                                                               xc[1], ym[0], yp[0], xm[0], xp[0]);
+      const double rv1 = bv.y - Stencil<double, double>::apply(xc[1], bxv.y, bxr, byv.y, byu.y, bzc.y, bzu.y, xc[0],
+                                                               right, ym[1], yp[1], xm[1], xp[1]);
+      if (any_in) {
+        const bool in1 = i0 + 1 < g.nx;
+        double2 xo;
+        xo.x = xc[0];
+        xo.y = in1 ? xc[1] : 0.0;
+        *reinterpret_cast<double2*>(xd + c) = xo;
+        ET ro;
+        ro.x = (T)rv0;
+        ro.y = in1 ? (T)rv1 : (T)0;
+        *reinterpret_cast<ET*>(r + c) = ro;
+        v[0] += rv0;
+        v[1] += rv0 * rv0;
+        v[2] = fmax(v[2], fabs(rv0));
+        if (in1) {
+          v[0] += rv1;
+          v[1] += rv1 * rv1;
+          v[2] = fmax(v[2], fabs(rv1));
+        }
+      }
+      xm[0] = xc[0];
+      xm[1] = xc[1];
+      xc[0] = xp[0];
+      xc[1] = xp[1];
+      bzc = bzu;
+    }
+  }
+  const Op ops[3] = {Op::Sum, Op::Sum, Op::Max};
+  double out[3];
+  if (grid_reduce<3, REL_TX * REL_TY>(v, ops, red, 0, out)) {
+    if (threadIdx.x == 0 && threadIdx.y == 0) {
+      s->xbuf ^= 1;
+      s->e_reset = 1;
+      s->do_reliable = 0;
+      s->reliable_count += 1;
+      const double m = out[0] * s->inv_nfluid;
+      s->rshift = m;
+      const double rr = fmax(out[1] - out[0] * m, 0.0);
+      s->rr = rr;
+      s->rr_anchor = rr;
+      s->rmax = out[2];
+      s->true_rr = rr;
+      s->true_rmax = out[2];
+      if (!isfinite(out[1])) { s->status = 3; s->done = 1; return; }
+      const bool ok = (s->stop_rule == 1) ? (out[2] < s->tol_max) : (rr <= s->tol2bb);
+      if (ok) { s->status = 0; s->done = 1; }
+      else if (s->iter >= s->max_iter) { s->status = 1; s->done = 1; }
+    }
+  }
+}
+
 // rz_new = (r - shift).z over all cells (z is 0 where the diagonal is 0, so
 // the shift needs no mask), beta = rz_new / rz.
 template <class T>
