@@ -88,7 +88,7 @@ typedef struct {
   int coarse_sweeps;      /* symmetric sweep pairs on the coarsest grid, default 8 */
   int check_every;        /* residual tests every check_every iterations (device side), default 1 */
   double reliable_delta;  /* MIXED: recompute the FP64 true residual when the FP32 residual has
-                             fallen by this factor since the last recomputation, default 1e-2 */
+                             fallen by this factor since the last recomputation, default 1e-4 */
   int bf16_coarse_cells;  /* MIXED: grids with at most this many cells store BF16 coefficients
                              (default 4096, i.e. 16^3 and below); 0 disables BF16 */
 } smac_options;

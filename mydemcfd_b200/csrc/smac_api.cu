@@ -624,7 +624,7 @@ smac_status smac_default_options(smac_options* o) {
   o->nu2 = 2;
   o->coarse_sweeps = 8;
   o->check_every = 1;
-  o->reliable_delta = 1e-2;
+  o->reliable_delta = 1e-4;
   o->bf16_coarse_cells = COARSE_CELLS;
   return SMAC_OK;
 }
@@ -969,9 +969,9 @@ smac_status run_solve(smac_handle* h, const double** xout) {
   CK(cudaMemcpyAsync(h->s, h->hs, sizeof(Scalars), cudaMemcpyHostToDevice, h->stream));
   CK(cudaMemsetAsync(base_of(g, h->x64a), 0, bytes, h->stream));
   if (mixed) {
-    CK(cudaMemsetAsync(base_of(g, h->x64b), 0, bytes, h->stream));
+    // x64b and e32 need no clearing: a reliable update writes every cell of
+    // x64b, and the first x/r update sets e = alpha d (e_reset)
     CK(cudaMemsetAsync(base_of(g, h->d32), 0, sizeof(float) * (size_t)g.alloc, h->stream));
-    CK(cudaMemsetAsync(base_of(g, h->e32), 0, sizeof(float) * (size_t)g.alloc, h->stream));
   } else {
     CK(cudaMemsetAsync(base_of(g, h->d64), 0, bytes, h->stream));
   }
@@ -1094,9 +1094,10 @@ smac_status run_solve(smac_handle* h, const double** xout) {
   } else {
     *xout = h->hs->xbuf ? h->x64b : h->x64a;
   }
-  if (mixed || h->hs->status != 0) {
-    // true residual of the final iterate (mixed: already computed unless
-    // the solve stopped without a final recomputation)
+  if (h->hs->status != 0) {
+    // true residual of the final iterate of a solve that did not converge
+    // (a converged solve has just computed it: the FP64 check of the plain
+    // form, the last reliable update of the mixed form)
     auto S = stencil<double, double>(g, h->lv[0].bx64, h->lv[0].by64, h->lv[0].bz64);
     k_true_residual<<<grid_cells(g, kz), kBlock, 0, h->stream>>>(g, *xout, h->b64, S, h->r64, 0, h->red, h->s, kz);
     CKL();
