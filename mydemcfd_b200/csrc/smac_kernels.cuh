@@ -427,65 +427,9 @@ __global__ void __launch_bounds__(UPD_NT) k_update_flat(T* x, const T* __restric
 // Mixed precision: FP64 true residual.  x_new = x64[xbuf] + e (FP64 sum at
 // every stencil point), r = b - A64 x_new written as FP32, x_new stored in
 // the other FP64 buffer; the stopping test runs on this true residual.
-template <class T>
-__global__ void __launch_bounds__(TNT) k_reliable(Geom g, double* x64a, double* x64b, const T* __restrict__ e,
-                                                  const double* __restrict__ b, Stencil<double, double> S, T* r,
-                                                  RedBuf red, Scalars* s, int kz) {
-  if (s->done || !s->do_reliable) return;
-  const int i = blockIdx.x * TBX + threadIdx.x;
-  const int j = blockIdx.y * TBY + threadIdx.y;
-  const int k0 = blockIdx.z * kz;
-  const double* __restrict__ xs = s->xbuf ? x64b : x64a;
-  double* xd = s->xbuf ? x64a : x64b;
-  double v[3] = {0.0, 0.0, 0.0};
-  if (i < g.nx && j < g.ny) {
-    const int k1 = min(k0 + kz, g.nz);
-    int c = g.idx(i, j, k0);
-    auto X = [&](int cc) { return xs[cc] + (double)e[cc]; };
-    double xm = X(c - g.ps), xc = X(c);
-    for (int k = k0; k < k1; ++k, c += g.ps) {
-      const double xp = X(c + g.ps);
-      double wxm, wxp, wym, wyp, wzm, wzp;
-      S.coeffs(c, g.px, g.ps, wxm, wxp, wym, wyp, wzm, wzp);
-      const double rv = b[c] - Stencil<double, double>::apply(xc, wxm, wxp, wym, wyp, wzm, wzp, X(c - 1), X(c + 1),
-                                                              X(c - g.px), X(c + g.px), xm, xp);
-      xd[c] = xc;
-      r[c] = (T)rv;
-      v[0] += rv;
-      v[1] += rv * rv;
-      v[2] = fmax(v[2], fabs(rv));
-      xm = xc;
-      xc = xp;
-    }
-  }
-  const Op ops[3] = {Op::Sum, Op::Sum, Op::Max};
-  double out[3];
-  if (grid_reduce<3, TNT>(v, ops, red, 0, out)) {
-    if (threadIdx.x == 0 && threadIdx.y == 0) {
-      s->xbuf ^= 1;
-      s->e_reset = 1;
-      s->do_reliable = 0;
-      s->reliable_count += 1;
-      const double m = out[0] * s->inv_nfluid;
-      s->rshift = m;
-      const double rr = fmax(out[1] - out[0] * m, 0.0);
-      s->rr = rr;
-      s->rr_anchor = rr;
-      s->rmax = out[2];
-      s->true_rr = rr;
-      s->true_rmax = out[2];
-      if (!isfinite(out[1])) { s->status = 3; s->done = 1; return; }
-      const bool ok = (s->stop_rule == 1) ? (out[2] < s->tol_max) : (rr <= s->tol2bb);
-      if (ok) { s->status = 0; s->done = 1; }
-      else if (s->iter >= s->max_iter) { s->status = 1; s->done = 1; }
-    }
-  }
-}
-
-// The same with each thread on 2 consecutive cells of one row, marching kz
-// planes: FP64 rows as 16-byte vectors, x-neighbours across the pair from
-// the adjacent lanes (lanes 0 and 31 load them), per-cell arithmetic as in
-// k_reliable.
+// Each thread takes 2 consecutive cells of one row and marches kz planes:
+// FP64 rows move as 16-byte vectors, and x-neighbours across the pair come
+// from the adjacent lanes (lanes 0 and 31 load them).
 constexpr int REL_TX = 32, REL_TY = 4;
 template <class T>
 __global__ void __launch_bounds__(REL_TX * REL_TY) k_reliable_vec(Geom g, double* x64a, double* x64b,
@@ -969,22 +913,6 @@ __device__ __forceinline__ void cta_resid_restrict(const CoarseLevel& L, const C
   }
 }
 
-// x (this grid) += coarse x at the parent, for the coarsest hand-off where the
-// next step is the symmetric sweep (no fused half-sweep available).
-template <class T>
-__device__ __forceinline__ void cta_prolong(const CoarseLevel& L, const CoarseLevel& Lc) {
-  const Geom& g = L.g;
-  const Geom& gc = Lc.g;
-  T* x = (T*)L.x;
-  const T* xc = (const T*)Lc.x;
-  const int total = g.nx * g.ny * g.nz;
-  for (int t = threadIdx.x; t < total; t += blockDim.x) {
-    const int i = t % g.nx, j = (t / g.nx) % g.ny, k = t / (g.nx * g.ny);
-    const int c = g.idx(i, j, k);
-    x[c] = x[c] + xc[gc.idx(Lc.cx ? i >> 1 : i, Lc.cy ? j >> 1 : j, Lc.cz ? k >> 1 : k)];
-  }
-}
-
 template <class T, class C>
 __global__ void __launch_bounds__(1024) k_coarse_vcycle(CoarseSet set, int nu1, int nu2, int coarse_pairs,
                                                         const double* shift0, const Scalars* s) {
@@ -1096,14 +1024,6 @@ __global__ void k_correct(RefDims R, Geom g, double inv_dx, double inv_dy, doubl
   if (p && ix >= 1 && iy >= 1 && iz >= 1 && ix < Nx + 1 && iy < Ny + 1 && iz < Nz + 1) {
     if (ct[R.cell(ix, iy, iz)] == C_INTERIOR) p[R.cell(ix, iy, iz)] = DADD(p[R.cell(ix, iy, iz)], pd[R.cell(ix, iy, iz)]);
   }
-}
-
-// Zero the entries of the reference-layout write-only faces' ghosts are left
-// alone; zero a reference-layout cell array's interior (p_delta reset,
-// G_SMACSolver.cu:1273 zeroes the whole array).
-__global__ void k_fill(double* a, long long n, double v) {
-  long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  for (; t < n; t += (long long)gridDim.x * blockDim.x) a[t] = v;
 }
 
 // ------------------------------------------------------------------------

@@ -192,57 +192,10 @@ __global__ void __launch_bounds__(RB_NT) k_rbgs_sweep(Geom g, const T* __restric
 // zshift (the fluid mean of z) keeps d free of the constant null-space
 // component of the pure-Neumann operator, which would otherwise make p.Ap a
 // cancellation near the rounding floor; cells without unknowns keep d = 0.
-template <class T, class C>
-__global__ void __launch_bounds__(TNT) k_dir_matvec(Geom g, const T* __restrict__ z, T* __restrict__ d_old,
-                                                    T* __restrict__ d_new, Stencil<T, C> S, T* q,
-                                                    const uint8_t* __restrict__ fluid, RedBuf red, Scalars* s,
-                                                    int kz) {
-  if (s->done) return;
-  typedef acc_t<T> A;
-  const int i = blockIdx.x * TBX + threadIdx.x;
-  const int j = blockIdx.y * TBY + threadIdx.y;
-  const int k0 = blockIdx.z * kz;
-  const A beta = (A)s->beta;
-  const A zs = (A)s->zshift;
-  double v[1] = {0.0};
-  if (i < g.nx && j < g.ny) {
-    const int k1 = min(k0 + kz, g.nz);
-    int c = g.idx(i, j, k0);
-    // neighbours without unknowns enter through zero face weights only
-    auto D = [&](int cc) -> A { return Ar<A>::fma(beta, (A)d_old[cc], Ar<A>::add((A)z[cc], -zs)); };
-    A xm = D(c - g.ps), xc = D(c);
-    for (int k = k0; k < k1; ++k, c += g.ps) {
-      const A xp = D(c + g.ps);
-      if (!(fluid[c] & 2)) xc = (A)0;
-      A wxm, wxp, wym, wyp, wzm, wzp;
-      S.coeffs(c, g.px, g.ps, wxm, wxp, wym, wyp, wzm, wzp);
-      const A y = Stencil<T, C>::apply(xc, wxm, wxp, wym, wyp, wzm, wzp, D(c - 1), D(c + 1), D(c - g.px), D(c + g.px),
-                                       xm, xp);
-      d_new[c] = (T)xc;
-      q[c] = (T)y;
-      v[0] += (double)(T)xc * (double)(T)y;
-      xm = xc;
-      xc = xp;
-    }
-  }
-  const Op ops[1] = {Op::Sum};
-  double out[1];
-  if (grid_reduce<1, TNT>(v, ops, red, 0, out)) {
-    if (threadIdx.x == 0 && threadIdx.y == 0) {
-      const double pAp = out[0];
-      s->pAp = pAp;
-      if (!isfinite(pAp)) { s->status = 3; s->done = 1; }
-      else if (!(pAp > 0.0)) { s->status = 2; s->done = 1; }
-      else s->alpha = s->rz / pAp;
-    }
-  }
-}
-
-// The same operation with each thread on 16 bytes of consecutive cells of
-// one row (4 FP32 or 2 FP64), marching kz planes: rows and planes move as
-// 16-byte vectors, x-neighbours across the vector edge come from the
-// adjacent lanes (lanes 0 and 31 load them), and the per-cell arithmetic is
-// that of k_dir_matvec.
+// Each thread takes 16 bytes of consecutive cells of one row (4 FP32 or 2
+// FP64) and marches kz planes: rows and planes move as 16-byte vectors, and
+// x-neighbours across the vector edge come from the adjacent lanes (lanes 0
+// and 31 load them).
 constexpr int DMV_TX = 32, DMV_TY = 4;
 template <class T>
 __global__ void __launch_bounds__(DMV_TX * DMV_TY) k_dir_matvec_vec(Geom g, const T* __restrict__ z,
