@@ -277,28 +277,34 @@ def run_ours(args, ranks):
     sps_mixed = replicas.throughput(ranks, args.steps, ms_mixed)
     sps_plain = replicas.throughput(ranks, args.steps, ms_plain)
 
-    # end to end through the C ABI with host buffers: pinned u* in, u and p_delta out
+    # end to end through the C ABI with host buffers: pinned u* in, u and
+    # p_delta out, every projection's copies inside the timed region.  The
+    # projections go through the queued host-buffer entry points
+    # (smac_async_*), which overlap one projection's copies with its
+    # neighbours' solves; the timed region ends when the last outputs are in
+    # host memory.
     e2e = None
     if not args.no_e2e:
+        from mydemcfd_b200.solver import AsyncProjector
         host_in = [torch.from_numpy(np.ascontiguousarray(a)).pin_memory() for a in (case.vxs, case.vys, case.vzs)]
-        host_out = [torch.empty(sh[k], dtype=torch.float64).pin_memory() for k in "xyz"] + \
-                   [torch.empty(sh["cell"], dtype=torch.float64).pin_memory()]
-        dev_in = [torch.empty_like(t, device=dev) for t in host_in]
+        host_out = [[torch.empty(sh[k], dtype=torch.float64).pin_memory() for k in ("x", "y", "z", "cell")]
+                    for _ in range(2)]
+        proj = AsyncProjector(s_mixed)
 
-        def e2e_step():
-            for d, h in zip(dev_in, host_in):
-                d.copy_(h, non_blocking=True)
-            st = s_mixed.project(*dev_in, case.dt, pd, *out_v)
-            for h, d in zip(host_out, out_v + [pd]):
-                h.copy_(d, non_blocking=True)
-            return st
+        def e2e_run(k):
+            tickets = []
+            for i in range(k):
+                o = host_out[i % 2]
+                tickets.append(proj.submit(*host_in, case.dt, o[3], o[0], o[1], o[2]))
+            return [proj.wait(t) for t in tickets]
 
-        for _ in range(max(1, args.warmup // 2)):
-            e2e_step()
-        ms_e2e, _ = timed(e2e_step, args.steps)
+        e2e_run(max(2, args.warmup // 2))
+        ms_e2e, st_e2e = timed(lambda: e2e_run(args.steps), 1)
+        proj.close()
         e2e = {"value": replicas.throughput(ranks, args.steps, ms_e2e), "unit": "solves/s",
                "h2d_bytes_per_step": int(sum(t.numel() * 8 for t in host_in)),
-               "d2h_bytes_per_step": int(sum(t.numel() * 8 for t in host_out))}
+               "d2h_bytes_per_step": int(sum(t.numel() * 8 for t in host_out[0])),
+               "api": "smac_async_submit / smac_async_wait (host buffers, copies overlapped with neighbouring solves)"}
 
     # roofline of the dominant kernel: the fused red-black sweep of the fine
     # grid in FP32 (k_rbgs_tma<float>), timed with CUDA events on the

@@ -252,6 +252,28 @@ smac_status smac_apply_A_dot_noalloc(const smac_grid_desc* desc, const double* f
  * No counterpart in the reference (it has no Gauss-Seidel smoother). */
 smac_status smac_selftest_sweep(smac_handle* h, int precision, int mode, long long* mismatches);
 
+/* ---------------------------------------------------------------------------
+ * Projections with host buffers, queued.  A queue on a handle runs
+ * smac_project on inputs and outputs in host memory (the reference layout, as
+ * for smac_project), and overlaps each projection's copies with the solves of
+ * its neighbours: the input of the next projection is copied in and the
+ * outputs of the previous one are copied out while this one is solved.  Two
+ * device staging slots and a worker thread belong to the queue.  New: the
+ * reference solves one step at a time on device-resident arrays
+ * (G_SMACSolver::solve_poisson, CFD/G_SMACSolver.cu:1499-1501).
+ *
+ * smac_async_submit copies the input in (asynchronously) and returns a
+ * ticket; smac_async_wait(ticket) returns once that projection's outputs are
+ * in host memory, with its status and statistics.  Host buffers should be
+ * page-locked for the copies to overlap, and stay valid until the wait
+ * returns.  While a queue exists, the handle must not be used directly. */
+typedef struct smac_async smac_async;
+smac_status smac_async_create(smac_handle* h, smac_async** out);
+smac_status smac_async_submit(smac_async* a, const double* vxs, const double* vys, const double* vzs, double dt,
+                              double* p_delta, double* vx, double* vy, double* vz, unsigned long long* ticket);
+smac_status smac_async_wait(smac_async* a, unsigned long long ticket, smac_stats* stats);
+void smac_async_destroy(smac_async* a);
+
 #ifdef __cplusplus
 }
 #endif

@@ -63,7 +63,8 @@ EXPORTS = [
     "smac_level_shape", "smac_set_coefficients", "smac_box_types", "smac_assemble_vof",
     "smac_ibm_solid_fraction_spheres", "smac_ibm_set_solid_cells", "smac_divergence", "smac_solve",
     "smac_set_rhs", "smac_correct", "smac_project", "smac_project_adjoint", "smac_apply_A", "smac_time_kernel",
-    "smac_selftest_sweep", "smac_apply_A_dot_noalloc",
+    "smac_selftest_sweep", "smac_apply_A_dot_noalloc", "smac_async_create", "smac_async_submit",
+    "smac_async_wait", "smac_async_destroy",
 ]
 
 
@@ -99,6 +100,10 @@ def load(path: str = LIB_PATH):
         "smac_time_kernel": [vp, ip, ip, ctypes.POINTER(ctypes.c_float), ctypes.POINTER(d)],
         "smac_selftest_sweep": [vp, ip, ip, ctypes.POINTER(ctypes.c_longlong)],
         "smac_apply_A_dot_noalloc": [ctypes.POINTER(GridDesc), dp, dp, dp, u8p, u8p, u8p, u8p, dp, dp, dp, vp],
+        "smac_async_create": [vp, ctypes.POINTER(vp)],
+        "smac_async_submit": [vp, dp, dp, dp, d, dp, dp, dp, dp, ctypes.POINTER(ctypes.c_ulonglong)],
+        "smac_async_wait": [vp, ctypes.c_ulonglong, ctypes.POINTER(Stats)],
+        "smac_async_destroy": [vp],
     }
     for name, args in sig.items():
         fn = getattr(lib, name)

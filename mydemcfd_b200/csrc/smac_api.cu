@@ -112,7 +112,8 @@ struct smac_handle {
   bool use_tma = true;     // fused sweeps stage their tiles with the copy engine
   int tma_ctas[2] = {1, 1};  // resident CTAs per SM of the TMA sweep: [0] FP32, [1] FP64
   Scalars* s = nullptr;    // device
-  Scalars* hs = nullptr;   // pinned host mirror
+  Scalars* hs = nullptr;   // pinned, mapped host mirror of the device scalars
+  Scalars* hs_dev = nullptr;  // the mirror's device-side address
   cudaGraphExec_t graph[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};  // [precision][gmg]
   bool have_coeffs = false, have_rhs = false;
   double dt = 1.0;
@@ -156,6 +157,29 @@ inline dim3 grid_pairs(const Geom& g, int kz) {
 }
 inline dim3 grid_planes(int nx, int ny, int nz) { return dim3((nx + TBX - 1) / TBX, (ny + TBY - 1) / TBY, nz); }
 const dim3 kBlock(TBX, TBY, 1);
+
+// Scalars between the device and the mapped host mirror, and clearing of
+// solver buffers, by kernels on the handle's stream: copy engines would queue
+// these small operations behind bulk copies of other streams (smac_async).
+smac_status scalars_to_host(smac_handle* h) {
+  k_copy_words<<<1, 64, 0, h->stream>>>(reinterpret_cast<const unsigned*>(h->s), reinterpret_cast<unsigned*>(h->hs_dev),
+                                        (int)(sizeof(Scalars) / 4));
+  CKL();
+  return SMAC_OK;
+}
+smac_status scalars_to_device(smac_handle* h) {
+  k_copy_words<<<1, 64, 0, h->stream>>>(reinterpret_cast<const unsigned*>(h->hs_dev), reinterpret_cast<unsigned*>(h->s),
+                                        (int)(sizeof(Scalars) / 4));
+  CKL();
+  return SMAC_OK;
+}
+smac_status zero_async(smac_handle* h, void* p, size_t bytes) {
+  const long long n16 = (long long)(bytes / 16);
+  const int G = (int)std::max(1LL, std::min(4LL * h->num_sms, (n16 + 255) / 256));
+  k_zero16<<<G, 256, 0, h->stream>>>(reinterpret_cast<int4*>(p), n16);
+  CKL();
+  return SMAC_OK;
+}
 
 template <class T, class C>
 Stencil<T, C> stencil(const Geom&, const void* bx, const void* by, const void* bz) {
@@ -606,6 +630,16 @@ void setup_tma(smac_handle* h) {
 
 }  // namespace
 
+// Internal accessors for smac_async.cu.
+namespace smac {
+cudaStream_t handle_stream(const smac_handle* h) { return h->stream; }
+void handle_shape(const smac_handle* h, int* nx, int* ny, int* nz) {
+  *nx = h->desc.nx;
+  *ny = h->desc.ny;
+  *nz = h->desc.nz;
+}
+}  // namespace smac
+
 // ===========================================================================
 extern "C" {
 
@@ -754,8 +788,11 @@ smac_status smac_create(const smac_grid_desc* desc, const smac_options* opts, vo
   }
   if ((st = dalloc(h, &h->s, 1))) return fail(st);
   {
-    cudaError_t eh = cudaMallocHost((void**)&h->hs, sizeof(Scalars));
-    if (eh != cudaSuccess) { set_err("cudaMallocHost: %s", cudaGetErrorString(eh)); return fail(SMAC_CUDA_ERROR); }
+    // mapped, so that kernels move the scalars over PCIe without a copy
+    // engine: a copy would queue behind bulk copies of other streams
+    cudaError_t eh = cudaHostAlloc((void**)&h->hs, sizeof(Scalars), cudaHostAllocMapped);
+    if (eh == cudaSuccess) eh = cudaHostGetDevicePointer((void**)&h->hs_dev, h->hs, 0);
+    if (eh != cudaSuccess) { set_err("cudaHostAlloc: %s", cudaGetErrorString(eh)); return fail(SMAC_CUDA_ERROR); }
     memset(h->hs, 0, sizeof(Scalars));
   }
   h->num_sms = prop.multiProcessorCount;
@@ -852,7 +889,7 @@ smac_status smac_set_coefficients(smac_handle* h, const double* fbx, const doubl
     }
     CKL();
   }
-  CK(cudaMemcpyAsync(h->hs, h->s, sizeof(Scalars), cudaMemcpyDeviceToHost, h->stream));
+  TRY(scalars_to_host(h));
   CK(cudaStreamSynchronize(h->stream));
   h->nfluid = h->hs->sum_tmp;
   h->have_coeffs = true;
@@ -966,14 +1003,14 @@ smac_status run_solve(smac_handle* h, const double** xout) {
   init.inv_nfluid = (pure && h->nfluid > 0) ? 1.0 / h->nfluid : 0.0;
   init.mixed = mixed ? 1 : 0;
   *h->hs = init;
-  CK(cudaMemcpyAsync(h->s, h->hs, sizeof(Scalars), cudaMemcpyHostToDevice, h->stream));
-  CK(cudaMemsetAsync(base_of(g, h->x64a), 0, bytes, h->stream));
+  TRY(scalars_to_device(h));
+  TRY(zero_async(h, base_of(g, h->x64a), bytes));
   if (mixed) {
     // x64b and e32 need no clearing: a reliable update writes every cell of
     // x64b, and the first x/r update sets e = alpha d (e_reset)
-    CK(cudaMemsetAsync(base_of(g, h->d32), 0, sizeof(float) * (size_t)g.alloc, h->stream));
+    TRY(zero_async(h, base_of(g, h->d32), sizeof(float) * (size_t)g.alloc));
   } else {
-    CK(cudaMemsetAsync(base_of(g, h->d64), 0, bytes, h->stream));
+    TRY(zero_async(h, base_of(g, h->d64), bytes));
   }
   const dim3 gr = grid_cells(g, kz);
   k_setup_sum<double><<<gr, kBlock, 0, h->stream>>>(g, h->b64, h->red, h->s, kz);
@@ -1001,7 +1038,7 @@ smac_status run_solve(smac_handle* h, const double** xout) {
     int batch = 1;
     for (int q = 0; q < batch; ++q) CK(cudaGraphLaunch(ex, h->stream));
     launched += 2 * batch;
-    CK(cudaMemcpyAsync(h->hs, h->s, sizeof(Scalars), cudaMemcpyDeviceToHost, h->stream));
+    TRY(scalars_to_host(h));
     CK(cudaStreamSynchronize(h->stream));
     if (h->hs->done) {
       if (h->hs->status == 2 && restarts < 3) {
@@ -1017,7 +1054,7 @@ smac_status run_solve(smac_handle* h, const double** xout) {
           h->hs->done = 0;
           h->hs->status = 0;
           h->hs->do_reliable = 1;
-          CK(cudaMemcpyAsync(h->s, h->hs, sizeof(Scalars), cudaMemcpyHostToDevice, h->stream));
+          TRY(scalars_to_device(h));
           launch_reliable(h, g, S, kz);
           CKL();
         } else {
@@ -1026,7 +1063,7 @@ smac_status run_solve(smac_handle* h, const double** xout) {
           CKL();
         }
         account(h, g, 6 * 8, 1);
-        CK(cudaMemcpyAsync(h->hs, h->s, sizeof(Scalars), cudaMemcpyDeviceToHost, h->stream));
+        TRY(scalars_to_host(h));
         CK(cudaStreamSynchronize(h->stream));
         const Scalars& hs = *h->hs;
         const bool ok = (o.stop_rule == 1) ? (hs.true_rmax < hs.tol_max) : (hs.true_rr <= hs.tol2bb);
@@ -1041,13 +1078,13 @@ smac_status run_solve(smac_handle* h, const double** xout) {
         }
         ++restarts;
         if (mixed)
-          CK(cudaMemsetAsync(base_of(g, h->d32), 0, sizeof(float) * (size_t)g.alloc, h->stream));
+          TRY(zero_async(h, base_of(g, h->d32), sizeof(float) * (size_t)g.alloc));
         else
-          CK(cudaMemsetAsync(base_of(g, h->d64), 0, sizeof(double) * (size_t)g.alloc, h->stream));
+          TRY(zero_async(h, base_of(g, h->d64), sizeof(double) * (size_t)g.alloc));
         h->hs->done = 0;
         h->hs->first = 1;
         h->hs->status = 0;
-        CK(cudaMemcpyAsync(h->s, h->hs, sizeof(Scalars), cudaMemcpyHostToDevice, h->stream));
+        TRY(scalars_to_device(h));
         continue;
       }
       if (!mixed && h->hs->status == 0) {
@@ -1056,7 +1093,7 @@ smac_status run_solve(smac_handle* h, const double** xout) {
         k_true_residual<<<grid_cells(g, kz), kBlock, 0, h->stream>>>(g, h->x64a, h->b64, S, h->r64, 0, h->red, h->s, kz);
         CKL();
         account(h, g, 5 * 8, 1);
-        CK(cudaMemcpyAsync(h->hs, h->s, sizeof(Scalars), cudaMemcpyDeviceToHost, h->stream));
+        TRY(scalars_to_host(h));
         CK(cudaStreamSynchronize(h->stream));
         const Scalars& hs = *h->hs;
         const bool ok = (o.stop_rule == 1) ? (hs.true_rmax < hs.tol_max) : (hs.true_rr <= hs.tol2bb);
@@ -1067,13 +1104,13 @@ smac_status run_solve(smac_handle* h, const double** xout) {
                                                                         kz);
           CKL();
           account(h, g, 6 * 8, 1);
-          CK(cudaMemsetAsync(base_of(g, h->d64), 0, bytes, h->stream));
-          CK(cudaMemcpyAsync(h->hs, h->s, sizeof(Scalars), cudaMemcpyDeviceToHost, h->stream));
+          TRY(zero_async(h, base_of(g, h->d64), bytes));
+          TRY(scalars_to_host(h));
           CK(cudaStreamSynchronize(h->stream));
           h->hs->done = 0;
           h->hs->first = 1;
           h->hs->status = 0;
-          CK(cudaMemcpyAsync(h->s, h->hs, sizeof(Scalars), cudaMemcpyHostToDevice, h->stream));
+          TRY(scalars_to_device(h));
           continue;
         }
       }
@@ -1102,7 +1139,7 @@ smac_status run_solve(smac_handle* h, const double** xout) {
     k_true_residual<<<grid_cells(g, kz), kBlock, 0, h->stream>>>(g, *xout, h->b64, S, h->r64, 0, h->red, h->s, kz);
     CKL();
     account(h, g, 5 * 8, 1);
-    CK(cudaMemcpyAsync(h->hs, h->s, sizeof(Scalars), cudaMemcpyDeviceToHost, h->stream));
+    TRY(scalars_to_host(h));
     CK(cudaStreamSynchronize(h->stream));
   }
   return SMAC_OK;
@@ -1146,7 +1183,7 @@ smac_status smac_solve(smac_handle* h, double* p_delta, smac_stats* stats) {
   TRY(run_solve(h, &x));
   TRY(export_solution(h, x, p_delta));
   if (stats) {
-    CK(cudaMemcpyAsync(h->hs, h->s, sizeof(Scalars), cudaMemcpyDeviceToHost, h->stream));
+    TRY(scalars_to_host(h));
     CK(cudaStreamSynchronize(h->stream));
     fill_stats(h, stats);
   }
@@ -1273,7 +1310,7 @@ smac_status smac_time_kernel(smac_handle* h, int kernel_id, int reps, float* ms,
   st.tol2bb = -1.0;
   st.tol_max = -1.0;
   *h->hs = st;
-  CK(cudaMemcpyAsync(h->s, h->hs, sizeof(Scalars), cudaMemcpyHostToDevice, h->stream));
+  TRY(scalars_to_device(h));
   // non-zero operands: d = z = b (FP64), d32 = r32 = z32 = b, so that p.Ap > 0
   CK(cudaMemcpyAsync(base_of(g, h->d64), base_of(g, h->b64), sizeof(double) * (size_t)g.alloc, cudaMemcpyDeviceToDevice,
                      h->stream));
@@ -1423,7 +1460,7 @@ smac_status smac_selftest_sweep(smac_handle* h, int precision, int mode, long lo
   // the V-cycle's shift must be finite; a state with shift 0 is used
   Scalars st{};
   *h->hs = st;
-  CK(cudaMemcpyAsync(h->s, h->hs, sizeof(Scalars), cudaMemcpyHostToDevice, h->stream));
+  TRY(scalars_to_device(h));
   if (precision == SMAC_PRECISION_FP64)
     return sweep_selftest<double, double>(h, mode, h->z64, h->tmp64, h->z64b, h->r64, h->lv[0].bx64, h->lv[0].by64,
                                           h->lv[0].bz64, h->lv[1].x64, mismatches);

@@ -147,6 +147,17 @@ __global__ void k_coarsen_coeffs(Geom gf, Geom gc, int cx, int cy, int cz, const
   }
 }
 
+// Word copy of a small struct (the solver scalars to and from their mapped
+// host mirror) and a 16-byte clearing loop.
+static_assert(sizeof(Scalars) % 4 == 0, "scalar block in words");
+__global__ void k_copy_words(const unsigned* __restrict__ src, unsigned* __restrict__ dst, int n) {
+  for (int t = threadIdx.x; t < n; t += blockDim.x) dst[t] = src[t];
+}
+__global__ void k_zero16(int4* p, long long n16) {
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n16; t += (long long)gridDim.x * blockDim.x)
+    p[t] = make_int4(0, 0, 0, 0);
+}
+
 // FP64 -> C copy of a whole padded array (fine-level FP32 / BF16 coefficients).
 template <class C>
 __global__ void k_convert(const double* __restrict__ a, C* b, long long n) {

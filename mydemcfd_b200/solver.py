@@ -235,6 +235,51 @@ class B200PressureSolver:
             pass
 
 
+class AsyncProjector:
+    """Queued projections with host buffers (smac_async_*): submit() copies
+    u* in and returns a ticket, wait(ticket) returns once u and p_delta are in
+    the host buffers, with the projection's statistics.  The next
+    projection's input copy and the previous one's output copy overlap the
+    current solve.  Host tensors should be pinned (tensor.pin_memory()) and
+    stay alive until their wait returns; the solver must not be used directly
+    while the projector is open."""
+
+    def __init__(self, solver: "B200PressureSolver"):
+        self._lib = solver._lib
+        self._solver = solver
+        a = ctypes.c_void_p()
+        nat.check(self._lib.smac_async_create(solver._h, ctypes.byref(a)))
+        self._a = a
+
+    def submit(self, vxs, vys, vzs, dt, p_delta, vx, vy, vz) -> int:
+        for t in (vxs, vys, vzs, p_delta, vx, vy, vz):
+            if t.device.type != "cpu" or t.dtype != torch.float64 or not t.is_contiguous():
+                raise ValueError("AsyncProjector: host float64 contiguous tensors expected")
+        ticket = ctypes.c_ulonglong()
+        hp = lambda t: ctypes.c_void_p(t.data_ptr())
+        nat.check(self._lib.smac_async_submit(self._a, hp(vxs), hp(vys), hp(vzs), ctypes.c_double(dt), hp(p_delta),
+                                              hp(vx), hp(vy), hp(vz), ctypes.byref(ticket)))
+        return ticket.value
+
+    def wait(self, ticket: int, raise_on_fail=True) -> dict:
+        st = nat.Stats()
+        rc = self._lib.smac_async_wait(self._a, ctypes.c_ulonglong(ticket), ctypes.byref(st))
+        if raise_on_fail:
+            nat.check(rc)
+        return st.as_dict()
+
+    def close(self):
+        if getattr(self, "_a", None):
+            self._lib.smac_async_destroy(self._a)
+            self._a = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 class SMACStep:
     """The G_SMACSolver calls around the seam, in the reference's order
     (CFD/main.cu:313-315): solve_poisson(), then correct_vof_velocity()."""

@@ -14,7 +14,7 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 def header_functions():
     txt = open(os.path.join(ROOT, "include", "smac_b200.h")).read()
-    return sorted(set(re.findall(r"^(?:smac_status|const char\*)\s+(smac_\w+)\s*\(", txt, re.M)))
+    return sorted(set(re.findall(r"^(?:smac_status|const char\*|void)\s+(smac_\w+)\s*\(", txt, re.M)))
 
 
 @pytest.fixture(scope="module")
@@ -43,6 +43,10 @@ def test_null_arguments_are_refused(lib):
     assert "null" in nat.last_error()
     assert lib.smac_solve(None, None, None) == nat.BAD_ARG
     assert lib.smac_destroy(None) == nat.OK
+    assert lib.smac_async_create(None, None) == nat.BAD_ARG
+    assert lib.smac_async_submit(None, None, None, None, 1.0, None, None, None, None, None) == nat.BAD_ARG
+    assert lib.smac_async_wait(None, 0, None) == nat.BAD_ARG
+    lib.smac_async_destroy(None)
 
 
 def test_bad_options_are_refused(lib):
