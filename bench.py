@@ -325,6 +325,16 @@ def run_ours(args, ranks):
         ms, b = s_mixed.time_kernel(kid, reps=10)
         kernel_table[name] = {"ms": ms, "GB/s": b / (ms / 1e3) / 1e9}
 
+    # the solve alone (RHS in place; MG-PCG and the export of p_delta), beside
+    # the whole projection
+    solve_only = {}
+    for name, s in (("mixed", s_mixed), ("plain_fp64", s_plain)):
+        s.divergence(g, case.dt)
+        s.solve_rhs(pd)
+        ms_s, _ = timed(lambda: s.solve_rhs(pd), args.steps)
+        solve_only[name] = {"value": replicas.throughput(ranks, args.steps, ms_s), "unit": "solves/s",
+                            "ms_per_solve": ms_s / args.steps}
+
     # error of each result against an FP64 solve to 1e-12 of the same input
     # (relative 2-norm over the fluid cells, fluid mean removed)
     fluid = torch.from_numpy(W.interior(case.ct) == W.C_INTERIOR).to(dev)
@@ -361,6 +371,7 @@ def run_ours(args, ranks):
                   "alg_GBps": st_mixed[-1]["alg_bytes"] * args.steps / (ms_mixed / 1e3) / 1e9,
                   "error_vs_fp64_1e-12": err(p_mixed)},
         "speedup_mixed_vs_plain": sps_mixed / sps_plain,
+        "solve_only": solve_only,
         "e2e": e2e,
         "gpu_launches": launches,
         "roofline": roofline,
