@@ -148,6 +148,16 @@ smac_status smac_assemble_vof(const smac_grid_desc* desc, const double* alpha, d
                               const uint8_t* fzt, double* rho, double* fbx, double* fby, double* fbz,
                               double* firx, double* firy, double* firz, void* cuda_stream);
 
+/* Outlet boundary faces: f_b = 2 f_b of the neighbouring face on the interior
+ * side, where p = 0 is imposed.  G_SMACSolver::update_boundary_faces
+ * (CFD/G_SMACSolver_VoF.cu:1798-1950), run after smac_assemble_vof.  The
+ * marks (face arrays, uint8) give the interior side of an outlet face:
+ * 1 -> +1, 2 -> -1 (the reference's f_*internal_id_); 0 leaves a face as it
+ * is (walls keep f_b = 0).  Marked faces must have unmarked neighbours on the
+ * interior side (outlets on domain sides). */
+smac_status smac_update_boundary_faces(const smac_grid_desc* d, const uint8_t* fxo, const uint8_t* fyo,
+                                       const uint8_t* fzo, double* fbx, double* fby, double* fbz, void* stream);
+
 /* IBM solid fraction of cells 1..N+1 by 8^3 sub-sampling
  * (k_get_solid_fraction, CFD/G_SMACSolver_IBM.cu:94-147, clip >= 0.99 -> 1)
  * for a union of non-overlapping spheres (x, y, z, r per sphere, HOST array

@@ -64,7 +64,7 @@ EXPORTS = [
     "smac_ibm_solid_fraction_spheres", "smac_ibm_set_solid_cells", "smac_divergence", "smac_solve",
     "smac_set_rhs", "smac_correct", "smac_project", "smac_project_adjoint", "smac_apply_A", "smac_time_kernel",
     "smac_selftest_sweep", "smac_apply_A_dot_noalloc", "smac_async_create", "smac_async_submit",
-    "smac_async_wait", "smac_async_destroy",
+    "smac_async_wait", "smac_async_destroy", "smac_update_boundary_faces",
 ]
 
 
@@ -104,6 +104,7 @@ def load(path: str = LIB_PATH):
         "smac_async_submit": [vp, dp, dp, dp, d, dp, dp, dp, dp, ctypes.POINTER(ctypes.c_ulonglong)],
         "smac_async_wait": [vp, ctypes.c_ulonglong, ctypes.POINTER(Stats)],
         "smac_async_destroy": [vp],
+        "smac_update_boundary_faces": [ctypes.POINTER(GridDesc), u8p, u8p, u8p, dp, dp, dp, vp],
     }
     for name, args in sig.items():
         fn = getattr(lib, name)

@@ -922,6 +922,23 @@ smac_status smac_assemble_vof(const smac_grid_desc* d, const double* alpha, doub
   return SMAC_OK;
 }
 
+smac_status smac_update_boundary_faces(const smac_grid_desc* d, const uint8_t* fxo, const uint8_t* fyo,
+                                       const uint8_t* fzo, double* fbx, double* fby, double* fbz, void* stream) {
+  if (!d || !fxo || !fyo || !fzo || !fbx || !fby || !fbz) {
+    set_err("smac_update_boundary_faces: null argument");
+    return SMAC_BAD_ARG;
+  }
+  if (d->nx < 1 || d->ny < 1 || d->nz < 1) {
+    set_err("smac_update_boundary_faces: bad grid %d x %d x %d", d->nx, d->ny, d->nz);
+    return SMAC_BAD_SHAPE;
+  }
+  RefDims R{d->nx, d->ny, d->nz};
+  k_outlet_faces<<<grid_planes(d->nx + 3, d->ny + 3, d->nz + 3), kBlock, 0, (cudaStream_t)stream>>>(R, fxo, fyo, fzo,
+                                                                                                    fbx, fby, fbz);
+  CKL();
+  return SMAC_OK;
+}
+
 smac_status smac_ibm_solid_fraction_spheres(const smac_grid_desc* d, const double origin[3], const double* spheres,
                                             int nsph, double* sf, void* stream) {
   if (!d || !origin || (!spheres && nsph > 0) || nsph < 0 || !sf) {

@@ -1210,6 +1210,37 @@ __global__ void k_vof_faces(RefDims R, const double* __restrict__ rho, const uin
   }
 }
 
+// Outlet boundary faces (G_SMACSolver::update_boundary_faces,
+// CFD/G_SMACSolver_VoF.cu:1798-1950): f_b = 2 f_b of the neighbouring face on
+// the interior side (p = 0 on the outlet); mark 1: side +1, 2: side -1, 0:
+// untouched.  Marked faces have unmarked neighbours, so no face is read after
+// it is written.
+__global__ void k_outlet_faces(RefDims R, const uint8_t* __restrict__ fxo, const uint8_t* __restrict__ fyo,
+                               const uint8_t* __restrict__ fzo, double* fbx, double* fby, double* fbz) {
+  const int ix = blockIdx.x * blockDim.x + threadIdx.x;
+  const int iy = blockIdx.y * blockDim.y + threadIdx.y;
+  const int iz = blockIdx.z;
+  const int Nx = R.Nx, Ny = R.Ny, Nz = R.Nz;
+  if (ix < Nx + 3 && iy < Ny + 2 && iz < Nz + 2) {
+    const long long f = R.xf(ix, iy, iz);
+    const uint8_t m = fxo[f];
+    if (m == 1 && ix + 1 < Nx + 3) fbx[f] = DMUL(2.0, fbx[R.xf(ix + 1, iy, iz)]);
+    if (m == 2 && ix >= 1) fbx[f] = DMUL(2.0, fbx[R.xf(ix - 1, iy, iz)]);
+  }
+  if (ix < Nx + 2 && iy < Ny + 3 && iz < Nz + 2) {
+    const long long f = R.yf(ix, iy, iz);
+    const uint8_t m = fyo[f];
+    if (m == 1 && iy + 1 < Ny + 3) fby[f] = DMUL(2.0, fby[R.yf(ix, iy + 1, iz)]);
+    if (m == 2 && iy >= 1) fby[f] = DMUL(2.0, fby[R.yf(ix, iy - 1, iz)]);
+  }
+  if (ix < Nx + 2 && iy < Ny + 2 && iz < Nz + 3) {
+    const long long f = R.zf(ix, iy, iz);
+    const uint8_t m = fzo[f];
+    if (m == 1 && iz + 1 < Nz + 3) fbz[f] = DMUL(2.0, fbz[R.zf(ix, iy, iz + 1)]);
+    if (m == 2 && iz >= 1) fbz[f] = DMUL(2.0, fbz[R.zf(ix, iy, iz - 1)]);
+  }
+}
+
 // Solid fraction by 8^3 sub-sampling (k_get_solid_fraction,
 // CFD/G_SMACSolver_IBM.cu:94-147) for a union of non-overlapping spheres.
 // Cells entirely inside or outside a sphere by a margin far above the

@@ -325,6 +325,16 @@ def assemble_vof_device(N, h, alpha, rho0, rho1, ct, fxt, fyt, fzt):
     return rho, fb, fir
 
 
+def update_boundary_faces_device(N, h, marks, fb):
+    """Outlet faces in place on the device face coefficients fb = (fbx, fby,
+    fbz): smac_update_boundary_faces (G_SMACSolver::update_boundary_faces).
+    marks: uint8 face tensors, 1 / 2 = interior side +1 / -1, 0 = untouched."""
+    d = nat.GridDesc(*N, *h)
+    s = torch.cuda.current_stream().cuda_stream
+    nat.check(nat.load().smac_update_boundary_faces(ctypes.byref(d), *map(_ptr, marks), *map(_ptr, fb),
+                                                    ctypes.c_void_p(s)))
+
+
 def ibm_solid_fraction_device(N, h, origin, spheres, device="cuda"):
     sh = shapes(N)
     sf = torch.zeros(sh["cell"], dtype=torch.float64, device=device)

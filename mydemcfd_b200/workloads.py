@@ -141,6 +141,26 @@ def face_coeffs_vof(N, alpha, rho0, rho1, ct, fxt, fyt, fzt):
     return rho, (fbx, fby, fbz)
 
 
+def outlet_marks(N, sides):
+    """Face marks for outlets on domain sides ("x-", "x+", "y-", ...): the
+    boundary faces of that side get 1 (interior on the +1 side, low sides)
+    or 2 (interior on the -1 side, high sides), the reference's
+    f_*internal_id_ convention (CFD/G_SMACSolver_VoF.cu:1818-1833)."""
+    nx, ny, nz = N
+    sh = shapes(N)
+    marks = {k: np.zeros(sh[k], dtype=np.uint8) for k in "xyz"}
+    for s in sides:
+        a, side = s[0], s[1]
+        m = marks[a]
+        if a == "x":
+            m[1:nz + 1, 1:ny + 1, 1 if side == "-" else nx + 1] = 1 if side == "-" else 2
+        elif a == "y":
+            m[1:nz + 1, 1 if side == "-" else ny + 1, 1:nx + 1] = 1 if side == "-" else 2
+        else:
+            m[1 if side == "-" else nz + 1, 1:ny + 1, 1:nx + 1] = 1 if side == "-" else 2
+    return marks["x"], marks["y"], marks["z"]
+
+
 def constant_coeffs(N, fxt, fyt, fzt, value=1.0):
     """rho = 1 everywhere: f_b = 1 on F_INTERIOR faces, 0 on the others."""
     return tuple(np.where(t == F_INTERIOR, value, 0.0) for t in (fxt, fyt, fzt))

@@ -148,6 +148,15 @@ def set_solid_cells(N, sf, ct, fxt, fyt, fzt):
     lib().orc_set_solid_cells(*N, _p(sf), _u8(ct), _u8(fxt), _u8(fyt), _u8(fzt))
 
 
+def update_boundary_faces(N, fxo, fyo, fzo, fbx, fby, fbz):
+    """Outlet rule of G_SMACSolver::update_boundary_faces
+    (CFD/G_SMACSolver_VoF.cu:1798-1950) on copies of the face coefficients;
+    marks 1 / 2 give the interior side +1 / -1."""
+    fbx, fby, fbz = (np.array(a, dtype=np.float64, order="C", copy=True) for a in (fbx, fby, fbz))
+    lib().orc_update_boundary_faces(*N, _u8(fxo), _u8(fyo), _u8(fzo), _p(fbx), _p(fby), _p(fbz))
+    return fbx, fby, fbz
+
+
 def face_coeffs_vof(N, alpha, rho0, rho1, ct, fxt, fyt, fzt):
     rho = np.ones(cell_shape(N), np.float64)
     fbx = np.zeros(xface_shape(N)); fby = np.zeros(yface_shape(N)); fbz = np.zeros(zface_shape(N))

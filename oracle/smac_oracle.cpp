@@ -620,6 +620,40 @@ void orc_set_solid_cells(int Nx, int Ny, int Nz, const double* sf, uint8_t* ct, 
 // f_b = f_inv_rho = 1/(0.5(rho_L+rho_R)) on F_INTERIOR faces, 0 elsewhere.
 // rho must hold valid values on non-fluid cells on entry (only F_INTERIOR
 // faces read it, and those touch fluid cells only).
+// Outlet boundary faces (G_SMACSolver::update_boundary_faces,
+// CFD/G_SMACSolver_VoF.cu:1798-1950): f_b of an outlet face is twice the f_b
+// of the face next to it on the interior side (p = 0 on the outlet).  The
+// mark of a face gives that side: 1 -> +1 (f_xinternal_id_ >= 0), 2 -> -1;
+// 0 leaves the face alone (walls are already 0 from the face assembly).
+// Marked faces must have unmarked interior neighbours (outlets on domain
+// sides), so the result does not depend on the update order.
+void orc_update_boundary_faces(int Nx, int Ny, int Nz, const uint8_t* fxo, const uint8_t* fyo, const uint8_t* fzo,
+                               double* fbx, double* fby, double* fbz) {
+  View<const uint8_t> OX{fxo, Nx + 3, Ny + 2, Nz + 2}, OY{fyo, Nx + 2, Ny + 3, Nz + 2}, OZ{fzo, Nx + 2, Ny + 2, Nz + 3};
+  Arr BX{fbx, Nx + 3, Ny + 2, Nz + 2}, BY{fby, Nx + 2, Ny + 3, Nz + 2}, BZ{fbz, Nx + 2, Ny + 2, Nz + 3};
+  for (int iz = 0; iz < Nz + 2; ++iz)
+    for (int iy = 0; iy < Ny + 2; ++iy)
+      for (int ix = 0; ix < Nx + 3; ++ix) {
+        const uint8_t m = OX(ix, iy, iz);
+        if (m == 1 && ix + 1 < Nx + 3) BX(ix, iy, iz) = 2.0 * BX(ix + 1, iy, iz);
+        if (m == 2 && ix >= 1) BX(ix, iy, iz) = 2.0 * BX(ix - 1, iy, iz);
+      }
+  for (int iz = 0; iz < Nz + 2; ++iz)
+    for (int iy = 0; iy < Ny + 3; ++iy)
+      for (int ix = 0; ix < Nx + 2; ++ix) {
+        const uint8_t m = OY(ix, iy, iz);
+        if (m == 1 && iy + 1 < Ny + 3) BY(ix, iy, iz) = 2.0 * BY(ix, iy + 1, iz);
+        if (m == 2 && iy >= 1) BY(ix, iy, iz) = 2.0 * BY(ix, iy - 1, iz);
+      }
+  for (int iz = 0; iz < Nz + 3; ++iz)
+    for (int iy = 0; iy < Ny + 2; ++iy)
+      for (int ix = 0; ix < Nx + 2; ++ix) {
+        const uint8_t m = OZ(ix, iy, iz);
+        if (m == 1 && iz + 1 < Nz + 3) BZ(ix, iy, iz) = 2.0 * BZ(ix, iy, iz + 1);
+        if (m == 2 && iz >= 1) BZ(ix, iy, iz) = 2.0 * BZ(ix, iy, iz - 1);
+      }
+}
+
 void orc_face_coeffs_vof(int Nx, int Ny, int Nz, const double* alpha, double rho0, double rho1,
                          const uint8_t* ct, const uint8_t* fxt, const uint8_t* fyt, const uint8_t* fzt,
                          double* rho, double* fbx, double* fby, double* fbz, double* firx, double* firy,

@@ -14,7 +14,8 @@ import torch
 from mydemcfd_b200 import _native as nat
 from mydemcfd_b200 import workloads as W
 from mydemcfd_b200.solver import (B200PressureSolver, DeviceGrid, SMACStep, assemble_vof_device,
-                                  box_types_device, ibm_set_solid_device, ibm_solid_fraction_device)
+                                  box_types_device, ibm_set_solid_device, ibm_solid_fraction_device,
+                                  update_boundary_faces_device)
 
 from _cases import fluid_demeaned, load_golden, golden_names, oracle_solid_fraction, ref_grid, rel_err
 
@@ -223,6 +224,27 @@ def test_vof_1000_to_1(oracle_lib, precision):
     pd_o, _, _ = O.solve(ref_grid(case), tol=1e-13, stop_rule=O.STOP_REL_TRUE, max_iter=1000)
     err = rel_err(fluid_demeaned(W.interior(cpu(g.p_delta_)), case.ct), fluid_demeaned(W.interior(pd_o), case.ct))
     assert err < 1e-4
+
+
+def test_outlet_faces_bit_exact_and_outlet_solve(oracle_lib):
+    """Outlets on two sides (p = 0 there): the face rule is bit exact against
+    the oracle, and the non-singular GMG-PCG solve matches the oracle's."""
+    import dataclasses
+    O = oracle_lib
+    case = W.vof_case(32, seed=21, ratio=100.0)
+    marks = W.outlet_marks(case.N, ("x+", "y-"))
+    fb_o = O.update_boundary_faces(case.N, *marks, case.fbx, case.fby, case.fbz)
+    fb_d = [torch.from_numpy(np.ascontiguousarray(a)).cuda() for a in (case.fbx, case.fby, case.fbz)]
+    update_boundary_faces_device(case.N, case.h, [torch.from_numpy(m).cuda() for m in marks], fb_d)
+    torch.cuda.synchronize()
+    for a, b in zip(fb_d, fb_o):
+        assert np.array_equal(cpu(a), b)
+    oc = dataclasses.replace(case, fbx=fb_o[0], fby=fb_o[1], fbz=fb_o[2])
+    g, s, st = solve_gpu(oc, tol=1e-12, solver_type=nat.GMG_PCG)
+    assert st["status"] == 0
+    pd_o, _, st_o = O.solve(ref_grid(oc), solver_type=O.GMG_PCG, tol=1e-13, stop_rule=O.STOP_REL_TRUE, max_iter=1000)
+    assert st_o["converged"]
+    assert rel_err(W.interior(cpu(g.p_delta_)), W.interior(pd_o)) < 1e-9
 
 
 def test_ibm_solids_stay_zero_and_match_oracle(oracle_lib):

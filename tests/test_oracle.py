@@ -177,3 +177,21 @@ def test_oracle_matches_reference_golden(oracle_lib, name):
         assert np.array_equal(vy[case.fyt == W.F_INTERIOR], arr["vy"][case.fyt == W.F_INTERIOR])
         assert np.array_equal(vz[case.fzt == W.F_INTERIOR], arr["vz"][case.fzt == W.F_INTERIOR])
         assert np.array_equal(W.interior(p), W.interior(arr["p"]))
+
+
+def test_outlet_faces_twice_the_interior_neighbour(oracle_lib):
+    O = oracle_lib
+    N = (6, 5, 4)
+    ct, fxt, fyt, fzt = W.box_types(N)
+    rng = np.random.default_rng(3)
+    fb = [np.where(t == W.F_INTERIOR, rng.uniform(0.1, 1.0, t.shape), 0.0) for t in (fxt, fyt, fzt)]
+    marks = W.outlet_marks(N, ("x+", "z-"))
+    out = O.update_boundary_faces(N, *marks, *fb)
+    nx, ny, nz = N
+    mx, _, mz = marks
+    assert int((mx == 2).sum()) == ny * nz and int((mz == 1).sum()) == nx * ny
+    np.testing.assert_array_equal(out[0][:, :, nx + 1][mx[:, :, nx + 1] == 2],
+                                  2.0 * fb[0][:, :, nx][mx[:, :, nx + 1] == 2])
+    np.testing.assert_array_equal(out[2][1][mz[1] == 1], 2.0 * fb[2][2][mz[1] == 1])
+    for o, f, m in zip(out, fb, marks):
+        np.testing.assert_array_equal(o[m == 0], f[m == 0])
