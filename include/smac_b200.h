@@ -217,6 +217,57 @@ smac_status smac_project(smac_handle* h, const double* vxs, const double* vys, c
 smac_status smac_project_adjoint(smac_handle* h, const double* gvx, const double* gvy, const double* gvz,
                                  double* gvxs, double* gvys, double* gvzs, double* phi, smac_stats* stats);
 
+/* ---- after the projection ------------------------------------------------
+ * The reference's G_SMACSolver::update_boundary_ghost and make_face_gradp
+ * (CFD/G_SMACSolver.cu:1144-1363, CFD/G_BoundaryFunctions.cu:143-560), the
+ * consumers of p.  Grid-only calls (no handle), asynchronous on `stream`. */
+
+/* Pressure in solid and ghost cells (k_update_cell_boundary_pressure +
+ * k_update_cell_ghost_pressure, CFD/G_SMACSolver.cu:1144-1267), in place:
+ * a C_SOLID cell takes p of its first C_INTERIOR neighbour (x-, x+, y-, y+,
+ * z-, z+) shifted by rho g h (0 without one); every ghost cell then takes p
+ * of the nearest interior cell plus rho(src) g.r.  rho (cells) may be NULL
+ * (rho = 1); (gx, gy, gz) is SMACSolver::gx_, gy_, gz_. */
+smac_status smac_update_pressure_ghost(const smac_grid_desc* d, const uint8_t* celltype, const double* rho,
+                                       double gx, double gy, double gz, double* p, void* stream);
+
+/* The boundary-condition table bc_ (CFD/memberList/boundaryConditionMembers.def),
+ * HOST arrays of num_ids entries (1..256): BoundaryType codes (CFD/Enums.h:10-16:
+ * 0 no-slip, 1 slip, 2 inflow, 3 outflow, 4 outlet) and boundary velocities. */
+typedef struct {
+  int num_ids;
+  const uint8_t* type;
+  const double *vx, *vy, *vz;
+} smac_boundary_table;
+
+/* Velocity part of update_boundary_ghost, in place on (vx, vy, vz):
+ *  1. outlet faces (k_update_v*_outlet, CFD/G_BoundaryFunctions.cu:143-255):
+ *     a face with outlet mark 1 (interior side +1) or 2 (side -1) -- the marks
+ *     of smac_update_boundary_faces -- gets v = v* + sign f_b dt p_delta(face
+ *     index + side) / h, sign = -side; skipped when fxo/fyo/fzo are NULL;
+ *  2. ghost faces across each family's two tangential axes
+ *     (k_update_v*_ghost, :277-520) by the type of the id in f_*bcid_ of the
+ *     first face inside: inflow 2(1-lam)v_b - v2, no-slip -v2, outlet
+ *     2 v1 - v2, slip v2, outflow v1 (v1, v2 the first and second faces
+ *     inside, lam the f_ibm_area_solid_fraction_* entry of the first; lam*
+ *     may be NULL: 0); edge corners the mean of their two ghost neighbours
+ *     (k_update_v*_ghost_corner).
+ * Every grid extent must be >= 2.  bcid entries >= num_ids read as no-slip
+ * with velocity 0. */
+smac_status smac_update_velocity_ghost(const smac_grid_desc* d, const smac_boundary_table* bc, const uint8_t* fxbcid,
+                                       const uint8_t* fybcid, const uint8_t* fzbcid, const uint8_t* fxo,
+                                       const uint8_t* fyo, const uint8_t* fzo, const double* lamx, const double* lamy,
+                                       const double* lamz, const double* vxs, const double* vys, const double* vzs,
+                                       const double* fbx, const double* fby, const double* fbz, const double* p_delta,
+                                       double dt, double* vx, double* vy, double* vz, void* stream);
+
+/* Face pressure gradient, G_SMACSolver::make_face_gradp
+ * (CFD/G_SMACSolver.cu:1277-1343): gp_x(i) = (p(i) - p(i-x)) / dx and so on,
+ * on face indices 1..N+1 of every axis of each family (other entries are not
+ * written). */
+smac_status smac_face_gradp(const smac_grid_desc* d, const double* p, double* gpx, double* gpy, double* gpz,
+                            void* stream);
+
 /* y = A x with the FP64 fine operator (cells, reference layout, interior
  * entries); the reference's k_build_vof_poisson_Ap (G_PCGSolver.cu:214-245). */
 smac_status smac_apply_A(smac_handle* h, const double* x, double* y);

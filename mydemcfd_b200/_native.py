@@ -49,6 +49,12 @@ class Stats(ctypes.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+class BoundaryTable(ctypes.Structure):
+    """smac_boundary_table: the bc_ table (HOST arrays)."""
+    _fields_ = [("num_ids", ctypes.c_int), ("type", ctypes.c_void_p), ("vx", ctypes.c_void_p),
+                ("vy", ctypes.c_void_p), ("vz", ctypes.c_void_p)]
+
+
 class SmacError(RuntimeError):
     def __init__(self, status, msg):
         super().__init__(f"{STATUS_NAMES.get(status, status)}: {msg}")
@@ -64,7 +70,8 @@ EXPORTS = [
     "smac_ibm_solid_fraction_spheres", "smac_ibm_set_solid_cells", "smac_divergence", "smac_solve",
     "smac_set_rhs", "smac_correct", "smac_project", "smac_project_adjoint", "smac_apply_A", "smac_time_kernel",
     "smac_selftest_sweep", "smac_apply_A_dot_noalloc", "smac_async_create", "smac_async_submit",
-    "smac_async_wait", "smac_async_destroy", "smac_update_boundary_faces",
+    "smac_async_wait", "smac_async_destroy", "smac_update_boundary_faces", "smac_update_pressure_ghost",
+    "smac_update_velocity_ghost", "smac_face_gradp",
 ]
 
 
@@ -105,6 +112,10 @@ def load(path: str = LIB_PATH):
         "smac_async_wait": [vp, ctypes.c_ulonglong, ctypes.POINTER(Stats)],
         "smac_async_destroy": [vp],
         "smac_update_boundary_faces": [ctypes.POINTER(GridDesc), u8p, u8p, u8p, dp, dp, dp, vp],
+        "smac_update_pressure_ghost": [ctypes.POINTER(GridDesc), u8p, dp, d, d, d, dp, vp],
+        "smac_update_velocity_ghost": [ctypes.POINTER(GridDesc), ctypes.POINTER(BoundaryTable), u8p, u8p, u8p,
+                                       u8p, u8p, u8p, dp, dp, dp, dp, dp, dp, dp, dp, dp, dp, d, dp, dp, dp, vp],
+        "smac_face_gradp": [ctypes.POINTER(GridDesc), dp, dp, dp, dp, vp],
     }
     for name, args in sig.items():
         fn = getattr(lib, name)

@@ -72,6 +72,20 @@ class DeviceGrid:
     f_sx_: torch.Tensor | None = None
     f_sy_: torch.Tensor | None = None
     f_sz_: torch.Tensor | None = None
+    # read or written only by the pass after the projection
+    rho_: torch.Tensor | None = None
+    f_xbcid_: torch.Tensor | None = None
+    f_ybcid_: torch.Tensor | None = None
+    f_zbcid_: torch.Tensor | None = None
+    f_xoutlet_: torch.Tensor | None = None      # outlet marks (1 / 2: interior side +1 / -1)
+    f_youtlet_: torch.Tensor | None = None
+    f_zoutlet_: torch.Tensor | None = None
+    f_ibm_area_solid_fraction_x_: torch.Tensor | None = None
+    f_ibm_area_solid_fraction_y_: torch.Tensor | None = None
+    f_ibm_area_solid_fraction_z_: torch.Tensor | None = None
+    f_gradp_x_: torch.Tensor | None = None
+    f_gradp_y_: torch.Tensor | None = None
+    f_gradp_z_: torch.Tensor | None = None
 
     @property
     def N(self):
@@ -280,14 +294,34 @@ class AsyncProjector:
             pass
 
 
+@dataclass
+class BoundaryConditions:
+    """bc_ (CFD/memberList/boundaryConditionMembers.def): per boundary id its
+    BoundaryType (CFD/Enums.h:10-16) and boundary velocity, host arrays."""
+    bcType_: np.ndarray
+    vx_: np.ndarray
+    vy_: np.ndarray
+    vz_: np.ndarray
+
+    def table(self):
+        """(smac_boundary_table, the arrays it points into)."""
+        keep = [np.ascontiguousarray(self.bcType_, np.uint8)] + \
+            [np.ascontiguousarray(a, np.float64) for a in (self.vx_, self.vy_, self.vz_)]
+        t = nat.BoundaryTable(len(keep[0]), *(a.ctypes.data for a in keep))
+        return t, keep
+
+
 class SMACStep:
     """The G_SMACSolver calls around the seam, in the reference's order
-    (CFD/main.cu:313-315): solve_poisson(), then correct_vof_velocity()."""
+    (CFD/main.cu:313-317): solve_poisson(), correct_vof_velocity(),
+    update_boundary_ghost(), make_face_gradp()."""
 
-    def __init__(self, grid: DeviceGrid, dt: float = 1.0):
+    def __init__(self, grid: DeviceGrid, dt: float = 1.0, g=(0.0, 0.0, 0.0), bc: BoundaryConditions | None = None):
         self.grid_ = grid
         self.dt_ = float(dt)
         self.inv_dt_ = 1.0 / self.dt_
+        self.gx_, self.gy_, self.gz_ = (float(x) for x in g)
+        self.bc_ = bc
         self.pressure_solver_: B200PressureSolver | None = None
 
     def solve_poisson(self):
@@ -295,6 +329,30 @@ class SMACStep:
 
     def correct_vof_velocity(self):
         self.pressure_solver_.correct(self.grid_, self.dt_, zero_p_delta=True)
+
+    def update_boundary_ghost(self):
+        """G_SMACSolver::update_boundary_ghost (CFD/G_SMACSolver.cu:1345-1363):
+        p in solid and ghost cells, then outlet and ghost velocities."""
+        g = self.grid_
+        update_pressure_ghost_device(g.N, (g.dx_, g.dy_, g.dz_), g.celltype_, g.rho_, (self.gx_, self.gy_, self.gz_),
+                                     g.p_)
+        if self.bc_ is None or g.f_xbcid_ is None:
+            raise ValueError("update_boundary_ghost needs the boundary table bc_ and the grid's f_*bcid_")
+        marks = None if g.f_xoutlet_ is None else (g.f_xoutlet_, g.f_youtlet_, g.f_zoutlet_)
+        lam = None if g.f_ibm_area_solid_fraction_x_ is None else (
+            g.f_ibm_area_solid_fraction_x_, g.f_ibm_area_solid_fraction_y_, g.f_ibm_area_solid_fraction_z_)
+        update_velocity_ghost_device(g.N, (g.dx_, g.dy_, g.dz_), self.bc_, (g.f_xbcid_, g.f_ybcid_, g.f_zbcid_),
+                                     marks, lam, (g.f_vx_star_, g.f_vy_star_, g.f_vz_star_), (g.f_bx_, g.f_by_, g.f_bz_),
+                                     g.p_delta_, self.dt_, (g.f_vx_, g.f_vy_, g.f_vz_))
+
+    def make_face_gradp(self):
+        """G_SMACSolver::make_face_gradp (CFD/G_SMACSolver.cu:1336-1343)."""
+        g = self.grid_
+        if g.f_gradp_x_ is None:
+            sh = shapes(g.N)
+            g.f_gradp_x_, g.f_gradp_y_, g.f_gradp_z_ = (torch.zeros(sh[k], dtype=torch.float64, device=g.p_.device)
+                                                        for k in "xyz")
+        face_gradp_device(g.N, (g.dx_, g.dy_, g.dz_), g.p_, (g.f_gradp_x_, g.f_gradp_y_, g.f_gradp_z_))
 
 
 # -- set-up helpers on the device (reference layout) --------------------------
@@ -353,3 +411,36 @@ def ibm_set_solid_device(N, sf, ct, fxt, fyt, fzt):
     s = torch.cuda.current_stream().cuda_stream
     nat.check(nat.load().smac_ibm_set_solid_cells(ctypes.byref(d), _ptr(sf), _ptr(ct), _ptr(fxt), _ptr(fyt),
                                                   _ptr(fzt), ctypes.c_void_p(s)))
+
+
+# -- the pass after the projection (update_boundary_ghost, make_face_gradp) --
+def update_pressure_ghost_device(N, h, ct, rho, g, p):
+    """smac_update_pressure_ghost in place on p (cells); rho None means 1."""
+    d = nat.GridDesc(*N, *h)
+    s = torch.cuda.current_stream().cuda_stream
+    dd = ctypes.c_double
+    nat.check(nat.load().smac_update_pressure_ghost(ctypes.byref(d), _ptr(ct), _ptr(rho), dd(g[0]), dd(g[1]),
+                                                    dd(g[2]), _ptr(p), ctypes.c_void_p(s)))
+
+
+def update_velocity_ghost_device(N, h, bc: BoundaryConditions, bcid, marks, lam, vs, fb, p_delta, dt, v):
+    """smac_update_velocity_ghost in place on v = (vx, vy, vz): outlet faces
+    (marks None: none), then ghost faces and corners; lam None means 0."""
+    d = nat.GridDesc(*N, *h)
+    s = torch.cuda.current_stream().cuda_stream
+    table, keep = bc.table()
+    marks = marks if marks is not None else (None, None, None)
+    lam = lam if lam is not None else (None, None, None)
+    if marks[0] is None:
+        vs, fb, p_delta = (None, None, None), (None, None, None), None
+    nat.check(nat.load().smac_update_velocity_ghost(
+        ctypes.byref(d), ctypes.byref(table), *map(_ptr, bcid), *map(_ptr, marks), *map(_ptr, lam), *map(_ptr, vs),
+        *map(_ptr, fb), _ptr(p_delta), ctypes.c_double(dt), *map(_ptr, v), ctypes.c_void_p(s)))
+    del keep
+
+
+def face_gradp_device(N, h, p, gp):
+    """smac_face_gradp: gp = (gpx, gpy, gpz) face tensors, faces 1..N+1 written."""
+    d = nat.GridDesc(*N, *h)
+    s = torch.cuda.current_stream().cuda_stream
+    nat.check(nat.load().smac_face_gradp(ctypes.byref(d), _ptr(p), *map(_ptr, gp), ctypes.c_void_p(s)))

@@ -288,3 +288,80 @@ def demean_fluid(p, ct):
     pi[m] -= pi[m].mean()
     pi[~m] = 0.0
     return pi
+
+
+# Boundary types, CFD/Enums.h:10-16
+BC_NOSLIP, BC_SLIP, BC_INFLOW, BC_OUTFLOW, BC_OUTLET = 0, 1, 2, 3, 4
+
+
+@dataclass
+class PostCase:
+    """Inputs of the pass after the projection (update_boundary_ghost and
+    make_face_gradp), all in the reference layout."""
+    N: tuple
+    h: tuple
+    dt: float
+    g: tuple
+    bc_type: np.ndarray   # bc_.bcType_ per boundary id (uint8)
+    bc_v: tuple           # bc_.vx_, vy_, vz_ per boundary id
+    ct: np.ndarray
+    ft: tuple             # f_xtype_, f_ytype_, f_ztype_
+    bcid: tuple           # f_*bcid_ (uint8)
+    marks: tuple          # outlet marks: 1 interior side +1, 2 interior side -1
+    internal_id: tuple    # f_*internal_id_ (int32): +1 / -1 on outlet faces, 0 elsewhere
+    lam: tuple            # f_ibm_area_solid_fraction_* (or None)
+    p: np.ndarray
+    p_delta: np.ndarray
+    rho: np.ndarray
+    vs: tuple             # v*
+    fb: tuple
+    v: tuple              # velocity after the correction
+
+
+def post_case(N, seed, h=(0.03125, 0.03125, 0.03125), dt=0.5, g=(0.0, -1.5, -9.8), sides=("x+", "z-"),
+              solid_fraction=0.0, lam=True):
+    """Seeded inputs for the post-projection pass.  Boundary ids 0..4 carry
+    the types NOSLIP, SLIP, INFLOW, OUTFLOW, OUTLET with U[-1,1) boundary
+    velocities; every face gets a U{0..3} id except the outlet faces of
+    `sides`, which get id 4 (so the marks and the ids agree).  With
+    solid_fraction > 0 that share of the cells 2..N-1 (in clusters, so some
+    have no interior neighbour) become C_SOLID.  Fields are U[-1,1) (rho in
+    [1, 1000), f_b in [0.1, 1) on F_INTERIOR faces, lam in [0, 1))."""
+    N = tuple(int(n) for n in N)
+    sh = shapes(N)
+    rnd = lambda tag, key, lo=-1.0, hi=1.0: (lo + (hi - lo) * uniform01(substream(seed, tag),  # noqa: E731
+                                                                         int(np.prod(sh[key])))).reshape(sh[key])
+    ct, fxt, fyt, fzt = box_types(N)
+    if solid_fraction > 0.0:
+        nx, ny, nz = N
+        # clusters: coarse blocks of 2^3 cells switched on together, then thinned
+        blk = (uniform01(substream(seed, 90), int(np.prod(sh["cell"]))).reshape(sh["cell"]) < solid_fraction)
+        coarse = blk[::2, ::2, ::2]
+        dense = np.repeat(np.repeat(np.repeat(coarse, 2, 0), 2, 1), 2, 2)[:sh["cell"][0], :sh["cell"][1],
+                                                                           :sh["cell"][2]]
+        thin = uniform01(substream(seed, 91), int(np.prod(sh["cell"]))).reshape(sh["cell"]) < 0.85
+        sf = np.zeros(sh["cell"])
+        inner = np.zeros(sh["cell"], bool)
+        inner[2:nz, 2:ny, 2:nx] = True
+        sf[inner & dense & thin] = 1.0
+        set_solid_cells(sf, ct, fxt, fyt, fzt)
+    marks = outlet_marks(N, sides)
+    bcid = []
+    for tag, (key, m) in enumerate(zip("xyz", marks)):
+        ids = np.minimum((uniform01(substream(seed, 10 + tag), int(np.prod(sh[key]))) * 4).astype(np.uint8),
+                         3).reshape(sh[key])
+        ids[m != 0] = BC_OUTLET
+        bcid.append(np.ascontiguousarray(ids))
+    internal_id = tuple(np.where(m == 1, 1, np.where(m == 2, -1, 0)).astype(np.int32) for m in marks)
+    bc_type = np.array([BC_NOSLIP, BC_SLIP, BC_INFLOW, BC_OUTFLOW, BC_OUTLET], np.uint8)
+    bc_v = tuple(uniform_pm1(substream(seed, 20 + k), 5) for k in range(3))
+    lam_t = tuple(np.ascontiguousarray(rnd(30 + k, key, 0.0, 1.0)) for k, key in enumerate("xyz")) if lam else None
+    fb = tuple(np.where(t == F_INTERIOR, rnd(40 + k, key, 0.1, 1.0), 0.0) for k, (key, t) in
+               enumerate(zip("xyz", (fxt, fyt, fzt))))
+    return PostCase(N=N, h=tuple(float(x) for x in h), dt=float(dt), g=tuple(float(x) for x in g),
+                    bc_type=bc_type, bc_v=bc_v, ct=ct, ft=(fxt, fyt, fzt), bcid=tuple(bcid), marks=marks,
+                    internal_id=internal_id, lam=lam_t, p=rnd(50, "cell"), p_delta=rnd(51, "cell"),
+                    rho=rnd(52, "cell", 1.0, 1000.0),
+                    vs=tuple(np.ascontiguousarray(rnd(60 + k, key)) for k, key in enumerate("xyz")),
+                    fb=tuple(np.ascontiguousarray(a) for a in fb),
+                    v=tuple(np.ascontiguousarray(rnd(70 + k, key)) for k, key in enumerate("xyz")))

@@ -157,6 +157,61 @@ def update_boundary_faces(N, fxo, fyo, fzo, fbx, fby, fbz):
     return fbx, fby, fbz
 
 
+def pressure_ghost(N, h, g, ct, rho, p):
+    """Pressure part of G_SMACSolver::update_boundary_ghost
+    (CFD/G_SMACSolver.cu:1144-1267) on a copy of p: C_SOLID cells from their
+    first C_INTERIOR neighbour, ghost cells from the nearest interior cell,
+    both shifted hydrostatically by rho g."""
+    p = np.array(p, dtype=np.float64, order="C", copy=True)
+    rho = np.ascontiguousarray(rho, dtype=np.float64)
+    c = ctypes.c_double
+    lib().orc_pressure_ghost(*N, c(h[0]), c(h[1]), c(h[2]), c(g[0]), c(g[1]), c(g[2]), _u8(ct), _p(rho), _p(p))
+    return p
+
+
+def face_gradp(N, h, p):
+    """G_SMACSolver::make_face_gradp (CFD/G_SMACSolver.cu:1277-1343): face
+    pressure gradients on faces 1..N+1 of each family; other entries 0."""
+    p = np.ascontiguousarray(p, dtype=np.float64)
+    gx = np.zeros(xface_shape(N)); gy = np.zeros(yface_shape(N)); gz = np.zeros(zface_shape(N))
+    c = ctypes.c_double
+    lib().orc_face_gradp(*N, c(h[0]), c(h[1]), c(h[2]), _p(p), _p(gx), _p(gy), _p(gz))
+    return gx, gy, gz
+
+
+def velocity_outlet(N, h, dt, marks, vs, fb, p_delta, v):
+    """k_update_v{x,y,z}_outlet (CFD/G_BoundaryFunctions.cu:143-255) on copies
+    of the velocities v."""
+    v = [np.array(a, dtype=np.float64, order="C", copy=True) for a in v]
+    c = ctypes.c_double
+    lib().orc_velocity_outlet(*N, c(h[0]), c(h[1]), c(h[2]), c(dt), *(_u8(m) for m in marks),
+                              *(_p(np.ascontiguousarray(a)) for a in vs), *(_p(np.ascontiguousarray(a)) for a in fb),
+                              _p(np.ascontiguousarray(p_delta)), *(_p(a) for a in v))
+    return tuple(v)
+
+
+def velocity_ghost(N, bc_type, bc_v, bcid, lam, v):
+    """k_update_v*_ghost + k_update_v*_ghost_corner
+    (CFD/G_BoundaryFunctions.cu:277-560) on copies of the velocities v."""
+    v = [np.array(a, dtype=np.float64, order="C", copy=True) for a in v]
+    bct = np.ascontiguousarray(bc_type, np.uint8)
+    bv = [np.ascontiguousarray(a, np.float64) for a in bc_v]
+    lam = (None, None, None) if lam is None else tuple(np.ascontiguousarray(a) for a in lam)
+    lib().orc_velocity_ghost(*N, _u8(bct), *(_p(a) for a in bv), *(_u8(np.ascontiguousarray(b)) for b in bcid),
+                             *(_p(a) for a in lam), *(_p(a) for a in v))
+    return tuple(v)
+
+
+def post_pass(case):
+    """G_SMACSolver::update_boundary_ghost then make_face_gradp
+    (CFD/G_SMACSolver.cu:1277-1363) on a workloads.PostCase: returns
+    (p, (vx, vy, vz), (gpx, gpy, gpz))."""
+    p = pressure_ghost(case.N, case.h, case.g, case.ct, case.rho, case.p)
+    v = velocity_outlet(case.N, case.h, case.dt, case.marks, case.vs, case.fb, case.p_delta, case.v)
+    v = velocity_ghost(case.N, case.bc_type, case.bc_v, case.bcid, case.lam, v)
+    return p, v, face_gradp(case.N, case.h, p)
+
+
 def face_coeffs_vof(N, alpha, rho0, rho1, ct, fxt, fyt, fzt):
     rho = np.ones(cell_shape(N), np.float64)
     fbx = np.zeros(xface_shape(N)); fby = np.zeros(yface_shape(N)); fbz = np.zeros(zface_shape(N))

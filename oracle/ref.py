@@ -103,3 +103,90 @@ def solve(case, solver_type=3, tol=1e-11, levels=4, do_correct=True, eps=None, e
     out["solve_ms"] = o.solve_ms
     out["correct_ms"] = o.correct_ms
     return out
+
+
+class RefPostInputs(ctypes.Structure):
+    _fields_ = [
+        ("Nx", ctypes.c_int), ("Ny", ctypes.c_int), ("Nz", ctypes.c_int),
+        ("Lx", ctypes.c_double), ("Ly", ctypes.c_double), ("Lz", ctypes.c_double), ("dt", ctypes.c_double),
+        ("gx", ctypes.c_double), ("gy", ctypes.c_double), ("gz", ctypes.c_double),
+        ("num_ids", ctypes.c_int), ("bc_type", _u8p), ("bc_vx", _dp), ("bc_vy", _dp), ("bc_vz", _dp),
+        ("p", _dp), ("p_delta", _dp), ("rho", _dp),
+        ("ct", _u8p), ("fxt", _u8p), ("fyt", _u8p), ("fzt", _u8p), ("fxbcid", _u8p), ("fybcid", _u8p),
+        ("fzbcid", _u8p),
+        ("fxid", ctypes.POINTER(ctypes.c_int)), ("fyid", ctypes.POINTER(ctypes.c_int)),
+        ("fzid", ctypes.POINTER(ctypes.c_int)),
+        ("lamx", _dp), ("lamy", _dp), ("lamz", _dp),
+        ("vxs", _dp), ("vys", _dp), ("vzs", _dp), ("fbx", _dp), ("fby", _dp), ("fbz", _dp),
+        ("vx", _dp), ("vy", _dp), ("vz", _dp),
+    ]
+
+
+class RefPostOutputs(ctypes.Structure):
+    _fields_ = [(k, _dp) for k in ("p", "vx", "vy", "vz", "gpx", "gpy", "gpz")]
+
+
+def grid_spacing(N, h):
+    """The spacing the reference computes from the domain size: (N h) / N."""
+    return tuple(float(np.float64(n * hh) / np.float64(n)) for n, hh in zip(N, h))
+
+
+def post(case):
+    """Run the reference's update_boundary_ghost + make_face_gradp on a
+    mydemcfd_b200.workloads.PostCase (lam None -> zeros)."""
+    L = lib()
+    if not hasattr(L, "_post_set"):
+        L.ref_post.restype = ctypes.c_int
+        L.ref_post.argtypes = [ctypes.POINTER(RefPostInputs), ctypes.POINTER(RefPostOutputs)]
+        L._post_set = True
+    nx, ny, nz = case.N
+    ghost = np.ones(case.ct.shape, bool)
+    ghost[1:nz + 1, 1:ny + 1, 1:nx + 1] = False
+    # a C_SOLID ghost cell would make the reference read the cell type one
+    # entry past its own index range
+    assert not np.any(case.ct[ghost] == 3), "solid ghost cells are not passed to the reference"
+    i = RefPostInputs()
+    i.Nx, i.Ny, i.Nz = case.N
+    i.Lx, i.Ly, i.Lz = (n * hh for n, hh in zip(case.N, case.h))
+    i.dt = case.dt
+    i.gx, i.gy, i.gz = case.g
+    keep = []
+
+    def d(a):
+        a = np.ascontiguousarray(a, np.float64)
+        keep.append(a)
+        return _p(a)
+
+    def u8(a):
+        a = np.ascontiguousarray(a, np.uint8)
+        keep.append(a)
+        return _p(a, ctypes.c_uint8)
+
+    def i32(a):
+        a = np.ascontiguousarray(a, np.int32)
+        keep.append(a)
+        return _p(a, ctypes.c_int)
+
+    i.num_ids = len(case.bc_type)
+    i.bc_type = u8(case.bc_type)
+    i.bc_vx, i.bc_vy, i.bc_vz = (d(a) for a in case.bc_v)
+    i.p, i.p_delta, i.rho = d(case.p), d(case.p_delta), d(case.rho)
+    i.ct = u8(case.ct)
+    i.fxt, i.fyt, i.fzt = (u8(a) for a in case.ft)
+    i.fxbcid, i.fybcid, i.fzbcid = (u8(a) for a in case.bcid)
+    i.fxid, i.fyid, i.fzid = (i32(a) for a in case.internal_id)
+    lam = case.lam if case.lam is not None else tuple(np.zeros(a.shape) for a in case.v)
+    i.lamx, i.lamy, i.lamz = (d(a) for a in lam)
+    i.vxs, i.vys, i.vzs = (d(a) for a in case.vs)
+    i.fbx, i.fby, i.fbz = (d(a) for a in case.fb)
+    i.vx, i.vy, i.vz = (d(a) for a in case.v)
+    out = {"p": np.zeros(case.p.shape), "vx": np.zeros(case.v[0].shape), "vy": np.zeros(case.v[1].shape),
+           "vz": np.zeros(case.v[2].shape), "gpx": np.zeros(case.v[0].shape), "gpy": np.zeros(case.v[1].shape),
+           "gpz": np.zeros(case.v[2].shape)}
+    o = RefPostOutputs()
+    for k, a in out.items():
+        setattr(o, k, _p(a))
+    rc = L.ref_post(ctypes.byref(i), ctypes.byref(o))
+    if rc != 0:
+        raise RuntimeError(f"ref_post returned {rc}")
+    return out

@@ -7,7 +7,9 @@
 // It follows the reference driver's set-up (CFD/main.cu:183-243): a host
 // SMACSolver with calloc'ed members, G_SMACSolver::solver_malloc + cpuTogpu,
 // G_PCGSolver + G_GMGSolver::initialize, set_solver, tol_, then
-// G_SMACSolver::solve_poisson() and correct_vof_velocity().
+// G_SMACSolver::solve_poisson() and correct_vof_velocity().  A second entry,
+// ref_post, runs the pass after the projection (update_boundary_ghost and
+// make_face_gradp) on given arrays.
 //
 // Two things the reference leaves to chance are pinned here: every multigrid
 // level array is zeroed after G_GMGSolver::initialize (the reference reads
@@ -188,6 +190,74 @@ int ref_solve(const ref_inputs* in, ref_outputs* out) {
   cudaEventDestroy(ev0);
   cudaEventDestroy(ev1);
   if (gmg) gmgs.free_levels();
+  g.solver_free();
+  solv.solver_free();
+  return e == cudaSuccess ? 0 : -2;
+}
+
+struct ref_post_inputs {
+  int Nx, Ny, Nz;
+  double Lx, Ly, Lz, dt, gx, gy, gz;
+  int num_ids;                         // bc_.num_boundary_id_
+  const uint8_t* bc_type;              // bc_.bcType_
+  const double *bc_vx, *bc_vy, *bc_vz; // bc_.vx_, vy_, vz_
+  const double *p, *p_delta, *rho;
+  const uint8_t *ct, *fxt, *fyt, *fzt, *fxbcid, *fybcid, *fzbcid;
+  const int *fxid, *fyid, *fzid;       // f_*internal_id_
+  const double *lamx, *lamy, *lamz;    // f_ibm_area_solid_fraction_*
+  const double *vxs, *vys, *vzs, *fbx, *fby, *fbz, *vx, *vy, *vz;
+};
+
+struct ref_post_outputs {
+  double *p, *vx, *vy, *vz, *gpx, *gpy, *gpz;
+};
+
+// G_SMACSolver::update_boundary_ghost then make_face_gradp
+// (CFD/G_SMACSolver.cu:1277-1363), the reference's pass after the projection,
+// on host arrays.  Returns 0 on success, -2 on a CUDA error.
+int ref_post(const ref_post_inputs* in, ref_post_outputs* out) {
+  const int Nx = in->Nx, Ny = in->Ny, Nz = in->Nz;
+  SMACSolver solv;
+  solv.set_calc_properties(0., 0., 0., in->Lx, in->Ly, in->Lz, Nx, Ny, Nz);
+  solv.grid_.bc_.num_boundary_id_ = in->num_ids;
+  solv.solver_malloc();
+  solv.gx_ = in->gx; solv.gy_ = in->gy; solv.gz_ = in->gz;
+  solv.dt_ = in->dt;
+  solv.inv_dt_ = 1. / in->dt;
+  StaggeredGrid& hg = solv.grid_;
+  put(hg.p_, in->p); put(hg.p_delta_, in->p_delta); put(hg.rho_, in->rho);
+  put(hg.celltype_, in->ct); put(hg.f_xtype_, in->fxt); put(hg.f_ytype_, in->fyt); put(hg.f_ztype_, in->fzt);
+  put(hg.f_xbcid_, in->fxbcid); put(hg.f_ybcid_, in->fybcid); put(hg.f_zbcid_, in->fzbcid);
+  put(hg.f_xinternal_id_, in->fxid); put(hg.f_yinternal_id_, in->fyid); put(hg.f_zinternal_id_, in->fzid);
+  put(hg.f_ibm_area_solid_fraction_x_, in->lamx); put(hg.f_ibm_area_solid_fraction_y_, in->lamy);
+  put(hg.f_ibm_area_solid_fraction_z_, in->lamz);
+  put(hg.f_vx_star_, in->vxs); put(hg.f_vy_star_, in->vys); put(hg.f_vz_star_, in->vzs);
+  put(hg.f_bx_, in->fbx); put(hg.f_by_, in->fby); put(hg.f_bz_, in->fbz);
+  put(hg.f_vx_, in->vx); put(hg.f_vy_, in->vy); put(hg.f_vz_, in->vz);
+  std::memcpy(hg.bc_.bcType_.data_, in->bc_type, (size_t)in->num_ids);
+  std::memcpy(hg.bc_.vx_.data_, in->bc_vx, sizeof(double) * (size_t)in->num_ids);
+  std::memcpy(hg.bc_.vy_.data_, in->bc_vy, sizeof(double) * (size_t)in->num_ids);
+  std::memcpy(hg.bc_.vz_.data_, in->bc_vz, sizeof(double) * (size_t)in->num_ids);
+
+  G_SMACSolver g;
+  g.set_calc_properties(0., 0., 0., in->Lx, in->Ly, in->Lz, Nx, Ny, Nz);
+  g.grid_.bc_.num_boundary_id_ = in->num_ids;
+  g.solver_malloc();
+  g.cpuTogpu(solv.grid_);
+  g.set_block_grid(Nx, Ny, Nz);
+  g.dt_ = in->dt;
+  g.inv_dt_ = 1. / in->dt;
+  g.update_boundary_ghost(solv);
+  g.make_face_gradp();
+  cudaDeviceSynchronize();
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) {
+    g.gpuTocpu(solv.grid_);
+    get(hg.p_, out->p);
+    get(hg.f_vx_, out->vx); get(hg.f_vy_, out->vy); get(hg.f_vz_, out->vz);
+    get(hg.f_gradp_x_, out->gpx); get(hg.f_gradp_y_, out->gpy); get(hg.f_gradp_z_, out->gpz);
+    e = cudaGetLastError();
+  }
   g.solver_free();
   solv.solver_free();
   return e == cudaSuccess ? 0 : -2;

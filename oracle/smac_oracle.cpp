@@ -620,6 +620,176 @@ void orc_set_solid_cells(int Nx, int Ny, int Nz, const double* sf, uint8_t* ct, 
 // f_b = f_inv_rho = 1/(0.5(rho_L+rho_R)) on F_INTERIOR faces, 0 elsewhere.
 // rho must hold valid values on non-fluid cells on entry (only F_INTERIOR
 // faces read it, and those touch fluid cells only).
+// Pressure in solid and ghost cells after a projection, the pressure part of
+// G_SMACSolver::update_boundary_ghost (CFD/G_SMACSolver.cu:1144-1267):
+//  1. a C_SOLID cell takes p of its first C_INTERIOR neighbour in the order
+//     x-, x+, y-, y+, z-, z+, shifted hydrostatically by rho g h (0 without
+//     such a neighbour);
+//  2. every ghost cell (an index 0 or N+1) takes p of the nearest interior
+//     cell (indices clamped to 1..N), shifted by rho(src) g.r.
+// The reference's first kernel also writes the ghost cells, racing at edges
+// and corners; its second kernel overwrites all of them, so this final
+// state is the reference's.
+void orc_pressure_ghost(int Nx, int Ny, int Nz, double dx, double dy, double dz, double gx, double gy, double gz,
+                        const uint8_t* ct, const double* rho, double* p) {
+  View<const uint8_t> C{ct, Nx + 2, Ny + 2, Nz + 2};
+  View<const double> R{rho, Nx + 2, Ny + 2, Nz + 2};
+  Arr P{p, Nx + 2, Ny + 2, Nz + 2};
+  for (int iz = 1; iz <= Nz; ++iz)
+    for (int iy = 1; iy <= Ny; ++iy)
+      for (int ix = 1; ix <= Nx; ++ix) {
+        if (C(ix, iy, iz) != C_SOLID) continue;
+        double v;
+        if (C(ix - 1, iy, iz) == C_INTERIOR) v = P(ix - 1, iy, iz) + R(ix - 1, iy, iz) * gx * dx;
+        else if (C(ix + 1, iy, iz) == C_INTERIOR) v = P(ix + 1, iy, iz) - R(ix + 1, iy, iz) * gx * dx;
+        else if (C(ix, iy - 1, iz) == C_INTERIOR) v = P(ix, iy - 1, iz) + R(ix, iy - 1, iz) * gy * dy;
+        else if (C(ix, iy + 1, iz) == C_INTERIOR) v = P(ix, iy + 1, iz) - R(ix, iy + 1, iz) * gy * dy;
+        else if (C(ix, iy, iz - 1) == C_INTERIOR) v = P(ix, iy, iz - 1) + R(ix, iy, iz - 1) * gz * dz;
+        else if (C(ix, iy, iz + 1) == C_INTERIOR) v = P(ix, iy, iz + 1) - R(ix, iy, iz + 1) * gz * dz;
+        else v = 0.;
+        P(ix, iy, iz) = v;
+      }
+  for (int iz = 0; iz < Nz + 2; ++iz)
+    for (int iy = 0; iy < Ny + 2; ++iy)
+      for (int ix = 0; ix < Nx + 2; ++ix) {
+        const bool ghost = ix == 0 || ix == Nx + 1 || iy == 0 || iy == Ny + 1 || iz == 0 || iz == Nz + 1;
+        if (!ghost) continue;
+        const int sx = ix == 0 ? 1 : ix == Nx + 1 ? Nx : ix;
+        const int sy = iy == 0 ? 1 : iy == Ny + 1 ? Ny : iy;
+        const int sz = iz == 0 ? 1 : iz == Nz + 1 ? Nz : iz;
+        const double rx = (double)(ix - sx) * dx, ry = (double)(iy - sy) * dy, rz = (double)(iz - sz) * dz;
+        P(ix, iy, iz) = P(sx, sy, sz) + R(sx, sy, sz) * (rx * gx + ry * gy + rz * gz);
+      }
+}
+
+// Face pressure gradient, G_SMACSolver::make_face_gradp
+// (CFD/G_SMACSolver.cu:1277-1343): g_x(ix) = (p(ix) - p(ix-1)) / dx on faces
+// 1..N+1 of each family (rows and planes 1..N+1 as the reference's threads).
+void orc_face_gradp(int Nx, int Ny, int Nz, double dx, double dy, double dz, const double* p, double* gpx,
+                    double* gpy, double* gpz) {
+  View<const double> P{p, Nx + 2, Ny + 2, Nz + 2};
+  Arr GX{gpx, Nx + 3, Ny + 2, Nz + 2}, GY{gpy, Nx + 2, Ny + 3, Nz + 2}, GZ{gpz, Nx + 2, Ny + 2, Nz + 3};
+  const double ix_ = 1. / dx, iy_ = 1. / dy, iz_ = 1. / dz;
+  for (int iz = 1; iz < Nz + 2; ++iz)
+    for (int iy = 1; iy < Ny + 2; ++iy)
+      for (int ix = 1; ix < Nx + 2; ++ix) {
+        GX(ix, iy, iz) = (P(ix, iy, iz) - P(ix - 1, iy, iz)) * ix_;
+        GY(ix, iy, iz) = (P(ix, iy, iz) - P(ix, iy - 1, iz)) * iy_;
+        GZ(ix, iy, iz) = (P(ix, iy, iz) - P(ix, iy, iz - 1)) * iz_;
+      }
+}
+
+// Velocity on outlet faces, k_update_v{x,y,z}_outlet
+// (CFD/G_BoundaryFunctions.cu:143-255), run by update_boundary_ghost: a face
+// with the outlet mark m (1: interior side +1, 2: interior side -1) gets
+//   v = v* + sign f_b dt p_delta(interior cell) / h,  sign = +1 for m = 2, -1 for m = 1,
+// for face indices 1..N+1 on all three axes (the reference's thread range).
+// Other mark values, and marks whose interior cell index would pass N+1
+// (where the reference reads the next row), are left alone.
+void orc_velocity_outlet(int Nx, int Ny, int Nz, double dx, double dy, double dz, double dt, const uint8_t* fxo,
+                         const uint8_t* fyo, const uint8_t* fzo, const double* vxs, const double* vys,
+                         const double* vzs, const double* fbx, const double* fby, const double* fbz,
+                         const double* pd, double* vx, double* vy, double* vz) {
+  View<const uint8_t> MX{fxo, Nx + 3, Ny + 2, Nz + 2}, MY{fyo, Nx + 2, Ny + 3, Nz + 2}, MZ{fzo, Nx + 2, Ny + 2, Nz + 3};
+  View<const double> SX{vxs, Nx + 3, Ny + 2, Nz + 2}, SY{vys, Nx + 2, Ny + 3, Nz + 2}, SZ{vzs, Nx + 2, Ny + 2, Nz + 3};
+  View<const double> BX{fbx, Nx + 3, Ny + 2, Nz + 2}, BY{fby, Nx + 2, Ny + 3, Nz + 2}, BZ{fbz, Nx + 2, Ny + 2, Nz + 3};
+  View<const double> P{pd, Nx + 2, Ny + 2, Nz + 2};
+  Arr VX{vx, Nx + 3, Ny + 2, Nz + 2}, VY{vy, Nx + 2, Ny + 3, Nz + 2}, VZ{vz, Nx + 2, Ny + 2, Nz + 3};
+  const double ix_ = 1. / dx, iy_ = 1. / dy, iz_ = 1. / dz;
+  for (int iz = 1; iz < Nz + 2; ++iz)
+    for (int iy = 1; iy < Ny + 2; ++iy)
+      for (int ix = 1; ix < Nx + 2; ++ix) {
+        if (const uint8_t m = MX(ix, iy, iz); (m == 1 || m == 2) && ix + (m == 1) <= Nx + 1) {
+          const int s = m == 1 ? 1 : -1;
+          const double sign = s < 0 ? 1. : -1.;
+          VX(ix, iy, iz) = SX(ix, iy, iz) + sign * BX(ix, iy, iz) * dt * P(ix + s, iy, iz) * ix_;
+        }
+        if (const uint8_t m = MY(ix, iy, iz); (m == 1 || m == 2) && iy + (m == 1) <= Ny + 1) {
+          const int s = m == 1 ? 1 : -1;
+          const double sign = s < 0 ? 1. : -1.;
+          VY(ix, iy, iz) = SY(ix, iy, iz) + sign * BY(ix, iy, iz) * dt * P(ix, iy + s, iz) * iy_;
+        }
+        if (const uint8_t m = MZ(ix, iy, iz); (m == 1 || m == 2) && iz + (m == 1) <= Nz + 1) {
+          const int s = m == 1 ? 1 : -1;
+          const double sign = s < 0 ? 1. : -1.;
+          VZ(ix, iy, iz) = SZ(ix, iy, iz) + sign * BZ(ix, iy, iz) * dt * P(ix, iy, iz + s) * iz_;
+        }
+      }
+}
+
+}  // extern "C"
+
+namespace {
+
+// d_get_velocity_ghost_value (CFD/G_BoundaryFunctions.cu:258-275); boundary
+// types from CFD/Enums.h:10-16.
+double ghost_value(uint8_t type, double vb, double lam, double bnd, double inner) {
+  if (type == 2) return 2.0 * (1.0 - lam) * vb - inner;  // BC_INFLOW
+  if (type == 0) return -inner;                          // BC_NOSLIP
+  if (type == 4) return 2.0 * bnd - inner;               // BC_OUTLET
+  if (type == 1) return inner;                           // BC_SLIP
+  return bnd;                                            // BC_OUTFLOW
+}
+
+// One face family: normal axis a, ghosts across the two other axes b < c.
+// k_update_v*_ghost then k_update_v*_ghost_corner
+// (CFD/G_BoundaryFunctions.cu:277-560).
+void velocity_ghost_family(const int N[3], int a, const uint8_t* bct, const double* bvel, const uint8_t* bcid,
+                           const double* lam, double* v) {
+  int S[3] = {N[0] + 2, N[1] + 2, N[2] + 2};
+  S[a] += 1;
+  auto at = [&](const int i[3]) { return ((size_t)i[2] * S[1] + i[1]) * S[0] + i[0]; };
+  const int b = a == 0 ? 1 : 0, c = a == 2 ? 1 : 2;
+  int i[3];
+  for (int ia = 1; ia < N[a] + 2; ++ia) {
+    i[a] = ia;
+    // edges of the b-c ring, corners excluded
+    for (int side = 0; side < 4; ++side) {
+      const int g = side < 2 ? b : c, o = side < 2 ? c : b;  // ghost axis, other axis
+      const bool low = (side & 1) == 0;
+      for (int io = 1; io <= N[o]; ++io) {
+        i[o] = io;
+        int ib[3] = {i[0], i[1], i[2]}, in[3] = {i[0], i[1], i[2]};
+        ib[g] = low ? 1 : N[g];
+        in[g] = low ? 2 : N[g] - 1;
+        i[g] = low ? 0 : N[g] + 1;
+        const int id = bcid[at(ib)];
+        v[at(i)] = ghost_value(bct[id], bvel[id], lam ? lam[at(ib)] : 0., v[at(ib)], v[at(in)]);
+      }
+    }
+    // corners: the mean of the two neighbouring ghost values
+    for (int cb = 0; cb < 2; ++cb)
+      for (int cc = 0; cc < 2; ++cc) {
+        i[b] = cb ? N[b] + 1 : 0;
+        i[c] = cc ? N[c] + 1 : 0;
+        int j1[3] = {i[0], i[1], i[2]}, j2[3] = {i[0], i[1], i[2]};
+        j1[c] = cc ? N[c] : 1;  // ghost across b, inner along c
+        j2[b] = cb ? N[b] : 1;  // ghost across c, inner along b
+        v[at(i)] = 0.5 * (v[at(j1)] + v[at(j2)]);
+      }
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+// Ghost velocities of update_boundary_ghost (k_update_v*_ghost and
+// k_update_v*_ghost_corner, CFD/G_BoundaryFunctions.cu:277-560): ghost faces
+// across the two tangential axes take the boundary rule of the bc id of the
+// first face inside; corners take the mean of their two ghost neighbours.
+// bct/bvx/bvy/bvz: the boundary table (bc_.bcType_, bc_.v*_); lam* may be
+// NULL (no IBM area fractions).
+void orc_velocity_ghost(int Nx, int Ny, int Nz, const uint8_t* bct, const double* bvx, const double* bvy,
+                        const double* bvz, const uint8_t* fxbcid, const uint8_t* fybcid, const uint8_t* fzbcid,
+                        const double* lamx, const double* lamy, const double* lamz, double* vx, double* vy,
+                        double* vz) {
+  const int N[3] = {Nx, Ny, Nz};
+  velocity_ghost_family(N, 0, bct, bvx, fxbcid, lamx, vx);
+  velocity_ghost_family(N, 1, bct, bvy, fybcid, lamy, vy);
+  velocity_ghost_family(N, 2, bct, bvz, fzbcid, lamz, vz);
+}
+
 // Outlet boundary faces (G_SMACSolver::update_boundary_faces,
 // CFD/G_SMACSolver_VoF.cu:1798-1950): f_b of an outlet face is twice the f_b
 // of the face next to it on the interior side (p = 0 on the outlet).  The

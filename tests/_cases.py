@@ -42,9 +42,26 @@ def build_case(spec):
 
 
 def golden_names():
+    """Fixtures of the reference's solve (the post-projection ones excluded)."""
     if not os.path.isdir(GOLDEN):
         return []
-    return sorted(f[:-4] for f in os.listdir(GOLDEN) if f.endswith(".npz"))
+    return sorted(f[:-4] for f in os.listdir(GOLDEN) if f.endswith(".npz") and not f.startswith("post"))
+
+
+def post_golden_names():
+    """Fixtures of the reference's update_boundary_ghost + make_face_gradp."""
+    if not os.path.isdir(GOLDEN):
+        return []
+    return sorted(f[:-4] for f in os.listdir(GOLDEN) if f.endswith(".npz") and f.startswith("post"))
+
+
+def post_case_from_spec(spec):
+    """workloads.post_case from a fixture's JSON spec (lists back to tuples)."""
+    spec = dict(spec)
+    for k in ("N", "sides", "g", "h"):
+        if k in spec:
+            spec[k] = tuple(spec[k])
+    return W.post_case(**spec)
 
 
 def load_golden(name):

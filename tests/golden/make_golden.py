@@ -7,6 +7,7 @@ seeds by mydemcfd_b200.workloads (SplitMix64), so a fixture holds only the
 reference's outputs and the parameters that produced them.
 
     python tests/golden/make_golden.py --out tests/golden
+    python tests/golden/make_golden.py --out tests/golden --post-only
 """
 from __future__ import annotations
 
@@ -38,6 +39,15 @@ CASES = [
 ]
 
 
+# The pass after the projection (update_boundary_ghost + make_face_gradp):
+# (name, workloads.post_case kwargs); every output array is stored.
+POST_CASES = [
+    ("post12x10x8_s1", dict(N=(12, 10, 8), seed=1, sides=("x+", "z-"))),
+    ("post16_s2_solid", dict(N=(16, 16, 16), seed=2, sides=("x-", "y+"), solid_fraction=0.35)),
+    ("post9x7x11_s3_nolam", dict(N=(9, 7, 11), seed=3, sides=("x+", "y-", "z+"), lam=False, g=(0.3, 0.0, -9.8))),
+]
+
+
 def oracle_solid_fraction(N, h, origin, spheres):
     return O.solid_fraction_spheres(N, h, origin, spheres)
 
@@ -63,8 +73,19 @@ def sparse_sample(a, stride=97):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--out", default=os.path.join(ROOT, "tests", "golden"))
+    ap.add_argument("--post-only", action="store_true", help="only the post-projection fixtures")
     args = ap.parse_args()
     os.makedirs(args.out, exist_ok=True)
+    post_index = {}
+    for name, spec in POST_CASES:
+        r = REF.post(W.post_case(**spec))
+        np.savez_compressed(os.path.join(args.out, name + ".npz"), meta=np.array(json.dumps(spec)), **r)
+        post_index[name] = spec
+        print(name, spec, flush=True)
+    with open(os.path.join(args.out, "post_index.json"), "w") as f:
+        json.dump(post_index, f, indent=1, sort_keys=True)
+    if args.post_only:
+        return
     index = {}
     for name, spec, st, tol, levels, store_v in CASES:
         case = build_case(spec)

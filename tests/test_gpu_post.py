@@ -1,0 +1,139 @@
+"""The pass after the projection on the GPU (smac_update_pressure_ghost,
+smac_update_velocity_ghost, smac_face_gradp) against the oracle and the
+reference.
+
+Every output is element-wise arithmetic of the inputs, so the bar is bit
+equality: with the oracle on seeded inputs (small and 256^3), with the
+golden vectors of the reference's own update_boundary_ghost +
+make_face_gradp, and with the reference library itself where it is built.
+"""
+import numpy as np
+import pytest
+import torch
+
+from mydemcfd_b200 import _native as nat
+from mydemcfd_b200 import workloads as W
+from mydemcfd_b200.solver import (BoundaryConditions, DeviceGrid, SMACStep, face_gradp_device,
+                                  update_pressure_ghost_device, update_velocity_ghost_device)
+from oracle import oracle as O
+from oracle import ref as REF
+
+from _cases import load_golden, post_case_from_spec, post_golden_names
+
+pytestmark = pytest.mark.gpu
+
+
+def _cuda(a):
+    return torch.from_numpy(np.ascontiguousarray(a)).cuda()
+
+
+def _misaligned(a, offset=3):
+    """A contiguous CUDA copy of uint8 array a whose data pointer is not 16-byte aligned."""
+    buf = torch.zeros(a.size + 32, dtype=torch.uint8, device="cuda")
+    t = buf[offset:offset + a.size].view(a.shape)
+    t.copy_(torch.from_numpy(np.ascontiguousarray(a)))
+    assert t.data_ptr() % 16 != 0
+    return t
+
+
+def run_post(c, misaligned=False):
+    """The three calls on device copies of a workloads.PostCase."""
+    u8 = _misaligned if misaligned else _cuda
+    p = _cuda(c.p)
+    v = [_cuda(a) for a in c.v]
+    gp = [torch.zeros(a.shape, dtype=torch.float64, device="cuda") for a in c.v]
+    update_pressure_ghost_device(c.N, c.h, u8(c.ct), _cuda(c.rho), c.g, p)
+    bc = BoundaryConditions(c.bc_type, *c.bc_v)
+    update_velocity_ghost_device(c.N, c.h, bc, [u8(a) for a in c.bcid], [u8(a) for a in c.marks],
+                                 None if c.lam is None else [_cuda(a) for a in c.lam], [_cuda(a) for a in c.vs],
+                                 [_cuda(a) for a in c.fb], _cuda(c.p_delta), c.dt, v)
+    face_gradp_device(c.N, c.h, p, gp)
+    torch.cuda.synchronize()
+    return p.cpu().numpy(), tuple(a.cpu().numpy() for a in v), tuple(a.cpu().numpy() for a in gp)
+
+
+def _assert_equal(got, want):
+    p, v, gp = got
+    p2, v2, gp2 = want
+    assert np.array_equal(p, p2)
+    for k, a, b in zip(("vx", "vy", "vz", "gpx", "gpy", "gpz"), v + gp, v2 + gp2):
+        assert np.array_equal(a, b), k
+
+
+@pytest.mark.parametrize("spec,misaligned", [
+    (dict(N=(12, 10, 8), seed=1, sides=("x+", "z-")), False),
+    (dict(N=(16, 16, 16), seed=2, sides=("x-", "y+"), solid_fraction=0.35), False),
+    (dict(N=(9, 7, 11), seed=3, sides=("x+", "y-", "z+"), lam=False, g=(0.3, 0.0, -9.8)), True),
+    (dict(N=(33, 17, 2), seed=4, sides=("z+",), solid_fraction=0.2), True),
+])
+def test_post_pass_bit_exact_against_oracle(spec, misaligned):
+    c = W.post_case(**spec)
+    _assert_equal(run_post(c, misaligned), O.post_pass(c))
+
+
+@pytest.mark.parametrize("name", post_golden_names())
+def test_post_pass_bit_exact_against_reference_golden(name):
+    meta, arr = load_golden(name)
+    c = post_case_from_spec(meta)
+    want = (arr["p"], (arr["vx"], arr["vy"], arr["vz"]), (arr["gpx"], arr["gpy"], arr["gpz"]))
+    _assert_equal(run_post(c), want)
+
+
+@pytest.mark.skipif(not REF.available(), reason="reference build oracle/_ref not present")
+def test_post_pass_bit_exact_against_reference_library():
+    c = W.post_case((24, 20, 16), seed=9, sides=("x+", "y-", "z-"), solid_fraction=0.3, g=(0.5, -1.0, -9.8))
+    r = REF.post(c)
+    _assert_equal(run_post(c), (r["p"], (r["vx"], r["vy"], r["vz"]), (r["gpx"], r["gpy"], r["gpz"])))
+
+
+def test_post_pass_256_bit_exact_and_gradp_bandwidth():
+    c = W.post_case((256, 256, 256), seed=6, sides=("x+", "z-"), solid_fraction=0.05)
+    _assert_equal(run_post(c), O.post_pass(c))
+    # face gradient: p read once, three face arrays written
+    p = _cuda(c.p)
+    gp = [torch.empty(a.shape, dtype=torch.float64, device="cuda") for a in c.v]
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    times = []
+    for _ in range(8):
+        flush.fill_(1)
+        e0.record()
+        face_gradp_device(c.N, c.h, p, gp)
+        e1.record()
+        torch.cuda.synchronize()
+        times.append(e0.elapsed_time(e1))
+    ms = sorted(times)[len(times) // 2]
+    n = 257 ** 3
+    alg = 8.0 * (258 ** 3 + 3 * n)
+    print(f"face_gradp 256^3: {ms * 1e3:.1f} us, {alg / ms / 1e6:.0f} GB/s algorithmic")
+    assert ms < 1.0
+
+
+def test_smac_step_post_calls_match_oracle():
+    """SMACStep.update_boundary_ghost + make_face_gradp on a DeviceGrid."""
+    c = W.post_case((20, 16, 12), seed=8, sides=("y+",), solid_fraction=0.2, g=(0.0, 0.0, -9.8))
+    sh = W.shapes(c.N)
+    g = DeviceGrid(*c.N, *c.h, *(_cuda(a) for a in c.vs), *(_cuda(a) for a in c.fb), *(_cuda(a) for a in c.fb),
+                   _cuda(c.ct), *(_cuda(a) for a in c.ft), _cuda(c.p), _cuda(c.p_delta),
+                   torch.zeros(sh["cell"], dtype=torch.float64, device="cuda"), *(_cuda(a) for a in c.v))
+    g.rho_ = _cuda(c.rho)
+    g.f_xbcid_, g.f_ybcid_, g.f_zbcid_ = (_cuda(a) for a in c.bcid)
+    g.f_xoutlet_, g.f_youtlet_, g.f_zoutlet_ = (_cuda(a) for a in c.marks)
+    g.f_ibm_area_solid_fraction_x_, g.f_ibm_area_solid_fraction_y_, g.f_ibm_area_solid_fraction_z_ = (
+        _cuda(a) for a in c.lam)
+    step = SMACStep(g, c.dt, g=c.g, bc=BoundaryConditions(c.bc_type, *c.bc_v))
+    step.update_boundary_ghost()
+    step.make_face_gradp()
+    torch.cuda.synchronize()
+    got = (g.p_.cpu().numpy(), tuple(a.cpu().numpy() for a in (g.f_vx_, g.f_vy_, g.f_vz_)),
+           tuple(a.cpu().numpy() for a in (g.f_gradp_x_, g.f_gradp_y_, g.f_gradp_z_)))
+    _assert_equal(got, O.post_pass(c))
+
+
+def test_velocity_ghost_refuses_single_cell_extent():
+    c = W.post_case((4, 4, 4), seed=1)
+    bc = BoundaryConditions(c.bc_type, *c.bc_v)
+    v = [_cuda(a) for a in c.v]
+    with pytest.raises(nat.SmacError):
+        update_velocity_ghost_device((4, 1, 4), c.h, bc, [_cuda(a) for a in c.bcid], None, None, (None,) * 3,
+                                     (None,) * 3, None, c.dt, v)

@@ -66,3 +66,25 @@ def test_no_device_is_reported(lib):
     rc = lib.smac_create(ctypes.byref(d), None, None, ctypes.byref(h))
     assert rc == nat.NO_DEVICE
     assert h.value is None
+
+
+def test_post_pass_arguments_are_checked_before_any_device_work(lib):
+    fake = ctypes.c_void_p(256)  # never dereferenced: every call below fails its argument checks
+    d = nat.GridDesc(8, 8, 8, 0.125, 0.125, 0.125)
+    assert lib.smac_update_pressure_ghost(ctypes.byref(d), None, None, 0.0, 0.0, -9.8, fake, None) == nat.BAD_ARG
+    flat = nat.GridDesc(8, 0, 8, 0.125, 0.125, 0.125)
+    assert lib.smac_update_pressure_ghost(ctypes.byref(flat), fake, None, 0.0, 0.0, -9.8, fake, None) == nat.BAD_SHAPE
+    assert lib.smac_face_gradp(ctypes.byref(flat), fake, fake, fake, fake, None) == nat.BAD_SHAPE
+    assert lib.smac_face_gradp(ctypes.byref(d), fake, None, fake, fake, None) == nat.BAD_ARG
+    import numpy as np
+    types = np.zeros(1, np.uint8)
+    vel = np.zeros(1)
+    empty = nat.BoundaryTable(0, types.ctypes.data, vel.ctypes.data, vel.ctypes.data, vel.ctypes.data)
+    args = (fake,) * 3 + (None,) * 3 + (None,) * 3 + (None,) * 6 + (None, 1.0) + (fake,) * 3 + (None,)
+    assert lib.smac_update_velocity_ghost(ctypes.byref(d), ctypes.byref(empty), *args) == nat.BAD_ARG
+    one = nat.BoundaryTable(1, types.ctypes.data, vel.ctypes.data, vel.ctypes.data, vel.ctypes.data)
+    thin = nat.GridDesc(8, 1, 8, 0.125, 0.125, 0.125)
+    assert lib.smac_update_velocity_ghost(ctypes.byref(thin), ctypes.byref(one), *args) == nat.BAD_SHAPE
+    # outlet marks without p_delta
+    bad = (fake,) * 3 + (fake,) * 3 + (None,) * 3 + (fake,) * 6 + (None, 1.0) + (fake,) * 3 + (None,)
+    assert lib.smac_update_velocity_ghost(ctypes.byref(d), ctypes.byref(one), *bad) == nat.BAD_ARG

@@ -6,7 +6,8 @@ import pytest
 
 from mydemcfd_b200 import workloads as W
 
-from _cases import build_case, fluid_demeaned, golden_names, load_golden, ref_grid, rel_err
+from _cases import (build_case, fluid_demeaned, golden_names, load_golden, post_case_from_spec, post_golden_names,
+                    ref_grid, rel_err)
 
 
 def test_box_types_match_reference_setup(oracle_lib):
@@ -195,3 +196,138 @@ def test_outlet_faces_twice_the_interior_neighbour(oracle_lib):
     np.testing.assert_array_equal(out[2][1][mz[1] == 1], 2.0 * fb[2][2][mz[1] == 1])
     for o, f, m in zip(out, fb, marks):
         np.testing.assert_array_equal(o[m == 0], f[m == 0])
+
+
+# ---------------------------------------------------------------------------
+# the pass after the projection (update_boundary_ghost + make_face_gradp)
+
+def _post_loops(c):
+    """A second restatement in plain loops, written from the reference's
+    kernels (CFD/G_SMACSolver.cu:1144-1343, CFD/G_BoundaryFunctions.cu:143-560),
+    with the reference's evaluation order."""
+    nx, ny, nz = c.N
+    dx, dy, dz = c.h
+    gx, gy, gz = c.g
+    p = c.p.copy()
+    ct, rho = c.ct, c.rho
+    for iz in range(1, nz + 1):
+        for iy in range(1, ny + 1):
+            for ix in range(1, nx + 1):
+                if ct[iz, iy, ix] != W.C_SOLID:
+                    continue
+                v = 0.0
+                for (jx, jy, jz, s, gg, hh) in ((ix - 1, iy, iz, 1, gx, dx), (ix + 1, iy, iz, -1, gx, dx),
+                                                 (ix, iy - 1, iz, 1, gy, dy), (ix, iy + 1, iz, -1, gy, dy),
+                                                 (ix, iy, iz - 1, 1, gz, dz), (ix, iy, iz + 1, -1, gz, dz)):
+                    if ct[jz, jy, jx] == W.C_INTERIOR:
+                        t = rho[jz, jy, jx] * gg * hh
+                        v = p[jz, jy, jx] + t if s > 0 else p[jz, jy, jx] - t
+                        break
+                p[iz, iy, ix] = v
+    for iz in range(nz + 2):
+        for iy in range(ny + 2):
+            for ix in range(nx + 2):
+                if 0 < ix <= nx and 0 < iy <= ny and 0 < iz <= nz:
+                    continue
+                sx, sy, sz = min(max(ix, 1), nx), min(max(iy, 1), ny), min(max(iz, 1), nz)
+                r = (ix - sx) * dx * gx + (iy - sy) * dy * gy + (iz - sz) * dz * gz
+                p[iz, iy, ix] = p[sz, sy, sx] + rho[sz, sy, sx] * r
+    v = [a.copy() for a in c.v]
+    inv = (1.0 / dx, 1.0 / dy, 1.0 / dz)
+    for a in range(3):
+        m = c.marks[a]
+        for (iz, iy, ix) in zip(*np.nonzero(m)):
+            if not (1 <= ix <= nx + 1 and 1 <= iy <= ny + 1 and 1 <= iz <= nz + 1):
+                continue
+            s = 1 if m[iz, iy, ix] == 1 else -1
+            cidx = [ix, iy, iz]
+            cidx[a] += s
+            sign = 1.0 if s < 0 else -1.0
+            v[a][iz, iy, ix] = c.vs[a][iz, iy, ix] + sign * c.fb[a][iz, iy, ix] * c.dt * \
+                c.p_delta[cidx[2], cidx[1], cidx[0]] * inv[a]
+
+    def rule(t, vb, lam, bnd, inner):
+        return {2: 2.0 * (1.0 - lam) * vb - inner, 0: -inner, 4: 2.0 * bnd - inner, 1: inner}.get(int(t), bnd)
+
+    N = (nx, ny, nz)
+    for a in range(3):
+        b, cc = [k for k in range(3) if k != a]
+        arr, ids = v[a], c.bcid[a]
+        lam = c.lam[a] if c.lam is not None else np.zeros(arr.shape)
+        get = lambda A, i: A[i[2], i[1], i[0]]  # noqa: E731
+
+        def ghost(i, gax):
+            low = i[gax] == 0
+            ib, inn = list(i), list(i)
+            ib[gax] = 1 if low else N[gax]
+            inn[gax] = 2 if low else N[gax] - 1
+            t = get(ids, ib)
+            return rule(c.bc_type[t], c.bc_v[a][t], get(lam, ib), get(arr, ib), get(arr, inn))
+
+        for ia in range(1, N[a] + 2):
+            for gax, oax in ((b, cc), (cc, b)):
+                for side in (0, N[gax] + 1):
+                    for io in range(1, N[oax] + 1):
+                        i = [0, 0, 0]
+                        i[a], i[gax], i[oax] = ia, side, io
+                        arr[i[2], i[1], i[0]] = ghost(i, gax)
+            for sb in (0, N[b] + 1):
+                for sc in (0, N[cc] + 1):
+                    i = [0, 0, 0]
+                    i[a], i[b], i[cc] = ia, sb, sc
+                    j1, j2 = list(i), list(i)
+                    j1[cc] = 1 if sc == 0 else N[cc]
+                    j2[b] = 1 if sb == 0 else N[b]
+                    arr[i[2], i[1], i[0]] = 0.5 * (get(arr, j1) + get(arr, j2))
+    gp = [np.zeros(a.shape) for a in c.v]
+    for iz in range(1, nz + 2):
+        for iy in range(1, ny + 2):
+            for ix in range(1, nx + 2):
+                gp[0][iz, iy, ix] = (p[iz, iy, ix] - p[iz, iy, ix - 1]) * inv[0]
+                gp[1][iz, iy, ix] = (p[iz, iy, ix] - p[iz, iy - 1, ix]) * inv[1]
+                gp[2][iz, iy, ix] = (p[iz, iy, ix] - p[iz - 1, iy, ix]) * inv[2]
+    return p, tuple(v), tuple(gp)
+
+
+@pytest.mark.parametrize("spec", [
+    dict(N=(7, 6, 5), seed=1, sides=("x+", "z-")),
+    dict(N=(8, 8, 6), seed=2, sides=("x-", "y+", "z+"), solid_fraction=0.4),
+    dict(N=(5, 7, 4), seed=3, sides=(), lam=False, g=(0.3, 0.0, -9.8)),
+])
+def test_post_pass_oracle_equals_loop_restatement(oracle_lib, spec):
+    c = W.post_case(**spec)
+    if spec.get("solid_fraction"):
+        assert int((c.ct == W.C_SOLID).sum()) > 0
+    p, v, gp = oracle_lib.post_pass(c)
+    p2, v2, gp2 = _post_loops(c)
+    assert np.array_equal(p, p2)
+    for a, b in zip(v + gp, v2 + gp2):
+        assert np.array_equal(a, b)
+    # only solid and ghost cells change
+    changed = p != c.p
+    assert not np.any(changed & (c.ct == W.C_INTERIOR))
+
+
+def test_post_pass_solid_cell_without_fluid_neighbour_gets_zero(oracle_lib):
+    c = W.post_case((8, 8, 8), seed=5, sides=(), solid_fraction=0.0)
+    c.ct[3:6, 3:6, 3:6] = W.C_SOLID  # the centre (4,4,4) has only solid neighbours
+    p, _, _ = oracle_lib.post_pass(c)
+    assert p[4, 4, 4] == 0.0
+    # a face cell of the block takes its fluid neighbour's value, shifted
+    assert p[4, 4, 3] == c.p[4, 4, 2] + c.rho[4, 4, 2] * c.g[0] * c.h[0]
+
+
+POST_GOLDEN = post_golden_names()
+
+
+@pytest.mark.skipif(not POST_GOLDEN, reason="no post-projection golden vectors")
+@pytest.mark.parametrize("name", POST_GOLDEN)
+def test_post_pass_oracle_matches_reference_golden(oracle_lib, name):
+    """The oracle against the reference's own update_boundary_ghost +
+    make_face_gradp run on the same seeded inputs: every entry bit exact."""
+    meta, arr = load_golden(name)
+    c = post_case_from_spec(meta)
+    p, v, gp = oracle_lib.post_pass(c)
+    assert np.array_equal(p, arr["p"])
+    for k, a in zip(("vx", "vy", "vz", "gpx", "gpy", "gpz"), v + gp):
+        assert np.array_equal(a, arr[k]), k
