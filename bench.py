@@ -335,6 +335,8 @@ def run_ours(args, ranks):
         solve_only[name] = {"value": replicas.throughput(ranks, args.steps, ms_s), "unit": "solves/s",
                             "ms_per_solve": ms_s / args.steps}
 
+    post_pass = post_pass_timings(case, g, pd, out_v, dev, stream)
+
     # error of each result against an FP64 solve to 1e-12 of the same input
     # (relative 2-norm over the fluid cells, fluid mean removed)
     fluid = torch.from_numpy(W.interior(case.ct) == W.C_INTERIOR).to(dev)
@@ -372,6 +374,7 @@ def run_ours(args, ranks):
                   "error_vs_fp64_1e-12": err(p_mixed)},
         "speedup_mixed_vs_plain": sps_mixed / sps_plain,
         "solve_only": solve_only,
+        "post_pass": post_pass,
         "e2e": e2e,
         "gpu_launches": launches,
         "roofline": roofline,
@@ -386,6 +389,73 @@ def run_ours(args, ranks):
     s_mixed.close()
     s_plain.close()
     replicas.finish(ranks)
+
+
+def post_pass_timings(case, g, p, v, dev, stream):
+    """The calls either side of the projection on the bench grid: before it
+    update_vstar_boundary, after it update_boundary_ghost + make_face_gradp.
+    Device time of each call (its launches replayed from a CUDA graph, CUDA
+    events, median of 10, each after an L2 flush) and the algorithmic bytes
+    it moves.  Inputs: the projected pressure and velocity, no-slip walls
+    with an outlet on x+."""
+    import torch
+
+    from mydemcfd_b200 import workloads as W
+    from mydemcfd_b200.solver import (BoundaryConditions, face_gradp_device, update_pressure_ghost_device,
+                                      update_velocity_ghost_device, update_vstar_boundary_device)
+    N, h = case.N, case.h
+    sh = W.shapes(N)
+    bcid = [torch.zeros(sh[k], dtype=torch.uint8, device=dev) for k in "xyz"]
+    marks = [torch.from_numpy(m).to(dev) for m in W.outlet_marks(N, ("x+",))]
+    bc = BoundaryConditions(np.zeros(1, np.uint8), np.zeros(1), np.zeros(1), np.zeros(1))
+    gp = [torch.empty(sh[k], dtype=torch.float64, device=dev) for k in "xyz"]
+    vs = (g.f_vx_star_, g.f_vy_star_, g.f_vz_star_)
+    fb = (g.f_bx_, g.f_by_, g.f_bz_)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    vs_copy = [t.clone() for t in vs]
+    calls = {
+        "vstar_boundary": lambda: update_vstar_boundary_device(N, h, bc, (g.f_xtype_, g.f_ytype_, g.f_ztype_), bcid,
+                                                               marks, None, vs_copy),
+        "pressure_ghost": lambda: update_pressure_ghost_device(N, h, g.celltype_, None, (0.0, 0.0, -9.8), p),
+        "velocity_ghost": lambda: update_velocity_ghost_device(N, h, bc, bcid, marks, None, vs, fb, p, case.dt, v),
+        "face_gradp": lambda: face_gradp_device(N, h, p, gp),
+    }
+    nx, ny, nz = N
+    ncell = (nx + 2) * (ny + 2) * (nz + 2)
+    nghost = ncell - nx * ny * nz
+    nface = sum(int(np.prod(sh[k])) for k in "xyz")
+    ring = sum(2 * (N[a] + 1) * (N[b] + N[c] + 2) for a, b, c in ((0, 1, 2), (1, 0, 2), (2, 0, 1)))
+    nwall = 2 * ((ny * nz) + (nx * nz) + (nx * ny))
+    alg = {
+        # face types scanned; per wall face its id read and u* written
+        "vstar_boundary": nface + nwall * (1 + 8),
+        # cell types scanned; per ghost cell: its source's p and type read, p written
+        "pressure_ghost": ncell + nghost * (8 + 1 + 8),
+        # marks scanned; per outlet face v*, f_b, p_delta read, v written; per
+        # ghost face two velocities, the id and the face written
+        "velocity_ghost": nface + ny * nz * 32 + ring * (8 + 8 + 1 + 8),
+        # p read once, three face arrays written on the (N+1)^3 box
+        "face_gradp": 8 * (ncell + 3 * (nx + 1) * (ny + 1) * (nz + 1)),
+    }
+    out = {}
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    for name, fn in calls.items():
+        fn()
+        torch.cuda.synchronize()
+        graph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(graph):
+            fn()
+        ts = []
+        for _ in range(10):
+            flush.fill_(1)
+            e0.record(stream)
+            graph.replay()
+            e1.record(stream)
+            torch.cuda.synchronize()
+            ts.append(e0.elapsed_time(e1))
+        ms = sorted(ts)[len(ts) // 2]
+        out[name] = {"us": ms * 1e3, "alg_bytes": alg[name], "GB/s": alg[name] / (ms / 1e3) / 1e9}
+    return out
 
 
 def run_kernel_only(args):

@@ -240,6 +240,22 @@ typedef struct {
   const double *vx, *vy, *vz;
 } smac_boundary_table;
 
+/* Wall-face u* before the projection, G_SMACSolver::update_vstar_boundary
+ * (CFD/G_SMACSolver.cu:1044-1052, k_update_v*star_boundary,
+ * CFD/G_BoundaryFunctions.cu:3-71, CFD/G_BoundaryFunctions.h:369-470), in
+ * place on (vxs, vys, vzs): every F_BOUNDARY face with indices 1..N+1 gets,
+ * by the type of its id in f_*bcid_: inflow (1 - lam) v_b, no-slip 0,
+ * outlet the u* of the next face on its interior side (outlet mark 2: -1,
+ * otherwise +1), slip and outflow 0.  With no-slip walls this makes the
+ * pure-Neumann system compatible (sum of D u* = 0).  Marks and lam may be
+ * NULL.  An outlet face whose neighbour is also F_BOUNDARY reads a value
+ * that another thread may be writing, as in the reference. */
+smac_status smac_update_vstar_boundary(const smac_grid_desc* d, const smac_boundary_table* bc, const uint8_t* fxt,
+                                      const uint8_t* fyt, const uint8_t* fzt, const uint8_t* fxbcid,
+                                      const uint8_t* fybcid, const uint8_t* fzbcid, const uint8_t* fxo,
+                                      const uint8_t* fyo, const uint8_t* fzo, const double* lamx, const double* lamy,
+                                      const double* lamz, double* vxs, double* vys, double* vzs, void* stream);
+
 /* Velocity part of update_boundary_ghost, in place on (vx, vy, vz):
  *  1. outlet faces (k_update_v*_outlet, CFD/G_BoundaryFunctions.cu:143-255):
  *     a face with outlet mark 1 (interior side +1) or 2 (side -1) -- the marks

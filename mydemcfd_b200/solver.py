@@ -313,8 +313,8 @@ class BoundaryConditions:
 
 class SMACStep:
     """The G_SMACSolver calls around the seam, in the reference's order
-    (CFD/main.cu:313-317): solve_poisson(), correct_vof_velocity(),
-    update_boundary_ghost(), make_face_gradp()."""
+    (CFD/main.cu:309-317): update_vstar_boundary(), solve_poisson(),
+    correct_vof_velocity(), update_boundary_ghost(), make_face_gradp()."""
 
     def __init__(self, grid: DeviceGrid, dt: float = 1.0, g=(0.0, 0.0, 0.0), bc: BoundaryConditions | None = None):
         self.grid_ = grid
@@ -323,6 +323,19 @@ class SMACStep:
         self.gx_, self.gy_, self.gz_ = (float(x) for x in g)
         self.bc_ = bc
         self.pressure_solver_: B200PressureSolver | None = None
+
+    def update_vstar_boundary(self):
+        """G_SMACSolver::update_vstar_boundary (CFD/G_SMACSolver.cu:1044-1052):
+        wall u* before the projection."""
+        g = self.grid_
+        if self.bc_ is None or g.f_xbcid_ is None:
+            raise ValueError("update_vstar_boundary needs the boundary table bc_ and the grid's f_*bcid_")
+        marks = None if g.f_xoutlet_ is None else (g.f_xoutlet_, g.f_youtlet_, g.f_zoutlet_)
+        lam = None if g.f_ibm_area_solid_fraction_x_ is None else (
+            g.f_ibm_area_solid_fraction_x_, g.f_ibm_area_solid_fraction_y_, g.f_ibm_area_solid_fraction_z_)
+        update_vstar_boundary_device(g.N, (g.dx_, g.dy_, g.dz_), self.bc_, (g.f_xtype_, g.f_ytype_, g.f_ztype_),
+                                     (g.f_xbcid_, g.f_ybcid_, g.f_zbcid_), marks, lam,
+                                     (g.f_vx_star_, g.f_vy_star_, g.f_vz_star_))
 
     def solve_poisson(self):
         return self.pressure_solver_.solve(self)
@@ -436,6 +449,20 @@ def update_velocity_ghost_device(N, h, bc: BoundaryConditions, bcid, marks, lam,
     nat.check(nat.load().smac_update_velocity_ghost(
         ctypes.byref(d), ctypes.byref(table), *map(_ptr, bcid), *map(_ptr, marks), *map(_ptr, lam), *map(_ptr, vs),
         *map(_ptr, fb), _ptr(p_delta), ctypes.c_double(dt), *map(_ptr, v), ctypes.c_void_p(s)))
+    del keep
+
+
+def update_vstar_boundary_device(N, h, bc: BoundaryConditions, ft, bcid, marks, lam, vs):
+    """smac_update_vstar_boundary in place on vs = (vxs, vys, vzs): the wall
+    u* of every F_BOUNDARY face; marks / lam None mean none / 0."""
+    d = nat.GridDesc(*N, *h)
+    s = torch.cuda.current_stream().cuda_stream
+    table, keep = bc.table()
+    marks = marks if marks is not None else (None, None, None)
+    lam = lam if lam is not None else (None, None, None)
+    nat.check(nat.load().smac_update_vstar_boundary(
+        ctypes.byref(d), ctypes.byref(table), *map(_ptr, ft), *map(_ptr, bcid), *map(_ptr, marks), *map(_ptr, lam),
+        *map(_ptr, vs), ctypes.c_void_p(s)))
     del keep
 
 

@@ -319,13 +319,13 @@ class PostCase:
 
 
 def post_case(N, seed, h=(0.03125, 0.03125, 0.03125), dt=0.5, g=(0.0, -1.5, -9.8), sides=("x+", "z-"),
-              solid_fraction=0.0, lam=True):
+              solid_fraction=0.0, lam=True, solid_margin=2):
     """Seeded inputs for the post-projection pass.  Boundary ids 0..4 carry
     the types NOSLIP, SLIP, INFLOW, OUTFLOW, OUTLET with U[-1,1) boundary
     velocities; every face gets a U{0..3} id except the outlet faces of
     `sides`, which get id 4 (so the marks and the ids agree).  With
-    solid_fraction > 0 that share of the cells 2..N-1 (in clusters, so some
-    have no interior neighbour) become C_SOLID.  Fields are U[-1,1) (rho in
+    solid_fraction > 0 that share of the cells m..N+1-m, m = solid_margin
+    (in clusters, so some have no interior neighbour) become C_SOLID.  Fields are U[-1,1) (rho in
     [1, 1000), f_b in [0.1, 1) on F_INTERIOR faces, lam in [0, 1))."""
     N = tuple(int(n) for n in N)
     sh = shapes(N)
@@ -342,7 +342,8 @@ def post_case(N, seed, h=(0.03125, 0.03125, 0.03125), dt=0.5, g=(0.0, -1.5, -9.8
         thin = uniform01(substream(seed, 91), int(np.prod(sh["cell"]))).reshape(sh["cell"]) < 0.85
         sf = np.zeros(sh["cell"])
         inner = np.zeros(sh["cell"], bool)
-        inner[2:nz, 2:ny, 2:nx] = True
+        m = solid_margin
+        inner[m:nz + 2 - m, m:ny + 2 - m, m:nx + 2 - m] = True
         sf[inner & dense & thin] = 1.0
         set_solid_cells(sf, ct, fxt, fyt, fzt)
     marks = outlet_marks(N, sides)

@@ -202,6 +202,20 @@ def velocity_ghost(N, bc_type, bc_v, bcid, lam, v):
     return tuple(v)
 
 
+def vstar_boundary(N, bc_type, bc_v, ft, bcid, marks, lam, vs):
+    """G_SMACSolver::update_vstar_boundary (k_update_v*star_boundary,
+    CFD/G_BoundaryFunctions.cu:3-71) on copies of u*; marks/lam may be None."""
+    vs = [np.array(a, dtype=np.float64, order="C", copy=True) for a in vs]
+    bct = np.ascontiguousarray(bc_type, np.uint8)
+    bv = [np.ascontiguousarray(a, np.float64) for a in bc_v]
+    marks = (None, None, None) if marks is None else tuple(np.ascontiguousarray(m, np.uint8) for m in marks)
+    lam = (None, None, None) if lam is None else tuple(np.ascontiguousarray(a) for a in lam)
+    lib().orc_vstar_boundary(*N, _u8(bct), *(_p(a) for a in bv), *(_u8(np.ascontiguousarray(t)) for t in ft),
+                             *(_u8(np.ascontiguousarray(b)) for b in bcid), *(_u8(m) for m in marks),
+                             *(_p(a) for a in lam), *(_p(a) for a in vs))
+    return tuple(vs)
+
+
 def post_pass(case):
     """G_SMACSolver::update_boundary_ghost then make_face_gradp
     (CFD/G_SMACSolver.cu:1277-1363) on a workloads.PostCase: returns

@@ -123,7 +123,8 @@ class RefPostInputs(ctypes.Structure):
 
 
 class RefPostOutputs(ctypes.Structure):
-    _fields_ = [(k, _dp) for k in ("p", "vx", "vy", "vz", "gpx", "gpy", "gpz")]
+    _fields_ = [(k, _dp) for k in ("p", "vx", "vy", "vz", "gpx", "gpy", "gpz")] + \
+        [("ghost_ms", ctypes.c_double), ("gradp_ms", ctypes.c_double)]
 
 
 def grid_spacing(N, h):
@@ -131,14 +132,7 @@ def grid_spacing(N, h):
     return tuple(float(np.float64(n * hh) / np.float64(n)) for n, hh in zip(N, h))
 
 
-def post(case):
-    """Run the reference's update_boundary_ghost + make_face_gradp on a
-    mydemcfd_b200.workloads.PostCase (lam None -> zeros)."""
-    L = lib()
-    if not hasattr(L, "_post_set"):
-        L.ref_post.restype = ctypes.c_int
-        L.ref_post.argtypes = [ctypes.POINTER(RefPostInputs), ctypes.POINTER(RefPostOutputs)]
-        L._post_set = True
+def _post_inputs(case, keep):
     nx, ny, nz = case.N
     ghost = np.ones(case.ct.shape, bool)
     ghost[1:nz + 1, 1:ny + 1, 1:nx + 1] = False
@@ -150,7 +144,6 @@ def post(case):
     i.Lx, i.Ly, i.Lz = (n * hh for n, hh in zip(case.N, case.h))
     i.dt = case.dt
     i.gx, i.gy, i.gz = case.g
-    keep = []
 
     def d(a):
         a = np.ascontiguousarray(a, np.float64)
@@ -180,6 +173,40 @@ def post(case):
     i.vxs, i.vys, i.vzs = (d(a) for a in case.vs)
     i.fbx, i.fby, i.fbz = (d(a) for a in case.fb)
     i.vx, i.vy, i.vz = (d(a) for a in case.v)
+    return i
+
+
+def _post_lib():
+    L = lib()
+    if not hasattr(L, "_post_set"):
+        L.ref_post.restype = ctypes.c_int
+        L.ref_post.argtypes = [ctypes.POINTER(RefPostInputs), ctypes.POINTER(RefPostOutputs)]
+        L.ref_vstar.restype = ctypes.c_int
+        L.ref_vstar.argtypes = [ctypes.POINTER(RefPostInputs), _dp, _dp, _dp, _dp]
+        L._post_set = True
+    return L
+
+
+def vstar(case):
+    """Run the reference's update_vstar_boundary on the u* of a
+    mydemcfd_b200.workloads.PostCase: returns (vxs, vys, vzs, ms)."""
+    keep = []
+    i = _post_inputs(case, keep)
+    out = [np.zeros(a.shape) for a in case.vs]
+    ms = ctypes.c_double(0.0)
+    rc = _post_lib().ref_vstar(ctypes.byref(i), *(_p(a) for a in out), ctypes.byref(ms))
+    if rc != 0:
+        raise RuntimeError(f"ref_vstar returned {rc}")
+    return (*out, ms.value)
+
+
+def post(case):
+    """Run the reference's update_boundary_ghost + make_face_gradp on a
+    mydemcfd_b200.workloads.PostCase (lam None -> zeros); also returns the
+    device time of each call (ghost_ms, gradp_ms)."""
+    keep = []
+    i = _post_inputs(case, keep)
+    L = _post_lib()
     out = {"p": np.zeros(case.p.shape), "vx": np.zeros(case.v[0].shape), "vy": np.zeros(case.v[1].shape),
            "vz": np.zeros(case.v[2].shape), "gpx": np.zeros(case.v[0].shape), "gpy": np.zeros(case.v[1].shape),
            "gpz": np.zeros(case.v[2].shape)}
@@ -189,4 +216,5 @@ def post(case):
     rc = L.ref_post(ctypes.byref(i), ctypes.byref(o))
     if rc != 0:
         raise RuntimeError(f"ref_post returned {rc}")
+    out["ghost_ms"], out["gradp_ms"] = o.ghost_ms, o.gradp_ms
     return out

@@ -7,9 +7,10 @@
 // It follows the reference driver's set-up (CFD/main.cu:183-243): a host
 // SMACSolver with calloc'ed members, G_SMACSolver::solver_malloc + cpuTogpu,
 // G_PCGSolver + G_GMGSolver::initialize, set_solver, tol_, then
-// G_SMACSolver::solve_poisson() and correct_vof_velocity().  A second entry,
-// ref_post, runs the pass after the projection (update_boundary_ghost and
-// make_face_gradp) on given arrays.
+// G_SMACSolver::solve_poisson() and correct_vof_velocity().  Two more
+// entries run the calls either side of it on given arrays: ref_vstar
+// (update_vstar_boundary) and ref_post (update_boundary_ghost and
+// make_face_gradp).
 //
 // Two things the reference leaves to chance are pinned here: every multigrid
 // level array is zeroed after G_GMGSolver::initialize (the reference reads
@@ -210,14 +211,14 @@ struct ref_post_inputs {
 
 struct ref_post_outputs {
   double *p, *vx, *vy, *vz, *gpx, *gpy, *gpz;
+  double ghost_ms;  // device time of update_boundary_ghost (CUDA events, legacy stream)
+  double gradp_ms;  // device time of make_face_gradp
 };
 
-// G_SMACSolver::update_boundary_ghost then make_face_gradp
-// (CFD/G_SMACSolver.cu:1277-1363), the reference's pass after the projection,
-// on host arrays.  Returns 0 on success, -2 on a CUDA error.
-int ref_post(const ref_post_inputs* in, ref_post_outputs* out) {
+// The grid of a ref_post_inputs on host and device, as the reference's
+// driver sets it up (CFD/main.cu:183-243).
+static void post_setup(const ref_post_inputs* in, SMACSolver& solv, G_SMACSolver& g) {
   const int Nx = in->Nx, Ny = in->Ny, Nz = in->Nz;
-  SMACSolver solv;
   solv.set_calc_properties(0., 0., 0., in->Lx, in->Ly, in->Lz, Nx, Ny, Nz);
   solv.grid_.bc_.num_boundary_id_ = in->num_ids;
   solv.solver_malloc();
@@ -239,7 +240,6 @@ int ref_post(const ref_post_inputs* in, ref_post_outputs* out) {
   std::memcpy(hg.bc_.vy_.data_, in->bc_vy, sizeof(double) * (size_t)in->num_ids);
   std::memcpy(hg.bc_.vz_.data_, in->bc_vz, sizeof(double) * (size_t)in->num_ids);
 
-  G_SMACSolver g;
   g.set_calc_properties(0., 0., 0., in->Lx, in->Ly, in->Lz, Nx, Ny, Nz);
   g.grid_.bc_.num_boundary_id_ = in->num_ids;
   g.solver_malloc();
@@ -247,15 +247,65 @@ int ref_post(const ref_post_inputs* in, ref_post_outputs* out) {
   g.set_block_grid(Nx, Ny, Nz);
   g.dt_ = in->dt;
   g.inv_dt_ = 1. / in->dt;
-  g.update_boundary_ghost(solv);
-  g.make_face_gradp();
   cudaDeviceSynchronize();
+}
+
+// G_SMACSolver::update_boundary_ghost then make_face_gradp
+// (CFD/G_SMACSolver.cu:1277-1363), the reference's pass after the projection,
+// on host arrays.  Returns 0 on success, -2 on a CUDA error.
+int ref_post(const ref_post_inputs* in, ref_post_outputs* out) {
+  SMACSolver solv;
+  G_SMACSolver g;
+  post_setup(in, solv, g);
+  StaggeredGrid& hg = solv.grid_;
+  cudaEvent_t ev[3];
+  for (auto& x : ev) cudaEventCreate(&x);
+  cudaEventRecord(ev[0], 0);
+  g.update_boundary_ghost(solv);
+  cudaEventRecord(ev[1], 0);
+  g.make_face_gradp();
+  cudaEventRecord(ev[2], 0);
+  cudaDeviceSynchronize();
+  float ms0 = 0.f, ms1 = 0.f;
+  cudaEventElapsedTime(&ms0, ev[0], ev[1]);
+  cudaEventElapsedTime(&ms1, ev[1], ev[2]);
+  out->ghost_ms = ms0;
+  out->gradp_ms = ms1;
+  for (auto& x : ev) cudaEventDestroy(x);
   cudaError_t e = cudaGetLastError();
   if (e == cudaSuccess) {
     g.gpuTocpu(solv.grid_);
     get(hg.p_, out->p);
     get(hg.f_vx_, out->vx); get(hg.f_vy_, out->vy); get(hg.f_vz_, out->vz);
     get(hg.f_gradp_x_, out->gpx); get(hg.f_gradp_y_, out->gpy); get(hg.f_gradp_z_, out->gpz);
+    e = cudaGetLastError();
+  }
+  g.solver_free();
+  solv.solver_free();
+  return e == cudaSuccess ? 0 : -2;
+}
+
+// G_SMACSolver::update_vstar_boundary (CFD/G_SMACSolver.cu:1044-1052) on the
+// u* of a ref_post_inputs; *ms receives its device time.
+int ref_vstar(const ref_post_inputs* in, double* vxs, double* vys, double* vzs, double* ms) {
+  SMACSolver solv;
+  G_SMACSolver g;
+  post_setup(in, solv, g);
+  StaggeredGrid& hg = solv.grid_;
+  cudaEvent_t ev[2];
+  for (auto& x : ev) cudaEventCreate(&x);
+  cudaEventRecord(ev[0], 0);
+  g.update_vstar_boundary();
+  cudaEventRecord(ev[1], 0);
+  cudaDeviceSynchronize();
+  float t = 0.f;
+  cudaEventElapsedTime(&t, ev[0], ev[1]);
+  *ms = t;
+  for (auto& x : ev) cudaEventDestroy(x);
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) {
+    g.gpuTocpu(solv.grid_);
+    get(hg.f_vx_star_, vxs); get(hg.f_vy_star_, vys); get(hg.f_vz_star_, vzs);
     e = cudaGetLastError();
   }
   g.solver_free();

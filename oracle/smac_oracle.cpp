@@ -790,6 +790,50 @@ void orc_velocity_ghost(int Nx, int Ny, int Nz, const uint8_t* bct, const double
   velocity_ghost_family(N, 2, bct, bvz, fzbcid, lamz, vz);
 }
 
+// Wall-face u*, G_SMACSolver::update_vstar_boundary
+// (CFD/G_SMACSolver.cu:1044-1052 -> k_update_v{x,y,z}star_boundary,
+// CFD/G_BoundaryFunctions.cu:3-71, rules d_get_v*star_*face,
+// CFD/G_BoundaryFunctions.h:369-470): on every F_BOUNDARY face with indices
+// 1..N+1, by the type of its boundary id: inflow (1 - lam) v_b, no-slip 0,
+// outlet the u* of the next face on the side given by the outlet mark
+// (2: -1, otherwise +1, the reference's f_*internal_id_ < 0 test), others 0.
+// Families in the order x, y, z, faces in index order (an outlet face whose
+// neighbour is itself F_BOUNDARY is a race in the reference).
+void orc_vstar_boundary(int Nx, int Ny, int Nz, const uint8_t* bct, const double* bvx, const double* bvy,
+                        const double* bvz, const uint8_t* fxt, const uint8_t* fyt, const uint8_t* fzt,
+                        const uint8_t* fxbcid, const uint8_t* fybcid, const uint8_t* fzbcid, const uint8_t* fxo,
+                        const uint8_t* fyo, const uint8_t* fzo, const double* lamx, const double* lamy,
+                        const double* lamz, double* vxs, double* vys, double* vzs) {
+  const int N[3] = {Nx, Ny, Nz};
+  const uint8_t* ft[3] = {fxt, fyt, fzt};
+  const uint8_t* id[3] = {fxbcid, fybcid, fzbcid};
+  const uint8_t* mk[3] = {fxo, fyo, fzo};
+  const double* lam[3] = {lamx, lamy, lamz};
+  const double* bv[3] = {bvx, bvy, bvz};
+  double* vs[3] = {vxs, vys, vzs};
+  for (int a = 0; a < 3; ++a) {
+    int S[3] = {Nx + 2, Ny + 2, Nz + 2};
+    S[a] += 1;
+    const size_t stride = a == 0 ? 1 : a == 1 ? (size_t)S[0] : (size_t)S[0] * S[1];
+    for (int iz = 1; iz < N[2] + 2; ++iz)
+      for (int iy = 1; iy < N[1] + 2; ++iy)
+        for (int ix = 1; ix < N[0] + 2; ++ix) {
+          const size_t f = ((size_t)iz * S[1] + iy) * S[0] + ix;
+          if (ft[a][f] != F_BOUNDARY) continue;
+          const int b = id[a][f];
+          const uint8_t t = bct[b];
+          double v = 0.;
+          if (t == 2) {  // BC_INFLOW
+            v = (1. - (lam[a] ? lam[a][f] : 0.)) * bv[a][b];
+          } else if (t == 4) {  // BC_OUTLET
+            const bool low = mk[a] && mk[a][f] == 2;
+            v = low ? vs[a][f - stride] : vs[a][f + stride];
+          }
+          vs[a][f] = v;
+        }
+  }
+}
+
 // Outlet boundary faces (G_SMACSolver::update_boundary_faces,
 // CFD/G_SMACSolver_VoF.cu:1798-1950): f_b of an outlet face is twice the f_b
 // of the face next to it on the interior side (p = 0 on the outlet).  The

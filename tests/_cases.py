@@ -42,10 +42,18 @@ def build_case(spec):
 
 
 def golden_names():
-    """Fixtures of the reference's solve (the post-projection ones excluded)."""
+    """Fixtures of the reference's solve (those of the calls around it excluded)."""
     if not os.path.isdir(GOLDEN):
         return []
-    return sorted(f[:-4] for f in os.listdir(GOLDEN) if f.endswith(".npz") and not f.startswith("post"))
+    return sorted(f[:-4] for f in os.listdir(GOLDEN)
+                  if f.endswith(".npz") and not f.startswith("post") and not f.startswith("vstar"))
+
+
+def vstar_golden_names():
+    """Fixtures of the reference's update_vstar_boundary."""
+    if not os.path.isdir(GOLDEN):
+        return []
+    return sorted(f[:-4] for f in os.listdir(GOLDEN) if f.endswith(".npz") and f.startswith("vstar"))
 
 
 def post_golden_names():

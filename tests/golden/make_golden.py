@@ -47,6 +47,15 @@ POST_CASES = [
     ("post9x7x11_s3_nolam", dict(N=(9, 7, 11), seed=3, sides=("x+", "y-", "z+"), lam=False, g=(0.3, 0.0, -9.8))),
 ]
 
+# The wall u* rule before the projection (update_vstar_boundary); solids keep
+# off the outlets' neighbours (an outlet face reading an F_BOUNDARY face is a
+# race in the reference).
+VSTAR_CASES = [
+    ("vstar12x10x8_s1", dict(N=(12, 10, 8), seed=1, sides=("x+", "z-"))),
+    ("vstar16_s2_solid", dict(N=(16, 16, 16), seed=2, sides=("x-", "y+"), solid_fraction=0.35, solid_margin=3)),
+    ("vstar9x7x11_s3_nolam", dict(N=(9, 7, 11), seed=3, sides=("x+", "y-", "z+"), lam=False)),
+]
+
 
 def oracle_solid_fraction(N, h, origin, spheres):
     return O.solid_fraction_spheres(N, h, origin, spheres)
@@ -73,13 +82,21 @@ def sparse_sample(a, stride=97):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--out", default=os.path.join(ROOT, "tests", "golden"))
-    ap.add_argument("--post-only", action="store_true", help="only the post-projection fixtures")
+    ap.add_argument("--post-only", action="store_true",
+                    help="only the fixtures of the calls either side of the projection")
     args = ap.parse_args()
     os.makedirs(args.out, exist_ok=True)
     post_index = {}
     for name, spec in POST_CASES:
         r = REF.post(W.post_case(**spec))
-        np.savez_compressed(os.path.join(args.out, name + ".npz"), meta=np.array(json.dumps(spec)), **r)
+        arrays = {k: v for k, v in r.items() if isinstance(v, np.ndarray)}  # outputs, not the timings
+        np.savez_compressed(os.path.join(args.out, name + ".npz"), meta=np.array(json.dumps(spec)), **arrays)
+        post_index[name] = spec
+        print(name, spec, flush=True)
+    for name, spec in VSTAR_CASES:
+        vxs, vys, vzs, _ = REF.vstar(W.post_case(**spec))
+        np.savez_compressed(os.path.join(args.out, name + ".npz"), meta=np.array(json.dumps(spec)), vxs=vxs,
+                            vys=vys, vzs=vzs)
         post_index[name] = spec
         print(name, spec, flush=True)
     with open(os.path.join(args.out, "post_index.json"), "w") as f:

@@ -1,6 +1,7 @@
-"""The pass after the projection on the GPU (smac_update_pressure_ghost,
-smac_update_velocity_ghost, smac_face_gradp) against the oracle and the
-reference.
+"""The calls either side of the projection on the GPU: before it the wall u*
+rule (smac_update_vstar_boundary), after it the pass over p
+(smac_update_pressure_ghost, smac_update_velocity_ghost, smac_face_gradp),
+against the oracle and the reference.
 
 Every output is element-wise arithmetic of the inputs, so the bar is bit
 equality: with the oracle on seeded inputs (small and 256^3), with the
@@ -14,11 +15,12 @@ import torch
 from mydemcfd_b200 import _native as nat
 from mydemcfd_b200 import workloads as W
 from mydemcfd_b200.solver import (BoundaryConditions, DeviceGrid, SMACStep, face_gradp_device,
-                                  update_pressure_ghost_device, update_velocity_ghost_device)
+                                  update_pressure_ghost_device, update_velocity_ghost_device,
+                                  update_vstar_boundary_device)
 from oracle import oracle as O
 from oracle import ref as REF
 
-from _cases import load_golden, post_case_from_spec, post_golden_names
+from _cases import load_golden, post_case_from_spec, post_golden_names, vstar_golden_names
 
 pytestmark = pytest.mark.gpu
 
@@ -97,6 +99,7 @@ def test_post_pass_256_bit_exact_and_gradp_bandwidth():
     times = []
     for _ in range(8):
         flush.fill_(1)
+        torch.cuda._sleep(400000)  # the host's call overhead stays outside the events
         e0.record()
         face_gradp_device(c.N, c.h, p, gp)
         e1.record()
@@ -107,6 +110,55 @@ def test_post_pass_256_bit_exact_and_gradp_bandwidth():
     alg = 8.0 * (258 ** 3 + 3 * n)
     print(f"face_gradp 256^3: {ms * 1e3:.1f} us, {alg / ms / 1e6:.0f} GB/s algorithmic")
     assert ms < 1.0
+
+
+def _device_ms(fn, reps=8):
+    """Median device time of fn's launches, replayed from a CUDA graph so
+    that no host time falls between them (CUDA events, L2 flushed before
+    each replay)."""
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    fn()
+    torch.cuda.synchronize()
+    graph = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(graph):
+        fn()
+    ts = []
+    for _ in range(reps):
+        flush.fill_(1)
+        torch.cuda._sleep(400000)
+        e0.record()
+        graph.replay()
+        e1.record()
+        torch.cuda.synchronize()
+        ts.append(e0.elapsed_time(e1))
+    return sorted(ts)[len(ts) // 2]
+
+
+@pytest.mark.skipif(not REF.available(), reason="reference build oracle/_ref not present")
+def test_post_pass_against_reference_time_256():
+    """update_boundary_ghost and make_face_gradp: this build's calls against
+    the reference's own kernels on the same 256^3 inputs, device time."""
+    c = W.post_case((256, 256, 256), seed=7, sides=("x+",), solid_fraction=0.05)
+    REF.post(c)  # loads the reference's kernels
+    r = REF.post(c)
+    p = _cuda(c.p)
+    v = [_cuda(a) for a in c.v]
+    gp = [torch.zeros(a.shape, dtype=torch.float64, device="cuda") for a in c.v]
+    ct, rho = _cuda(c.ct), _cuda(c.rho)
+    bcid, marks = [_cuda(a) for a in c.bcid], [_cuda(a) for a in c.marks]
+    lam, vs, fb, pd = [_cuda(a) for a in c.lam], [_cuda(a) for a in c.vs], [_cuda(a) for a in c.fb], _cuda(c.p_delta)
+    bc = BoundaryConditions(c.bc_type, *c.bc_v)
+
+    def ghost():
+        update_pressure_ghost_device(c.N, c.h, ct, rho, c.g, p)
+        update_velocity_ghost_device(c.N, c.h, bc, bcid, marks, lam, vs, fb, pd, c.dt, v)
+
+    ms_ghost = _device_ms(ghost)
+    ms_gradp = _device_ms(lambda: face_gradp_device(c.N, c.h, p, gp))
+    print(f"update_boundary_ghost 256^3: {ms_ghost * 1e3:.1f} us (reference {r['ghost_ms'] * 1e3:.1f} us); "
+          f"make_face_gradp: {ms_gradp * 1e3:.1f} us (reference {r['gradp_ms'] * 1e3:.1f} us)")
+    assert ms_ghost + ms_gradp < r["ghost_ms"] + r["gradp_ms"]
 
 
 def test_smac_step_post_calls_match_oracle():
@@ -137,3 +189,48 @@ def test_velocity_ghost_refuses_single_cell_extent():
     with pytest.raises(nat.SmacError):
         update_velocity_ghost_device((4, 1, 4), c.h, bc, [_cuda(a) for a in c.bcid], None, None, (None,) * 3,
                                      (None,) * 3, None, c.dt, v)
+
+
+def run_vstar(c, misaligned=False):
+    u8 = _misaligned if misaligned else _cuda
+    vs = [_cuda(a) for a in c.vs]
+    update_vstar_boundary_device(c.N, c.h, BoundaryConditions(c.bc_type, *c.bc_v), [u8(a) for a in c.ft],
+                                 [u8(a) for a in c.bcid], [u8(a) for a in c.marks],
+                                 None if c.lam is None else [_cuda(a) for a in c.lam], vs)
+    torch.cuda.synchronize()
+    return tuple(a.cpu().numpy() for a in vs)
+
+
+@pytest.mark.parametrize("spec,misaligned", [
+    (dict(N=(12, 10, 8), seed=1, sides=("x+", "z-")), False),
+    (dict(N=(16, 16, 16), seed=2, sides=("x-", "y+"), solid_fraction=0.35, solid_margin=3), True),
+    (dict(N=(33, 17, 5), seed=4, sides=("z+", "x-"), lam=False, solid_fraction=0.2, solid_margin=3), True),
+])
+def test_vstar_boundary_bit_exact_against_oracle(spec, misaligned):
+    c = W.post_case(**spec)
+    want = O.vstar_boundary(c.N, c.bc_type, c.bc_v, c.ft, c.bcid, c.marks, c.lam, c.vs)
+    for a, b in zip(run_vstar(c, misaligned), want):
+        assert np.array_equal(a, b)
+
+
+@pytest.mark.parametrize("name", vstar_golden_names())
+def test_vstar_boundary_bit_exact_against_reference_golden(name):
+    meta, arr = load_golden(name)
+    c = post_case_from_spec(meta)
+    for k, a in zip(("vxs", "vys", "vzs"), run_vstar(c)):
+        assert np.array_equal(a, arr[k]), k
+
+
+@pytest.mark.skipif(not REF.available(), reason="reference build oracle/_ref not present")
+def test_vstar_boundary_against_reference_library_and_time_256():
+    c = W.post_case((256, 256, 256), seed=5, sides=("x+", "z-"), solid_fraction=0.05, solid_margin=3)
+    REF.vstar(c)  # loads the reference's kernels
+    *ref, ref_ms = REF.vstar(c)
+    for a, b in zip(run_vstar(c), ref):
+        assert np.array_equal(a, b)
+    vs = [_cuda(a) for a in c.vs]
+    args = (c.N, c.h, BoundaryConditions(c.bc_type, *c.bc_v), [_cuda(a) for a in c.ft], [_cuda(a) for a in c.bcid],
+            [_cuda(a) for a in c.marks], [_cuda(a) for a in c.lam], vs)
+    ms = _device_ms(lambda: update_vstar_boundary_device(*args))
+    print(f"update_vstar_boundary 256^3: {ms * 1e3:.1f} us (reference {ref_ms * 1e3:.1f} us)")
+    assert ms < ref_ms

@@ -7,7 +7,7 @@ import pytest
 from mydemcfd_b200 import workloads as W
 
 from _cases import (build_case, fluid_demeaned, golden_names, load_golden, post_case_from_spec, post_golden_names,
-                    ref_grid, rel_err)
+                    ref_grid, rel_err, vstar_golden_names)
 
 
 def test_box_types_match_reference_setup(oracle_lib):
@@ -330,4 +330,77 @@ def test_post_pass_oracle_matches_reference_golden(oracle_lib, name):
     p, v, gp = oracle_lib.post_pass(c)
     assert np.array_equal(p, arr["p"])
     for k, a in zip(("vx", "vy", "vz", "gpx", "gpy", "gpz"), v + gp):
+        assert np.array_equal(a, arr[k]), k
+
+
+# ---------------------------------------------------------------------------
+# the wall u* rule before the projection (update_vstar_boundary)
+
+def _vstar_loops(c):
+    """A second restatement in loops of d_get_v*star_*face
+    (CFD/G_BoundaryFunctions.h:369-470)."""
+    vs = [a.copy() for a in c.vs]
+    N = c.N
+    for a in range(3):
+        t, ids, m = c.ft[a], c.bcid[a], c.marks[a]
+        lam = c.lam[a] if c.lam is not None else np.zeros(t.shape)
+        for iz in range(1, N[2] + 2):
+            for iy in range(1, N[1] + 2):
+                for ix in range(1, N[0] + 2):
+                    if t[iz, iy, ix] != W.F_BOUNDARY:
+                        continue
+                    b = ids[iz, iy, ix]
+                    typ = c.bc_type[b]
+                    val = 0.0
+                    if typ == W.BC_INFLOW:
+                        val = (1.0 - lam[iz, iy, ix]) * c.bc_v[a][b]
+                    elif typ == W.BC_OUTLET:
+                        j = [ix, iy, iz]
+                        j[a] += -1 if m[iz, iy, ix] == 2 else 1
+                        val = vs[a][j[2], j[1], j[0]]
+                    vs[a][iz, iy, ix] = val
+    return tuple(vs)
+
+
+@pytest.mark.parametrize("spec", [
+    dict(N=(7, 6, 5), seed=1, sides=("x+", "z-")),
+    dict(N=(9, 8, 8), seed=2, sides=("x-", "y+", "z+"), solid_fraction=0.4, solid_margin=3),
+    dict(N=(5, 7, 4), seed=3, sides=("y-",), lam=False),
+])
+def test_vstar_boundary_oracle_equals_loop_restatement(oracle_lib, spec):
+    c = W.post_case(**spec)
+    got = oracle_lib.vstar_boundary(c.N, c.bc_type, c.bc_v, c.ft, c.bcid, c.marks, c.lam, c.vs)
+    want = _vstar_loops(c)
+    for a, b in zip(got, want):
+        assert np.array_equal(a, b)
+    # interior faces keep u*
+    for a, t, v in zip(got, c.ft, c.vs):
+        assert np.array_equal(a[t == W.F_INTERIOR], v[t == W.F_INTERIOR])
+
+
+def test_vstar_boundary_noslip_walls_make_the_neumann_system_compatible(oracle_lib):
+    """With no-slip walls the wall u* is 0, so the divergence of u* sums to 0
+    over the box (the pure-Neumann system's compatibility condition)."""
+    c = W.post_case((10, 9, 8), seed=4, sides=())
+    only_noslip = np.zeros(5, np.uint8)
+    vs = oracle_lib.vstar_boundary(c.N, only_noslip, c.bc_v, c.ft, c.bcid, None, None, c.vs)
+    nx, ny, nz = c.N
+    for a, t in zip(vs, c.ft):
+        assert np.all(a[t == W.F_BOUNDARY] == 0.0)
+    net = (vs[0][1:nz + 1, 1:ny + 1, nx + 1].sum() - vs[0][1:nz + 1, 1:ny + 1, 1].sum()
+           + vs[1][1:nz + 1, ny + 1, 1:nx + 1].sum() - vs[1][1:nz + 1, 1, 1:nx + 1].sum()
+           + vs[2][nz + 1, 1:ny + 1, 1:nx + 1].sum() - vs[2][1, 1:ny + 1, 1:nx + 1].sum())
+    assert net == 0.0
+
+
+VSTAR_GOLDEN = vstar_golden_names()
+
+
+@pytest.mark.skipif(not VSTAR_GOLDEN, reason="no update_vstar_boundary golden vectors")
+@pytest.mark.parametrize("name", VSTAR_GOLDEN)
+def test_vstar_boundary_oracle_matches_reference_golden(oracle_lib, name):
+    meta, arr = load_golden(name)
+    c = post_case_from_spec(meta)
+    got = oracle_lib.vstar_boundary(c.N, c.bc_type, c.bc_v, c.ft, c.bcid, c.marks, c.lam, c.vs)
+    for k, a in zip(("vxs", "vys", "vzs"), got):
         assert np.array_equal(a, arr[k]), k
