@@ -256,6 +256,25 @@ smac_status smac_update_vstar_boundary(const smac_grid_desc* d, const smac_bound
                                       const uint8_t* fyo, const uint8_t* fzo, const double* lamx, const double* lamy,
                                       const double* lamz, double* vxs, double* vys, double* vzs, void* stream);
 
+/* Surface-tension face force f_s from the volume fraction,
+ * G_SMACSolver::calc_surface_tension (CFD/G_SMACSolver_VoF.cu:435-445):
+ *  1. on C_INTERIOR cells: grad alpha (central differences, one-sided next to
+ *     non-interior cells), |grad alpha| into grad_mag, the unit normal into
+ *     nx/ny/nz (0 where |grad|^2 <= 1e-12); other cells keep their values
+ *     (k_calc_interface_normal :87-182);
+ *  2. on cells 1..N: kappa = -div n, 0 outside 0.01 <= alpha <= 0.99, a
+ *     neighbour counting only if C_INTERIOR with |grad alpha| > 1e-6
+ *     (k_calc_curvature :184-290);
+ *  3. every entry of fsx/fsy/fsz: sigma kappa_f (alpha_R - alpha_L) / h on
+ *     faces 2..N along their axis and 1..N across between two C_INTERIOR
+ *     cells (kappa_f the mean of the cells' kappa where 0.01 < alpha < 0.99),
+ *     0 elsewhere (k_calc_surface_tension_face :292-433).
+ * nx, ny, nz, kappa, grad_mag are cell arrays: the grid's nx_, ny_, nz_,
+ * kappa_ and p_tmp_, read and written as the reference does. */
+smac_status smac_surface_tension(const smac_grid_desc* d, const double* alpha, const uint8_t* celltype, double sigma,
+                                 double* nx, double* ny, double* nz, double* kappa, double* grad_mag, double* fsx,
+                                 double* fsy, double* fsz, void* stream);
+
 /* Velocity part of update_boundary_ghost, in place on (vx, vy, vz):
  *  1. outlet faces (k_update_v*_outlet, CFD/G_BoundaryFunctions.cu:143-255):
  *     a face with outlet mark 1 (interior side +1) or 2 (side -1) -- the marks

@@ -71,7 +71,7 @@ EXPORTS = [
     "smac_set_rhs", "smac_correct", "smac_project", "smac_project_adjoint", "smac_apply_A", "smac_time_kernel",
     "smac_selftest_sweep", "smac_apply_A_dot_noalloc", "smac_async_create", "smac_async_submit",
     "smac_async_wait", "smac_async_destroy", "smac_update_boundary_faces", "smac_update_pressure_ghost",
-    "smac_update_velocity_ghost", "smac_face_gradp", "smac_update_vstar_boundary",
+    "smac_update_velocity_ghost", "smac_face_gradp", "smac_update_vstar_boundary", "smac_surface_tension",
 ]
 
 
@@ -116,6 +116,7 @@ def load(path: str = LIB_PATH):
         "smac_update_velocity_ghost": [ctypes.POINTER(GridDesc), ctypes.POINTER(BoundaryTable), u8p, u8p, u8p,
                                        u8p, u8p, u8p, dp, dp, dp, dp, dp, dp, dp, dp, dp, dp, d, dp, dp, dp, vp],
         "smac_face_gradp": [ctypes.POINTER(GridDesc), dp, dp, dp, dp, vp],
+        "smac_surface_tension": [ctypes.POINTER(GridDesc), dp, u8p, d, dp, dp, dp, dp, dp, dp, dp, dp, vp],
         "smac_update_vstar_boundary": [ctypes.POINTER(GridDesc), ctypes.POINTER(BoundaryTable), u8p, u8p, u8p, u8p,
                                        u8p, u8p, u8p, u8p, u8p, dp, dp, dp, dp, dp, dp, vp],
     }

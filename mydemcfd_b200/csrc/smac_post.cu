@@ -1,5 +1,6 @@
-// smac_post.cu -- the pass after the projection: pressure in solid and ghost
-// cells, outlet and ghost velocities, face pressure gradient.
+// smac_post.cu -- the calls either side of the projection: before it the wall
+// u* rule and the surface-tension force; after it the pressure in solid and
+// ghost cells, outlet and ghost velocities, and the face pressure gradient.
 //
 // The reference runs it as G_SMACSolver::update_boundary_ghost followed by
 // make_face_gradp (CFD/G_SMACSolver.cu:1144-1363, CFD/G_BoundaryFunctions.cu:
@@ -553,6 +554,177 @@ __global__ void __launch_bounds__(GP_TX* GP_TY) k_face_gradp(RefDims R, const do
   gz[R.zf(ix, iy, iz)] = DMUL(DSUB(pc, __ldg(p + c - sxy)), idz);
 }
 
+// ---------------------------------------------------------------------------
+// Surface tension (G_SMACSolver::calc_surface_tension,
+// CFD/G_SMACSolver_VoF.cu:87-445): normals, curvature, face force
+
+struct StArgs {
+  RefDims R;
+  const double* alpha;
+  const uint8_t* ct;
+  double* nx;
+  double* ny;
+  double* nz;
+  double* kappa;
+  double* gm;  // |grad alpha| (the reference's p_tmp_)
+  double* fs[3];
+  double sigma;
+  double ih[3], i2h[3];  // 1/h and 1/(2h), computed as the reference does
+};
+
+// One-sided or central difference along an axis from the two neighbours'
+// flags (the branches of k_calc_interface_normal / k_calc_curvature).
+__device__ __forceinline__ double st_diff(bool p, bool m, double fp, double f0, double fm, double i2h, double ih) {
+  if (p && m) return DMUL(DSUB(fp, fm), i2h);
+  if (p) return DMUL(DSUB(fp, f0), ih);
+  if (m) return DMUL(DSUB(f0, fm), ih);
+  return 0.0;
+}
+
+// Pass 1, k_calc_interface_normal (:87-182): grad alpha, |grad alpha| and the
+// unit normal of every C_INTERIOR cell; other cells are left as they are.
+__global__ void __launch_bounds__(256) k_st_normal(StArgs A) {
+  const RefDims& R = A.R;
+  const int ix = blockIdx.x * 32 + threadIdx.x + 1, iy = blockIdx.y * 8 + threadIdx.y + 1, iz = blockIdx.z + 1;
+  if (ix > R.Nx || iy > R.Ny) return;
+  const long long sx = R.Nx + 2, sxy = sx * (R.Ny + 2), c = R.cell(ix, iy, iz);
+  if (A.ct[c] != kInterior) return;
+  const double* a = A.alpha;
+  const double gx = st_diff(A.ct[c + 1] == kInterior, A.ct[c - 1] == kInterior, a[c + 1], a[c], a[c - 1], A.i2h[0],
+                            A.ih[0]);
+  const double gy = st_diff(A.ct[c + sx] == kInterior, A.ct[c - sx] == kInterior, a[c + sx], a[c], a[c - sx],
+                            A.i2h[1], A.ih[1]);
+  const double gz = st_diff(A.ct[c + sxy] == kInterior, A.ct[c - sxy] == kInterior, a[c + sxy], a[c], a[c - sxy],
+                            A.i2h[2], A.ih[2]);
+  const double mag2 = DADD(DADD(DMUL(gx, gx), DMUL(gy, gy)), DMUL(gz, gz));
+  const double mag = __dsqrt_rn(mag2);
+  A.gm[c] = mag;
+  if (mag2 > 1e-12) {
+    const double inv = __ddiv_rn(1.0, mag);
+    A.nx[c] = DMUL(gx, inv);
+    A.ny[c] = DMUL(gy, inv);
+    A.nz[c] = DMUL(gz, inv);
+  } else {
+    A.nx[c] = 0.0;
+    A.ny[c] = 0.0;
+    A.nz[c] = 0.0;
+  }
+}
+
+// Curvature of cell (ix,iy,iz) in 1..N, k_calc_curvature (:184-290):
+// 0 outside 0.01 <= alpha <= 0.99, else -div n, a neighbour counting where
+// it is C_INTERIOR with |grad alpha| > 1e-6.
+__device__ double st_kappa(const StArgs& A, int ix, int iy, int iz) {
+  const RefDims& R = A.R;
+  const long long sx = R.Nx + 2, sxy = sx * (R.Ny + 2), c = R.cell(ix, iy, iz);
+  const double a = A.alpha[c];
+  if (a > 0.99 || a < 0.01) return 0.0;
+  auto ok = [&](long long n) { return A.ct[n] == kInterior && A.gm[n] > 1e-6; };
+  const double dnx = st_diff(ok(c + 1), ok(c - 1), A.nx[c + 1], A.nx[c], A.nx[c - 1], A.i2h[0], A.ih[0]);
+  const double dny = st_diff(ok(c + sx), ok(c - sx), A.ny[c + sx], A.ny[c], A.ny[c - sx], A.i2h[1], A.ih[1]);
+  const double dnz = st_diff(ok(c + sxy), ok(c - sxy), A.nz[c + sxy], A.nz[c], A.nz[c - sxy], A.i2h[2], A.ih[2]);
+  return -DADD(DADD(dnx, dny), dnz);
+}
+
+// Face force between cells m (low) and p (high), k_calc_surface_tension_face
+// (:292-433): sigma kappa_f (alpha_p - alpha_m) / h.
+__device__ __forceinline__ double st_force(double sigma, double ap, double am, double kp, double km, double ih) {
+  const bool vp = ap > 1e-2 && ap < 1 - 1e-2, vm = am > 1e-2 && am < 1 - 1e-2;
+  const double kf = vp && vm ? DMUL(0.5, DADD(kp, km)) : vp ? kp : vm ? km : 0.0;
+  return DMUL(DMUL(DMUL(sigma, kf), DSUB(ap, am)), ih);
+}
+
+constexpr int ST_TX = 32, ST_TY = 8;
+
+// Pass 2: curvature and face force fused.  A block owns a 32 x 8 tile of one
+// plane: each thread computes its cell's curvature (stored) and the one
+// below it, 40 threads also the tile's low-x column and low-y row (into a
+// shared tile), and after one barrier every thread writes the three faces on
+// the low side of its cell.  Cells with alpha outside [0.01, 0.99], most of
+// them, cost one load per curvature, so the recomputation is cheap; a
+// z-march that carried the curvature below in a register ran at a quarter of
+// the occupancy (one barrier per plane, serial planes) and took 2.5x as long.
+// Faces 1..N of every family are written (0 where the reference's memset
+// leaves 0); the rest is k_st_rim's.
+__global__ void __launch_bounds__(ST_TX* ST_TY, 4) k_st_force(StArgs A) {
+  __shared__ double ks[ST_TY + 1][ST_TX + 1];
+  const RefDims& R = A.R;
+  const int tx = threadIdx.x, ty = threadIdx.y, t = ty * ST_TX + tx;
+  const int x0 = blockIdx.x * ST_TX, y0 = blockIdx.y * ST_TY, iz = blockIdx.z + 1;
+  const int ix = x0 + tx + 1, iy = y0 + ty + 1;
+  const bool in = ix <= R.Nx && iy <= R.Ny;
+  // the extra cell: column x0 (rows y0+1..y0+8) or row y0 (columns x0+1..x0+32)
+  const bool hcol = t < ST_TY, hrow = t >= ST_TY && t < ST_TY + ST_TX;
+  const int hx = hcol ? x0 : x0 + 1 + (t - ST_TY), hy = hcol ? y0 + 1 + t : y0;
+  const bool hin = (hcol || hrow) && hx >= 1 && hx <= R.Nx && hy >= 1 && hy <= R.Ny;
+  const long long sx = R.Nx + 2, sxy = sx * (R.Ny + 2);
+  double k = 0.0, kb = 0.0, a0 = 0.0, ax = 0.0, ay = 0.0, az = 0.0;
+  bool fx = false, fy = false, fz = false;
+  long long c = 0;
+  if (in) {
+    // everything the faces need but the shared tile, before the barrier
+    c = R.cell(ix, iy, iz);
+    const bool c0 = A.ct[c] == kInterior;
+    fx = ix >= 2 && c0 && A.ct[c - 1] == kInterior;
+    fy = iy >= 2 && c0 && A.ct[c - sx] == kInterior;
+    fz = iz >= 2 && c0 && A.ct[c - sxy] == kInterior;
+    a0 = A.alpha[c];
+    ax = A.alpha[c - 1];
+    ay = A.alpha[c - sx];
+    az = A.alpha[c - sxy];
+    k = st_kappa(A, ix, iy, iz);
+    if (fz) kb = st_kappa(A, ix, iy, iz - 1);
+    A.kappa[c] = k;
+  }
+  ks[ty + 1][tx + 1] = k;
+  if (hcol || hrow) {
+    const double kh = hin ? st_kappa(A, hx, hy, iz) : 0.0;
+    if (hcol) ks[t + 1][0] = kh;
+    else ks[0][t - ST_TY + 1] = kh;
+  }
+  __syncthreads();
+  if (!in) return;
+  A.fs[0][R.xf(ix, iy, iz)] = fx ? st_force(A.sigma, a0, ax, k, ks[ty + 1][tx], A.ih[0]) : 0.0;
+  A.fs[1][R.yf(ix, iy, iz)] = fy ? st_force(A.sigma, a0, ay, k, ks[ty][tx + 1], A.ih[1]) : 0.0;
+  A.fs[2][R.zf(ix, iy, iz)] = fz ? st_force(A.sigma, a0, az, k, kb, A.ih[2]) : 0.0;
+}
+
+// Zero of every face outside the box 1..N of each family (the part of the
+// reference's memset that k_st_force does not overwrite).  blockIdx.y:
+// family * 3 + group; group 0 the planes z outside 1..Nz, group 1 the rows y
+// outside 1..Ny of planes 1..Nz, group 2 the entries x outside 1..Nx of the
+// remaining rows.  An axis of S entries has S - N outside indices: 0 and
+// N+1 .. S-1.
+__global__ void __launch_bounds__(256) k_st_rim(StArgs A) {
+  const RefDims& R = A.R;
+  const int f = blockIdx.y / 3, grp = blockIdx.y % 3;
+  const uint32_t B0 = R.Nx, B1 = R.Ny, B2 = R.Nz;
+  const uint32_t S0 = B0 + 2 + (f == 0), S1 = B1 + 2 + (f == 1), S2 = B2 + 2 + (f == 2);
+  const uint32_t o0 = S0 - B0, o1 = S1 - B1, o2 = S2 - B2;
+  const uint32_t total = grp == 0 ? o2 * S0 * S1 : grp == 1 ? B2 * o1 * S0 : B2 * B1 * o0;
+  double* fs = A.fs[f];
+  for (uint32_t u = blockIdx.x * blockDim.x + threadIdx.x; u < total; u += gridDim.x * blockDim.x) {
+    uint32_t x, y, z;
+    if (grp == 0) {
+      const uint32_t zi = u / (S0 * S1), r = u - zi * (S0 * S1);
+      z = zi == 0 ? 0 : B2 + zi;
+      y = r / S0;
+      x = r - y * S0;
+    } else if (grp == 1) {
+      const uint32_t zi = u / (o1 * S0), r = u - zi * (o1 * S0), yi = r / S0;
+      z = 1 + zi;
+      y = yi == 0 ? 0 : B1 + yi;
+      x = r - yi * S0;
+    } else {
+      const uint32_t zi = u / (B1 * o0), r = u - zi * (B1 * o0), yi = r / o0, xi = r - yi * o0;
+      z = 1 + zi;
+      y = 1 + yi;
+      x = xi == 0 ? 0 : B0 + xi;
+    }
+    fs[((long long)z * S1 + y) * S0 + x] = 0.0;
+  }
+}
+
 int sm_count() {
   static int n = 0;
   if (!n) {
@@ -719,6 +891,37 @@ smac_status smac_update_vstar_boundary(const smac_grid_desc* d, const smac_bound
   fill_table(&V.bc, bc);
   const long long nmax = V.n[0] > V.n[1] ? (V.n[0] > V.n[2] ? V.n[0] : V.n[2]) : (V.n[1] > V.n[2] ? V.n[1] : V.n[2]);
   k_vstar_boundary<<<dim3(scan_blocks_for(nmax, sm_count()), 3), kPostThreads, 0, (cudaStream_t)stream>>>(V);
+  return launch_status(fn);
+}
+
+smac_status smac_surface_tension(const smac_grid_desc* d, const double* alpha, const uint8_t* celltype, double sigma,
+                                 double* nx, double* ny, double* nz, double* kappa, double* grad_mag, double* fsx,
+                                 double* fsy, double* fsz, void* stream) {
+  static const char* fn = "smac_surface_tension";
+  if (!d || !alpha || !celltype || !nx || !ny || !nz || !kappa || !grad_mag || !fsx || !fsy || !fsz) {
+    smac::set_error_text("%s: null argument", fn);
+    return SMAC_BAD_ARG;
+  }
+  if (bad_desc(d, fn, 1)) return SMAC_BAD_SHAPE;
+  StArgs A;
+  A.R = RefDims{d->nx, d->ny, d->nz};
+  A.alpha = alpha;
+  A.ct = celltype;
+  A.nx = nx; A.ny = ny; A.nz = nz;
+  A.kappa = kappa;
+  A.gm = grad_mag;
+  A.fs[0] = fsx; A.fs[1] = fsy; A.fs[2] = fsz;
+  A.sigma = sigma;
+  const double h[3] = {d->dx, d->dy, d->dz};
+  for (int k = 0; k < 3; ++k) {
+    A.ih[k] = 1. / h[k];
+    A.i2h[k] = 1. / (2. * h[k]);
+  }
+  cudaStream_t s = (cudaStream_t)stream;
+  const unsigned bx = (unsigned)((d->nx + ST_TX - 1) / ST_TX), by = (unsigned)((d->ny + ST_TY - 1) / ST_TY);
+  k_st_rim<<<dim3(64, 9), 256, 0, s>>>(A);
+  k_st_normal<<<dim3(bx, by, (unsigned)d->nz), dim3(32, 8), 0, s>>>(A);
+  k_st_force<<<dim3(bx, by, (unsigned)d->nz), dim3(ST_TX, ST_TY), 0, s>>>(A);
   return launch_status(fn);
 }
 

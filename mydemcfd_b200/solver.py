@@ -466,6 +466,16 @@ def update_vstar_boundary_device(N, h, bc: BoundaryConditions, ft, bcid, marks, 
     del keep
 
 
+def surface_tension_device(N, h, alpha, ct, sigma, work, fs):
+    """smac_surface_tension: work = (nx, ny, nz, kappa, grad_mag) cell tensors
+    (the grid's nx_, ny_, nz_, kappa_, p_tmp_), fs = (fsx, fsy, fsz) face
+    tensors, all written as G_SMACSolver::calc_surface_tension writes them."""
+    d = nat.GridDesc(*N, *h)
+    s = torch.cuda.current_stream().cuda_stream
+    nat.check(nat.load().smac_surface_tension(ctypes.byref(d), _ptr(alpha), _ptr(ct), ctypes.c_double(sigma),
+                                              *map(_ptr, work), *map(_ptr, fs), ctypes.c_void_p(s)))
+
+
 def face_gradp_device(N, h, p, gp):
     """smac_face_gradp: gp = (gpx, gpy, gpz) face tensors, faces 1..N+1 written."""
     d = nat.GridDesc(*N, *h)

@@ -366,3 +366,40 @@ def post_case(N, seed, h=(0.03125, 0.03125, 0.03125), dt=0.5, g=(0.0, -1.5, -9.8
                     vs=tuple(np.ascontiguousarray(rnd(60 + k, key)) for k, key in enumerate("xyz")),
                     fb=tuple(np.ascontiguousarray(a) for a in fb),
                     v=tuple(np.ascontiguousarray(rnd(70 + k, key)) for k, key in enumerate("xyz")))
+
+
+def surface_case(N, seed, kind="sphere", solid_fraction=0.0, sigma=0.07, h=0.03125):
+    """Inputs of the surface-tension force: (N, h, alpha, ct, sigma).
+    kind "sphere": a sphere of radius 0.3 of the smallest extent, centred
+    U[0.35, 0.65] of the box, alpha ramped over 1.5 cells; kind "random":
+    alpha U[0,1) with 30% set to 0, 20% to 1 and 10% within 1e-3 of the
+    0.01 / 0.99 thresholds.  solid_fraction > 0 turns that share of the cells
+    2..N-1 C_SOLID (single cells).  h is a power of two, so the reference's
+    spacing (N h) / N equals it."""
+    N = tuple(int(n) for n in N)
+    hh = (float(h),) * 3
+    sh = shapes(N)
+    ncell = int(np.prod(sh["cell"]))
+    ct, fxt, fyt, fzt = box_types(N)
+    if kind == "sphere":
+        u = uniform01(substream(seed, 80), 3)
+        ext = np.array(N, np.float64) * h
+        centre = (0.35 + 0.3 * u) * ext
+        alpha = sphere_alpha(N, hh, centre, 0.3 * ext.min(), 1.5)
+    else:
+        u = uniform01(substream(seed, 81), ncell)
+        v = uniform01(substream(seed, 82), ncell)
+        alpha = u.copy()
+        alpha[v < 0.3] = 0.0
+        alpha[(v >= 0.3) & (v < 0.5)] = 1.0
+        near = (v >= 0.5) & (v < 0.6)
+        alpha[near] = np.where(u[near] < 0.5, 0.01, 0.99) + (u[near] - 0.5) * 2e-3
+        alpha = alpha.reshape(sh["cell"])
+    if solid_fraction > 0.0:
+        nx, ny, nz = N
+        w = uniform01(substream(seed, 83), ncell).reshape(sh["cell"])
+        inner = np.zeros(sh["cell"], bool)
+        inner[2:nz, 2:ny, 2:nx] = True
+        sf = np.where(inner & (w < solid_fraction), 1.0, 0.0)
+        set_solid_cells(sf, ct, fxt, fyt, fzt)
+    return N, hh, np.ascontiguousarray(alpha), ct, float(sigma)

@@ -216,6 +216,22 @@ def vstar_boundary(N, bc_type, bc_v, ft, bcid, marks, lam, vs):
     return tuple(vs)
 
 
+def surface_tension(N, h, alpha, ct, sigma, nx=None, ny=None, nz=None, kappa=None, gm=None):
+    """G_SMACSolver::calc_surface_tension (CFD/G_SMACSolver_VoF.cu:435-445):
+    returns (fsx, fsy, fsz, nx, ny, nz, kappa, gm); the work arrays start from
+    the given ones (zeros by default), as the reference's keep their values
+    where it does not write them."""
+    sh = cell_shape(N)
+    work = [np.zeros(sh) if a is None else np.array(a, dtype=np.float64, order="C", copy=True)
+            for a in (nx, ny, nz, kappa, gm)]
+    fs = [np.zeros(xface_shape(N)), np.zeros(yface_shape(N)), np.zeros(zface_shape(N))]
+    c = ctypes.c_double
+    lib().orc_surface_tension(*N, c(h[0]), c(h[1]), c(h[2]), _p(np.ascontiguousarray(alpha, np.float64)),
+                              _u8(np.ascontiguousarray(ct, np.uint8)), c(sigma), *(_p(a) for a in work),
+                              *(_p(a) for a in fs))
+    return (*fs, *work)
+
+
 def post_pass(case):
     """G_SMACSolver::update_boundary_ghost then make_face_gradp
     (CFD/G_SMACSolver.cu:1277-1363) on a workloads.PostCase: returns

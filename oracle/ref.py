@@ -218,3 +218,38 @@ def post(case):
         raise RuntimeError(f"ref_post returned {rc}")
     out["ghost_ms"], out["gradp_ms"] = o.ghost_ms, o.gradp_ms
     return out
+
+
+class RefStIO(ctypes.Structure):
+    _fields_ = [("Nx", ctypes.c_int), ("Ny", ctypes.c_int), ("Nz", ctypes.c_int),
+                ("Lx", ctypes.c_double), ("Ly", ctypes.c_double), ("Lz", ctypes.c_double),
+                ("sigma", ctypes.c_double), ("alpha", _dp), ("ct", _u8p)] + \
+        [(k, _dp) for k in ("nx", "ny", "nz", "kappa", "gm", "fsx", "fsy", "fsz")] + [("ms", ctypes.c_double)]
+
+
+def surface_tension(N, h, alpha, ct, sigma):
+    """Run the reference's calc_surface_tension on zeroed work arrays:
+    returns (fsx, fsy, fsz, nx, ny, nz, kappa, gm, ms)."""
+    L = lib()
+    if not hasattr(L, "_st_set"):
+        L.ref_surface_tension.restype = ctypes.c_int
+        L.ref_surface_tension.argtypes = [ctypes.POINTER(RefStIO)]
+        L._st_set = True
+    nx_, ny_, nz_ = N
+    cell = (nz_ + 2, ny_ + 2, nx_ + 2)
+    shapes = [(nz_ + 2, ny_ + 2, nx_ + 3), (nz_ + 2, ny_ + 3, nx_ + 2), (nz_ + 3, ny_ + 2, nx_ + 2)]
+    alpha = np.ascontiguousarray(alpha, np.float64)
+    ct = np.ascontiguousarray(ct, np.uint8)
+    work = [np.zeros(cell) for _ in range(5)]
+    fs = [np.zeros(s) for s in shapes]
+    io = RefStIO()
+    io.Nx, io.Ny, io.Nz = N
+    io.Lx, io.Ly, io.Lz = (n * hh for n, hh in zip(N, h))
+    io.sigma = sigma
+    io.alpha, io.ct = _p(alpha), _p(ct, ctypes.c_uint8)
+    io.nx, io.ny, io.nz, io.kappa, io.gm = (_p(a) for a in work)
+    io.fsx, io.fsy, io.fsz = (_p(a) for a in fs)
+    rc = L.ref_surface_tension(ctypes.byref(io))
+    if rc != 0:
+        raise RuntimeError(f"ref_surface_tension returned {rc}")
+    return (*fs, *work, io.ms)

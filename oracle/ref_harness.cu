@@ -7,10 +7,10 @@
 // It follows the reference driver's set-up (CFD/main.cu:183-243): a host
 // SMACSolver with calloc'ed members, G_SMACSolver::solver_malloc + cpuTogpu,
 // G_PCGSolver + G_GMGSolver::initialize, set_solver, tol_, then
-// G_SMACSolver::solve_poisson() and correct_vof_velocity().  Two more
-// entries run the calls either side of it on given arrays: ref_vstar
-// (update_vstar_boundary) and ref_post (update_boundary_ghost and
-// make_face_gradp).
+// G_SMACSolver::solve_poisson() and correct_vof_velocity().  More entries
+// run the calls either side of it on given arrays: ref_vstar
+// (update_vstar_boundary), ref_surface_tension (calc_surface_tension) and
+// ref_post (update_boundary_ghost and make_face_gradp).
 //
 // Two things the reference leaves to chance are pinned here: every multigrid
 // level array is zeroed after G_GMGSolver::initialize (the reference reads
@@ -306,6 +306,57 @@ int ref_vstar(const ref_post_inputs* in, double* vxs, double* vys, double* vzs, 
   if (e == cudaSuccess) {
     g.gpuTocpu(solv.grid_);
     get(hg.f_vx_star_, vxs); get(hg.f_vy_star_, vys); get(hg.f_vz_star_, vzs);
+    e = cudaGetLastError();
+  }
+  g.solver_free();
+  solv.solver_free();
+  return e == cudaSuccess ? 0 : -2;
+}
+
+struct ref_st_io {
+  int Nx, Ny, Nz;
+  double Lx, Ly, Lz, sigma;
+  const double* alpha;
+  const uint8_t* ct;
+  double *nx, *ny, *nz, *kappa, *gm;  // in: initial contents (nx_, ny_, nz_, kappa_, p_tmp_); out: final
+  double *fsx, *fsy, *fsz;            // out
+  double ms;                          // out: device time of calc_surface_tension
+};
+
+// G_SMACSolver::calc_surface_tension (CFD/G_SMACSolver_VoF.cu:435-445) on
+// host arrays.  Returns 0 on success, -2 on a CUDA error.
+int ref_surface_tension(ref_st_io* io) {
+  const int Nx = io->Nx, Ny = io->Ny, Nz = io->Nz;
+  SMACSolver solv;
+  solv.set_calc_properties(0., 0., 0., io->Lx, io->Ly, io->Lz, Nx, Ny, Nz);
+  solv.grid_.bc_.num_boundary_id_ = 1;
+  solv.solver_malloc();
+  StaggeredGrid& hg = solv.grid_;
+  put(hg.alpha_, io->alpha); put(hg.celltype_, io->ct);
+  put(hg.nx_, io->nx); put(hg.ny_, io->ny); put(hg.nz_, io->nz); put(hg.kappa_, io->kappa); put(hg.p_tmp_, io->gm);
+  hg.sigma_.data_[0] = io->sigma;
+  G_SMACSolver g;
+  g.set_calc_properties(0., 0., 0., io->Lx, io->Ly, io->Lz, Nx, Ny, Nz);
+  g.grid_.bc_.num_boundary_id_ = 1;
+  g.solver_malloc();
+  g.cpuTogpu(solv.grid_);
+  g.set_block_grid(Nx, Ny, Nz);
+  cudaDeviceSynchronize();
+  cudaEvent_t ev[2];
+  for (auto& x : ev) cudaEventCreate(&x);
+  cudaEventRecord(ev[0], 0);
+  g.calc_surface_tension();
+  cudaEventRecord(ev[1], 0);
+  cudaDeviceSynchronize();
+  float t = 0.f;
+  cudaEventElapsedTime(&t, ev[0], ev[1]);
+  io->ms = t;
+  for (auto& x : ev) cudaEventDestroy(x);
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) {
+    g.gpuTocpu(solv.grid_);
+    get(hg.nx_, io->nx); get(hg.ny_, io->ny); get(hg.nz_, io->nz); get(hg.kappa_, io->kappa); get(hg.p_tmp_, io->gm);
+    get(hg.f_sx_, io->fsx); get(hg.f_sy_, io->fsy); get(hg.f_sz_, io->fsz);
     e = cudaGetLastError();
   }
   g.solver_free();

@@ -834,6 +834,111 @@ void orc_vstar_boundary(int Nx, int Ny, int Nz, const uint8_t* bct, const double
   }
 }
 
+// Surface-tension face force, G_SMACSolver::calc_surface_tension
+// (CFD/G_SMACSolver_VoF.cu:435-445): the three reference kernels in order.
+//  1. k_calc_interface_normal (:87-182): on C_INTERIOR cells, grad alpha by
+//     central differences (one-sided next to non-interior cells, 0 with no
+//     interior neighbour on either side), |grad| into gm, n = grad / |grad|
+//     (0 when |grad|^2 <= 1e-12).  Other cells keep n and gm.
+//  2. k_calc_curvature (:184-290): on cells 1..N, kappa = 0 where alpha >
+//     0.99 or < 0.01, else -div n by the same differences, a neighbour
+//     counting only if C_INTERIOR with gm > 1e-6.
+//  3. k_calc_surface_tension_face (:292-433): f_s = 0 everywhere, then on
+//     faces 2..N along their axis (1..N across) between two C_INTERIOR cells
+//     f_s = sigma kappa_f (alpha_R - alpha_L) / h, kappa_f the mean of the
+//     two cells' kappa where both have 0.01 < alpha < 0.99, the one that
+//     has, or 0.
+// nx/ny/nz/gm/kappa are in-out cell arrays (the grid's nx_, ny_, nz_, p_tmp_
+// and kappa_), f_s three face arrays.
+void orc_surface_tension(int Nx, int Ny, int Nz, double dx, double dy, double dz, const double* alpha,
+                         const uint8_t* ct, double sigma, double* nx, double* ny, double* nz, double* kappa,
+                         double* gm, double* fsx, double* fsy, double* fsz) {
+  View<const double> A{alpha, Nx + 2, Ny + 2, Nz + 2};
+  View<const uint8_t> C{ct, Nx + 2, Ny + 2, Nz + 2};
+  Arr NX{nx, Nx + 2, Ny + 2, Nz + 2}, NY{ny, Nx + 2, Ny + 2, Nz + 2}, NZ{nz, Nx + 2, Ny + 2, Nz + 2};
+  Arr K{kappa, Nx + 2, Ny + 2, Nz + 2}, G{gm, Nx + 2, Ny + 2, Nz + 2};
+  Arr FX{fsx, Nx + 3, Ny + 2, Nz + 2}, FY{fsy, Nx + 2, Ny + 3, Nz + 2}, FZ{fsz, Nx + 2, Ny + 2, Nz + 3};
+  const double idx = 1. / dx, idy = 1. / dy, idz = 1. / dz;
+  const double i2dx = 1. / (2. * dx), i2dy = 1. / (2. * dy), i2dz = 1. / (2. * dz);
+  // difference of f along one axis from the two neighbours' flags
+  auto diff = [](bool p, bool m, double fp, double f0, double fm, double i2h, double ih) {
+    if (p && m) return (fp - fm) * i2h;
+    if (p) return (fp - f0) * ih;
+    if (m) return (f0 - fm) * ih;
+    return 0.0;
+  };
+  for (int iz = 1; iz <= Nz; ++iz)
+    for (int iy = 1; iy <= Ny; ++iy)
+      for (int ix = 1; ix <= Nx; ++ix) {
+        if (C(ix, iy, iz) != C_INTERIOR) continue;
+        const double gx = diff(C(ix + 1, iy, iz) == C_INTERIOR, C(ix - 1, iy, iz) == C_INTERIOR, A(ix + 1, iy, iz),
+                               A(ix, iy, iz), A(ix - 1, iy, iz), i2dx, idx);
+        const double gy = diff(C(ix, iy + 1, iz) == C_INTERIOR, C(ix, iy - 1, iz) == C_INTERIOR, A(ix, iy + 1, iz),
+                               A(ix, iy, iz), A(ix, iy - 1, iz), i2dy, idy);
+        const double gz = diff(C(ix, iy, iz + 1) == C_INTERIOR, C(ix, iy, iz - 1) == C_INTERIOR, A(ix, iy, iz + 1),
+                               A(ix, iy, iz), A(ix, iy, iz - 1), i2dz, idz);
+        const double mag2 = gx * gx + gy * gy + gz * gz;
+        const double mag = std::sqrt(mag2);
+        G(ix, iy, iz) = mag;
+        if (mag2 > 1e-12) {
+          const double inv = 1. / mag;
+          NX(ix, iy, iz) = gx * inv;
+          NY(ix, iy, iz) = gy * inv;
+          NZ(ix, iy, iz) = gz * inv;
+        } else {
+          NX(ix, iy, iz) = 0.;
+          NY(ix, iy, iz) = 0.;
+          NZ(ix, iy, iz) = 0.;
+        }
+      }
+  const double th = 1e-6;
+  auto ok = [&](int x, int y, int z) { return C(x, y, z) == C_INTERIOR && G(x, y, z) > th; };
+  for (int iz = 1; iz <= Nz; ++iz)
+    for (int iy = 1; iy <= Ny; ++iy)
+      for (int ix = 1; ix <= Nx; ++ix) {
+        const double a = A(ix, iy, iz);
+        if (a > 0.99 || a < 0.01) {
+          K(ix, iy, iz) = 0.;
+          continue;
+        }
+        const double dnx = diff(ok(ix + 1, iy, iz), ok(ix - 1, iy, iz), NX(ix + 1, iy, iz), NX(ix, iy, iz),
+                                NX(ix - 1, iy, iz), i2dx, idx);
+        const double dny = diff(ok(ix, iy + 1, iz), ok(ix, iy - 1, iz), NY(ix, iy + 1, iz), NY(ix, iy, iz),
+                                NY(ix, iy - 1, iz), i2dy, idy);
+        const double dnz = diff(ok(ix, iy, iz + 1), ok(ix, iy, iz - 1), NZ(ix, iy, iz + 1), NZ(ix, iy, iz),
+                                NZ(ix, iy, iz - 1), i2dz, idz);
+        K(ix, iy, iz) = -1.0 * (dnx + dny + dnz);
+      }
+  std::fill(fsx, fsx + FX.size(), 0.0);
+  std::fill(fsy, fsy + FY.size(), 0.0);
+  std::fill(fsz, fsz + FZ.size(), 0.0);
+  auto valid = [&](int x, int y, int z) { return A(x, y, z) > 1e-2 && A(x, y, z) < 1 - 1e-2; };
+  auto kface = [&](int x, int y, int z, int xm, int ym, int zm) {
+    const bool vp = valid(x, y, z), vm = valid(xm, ym, zm);
+    if (vp && vm) return 0.5 * (K(x, y, z) + K(xm, ym, zm));
+    if (vp) return K(x, y, z);
+    if (vm) return K(xm, ym, zm);
+    return 0.0;
+  };
+  for (int iz = 1; iz <= Nz; ++iz)
+    for (int iy = 1; iy <= Ny; ++iy)
+      for (int ix = 1; ix <= Nx; ++ix) {
+        const bool c0 = C(ix, iy, iz) == C_INTERIOR;
+        if (ix >= 2)
+          FX(ix, iy, iz) = c0 && C(ix - 1, iy, iz) == C_INTERIOR
+                               ? sigma * kface(ix, iy, iz, ix - 1, iy, iz) * (A(ix, iy, iz) - A(ix - 1, iy, iz)) * idx
+                               : 0.0;
+        if (iy >= 2)
+          FY(ix, iy, iz) = c0 && C(ix, iy - 1, iz) == C_INTERIOR
+                               ? sigma * kface(ix, iy, iz, ix, iy - 1, iz) * (A(ix, iy, iz) - A(ix, iy - 1, iz)) * idy
+                               : 0.0;
+        if (iz >= 2)
+          FZ(ix, iy, iz) = c0 && C(ix, iy, iz - 1) == C_INTERIOR
+                               ? sigma * kface(ix, iy, iz, ix, iy, iz - 1) * (A(ix, iy, iz) - A(ix, iy, iz - 1)) * idz
+                               : 0.0;
+      }
+}
+
 // Outlet boundary faces (G_SMACSolver::update_boundary_faces,
 // CFD/G_SMACSolver_VoF.cu:1798-1950): f_b of an outlet face is twice the f_b
 // of the face next to it on the interior side (p = 0 on the outlet).  The

@@ -46,7 +46,20 @@ def golden_names():
     if not os.path.isdir(GOLDEN):
         return []
     return sorted(f[:-4] for f in os.listdir(GOLDEN)
-                  if f.endswith(".npz") and not f.startswith("post") and not f.startswith("vstar"))
+                  if f.endswith(".npz") and not f.startswith(("post", "vstar", "surface")))
+
+
+def surface_golden_names():
+    """Fixtures of the reference's calc_surface_tension."""
+    if not os.path.isdir(GOLDEN):
+        return []
+    return sorted(f[:-4] for f in os.listdir(GOLDEN) if f.endswith(".npz") and f.startswith("surface"))
+
+
+def surface_case_from_spec(spec):
+    spec = dict(spec)
+    spec["N"] = tuple(spec["N"])
+    return W.surface_case(**spec)
 
 
 def vstar_golden_names():

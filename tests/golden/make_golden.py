@@ -56,6 +56,14 @@ VSTAR_CASES = [
     ("vstar9x7x11_s3_nolam", dict(N=(9, 7, 11), seed=3, sides=("x+", "y-", "z+"), lam=False)),
 ]
 
+# The surface-tension force (calc_surface_tension): workloads.surface_case
+# kwargs; the work arrays start at zero as the reference driver's do.
+SURFACE_CASES = [
+    ("surface24_s3_sphere", dict(N=(24, 24, 24), seed=3, kind="sphere")),
+    ("surface20x16x12_s5_random", dict(N=(20, 16, 12), seed=5, kind="random", solid_fraction=0.15)),
+    ("surface18x20x16_s6_sphere_solid", dict(N=(18, 20, 16), seed=6, kind="sphere", solid_fraction=0.1)),
+]
+
 
 def oracle_solid_fraction(N, h, origin, spheres):
     return O.solid_fraction_spheres(N, h, origin, spheres)
@@ -97,6 +105,13 @@ def main():
         vxs, vys, vzs, _ = REF.vstar(W.post_case(**spec))
         np.savez_compressed(os.path.join(args.out, name + ".npz"), meta=np.array(json.dumps(spec)), vxs=vxs,
                             vys=vys, vzs=vzs)
+        post_index[name] = spec
+        print(name, spec, flush=True)
+    for name, spec in SURFACE_CASES:
+        N, h, alpha, ct, sigma = W.surface_case(**spec)
+        fsx, fsy, fsz, nx, ny, nz, kappa, gm, _ = REF.surface_tension(N, h, alpha, ct, sigma)
+        np.savez_compressed(os.path.join(args.out, name + ".npz"), meta=np.array(json.dumps(spec)), fsx=fsx, fsy=fsy,
+                            fsz=fsz, nx=nx, ny=ny, nz=nz, kappa=kappa, gm=gm)
         post_index[name] = spec
         print(name, spec, flush=True)
     with open(os.path.join(args.out, "post_index.json"), "w") as f:

@@ -1,5 +1,6 @@
 """The calls either side of the projection on the GPU: before it the wall u*
-rule (smac_update_vstar_boundary), after it the pass over p
+rule (smac_update_vstar_boundary) and the surface-tension force
+(smac_surface_tension), after it the pass over p
 (smac_update_pressure_ghost, smac_update_velocity_ghost, smac_face_gradp),
 against the oracle and the reference.
 
@@ -15,12 +16,13 @@ import torch
 from mydemcfd_b200 import _native as nat
 from mydemcfd_b200 import workloads as W
 from mydemcfd_b200.solver import (BoundaryConditions, DeviceGrid, SMACStep, face_gradp_device,
-                                  update_pressure_ghost_device, update_velocity_ghost_device,
+                                  surface_tension_device, update_pressure_ghost_device, update_velocity_ghost_device,
                                   update_vstar_boundary_device)
 from oracle import oracle as O
 from oracle import ref as REF
 
-from _cases import load_golden, post_case_from_spec, post_golden_names, vstar_golden_names
+from _cases import (load_golden, post_case_from_spec, post_golden_names, surface_case_from_spec,
+                    surface_golden_names, vstar_golden_names)
 
 pytestmark = pytest.mark.gpu
 
@@ -233,4 +235,58 @@ def test_vstar_boundary_against_reference_library_and_time_256():
             [_cuda(a) for a in c.marks], [_cuda(a) for a in c.lam], vs)
     ms = _device_ms(lambda: update_vstar_boundary_device(*args))
     print(f"update_vstar_boundary 256^3: {ms * 1e3:.1f} us (reference {ref_ms * 1e3:.1f} us)")
+    assert ms < ref_ms
+
+
+ST_KEYS = ("fsx", "fsy", "fsz", "nx", "ny", "nz", "kappa", "gm")
+
+
+def run_surface(N, h, alpha, ct, sigma, work=None):
+    sh = W.shapes(N)
+    work = [torch.zeros(sh["cell"], dtype=torch.float64, device="cuda") for _ in range(5)] if work is None else \
+        [_cuda(a) for a in work]
+    fs = [torch.full(sh[k], np.nan, dtype=torch.float64, device="cuda") for k in "xyz"]
+    surface_tension_device(N, h, _cuda(alpha), _cuda(ct), sigma, work, fs)
+    torch.cuda.synchronize()
+    return tuple(a.cpu().numpy() for a in fs + work)
+
+
+@pytest.mark.parametrize("spec", [
+    dict(N=(24, 24, 24), seed=3, kind="sphere"),
+    dict(N=(20, 16, 12), seed=5, kind="random", solid_fraction=0.15),
+    dict(N=(37, 19, 23), seed=7, kind="sphere", solid_fraction=0.1),
+])
+def test_surface_tension_bit_exact_against_oracle(spec):
+    N, h, alpha, ct, sigma = W.surface_case(**spec)
+    # work arrays with prior contents: cells the reference does not write keep them
+    sh = W.shapes(N)
+    work = [W.uniform_pm1(900 + k, int(np.prod(sh["cell"]))).reshape(sh["cell"]) for k in range(5)]
+    got = run_surface(N, h, alpha, ct, sigma, work)
+    want = O.surface_tension(N, h, alpha, ct, sigma, *work)
+    for k, a, b in zip(ST_KEYS, got, want):
+        assert np.array_equal(a, b), k
+
+
+@pytest.mark.parametrize("name", surface_golden_names())
+def test_surface_tension_bit_exact_against_reference_golden(name):
+    meta, arr = load_golden(name)
+    got = run_surface(*surface_case_from_spec(meta))
+    for k, a in zip(ST_KEYS, got):
+        assert np.array_equal(a, arr[k]), k
+
+
+@pytest.mark.skipif(not REF.available(), reason="reference build oracle/_ref not present")
+def test_surface_tension_against_reference_library_and_time_192():
+    N, h, alpha, ct, sigma = W.surface_case((192, 192, 192), seed=4, kind="sphere", solid_fraction=0.02)
+    REF.surface_tension(N, h, alpha, ct, sigma)  # loads the reference's kernels
+    *ref, ref_ms = REF.surface_tension(N, h, alpha, ct, sigma)
+    got = run_surface(N, h, alpha, ct, sigma)
+    for k, a, b in zip(ST_KEYS, got, ref):
+        assert np.array_equal(a, b), k
+    sh = W.shapes(N)
+    work = [torch.zeros(sh["cell"], dtype=torch.float64, device="cuda") for _ in range(5)]
+    fs = [torch.zeros(sh[k], dtype=torch.float64, device="cuda") for k in "xyz"]
+    a_d, ct_d = _cuda(alpha), _cuda(ct)
+    ms = _device_ms(lambda: surface_tension_device(N, h, a_d, ct_d, sigma, work, fs))
+    print(f"calc_surface_tension 192^3: {ms * 1e3:.1f} us (reference {ref_ms * 1e3:.1f} us)")
     assert ms < ref_ms

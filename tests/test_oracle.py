@@ -7,7 +7,7 @@ import pytest
 from mydemcfd_b200 import workloads as W
 
 from _cases import (build_case, fluid_demeaned, golden_names, load_golden, post_case_from_spec, post_golden_names,
-                    ref_grid, rel_err, vstar_golden_names)
+                    ref_grid, rel_err, surface_case_from_spec, surface_golden_names, vstar_golden_names)
 
 
 def test_box_types_match_reference_setup(oracle_lib):
@@ -403,4 +403,117 @@ def test_vstar_boundary_oracle_matches_reference_golden(oracle_lib, name):
     c = post_case_from_spec(meta)
     got = oracle_lib.vstar_boundary(c.N, c.bc_type, c.bc_v, c.ft, c.bcid, c.marks, c.lam, c.vs)
     for k, a in zip(("vxs", "vys", "vzs"), got):
+        assert np.array_equal(a, arr[k]), k
+
+
+# ---------------------------------------------------------------------------
+# the surface-tension force (calc_surface_tension)
+
+def _surface_loops(N, h, alpha, ct, sigma):
+    """A second restatement in loops of k_calc_interface_normal,
+    k_calc_curvature and k_calc_surface_tension_face
+    (CFD/G_SMACSolver_VoF.cu:87-433), from zeroed work arrays."""
+    import math
+    nx_, ny_, nz_ = N
+    sh = W.shapes(N)
+    n = [np.zeros(sh["cell"]) for _ in range(3)]
+    gm = np.zeros(sh["cell"])
+    kap = np.zeros(sh["cell"])
+    ih = [1.0 / x for x in h]
+    i2h = [1.0 / (2.0 * x) for x in h]
+    I = W.C_INTERIOR
+
+    def d(p, m, fp, f0, fm, a):
+        if p and m:
+            return (fp - fm) * i2h[a]
+        if p:
+            return (fp - f0) * ih[a]
+        if m:
+            return (f0 - fm) * ih[a]
+        return 0.0
+
+    off = [(1, 0, 0), (0, 1, 0), (0, 0, 1)]
+    for z in range(1, nz_ + 1):
+        for y in range(1, ny_ + 1):
+            for x in range(1, nx_ + 1):
+                if ct[z, y, x] != I:
+                    continue
+                g = []
+                for a, (ox, oy, oz) in enumerate(off):
+                    g.append(d(ct[z + oz, y + oy, x + ox] == I, ct[z - oz, y - oy, x - ox] == I,
+                               alpha[z + oz, y + oy, x + ox], alpha[z, y, x], alpha[z - oz, y - oy, x - ox], a))
+                m2 = g[0] * g[0] + g[1] * g[1] + g[2] * g[2]
+                m = math.sqrt(m2)
+                gm[z, y, x] = m
+                for a in range(3):
+                    n[a][z, y, x] = g[a] * (1.0 / m) if m2 > 1e-12 else 0.0
+    for z in range(1, nz_ + 1):
+        for y in range(1, ny_ + 1):
+            for x in range(1, nx_ + 1):
+                a0 = alpha[z, y, x]
+                if a0 > 0.99 or a0 < 0.01:
+                    kap[z, y, x] = 0.0
+                    continue
+                s = []
+                for a, (ox, oy, oz) in enumerate(off):
+                    okp = ct[z + oz, y + oy, x + ox] == I and gm[z + oz, y + oy, x + ox] > 1e-6
+                    okm = ct[z - oz, y - oy, x - ox] == I and gm[z - oz, y - oy, x - ox] > 1e-6
+                    s.append(d(okp, okm, n[a][z + oz, y + oy, x + ox], n[a][z, y, x], n[a][z - oz, y - oy, x - ox], a))
+                kap[z, y, x] = -1.0 * (s[0] + s[1] + s[2])
+    fs = [np.zeros(sh[k]) for k in "xyz"]
+
+    def valid(v):
+        return 1e-2 < v < 1 - 1e-2
+
+    for a, (ox, oy, oz) in enumerate(off):
+        for z in range(1 + oz, nz_ + 1):
+            for y in range(1 + oy, ny_ + 1):
+                for x in range(1 + ox, nx_ + 1):
+                    if not (ct[z, y, x] == I and ct[z - oz, y - oy, x - ox] == I):
+                        continue
+                    ap, am = alpha[z, y, x], alpha[z - oz, y - oy, x - ox]
+                    kp, km = kap[z, y, x], kap[z - oz, y - oy, x - ox]
+                    kf = 0.5 * (kp + km) if valid(ap) and valid(am) else kp if valid(ap) else km if valid(am) else 0.0
+                    fs[a][z, y, x] = sigma * kf * (ap - am) * ih[a]
+    return (*fs, *n, kap, gm)
+
+
+@pytest.mark.parametrize("spec", [
+    dict(N=(10, 9, 8), seed=3, kind="sphere"),
+    dict(N=(9, 8, 7), seed=5, kind="random", solid_fraction=0.15),
+])
+def test_surface_tension_oracle_equals_loop_restatement(oracle_lib, spec):
+    N, h, alpha, ct, sigma = W.surface_case(**spec)
+    got = oracle_lib.surface_tension(N, h, alpha, ct, sigma)
+    want = _surface_loops(N, h, alpha, ct, sigma)
+    for k, a, b in zip(("fsx", "fsy", "fsz", "nx", "ny", "nz", "kappa", "gm"), got, want):
+        assert np.array_equal(a, b), k
+
+
+def test_surface_tension_sphere_curvature_is_two_over_radius(oracle_lib):
+    """Known answer: on a resolved sphere the curvature -div n of the cells
+    well inside the interface band is 2/R (n points from the outside in, alpha
+    being 1 inside), within the discretisation error."""
+    n = 48
+    N, h = (n, n, n), (1.0 / 32,) * 3
+    ext = n * h[0]
+    centre, R = (0.5 * ext,) * 3, 0.3 * ext
+    alpha = np.ascontiguousarray(W.sphere_alpha(N, h, centre, R, 3.0))
+    ct = W.box_types(N)[0]
+    _, _, _, _, _, _, kappa, _ = oracle_lib.surface_tension(N, h, alpha, ct, 1.0)
+    band = (alpha > 0.3) & (alpha < 0.7)
+    k = kappa[band]
+    assert abs(np.median(k) - 2.0 / R) < 0.05 * (2.0 / R)
+
+
+SURFACE_GOLDEN = surface_golden_names()
+
+
+@pytest.mark.skipif(not SURFACE_GOLDEN, reason="no calc_surface_tension golden vectors")
+@pytest.mark.parametrize("name", SURFACE_GOLDEN)
+def test_surface_tension_oracle_matches_reference_golden(oracle_lib, name):
+    meta, arr = load_golden(name)
+    N, h, alpha, ct, sigma = surface_case_from_spec(meta)
+    got = oracle_lib.surface_tension(N, h, alpha, ct, sigma)
+    for k, a in zip(("fsx", "fsy", "fsz", "nx", "ny", "nz", "kappa", "gm"), got):
         assert np.array_equal(a, arr[k]), k
