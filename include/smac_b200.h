@@ -240,6 +240,34 @@ typedef struct {
   const double *vx, *vy, *vz;
 } smac_boundary_table;
 
+/* The fields the momentum predictor reads (G_StaggeredGrid members, device
+ * pointers in the reference layout; the marked ones may be NULL, read as 0). */
+typedef struct {
+  const uint8_t *fxt, *fyt, *fzt;           /* f_*type_ */
+  const uint8_t *fxbcid, *fybcid, *fzbcid;  /* f_*bcid_ */
+  const double *lamx, *lamy, *lamz;         /* f_ibm_area_solid_fraction_*_ (NULL: 0) */
+  const double *vx, *vy, *vz;               /* f_v*_: the velocity at time n */
+  const double *mfx, *mfy, *mfz;            /* f_mf*_: advecting face velocities */
+  const double *mux, *muy, *muz;            /* f_mu*_: face viscosities */
+  const double *mu, *rho_old, *p;           /* mu_, rho_old_, p_ (cells) */
+  const double *fbx, *fby, *fbz;            /* f_b*_: 1/rho on faces */
+  const double *impx, *impy, *impz;         /* f_coupling_impulse_*_ (NULL: 0) */
+  const double *sfx, *sfy, *sfz;            /* f_ibm_solid_fraction_*_ (NULL: 0) */
+} smac_momentum_fields;
+
+/* The momentum predictor, G_SMACSolver::get_vof_vstar_rhouu_consistent
+ * (CFD/G_SMACSolver.cu:1062-1070; k_get_vof_vstar_rhouu_consistent_{x,y,z}
+ * :90-1012, boundary rules CFD/G_BoundaryFunctions.h:9-367): on every
+ * F_INTERIOR face with indices 1..N+1,
+ *   u* = (1/rho)(rho_old u + impulse/V) + dt((1/rho)(div tau - div(mf u) - grad p) + g),
+ * times (1 - IBM solid fraction); tau the Newtonian stress with the cell and
+ * face viscosities, convection MUSCL with the minmod limiter, neighbours past
+ * a wall mirrored about it (slip and outlet walls copied).  Other faces of
+ * (vxs, vys, vzs) are not written.  Every grid extent must be >= 2. */
+smac_status smac_predict_vstar(const smac_grid_desc* d, const smac_boundary_table* bc, const smac_momentum_fields* mf,
+                               double dt, double gx, double gy, double gz, double* vxs, double* vys, double* vzs,
+                               void* stream);
+
 /* Wall-face u* before the projection, G_SMACSolver::update_vstar_boundary
  * (CFD/G_SMACSolver.cu:1044-1052, k_update_v*star_boundary,
  * CFD/G_BoundaryFunctions.cu:3-71, CFD/G_BoundaryFunctions.h:369-470), in

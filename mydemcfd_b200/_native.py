@@ -55,6 +55,14 @@ class BoundaryTable(ctypes.Structure):
                 ("vy", ctypes.c_void_p), ("vz", ctypes.c_void_p)]
 
 
+class MomentumFields(ctypes.Structure):
+    """smac_momentum_fields: the device arrays the momentum predictor reads."""
+    _fields_ = [(k, ctypes.c_void_p) for k in (
+        "fxt", "fyt", "fzt", "fxbcid", "fybcid", "fzbcid", "lamx", "lamy", "lamz", "vx", "vy", "vz",
+        "mfx", "mfy", "mfz", "mux", "muy", "muz", "mu", "rho_old", "p", "fbx", "fby", "fbz",
+        "impx", "impy", "impz", "sfx", "sfy", "sfz")]
+
+
 class SmacError(RuntimeError):
     def __init__(self, status, msg):
         super().__init__(f"{STATUS_NAMES.get(status, status)}: {msg}")
@@ -72,6 +80,7 @@ EXPORTS = [
     "smac_selftest_sweep", "smac_apply_A_dot_noalloc", "smac_async_create", "smac_async_submit",
     "smac_async_wait", "smac_async_destroy", "smac_update_boundary_faces", "smac_update_pressure_ghost",
     "smac_update_velocity_ghost", "smac_face_gradp", "smac_update_vstar_boundary", "smac_surface_tension",
+    "smac_predict_vstar",
 ]
 
 
@@ -117,6 +126,8 @@ def load(path: str = LIB_PATH):
                                        u8p, u8p, u8p, dp, dp, dp, dp, dp, dp, dp, dp, dp, dp, d, dp, dp, dp, vp],
         "smac_face_gradp": [ctypes.POINTER(GridDesc), dp, dp, dp, dp, vp],
         "smac_surface_tension": [ctypes.POINTER(GridDesc), dp, u8p, d, dp, dp, dp, dp, dp, dp, dp, dp, vp],
+        "smac_predict_vstar": [ctypes.POINTER(GridDesc), ctypes.POINTER(BoundaryTable), ctypes.POINTER(MomentumFields),
+                               d, d, d, d, dp, dp, dp, vp],
         "smac_update_vstar_boundary": [ctypes.POINTER(GridDesc), ctypes.POINTER(BoundaryTable), u8p, u8p, u8p, u8p,
                                        u8p, u8p, u8p, u8p, u8p, dp, dp, dp, dp, dp, dp, vp],
     }

@@ -1,6 +1,7 @@
-// smac_post.cu -- the calls either side of the projection: before it the wall
-// u* rule and the surface-tension force; after it the pressure in solid and
-// ghost cells, outlet and ghost velocities, and the face pressure gradient.
+// smac_post.cu -- the calls either side of the projection: before it the
+// momentum predictor u*, the wall u* rule and the surface-tension force;
+// after it the pressure in solid and ghost cells, outlet and ghost
+// velocities, and the face pressure gradient.
 //
 // The reference runs it as G_SMACSolver::update_boundary_ghost followed by
 // make_face_gradp (CFD/G_SMACSolver.cu:1144-1363, CFD/G_BoundaryFunctions.cu:
@@ -725,6 +726,220 @@ __global__ void __launch_bounds__(256) k_st_rim(StArgs A) {
   }
 }
 
+// ---------------------------------------------------------------------------
+// Momentum predictor u* (G_SMACSolver::get_vof_vstar_rhouu_consistent,
+// k_get_vof_vstar_rhouu_consistent_{x,y,z}, CFD/G_SMACSolver.cu:90-1070,
+// boundary rules CFD/G_BoundaryFunctions.h:9-367)
+
+struct MomArgs {
+  int N[3];
+  const uint8_t* ft[3];
+  const uint8_t* id[3];
+  const double* lam[3];  // nullptr: 0
+  const double* v[3];
+  const double* mf[3];
+  const double* muf[3];
+  const double* mu;
+  const double* rho_old;
+  const double* p;
+  const double* fb[3];
+  const double* imp[3];  // nullptr: 0
+  const double* sf[3];   // nullptr: 0
+  double* vs[3];
+  double dt, g[3], ih[3], ih2[3], inv_volume;
+  BcTable bc;
+};
+
+template <int F>
+__device__ __forceinline__ long long mface(const MomArgs& A, int x, int y, int z) {
+  const long long S0 = A.N[0] + 2 + (F == 0), S1 = A.N[1] + 2 + (F == 1);
+  return ((long long)z * S1 + y) * S0 + x;
+}
+__device__ __forceinline__ long long mcell(const MomArgs& A, int x, int y, int z) {
+  return ((long long)z * (A.N[1] + 2) + y) * (A.N[0] + 2) + x;
+}
+template <int AX>
+__device__ __forceinline__ void step(int& x, int& y, int& z, int s) {
+  if (AX == 0) x += s;
+  else if (AX == 1) y += s;
+  else z += s;
+}
+
+// d_get_v{B}_{B}face (G_BoundaryFunctions.h:9-98): family-B velocity at a
+// face, boundary faces by their type; the x rule passes the stored value
+// through for outlets only, the y and z rules for slip too.
+template <int B>
+__device__ __forceinline__ double m_face_val(const MomArgs& A, int x, int y, int z) {
+  const long long f = mface<B>(A, x, y, z);
+  const uint8_t t = A.ft[B][f];
+  if (t == 0) return A.v[B][f];  // F_INTERIOR
+  if (t == 1) {                  // F_BOUNDARY
+    const int bid = A.id[B][f];
+    const uint8_t bt = A.bc.type[bid];
+    if (bt == 2) return DMUL(DSUB(1.0, A.lam[B] ? A.lam[B][f] : 0.0), A.bc.bv[B][bid]);
+    if (bt == 0) return 0.0;
+    if (bt == 4 || (B != 0 && bt == 1)) return A.v[B][f];
+  }
+  return 0.0;
+}
+
+// d_get_v{AF}_{D}dir (G_BoundaryFunctions.h:100-367): family-AF velocity
+// next to face (x,y,z) along D != AF on side s, mirrored about a wall.
+template <int AF, int D>
+__device__ __forceinline__ double m_dir_val(const MomArgs& A, int x, int y, int z, int s) {
+  const double inside = A.v[AF][mface<AF>(A, x, y, z)];
+  int x2 = x, y2 = y, z2 = z;
+  step<D>(x2, y2, z2, s);
+  const long long f2 = mface<AF>(A, x2, y2, z2);
+  if (A.ft[AF][f2] == 0) return A.v[AF][f2];
+  int xf = x, yf = y, zf = z;
+  if (s > 0) step<D>(xf, yf, zf, 1);
+  int xg = xf, yg = yf, zg = zf;
+  step<AF>(xg, yg, zg, -1);
+  const long long ff = mface<D>(A, xf, yf, zf), fg = mface<D>(A, xg, yg, zg);
+  double wall = 0.0;
+  int count = 0;
+  if (A.ft[D][ff] == 1) {
+    wall = DADD(wall, A.bc.bv[AF][A.id[D][ff]]);
+    ++count;
+  }
+  if (A.ft[D][fg] == 1) {
+    wall = DADD(wall, A.bc.bv[AF][A.id[D][fg]]);
+    ++count;
+  }
+  if (count > 0) wall = __ddiv_rn(wall, (double)count);
+  const uint8_t bt = A.bc.type[A.id[D][ff]];
+  if (bt == 1 || bt == 4) return inside;
+  return DSUB(DMUL(2.0, wall), inside);
+}
+
+__device__ __forceinline__ double m_minmod(double dp, double dm) {
+  if (DMUL(dp, dm) > 0.0) return fabs(dp) < fabs(dm) ? dp : dm;
+  return 0.0;
+}
+
+// The two other axes of AF in ascending order, as compile-time values.
+template <int AF> struct Others { static constexpr int D0 = AF == 0 ? 1 : 0, D1 = AF == 2 ? 1 : 2; };
+
+// Viscous cross term of axis D: (tau_D+ - tau_D-) / h_D.
+template <int AF, int D>
+__device__ __forceinline__ double m_cross(const MomArgs& A, int x, int y, int z, double v0) {
+  int xd = x, yd = y, zd = z;
+  step<D>(xd, yd, zd, 1);
+  int xda = xd, yda = yd, zda = zd;
+  step<AF>(xda, yda, zda, -1);
+  int xm = x, ym = y, zm = z;
+  step<AF>(xm, ym, zm, -1);
+  const double wp0 = m_face_val<D>(A, xd, yd, zd), wpm = m_face_val<D>(A, xda, yda, zda);
+  const double w0 = m_face_val<D>(A, x, y, z), wm = m_face_val<D>(A, xm, ym, zm);
+  const double vdp = m_dir_val<AF, D>(A, x, y, z, +1), vdm = m_dir_val<AF, D>(A, x, y, z, -1);
+  const double mup = DMUL(0.5, DADD(A.muf[D][mface<D>(A, xd, yd, zd)], A.muf[D][mface<D>(A, xda, yda, zda)]));
+  const double tp = DMUL(mup, DADD(DMUL(DSUB(wp0, wpm), A.ih[AF]), DMUL(DSUB(vdp, v0), A.ih[D])));
+  const double mum = DMUL(0.5, DADD(A.muf[D][mface<D>(A, x, y, z)], A.muf[D][mface<D>(A, xm, ym, zm)]));
+  const double tm = DMUL(mum, DADD(DMUL(DSUB(w0, wm), A.ih[AF]), DMUL(DSUB(v0, vdm), A.ih[D])));
+  return DMUL(DSUB(tp, tm), A.ih[D]);
+}
+
+// Neighbour of family-AF face (x,y,z) along D on side s: the face rule along
+// AF itself, the mirrored rule across.
+template <int AF, int D>
+__device__ __forceinline__ double m_neigh(const MomArgs& A, int x, int y, int z, int s) {
+  if (D == AF) {
+    int xs = x, ys = y, zs = z;
+    step<AF>(xs, ys, zs, s);
+    return m_face_val<AF>(A, xs, ys, zs);
+  }
+  return m_dir_val<AF, D == AF ? Others<AF>::D0 : D>(A, x, y, z, s);
+}
+
+// MUSCL (minmod) value at the upwind face (x,y,z) for a flux through a
+// D-side of the control volume; upwind_v itself where the face has no
+// stencil (not F_INTERIOR).
+template <int AF, int D>
+__device__ __forceinline__ double m_recon(const MomArgs& A, double flux, int x, int y, int z, double upwind_v) {
+  const long long f = mface<AF>(A, x, y, z);
+  if (A.ft[AF][f] != 0) return upwind_v;
+  const double vu = A.v[AF][f];
+  const double su = m_minmod(DSUB(m_neigh<AF, D>(A, x, y, z, +1), vu), DSUB(vu, m_neigh<AF, D>(A, x, y, z, -1)));
+  const double dir = flux < 0.0 ? -1.0 : 1.0;
+  return DADD(upwind_v, DMUL(DMUL(dir, 0.5), su));
+}
+
+// Convection through the two D-sides, (M+ - M-) / h_D.
+template <int AF, int D>
+__device__ __forceinline__ double m_conv(const MomArgs& A, int x, int y, int z, double v0, double nplus,
+                                         double nminus) {
+  int xm = x, ym = y, zm = z;
+  step<AF>(xm, ym, zm, -1);
+  double fp, fm;
+  if (D == AF) {
+    int xp = x, yp = y, zp = z;
+    step<AF>(xp, yp, zp, 1);
+    fp = DMUL(0.5, DADD(A.mf[AF][mface<AF>(A, x, y, z)], A.mf[AF][mface<AF>(A, xp, yp, zp)]));
+    fm = DMUL(0.5, DADD(A.mf[AF][mface<AF>(A, xm, ym, zm)], A.mf[AF][mface<AF>(A, x, y, z)]));
+  } else {
+    int xd = x, yd = y, zd = z;
+    step<D>(xd, yd, zd, 1);
+    int xda = xd, yda = yd, zda = zd;
+    step<AF>(xda, yda, zda, -1);
+    fp = DMUL(0.5, DADD(A.mf[D][mface<D>(A, xda, yda, zda)], A.mf[D][mface<D>(A, xd, yd, zd)]));
+    fm = DMUL(0.5, DADD(A.mf[D][mface<D>(A, x, y, z)], A.mf[D][mface<D>(A, xm, ym, zm)]));
+  }
+  int xu = x, yu = y, zu = z;
+  if (!(fp > 0.0)) step<D>(xu, yu, zu, 1);
+  const double up = m_recon<AF, D>(A, fp, xu, yu, zu, fp > 0.0 ? v0 : nplus);
+  int xv = x, yv = y, zv = z;
+  if (fm > 0.0) step<D>(xv, yv, zv, -1);
+  const double um = m_recon<AF, D>(A, fm, xv, yv, zv, fm > 0.0 ? nminus : v0);
+  return DMUL(DSUB(DMUL(fp, up), DMUL(fm, um)), A.ih[D]);
+}
+
+template <int AF>
+__device__ __forceinline__ double m_vstar(const MomArgs& A, int x, int y, int z) {
+  constexpr int D0 = Others<AF>::D0, D1 = Others<AF>::D1;
+  const long long f = mface<AF>(A, x, y, z);
+  const double v0 = A.v[AF][f];
+  int xm = x, ym = y, zm = z;
+  step<AF>(xm, ym, zm, -1);
+  const double vp = m_neigh<AF, AF>(A, x, y, z, +1), vm = m_neigh<AF, AF>(A, x, y, z, -1);
+  // viscous: the own axis, then the other two in axis order
+  const double tau_p = DMUL(A.mu[mcell(A, x, y, z)], DSUB(vp, v0));
+  const double tau_m = DMUL(A.mu[mcell(A, xm, ym, zm)], DSUB(v0, vm));
+  double tmp = DMUL(DMUL(2.0, DSUB(tau_p, tau_m)), A.ih2[AF]);
+  tmp = DADD(tmp, m_cross<AF, D0>(A, x, y, z, v0));
+  tmp = DADD(tmp, m_cross<AF, D1>(A, x, y, z, v0));
+  // convection in axis order
+  tmp = DSUB(tmp, m_conv<AF, 0>(A, x, y, z, v0, m_neigh<AF, 0>(A, x, y, z, +1), m_neigh<AF, 0>(A, x, y, z, -1)));
+  tmp = DSUB(tmp, m_conv<AF, 1>(A, x, y, z, v0, m_neigh<AF, 1>(A, x, y, z, +1), m_neigh<AF, 1>(A, x, y, z, -1)));
+  tmp = DSUB(tmp, m_conv<AF, 2>(A, x, y, z, v0, m_neigh<AF, 2>(A, x, y, z, +1), m_neigh<AF, 2>(A, x, y, z, -1)));
+  const double inv_rho = A.fb[AF][f];
+  const double rho_old_f = DMUL(0.5, DADD(A.rho_old[mcell(A, x, y, z)], A.rho_old[mcell(A, xm, ym, zm)]));
+  tmp = DSUB(tmp, DMUL(DSUB(A.p[mcell(A, x, y, z)], A.p[mcell(A, xm, ym, zm)]), A.ih[AF]));
+  const double coupling = DMUL(A.imp[AF] ? A.imp[AF][f] : 0.0, A.inv_volume);
+  const double vs = DADD(DMUL(inv_rho, DADD(DMUL(v0, rho_old_f), coupling)),
+                         DMUL(A.dt, DADD(DMUL(inv_rho, tmp), A.g[AF])));
+  return DMUL(DSUB(1.0, A.sf[AF] ? A.sf[AF][f] : 0.0), vs);
+}
+
+// One thread per face index (x, y) of plane z of the box 1..N+1; blockIdx.z
+// runs over the three families' planes.  Only F_INTERIOR faces are written.
+__global__ void __launch_bounds__(256) k_predict_vstar(MomArgs A) {
+  const int fam = blockIdx.z / (A.N[2] + 1);
+  const int z = blockIdx.z % (A.N[2] + 1) + 1;
+  const int x = blockIdx.x * 32 + threadIdx.x + 1, y = blockIdx.y * 8 + threadIdx.y + 1;
+  if (x > A.N[0] + 1 || y > A.N[1] + 1) return;
+  if (fam == 0) {
+    const long long f = mface<0>(A, x, y, z);
+    if (A.ft[0][f] == 0) A.vs[0][f] = m_vstar<0>(A, x, y, z);
+  } else if (fam == 1) {
+    const long long f = mface<1>(A, x, y, z);
+    if (A.ft[1][f] == 0) A.vs[1][f] = m_vstar<1>(A, x, y, z);
+  } else {
+    const long long f = mface<2>(A, x, y, z);
+    if (A.ft[2][f] == 0) A.vs[2][f] = m_vstar<2>(A, x, y, z);
+  }
+}
+
 int sm_count() {
   static int n = 0;
   if (!n) {
@@ -922,6 +1137,53 @@ smac_status smac_surface_tension(const smac_grid_desc* d, const double* alpha, c
   k_st_rim<<<dim3(64, 9), 256, 0, s>>>(A);
   k_st_normal<<<dim3(bx, by, (unsigned)d->nz), dim3(32, 8), 0, s>>>(A);
   k_st_force<<<dim3(bx, by, (unsigned)d->nz), dim3(ST_TX, ST_TY), 0, s>>>(A);
+  return launch_status(fn);
+}
+
+smac_status smac_predict_vstar(const smac_grid_desc* d, const smac_boundary_table* bc, const smac_momentum_fields* mf,
+                               double dt, double gx, double gy, double gz, double* vxs, double* vys, double* vzs,
+                               void* stream) {
+  static const char* fn = "smac_predict_vstar";
+  if (!d || !bc || !mf || !vxs || !vys || !vzs) {
+    smac::set_error_text("%s: null argument", fn);
+    return SMAC_BAD_ARG;
+  }
+  const void* need[] = {mf->fxt, mf->fyt, mf->fzt, mf->fxbcid, mf->fybcid, mf->fzbcid, mf->vx, mf->vy, mf->vz,
+                        mf->mfx, mf->mfy, mf->mfz, mf->mux, mf->muy, mf->muz, mf->mu, mf->rho_old, mf->p,
+                        mf->fbx, mf->fby, mf->fbz};
+  for (const void* q : need)
+    if (!q) {
+      smac::set_error_text("%s: a required field is null", fn);
+      return SMAC_BAD_ARG;
+    }
+  if (bad_table(bc, fn)) return SMAC_BAD_ARG;
+  // the mirrored neighbours read two faces inside across every axis
+  if (bad_desc(d, fn, 2)) return SMAC_BAD_SHAPE;
+  MomArgs A;
+  std::memset(&A, 0, sizeof(A));
+  A.N[0] = d->nx; A.N[1] = d->ny; A.N[2] = d->nz;
+  A.ft[0] = mf->fxt; A.ft[1] = mf->fyt; A.ft[2] = mf->fzt;
+  A.id[0] = mf->fxbcid; A.id[1] = mf->fybcid; A.id[2] = mf->fzbcid;
+  A.lam[0] = mf->lamx; A.lam[1] = mf->lamy; A.lam[2] = mf->lamz;
+  A.v[0] = mf->vx; A.v[1] = mf->vy; A.v[2] = mf->vz;
+  A.mf[0] = mf->mfx; A.mf[1] = mf->mfy; A.mf[2] = mf->mfz;
+  A.muf[0] = mf->mux; A.muf[1] = mf->muy; A.muf[2] = mf->muz;
+  A.mu = mf->mu; A.rho_old = mf->rho_old; A.p = mf->p;
+  A.fb[0] = mf->fbx; A.fb[1] = mf->fby; A.fb[2] = mf->fbz;
+  A.imp[0] = mf->impx; A.imp[1] = mf->impy; A.imp[2] = mf->impz;
+  A.sf[0] = mf->sfx; A.sf[1] = mf->sfy; A.sf[2] = mf->sfz;
+  A.vs[0] = vxs; A.vs[1] = vys; A.vs[2] = vzs;
+  A.dt = dt;
+  A.g[0] = gx; A.g[1] = gy; A.g[2] = gz;
+  const double h[3] = {d->dx, d->dy, d->dz};
+  for (int k = 0; k < 3; ++k) {
+    A.ih[k] = 1. / h[k];
+    A.ih2[k] = 1. / (h[k] * h[k]);
+  }
+  A.inv_volume = A.ih[0] * A.ih[1] * A.ih[2];
+  fill_table(&A.bc, bc);
+  const dim3 grid((unsigned)((d->nx + 1 + 31) / 32), (unsigned)((d->ny + 1 + 7) / 8), 3u * (unsigned)(d->nz + 1));
+  k_predict_vstar<<<grid, dim3(32, 8), 0, (cudaStream_t)stream>>>(A);
   return launch_status(fn);
 }
 

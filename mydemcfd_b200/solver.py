@@ -476,6 +476,23 @@ def surface_tension_device(N, h, alpha, ct, sigma, work, fs):
                                               *map(_ptr, work), *map(_ptr, fs), ctypes.c_void_p(s)))
 
 
+def predict_vstar_device(N, h, bc: BoundaryConditions, fields: dict, dt, g, vs):
+    """smac_predict_vstar: u* of every F_INTERIOR face into vs = (vxs, vys,
+    vzs).  fields maps the smac_momentum_fields names (fxt .. sfz) to CUDA
+    tensors; lam*/imp*/sf* may be missing (0)."""
+    d = nat.GridDesc(*N, *h)
+    s = torch.cuda.current_stream().cuda_stream
+    table, keep = bc.table()
+    mf = nat.MomentumFields()
+    for name, _ in nat.MomentumFields._fields_:
+        t = fields.get(name)
+        setattr(mf, name, None if t is None else _ptr(t).value)
+    dd = ctypes.c_double
+    nat.check(nat.load().smac_predict_vstar(ctypes.byref(d), ctypes.byref(table), ctypes.byref(mf), dd(dt), dd(g[0]),
+                                            dd(g[1]), dd(g[2]), *map(_ptr, vs), ctypes.c_void_p(s)))
+    del keep
+
+
 def face_gradp_device(N, h, p, gp):
     """smac_face_gradp: gp = (gpx, gpy, gpz) face tensors, faces 1..N+1 written."""
     d = nat.GridDesc(*N, *h)

@@ -403,3 +403,69 @@ def surface_case(N, seed, kind="sphere", solid_fraction=0.0, sigma=0.07, h=0.031
         sf = np.where(inner & (w < solid_fraction), 1.0, 0.0)
         set_solid_cells(sf, ct, fxt, fyt, fzt)
     return N, hh, np.ascontiguousarray(alpha), ct, float(sigma)
+
+
+@dataclass
+class MomentumCase:
+    """Inputs of the momentum predictor u* (get_vof_vstar_rhouu_consistent),
+    reference layout; lam / imp / sf may be None (zero)."""
+    N: tuple
+    h: tuple
+    dt: float
+    g: tuple
+    bc_type: np.ndarray
+    bc_v: tuple
+    ct: np.ndarray
+    ft: tuple
+    bcid: tuple
+    lam: tuple
+    v: tuple       # f_v*_ at time n
+    mf: tuple      # f_mf*_: advecting face velocities
+    muf: tuple     # f_mu*_: face viscosities
+    mu: np.ndarray
+    rho_old: np.ndarray
+    p: np.ndarray
+    fb: tuple      # f_b*: 1/rho on faces
+    imp: tuple     # f_coupling_impulse_*
+    sf: tuple      # f_ibm_solid_fraction_*
+    vs: tuple      # f_v*_star_ before the call (faces it does not write keep these)
+
+
+def momentum_case(N, seed, sides=("x+", "z-"), solid_fraction=0.0, extras=True, dt=0.01, g=(0.0, 0.0, -9.8)):
+    """Seeded momentum-predictor inputs on the boundary set-up of post_case
+    (all five boundary types, outlets on `sides`, clustered solids).  Fields:
+    v, v* U[-1,1); mf U[-1,1) with 10% exact zeros (the flux-sign ties);
+    face and cell viscosities U[1e-3, 1e-2); rho_old U[1, 1000); p U[-1,1);
+    f_b U[1e-3, 1); with extras the coupling impulse U[-1e-6, 1e-6), the IBM
+    area and solid fractions U[0,1) with half of them 0."""
+    base = post_case(N, seed, h=(0.03125, 0.03125, 0.03125), dt=dt, g=g, sides=sides, solid_fraction=solid_fraction,
+                     lam=extras, solid_margin=3)
+    sh = shapes(base.N)
+
+    def rnd(tag, key, lo=-1.0, hi=1.0):
+        n = int(np.prod(sh[key]))
+        return np.ascontiguousarray((lo + (hi - lo) * uniform01(substream(seed, tag), n)).reshape(sh[key]))
+
+    def half_zero(a, tag):
+        return np.where(uniform01(substream(seed, tag), a.size).reshape(a.shape) < 0.5, 0.0, a)
+
+    def extra(t0, lo, hi):
+        if not extras:
+            return None
+        return tuple(np.ascontiguousarray(half_zero(rnd(t0 + k, key, lo, hi), t0 + 10 + k))
+                     for k, key in enumerate("xyz"))
+
+    mf = []
+    for k, key in enumerate("xyz"):
+        a = rnd(100 + k, key)
+        a[uniform01(substream(seed, 110 + k), a.size).reshape(a.shape) < 0.1] = 0.0
+        mf.append(a)
+    return MomentumCase(
+        N=base.N, h=base.h, dt=base.dt, g=base.g, bc_type=base.bc_type, bc_v=base.bc_v, ct=base.ct, ft=base.ft,
+        bcid=base.bcid, lam=base.lam,
+        v=tuple(rnd(120 + k, key) for k, key in enumerate("xyz")), mf=tuple(mf),
+        muf=tuple(rnd(130 + k, key, 1e-3, 1e-2) for k, key in enumerate("xyz")),
+        mu=rnd(140, "cell", 1e-3, 1e-2), rho_old=rnd(141, "cell", 1.0, 1000.0), p=rnd(142, "cell"),
+        fb=tuple(rnd(150 + k, key, 1e-3, 1.0) for k, key in enumerate("xyz")),
+        imp=extra(160, -1e-6, 1e-6), sf=extra(180, 0.0, 1.0),
+        vs=tuple(rnd(200 + k, key) for k, key in enumerate("xyz")))

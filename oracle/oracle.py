@@ -232,6 +232,40 @@ def surface_tension(N, h, alpha, ct, sigma, nx=None, ny=None, nz=None, kappa=Non
     return (*fs, *work)
 
 
+def predict_vstar(m):
+    """G_SMACSolver::get_vof_vstar_rhouu_consistent (CFD/G_SMACSolver.cu:90-1070)
+    on a workloads.MomentumCase: returns (vxs, vys, vzs), copies of m.vs with
+    every F_INTERIOR face predicted."""
+    vs = [np.array(a, dtype=np.float64, order="C", copy=True) for a in m.vs]
+    keep = []
+
+    def arr3(arrs, dtype):
+        if arrs is None:
+            return (ctypes.c_void_p * 3)(None, None, None)
+        out = []
+        for a in arrs:
+            a = np.ascontiguousarray(a, dtype)
+            keep.append(a)
+            out.append(a.ctypes.data)
+        return (ctypes.c_void_p * 3)(*out)
+
+    def one(a):
+        a = np.ascontiguousarray(a, np.float64)
+        keep.append(a)
+        return _p(a)
+
+    c = ctypes.c_double
+    bct = np.ascontiguousarray(m.bc_type, np.uint8)
+    bv = [np.ascontiguousarray(a, np.float64) for a in m.bc_v]
+    vsp = (ctypes.c_void_p * 3)(*(a.ctypes.data for a in vs))
+    lib().orc_predict_vstar(*m.N, c(m.h[0]), c(m.h[1]), c(m.h[2]), c(m.dt), c(m.g[0]), c(m.g[1]), c(m.g[2]),
+                            _u8(bct), *(_p(a) for a in bv), arr3(m.ft, np.uint8), arr3(m.bcid, np.uint8),
+                            arr3(m.lam, np.float64), arr3(m.v, np.float64), arr3(m.mf, np.float64),
+                            arr3(m.muf, np.float64), one(m.mu), one(m.rho_old), one(m.p), arr3(m.fb, np.float64),
+                            arr3(m.imp, np.float64), arr3(m.sf, np.float64), vsp)
+    return tuple(vs)
+
+
 def post_pass(case):
     """G_SMACSolver::update_boundary_ghost then make_face_gradp
     (CFD/G_SMACSolver.cu:1277-1363) on a workloads.PostCase: returns

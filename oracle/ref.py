@@ -253,3 +253,52 @@ def surface_tension(N, h, alpha, ct, sigma):
     if rc != 0:
         raise RuntimeError(f"ref_surface_tension returned {rc}")
     return (*fs, *work, io.ms)
+
+
+class RefMomIO(ctypes.Structure):
+    _fields_ = [("Nx", ctypes.c_int), ("Ny", ctypes.c_int), ("Nz", ctypes.c_int)] + \
+        [(k, ctypes.c_double) for k in ("Lx", "Ly", "Lz", "dt", "gx", "gy", "gz")] + \
+        [("num_ids", ctypes.c_int), ("bc_type", _u8p), ("bc_vx", _dp), ("bc_vy", _dp), ("bc_vz", _dp)] + \
+        [(k, ctypes.c_void_p * 3) for k in ("ft", "bcid", "lam", "v", "mf", "muf", "fb", "imp", "sf")] + \
+        [("mu", _dp), ("rho_old", _dp), ("p", _dp), ("vs", ctypes.c_void_p * 3), ("ms", ctypes.c_double)]
+
+
+def predict_vstar(m):
+    """Run the reference's get_vof_vstar_rhouu_consistent on a
+    mydemcfd_b200.workloads.MomentumCase (None fields as zeros): returns
+    (vxs, vys, vzs, ms)."""
+    L = lib()
+    if not hasattr(L, "_mom_set"):
+        L.ref_predict_vstar.restype = ctypes.c_int
+        L.ref_predict_vstar.argtypes = [ctypes.POINTER(RefMomIO)]
+        L._mom_set = True
+    keep = []
+
+    def arr(a, dtype=np.float64):
+        a = np.ascontiguousarray(a, dtype)
+        keep.append(a)
+        return a
+
+    def three(arrs, dtype=np.float64, like=None):
+        if arrs is None:
+            arrs = tuple(np.zeros(x.shape) for x in like)
+        return (ctypes.c_void_p * 3)(*(arr(a, dtype).ctypes.data for a in arrs))
+
+    io = RefMomIO()
+    io.Nx, io.Ny, io.Nz = m.N
+    io.Lx, io.Ly, io.Lz = (n * hh for n, hh in zip(m.N, m.h))
+    io.dt = m.dt
+    io.gx, io.gy, io.gz = m.g
+    io.num_ids = len(m.bc_type)
+    io.bc_type = _p(arr(m.bc_type, np.uint8), ctypes.c_uint8)
+    io.bc_vx, io.bc_vy, io.bc_vz = (_p(arr(a)) for a in m.bc_v)
+    io.ft, io.bcid = three(m.ft, np.uint8), three(m.bcid, np.uint8)
+    io.lam, io.imp, io.sf = three(m.lam, like=m.v), three(m.imp, like=m.v), three(m.sf, like=m.v)
+    io.v, io.mf, io.muf, io.fb = three(m.v), three(m.mf), three(m.muf), three(m.fb)
+    io.mu, io.rho_old, io.p = _p(arr(m.mu)), _p(arr(m.rho_old)), _p(arr(m.p))
+    out = [np.array(a, dtype=np.float64, order="C", copy=True) for a in m.vs]
+    io.vs = (ctypes.c_void_p * 3)(*(a.ctypes.data for a in out))
+    rc = L.ref_predict_vstar(ctypes.byref(io))
+    if rc != 0:
+        raise RuntimeError(f"ref_predict_vstar returned {rc}")
+    return (*out, io.ms)

@@ -8,9 +8,10 @@
 // SMACSolver with calloc'ed members, G_SMACSolver::solver_malloc + cpuTogpu,
 // G_PCGSolver + G_GMGSolver::initialize, set_solver, tol_, then
 // G_SMACSolver::solve_poisson() and correct_vof_velocity().  More entries
-// run the calls either side of it on given arrays: ref_vstar
-// (update_vstar_boundary), ref_surface_tension (calc_surface_tension) and
-// ref_post (update_boundary_ghost and make_face_gradp).
+// run the calls either side of it on given arrays: ref_predict_vstar
+// (get_vof_vstar_rhouu_consistent), ref_vstar (update_vstar_boundary),
+// ref_surface_tension (calc_surface_tension) and ref_post
+// (update_boundary_ghost and make_face_gradp).
 //
 // Two things the reference leaves to chance are pinned here: every multigrid
 // level array is zeroed after G_GMGSolver::initialize (the reference reads
@@ -357,6 +358,79 @@ int ref_surface_tension(ref_st_io* io) {
     g.gpuTocpu(solv.grid_);
     get(hg.nx_, io->nx); get(hg.ny_, io->ny); get(hg.nz_, io->nz); get(hg.kappa_, io->kappa); get(hg.p_tmp_, io->gm);
     get(hg.f_sx_, io->fsx); get(hg.f_sy_, io->fsy); get(hg.f_sz_, io->fsz);
+    e = cudaGetLastError();
+  }
+  g.solver_free();
+  solv.solver_free();
+  return e == cudaSuccess ? 0 : -2;
+}
+
+struct ref_mom_io {
+  int Nx, Ny, Nz;
+  double Lx, Ly, Lz, dt, gx, gy, gz;
+  int num_ids;
+  const uint8_t* bc_type;
+  const double *bc_vx, *bc_vy, *bc_vz;
+  const uint8_t *ft[3], *bcid[3];
+  const double *lam[3], *v[3], *mf[3], *muf[3], *fb[3], *imp[3], *sf[3];
+  const double *mu, *rho_old, *p;
+  double* vs[3];  // in: u* before the call; out: after it
+  double ms;      // out: device time
+};
+
+// G_SMACSolver::get_vof_vstar_rhouu_consistent (CFD/G_SMACSolver.cu:1062-1070)
+// on host arrays.  Returns 0 on success, -2 on a CUDA error.
+int ref_predict_vstar(ref_mom_io* io) {
+  const int Nx = io->Nx, Ny = io->Ny, Nz = io->Nz;
+  SMACSolver solv;
+  solv.set_calc_properties(0., 0., 0., io->Lx, io->Ly, io->Lz, Nx, Ny, Nz);
+  solv.grid_.bc_.num_boundary_id_ = io->num_ids;
+  solv.solver_malloc();
+  solv.dt_ = io->dt;
+  solv.inv_dt_ = 1. / io->dt;
+  solv.gx_ = io->gx; solv.gy_ = io->gy; solv.gz_ = io->gz;
+  StaggeredGrid& hg = solv.grid_;
+  put(hg.f_xtype_, io->ft[0]); put(hg.f_ytype_, io->ft[1]); put(hg.f_ztype_, io->ft[2]);
+  put(hg.f_xbcid_, io->bcid[0]); put(hg.f_ybcid_, io->bcid[1]); put(hg.f_zbcid_, io->bcid[2]);
+  put(hg.f_ibm_area_solid_fraction_x_, io->lam[0]); put(hg.f_ibm_area_solid_fraction_y_, io->lam[1]);
+  put(hg.f_ibm_area_solid_fraction_z_, io->lam[2]);
+  put(hg.f_vx_, io->v[0]); put(hg.f_vy_, io->v[1]); put(hg.f_vz_, io->v[2]);
+  put(hg.f_mfx_, io->mf[0]); put(hg.f_mfy_, io->mf[1]); put(hg.f_mfz_, io->mf[2]);
+  put(hg.f_mux_, io->muf[0]); put(hg.f_muy_, io->muf[1]); put(hg.f_muz_, io->muf[2]);
+  put(hg.f_bx_, io->fb[0]); put(hg.f_by_, io->fb[1]); put(hg.f_bz_, io->fb[2]);
+  put(hg.f_coupling_impulse_x_, io->imp[0]); put(hg.f_coupling_impulse_y_, io->imp[1]);
+  put(hg.f_coupling_impulse_z_, io->imp[2]);
+  put(hg.f_ibm_solid_fraction_x_, io->sf[0]); put(hg.f_ibm_solid_fraction_y_, io->sf[1]);
+  put(hg.f_ibm_solid_fraction_z_, io->sf[2]);
+  put(hg.mu_, io->mu); put(hg.rho_old_, io->rho_old); put(hg.p_, io->p);
+  put(hg.f_vx_star_, io->vs[0]); put(hg.f_vy_star_, io->vs[1]); put(hg.f_vz_star_, io->vs[2]);
+  std::memcpy(hg.bc_.bcType_.data_, io->bc_type, (size_t)io->num_ids);
+  std::memcpy(hg.bc_.vx_.data_, io->bc_vx, sizeof(double) * (size_t)io->num_ids);
+  std::memcpy(hg.bc_.vy_.data_, io->bc_vy, sizeof(double) * (size_t)io->num_ids);
+  std::memcpy(hg.bc_.vz_.data_, io->bc_vz, sizeof(double) * (size_t)io->num_ids);
+  G_SMACSolver g;
+  g.set_calc_properties(0., 0., 0., io->Lx, io->Ly, io->Lz, Nx, Ny, Nz);
+  g.grid_.bc_.num_boundary_id_ = io->num_ids;
+  g.solver_malloc();
+  g.cpuTogpu(solv.grid_);
+  g.set_block_grid(Nx, Ny, Nz);
+  g.dt_ = io->dt;
+  g.inv_dt_ = 1. / io->dt;
+  cudaDeviceSynchronize();
+  cudaEvent_t ev[2];
+  for (auto& x : ev) cudaEventCreate(&x);
+  cudaEventRecord(ev[0], 0);
+  g.get_vof_vstar_rhouu_consistent(solv);
+  cudaEventRecord(ev[1], 0);
+  cudaDeviceSynchronize();
+  float t = 0.f;
+  cudaEventElapsedTime(&t, ev[0], ev[1]);
+  io->ms = t;
+  for (auto& x : ev) cudaEventDestroy(x);
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) {
+    g.gpuTocpu(solv.grid_);
+    get(hg.f_vx_star_, io->vs[0]); get(hg.f_vy_star_, io->vs[1]); get(hg.f_vz_star_, io->vs[2]);
     e = cudaGetLastError();
   }
   g.solver_free();

@@ -939,6 +939,205 @@ void orc_surface_tension(int Nx, int Ny, int Nz, double dx, double dy, double dz
       }
 }
 
+}  // extern "C"
+
+namespace {
+
+// The fields of the momentum predictor, per family a = x, y, z where a field
+// lives on faces.  Cells are (Nx+2)(Ny+2)(Nz+2), family-a faces have one
+// more entry along a.
+struct MomFields {
+  int N[3];
+  const uint8_t* bct;      // boundary types per id
+  const double* bv[3];     // boundary velocity components per id
+  const uint8_t* ft[3];    // face types
+  const uint8_t* id[3];    // boundary ids
+  const double* lam[3];    // IBM area fractions (nullptr: 0)
+  const double* v[3];      // velocity at time n
+  const double* mf[3];     // advecting face velocities
+  const double* muf[3];    // face viscosities
+  const double* mu;        // cell viscosity
+  const double* rho_old;   // cell density at time n
+  const double* p;         // cell pressure
+  const double* fb[3];     // 1/rho on faces
+  const double* imp[3];    // coupling impulse (nullptr: 0)
+  const double* sf[3];     // IBM solid fraction of the face (nullptr: 0)
+};
+
+struct Idx3 {
+  int i[3];
+};
+
+inline size_t face_off(const MomFields& F, int a, const Idx3& q) {
+  const size_t S0 = F.N[0] + 2 + (a == 0), S1 = F.N[1] + 2 + (a == 1);
+  return ((size_t)q.i[2] * S1 + q.i[1]) * S0 + q.i[0];
+}
+inline size_t cell_off(const MomFields& F, const Idx3& q) {
+  return ((size_t)q.i[2] * (F.N[1] + 2) + q.i[1]) * (F.N[0] + 2) + q.i[0];
+}
+inline Idx3 shifted(Idx3 q, int axis, int s) {
+  q.i[axis] += s;
+  return q;
+}
+
+// d_get_v{b}_{b}face (CFD/G_BoundaryFunctions.h:9-98): velocity of family b
+// at face q, boundary faces by their type.  The x-face rule passes the
+// stored value through for outlets only, the y and z rules also for slip.
+double face_val(const MomFields& F, int b, const Idx3& q) {
+  const size_t f = face_off(F, b, q);
+  const uint8_t t = F.ft[b][f];
+  if (t == F_INTERIOR) return F.v[b][f];
+  if (t == F_BOUNDARY) {
+    const int bid = F.id[b][f];
+    const uint8_t bt = F.bct[bid];
+    if (bt == 2) return (1. - (F.lam[b] ? F.lam[b][f] : 0.)) * F.bv[b][bid];  // BC_INFLOW
+    if (bt == 0) return 0.;                                                  // BC_NOSLIP
+    if (bt == 4 || (b != 0 && bt == 1)) return F.v[b][f];                    // BC_OUTLET (and BC_SLIP for y, z)
+  }
+  return 0.;
+}
+
+// d_get_v{a}_{d}dir (CFD/G_BoundaryFunctions.h:100-367): velocity of family
+// a next to face q along axis d != a on side s; a non-interior neighbour is
+// mirrored about the wall (the mean velocity of the one or two family-d
+// boundary faces there), or copied for slip and outlet walls.
+double dir_val(const MomFields& F, int a, int d, const Idx3& q, int s) {
+  const double inside = F.v[a][face_off(F, a, q)];
+  const Idx3 q2 = shifted(q, d, s);
+  if (F.ft[a][face_off(F, a, q2)] == F_INTERIOR) return F.v[a][face_off(F, a, q2)];
+  const Idx3 qf = s > 0 ? shifted(q, d, 1) : q;
+  const Idx3 qg = shifted(qf, a, -1);
+  double wall = 0.;
+  int count = 0;
+  const size_t ff = face_off(F, d, qf), fg = face_off(F, d, qg);
+  if (F.ft[d][ff] == F_BOUNDARY) {
+    wall += F.bv[a][F.id[d][ff]];
+    count++;
+  }
+  if (F.ft[d][fg] == F_BOUNDARY) {
+    wall += F.bv[a][F.id[d][fg]];
+    count++;
+  }
+  if (count > 0) wall /= (double)count;
+  const uint8_t bt = F.bct[F.id[d][ff]];
+  if (bt == 1 || bt == 4) return inside;  // BC_SLIP, BC_OUTLET
+  return 2.0 * wall - inside;
+}
+
+double minmod(double dp, double dm) {  // d_minmod, CFD/G_SMACSolver.cu:67-88
+  if (dp * dm > 0.) return std::fabs(dp) < std::fabs(dm) ? dp : dm;
+  return 0.;
+}
+double sgn1(double x) { return x < 0 ? -1. : 1.; }  // sgn, CFD/G_SMACSolver.h:130-139
+
+// u* of the F_INTERIOR face q of family a: k_get_vof_vstar_rhouu_consistent_{x,y,z}
+// (CFD/G_SMACSolver.cu:90-1012) with the family's axis as a parameter.
+double vstar_face(const MomFields& F, int a, const Idx3& q, const double ih[3], const double ih2[3], double dt,
+                  double g) {
+  const double v0 = F.v[a][face_off(F, a, q)];
+  const double vp = face_val(F, a, shifted(q, a, 1)), vm = face_val(F, a, shifted(q, a, -1));
+  double vdp[3] = {0, 0, 0}, vdm[3] = {0, 0, 0};
+  for (int d = 0; d < 3; ++d)
+    if (d != a) {
+      vdp[d] = dir_val(F, a, d, q, +1);
+      vdm[d] = dir_val(F, a, d, q, -1);
+    }
+  // viscous: the own axis, then the other two in axis order
+  const Idx3 cm = shifted(q, a, -1);
+  const double tau_p = F.mu[cell_off(F, q)] * (vp - v0);
+  const double tau_m = F.mu[cell_off(F, cm)] * (v0 - vm);
+  double tmp = 2. * (tau_p - tau_m) * ih2[a];
+  for (int d = 0; d < 3; ++d) {
+    if (d == a) continue;
+    const Idx3 qd = shifted(q, d, 1), qda = shifted(qd, a, -1);
+    const double wp0 = face_val(F, d, qd), wpm = face_val(F, d, qda);
+    const double w0 = face_val(F, d, q), wm = face_val(F, d, cm);
+    const double mup = 0.5 * (F.muf[d][face_off(F, d, qd)] + F.muf[d][face_off(F, d, qda)]);
+    const double tp = mup * ((wp0 - wpm) * ih[a] + (vdp[d] - v0) * ih[d]);
+    const double mum = 0.5 * (F.muf[d][face_off(F, d, q)] + F.muf[d][face_off(F, d, cm)]);
+    const double tm = mum * ((w0 - wm) * ih[a] + (v0 - vdm[d]) * ih[d]);
+    tmp += (tp - tm) * ih[d];
+  }
+  // convection, MUSCL with minmod, in axis order
+  for (int d = 0; d < 3; ++d) {
+    double fp, fm;
+    if (d == a) {
+      fp = 0.5 * (F.mf[a][face_off(F, a, q)] + F.mf[a][face_off(F, a, shifted(q, a, 1))]);
+      fm = 0.5 * (F.mf[a][face_off(F, a, cm)] + F.mf[a][face_off(F, a, q)]);
+    } else {
+      const Idx3 qd = shifted(q, d, 1);
+      fp = 0.5 * (F.mf[d][face_off(F, d, shifted(qd, a, -1))] + F.mf[d][face_off(F, d, qd)]);
+      fm = 0.5 * (F.mf[d][face_off(F, d, q)] + F.mf[d][face_off(F, d, cm)]);
+    }
+    const double nplus = d == a ? vp : vdp[d], nminus = d == a ? vm : vdm[d];
+    auto reconstruct = [&](double flux, const Idx3& up, double upwind_v) {
+      if (F.ft[a][face_off(F, a, up)] != F_INTERIOR) return upwind_v;
+      const double vu = F.v[a][face_off(F, a, up)];
+      const double np = d == a ? face_val(F, a, shifted(up, a, 1)) : dir_val(F, a, d, up, +1);
+      const double nm = d == a ? face_val(F, a, shifted(up, a, -1)) : dir_val(F, a, d, up, -1);
+      const double su = minmod(np - vu, vu - nm);
+      const int dir = (int)sgn1(flux);
+      return upwind_v + dir * 0.5 * su;
+    };
+    const double up_p = reconstruct(fp, fp > 0. ? q : shifted(q, d, 1), fp > 0. ? v0 : nplus);
+    const double up_m = reconstruct(fm, fm > 0. ? shifted(q, d, -1) : q, fm > 0. ? nminus : v0);
+    const double Mp = fp * up_p, Mm = fm * up_m;
+    tmp -= (Mp - Mm) * ih[d];
+  }
+  const size_t f = face_off(F, a, q);
+  const double inv_rho = F.fb[a][f];
+  const double rho_old_f = 0.5 * (F.rho_old[cell_off(F, q)] + F.rho_old[cell_off(F, cm)]);
+  tmp -= (F.p[cell_off(F, q)] - F.p[cell_off(F, cm)]) * ih[a];
+  const double inv_volume = ih[0] * ih[1] * ih[2];
+  const double coupling = (F.imp[a] ? F.imp[a][f] : 0.) * inv_volume;
+  double vs = inv_rho * (v0 * rho_old_f + coupling) + dt * (inv_rho * tmp + g);
+  vs = (1.0 - (F.sf[a] ? F.sf[a][f] : 0.)) * vs;
+  return vs;
+}
+
+}  // namespace
+
+extern "C" {
+
+// The momentum predictor u*, G_SMACSolver::get_vof_vstar_rhouu_consistent
+// (CFD/G_SMACSolver.cu:1062-1070): on every F_INTERIOR face with indices
+// 1..N+1, u* = (1/rho)(rho_old u + impulse/V) + dt((1/rho)(viscous -
+// convection - grad p) + g), scaled by 1 - IBM solid fraction.  Families in
+// the order x, y, z (independent: each reads only time-n fields).  Arrays
+// per family in the argument triples; lam/imp/sf may be NULL (0).
+void orc_predict_vstar(int Nx, int Ny, int Nz, double dx, double dy, double dz, double dt, double gx, double gy,
+                       double gz, const uint8_t* bct, const double* bvx, const double* bvy, const double* bvz,
+                       const uint8_t* const* ft, const uint8_t* const* id, const double* const* lam,
+                       const double* const* v, const double* const* mf, const double* const* muf, const double* mu,
+                       const double* rho_old, const double* p, const double* const* fb, const double* const* imp,
+                       const double* const* sf, double* const* vs) {
+  MomFields F;
+  F.N[0] = Nx; F.N[1] = Ny; F.N[2] = Nz;
+  F.bct = bct;
+  F.bv[0] = bvx; F.bv[1] = bvy; F.bv[2] = bvz;
+  for (int a = 0; a < 3; ++a) {
+    F.ft[a] = ft[a]; F.id[a] = id[a]; F.lam[a] = lam[a]; F.v[a] = v[a]; F.mf[a] = mf[a]; F.muf[a] = muf[a];
+    F.fb[a] = fb[a]; F.imp[a] = imp[a]; F.sf[a] = sf[a];
+  }
+  F.mu = mu; F.rho_old = rho_old; F.p = p;
+  const double h[3] = {dx, dy, dz};
+  double ih[3], ih2[3];
+  for (int a = 0; a < 3; ++a) {
+    ih[a] = 1. / h[a];
+    ih2[a] = 1. / (h[a] * h[a]);
+  }
+  const double g[3] = {gx, gy, gz};
+  for (int a = 0; a < 3; ++a)
+    for (int iz = 1; iz <= Nz + 1; ++iz)
+      for (int iy = 1; iy <= Ny + 1; ++iy)
+        for (int ix = 1; ix <= Nx + 1; ++ix) {
+          const Idx3 q{{ix, iy, iz}};
+          const size_t f = face_off(F, a, q);
+          if (F.ft[a][f] != F_INTERIOR) continue;
+          vs[a][f] = vstar_face(F, a, q, ih, ih2, dt, g[a]);
+        }
+}
+
 // Outlet boundary faces (G_SMACSolver::update_boundary_faces,
 // CFD/G_SMACSolver_VoF.cu:1798-1950): f_b of an outlet face is twice the f_b
 // of the face next to it on the interior side (p = 0 on the outlet).  The

@@ -46,7 +46,7 @@ def golden_names():
     if not os.path.isdir(GOLDEN):
         return []
     return sorted(f[:-4] for f in os.listdir(GOLDEN)
-                  if f.endswith(".npz") and not f.startswith(("post", "vstar", "surface")))
+                  if f.endswith(".npz") and not f.startswith(("post", "vstar", "surface", "mom")))
 
 
 def surface_golden_names():
@@ -101,3 +101,18 @@ def fluid_demeaned(p_interior, ct):
 def rel_err(a, b):
     nb = np.linalg.norm(b)
     return np.linalg.norm(a - b) / (nb if nb > 0 else 1.0)
+
+
+def momentum_golden_names():
+    """Fixtures of the reference's get_vof_vstar_rhouu_consistent."""
+    if not os.path.isdir(GOLDEN):
+        return []
+    return sorted(f[:-4] for f in os.listdir(GOLDEN) if f.endswith(".npz") and f.startswith("mom"))
+
+
+def momentum_case_from_spec(spec):
+    spec = dict(spec)
+    for k in ("N", "sides", "g"):
+        if k in spec:
+            spec[k] = tuple(spec[k])
+    return W.momentum_case(**spec)

@@ -64,6 +64,13 @@ SURFACE_CASES = [
     ("surface18x20x16_s6_sphere_solid", dict(N=(18, 20, 16), seed=6, kind="sphere", solid_fraction=0.1)),
 ]
 
+# The momentum predictor (get_vof_vstar_rhouu_consistent): workloads.momentum_case kwargs.
+MOMENTUM_CASES = [
+    ("mom12x10x8_s1", dict(N=(12, 10, 8), seed=1, sides=("x+", "z-"))),
+    ("mom16_s2_solid", dict(N=(16, 16, 16), seed=2, sides=("x-", "y+"), solid_fraction=0.3)),
+    ("mom9x7x11_s3_noextras", dict(N=(9, 7, 11), seed=3, sides=("y-",), extras=False)),
+]
+
 
 def oracle_solid_fraction(N, h, origin, spheres):
     return O.solid_fraction_spheres(N, h, origin, spheres)
@@ -112,6 +119,12 @@ def main():
         fsx, fsy, fsz, nx, ny, nz, kappa, gm, _ = REF.surface_tension(N, h, alpha, ct, sigma)
         np.savez_compressed(os.path.join(args.out, name + ".npz"), meta=np.array(json.dumps(spec)), fsx=fsx, fsy=fsy,
                             fsz=fsz, nx=nx, ny=ny, nz=nz, kappa=kappa, gm=gm)
+        post_index[name] = spec
+        print(name, spec, flush=True)
+    for name, spec in MOMENTUM_CASES:
+        vxs, vys, vzs, _ = REF.predict_vstar(W.momentum_case(**spec))
+        np.savez_compressed(os.path.join(args.out, name + ".npz"), meta=np.array(json.dumps(spec)), vxs=vxs,
+                            vys=vys, vzs=vzs)
         post_index[name] = spec
         print(name, spec, flush=True)
     with open(os.path.join(args.out, "post_index.json"), "w") as f:

@@ -1,5 +1,6 @@
-"""The calls either side of the projection on the GPU: before it the wall u*
-rule (smac_update_vstar_boundary) and the surface-tension force
+"""The calls either side of the projection on the GPU: before it the
+momentum predictor (smac_predict_vstar), the wall u* rule
+(smac_update_vstar_boundary) and the surface-tension force
 (smac_surface_tension), after it the pass over p
 (smac_update_pressure_ghost, smac_update_velocity_ghost, smac_face_gradp),
 against the oracle and the reference.
@@ -15,14 +16,14 @@ import torch
 
 from mydemcfd_b200 import _native as nat
 from mydemcfd_b200 import workloads as W
-from mydemcfd_b200.solver import (BoundaryConditions, DeviceGrid, SMACStep, face_gradp_device,
+from mydemcfd_b200.solver import (BoundaryConditions, DeviceGrid, SMACStep, face_gradp_device, predict_vstar_device,
                                   surface_tension_device, update_pressure_ghost_device, update_velocity_ghost_device,
                                   update_vstar_boundary_device)
 from oracle import oracle as O
 from oracle import ref as REF
 
-from _cases import (load_golden, post_case_from_spec, post_golden_names, surface_case_from_spec,
-                    surface_golden_names, vstar_golden_names)
+from _cases import (load_golden, momentum_case_from_spec, momentum_golden_names, post_case_from_spec,
+                    post_golden_names, surface_case_from_spec, surface_golden_names, vstar_golden_names)
 
 pytestmark = pytest.mark.gpu
 
@@ -289,4 +290,66 @@ def test_surface_tension_against_reference_library_and_time_192():
     a_d, ct_d = _cuda(alpha), _cuda(ct)
     ms = _device_ms(lambda: surface_tension_device(N, h, a_d, ct_d, sigma, work, fs))
     print(f"calc_surface_tension 192^3: {ms * 1e3:.1f} us (reference {ref_ms * 1e3:.1f} us)")
+    assert ms < ref_ms
+
+
+def _momentum_fields(m):
+    f = {}
+    for k, ax in enumerate("xyz"):
+        f["f" + ax + "t"] = _cuda(m.ft[k])
+        f["f" + ax + "bcid"] = _cuda(m.bcid[k])
+        f["v" + ax] = _cuda(m.v[k])
+        f["mf" + ax] = _cuda(m.mf[k])
+        f["mu" + ax] = _cuda(m.muf[k])
+        f["fb" + ax] = _cuda(m.fb[k])
+        if m.lam is not None:
+            f["lam" + ax] = _cuda(m.lam[k])
+        if m.imp is not None:
+            f["imp" + ax] = _cuda(m.imp[k])
+        if m.sf is not None:
+            f["sf" + ax] = _cuda(m.sf[k])
+    f["mu"], f["rho_old"], f["p"] = _cuda(m.mu), _cuda(m.rho_old), _cuda(m.p)
+    return f
+
+
+def run_predict(m):
+    vs = [_cuda(a) for a in m.vs]
+    predict_vstar_device(m.N, m.h, BoundaryConditions(m.bc_type, *m.bc_v), _momentum_fields(m), m.dt, m.g, vs)
+    torch.cuda.synchronize()
+    return tuple(a.cpu().numpy() for a in vs)
+
+
+@pytest.mark.parametrize("spec", [
+    dict(N=(12, 10, 8), seed=1, sides=("x+", "z-")),
+    dict(N=(16, 16, 16), seed=2, sides=("x-", "y+"), solid_fraction=0.3),
+    dict(N=(9, 7, 11), seed=3, sides=("y-",), extras=False),
+    dict(N=(33, 18, 20), seed=5, sides=("x-", "x+", "z+"), solid_fraction=0.2),
+])
+def test_predict_vstar_bit_exact_against_oracle(spec):
+    m = W.momentum_case(**spec)
+    for k, a, b in zip(("vxs", "vys", "vzs"), run_predict(m), O.predict_vstar(m)):
+        assert np.array_equal(a, b), k
+
+
+@pytest.mark.parametrize("name", momentum_golden_names())
+def test_predict_vstar_bit_exact_against_reference_golden(name):
+    meta, arr = load_golden(name)
+    for k, a in zip(("vxs", "vys", "vzs"), run_predict(momentum_case_from_spec(meta))):
+        assert np.array_equal(a, arr[k]), k
+
+
+@pytest.mark.skipif(not REF.available(), reason="reference build oracle/_ref not present")
+def test_predict_vstar_against_reference_library_128_and_time_256():
+    m = W.momentum_case((128, 128, 128), seed=6, sides=("x+", "z-"), solid_fraction=0.05)
+    *ref, _ = REF.predict_vstar(m)
+    for k, a, b in zip(("vxs", "vys", "vzs"), run_predict(m), ref):
+        assert np.array_equal(a, b), k
+    m = W.momentum_case((256, 256, 256), seed=7, sides=("x+",), solid_fraction=0.02)
+    REF.predict_vstar(m)  # loads the reference's kernels
+    *_, ref_ms = REF.predict_vstar(m)
+    fields = _momentum_fields(m)
+    vs = [_cuda(a) for a in m.vs]
+    bc = BoundaryConditions(m.bc_type, *m.bc_v)
+    ms = _device_ms(lambda: predict_vstar_device(m.N, m.h, bc, fields, m.dt, m.g, vs))
+    print(f"get_vof_vstar_rhouu_consistent 256^3: {ms * 1e3:.1f} us (reference {ref_ms * 1e3:.1f} us)")
     assert ms < ref_ms

@@ -7,7 +7,8 @@ import pytest
 from mydemcfd_b200 import workloads as W
 
 from _cases import (build_case, fluid_demeaned, golden_names, load_golden, post_case_from_spec, post_golden_names,
-                    ref_grid, rel_err, surface_case_from_spec, surface_golden_names, vstar_golden_names)
+                    ref_grid, rel_err, surface_case_from_spec, surface_golden_names, vstar_golden_names,
+                    momentum_case_from_spec, momentum_golden_names)
 
 
 def test_box_types_match_reference_setup(oracle_lib):
@@ -516,4 +517,45 @@ def test_surface_tension_oracle_matches_reference_golden(oracle_lib, name):
     N, h, alpha, ct, sigma = surface_case_from_spec(meta)
     got = oracle_lib.surface_tension(N, h, alpha, ct, sigma)
     for k, a in zip(("fsx", "fsy", "fsz", "nx", "ny", "nz", "kappa", "gm"), got):
+        assert np.array_equal(a, arr[k]), k
+
+
+# ---------------------------------------------------------------------------
+# the momentum predictor (get_vof_vstar_rhouu_consistent)
+
+def test_predict_vstar_fluid_at_rest_is_pressure_and_gravity(oracle_lib):
+    """Known answer: with u = 0, no advecting flux and zero boundary
+    velocities every stress and flux term is 0, so on each F_INTERIOR face
+    u* = (1 - s)(f_b (0 + I/V) + dt (f_b (-(p - p_m)/h) + g))."""
+    import dataclasses
+    m = W.momentum_case((8, 7, 6), seed=4, solid_fraction=0.3)
+    zero = lambda arrs: tuple(np.zeros_like(a) for a in arrs)  # noqa: E731
+    m = dataclasses.replace(m, v=zero(m.v), mf=zero(m.mf), bc_v=zero(m.bc_v))
+    got = oracle_lib.predict_vstar(m)
+    inv_vol = (1.0 / m.h[0]) * (1.0 / m.h[1]) * (1.0 / m.h[2])
+    for a in range(3):
+        t = m.ft[a]
+        z, y, x = np.nonzero(t == W.F_INTERIOR)
+        cz, cy, cx = z.copy(), y.copy(), x.copy()
+        (cx, cy, cz)[a][...] -= 1
+        dp = (m.p[z, y, x] - m.p[cz, cy, cx]) * (1.0 / m.h[a])
+        tmp = 0.0 - dp
+        fb = m.fb[a][z, y, x]
+        coup = m.imp[a][z, y, x] * inv_vol
+        want = fb * (0.0 * (0.5 * (m.rho_old[z, y, x] + m.rho_old[cz, cy, cx])) + coup) + m.dt * (fb * tmp + m.g[a])
+        want = (1.0 - m.sf[a][z, y, x]) * want
+        np.testing.assert_array_equal(got[a][z, y, x], want)
+        # other faces keep their u*
+        np.testing.assert_array_equal(got[a][t != W.F_INTERIOR], m.vs[a][t != W.F_INTERIOR])
+
+
+MOMENTUM_GOLDEN = momentum_golden_names()
+
+
+@pytest.mark.skipif(not MOMENTUM_GOLDEN, reason="no momentum-predictor golden vectors")
+@pytest.mark.parametrize("name", MOMENTUM_GOLDEN)
+def test_predict_vstar_oracle_matches_reference_golden(oracle_lib, name):
+    meta, arr = load_golden(name)
+    got = oracle_lib.predict_vstar(momentum_case_from_spec(meta))
+    for k, a in zip(("vxs", "vys", "vzs"), got):
         assert np.array_equal(a, arr[k]), k
