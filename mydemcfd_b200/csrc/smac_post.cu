@@ -747,30 +747,15 @@ struct MomArgs {
   const double* sf[3];   // nullptr: 0
   double* vs[3];
   double dt, g[3], ih[3], ih2[3], inv_volume;
+  long long st[4][3];  // index strides along x, y, z of the three face families and (3) the cells
   BcTable bc;
 };
 
-template <int F>
-__device__ __forceinline__ long long mface(const MomArgs& A, int x, int y, int z) {
-  const long long S0 = A.N[0] + 2 + (F == 0), S1 = A.N[1] + 2 + (F == 1);
-  return ((long long)z * S1 + y) * S0 + x;
-}
-__device__ __forceinline__ long long mcell(const MomArgs& A, int x, int y, int z) {
-  return ((long long)z * (A.N[1] + 2) + y) * (A.N[0] + 2) + x;
-}
-template <int AX>
-__device__ __forceinline__ void step(int& x, int& y, int& z, int s) {
-  if (AX == 0) x += s;
-  else if (AX == 1) y += s;
-  else z += s;
-}
-
-// d_get_v{B}_{B}face (G_BoundaryFunctions.h:9-98): family-B velocity at a
-// face, boundary faces by their type; the x rule passes the stored value
+// d_get_v{B}_{B}face (G_BoundaryFunctions.h:9-98): family-B velocity at
+// face f, boundary faces by their type; the x rule passes the stored value
 // through for outlets only, the y and z rules for slip too.
 template <int B>
-__device__ __forceinline__ double m_face_val(const MomArgs& A, int x, int y, int z) {
-  const long long f = mface<B>(A, x, y, z);
+__device__ __forceinline__ double m_face_val(const MomArgs& A, long long f) {
   const uint8_t t = A.ft[B][f];
   if (t == 0) return A.v[B][f];  // F_INTERIOR
   if (t == 1) {                  // F_BOUNDARY
@@ -784,19 +769,14 @@ __device__ __forceinline__ double m_face_val(const MomArgs& A, int x, int y, int
 }
 
 // d_get_v{AF}_{D}dir (G_BoundaryFunctions.h:100-367): family-AF velocity
-// next to face (x,y,z) along D != AF on side s, mirrored about a wall.
+// next to a face along D != AF on side s, mirrored about a wall.  fa, fd:
+// the face's index in the family-AF and family-D layouts.
 template <int AF, int D>
-__device__ __forceinline__ double m_dir_val(const MomArgs& A, int x, int y, int z, int s) {
-  const double inside = A.v[AF][mface<AF>(A, x, y, z)];
-  int x2 = x, y2 = y, z2 = z;
-  step<D>(x2, y2, z2, s);
-  const long long f2 = mface<AF>(A, x2, y2, z2);
+__device__ __forceinline__ double m_dir_val(const MomArgs& A, long long fa, long long fd, int s) {
+  const long long f2 = s > 0 ? fa + A.st[AF][D] : fa - A.st[AF][D];
   if (A.ft[AF][f2] == 0) return A.v[AF][f2];
-  int xf = x, yf = y, zf = z;
-  if (s > 0) step<D>(xf, yf, zf, 1);
-  int xg = xf, yg = yf, zg = zf;
-  step<AF>(xg, yg, zg, -1);
-  const long long ff = mface<D>(A, xf, yf, zf), fg = mface<D>(A, xg, yg, zg);
+  const double inside = A.v[AF][fa];
+  const long long ff = s > 0 ? fd + A.st[D][D] : fd, fg = ff - A.st[D][AF];
   double wall = 0.0;
   int count = 0;
   if (A.ft[D][ff] == 1) {
@@ -821,122 +801,123 @@ __device__ __forceinline__ double m_minmod(double dp, double dm) {
 // The two other axes of AF in ascending order, as compile-time values.
 template <int AF> struct Others { static constexpr int D0 = AF == 0 ? 1 : 0, D1 = AF == 2 ? 1 : 2; };
 
-// Viscous cross term of axis D: (tau_D+ - tau_D-) / h_D.
+// Viscous cross term of axis D: (tau_D+ - tau_D-) / h_D.  b: the face's
+// indices in the three family layouts; vdp, vdm: its mirrored neighbours
+// along D.
 template <int AF, int D>
-__device__ __forceinline__ double m_cross(const MomArgs& A, int x, int y, int z, double v0) {
-  int xd = x, yd = y, zd = z;
-  step<D>(xd, yd, zd, 1);
-  int xda = xd, yda = yd, zda = zd;
-  step<AF>(xda, yda, zda, -1);
-  int xm = x, ym = y, zm = z;
-  step<AF>(xm, ym, zm, -1);
-  const double wp0 = m_face_val<D>(A, xd, yd, zd), wpm = m_face_val<D>(A, xda, yda, zda);
-  const double w0 = m_face_val<D>(A, x, y, z), wm = m_face_val<D>(A, xm, ym, zm);
-  const double vdp = m_dir_val<AF, D>(A, x, y, z, +1), vdm = m_dir_val<AF, D>(A, x, y, z, -1);
-  const double mup = DMUL(0.5, DADD(A.muf[D][mface<D>(A, xd, yd, zd)], A.muf[D][mface<D>(A, xda, yda, zda)]));
+__device__ __forceinline__ double m_cross(const MomArgs& A, const long long* b, double v0, double vdp, double vdm) {
+  const long long qd = b[D] + A.st[D][D], qda = qd - A.st[D][AF], q = b[D], qm = b[D] - A.st[D][AF];
+  const double wp0 = m_face_val<D>(A, qd), wpm = m_face_val<D>(A, qda);
+  const double w0 = m_face_val<D>(A, q), wm = m_face_val<D>(A, qm);
+  const double mup = DMUL(0.5, DADD(A.muf[D][qd], A.muf[D][qda]));
   const double tp = DMUL(mup, DADD(DMUL(DSUB(wp0, wpm), A.ih[AF]), DMUL(DSUB(vdp, v0), A.ih[D])));
-  const double mum = DMUL(0.5, DADD(A.muf[D][mface<D>(A, x, y, z)], A.muf[D][mface<D>(A, xm, ym, zm)]));
+  const double mum = DMUL(0.5, DADD(A.muf[D][q], A.muf[D][qm]));
   const double tm = DMUL(mum, DADD(DMUL(DSUB(w0, wm), A.ih[AF]), DMUL(DSUB(v0, vdm), A.ih[D])));
   return DMUL(DSUB(tp, tm), A.ih[D]);
 }
 
-// Neighbour of family-AF face (x,y,z) along D on side s: the face rule along
-// AF itself, the mirrored rule across.
+// The neighbour two faces away along D on side s (the one value the MUSCL
+// reconstruction at an upwind neighbour needs that the face's own
+// stencil does not hold): the face rule along AF, the mirrored rule across.
 template <int AF, int D>
-__device__ __forceinline__ double m_neigh(const MomArgs& A, int x, int y, int z, int s) {
-  if (D == AF) {
-    int xs = x, ys = y, zs = z;
-    step<AF>(xs, ys, zs, s);
-    return m_face_val<AF>(A, xs, ys, zs);
-  }
-  return m_dir_val<AF, D == AF ? Others<AF>::D0 : D>(A, x, y, z, s);
+__device__ __forceinline__ double m_far(const MomArgs& A, const long long* b, int s) {
+  if (D == AF) return m_face_val<AF>(A, b[AF] + 2 * s * A.st[AF][AF]);
+  const long long fa = b[AF] + s * A.st[AF][D], fd = b[D] + s * A.st[D][D];
+  return m_dir_val<AF, D == AF ? Others<AF>::D0 : D>(A, fa, fd, s);
 }
 
-// MUSCL (minmod) value at the upwind face (x,y,z) for a flux through a
-// D-side of the control volume; upwind_v itself where the face has no
-// stencil (not F_INTERIOR).
-template <int AF, int D>
-__device__ __forceinline__ double m_recon(const MomArgs& A, double flux, int x, int y, int z, double upwind_v) {
-  const long long f = mface<AF>(A, x, y, z);
-  if (A.ft[AF][f] != 0) return upwind_v;
-  const double vu = A.v[AF][f];
-  const double su = m_minmod(DSUB(m_neigh<AF, D>(A, x, y, z, +1), vu), DSUB(vu, m_neigh<AF, D>(A, x, y, z, -1)));
+__device__ __forceinline__ double m_muscl(double upwind_v, double flux, double su) {
   const double dir = flux < 0.0 ? -1.0 : 1.0;
   return DADD(upwind_v, DMUL(DMUL(dir, 0.5), su));
 }
 
-// Convection through the two D-sides, (M+ - M-) / h_D.
+// Convection through the two D-sides of the control volume, (M+ - M-)/h_D,
+// with MUSCL (minmod) values at the upwind faces (k_get_vof_vstar_* :150-290).
+// np, nm: the face's neighbours along D.  At the face itself the limiter
+// uses np and nm; at an F_INTERIOR upwind neighbour its value is np (or nm),
+// its inner neighbour the face itself, its outer one m_far; a neighbour
+// that is not F_INTERIOR gives its value unlimited.
 template <int AF, int D>
-__device__ __forceinline__ double m_conv(const MomArgs& A, int x, int y, int z, double v0, double nplus,
-                                         double nminus) {
-  int xm = x, ym = y, zm = z;
-  step<AF>(xm, ym, zm, -1);
+__device__ __forceinline__ double m_conv(const MomArgs& A, const long long* b, double v0, double np, double nm) {
   double fp, fm;
   if (D == AF) {
-    int xp = x, yp = y, zp = z;
-    step<AF>(xp, yp, zp, 1);
-    fp = DMUL(0.5, DADD(A.mf[AF][mface<AF>(A, x, y, z)], A.mf[AF][mface<AF>(A, xp, yp, zp)]));
-    fm = DMUL(0.5, DADD(A.mf[AF][mface<AF>(A, xm, ym, zm)], A.mf[AF][mface<AF>(A, x, y, z)]));
+    const long long f = b[AF], s = A.st[AF][AF];
+    fp = DMUL(0.5, DADD(A.mf[AF][f], A.mf[AF][f + s]));
+    fm = DMUL(0.5, DADD(A.mf[AF][f - s], A.mf[AF][f]));
   } else {
-    int xd = x, yd = y, zd = z;
-    step<D>(xd, yd, zd, 1);
-    int xda = xd, yda = yd, zda = zd;
-    step<AF>(xda, yda, zda, -1);
-    fp = DMUL(0.5, DADD(A.mf[D][mface<D>(A, xda, yda, zda)], A.mf[D][mface<D>(A, xd, yd, zd)]));
-    fm = DMUL(0.5, DADD(A.mf[D][mface<D>(A, x, y, z)], A.mf[D][mface<D>(A, xm, ym, zm)]));
+    const long long qd = b[D] + A.st[D][D], qda = qd - A.st[D][AF];
+    fp = DMUL(0.5, DADD(A.mf[D][qda], A.mf[D][qd]));
+    fm = DMUL(0.5, DADD(A.mf[D][b[D]], A.mf[D][b[D] - A.st[D][AF]]));
   }
-  int xu = x, yu = y, zu = z;
-  if (!(fp > 0.0)) step<D>(xu, yu, zu, 1);
-  const double up = m_recon<AF, D>(A, fp, xu, yu, zu, fp > 0.0 ? v0 : nplus);
-  int xv = x, yv = y, zv = z;
-  if (fm > 0.0) step<D>(xv, yv, zv, -1);
-  const double um = m_recon<AF, D>(A, fm, xv, yv, zv, fm > 0.0 ? nminus : v0);
+  const double su0 = (fp > 0.0 || !(fm > 0.0)) ? m_minmod(DSUB(np, v0), DSUB(v0, nm)) : 0.0;
+  double up, um;
+  if (fp > 0.0) {
+    up = m_muscl(v0, fp, su0);
+  } else if (A.ft[AF][b[AF] + A.st[AF][D]] == 0) {
+    up = m_muscl(np, fp, m_minmod(DSUB(m_far<AF, D>(A, b, +1), np), DSUB(np, v0)));
+  } else {
+    up = np;
+  }
+  if (!(fm > 0.0)) {
+    um = m_muscl(v0, fm, su0);
+  } else if (A.ft[AF][b[AF] - A.st[AF][D]] == 0) {
+    um = m_muscl(nm, fm, m_minmod(DSUB(v0, nm), DSUB(nm, m_far<AF, D>(A, b, -1))));
+  } else {
+    um = nm;
+  }
   return DMUL(DSUB(DMUL(fp, up), DMUL(fm, um)), A.ih[D]);
 }
 
+// u* of the F_INTERIOR family-AF face with indices b[0..2] in the family
+// layouts and b[3] in the cells.
 template <int AF>
-__device__ __forceinline__ double m_vstar(const MomArgs& A, int x, int y, int z) {
+__device__ __forceinline__ double m_vstar(const MomArgs& A, const long long* b) {
   constexpr int D0 = Others<AF>::D0, D1 = Others<AF>::D1;
-  const long long f = mface<AF>(A, x, y, z);
+  const long long f = b[AF], c = b[3], cm = b[3] - A.st[3][AF];
   const double v0 = A.v[AF][f];
-  int xm = x, ym = y, zm = z;
-  step<AF>(xm, ym, zm, -1);
-  const double vp = m_neigh<AF, AF>(A, x, y, z, +1), vm = m_neigh<AF, AF>(A, x, y, z, -1);
+  const double vp = m_face_val<AF>(A, f + A.st[AF][AF]), vm = m_face_val<AF>(A, f - A.st[AF][AF]);
+  const double p0 = m_dir_val<AF, D0>(A, f, b[D0], +1), m0 = m_dir_val<AF, D0>(A, f, b[D0], -1);
+  const double p1 = m_dir_val<AF, D1>(A, f, b[D1], +1), m1 = m_dir_val<AF, D1>(A, f, b[D1], -1);
   // viscous: the own axis, then the other two in axis order
-  const double tau_p = DMUL(A.mu[mcell(A, x, y, z)], DSUB(vp, v0));
-  const double tau_m = DMUL(A.mu[mcell(A, xm, ym, zm)], DSUB(v0, vm));
+  const double tau_p = DMUL(A.mu[c], DSUB(vp, v0));
+  const double tau_m = DMUL(A.mu[cm], DSUB(v0, vm));
   double tmp = DMUL(DMUL(2.0, DSUB(tau_p, tau_m)), A.ih2[AF]);
-  tmp = DADD(tmp, m_cross<AF, D0>(A, x, y, z, v0));
-  tmp = DADD(tmp, m_cross<AF, D1>(A, x, y, z, v0));
+  tmp = DADD(tmp, m_cross<AF, D0>(A, b, v0, p0, m0));
+  tmp = DADD(tmp, m_cross<AF, D1>(A, b, v0, p1, m1));
   // convection in axis order
-  tmp = DSUB(tmp, m_conv<AF, 0>(A, x, y, z, v0, m_neigh<AF, 0>(A, x, y, z, +1), m_neigh<AF, 0>(A, x, y, z, -1)));
-  tmp = DSUB(tmp, m_conv<AF, 1>(A, x, y, z, v0, m_neigh<AF, 1>(A, x, y, z, +1), m_neigh<AF, 1>(A, x, y, z, -1)));
-  tmp = DSUB(tmp, m_conv<AF, 2>(A, x, y, z, v0, m_neigh<AF, 2>(A, x, y, z, +1), m_neigh<AF, 2>(A, x, y, z, -1)));
+  const double npx = AF == 0 ? vp : (D0 == 0 ? p0 : p1), nmx = AF == 0 ? vm : (D0 == 0 ? m0 : m1);
+  const double npy = AF == 1 ? vp : (D0 == 1 ? p0 : p1), nmy = AF == 1 ? vm : (D0 == 1 ? m0 : m1);
+  const double npz = AF == 2 ? vp : p1, nmz = AF == 2 ? vm : m1;
+  tmp = DSUB(tmp, m_conv<AF, 0>(A, b, v0, npx, nmx));
+  tmp = DSUB(tmp, m_conv<AF, 1>(A, b, v0, npy, nmy));
+  tmp = DSUB(tmp, m_conv<AF, 2>(A, b, v0, npz, nmz));
   const double inv_rho = A.fb[AF][f];
-  const double rho_old_f = DMUL(0.5, DADD(A.rho_old[mcell(A, x, y, z)], A.rho_old[mcell(A, xm, ym, zm)]));
-  tmp = DSUB(tmp, DMUL(DSUB(A.p[mcell(A, x, y, z)], A.p[mcell(A, xm, ym, zm)]), A.ih[AF]));
+  const double rho_old_f = DMUL(0.5, DADD(A.rho_old[c], A.rho_old[cm]));
+  tmp = DSUB(tmp, DMUL(DSUB(A.p[c], A.p[cm]), A.ih[AF]));
   const double coupling = DMUL(A.imp[AF] ? A.imp[AF][f] : 0.0, A.inv_volume);
   const double vs = DADD(DMUL(inv_rho, DADD(DMUL(v0, rho_old_f), coupling)),
                          DMUL(A.dt, DADD(DMUL(inv_rho, tmp), A.g[AF])));
   return DMUL(DSUB(1.0, A.sf[AF] ? A.sf[AF][f] : 0.0), vs);
 }
 
-// One thread per face index (x, y) of plane z of the box 1..N+1; blockIdx.z
-// runs over the three families' planes.  Only F_INTERIOR faces are written.
+// One thread per face index (x, y) of plane z of the box 1..N+1;
+// blockIdx.z = 3 (z - 1) + family, so the three families of a plane run
+// together and share the arrays they all read (velocities, fluxes, cell
+// fields) through L2.  Only F_INTERIOR faces are written.
 __global__ void __launch_bounds__(256) k_predict_vstar(MomArgs A) {
-  const int fam = blockIdx.z / (A.N[2] + 1);
-  const int z = blockIdx.z % (A.N[2] + 1) + 1;
+  const int fam = blockIdx.z % 3;
+  const int z = blockIdx.z / 3 + 1;
   const int x = blockIdx.x * 32 + threadIdx.x + 1, y = blockIdx.y * 8 + threadIdx.y + 1;
   if (x > A.N[0] + 1 || y > A.N[1] + 1) return;
+  long long b[4];
+#pragma unroll
+  for (int k = 0; k < 4; ++k) b[k] = x * A.st[k][0] + y * A.st[k][1] + z * A.st[k][2];
   if (fam == 0) {
-    const long long f = mface<0>(A, x, y, z);
-    if (A.ft[0][f] == 0) A.vs[0][f] = m_vstar<0>(A, x, y, z);
+    if (A.ft[0][b[0]] == 0) A.vs[0][b[0]] = m_vstar<0>(A, b);
   } else if (fam == 1) {
-    const long long f = mface<1>(A, x, y, z);
-    if (A.ft[1][f] == 0) A.vs[1][f] = m_vstar<1>(A, x, y, z);
+    if (A.ft[1][b[1]] == 0) A.vs[1][b[1]] = m_vstar<1>(A, b);
   } else {
-    const long long f = mface<2>(A, x, y, z);
-    if (A.ft[2][f] == 0) A.vs[2][f] = m_vstar<2>(A, x, y, z);
+    if (A.ft[2][b[2]] == 0) A.vs[2][b[2]] = m_vstar<2>(A, b);
   }
 }
 
@@ -1181,6 +1162,12 @@ smac_status smac_predict_vstar(const smac_grid_desc* d, const smac_boundary_tabl
     A.ih2[k] = 1. / (h[k] * h[k]);
   }
   A.inv_volume = A.ih[0] * A.ih[1] * A.ih[2];
+  for (int k = 0; k < 4; ++k) {  // families 0..2, cells 3
+    const long long S0 = d->nx + 2 + (k == 0), S1 = d->ny + 2 + (k == 1);
+    A.st[k][0] = 1;
+    A.st[k][1] = S0;
+    A.st[k][2] = S0 * S1;
+  }
   fill_table(&A.bc, bc);
   const dim3 grid((unsigned)((d->nx + 1 + 31) / 32), (unsigned)((d->ny + 1 + 7) / 8), 3u * (unsigned)(d->nz + 1));
   k_predict_vstar<<<grid, dim3(32, 8), 0, (cudaStream_t)stream>>>(A);
