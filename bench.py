@@ -393,7 +393,8 @@ def run_ours(args, ranks):
 
 def post_pass_timings(case, g, p, v, dev, stream):
     """The calls either side of the projection on the bench grid: before it
-    update_vstar_boundary, after it update_boundary_ghost + make_face_gradp.
+    the momentum predictor and update_vstar_boundary, after it
+    update_boundary_ghost + make_face_gradp.
     Device time of each call (its launches replayed from a CUDA graph, CUDA
     events, median of 10, each after an L2 flush) and the algorithmic bytes
     it moves.  Inputs: the projected pressure and velocity, no-slip walls
@@ -401,8 +402,9 @@ def post_pass_timings(case, g, p, v, dev, stream):
     import torch
 
     from mydemcfd_b200 import workloads as W
-    from mydemcfd_b200.solver import (BoundaryConditions, face_gradp_device, update_pressure_ghost_device,
-                                      update_velocity_ghost_device, update_vstar_boundary_device)
+    from mydemcfd_b200.solver import (BoundaryConditions, face_gradp_device, predict_vstar_device,
+                                      update_pressure_ghost_device, update_velocity_ghost_device,
+                                      update_vstar_boundary_device)
     N, h = case.N, case.h
     sh = W.shapes(N)
     bcid = [torch.zeros(sh[k], dtype=torch.uint8, device=dev) for k in "xyz"]
@@ -413,7 +415,20 @@ def post_pass_timings(case, g, p, v, dev, stream):
     fb = (g.f_bx_, g.f_by_, g.f_bz_)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
     vs_copy = [t.clone() for t in vs]
+    # momentum-predictor fields: the projected velocity as both u and the
+    # advecting flux, face viscosities 1e-3, rho_old 1, f_b from the grid
+    mom = {"mu": torch.full(sh["cell"], 1e-3, dtype=torch.float64, device=dev),
+           "rho_old": torch.ones(sh["cell"], dtype=torch.float64, device=dev), "p": p}
+    for k, ax in enumerate("xyz"):
+        mom["f" + ax + "t"] = (g.f_xtype_, g.f_ytype_, g.f_ztype_)[k]
+        mom["f" + ax + "bcid"] = bcid[k]
+        mom["v" + ax] = v[k]
+        mom["mf" + ax] = v[k]
+        mom["mu" + ax] = torch.full(sh["xyz"[k]], 1e-3, dtype=torch.float64, device=dev)
+        mom["fb" + ax] = fb[k]
+    vs_pred = [t.clone() for t in vs]
     calls = {
+        "predict_vstar": lambda: predict_vstar_device(N, h, bc, mom, case.dt, (0.0, 0.0, -9.8), vs_pred),
         "vstar_boundary": lambda: update_vstar_boundary_device(N, h, bc, (g.f_xtype_, g.f_ytype_, g.f_ztype_), bcid,
                                                                marks, None, vs_copy),
         "pressure_ghost": lambda: update_pressure_ghost_device(N, h, g.celltype_, None, (0.0, 0.0, -9.8), p),
@@ -427,6 +442,10 @@ def post_pass_timings(case, g, p, v, dev, stream):
     ring = sum(2 * (N[a] + 1) * (N[b] + N[c] + 2) for a, b, c in ((0, 1, 2), (1, 0, 2), (2, 0, 1)))
     nwall = 2 * ((ny * nz) + (nx * nz) + (nx * ny))
     alg = {
+        # per cell, for the three families together: u, flux, face viscosity,
+        # f_b (8 B each) and the type (1 B) of each family's face; mu, rho_old
+        # and p; the three u* written
+        "predict_vstar": ncell * (3 * (4 * 8 + 1) + 3 * 8 + 3 * 8),
         # face types scanned; per wall face its id read and u* written
         "vstar_boundary": nface + nwall * (1 + 8),
         # cell types scanned; per ghost cell: its source's p and type read, p written
