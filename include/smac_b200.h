@@ -331,6 +331,27 @@ smac_status smac_update_velocity_ghost(const smac_grid_desc* d, const smac_bound
 smac_status smac_face_gradp(const smac_grid_desc* d, const double* p, double* gpx, double* gpy, double* gpz,
                             void* stream);
 
+/* ---- output ----------------------------------------------------------------
+ * FileInOut::output_vti_binary_cellData (CFD/FileInOut.cpp:144-262): a VTK
+ * ImageData file of the interior cells with four Float32 cell arrays in raw
+ * appended data, pressure, alpha, velocity (the mean of each cell's two faces,
+ * 3 components) and ibm_solid_fraction, each after its UInt32 byte count.
+ * Pack the appended block on the device, copy it to the host, write the file:
+ * the file equals the reference's byte for byte. */
+
+/* Bytes of the appended block: 16 + 24 Nx Ny Nz (0 for a bad grid). */
+size_t smac_vti_block_bytes(const smac_grid_desc* d);
+/* Build the appended block in device memory `block` (4-byte aligned,
+ * smac_vti_block_bytes long) from the cell arrays p, alpha, ibm_sf and the
+ * face arrays vx, vy, vz; alpha and ibm_sf may be NULL (written as 0).
+ * Grids whose velocity block would pass 2^32 bytes are refused (the file's
+ * size fields are UInt32). */
+smac_status smac_vti_pack(const smac_grid_desc* d, const double* p, const double* alpha, const double* vx,
+                          const double* vy, const double* vz, const double* ibm_sf, void* block, void* stream);
+/* Write the .vti file `path` around a packed block in HOST memory; origin is
+ * StaggeredGrid::origin_x_, y_, z_.  Host code only: it needs no GPU. */
+smac_status smac_vti_write(const smac_grid_desc* d, const double origin[3], const void* block_host, const char* path);
+
 /* y = A x with the FP64 fine operator (cells, reference layout, interior
  * entries); the reference's k_build_vof_poisson_Ap (G_PCGSolver.cu:214-245). */
 smac_status smac_apply_A(smac_handle* h, const double* x, double* y);

@@ -80,7 +80,7 @@ EXPORTS = [
     "smac_selftest_sweep", "smac_apply_A_dot_noalloc", "smac_async_create", "smac_async_submit",
     "smac_async_wait", "smac_async_destroy", "smac_update_boundary_faces", "smac_update_pressure_ghost",
     "smac_update_velocity_ghost", "smac_face_gradp", "smac_update_vstar_boundary", "smac_surface_tension",
-    "smac_predict_vstar",
+    "smac_predict_vstar", "smac_vti_block_bytes", "smac_vti_pack", "smac_vti_write",
 ]
 
 
@@ -128,6 +128,8 @@ def load(path: str = LIB_PATH):
         "smac_surface_tension": [ctypes.POINTER(GridDesc), dp, u8p, d, dp, dp, dp, dp, dp, dp, dp, dp, vp],
         "smac_predict_vstar": [ctypes.POINTER(GridDesc), ctypes.POINTER(BoundaryTable), ctypes.POINTER(MomentumFields),
                                d, d, d, d, dp, dp, dp, vp],
+        "smac_vti_pack": [ctypes.POINTER(GridDesc), dp, dp, dp, dp, dp, dp, vp, vp],
+        "smac_vti_write": [ctypes.POINTER(GridDesc), ctypes.POINTER(d), vp, ctypes.c_char_p],
         "smac_update_vstar_boundary": [ctypes.POINTER(GridDesc), ctypes.POINTER(BoundaryTable), u8p, u8p, u8p, u8p,
                                        u8p, u8p, u8p, u8p, u8p, dp, dp, dp, dp, dp, dp, vp],
     }
@@ -135,6 +137,8 @@ def load(path: str = LIB_PATH):
         fn = getattr(lib, name)
         fn.argtypes = args
         fn.restype = ctypes.c_int
+    lib.smac_vti_block_bytes.restype = ctypes.c_size_t
+    lib.smac_vti_block_bytes.argtypes = [ctypes.POINTER(GridDesc)]
     lib.smac_last_error_string.restype = ctypes.c_char_p
     lib.smac_last_error_string.argtypes = []
     _lib = lib

@@ -12,7 +12,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 LIB = os.path.join(HERE, "libsmac_b200.so")
 SOURCES = [os.path.join(HERE, "csrc", "smac_api.cu"), os.path.join(HERE, "csrc", "smac_noalloc.cu"),
-           os.path.join(HERE, "csrc", "smac_async.cu"), os.path.join(HERE, "csrc", "smac_post.cu")]
+           os.path.join(HERE, "csrc", "smac_async.cu"), os.path.join(HERE, "csrc", "smac_post.cu"),
+           os.path.join(HERE, "csrc", "smac_vti.cu")]
 DEPS = SOURCES + [
     os.path.join(HERE, "csrc", "smac_common.cuh"),
     os.path.join(HERE, "csrc", "smac_kernels.cuh"),

@@ -377,3 +377,25 @@ class RefGrid:
             setattr(pr, name, _u8(getattr(self, name)))
         self._keep = pr  # arrays are owned by self
         return pr
+
+
+def vti_block(N, p, alpha, vx, vy, vz, ibm_sf):
+    """The appended-data block of FileInOut::output_vti_binary_cellData
+    (CFD/FileInOut.cpp:208-254) in numpy: four Float32 cell arrays of the
+    interior cells, x fastest, each after its UInt32 byte count; the velocity
+    is the mean of each cell's two faces in FP64, then rounded to Float32.
+    alpha / ibm_sf None mean zeros."""
+    nx, ny, nz = N
+    inner = (slice(1, nz + 1), slice(1, ny + 1), slice(1, nx + 1))
+    n = nx * ny * nz
+    zeros = np.zeros((nz + 2, ny + 2, nx + 2))
+    ux = 0.5 * (vx[1:nz + 1, 1:ny + 1, 1:nx + 1] + vx[1:nz + 1, 1:ny + 1, 2:nx + 2])
+    uy = 0.5 * (vy[1:nz + 1, 1:ny + 1, 1:nx + 1] + vy[1:nz + 1, 2:ny + 2, 1:nx + 1])
+    uz = 0.5 * (vz[1:nz + 1, 1:ny + 1, 1:nx + 1] + vz[2:nz + 2, 1:ny + 1, 1:nx + 1])
+    vel = np.stack([ux, uy, uz], axis=-1).astype(np.float32).reshape(-1)
+    parts = []
+    for arr, cnt in ((p, n), (alpha if alpha is not None else zeros, n), (None, 3 * n),
+                     (ibm_sf if ibm_sf is not None else zeros, n)):
+        parts.append(np.array([4 * cnt], np.uint32).tobytes())
+        parts.append(vel.tobytes() if arr is None else arr[inner].astype(np.float32).reshape(-1).tobytes())
+    return b"".join(parts)

@@ -302,3 +302,28 @@ def predict_vstar(m):
     if rc != 0:
         raise RuntimeError(f"ref_predict_vstar returned {rc}")
     return (*out, io.ms)
+
+
+IO_LIB_PATH = os.path.join(_HERE, "_ref", "libref_io.so")
+_io_lib = None
+
+
+def io_available() -> bool:
+    return os.path.exists(IO_LIB_PATH)
+
+
+def write_vti(N, h, origin, p, alpha, vx, vy, vz, ibm_sf, outdir, step):
+    """Run the reference's FileInOut::output_vti_binary_cellData (host code,
+    oracle/_ref/libref_io.so) on the given reference-layout arrays; returns
+    the path of the file it wrote (<outdir>/result_<step:06d>.vti)."""
+    global _io_lib
+    if _io_lib is None:
+        _io_lib = ctypes.CDLL(IO_LIB_PATH)
+        _io_lib.ref_write_vti.restype = ctypes.c_int
+        _io_lib.ref_write_vti.argtypes = [ctypes.c_int] * 3 + [ctypes.c_double] * 6 + [_dp] * 6 + \
+            [ctypes.c_char_p, ctypes.c_int]
+    arrs = [np.ascontiguousarray(a, np.float64) for a in (p, alpha, vx, vy, vz, ibm_sf)]
+    rc = _io_lib.ref_write_vti(*N, *h, *origin, *(_p(a) for a in arrs), str(outdir).encode(), int(step))
+    if rc != 0:
+        raise RuntimeError(f"ref_write_vti returned {rc}")
+    return os.path.join(str(outdir), f"result_{int(step):06d}.vti")

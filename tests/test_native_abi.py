@@ -14,7 +14,7 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 def header_functions():
     txt = open(os.path.join(ROOT, "include", "smac_b200.h")).read()
-    return sorted(set(re.findall(r"^(?:smac_status|const char\*|void)\s+(smac_\w+)\s*\(", txt, re.M)))
+    return sorted(set(re.findall(r"^(?:smac_status|const char\*|void|size_t)\s+(smac_\w+)\s*\(", txt, re.M)))
 
 
 @pytest.fixture(scope="module")
