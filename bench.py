@@ -48,6 +48,10 @@ def parse():
     ap.add_argument("--kernel-only", type=int, default=None,
                     help="set up the workload and launch one kernel (smac_time_kernel id) a few times: a small, "
                          "self-contained command for ncu captures")
+    ap.add_argument("--around", default=None,
+                    choices=["predict_vstar", "vstar_boundary", "pressure_ghost", "velocity_ghost", "face_gradp"],
+                    help="set up the workload and launch one of the calls around the projection --reps times "
+                         "(for ncu captures)")
     ap.add_argument("--reps", type=int, default=3)
     return ap.parse_args()
 
@@ -391,14 +395,12 @@ def run_ours(args, ranks):
     replicas.finish(ranks)
 
 
-def post_pass_timings(case, g, p, v, dev, stream):
-    """The calls either side of the projection on the bench grid: before it
-    the momentum predictor and update_vstar_boundary, after it
-    update_boundary_ghost + make_face_gradp.
-    Device time of each call (its launches replayed from a CUDA graph, CUDA
-    events, median of 10, each after an L2 flush) and the algorithmic bytes
-    it moves.  Inputs: the projected pressure and velocity, no-slip walls
-    with an outlet on x+."""
+def around_calls(case, g, p, v, dev):
+    """The calls either side of the projection on the bench grid, as
+    closures, and the algorithmic bytes of each: before it the momentum
+    predictor and update_vstar_boundary, after it update_boundary_ghost +
+    make_face_gradp.  Inputs: pressure p and velocity v (device tensors),
+    no-slip walls with an outlet on x+."""
     import torch
 
     from mydemcfd_b200 import workloads as W
@@ -413,7 +415,6 @@ def post_pass_timings(case, g, p, v, dev, stream):
     gp = [torch.empty(sh[k], dtype=torch.float64, device=dev) for k in "xyz"]
     vs = (g.f_vx_star_, g.f_vy_star_, g.f_vz_star_)
     fb = (g.f_bx_, g.f_by_, g.f_bz_)
-    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
     vs_copy = [t.clone() for t in vs]
     # momentum-predictor fields: the projected velocity as both u and the
     # advecting flux, face viscosities 1e-3, rho_old 1, f_b from the grid
@@ -456,6 +457,16 @@ def post_pass_timings(case, g, p, v, dev, stream):
         # p read once, three face arrays written on the (N+1)^3 box
         "face_gradp": 8 * (ncell + 3 * (nx + 1) * (ny + 1) * (nz + 1)),
     }
+    return calls, alg
+
+
+def post_pass_timings(case, g, p, v, dev, stream):
+    """Device time of each call of around_calls (its launches replayed from a
+    CUDA graph, CUDA events, median of 10, each after an L2 flush) and the
+    algorithmic bytes it moves; p, v the projected pressure and velocity."""
+    import torch
+    calls, alg = around_calls(case, g, p, v, dev)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
     out = {}
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     for name, fn in calls.items():
@@ -475,6 +486,26 @@ def post_pass_timings(case, g, p, v, dev, stream):
         ms = sorted(ts)[len(ts) // 2]
         out[name] = {"us": ms * 1e3, "alg_bytes": alg[name], "GB/s": alg[name] / (ms / 1e3) / 1e9}
     return out
+
+
+def run_around(args):
+    """Set up the bench grid and launch one call of around_calls --reps
+    times: a small, self-contained command for ncu captures.  p is a seeded
+    U[-1,1) field, v the seeded u*."""
+    import torch
+
+    from mydemcfd_b200 import workloads as W
+    from mydemcfd_b200.solver import DeviceGrid
+    case = build_case(args)
+    g = DeviceGrid.from_case(case)
+    sh = W.shapes(case.N)
+    p = torch.from_numpy(W.uniform_pm1(77, int(np.prod(sh["cell"]))).reshape(sh["cell"])).cuda()
+    v = (g.f_vx_star_, g.f_vy_star_, g.f_vz_star_)
+    calls, alg = around_calls(case, g, p, [t.clone() for t in v], torch.device("cuda"))
+    for _ in range(args.reps):
+        calls[args.around]()
+    torch.cuda.synchronize()
+    print(json.dumps({"call": args.around, "n": args.n, "reps": args.reps, "alg_bytes": alg[args.around]}))
 
 
 def run_kernel_only(args):
@@ -498,6 +529,9 @@ def main():
     args = parse()
     if args.kernel_only is not None:
         run_kernel_only(args)
+        return
+    if args.around is not None:
+        run_around(args)
         return
     from mydemcfd_b200 import replicas
     ranks = replicas.from_env()
