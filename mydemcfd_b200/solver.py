@@ -86,6 +86,28 @@ class DeviceGrid:
     f_gradp_x_: torch.Tensor | None = None
     f_gradp_y_: torch.Tensor | None = None
     f_gradp_z_: torch.Tensor | None = None
+    # read by the momentum predictor
+    f_mfx_: torch.Tensor | None = None
+    f_mfy_: torch.Tensor | None = None
+    f_mfz_: torch.Tensor | None = None
+    f_mux_: torch.Tensor | None = None
+    f_muy_: torch.Tensor | None = None
+    f_muz_: torch.Tensor | None = None
+    mu_: torch.Tensor | None = None
+    rho_old_: torch.Tensor | None = None
+    f_coupling_impulse_x_: torch.Tensor | None = None
+    f_coupling_impulse_y_: torch.Tensor | None = None
+    f_coupling_impulse_z_: torch.Tensor | None = None
+    f_ibm_solid_fraction_x_: torch.Tensor | None = None
+    f_ibm_solid_fraction_y_: torch.Tensor | None = None
+    f_ibm_solid_fraction_z_: torch.Tensor | None = None
+    # read and written by the surface-tension force
+    alpha_: torch.Tensor | None = None
+    nx_: torch.Tensor | None = None
+    ny_: torch.Tensor | None = None
+    nz_: torch.Tensor | None = None
+    kappa_: torch.Tensor | None = None
+    p_tmp_: torch.Tensor | None = None
 
     @property
     def N(self):
@@ -312,9 +334,11 @@ class BoundaryConditions:
 
 
 class SMACStep:
-    """The G_SMACSolver calls around the seam, in the reference's order
-    (CFD/main.cu:309-317): update_vstar_boundary(), solve_poisson(),
-    correct_vof_velocity(), update_boundary_ghost(), make_face_gradp()."""
+    """The G_SMACSolver calls of a time step, in the reference's order
+    (CFD/main.cu:298-317): calc_surface_tension(sigma),
+    get_vof_vstar_rhouu_consistent(), update_vstar_boundary(),
+    solve_poisson(), correct_vof_velocity(), update_boundary_ghost(),
+    make_face_gradp()."""
 
     def __init__(self, grid: DeviceGrid, dt: float = 1.0, g=(0.0, 0.0, 0.0), bc: BoundaryConditions | None = None):
         self.grid_ = grid
@@ -323,6 +347,43 @@ class SMACStep:
         self.gx_, self.gy_, self.gz_ = (float(x) for x in g)
         self.bc_ = bc
         self.pressure_solver_: B200PressureSolver | None = None
+
+    def get_vof_vstar_rhouu_consistent(self):
+        """G_SMACSolver::get_vof_vstar_rhouu_consistent (CFD/G_SMACSolver.cu:1062-1070):
+        u* into f_v*_star_ from the grid's time-n fields (smac_predict_vstar)."""
+        g = self.grid_
+        need = ("f_mfx_", "f_mfy_", "f_mfz_", "f_mux_", "f_muy_", "f_muz_", "mu_", "rho_old_", "f_xbcid_")
+        if self.bc_ is None or any(getattr(g, k) is None for k in need):
+            raise ValueError("get_vof_vstar_rhouu_consistent needs bc_ and the grid's " + ", ".join(need))
+        f = {"mu": g.mu_, "rho_old": g.rho_old_, "p": g.p_}
+        for ax in "xyz":
+            f["f" + ax + "t"] = getattr(g, f"f_{ax}type_")
+            f["f" + ax + "bcid"] = getattr(g, f"f_{ax}bcid_")
+            f["lam" + ax] = getattr(g, f"f_ibm_area_solid_fraction_{ax}_")
+            f["v" + ax] = getattr(g, f"f_v{ax}_")
+            f["mf" + ax] = getattr(g, f"f_mf{ax}_")
+            f["mu" + ax] = getattr(g, f"f_mu{ax}_")
+            f["fb" + ax] = getattr(g, f"f_b{ax}_")
+            f["imp" + ax] = getattr(g, f"f_coupling_impulse_{ax}_")
+            f["sf" + ax] = getattr(g, f"f_ibm_solid_fraction_{ax}_")
+        predict_vstar_device(g.N, (g.dx_, g.dy_, g.dz_), self.bc_, f, self.dt_, (self.gx_, self.gy_, self.gz_),
+                             (g.f_vx_star_, g.f_vy_star_, g.f_vz_star_))
+
+    def calc_surface_tension(self, sigma: float):
+        """G_SMACSolver::calc_surface_tension (CFD/G_SMACSolver_VoF.cu:435-445):
+        normals, curvature and the face force into f_s*_ (smac_surface_tension);
+        sigma is the grid's sigma_."""
+        g = self.grid_
+        sh = shapes(g.N)
+        dev = g.p_.device
+        for k in ("nx_", "ny_", "nz_", "kappa_", "p_tmp_"):
+            if getattr(g, k) is None:
+                setattr(g, k, torch.zeros(sh["cell"], dtype=torch.float64, device=dev))
+        for ax in "xyz":
+            if getattr(g, f"f_s{ax}_") is None:
+                setattr(g, f"f_s{ax}_", torch.zeros(sh[ax], dtype=torch.float64, device=dev))
+        surface_tension_device(g.N, (g.dx_, g.dy_, g.dz_), g.alpha_, g.celltype_, sigma,
+                               (g.nx_, g.ny_, g.nz_, g.kappa_, g.p_tmp_), (g.f_sx_, g.f_sy_, g.f_sz_))
 
     def update_vstar_boundary(self):
         """G_SMACSolver::update_vstar_boundary (CFD/G_SMACSolver.cu:1044-1052):

@@ -353,3 +353,35 @@ def test_predict_vstar_against_reference_library_128_and_time_256():
     ms = _device_ms(lambda: predict_vstar_device(m.N, m.h, bc, fields, m.dt, m.g, vs))
     print(f"get_vof_vstar_rhouu_consistent 256^3: {ms * 1e3:.1f} us (reference {ref_ms * 1e3:.1f} us)")
     assert ms < ref_ms
+
+
+def test_smac_step_predictor_and_surface_tension_match_oracle():
+    """SMACStep.get_vof_vstar_rhouu_consistent and calc_surface_tension on a
+    DeviceGrid, against the oracle."""
+    m = W.momentum_case((14, 12, 10), seed=9, sides=("x+",), solid_fraction=0.2)
+    sh = W.shapes(m.N)
+    zc = lambda: torch.zeros(sh["cell"], dtype=torch.float64, device="cuda")  # noqa: E731
+    g = DeviceGrid(*m.N, *m.h, *(_cuda(a) for a in m.vs), *(_cuda(a) for a in m.fb), *(_cuda(a) for a in m.fb),
+                   _cuda(m.ct), *(_cuda(a) for a in m.ft), _cuda(m.p), zc(), zc(), *(_cuda(a) for a in m.v))
+    g.f_xbcid_, g.f_ybcid_, g.f_zbcid_ = (_cuda(a) for a in m.bcid)
+    g.f_ibm_area_solid_fraction_x_, g.f_ibm_area_solid_fraction_y_, g.f_ibm_area_solid_fraction_z_ = (
+        _cuda(a) for a in m.lam)
+    g.f_mfx_, g.f_mfy_, g.f_mfz_ = (_cuda(a) for a in m.mf)
+    g.f_mux_, g.f_muy_, g.f_muz_ = (_cuda(a) for a in m.muf)
+    g.mu_, g.rho_old_ = _cuda(m.mu), _cuda(m.rho_old)
+    g.f_coupling_impulse_x_, g.f_coupling_impulse_y_, g.f_coupling_impulse_z_ = (_cuda(a) for a in m.imp)
+    g.f_ibm_solid_fraction_x_, g.f_ibm_solid_fraction_y_, g.f_ibm_solid_fraction_z_ = (_cuda(a) for a in m.sf)
+    step = SMACStep(g, m.dt, g=m.g, bc=BoundaryConditions(m.bc_type, *m.bc_v))
+    step.get_vof_vstar_rhouu_consistent()
+    torch.cuda.synchronize()
+    for a, b in zip((g.f_vx_star_, g.f_vy_star_, g.f_vz_star_), O.predict_vstar(m)):
+        assert np.array_equal(a.cpu().numpy(), b)
+    N, h, alpha, ct, sigma = W.surface_case(m.N, seed=9, kind="sphere", h=m.h[0])
+    g.alpha_ = _cuda(alpha)
+    g.celltype_ = _cuda(ct)
+    step.calc_surface_tension(sigma)
+    torch.cuda.synchronize()
+    want = O.surface_tension(N, h, alpha, ct, sigma)
+    got = (g.f_sx_, g.f_sy_, g.f_sz_, g.nx_, g.ny_, g.nz_, g.kappa_, g.p_tmp_)
+    for k, a, b in zip(("fsx", "fsy", "fsz", "nx", "ny", "nz", "kappa", "gm"), got, want):
+        assert np.array_equal(a.cpu().numpy(), b), k
