@@ -369,6 +369,7 @@ def post_case(N, seed, h=(0.03125, 0.03125, 0.03125), dt=0.5, g=(0.0, -1.5, -9.8
 
 
 def surface_case(N, seed, kind="sphere", solid_fraction=0.0, sigma=0.07, h=0.03125):
+    # h: one spacing, or three (powers of two keep the reference's (N h) / N exact)
     """Inputs of the surface-tension force: (N, h, alpha, ct, sigma).
     kind "sphere": a sphere of radius 0.3 of the smallest extent, centred
     U[0.35, 0.65] of the box, alpha ramped over 1.5 cells; kind "random":
@@ -377,13 +378,13 @@ def surface_case(N, seed, kind="sphere", solid_fraction=0.0, sigma=0.07, h=0.031
     2..N-1 C_SOLID (single cells).  h is a power of two, so the reference's
     spacing (N h) / N equals it."""
     N = tuple(int(n) for n in N)
-    hh = (float(h),) * 3
+    hh = tuple(float(x) for x in h) if np.ndim(h) else (float(h),) * 3
     sh = shapes(N)
     ncell = int(np.prod(sh["cell"]))
     ct, fxt, fyt, fzt = box_types(N)
     if kind == "sphere":
         u = uniform01(substream(seed, 80), 3)
-        ext = np.array(N, np.float64) * h
+        ext = np.array(N, np.float64) * np.array(hh)
         centre = (0.35 + 0.3 * u) * ext
         alpha = sphere_alpha(N, hh, centre, 0.3 * ext.min(), 1.5)
     else:
@@ -431,15 +432,16 @@ class MomentumCase:
     vs: tuple      # f_v*_star_ before the call (faces it does not write keep these)
 
 
-def momentum_case(N, seed, sides=("x+", "z-"), solid_fraction=0.0, extras=True, dt=0.01, g=(0.0, 0.0, -9.8)):
+def momentum_case(N, seed, sides=("x+", "z-"), solid_fraction=0.0, extras=True, dt=0.01, g=(0.0, 0.0, -9.8),
+                  h=(0.03125, 0.03125, 0.03125)):
     """Seeded momentum-predictor inputs on the boundary set-up of post_case
     (all five boundary types, outlets on `sides`, clustered solids).  Fields:
     v, v* U[-1,1); mf U[-1,1) with 10% exact zeros (the flux-sign ties);
     face and cell viscosities U[1e-3, 1e-2); rho_old U[1, 1000); p U[-1,1);
     f_b U[1e-3, 1); with extras the coupling impulse U[-1e-6, 1e-6), the IBM
     area and solid fractions U[0,1) with half of them 0."""
-    base = post_case(N, seed, h=(0.03125, 0.03125, 0.03125), dt=dt, g=g, sides=sides, solid_fraction=solid_fraction,
-                     lam=extras, solid_margin=3)
+    base = post_case(N, seed, h=h, dt=dt, g=g, sides=sides, solid_fraction=solid_fraction, lam=extras,
+                     solid_margin=3)
     sh = shapes(base.N)
 
     def rnd(tag, key, lo=-1.0, hi=1.0):

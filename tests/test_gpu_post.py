@@ -385,3 +385,27 @@ def test_smac_step_predictor_and_surface_tension_match_oracle():
     got = (g.f_sx_, g.f_sy_, g.f_sz_, g.nx_, g.ny_, g.nz_, g.kappa_, g.p_tmp_)
     for k, a, b in zip(("fsx", "fsy", "fsz", "nx", "ny", "nz", "kappa", "gm"), got, want):
         assert np.array_equal(a.cpu().numpy(), b), k
+
+
+ANISO = (0.03125, 0.0625, 0.015625)  # powers of two: the reference's (N h) / N is exact
+
+
+@pytest.mark.skipif(not REF.available(), reason="reference build oracle/_ref not present")
+def test_anisotropic_spacing_bit_exact_against_reference_library():
+    """The calls around the projection with hx != hy != hz, against the
+    reference's kernels directly: predictor, surface tension, wall u* rule,
+    ghost/gradient pass."""
+    m = W.momentum_case((24, 20, 16), seed=11, sides=("x-", "z+"), solid_fraction=0.2, h=ANISO)
+    *ref, _ = REF.predict_vstar(m)
+    for k, a, b in zip(("vxs", "vys", "vzs"), run_predict(m), ref):
+        assert np.array_equal(a, b), k
+    N, h, alpha, ct, sigma = W.surface_case((20, 16, 24), seed=12, kind="sphere", solid_fraction=0.05, h=ANISO)
+    *ref, _ = REF.surface_tension(N, h, alpha, ct, sigma)
+    for k, a, b in zip(ST_KEYS, run_surface(N, h, alpha, ct, sigma), ref):
+        assert np.array_equal(a, b), k
+    c = W.post_case((18, 22, 14), seed=13, h=ANISO, sides=("y+", "z-"), solid_fraction=0.2, solid_margin=3)
+    r = REF.post(c)
+    _assert_equal(run_post(c), (r["p"], (r["vx"], r["vy"], r["vz"]), (r["gpx"], r["gpy"], r["gpz"])))
+    *ref, _ = REF.vstar(c)
+    for k, a, b in zip(("vxs", "vys", "vzs"), run_vstar(c), ref):
+        assert np.array_equal(a, b), k
