@@ -148,6 +148,38 @@ smac_status smac_assemble_vof(const smac_grid_desc* desc, const double* alpha, d
                               const uint8_t* fzt, double* rho, double* fbx, double* fby, double* fbz,
                               double* firx, double* firy, double* firz, void* cuda_stream);
 
+/* The two phases' densities and viscosities (G_SMACSolver::rho0_, rho1_,
+ * mu0_, mu1_; alpha = 1 is phase 1). */
+typedef struct {
+  double rho0, rho1, mu0, mu1;
+} smac_vof_params;
+
+/* Outputs of the property update (device pointers, reference layout); the
+ * marked ones may be NULL (not written). */
+typedef struct {
+  double *rho, *inv_rho, *mu;       /* cells: rho_, inv_rho_ (NULL ok), mu_ */
+  double *fbx, *fby, *fbz;          /* f_b*_ */
+  double *firx, *firy, *firz;       /* f_inv_rho*_ (NULL ok) */
+  double *rhox, *rhoy, *rhoz;       /* f_rho*_ (NULL ok) */
+  double *mux, *muy, *muz;          /* f_mu*_: the face viscosities the momentum predictor reads */
+} smac_property_fields;
+
+/* The whole property update, G_SMACSolver::update_properties_by_alpha
+ * (CFD/G_SMACSolver_VoF.cu:1543-1566), after its swap of rho_ and rho_old_
+ * (the caller swaps its two arrays):
+ *  - C_INTERIOR / C_NEAR_BOUNDARY cells 1..N+1: rho and mu linear in alpha,
+ *    inv_rho = 1/rho (:1374-1407);
+ *  - C_SOLID interior cells: rho and mu of the first C_INTERIOR neighbour
+ *    (x-, x+, y-, y+, z-, z+; 0 without one); ghost cells: those of the
+ *    nearest interior cell (:1241-1372, their final state);
+ *  - F_INTERIOR faces: rho_f = the two cells' mean, f_b = f_inv_rho =
+ *    1/rho_f, mu_f = the mean viscosity; other faces with indices 1..N+2
+ *    along, 1..N+1 across: f_b = f_inv_rho = 0 (:1409-1535).
+ * smac_assemble_vof is the subset that feeds the pressure operator. */
+smac_status smac_update_properties(const smac_grid_desc* d, const smac_vof_params* vp, const double* alpha,
+                                   const uint8_t* celltype, const uint8_t* fxt, const uint8_t* fyt, const uint8_t* fzt,
+                                   const smac_property_fields* out, void* stream);
+
 /* Outlet boundary faces: f_b = 2 f_b of the neighbouring face on the interior
  * side, where p = 0 is imposed.  G_SMACSolver::update_boundary_faces
  * (CFD/G_SMACSolver_VoF.cu:1798-1950), run after smac_assemble_vof.  The

@@ -63,6 +63,17 @@ class MomentumFields(ctypes.Structure):
         "impx", "impy", "impz", "sfx", "sfy", "sfz")]
 
 
+class VofParams(ctypes.Structure):
+    _fields_ = [(k, ctypes.c_double) for k in ("rho0", "rho1", "mu0", "mu1")]
+
+
+class PropertyFields(ctypes.Structure):
+    """smac_property_fields: the outputs of the property update."""
+    _fields_ = [(k, ctypes.c_void_p) for k in (
+        "rho", "inv_rho", "mu", "fbx", "fby", "fbz", "firx", "firy", "firz", "rhox", "rhoy", "rhoz",
+        "mux", "muy", "muz")]
+
+
 class SmacError(RuntimeError):
     def __init__(self, status, msg):
         super().__init__(f"{STATUS_NAMES.get(status, status)}: {msg}")
@@ -80,7 +91,7 @@ EXPORTS = [
     "smac_selftest_sweep", "smac_apply_A_dot_noalloc", "smac_async_create", "smac_async_submit",
     "smac_async_wait", "smac_async_destroy", "smac_update_boundary_faces", "smac_update_pressure_ghost",
     "smac_update_velocity_ghost", "smac_face_gradp", "smac_update_vstar_boundary", "smac_surface_tension",
-    "smac_predict_vstar", "smac_vti_block_bytes", "smac_vti_pack", "smac_vti_write",
+    "smac_predict_vstar", "smac_vti_block_bytes", "smac_vti_pack", "smac_vti_write", "smac_update_properties",
 ]
 
 
@@ -129,6 +140,8 @@ def load(path: str = LIB_PATH):
         "smac_predict_vstar": [ctypes.POINTER(GridDesc), ctypes.POINTER(BoundaryTable), ctypes.POINTER(MomentumFields),
                                d, d, d, d, dp, dp, dp, vp],
         "smac_vti_pack": [ctypes.POINTER(GridDesc), dp, dp, dp, dp, dp, dp, vp, vp],
+        "smac_update_properties": [ctypes.POINTER(GridDesc), ctypes.POINTER(VofParams), dp, u8p, u8p, u8p, u8p,
+                                   ctypes.POINTER(PropertyFields), vp],
         "smac_vti_write": [ctypes.POINTER(GridDesc), ctypes.POINTER(d), vp, ctypes.c_char_p],
         "smac_update_vstar_boundary": [ctypes.POINTER(GridDesc), ctypes.POINTER(BoundaryTable), u8p, u8p, u8p, u8p,
                                        u8p, u8p, u8p, u8p, u8p, dp, dp, dp, dp, dp, dp, vp],

@@ -925,6 +925,156 @@ __global__ void __launch_bounds__(256, 5) k_predict_vstar(MomArgs A) {
   }
 }
 
+// ---------------------------------------------------------------------------
+// Property update (G_SMACSolver::update_properties_by_alpha,
+// CFD/G_SMACSolver_VoF.cu:1241-1566)
+
+struct PropArgs {
+  RefDims R;
+  const double* alpha;
+  const uint8_t* ct;
+  const uint8_t* ft[3];
+  double* rho;
+  double* inv_rho;  // nullptr: not written
+  double* mu;
+  double* fb[3];
+  double* fir[3];   // nullptr: not written
+  double* frho[3];  // nullptr: not written
+  double* fmu[3];
+  double rho0, rho1, mu0, mu1;
+  long long ncell;
+  Shape2 shape;
+  int scan_blocks;
+  int gz_bx, gz_by, gy_bx, gy_bz, gx_by, gx_bz;
+};
+
+// Pass 1, k_update_cell_properties_by_alpha (:1374-1407): C_INTERIOR and
+// C_NEAR_BOUNDARY cells with indices 1..N+1.
+__global__ void __launch_bounds__(256) k_props_cells(PropArgs A) {
+  const RefDims& R = A.R;
+  const int x = blockIdx.x * 32 + threadIdx.x + 1, y = blockIdx.y * 8 + threadIdx.y + 1, z = blockIdx.z + 1;
+  if (x > R.Nx + 1 || y > R.Ny + 1) return;
+  const long long c = R.cell(x, y, z);
+  const uint8_t t = A.ct[c];
+  if (t != 0 && t != 1) return;  // C_INTERIOR, C_NEAR_BOUNDARY
+  const double a = A.alpha[c];
+  const double r = DADD(DMUL(DSUB(1.0, a), A.rho0), DMUL(a, A.rho1));
+  A.rho[c] = r;
+  if (A.inv_rho) A.inv_rho[c] = __ddiv_rn(1.0, r);
+  A.mu[c] = DADD(DMUL(DSUB(1.0, a), A.mu0), DMUL(a, A.mu1));
+}
+
+// rho and mu of the C_SOLID interior cell c: those of its first C_INTERIOR
+// neighbour (x-, x+, y-, y+, z-, z+), 0 without one
+// (k_update_cell_boundary_properties_by_alpha :1288-1340).
+__device__ __forceinline__ void solid_props(const PropArgs& A, long long c, double& r, double& m) {
+  const long long sx = A.R.Nx + 2, sxy = sx * (A.R.Ny + 2);
+  const long long nb[6] = {c - 1, c + 1, c - sx, c + sx, c - sxy, c + sxy};
+  const uint8_t t[6] = {A.ct[nb[0]], A.ct[nb[1]], A.ct[nb[2]], A.ct[nb[3]], A.ct[nb[4]], A.ct[nb[5]]};
+  r = 0.0;
+  m = 0.0;
+#pragma unroll
+  for (int k = 0; k < 6; ++k)
+    if (t[k] == kInterior) {
+      r = A.rho[nb[k]];
+      m = A.mu[nb[k]];
+      return;
+    }
+}
+
+// Pass 2: the final state of k_update_cell_boundary_properties_by_alpha +
+// k_update_cell_ghost_properties.  Scan blocks find the interior C_SOLID
+// cells; the other blocks take the ghost cells (2-D groups as in
+// k_pressure_ghost), each copying its nearest interior cell, computing that
+// cell's value itself if it is C_SOLID (its own neighbours are never
+// written here).
+__global__ void __launch_bounds__(kPostThreads) k_props_ghost(PropArgs A) {
+  const RefDims& R = A.R;
+  if ((int)blockIdx.x < A.scan_blocks) {
+    const long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long long nth = (long long)A.scan_blocks * blockDim.x;
+    __shared__ long long queue[kPostWarps * SCAN_QUEUE];
+    scan_compact<kSolid>(A.ct, A.ncell, tid, nth, queue + (threadIdx.x >> 5) * SCAN_QUEUE, [&](long long i) {
+      const Pos q = decode(i, A.shape);
+      if (q.x < 1 || q.x > R.Nx || q.y < 1 || q.y > R.Ny || q.z < 1 || q.z > R.Nz) return;
+      double r, m;
+      solid_props(A, i, r, m);
+      A.rho[i] = r;
+      A.mu[i] = m;
+    });
+    return;
+  }
+  int b = (int)blockIdx.x - A.scan_blocks;
+  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+  const int nz_blocks = 2 * A.gz_bx * A.gz_by, ny_blocks = 2 * A.gy_bx * A.gy_bz;
+  int ix, iy, iz;
+  if (b < nz_blocks) {
+    const int side = b / (A.gz_bx * A.gz_by);
+    b -= side * A.gz_bx * A.gz_by;
+    ix = (b % A.gz_bx) * 32 + tx;
+    iy = (b / A.gz_bx) * 8 + ty;
+    iz = side ? R.Nz + 1 : 0;
+    if (ix >= R.Nx + 2 || iy >= R.Ny + 2) return;
+  } else if ((b -= nz_blocks) < ny_blocks) {
+    const int side = b / (A.gy_bx * A.gy_bz);
+    b -= side * A.gy_bx * A.gy_bz;
+    ix = (b % A.gy_bx) * 32 + tx;
+    iz = 1 + (b / A.gy_bx) * 8 + ty;
+    iy = side ? R.Ny + 1 : 0;
+    if (ix >= R.Nx + 2 || iz > R.Nz) return;
+  } else {
+    b -= ny_blocks;
+    const int side = b / (A.gx_by * A.gx_bz);
+    b -= side * A.gx_by * A.gx_bz;
+    iy = 1 + (b % A.gx_by) * 32 + tx;
+    iz = 1 + (b / A.gx_by) * 8 + ty;
+    ix = side ? R.Nx + 1 : 0;
+    if (iy > R.Ny || iz > R.Nz) return;
+  }
+  const int sx_ = ix == 0 ? 1 : ix == R.Nx + 1 ? R.Nx : ix;
+  const int sy_ = iy == 0 ? 1 : iy == R.Ny + 1 ? R.Ny : iy;
+  const int sz_ = iz == 0 ? 1 : iz == R.Nz + 1 ? R.Nz : iz;
+  const long long s = R.cell(sx_, sy_, sz_), g = R.cell(ix, iy, iz);
+  double r = A.rho[s], m = A.mu[s];
+  if (A.ct[s] == kSolid) solid_props(A, s, r, m);
+  A.rho[g] = r;
+  A.mu[g] = m;
+}
+
+// Pass 3, k_update_{x,y,z}_face_properties_by_alpha (:1409-1535): one thread
+// per face index of the box 1..N+2 (each family up to its own extent).
+template <int F>
+__device__ __forceinline__ void face_props(const PropArgs& A, int x, int y, int z) {
+  const RefDims& R = A.R;
+  const long long S0 = R.Nx + 2 + (F == 0), S1 = R.Ny + 2 + (F == 1);
+  const long long f = ((long long)z * S1 + y) * S0 + x;
+  const int along = F == 0 ? x : F == 1 ? y : z, n_along = F == 0 ? R.Nx : F == 1 ? R.Ny : R.Nz;
+  // (a face at N+2 has no cell on its high side; typed F_INTERIOR it would
+  // be invalid input, and it is treated as a wall face)
+  if (A.ft[F][f] != 0 || along > n_along + 1) {
+    A.fb[F][f] = 0.0;
+    if (A.fir[F]) A.fir[F][f] = 0.0;
+    return;
+  }
+  const long long c = R.cell(x, y, z);
+  const long long cm = c - (F == 0 ? 1 : F == 1 ? (long long)(R.Nx + 2) : (long long)(R.Nx + 2) * (R.Ny + 2));
+  const double fr = DMUL(0.5, DADD(A.rho[c], A.rho[cm]));
+  if (A.frho[F]) A.frho[F][f] = fr;
+  const double b = __ddiv_rn(1.0, fr);
+  A.fb[F][f] = b;
+  if (A.fir[F]) A.fir[F][f] = b;
+  A.fmu[F][f] = DMUL(0.5, DADD(A.mu[c], A.mu[cm]));
+}
+
+__global__ void __launch_bounds__(256) k_props_faces(PropArgs A) {
+  const RefDims& R = A.R;
+  const int x = blockIdx.x * 32 + threadIdx.x + 1, y = blockIdx.y * 8 + threadIdx.y + 1, z = blockIdx.z + 1;
+  const bool xin = x <= R.Nx + 1, yin = y <= R.Ny + 1, zin = z <= R.Nz + 1;
+  if (x <= R.Nx + 2 && yin && zin) face_props<0>(A, x, y, z);
+  if (xin && y <= R.Ny + 2 && zin) face_props<1>(A, x, y, z);
+  if (xin && yin && z <= R.Nz + 2) face_props<2>(A, x, y, z);
+}
+
 int sm_count() {
   static int n = 0;
   if (!n) {
@@ -1175,6 +1325,45 @@ smac_status smac_predict_vstar(const smac_grid_desc* d, const smac_boundary_tabl
   fill_table(&A.bc, bc);
   const dim3 grid((unsigned)((d->nx + 1 + 31) / 32), (unsigned)((d->ny + 1 + 7) / 8), 3u * (unsigned)(d->nz + 1));
   k_predict_vstar<<<grid, dim3(32, 8), 0, (cudaStream_t)stream>>>(A);
+  return launch_status(fn);
+}
+
+smac_status smac_update_properties(const smac_grid_desc* d, const smac_vof_params* vp, const double* alpha,
+                                   const uint8_t* celltype, const uint8_t* fxt, const uint8_t* fyt, const uint8_t* fzt,
+                                   const smac_property_fields* out, void* stream) {
+  static const char* fn = "smac_update_properties";
+  if (!d || !vp || !alpha || !celltype || !fxt || !fyt || !fzt || !out || !out->rho || !out->mu || !out->fbx ||
+      !out->fby || !out->fbz || !out->mux || !out->muy || !out->muz) {
+    smac::set_error_text("%s: null argument", fn);
+    return SMAC_BAD_ARG;
+  }
+  if (bad_desc(d, fn, 1)) return SMAC_BAD_SHAPE;
+  PropArgs A;
+  std::memset(&A, 0, sizeof(A));
+  A.R = RefDims{d->nx, d->ny, d->nz};
+  A.alpha = alpha;
+  A.ct = celltype;
+  A.ft[0] = fxt; A.ft[1] = fyt; A.ft[2] = fzt;
+  A.rho = out->rho; A.inv_rho = out->inv_rho; A.mu = out->mu;
+  A.fb[0] = out->fbx; A.fb[1] = out->fby; A.fb[2] = out->fbz;
+  A.fir[0] = out->firx; A.fir[1] = out->firy; A.fir[2] = out->firz;
+  A.frho[0] = out->rhox; A.frho[1] = out->rhoy; A.frho[2] = out->rhoz;
+  A.fmu[0] = out->mux; A.fmu[1] = out->muy; A.fmu[2] = out->muz;
+  A.rho0 = vp->rho0; A.rho1 = vp->rho1; A.mu0 = vp->mu0; A.mu1 = vp->mu1;
+  const long long sx = d->nx + 2, sy = d->ny + 2, sz = d->nz + 2;
+  A.ncell = sx * sy * sz;
+  A.shape = make_shape2(sx, sy, A.ncell);
+  A.scan_blocks = scan_blocks_for(A.ncell, sm_count());
+  A.gz_bx = (int)((sx + 31) / 32); A.gz_by = (int)((sy + 7) / 8);
+  A.gy_bx = (int)((sx + 31) / 32); A.gy_bz = (d->nz + 7) / 8;
+  A.gx_by = (d->ny + 31) / 32;     A.gx_bz = (d->nz + 7) / 8;
+  const long long ghost_blocks = 2LL * (A.gz_bx * A.gz_by + A.gy_bx * A.gy_bz + A.gx_by * A.gx_bz);
+  cudaStream_t s = (cudaStream_t)stream;
+  k_props_cells<<<dim3((unsigned)((d->nx + 1 + 31) / 32), (unsigned)((d->ny + 1 + 7) / 8), (unsigned)(d->nz + 1)),
+                  dim3(32, 8), 0, s>>>(A);
+  k_props_ghost<<<(unsigned)(A.scan_blocks + ghost_blocks), kPostThreads, 0, s>>>(A);
+  k_props_faces<<<dim3((unsigned)((d->nx + 2 + 31) / 32), (unsigned)((d->ny + 2 + 7) / 8), (unsigned)(d->nz + 2)),
+                  dim3(32, 8), 0, s>>>(A);
   return launch_status(fn);
 }
 

@@ -95,6 +95,11 @@ class DeviceGrid:
     f_muz_: torch.Tensor | None = None
     mu_: torch.Tensor | None = None
     rho_old_: torch.Tensor | None = None
+    # written by the property update (besides rho_, mu_, f_b*_, f_inv_rho*_, f_mu*_)
+    inv_rho_: torch.Tensor | None = None
+    f_rhox_: torch.Tensor | None = None
+    f_rhoy_: torch.Tensor | None = None
+    f_rhoz_: torch.Tensor | None = None
     f_coupling_impulse_x_: torch.Tensor | None = None
     f_coupling_impulse_y_: torch.Tensor | None = None
     f_coupling_impulse_z_: torch.Tensor | None = None
@@ -369,6 +374,34 @@ class SMACStep:
         predict_vstar_device(g.N, (g.dx_, g.dy_, g.dz_), self.bc_, f, self.dt_, (self.gx_, self.gy_, self.gz_),
                              (g.f_vx_star_, g.f_vy_star_, g.f_vz_star_))
 
+    def update_properties_by_alpha(self, rho0: float, rho1: float, mu0: float, mu1: float):
+        """G_SMACSolver::update_properties_by_alpha (CFD/G_SMACSolver_VoF.cu:1544-1566):
+        rho_ and rho_old_ swap (the previous rho is kept as rho_old_), then
+        rho, 1/rho, mu of the cells and 1/rho (f_b and f_inv_rho), rho, mu of
+        the faces from alpha_ (smac_update_properties).  Missing outputs are
+        allocated."""
+        g = self.grid_
+        if g.alpha_ is None:
+            raise ValueError("update_properties_by_alpha needs the grid's alpha_")
+        sh = shapes(g.N)
+        dev = g.p_.device
+        for k in ("rho_", "rho_old_", "inv_rho_", "mu_"):
+            if getattr(g, k) is None:
+                setattr(g, k, torch.zeros(sh["cell"], dtype=torch.float64, device=dev))
+        for ax in "xyz":
+            for k in (f"f_b{ax}_", f"f_inv_rho{ax}_", f"f_rho{ax}_", f"f_mu{ax}_"):
+                if getattr(g, k) is None:
+                    setattr(g, k, torch.zeros(sh[ax], dtype=torch.float64, device=dev))
+        g.rho_, g.rho_old_ = g.rho_old_, g.rho_
+        out = {"rho": g.rho_, "inv_rho": g.inv_rho_, "mu": g.mu_}
+        for ax in "xyz":
+            out["fb" + ax] = getattr(g, f"f_b{ax}_")
+            out["fir" + ax] = getattr(g, f"f_inv_rho{ax}_")
+            out["rho" + ax] = getattr(g, f"f_rho{ax}_")
+            out["mu" + ax] = getattr(g, f"f_mu{ax}_")
+        update_properties_device(g.N, (g.dx_, g.dy_, g.dz_), rho0, rho1, mu0, mu1, g.alpha_, g.celltype_,
+                                 (g.f_xtype_, g.f_ytype_, g.f_ztype_), out)
+
     def calc_surface_tension(self, sigma: float):
         """G_SMACSolver::calc_surface_tension (CFD/G_SMACSolver_VoF.cu:435-445):
         normals, curvature and the face force into f_s*_ (smac_surface_tension);
@@ -552,6 +585,21 @@ def predict_vstar_device(N, h, bc: BoundaryConditions, fields: dict, dt, g, vs):
     nat.check(nat.load().smac_predict_vstar(ctypes.byref(d), ctypes.byref(table), ctypes.byref(mf), dd(dt), dd(g[0]),
                                             dd(g[1]), dd(g[2]), *map(_ptr, vs), ctypes.c_void_p(s)))
     del keep
+
+
+def update_properties_device(N, h, rho0, rho1, mu0, mu1, alpha, ct, ft, out: dict):
+    """smac_update_properties: out maps the smac_property_fields names (rho,
+    inv_rho, mu, fbx.., firx.., rhox.., mux..) to CUDA tensors written in place;
+    inv_rho, fir*, rho{x,y,z} may be missing."""
+    d = nat.GridDesc(*N, *h)
+    s = torch.cuda.current_stream().cuda_stream
+    f = nat.PropertyFields()
+    for name, _ in nat.PropertyFields._fields_:
+        t = out.get(name)
+        setattr(f, name, None if t is None else _ptr(t).value)
+    vp = nat.VofParams(rho0, rho1, mu0, mu1)
+    nat.check(nat.load().smac_update_properties(ctypes.byref(d), ctypes.byref(vp), _ptr(alpha), _ptr(ct),
+                                                *map(_ptr, ft), ctypes.byref(f), ctypes.c_void_p(s)))
 
 
 def face_gradp_device(N, h, p, gp):

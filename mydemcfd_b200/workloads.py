@@ -471,3 +471,29 @@ def momentum_case(N, seed, sides=("x+", "z-"), solid_fraction=0.0, extras=True, 
         fb=tuple(rnd(150 + k, key, 1e-3, 1.0) for k, key in enumerate("xyz")),
         imp=extra(160, -1e-6, 1e-6), sf=extra(180, 0.0, 1.0),
         vs=tuple(rnd(200 + k, key) for k, key in enumerate("xyz")))
+
+
+PROPERTY_KEYS = ("rho", "rho_old", "inv_rho", "mu", "fbx", "fby", "fbz", "firx", "firy", "firz", "rhox", "rhoy",
+                 "rhoz", "mux", "muy", "muz")
+
+
+def property_case(N, seed, solid_fraction=0.0, rho=(1.0, 1000.0), mu=(1e-3, 1e-1)):
+    """Inputs of the property update: alpha of a seeded sphere (1.5-cell
+    ramp) plus 20% of the cells U[0,1); box types with clustered solids
+    (post_case's rule); every output array filled with U[-1,1) beforehand,
+    so that entries the update must not write are checked too.  Returns
+    (N, h, (rho0, rho1, mu0, mu1), alpha, ct, ft, init)."""
+    base = post_case(N, seed, sides=(), solid_fraction=solid_fraction)
+    N = base.N
+    sh = shapes(N)
+    n = int(np.prod(sh["cell"]))
+    u = uniform01(substream(seed, 300), 3)
+    ext = np.array(N, np.float64) * np.array(base.h)
+    alpha = sphere_alpha(N, base.h, (0.3 + 0.4 * u) * ext, 0.25 * ext.min(), 1.5)
+    mix = uniform01(substream(seed, 301), n).reshape(sh["cell"]) < 0.2
+    alpha = np.where(mix, uniform01(substream(seed, 302), n).reshape(sh["cell"]), alpha)
+    init = {}
+    for k, key in enumerate(PROPERTY_KEYS):
+        kind = "cell" if key in ("rho", "rho_old", "inv_rho", "mu") else key[-1]
+        init[key] = uniform_pm1(substream(seed, 310 + k), int(np.prod(sh[kind]))).reshape(sh[kind])
+    return N, base.h, (rho[0], rho[1], mu[0], mu[1]), np.ascontiguousarray(alpha), base.ct, base.ft, init

@@ -399,3 +399,23 @@ def vti_block(N, p, alpha, vx, vy, vz, ibm_sf):
         parts.append(np.array([4 * cnt], np.uint32).tobytes())
         parts.append(vel.tobytes() if arr is None else arr[inner].astype(np.float32).reshape(-1).tobytes())
     return b"".join(parts)
+
+
+PROP_KEYS = ("rho", "inv_rho", "mu", "fbx", "fby", "fbz", "firx", "firy", "firz", "rhox", "rhoy", "rhoz",
+             "mux", "muy", "muz")
+
+
+def update_properties(N, rho0, rho1, mu0, mu1, alpha, ct, ft, init):
+    """G_SMACSolver::update_properties_by_alpha (CFD/G_SMACSolver_VoF.cu:1543-1566)
+    after its rho/rho_old swap, on copies of the arrays in `init` (a dict
+    with every PROP_KEYS entry); returns the updated dict."""
+    out = {k: np.array(init[k], dtype=np.float64, order="C", copy=True) for k in PROP_KEYS}
+    p3 = lambda ks: (ctypes.c_void_p * 3)(*(out[k].ctypes.data for k in ks))  # noqa: E731
+    fts = [np.ascontiguousarray(t, np.uint8) for t in ft]
+    c = ctypes.c_double
+    lib().orc_update_properties(*N, c(rho0), c(rho1), c(mu0), c(mu1), _p(np.ascontiguousarray(alpha, np.float64)),
+                                _u8(np.ascontiguousarray(ct, np.uint8)),
+                                (ctypes.c_void_p * 3)(*(t.ctypes.data for t in fts)), _p(out["rho"]),
+                                _p(out["inv_rho"]), _p(out["mu"]), p3(("fbx", "fby", "fbz")),
+                                p3(("firx", "firy", "firz")), p3(("rhox", "rhoy", "rhoz")), p3(("mux", "muy", "muz")))
+    return out

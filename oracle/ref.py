@@ -327,3 +327,43 @@ def write_vti(N, h, origin, p, alpha, vx, vy, vz, ibm_sf, outdir, step):
     if rc != 0:
         raise RuntimeError(f"ref_write_vti returned {rc}")
     return os.path.join(str(outdir), f"result_{int(step):06d}.vti")
+
+
+class RefPropsIO(ctypes.Structure):
+    _fields_ = [("Nx", ctypes.c_int), ("Ny", ctypes.c_int), ("Nz", ctypes.c_int)] + \
+        [(k, ctypes.c_double) for k in ("Lx", "Ly", "Lz", "rho0", "rho1", "mu0", "mu1")] + \
+        [("alpha", _dp), ("ct", _u8p), ("ft", ctypes.c_void_p * 3)] + \
+        [(k, _dp) for k in ("rho", "rho_old", "inv_rho", "mu")] + \
+        [(k, ctypes.c_void_p * 3) for k in ("fb", "fir", "frho", "fmu")] + [("ms", ctypes.c_double)]
+
+
+def update_properties(N, h, rho0, rho1, mu0, mu1, alpha, ct, ft, init):
+    """Run the reference's update_properties_by_alpha.  init: dict with the
+    arrays before the call (keys of oracle.PROP_KEYS plus rho_old, which the
+    reference's swap turns into rho); returns the dict after it (rho_old
+    holds the previous rho) and the device time."""
+    L = lib()
+    if not hasattr(L, "_props_set"):
+        L.ref_update_properties.restype = ctypes.c_int
+        L.ref_update_properties.argtypes = [ctypes.POINTER(RefPropsIO)]
+        L._props_set = True
+    keys = ("rho", "rho_old", "inv_rho", "mu", "fbx", "fby", "fbz", "firx", "firy", "firz", "rhox", "rhoy", "rhoz",
+            "mux", "muy", "muz")
+    out = {k: np.array(init[k], dtype=np.float64, order="C", copy=True) for k in keys}
+    keep = [np.ascontiguousarray(alpha, np.float64), np.ascontiguousarray(ct, np.uint8)] + \
+        [np.ascontiguousarray(t, np.uint8) for t in ft]
+    io = RefPropsIO()
+    io.Nx, io.Ny, io.Nz = N
+    io.Lx, io.Ly, io.Lz = (n * hh for n, hh in zip(N, h))
+    io.rho0, io.rho1, io.mu0, io.mu1 = rho0, rho1, mu0, mu1
+    io.alpha, io.ct = _p(keep[0]), _p(keep[1], ctypes.c_uint8)
+    io.ft = (ctypes.c_void_p * 3)(*(t.ctypes.data for t in keep[2:]))
+    for k in ("rho", "rho_old", "inv_rho", "mu"):
+        setattr(io, k, _p(out[k]))
+    for name, ks in (("fb", ("fbx", "fby", "fbz")), ("fir", ("firx", "firy", "firz")),
+                     ("frho", ("rhox", "rhoy", "rhoz")), ("fmu", ("mux", "muy", "muz"))):
+        setattr(io, name, (ctypes.c_void_p * 3)(*(out[k].ctypes.data for k in ks)))
+    rc = L.ref_update_properties(ctypes.byref(io))
+    if rc != 0:
+        raise RuntimeError(f"ref_update_properties returned {rc}")
+    return out, io.ms

@@ -9,7 +9,8 @@
 // G_PCGSolver + G_GMGSolver::initialize, set_solver, tol_, then
 // G_SMACSolver::solve_poisson() and correct_vof_velocity().  More entries
 // run the calls either side of it on given arrays: ref_predict_vstar
-// (get_vof_vstar_rhouu_consistent), ref_vstar (update_vstar_boundary),
+// (get_vof_vstar_rhouu_consistent), ref_update_properties
+// (update_properties_by_alpha), ref_vstar (update_vstar_boundary),
 // ref_surface_tension (calc_surface_tension) and ref_post
 // (update_boundary_ghost and make_face_gradp).
 //
@@ -431,6 +432,67 @@ int ref_predict_vstar(ref_mom_io* io) {
   if (e == cudaSuccess) {
     g.gpuTocpu(solv.grid_);
     get(hg.f_vx_star_, io->vs[0]); get(hg.f_vy_star_, io->vs[1]); get(hg.f_vz_star_, io->vs[2]);
+    e = cudaGetLastError();
+  }
+  g.solver_free();
+  solv.solver_free();
+  return e == cudaSuccess ? 0 : -2;
+}
+
+struct ref_props_io {
+  int Nx, Ny, Nz;
+  double Lx, Ly, Lz, rho0, rho1, mu0, mu1;
+  const double* alpha;
+  const uint8_t *ct, *ft[3];
+  // in: contents before the call, rho_old the array that becomes rho after
+  // the reference's swap; out: after it
+  double *rho, *rho_old, *inv_rho, *mu, *fb[3], *fir[3], *frho[3], *fmu[3];
+  double ms;
+};
+
+// G_SMACSolver::update_properties_by_alpha (CFD/G_SMACSolver_VoF.cu:1543-1566)
+// on host arrays.  Returns 0 on success, -2 on a CUDA error.
+int ref_update_properties(ref_props_io* io) {
+  const int Nx = io->Nx, Ny = io->Ny, Nz = io->Nz;
+  SMACSolver solv;
+  solv.set_calc_properties(0., 0., 0., io->Lx, io->Ly, io->Lz, Nx, Ny, Nz);
+  solv.grid_.bc_.num_boundary_id_ = 1;
+  solv.solver_malloc();
+  StaggeredGrid& hg = solv.grid_;
+  put(hg.alpha_, io->alpha); put(hg.celltype_, io->ct);
+  put(hg.f_xtype_, io->ft[0]); put(hg.f_ytype_, io->ft[1]); put(hg.f_ztype_, io->ft[2]);
+  put(hg.rho_, io->rho); put(hg.rho_old_, io->rho_old); put(hg.inv_rho_, io->inv_rho); put(hg.mu_, io->mu);
+  put(hg.f_bx_, io->fb[0]); put(hg.f_by_, io->fb[1]); put(hg.f_bz_, io->fb[2]);
+  put(hg.f_inv_rhox_, io->fir[0]); put(hg.f_inv_rhoy_, io->fir[1]); put(hg.f_inv_rhoz_, io->fir[2]);
+  put(hg.f_rhox_, io->frho[0]); put(hg.f_rhoy_, io->frho[1]); put(hg.f_rhoz_, io->frho[2]);
+  put(hg.f_mux_, io->fmu[0]); put(hg.f_muy_, io->fmu[1]); put(hg.f_muz_, io->fmu[2]);
+  G_SMACSolver g;
+  g.set_calc_properties(0., 0., 0., io->Lx, io->Ly, io->Lz, Nx, Ny, Nz);
+  g.grid_.bc_.num_boundary_id_ = 1;
+  g.solver_malloc();
+  g.cpuTogpu(solv.grid_);
+  g.set_block_grid(Nx, Ny, Nz);
+  g.rho0_ = io->rho0; g.rho1_ = io->rho1; g.mu0_ = io->mu0; g.mu1_ = io->mu1;
+  cudaDeviceSynchronize();
+  cudaEvent_t ev[2];
+  for (auto& x : ev) cudaEventCreate(&x);
+  cudaEventRecord(ev[0], 0);
+  g.update_properties_by_alpha();
+  cudaEventRecord(ev[1], 0);
+  cudaDeviceSynchronize();
+  float t = 0.f;
+  cudaEventElapsedTime(&t, ev[0], ev[1]);
+  io->ms = t;
+  for (auto& x : ev) cudaEventDestroy(x);
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) {
+    // the device grid's rho_/rho_old_ pointers were swapped; copy back by member
+    g.gpuTocpu(solv.grid_);
+    get(hg.rho_, io->rho); get(hg.rho_old_, io->rho_old); get(hg.inv_rho_, io->inv_rho); get(hg.mu_, io->mu);
+    get(hg.f_bx_, io->fb[0]); get(hg.f_by_, io->fb[1]); get(hg.f_bz_, io->fb[2]);
+    get(hg.f_inv_rhox_, io->fir[0]); get(hg.f_inv_rhoy_, io->fir[1]); get(hg.f_inv_rhoz_, io->fir[2]);
+    get(hg.f_rhox_, io->frho[0]); get(hg.f_rhoy_, io->frho[1]); get(hg.f_rhoz_, io->frho[2]);
+    get(hg.f_mux_, io->fmu[0]); get(hg.f_muy_, io->fmu[1]); get(hg.f_muz_, io->fmu[2]);
     e = cudaGetLastError();
   }
   g.solver_free();

@@ -1138,6 +1138,89 @@ void orc_predict_vstar(int Nx, int Ny, int Nz, double dx, double dy, double dz, 
         }
 }
 
+// The property update, G_SMACSolver::update_properties_by_alpha
+// (CFD/G_SMACSolver_VoF.cu:1543-1566), after its swap of rho_ and rho_old_
+// (which the caller does by swapping arrays):
+//  1. k_update_cell_properties_by_alpha (:1374-1407): on C_INTERIOR and
+//     C_NEAR_BOUNDARY cells with indices 1..N+1, rho = (1-a) rho0 + a rho1,
+//     inv_rho = 1/rho, mu = (1-a) mu0 + a mu1;
+//  2. k_update_cell_boundary_properties_by_alpha + k_update_cell_ghost_properties
+//     (:1241-1372), final state: a C_SOLID interior cell takes rho and mu of
+//     its first C_INTERIOR neighbour (x-, x+, y-, y+, z-, z+; 0 without
+//     one), every ghost cell those of the nearest interior cell;
+//  3. k_update_{x,y,z}_face_properties_by_alpha (:1409-1535): on F_INTERIOR
+//     faces rho_f = (rho_L + rho_R)/2, f_b = f_inv_rho = 1/rho_f,
+//     mu_f = (mu_L + mu_R)/2; on the other faces (indices 1..N+2 along, 1..N+1
+//     across) f_b = f_inv_rho = 0, rho_f and mu_f untouched.
+// inv_rho, fir*, frho* may be NULL (not written).
+void orc_update_properties(int Nx, int Ny, int Nz, double rho0, double rho1, double mu0, double mu1,
+                           const double* alpha, const uint8_t* ct, const uint8_t* const* ft, double* rho,
+                           double* inv_rho, double* mu, double* const* fb, double* const* fir, double* const* frho,
+                           double* const* fmu) {
+  View<const double> A{alpha, Nx + 2, Ny + 2, Nz + 2};
+  View<const uint8_t> C{ct, Nx + 2, Ny + 2, Nz + 2};
+  Arr R{rho, Nx + 2, Ny + 2, Nz + 2}, M{mu, Nx + 2, Ny + 2, Nz + 2};
+  for (int iz = 1; iz <= Nz + 1; ++iz)
+    for (int iy = 1; iy <= Ny + 1; ++iy)
+      for (int ix = 1; ix <= Nx + 1; ++ix) {
+        const uint8_t t = C(ix, iy, iz);
+        if (t != C_INTERIOR && t != C_NEAR_BOUNDARY) continue;
+        const double a = A(ix, iy, iz);
+        R(ix, iy, iz) = (1. - a) * rho0 + a * rho1;
+        if (inv_rho) inv_rho[((size_t)iz * (Ny + 2) + iy) * (Nx + 2) + ix] = 1. / R(ix, iy, iz);
+        M(ix, iy, iz) = (1. - a) * mu0 + a * mu1;
+      }
+  for (int iz = 1; iz <= Nz; ++iz)
+    for (int iy = 1; iy <= Ny; ++iy)
+      for (int ix = 1; ix <= Nx; ++ix) {
+        if (C(ix, iy, iz) != C_SOLID) continue;
+        const int nb[6][3] = {{ix - 1, iy, iz}, {ix + 1, iy, iz}, {ix, iy - 1, iz},
+                              {ix, iy + 1, iz}, {ix, iy, iz - 1}, {ix, iy, iz + 1}};
+        double r = 0., m = 0.;
+        for (const auto& q : nb)
+          if (C(q[0], q[1], q[2]) == C_INTERIOR) {
+            r = R(q[0], q[1], q[2]);
+            m = M(q[0], q[1], q[2]);
+            break;
+          }
+        R(ix, iy, iz) = r;
+        M(ix, iy, iz) = m;
+      }
+  for (int iz = 0; iz < Nz + 2; ++iz)
+    for (int iy = 0; iy < Ny + 2; ++iy)
+      for (int ix = 0; ix < Nx + 2; ++ix) {
+        if (!(ix == 0 || ix == Nx + 1 || iy == 0 || iy == Ny + 1 || iz == 0 || iz == Nz + 1)) continue;
+        const int sx = ix == 0 ? 1 : ix == Nx + 1 ? Nx : ix;
+        const int sy = iy == 0 ? 1 : iy == Ny + 1 ? Ny : iy;
+        const int sz = iz == 0 ? 1 : iz == Nz + 1 ? Nz : iz;
+        R(ix, iy, iz) = R(sx, sy, sz);
+        M(ix, iy, iz) = M(sx, sy, sz);
+      }
+  const int N[3] = {Nx, Ny, Nz};
+  for (int a = 0; a < 3; ++a) {
+    int S[3] = {Nx + 2, Ny + 2, Nz + 2};
+    S[a] += 1;
+    for (int iz = 1; iz <= Nz + 1 + (a == 2); ++iz)
+      for (int iy = 1; iy <= Ny + 1 + (a == 1); ++iy)
+        for (int ix = 1; ix <= Nx + 1 + (a == 0); ++ix) {
+          const size_t f = ((size_t)iz * S[1] + iy) * S[0] + ix;
+          if (ft[a][f] != F_INTERIOR) {
+            fb[a][f] = 0.;
+            if (fir[a]) fir[a][f] = 0.;
+            continue;
+          }
+          int q[3] = {ix, iy, iz};
+          q[a] -= 1;
+          const double fr = 0.5 * (R(ix, iy, iz) + R(q[0], q[1], q[2]));
+          if (frho[a]) frho[a][f] = fr;
+          fb[a][f] = 1. / fr;
+          if (fir[a]) fir[a][f] = fb[a][f];
+          fmu[a][f] = 0.5 * (M(ix, iy, iz) + M(q[0], q[1], q[2]));
+        }
+  }
+  (void)N;
+}
+
 // Outlet boundary faces (G_SMACSolver::update_boundary_faces,
 // CFD/G_SMACSolver_VoF.cu:1798-1950): f_b of an outlet face is twice the f_b
 // of the face next to it on the interior side (p = 0 on the outlet).  The

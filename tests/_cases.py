@@ -46,7 +46,7 @@ def golden_names():
     if not os.path.isdir(GOLDEN):
         return []
     return sorted(f[:-4] for f in os.listdir(GOLDEN)
-                  if f.endswith(".npz") and not f.startswith(("post", "vstar", "surface", "mom")))
+                  if f.endswith(".npz") and not f.startswith(("post", "vstar", "surface", "mom", "props")))
 
 
 def surface_golden_names():
@@ -116,3 +116,16 @@ def momentum_case_from_spec(spec):
         if k in spec:
             spec[k] = tuple(spec[k])
     return W.momentum_case(**spec)
+
+
+def property_golden_names():
+    """Fixtures of the reference's update_properties_by_alpha."""
+    if not os.path.isdir(GOLDEN):
+        return []
+    return sorted(f[:-4] for f in os.listdir(GOLDEN) if f.endswith(".npz") and f.startswith("props"))
+
+
+def property_case_from_spec(spec):
+    spec = dict(spec)
+    spec["N"] = tuple(spec["N"])
+    return W.property_case(**spec)

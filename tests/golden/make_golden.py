@@ -71,6 +71,12 @@ MOMENTUM_CASES = [
     ("mom9x7x11_s3_noextras", dict(N=(9, 7, 11), seed=3, sides=("y-",), extras=False)),
 ]
 
+# The property update (update_properties_by_alpha): workloads.property_case kwargs.
+PROPERTY_CASES = [
+    ("props12x10x8_s1", dict(N=(12, 10, 8), seed=1)),
+    ("props16_s2_solid", dict(N=(16, 16, 16), seed=2, solid_fraction=0.35)),
+]
+
 
 def oracle_solid_fraction(N, h, origin, spheres):
     return O.solid_fraction_spheres(N, h, origin, spheres)
@@ -125,6 +131,12 @@ def main():
         vxs, vys, vzs, _ = REF.predict_vstar(W.momentum_case(**spec))
         np.savez_compressed(os.path.join(args.out, name + ".npz"), meta=np.array(json.dumps(spec)), vxs=vxs,
                             vys=vys, vzs=vzs)
+        post_index[name] = spec
+        print(name, spec, flush=True)
+    for name, spec in PROPERTY_CASES:
+        N, h, (r0, r1, m0, m1), alpha, ct, ft, init = W.property_case(**spec)
+        out, _ = REF.update_properties(N, h, r0, r1, m0, m1, alpha, ct, ft, init)
+        np.savez_compressed(os.path.join(args.out, name + ".npz"), meta=np.array(json.dumps(spec)), **out)
         post_index[name] = spec
         print(name, spec, flush=True)
     with open(os.path.join(args.out, "post_index.json"), "w") as f:

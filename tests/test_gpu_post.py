@@ -17,13 +17,14 @@ import torch
 from mydemcfd_b200 import _native as nat
 from mydemcfd_b200 import workloads as W
 from mydemcfd_b200.solver import (BoundaryConditions, DeviceGrid, SMACStep, face_gradp_device, predict_vstar_device,
-                                  surface_tension_device, update_pressure_ghost_device, update_velocity_ghost_device,
-                                  update_vstar_boundary_device)
+                                  surface_tension_device, update_pressure_ghost_device, update_properties_device,
+                                  update_velocity_ghost_device, update_vstar_boundary_device)
 from oracle import oracle as O
 from oracle import ref as REF
 
 from _cases import (load_golden, momentum_case_from_spec, momentum_golden_names, post_case_from_spec,
-                    post_golden_names, surface_case_from_spec, surface_golden_names, vstar_golden_names)
+                    post_golden_names, property_case_from_spec, property_golden_names, surface_case_from_spec,
+                    surface_golden_names, vstar_golden_names)
 
 pytestmark = pytest.mark.gpu
 
@@ -409,3 +410,107 @@ def test_anisotropic_spacing_bit_exact_against_reference_library():
     *ref, _ = REF.vstar(c)
     for k, a, b in zip(("vxs", "vys", "vzs"), run_vstar(c), ref):
         assert np.array_equal(a, b), k
+
+
+# ---------------------------------------------------------------------------
+# the property update (update_properties_by_alpha)
+
+def _prop_tensors(init):
+    """CUDA copies of the arrays before the call, after the reference's
+    swap: the array written as rho is the former rho_old."""
+    t = {k: _cuda(v) for k, v in init.items() if k not in ("rho", "rho_old")}
+    t["rho"] = _cuda(init["rho_old"])
+    return t
+
+
+def run_props(N, h, prm, alpha, ct, ft, init):
+    t = _prop_tensors(init)
+    update_properties_device(N, h, *prm, _cuda(alpha), _cuda(ct), tuple(_cuda(a) for a in ft), t)
+    torch.cuda.synchronize()
+    return {k: v.cpu().numpy() for k, v in t.items()}
+
+
+def _oracle_props(N, prm, alpha, ct, ft, init):
+    src = dict(init)
+    src["rho"] = init["rho_old"]
+    return O.update_properties(N, *prm, alpha, ct, ft, src)
+
+
+@pytest.mark.parametrize("spec", [
+    dict(N=(12, 10, 8), seed=1),
+    dict(N=(16, 16, 16), seed=2, solid_fraction=0.35),
+    dict(N=(33, 18, 20), seed=5, solid_fraction=0.2),
+    dict(N=(1, 7, 5), seed=8, solid_fraction=0.1),
+])
+def test_update_properties_bit_exact_against_oracle(spec):
+    N, h, prm, alpha, ct, ft, init = W.property_case(**spec)
+    got = run_props(N, h, prm, alpha, ct, ft, init)
+    want = _oracle_props(N, prm, alpha, ct, ft, init)
+    for k in want:
+        assert np.array_equal(got[k], want[k]), k
+
+
+@pytest.mark.parametrize("name", property_golden_names())
+def test_update_properties_bit_exact_against_reference_golden(name):
+    meta, arr = load_golden(name)
+    N, h, prm, alpha, ct, ft, init = property_case_from_spec(meta)
+    got = run_props(N, h, prm, alpha, ct, ft, init)
+    for k in got:
+        assert np.array_equal(got[k], arr[k]), k
+
+
+def test_update_properties_optional_outputs_left_alone():
+    """inv_rho, f_inv_rho* and f_rho* may be absent: the others are written as before."""
+    N, h, prm, alpha, ct, ft, init = W.property_case((14, 9, 11), seed=9, solid_fraction=0.2)
+    t = _prop_tensors(init)
+    for k in ("inv_rho", "firx", "firy", "firz", "rhox", "rhoy", "rhoz"):
+        del t[k]
+    update_properties_device(N, h, *prm, _cuda(alpha), _cuda(ct), tuple(_cuda(a) for a in ft), t)
+    want = _oracle_props(N, prm, alpha, ct, ft, init)
+    for k, v in t.items():
+        assert np.array_equal(v.cpu().numpy(), want[k]), k
+
+
+@pytest.mark.skipif(not REF.available(), reason="reference build oracle/_ref not present")
+def test_update_properties_against_reference_library_and_time_256():
+    case = W.property_case((96, 80, 72), seed=11, solid_fraction=0.1)
+    N, h, prm, alpha, ct, ft, init = case
+    ref, _ = REF.update_properties(N, h, *prm, alpha, ct, ft, init)
+    got = run_props(*case)
+    for k in got:
+        assert np.array_equal(got[k], ref[k]), k
+    N, h, prm, alpha, ct, ft, init = W.property_case((256, 256, 256), seed=12, solid_fraction=0.02)
+    REF.update_properties(N, h, *prm, alpha, ct, ft, init)  # loads the reference's kernels
+    _, ref_ms = REF.update_properties(N, h, *prm, alpha, ct, ft, init)
+    t = _prop_tensors(init)
+    a, c, f = _cuda(alpha), _cuda(ct), tuple(_cuda(x) for x in ft)
+    ms = _device_ms(lambda: update_properties_device(N, h, *prm, a, c, f, t))
+    print(f"update_properties_by_alpha 256^3: {ms * 1e3:.1f} us (reference {ref_ms * 1e3:.1f} us)")
+    assert ms < ref_ms
+
+
+def test_smac_step_update_properties_swaps_and_matches_oracle():
+    N, h, prm, alpha, ct, ft, init = W.property_case((20, 12, 16), seed=13, solid_fraction=0.25)
+    c = W.post_case(N, 13, sides=())
+    sh = W.shapes(N)
+    zc = lambda: torch.zeros(sh["cell"], dtype=torch.float64, device="cuda")  # noqa: E731
+    g = DeviceGrid(*N, *h, *(_cuda(a) for a in c.vs), *(_cuda(a) for a in c.fb), *(_cuda(a) for a in c.fb),
+                   _cuda(ct), *(_cuda(a) for a in ft), _cuda(c.p), zc(), zc(), *(_cuda(a) for a in c.v))
+    g.alpha_ = _cuda(alpha)
+    g.rho_, g.rho_old_, g.inv_rho_, g.mu_ = (_cuda(init[k]) for k in ("rho", "rho_old", "inv_rho", "mu"))
+    for ax in "xyz":
+        setattr(g, f"f_b{ax}_", _cuda(init["fb" + ax]))
+        setattr(g, f"f_inv_rho{ax}_", _cuda(init["fir" + ax]))
+        setattr(g, f"f_rho{ax}_", _cuda(init["rho" + ax]))
+        setattr(g, f"f_mu{ax}_", _cuda(init["mu" + ax]))
+    prev_rho = g.rho_
+    SMACStep(g).update_properties_by_alpha(*prm)
+    torch.cuda.synchronize()
+    assert g.rho_old_ is prev_rho and np.array_equal(g.rho_old_.cpu().numpy(), init["rho"])
+    want = _oracle_props(N, prm, alpha, ct, ft, init)
+    got = {"rho": g.rho_, "inv_rho": g.inv_rho_, "mu": g.mu_}
+    for ax in "xyz":
+        got.update({"fb" + ax: getattr(g, f"f_b{ax}_"), "fir" + ax: getattr(g, f"f_inv_rho{ax}_"),
+                    "rho" + ax: getattr(g, f"f_rho{ax}_"), "mu" + ax: getattr(g, f"f_mu{ax}_")})
+    for k, v in got.items():
+        assert np.array_equal(v.cpu().numpy(), want[k]), k

@@ -8,7 +8,8 @@ from mydemcfd_b200 import workloads as W
 
 from _cases import (build_case, fluid_demeaned, golden_names, load_golden, post_case_from_spec, post_golden_names,
                     ref_grid, rel_err, surface_case_from_spec, surface_golden_names, vstar_golden_names,
-                    momentum_case_from_spec, momentum_golden_names)
+                    momentum_case_from_spec, momentum_golden_names, property_case_from_spec,
+                    property_golden_names)
 
 
 def test_box_types_match_reference_setup(oracle_lib):
@@ -559,3 +560,43 @@ def test_predict_vstar_oracle_matches_reference_golden(oracle_lib, name):
     got = oracle_lib.predict_vstar(momentum_case_from_spec(meta))
     for k, a in zip(("vxs", "vys", "vzs"), got):
         assert np.array_equal(a, arr[k]), k
+
+
+# ---------------------------------------------------------------------------
+# the property update (update_properties_by_alpha)
+
+def _oracle_props(O, N, prm, alpha, ct, ft, init):
+    """The oracle on the arrays as the call sees them: rho is the array the
+    reference's swap makes rho (the former rho_old)."""
+    src = dict(init)
+    src["rho"] = init["rho_old"]
+    return O.update_properties(N, *prm, alpha, ct, ft, src)
+
+
+def test_update_properties_single_phase_known_answer(oracle_lib):
+    """alpha = 0: rho = rho0 and mu = mu0 in every interior, solid-with-fluid
+    and ghost cell, f_b = 1/rho0 on F_INTERIOR faces and 0 on the others."""
+    N, h, prm, alpha, ct, ft, init = W.property_case((9, 8, 7), seed=3, solid_fraction=0.3)
+    out = _oracle_props(oracle_lib, N, prm, np.zeros_like(alpha), ct, ft, init)
+    rho0, _, mu0, _ = prm
+    fluid_or_ghost = (ct == W.C_INTERIOR) | (ct == W.C_GHOST)
+    assert np.all(out["rho"][fluid_or_ghost] == rho0) and np.all(out["mu"][fluid_or_ghost] == mu0)
+    for k, t in zip(("fbx", "fby", "fbz"), ft):
+        inner = t == W.F_INTERIOR
+        assert np.all(out[k][inner] == 1.0 / rho0)
+    # a face outside the written range keeps its value
+    assert out["fbx"][0, 0, 0] == init["fbx"][0, 0, 0]
+
+
+PROPERTY_GOLDEN = property_golden_names()
+
+
+@pytest.mark.skipif(not PROPERTY_GOLDEN, reason="no property-update golden vectors")
+@pytest.mark.parametrize("name", PROPERTY_GOLDEN)
+def test_update_properties_oracle_matches_reference_golden(oracle_lib, name):
+    meta, arr = load_golden(name)
+    N, h, prm, alpha, ct, ft, init = property_case_from_spec(meta)
+    out = _oracle_props(oracle_lib, N, prm, alpha, ct, ft, init)
+    for k in out:
+        assert np.array_equal(out[k], arr[k]), k
+    assert np.array_equal(arr["rho_old"], init["rho"])  # the swap keeps the previous rho
