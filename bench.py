@@ -49,7 +49,8 @@ def parse():
                     help="set up the workload and launch one kernel (smac_time_kernel id) a few times: a small, "
                          "self-contained command for ncu captures")
     ap.add_argument("--around", default=None,
-                    choices=["predict_vstar", "vstar_boundary", "pressure_ghost", "velocity_ghost", "face_gradp"],
+                    choices=["predict_vstar", "vstar_boundary", "pressure_ghost", "velocity_ghost", "face_gradp",
+                             "update_properties"],
                     help="set up the workload and launch one of the calls around the projection --reps times "
                          "(for ncu captures)")
     ap.add_argument("--reps", type=int, default=3)
@@ -399,14 +400,15 @@ def around_calls(case, g, p, v, dev):
     """The calls either side of the projection on the bench grid, as
     closures, and the algorithmic bytes of each: before it the momentum
     predictor and update_vstar_boundary, after it update_boundary_ghost +
-    make_face_gradp.  Inputs: pressure p and velocity v (device tensors),
-    no-slip walls with an outlet on x+."""
+    make_face_gradp, and the VoF property update.  Inputs: pressure p and
+    velocity v (device tensors), no-slip walls with an outlet on x+; the
+    property update takes alpha = (p + 1) / 2, rho 1 / 1000, mu 1e-3 / 1e-1."""
     import torch
 
     from mydemcfd_b200 import workloads as W
     from mydemcfd_b200.solver import (BoundaryConditions, face_gradp_device, predict_vstar_device,
-                                      update_pressure_ghost_device, update_velocity_ghost_device,
-                                      update_vstar_boundary_device)
+                                      update_pressure_ghost_device, update_properties_device,
+                                      update_velocity_ghost_device, update_vstar_boundary_device)
     N, h = case.N, case.h
     sh = W.shapes(N)
     bcid = [torch.zeros(sh[k], dtype=torch.uint8, device=dev) for k in "xyz"]
@@ -428,6 +430,12 @@ def around_calls(case, g, p, v, dev):
         mom["mu" + ax] = torch.full(sh["xyz"[k]], 1e-3, dtype=torch.float64, device=dev)
         mom["fb" + ax] = fb[k]
     vs_pred = [t.clone() for t in vs]
+    alpha = (p + 1.0) * 0.5
+    props = {k: torch.zeros(sh["cell"], dtype=torch.float64, device=dev) for k in ("rho", "inv_rho", "mu")}
+    for ax in "xyz":
+        for k in ("fb", "fir", "rho", "mu"):
+            props[k + ax] = torch.zeros(sh[ax], dtype=torch.float64, device=dev)
+    ft = (g.f_xtype_, g.f_ytype_, g.f_ztype_)
     calls = {
         "predict_vstar": lambda: predict_vstar_device(N, h, bc, mom, case.dt, (0.0, 0.0, -9.8), vs_pred),
         "vstar_boundary": lambda: update_vstar_boundary_device(N, h, bc, (g.f_xtype_, g.f_ytype_, g.f_ztype_), bcid,
@@ -435,6 +443,8 @@ def around_calls(case, g, p, v, dev):
         "pressure_ghost": lambda: update_pressure_ghost_device(N, h, g.celltype_, None, (0.0, 0.0, -9.8), p),
         "velocity_ghost": lambda: update_velocity_ghost_device(N, h, bc, bcid, marks, None, vs, fb, p, case.dt, v),
         "face_gradp": lambda: face_gradp_device(N, h, p, gp),
+        "update_properties": lambda: update_properties_device(N, h, 1.0, 1000.0, 1e-3, 1e-1, alpha, g.celltype_, ft,
+                                                              props),
     }
     nx, ny, nz = N
     ncell = (nx + 2) * (ny + 2) * (nz + 2)
@@ -456,6 +466,9 @@ def around_calls(case, g, p, v, dev):
         "velocity_ghost": nface + ny * nz * 32 + ring * (8 + 8 + 1 + 8),
         # p read once, three face arrays written on the (N+1)^3 box
         "face_gradp": 8 * (ncell + 3 * (nx + 1) * (ny + 1) * (nz + 1)),
+        # per cell its type and alpha read, rho, 1/rho and mu written; per face
+        # its type read, 1/rho (f_b and f_inv_rho), rho and mu written
+        "update_properties": ncell * (1 + 8 + 3 * 8) + nface * (1 + 4 * 8),
     }
     return calls, alg
 

@@ -175,6 +175,10 @@ typedef struct {
  *  - F_INTERIOR faces: rho_f = the two cells' mean, f_b = f_inv_rho =
  *    1/rho_f, mu_f = the mean viscosity; other faces with indices 1..N+2
  *    along, 1..N+1 across: f_b = f_inv_rho = 0 (:1409-1535).
+ * One launch computes every final value from alpha and the types.  The ghost
+ * layer must not hold C_INTERIOR cells next to C_SOLID interior cells (the
+ * reference's set-up types it C_GHOST, CFD/SMACSolver.cpp:220; there the
+ * reference's own passes would race).
  * smac_assemble_vof is the subset that feeds the pressure operator. */
 smac_status smac_update_properties(const smac_grid_desc* d, const smac_vof_params* vp, const double* alpha,
                                    const uint8_t* celltype, const uint8_t* fxt, const uint8_t* fyt, const uint8_t* fzt,
