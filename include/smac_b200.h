@@ -304,6 +304,27 @@ smac_status smac_predict_vstar(const smac_grid_desc* d, const smac_boundary_tabl
                                double dt, double gx, double gy, double gz, double* vxs, double* vys, double* vzs,
                                void* stream);
 
+/* The extra cell and face fields of the two-way-coupled predictor (device
+ * pointers, reference layout). */
+typedef struct {
+  const double *eps_old, *eps_new;            /* void_fraction_old_, void_fraction_ (cells) */
+  const double *inv_rhox, *inv_rhoy, *inv_rhoz; /* f_inv_rho*_ (read in place of mf's f_b*) */
+} smac_two_way_fields;
+
+/* The two-way-coupled momentum predictor,
+ * G_SMACSolver::get_vof_vstar_rhouu_consistent_two_way (CFD/G_SMACSolver.cu:
+ * 2196-2203; k_get_vof_vstar_rhouu_consistent_{x,y,z}_two_way :1538-2194),
+ * the step the CFD-DEM coupled solver takes (Coupling/main.cu:540): as
+ * smac_predict_vstar with each stress times the void fraction eps_old of its
+ * cell or edge (the mean of the four cells around an edge), the pressure
+ * gradient times the face's eps_old, and
+ *   u* = (f_inv_rho / eps_new_f)(eps_old_f rho_old_f u + dt (...) + impulse/V) + dt g,
+ * times (1 - IBM solid fraction).  mf's fbx..fbz are not read. */
+smac_status smac_predict_vstar_two_way(const smac_grid_desc* d, const smac_boundary_table* bc,
+                                       const smac_momentum_fields* mf, const smac_two_way_fields* tw, double dt,
+                                       double gx, double gy, double gz, double* vxs, double* vys, double* vzs,
+                                       void* stream);
+
 /* Wall-face u* before the projection, G_SMACSolver::update_vstar_boundary
  * (CFD/G_SMACSolver.cu:1044-1052, k_update_v*star_boundary,
  * CFD/G_BoundaryFunctions.cu:3-71, CFD/G_BoundaryFunctions.h:369-470), in

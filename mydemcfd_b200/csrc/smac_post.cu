@@ -742,9 +742,11 @@ struct MomArgs {
   const double* mu;
   const double* rho_old;
   const double* p;
-  const double* fb[3];
+  const double* fb[3];   // f_b (one-way) or f_inv_rho (two-way)
   const double* imp[3];  // nullptr: 0
   const double* sf[3];   // nullptr: 0
+  const double* eps_old;  // two-way only: void_fraction_old_, void_fraction_
+  const double* eps_new;
   double* vs[3];
   double dt, g[3], ih[3], ih2[3], inv_volume;
   long long st[4][3];  // index strides along x, y, z of the three face families and (3) the cells
@@ -801,10 +803,25 @@ __device__ __forceinline__ double m_minmod(double dp, double dm) {
 // The two other axes of AF in ascending order, as compile-time values.
 template <int AF> struct Others { static constexpr int D0 = AF == 0 ? 1 : 0, D1 = AF == 2 ? 1 : 2; };
 
-// Viscous cross term of axis D: (tau_D+ - tau_D-) / h_D.  b: the face's
-// indices in the three family layouts; vdp, vdm: its mirrored neighbours
-// along D.
+// Two-way form: eps_old averaged over the four cells around the edge on
+// side s along D of the family-AF face with high cell c: its two cells (cm,
+// c) and their neighbours along D, added in ascending index order as the
+// reference writes them (k_get_vof_vstar_rhouu_consistent_*_two_way,
+// CFD/G_SMACSolver.cu:1610-1622, 1832-1844, 2050-2062).
 template <int AF, int D>
+__device__ __forceinline__ double m_eps4(const MomArgs& A, long long c, int s) {
+  const long long sa = A.st[3][AF], sd = A.st[3][D];
+  const long long lc = s > 0 ? c : c - sd, lcm = lc - sa, hc = lc + sd, hcm = lcm + sd;
+  const double* e = A.eps_old;
+  const double sum = D > AF ? DADD(DADD(DADD(e[lcm], e[lc]), e[hcm]), e[hc]) : DADD(DADD(DADD(e[lcm], e[hcm]), e[lc]), e[hc]);
+  return DMUL(0.25, sum);
+}
+
+// Viscous cross term of axis D: (tau_D+ - tau_D-) / h_D, each stress times
+// its edge's eps_old in the two-way form.  b: the face's indices in the
+// three family layouts and (b[3]) its high cell; vdp, vdm: its mirrored
+// neighbours along D.
+template <int AF, int D, bool TW>
 __device__ __forceinline__ double m_cross(const MomArgs& A, const long long* b, double v0, double vdp, double vdm) {
   const long long qd = b[D] + A.st[D][D], qda = qd - A.st[D][AF], q = b[D], qm = b[D] - A.st[D][AF];
   const double wp0 = m_face_val<D>(A, qd), wpm = m_face_val<D>(A, qda);
@@ -813,6 +830,7 @@ __device__ __forceinline__ double m_cross(const MomArgs& A, const long long* b, 
   const double tp = DMUL(mup, DADD(DMUL(DSUB(wp0, wpm), A.ih[AF]), DMUL(DSUB(vdp, v0), A.ih[D])));
   const double mum = DMUL(0.5, DADD(A.muf[D][q], A.muf[D][qm]));
   const double tm = DMUL(mum, DADD(DMUL(DSUB(w0, wm), A.ih[AF]), DMUL(DSUB(v0, vdm), A.ih[D])));
+  if (TW) return DMUL(DSUB(DMUL(m_eps4<AF, D>(A, b[3], +1), tp), DMUL(m_eps4<AF, D>(A, b[3], -1), tm)), A.ih[D]);
   return DMUL(DSUB(tp, tm), A.ih[D]);
 }
 
@@ -869,8 +887,11 @@ __device__ __forceinline__ double m_conv(const MomArgs& A, const long long* b, d
 }
 
 // u* of the F_INTERIOR family-AF face with indices b[0..2] in the family
-// layouts and b[3] in the cells.
-template <int AF>
+// layouts and b[3] in the cells.  TW: the two-way-coupled form
+// (k_get_vof_vstar_rhouu_consistent_{x,y,z}_two_way, CFD/G_SMACSolver.cu:
+// 1538-2194): the stresses and the pressure gradient weighted by eps_old,
+// u* = (f_inv_rho / eps_new_f)(eps_old_f rho_old_f u + dt (...) + impulse/V) + dt g.
+template <int AF, bool TW>
 __device__ __forceinline__ double m_vstar(const MomArgs& A, const long long* b) {
   constexpr int D0 = Others<AF>::D0, D1 = Others<AF>::D1;
   const long long f = b[AF], c = b[3], cm = b[3] - A.st[3][AF];
@@ -881,9 +902,10 @@ __device__ __forceinline__ double m_vstar(const MomArgs& A, const long long* b) 
   // viscous: the own axis, then the other two in axis order
   const double tau_p = DMUL(A.mu[c], DSUB(vp, v0));
   const double tau_m = DMUL(A.mu[cm], DSUB(v0, vm));
-  double tmp = DMUL(DMUL(2.0, DSUB(tau_p, tau_m)), A.ih2[AF]);
-  tmp = DADD(tmp, m_cross<AF, D0>(A, b, v0, p0, m0));
-  tmp = DADD(tmp, m_cross<AF, D1>(A, b, v0, p1, m1));
+  double tmp = TW ? DMUL(DMUL(2.0, DSUB(DMUL(A.eps_old[c], tau_p), DMUL(A.eps_old[cm], tau_m))), A.ih2[AF])
+                  : DMUL(DMUL(2.0, DSUB(tau_p, tau_m)), A.ih2[AF]);
+  tmp = DADD(tmp, m_cross<AF, D0, TW>(A, b, v0, p0, m0));
+  tmp = DADD(tmp, m_cross<AF, D1, TW>(A, b, v0, p1, m1));
   // convection in axis order
   const double npx = AF == 0 ? vp : (D0 == 0 ? p0 : p1), nmx = AF == 0 ? vm : (D0 == 0 ? m0 : m1);
   const double npy = AF == 1 ? vp : (D0 == 1 ? p0 : p1), nmy = AF == 1 ? vm : (D0 == 1 ? m0 : m1);
@@ -893,10 +915,18 @@ __device__ __forceinline__ double m_vstar(const MomArgs& A, const long long* b) 
   tmp = DSUB(tmp, m_conv<AF, 2>(A, b, v0, npz, nmz));
   const double inv_rho = A.fb[AF][f];
   const double rho_old_f = DMUL(0.5, DADD(A.rho_old[c], A.rho_old[cm]));
-  tmp = DSUB(tmp, DMUL(DSUB(A.p[c], A.p[cm]), A.ih[AF]));
   const double coupling = DMUL(A.imp[AF] ? A.imp[AF][f] : 0.0, A.inv_volume);
-  const double vs = DADD(DMUL(inv_rho, DADD(DMUL(v0, rho_old_f), coupling)),
-                         DMUL(A.dt, DADD(DMUL(inv_rho, tmp), A.g[AF])));
+  double vs;
+  if (TW) {
+    const double eo = DMUL(0.5, DADD(A.eps_old[cm], A.eps_old[c]));
+    const double en = DMUL(0.5, DADD(A.eps_new[cm], A.eps_new[c]));
+    tmp = DSUB(tmp, DMUL(DMUL(eo, DSUB(A.p[c], A.p[cm])), A.ih[AF]));
+    const double ier = __ddiv_rn(inv_rho, en);
+    vs = DADD(DMUL(ier, DADD(DADD(DMUL(DMUL(eo, rho_old_f), v0), DMUL(A.dt, tmp)), coupling)), DMUL(A.dt, A.g[AF]));
+  } else {
+    tmp = DSUB(tmp, DMUL(DSUB(A.p[c], A.p[cm]), A.ih[AF]));
+    vs = DADD(DMUL(inv_rho, DADD(DMUL(v0, rho_old_f), coupling)), DMUL(A.dt, DADD(DMUL(inv_rho, tmp), A.g[AF])));
+  }
   return DMUL(DSUB(1.0, A.sf[AF] ? A.sf[AF][f] : 0.0), vs);
 }
 
@@ -908,6 +938,7 @@ __device__ __forceinline__ double m_vstar(const MomArgs& A, const long long* b) 
 // resident warps matter more than registers: 5 blocks per SM (48 registers,
 // a few spills to L1) measured 3.32 ms at 256^3, against 3.60 ms with 4
 // blocks, 4.27 ms with 3 and 3.43 ms with 6.
+template <bool TW>
 __global__ void __launch_bounds__(256, 5) k_predict_vstar(MomArgs A) {
   const int fam = blockIdx.z % 3;
   const int z = blockIdx.z / 3 + 1;
@@ -917,11 +948,11 @@ __global__ void __launch_bounds__(256, 5) k_predict_vstar(MomArgs A) {
 #pragma unroll
   for (int k = 0; k < 4; ++k) b[k] = x * A.st[k][0] + y * A.st[k][1] + z * A.st[k][2];
   if (fam == 0) {
-    if (A.ft[0][b[0]] == 0) A.vs[0][b[0]] = m_vstar<0>(A, b);
+    if (A.ft[0][b[0]] == 0) A.vs[0][b[0]] = m_vstar<0, TW>(A, b);
   } else if (fam == 1) {
-    if (A.ft[1][b[1]] == 0) A.vs[1][b[1]] = m_vstar<1>(A, b);
+    if (A.ft[1][b[1]] == 0) A.vs[1][b[1]] = m_vstar<1, TW>(A, b);
   } else {
-    if (A.ft[2][b[2]] == 0) A.vs[2][b[2]] = m_vstar<2>(A, b);
+    if (A.ft[2][b[2]] == 0) A.vs[2][b[2]] = m_vstar<2, TW>(A, b);
   }
 }
 
@@ -1301,17 +1332,23 @@ smac_status smac_surface_tension(const smac_grid_desc* d, const double* alpha, c
   return launch_status(fn);
 }
 
-smac_status smac_predict_vstar(const smac_grid_desc* d, const smac_boundary_table* bc, const smac_momentum_fields* mf,
-                               double dt, double gx, double gy, double gz, double* vxs, double* vys, double* vzs,
-                               void* stream) {
-  static const char* fn = "smac_predict_vstar";
+}  // extern "C"
+
+namespace {
+
+// The two predictor entries: tw == nullptr the one-way form with mf's f_b,
+// otherwise the two-way form with tw's eps and f_inv_rho.
+smac_status predict_vstar(const char* fn, const smac_grid_desc* d, const smac_boundary_table* bc,
+                          const smac_momentum_fields* mf, const smac_two_way_fields* tw, double dt, double gx,
+                          double gy, double gz, double* vxs, double* vys, double* vzs, void* stream) {
   if (!d || !bc || !mf || !vxs || !vys || !vzs) {
     smac::set_error_text("%s: null argument", fn);
     return SMAC_BAD_ARG;
   }
+  const double* const* inv_rho = tw ? &tw->inv_rhox : &mf->fbx;
   const void* need[] = {mf->fxt, mf->fyt, mf->fzt, mf->fxbcid, mf->fybcid, mf->fzbcid, mf->vx, mf->vy, mf->vz,
                         mf->mfx, mf->mfy, mf->mfz, mf->mux, mf->muy, mf->muz, mf->mu, mf->rho_old, mf->p,
-                        mf->fbx, mf->fby, mf->fbz};
+                        inv_rho[0], inv_rho[1], inv_rho[2], tw ? tw->eps_old : mf->p, tw ? tw->eps_new : mf->p};
   for (const void* q : need)
     if (!q) {
       smac::set_error_text("%s: a required field is null", fn);
@@ -1330,7 +1367,11 @@ smac_status smac_predict_vstar(const smac_grid_desc* d, const smac_boundary_tabl
   A.mf[0] = mf->mfx; A.mf[1] = mf->mfy; A.mf[2] = mf->mfz;
   A.muf[0] = mf->mux; A.muf[1] = mf->muy; A.muf[2] = mf->muz;
   A.mu = mf->mu; A.rho_old = mf->rho_old; A.p = mf->p;
-  A.fb[0] = mf->fbx; A.fb[1] = mf->fby; A.fb[2] = mf->fbz;
+  A.fb[0] = inv_rho[0]; A.fb[1] = inv_rho[1]; A.fb[2] = inv_rho[2];
+  if (tw) {
+    A.eps_old = tw->eps_old;
+    A.eps_new = tw->eps_new;
+  }
   A.imp[0] = mf->impx; A.imp[1] = mf->impy; A.imp[2] = mf->impz;
   A.sf[0] = mf->sfx; A.sf[1] = mf->sfy; A.sf[2] = mf->sfz;
   A.vs[0] = vxs; A.vs[1] = vys; A.vs[2] = vzs;
@@ -1350,8 +1391,32 @@ smac_status smac_predict_vstar(const smac_grid_desc* d, const smac_boundary_tabl
   }
   fill_table(&A.bc, bc);
   const dim3 grid((unsigned)((d->nx + 1 + 31) / 32), (unsigned)((d->ny + 1 + 7) / 8), 3u * (unsigned)(d->nz + 1));
-  k_predict_vstar<<<grid, dim3(32, 8), 0, (cudaStream_t)stream>>>(A);
+  if (tw)
+    k_predict_vstar<true><<<grid, dim3(32, 8), 0, (cudaStream_t)stream>>>(A);
+  else
+    k_predict_vstar<false><<<grid, dim3(32, 8), 0, (cudaStream_t)stream>>>(A);
   return launch_status(fn);
+}
+
+}  // namespace
+
+extern "C" {
+
+smac_status smac_predict_vstar(const smac_grid_desc* d, const smac_boundary_table* bc, const smac_momentum_fields* mf,
+                               double dt, double gx, double gy, double gz, double* vxs, double* vys, double* vzs,
+                               void* stream) {
+  return predict_vstar("smac_predict_vstar", d, bc, mf, nullptr, dt, gx, gy, gz, vxs, vys, vzs, stream);
+}
+
+smac_status smac_predict_vstar_two_way(const smac_grid_desc* d, const smac_boundary_table* bc,
+                                       const smac_momentum_fields* mf, const smac_two_way_fields* tw, double dt,
+                                       double gx, double gy, double gz, double* vxs, double* vys, double* vzs,
+                                       void* stream) {
+  if (!tw) {
+    smac::set_error_text("smac_predict_vstar_two_way: null argument");
+    return SMAC_BAD_ARG;
+  }
+  return predict_vstar("smac_predict_vstar_two_way", d, bc, mf, tw, dt, gx, gy, gz, vxs, vys, vzs, stream);
 }
 
 smac_status smac_update_properties(const smac_grid_desc* d, const smac_vof_params* vp, const double* alpha,

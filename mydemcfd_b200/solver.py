@@ -353,7 +353,7 @@ class SMACStep:
         self.bc_ = bc
         self.pressure_solver_: B200PressureSolver | None = None
 
-    def get_vof_vstar_rhouu_consistent(self):
+    def get_vof_vstar_rhouu_consistent(self, two_way: dict | None = None):
         """G_SMACSolver::get_vof_vstar_rhouu_consistent (CFD/G_SMACSolver.cu:1062-1070):
         u* into f_v*_star_ from the grid's time-n fields (smac_predict_vstar)."""
         g = self.grid_
@@ -372,7 +372,21 @@ class SMACStep:
             f["imp" + ax] = getattr(g, f"f_coupling_impulse_{ax}_")
             f["sf" + ax] = getattr(g, f"f_ibm_solid_fraction_{ax}_")
         predict_vstar_device(g.N, (g.dx_, g.dy_, g.dz_), self.bc_, f, self.dt_, (self.gx_, self.gy_, self.gz_),
-                             (g.f_vx_star_, g.f_vy_star_, g.f_vz_star_))
+                             (g.f_vx_star_, g.f_vy_star_, g.f_vz_star_), two_way=two_way)
+
+    def get_vof_vstar_rhouu_consistent_two_way(self):
+        """G_SMACSolver::get_vof_vstar_rhouu_consistent_two_way
+        (CFD/G_SMACSolver.cu:2196-2203): the two-way-coupled u* into
+        f_v*_star_, from the same fields as get_vof_vstar_rhouu_consistent
+        plus void_fraction_old_, void_fraction_ and f_inv_rho*_
+        (smac_predict_vstar_two_way)."""
+        g = self.grid_
+        need = ("void_fraction_old_", "void_fraction_")
+        if any(getattr(g, k) is None for k in need):
+            raise ValueError("get_vof_vstar_rhouu_consistent_two_way needs the grid's " + ", ".join(need))
+        self.get_vof_vstar_rhouu_consistent(two_way={
+            "eps_old": g.void_fraction_old_, "eps_new": g.void_fraction_, "inv_rhox": g.f_inv_rhox_,
+            "inv_rhoy": g.f_inv_rhoy_, "inv_rhoz": g.f_inv_rhoz_})
 
     def update_properties_by_alpha(self, rho0: float, rho1: float, mu0: float, mu1: float):
         """G_SMACSolver::update_properties_by_alpha (CFD/G_SMACSolver_VoF.cu:1544-1566):
@@ -570,10 +584,12 @@ def surface_tension_device(N, h, alpha, ct, sigma, work, fs):
                                               *map(_ptr, work), *map(_ptr, fs), ctypes.c_void_p(s)))
 
 
-def predict_vstar_device(N, h, bc: BoundaryConditions, fields: dict, dt, g, vs):
+def predict_vstar_device(N, h, bc: BoundaryConditions, fields: dict, dt, g, vs, two_way: dict | None = None):
     """smac_predict_vstar: u* of every F_INTERIOR face into vs = (vxs, vys,
     vzs).  fields maps the smac_momentum_fields names (fxt .. sfz) to CUDA
-    tensors; lam*/imp*/sf* may be missing (0)."""
+    tensors; lam*/imp*/sf* may be missing (0).  With two_way (the
+    smac_two_way_fields names eps_old, eps_new, inv_rhox.. to CUDA tensors)
+    the two-way-coupled form, smac_predict_vstar_two_way."""
     d = nat.GridDesc(*N, *h)
     s = torch.cuda.current_stream().cuda_stream
     table, keep = bc.table()
@@ -582,8 +598,17 @@ def predict_vstar_device(N, h, bc: BoundaryConditions, fields: dict, dt, g, vs):
         t = fields.get(name)
         setattr(mf, name, None if t is None else _ptr(t).value)
     dd = ctypes.c_double
-    nat.check(nat.load().smac_predict_vstar(ctypes.byref(d), ctypes.byref(table), ctypes.byref(mf), dd(dt), dd(g[0]),
-                                            dd(g[1]), dd(g[2]), *map(_ptr, vs), ctypes.c_void_p(s)))
+    if two_way is None:
+        nat.check(nat.load().smac_predict_vstar(ctypes.byref(d), ctypes.byref(table), ctypes.byref(mf), dd(dt),
+                                                dd(g[0]), dd(g[1]), dd(g[2]), *map(_ptr, vs), ctypes.c_void_p(s)))
+    else:
+        tw = nat.TwoWayFields()
+        for name, _ in nat.TwoWayFields._fields_:
+            t = two_way.get(name)
+            setattr(tw, name, None if t is None else _ptr(t).value)
+        nat.check(nat.load().smac_predict_vstar_two_way(ctypes.byref(d), ctypes.byref(table), ctypes.byref(mf),
+                                                        ctypes.byref(tw), dd(dt), dd(g[0]), dd(g[1]), dd(g[2]),
+                                                        *map(_ptr, vs), ctypes.c_void_p(s)))
     del keep
 
 

@@ -430,16 +430,21 @@ class MomentumCase:
     imp: tuple     # f_coupling_impulse_*
     sf: tuple      # f_ibm_solid_fraction_*
     vs: tuple      # f_v*_star_ before the call (faces it does not write keep these)
+    # the two-way-coupled predictor only (None: the one-way form)
+    eps_old: np.ndarray | None = None  # void_fraction_old_
+    eps_new: np.ndarray | None = None  # void_fraction_
+    fir: tuple | None = None           # f_inv_rho*_
 
 
 def momentum_case(N, seed, sides=("x+", "z-"), solid_fraction=0.0, extras=True, dt=0.01, g=(0.0, 0.0, -9.8),
-                  h=(0.03125, 0.03125, 0.03125)):
+                  h=(0.03125, 0.03125, 0.03125), two_way=False):
     """Seeded momentum-predictor inputs on the boundary set-up of post_case
     (all five boundary types, outlets on `sides`, clustered solids).  Fields:
     v, v* U[-1,1); mf U[-1,1) with 10% exact zeros (the flux-sign ties);
     face and cell viscosities U[1e-3, 1e-2); rho_old U[1, 1000); p U[-1,1);
     f_b U[1e-3, 1); with extras the coupling impulse U[-1e-6, 1e-6), the IBM
-    area and solid fractions U[0,1) with half of them 0."""
+    area and solid fractions U[0,1) with half of them 0.  two_way adds the
+    void fractions eps_old, eps_new U[0.4, 1) and f_inv_rho U[1e-3, 1)."""
     base = post_case(N, seed, h=h, dt=dt, g=g, sides=sides, solid_fraction=solid_fraction, lam=extras,
                      solid_margin=3)
     sh = shapes(base.N)
@@ -470,7 +475,10 @@ def momentum_case(N, seed, sides=("x+", "z-"), solid_fraction=0.0, extras=True, 
         mu=rnd(140, "cell", 1e-3, 1e-2), rho_old=rnd(141, "cell", 1.0, 1000.0), p=rnd(142, "cell"),
         fb=tuple(rnd(150 + k, key, 1e-3, 1.0) for k, key in enumerate("xyz")),
         imp=extra(160, -1e-6, 1e-6), sf=extra(180, 0.0, 1.0),
-        vs=tuple(rnd(200 + k, key) for k, key in enumerate("xyz")))
+        vs=tuple(rnd(200 + k, key) for k, key in enumerate("xyz")),
+        eps_old=rnd(210, "cell", 0.4, 1.0) if two_way else None,
+        eps_new=rnd(211, "cell", 0.4, 1.0) if two_way else None,
+        fir=tuple(rnd(212 + k, key, 1e-3, 1.0) for k, key in enumerate("xyz")) if two_way else None)
 
 
 PROPERTY_KEYS = ("rho", "rho_old", "inv_rho", "mu", "fbx", "fby", "fbz", "firx", "firy", "firz", "rhox", "rhoy",

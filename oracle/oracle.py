@@ -235,7 +235,9 @@ def surface_tension(N, h, alpha, ct, sigma, nx=None, ny=None, nz=None, kappa=Non
 def predict_vstar(m):
     """G_SMACSolver::get_vof_vstar_rhouu_consistent (CFD/G_SMACSolver.cu:90-1070)
     on a workloads.MomentumCase: returns (vxs, vys, vzs), copies of m.vs with
-    every F_INTERIOR face predicted."""
+    every F_INTERIOR face predicted.  A case with m.eps_old set takes the
+    two-way form, get_vof_vstar_rhouu_consistent_two_way (:1538-2203), with
+    m.fir in place of m.fb."""
     vs = [np.array(a, dtype=np.float64, order="C", copy=True) for a in m.vs]
     keep = []
 
@@ -258,11 +260,14 @@ def predict_vstar(m):
     bct = np.ascontiguousarray(m.bc_type, np.uint8)
     bv = [np.ascontiguousarray(a, np.float64) for a in m.bc_v]
     vsp = (ctypes.c_void_p * 3)(*(a.ctypes.data for a in vs))
-    lib().orc_predict_vstar(*m.N, c(m.h[0]), c(m.h[1]), c(m.h[2]), c(m.dt), c(m.g[0]), c(m.g[1]), c(m.g[2]),
-                            _u8(bct), *(_p(a) for a in bv), arr3(m.ft, np.uint8), arr3(m.bcid, np.uint8),
-                            arr3(m.lam, np.float64), arr3(m.v, np.float64), arr3(m.mf, np.float64),
-                            arr3(m.muf, np.float64), one(m.mu), one(m.rho_old), one(m.p), arr3(m.fb, np.float64),
-                            arr3(m.imp, np.float64), arr3(m.sf, np.float64), vsp)
+    tw = m.eps_old is not None
+    lib().orc_predict_vstar2(*m.N, c(m.h[0]), c(m.h[1]), c(m.h[2]), c(m.dt), c(m.g[0]), c(m.g[1]), c(m.g[2]),
+                             _u8(bct), *(_p(a) for a in bv), arr3(m.ft, np.uint8), arr3(m.bcid, np.uint8),
+                             arr3(m.lam, np.float64), arr3(m.v, np.float64), arr3(m.mf, np.float64),
+                             arr3(m.muf, np.float64), one(m.mu), one(m.rho_old), one(m.p),
+                             arr3(m.fir if tw else m.fb, np.float64), arr3(m.imp, np.float64),
+                             arr3(m.sf, np.float64), one(m.eps_old) if tw else None, one(m.eps_new) if tw else None,
+                             vsp)
     return tuple(vs)
 
 

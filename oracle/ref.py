@@ -260,11 +260,13 @@ class RefMomIO(ctypes.Structure):
         [(k, ctypes.c_double) for k in ("Lx", "Ly", "Lz", "dt", "gx", "gy", "gz")] + \
         [("num_ids", ctypes.c_int), ("bc_type", _u8p), ("bc_vx", _dp), ("bc_vy", _dp), ("bc_vz", _dp)] + \
         [(k, ctypes.c_void_p * 3) for k in ("ft", "bcid", "lam", "v", "mf", "muf", "fb", "imp", "sf")] + \
-        [("mu", _dp), ("rho_old", _dp), ("p", _dp), ("vs", ctypes.c_void_p * 3), ("ms", ctypes.c_double)]
+        [("mu", _dp), ("rho_old", _dp), ("p", _dp), ("vs", ctypes.c_void_p * 3), ("ms", ctypes.c_double),
+         ("eps_old", _dp), ("eps_new", _dp), ("fir", ctypes.c_void_p * 3)]
 
 
 def predict_vstar(m):
-    """Run the reference's get_vof_vstar_rhouu_consistent on a
+    """Run the reference's get_vof_vstar_rhouu_consistent (or, for a case
+    with eps_old set, get_vof_vstar_rhouu_consistent_two_way) on a
     mydemcfd_b200.workloads.MomentumCase (None fields as zeros): returns
     (vxs, vys, vzs, ms)."""
     L = lib()
@@ -296,6 +298,9 @@ def predict_vstar(m):
     io.lam, io.imp, io.sf = three(m.lam, like=m.v), three(m.imp, like=m.v), three(m.sf, like=m.v)
     io.v, io.mf, io.muf, io.fb = three(m.v), three(m.mf), three(m.muf), three(m.fb)
     io.mu, io.rho_old, io.p = _p(arr(m.mu)), _p(arr(m.rho_old)), _p(arr(m.p))
+    if m.eps_old is not None:
+        io.eps_old, io.eps_new = _p(arr(m.eps_old)), _p(arr(m.eps_new))
+        io.fir = three(m.fir)
     out = [np.array(a, dtype=np.float64, order="C", copy=True) for a in m.vs]
     io.vs = (ctypes.c_void_p * 3)(*(a.ctypes.data for a in out))
     rc = L.ref_predict_vstar(ctypes.byref(io))

@@ -377,9 +377,12 @@ struct ref_mom_io {
   const double *mu, *rho_old, *p;
   double* vs[3];  // in: u* before the call; out: after it
   double ms;      // out: device time
+  // set: the two-way form (void fractions and f_inv_rho); NULL: the one-way form
+  const double *eps_old, *eps_new, *fir[3];
 };
 
-// G_SMACSolver::get_vof_vstar_rhouu_consistent (CFD/G_SMACSolver.cu:1062-1070)
+// G_SMACSolver::get_vof_vstar_rhouu_consistent (CFD/G_SMACSolver.cu:1062-1070),
+// or with io->eps_old set get_vof_vstar_rhouu_consistent_two_way (:2196-2203),
 // on host arrays.  Returns 0 on success, -2 on a CUDA error.
 int ref_predict_vstar(ref_mom_io* io) {
   const int Nx = io->Nx, Ny = io->Ny, Nz = io->Nz;
@@ -404,6 +407,8 @@ int ref_predict_vstar(ref_mom_io* io) {
   put(hg.f_ibm_solid_fraction_x_, io->sf[0]); put(hg.f_ibm_solid_fraction_y_, io->sf[1]);
   put(hg.f_ibm_solid_fraction_z_, io->sf[2]);
   put(hg.mu_, io->mu); put(hg.rho_old_, io->rho_old); put(hg.p_, io->p);
+  put(hg.void_fraction_old_, io->eps_old); put(hg.void_fraction_, io->eps_new);
+  put(hg.f_inv_rhox_, io->fir[0]); put(hg.f_inv_rhoy_, io->fir[1]); put(hg.f_inv_rhoz_, io->fir[2]);
   put(hg.f_vx_star_, io->vs[0]); put(hg.f_vy_star_, io->vs[1]); put(hg.f_vz_star_, io->vs[2]);
   std::memcpy(hg.bc_.bcType_.data_, io->bc_type, (size_t)io->num_ids);
   std::memcpy(hg.bc_.vx_.data_, io->bc_vx, sizeof(double) * (size_t)io->num_ids);
@@ -421,7 +426,10 @@ int ref_predict_vstar(ref_mom_io* io) {
   cudaEvent_t ev[2];
   for (auto& x : ev) cudaEventCreate(&x);
   cudaEventRecord(ev[0], 0);
-  g.get_vof_vstar_rhouu_consistent(solv);
+  if (io->eps_old)
+    g.get_vof_vstar_rhouu_consistent_two_way(solv);
+  else
+    g.get_vof_vstar_rhouu_consistent(solv);
   cudaEventRecord(ev[1], 0);
   cudaDeviceSynchronize();
   float t = 0.f;

@@ -962,6 +962,8 @@ struct MomFields {
   const double* fb[3];     // 1/rho on faces
   const double* imp[3];    // coupling impulse (nullptr: 0)
   const double* sf[3];     // IBM solid fraction of the face (nullptr: 0)
+  const double* eps_old;   // two-way form only (nullptr: the one-way form)
+  const double* eps_new;
 };
 
 struct Idx3 {
@@ -1030,8 +1032,23 @@ double minmod(double dp, double dm) {  // d_minmod, CFD/G_SMACSolver.cu:67-88
 }
 double sgn1(double x) { return x < 0 ? -1. : 1.; }  // sgn, CFD/G_SMACSolver.h:130-139
 
+// Two-way form: eps_old averaged over the four cells around the edge on side
+// s along axis d of the family-a face q (its cells cm, c and their
+// neighbours along d), added in ascending index order as the reference
+// writes them (CFD/G_SMACSolver.cu:1610-1622, 1832-1844, 2050-2062).
+double eps_edge(const MomFields& F, int a, int d, const Idx3& q, int s) {
+  const Idx3 lc = s > 0 ? q : shifted(q, d, -1), lcm = shifted(lc, a, -1);
+  const Idx3 hc = shifted(lc, d, 1), hcm = shifted(lcm, d, 1);
+  const double* e = F.eps_old;
+  const double sum = d > a ? e[cell_off(F, lcm)] + e[cell_off(F, lc)] + e[cell_off(F, hcm)] + e[cell_off(F, hc)]
+                           : e[cell_off(F, lcm)] + e[cell_off(F, hcm)] + e[cell_off(F, lc)] + e[cell_off(F, hc)];
+  return 0.25 * sum;
+}
+
 // u* of the F_INTERIOR face q of family a: k_get_vof_vstar_rhouu_consistent_{x,y,z}
-// (CFD/G_SMACSolver.cu:90-1012) with the family's axis as a parameter.
+// (CFD/G_SMACSolver.cu:90-1012) with the family's axis as a parameter, or
+// with F.eps_old set the two-way form k_get_vof_vstar_rhouu_consistent_*_two_way
+// (:1538-2194).
 double vstar_face(const MomFields& F, int a, const Idx3& q, const double ih[3], const double ih2[3], double dt,
                   double g) {
   const double v0 = F.v[a][face_off(F, a, q)];
@@ -1046,7 +1063,9 @@ double vstar_face(const MomFields& F, int a, const Idx3& q, const double ih[3], 
   const Idx3 cm = shifted(q, a, -1);
   const double tau_p = F.mu[cell_off(F, q)] * (vp - v0);
   const double tau_m = F.mu[cell_off(F, cm)] * (v0 - vm);
-  double tmp = 2. * (tau_p - tau_m) * ih2[a];
+  const bool tw = F.eps_old != nullptr;
+  double tmp = tw ? 2. * (F.eps_old[cell_off(F, q)] * tau_p - F.eps_old[cell_off(F, cm)] * tau_m) * ih2[a]
+                  : 2. * (tau_p - tau_m) * ih2[a];
   for (int d = 0; d < 3; ++d) {
     if (d == a) continue;
     const Idx3 qd = shifted(q, d, 1), qda = shifted(qd, a, -1);
@@ -1056,7 +1075,10 @@ double vstar_face(const MomFields& F, int a, const Idx3& q, const double ih[3], 
     const double tp = mup * ((wp0 - wpm) * ih[a] + (vdp[d] - v0) * ih[d]);
     const double mum = 0.5 * (F.muf[d][face_off(F, d, q)] + F.muf[d][face_off(F, d, cm)]);
     const double tm = mum * ((w0 - wm) * ih[a] + (v0 - vdm[d]) * ih[d]);
-    tmp += (tp - tm) * ih[d];
+    if (tw)
+      tmp += (eps_edge(F, a, d, q, +1) * tp - eps_edge(F, a, d, q, -1) * tm) * ih[d];
+    else
+      tmp += (tp - tm) * ih[d];
   }
   // convection, MUSCL with minmod, in axis order
   for (int d = 0; d < 3; ++d) {
@@ -1087,10 +1109,19 @@ double vstar_face(const MomFields& F, int a, const Idx3& q, const double ih[3], 
   const size_t f = face_off(F, a, q);
   const double inv_rho = F.fb[a][f];
   const double rho_old_f = 0.5 * (F.rho_old[cell_off(F, q)] + F.rho_old[cell_off(F, cm)]);
-  tmp -= (F.p[cell_off(F, q)] - F.p[cell_off(F, cm)]) * ih[a];
   const double inv_volume = ih[0] * ih[1] * ih[2];
   const double coupling = (F.imp[a] ? F.imp[a][f] : 0.) * inv_volume;
-  double vs = inv_rho * (v0 * rho_old_f + coupling) + dt * (inv_rho * tmp + g);
+  double vs;
+  if (tw) {
+    const double eo = 0.5 * (F.eps_old[cell_off(F, cm)] + F.eps_old[cell_off(F, q)]);
+    const double en = 0.5 * (F.eps_new[cell_off(F, cm)] + F.eps_new[cell_off(F, q)]);
+    tmp -= eo * (F.p[cell_off(F, q)] - F.p[cell_off(F, cm)]) * ih[a];
+    const double inv_eps_rho = inv_rho / en;
+    vs = inv_eps_rho * (eo * rho_old_f * v0 + dt * tmp + coupling) + dt * g;
+  } else {
+    tmp -= (F.p[cell_off(F, q)] - F.p[cell_off(F, cm)]) * ih[a];
+    vs = inv_rho * (v0 * rho_old_f + coupling) + dt * (inv_rho * tmp + g);
+  }
   vs = (1.0 - (F.sf[a] ? F.sf[a][f] : 0.)) * vs;
   return vs;
 }
@@ -1105,13 +1136,18 @@ extern "C" {
 // convection - grad p) + g), scaled by 1 - IBM solid fraction.  Families in
 // the order x, y, z (independent: each reads only time-n fields).  Arrays
 // per family in the argument triples; lam/imp/sf may be NULL (0).
-void orc_predict_vstar(int Nx, int Ny, int Nz, double dx, double dy, double dz, double dt, double gx, double gy,
-                       double gz, const uint8_t* bct, const double* bvx, const double* bvy, const double* bvz,
-                       const uint8_t* const* ft, const uint8_t* const* id, const double* const* lam,
-                       const double* const* v, const double* const* mf, const double* const* muf, const double* mu,
-                       const double* rho_old, const double* p, const double* const* fb, const double* const* imp,
-                       const double* const* sf, double* const* vs) {
+// With eps_old and eps_new given (not NULL): the two-way form,
+// G_SMACSolver::get_vof_vstar_rhouu_consistent_two_way (:2196-2203), with fb
+// the faces' f_inv_rho.
+void orc_predict_vstar2(int Nx, int Ny, int Nz, double dx, double dy, double dz, double dt, double gx, double gy,
+                        double gz, const uint8_t* bct, const double* bvx, const double* bvy, const double* bvz,
+                        const uint8_t* const* ft, const uint8_t* const* id, const double* const* lam,
+                        const double* const* v, const double* const* mf, const double* const* muf, const double* mu,
+                        const double* rho_old, const double* p, const double* const* fb, const double* const* imp,
+                        const double* const* sf, const double* eps_old, const double* eps_new, double* const* vs) {
   MomFields F;
+  F.eps_old = eps_old;
+  F.eps_new = eps_new;
   F.N[0] = Nx; F.N[1] = Ny; F.N[2] = Nz;
   F.bct = bct;
   F.bv[0] = bvx; F.bv[1] = bvy; F.bv[2] = bvz;
@@ -1136,6 +1172,16 @@ void orc_predict_vstar(int Nx, int Ny, int Nz, double dx, double dy, double dz, 
           if (F.ft[a][f] != F_INTERIOR) continue;
           vs[a][f] = vstar_face(F, a, q, ih, ih2, dt, g[a]);
         }
+}
+
+void orc_predict_vstar(int Nx, int Ny, int Nz, double dx, double dy, double dz, double dt, double gx, double gy,
+                       double gz, const uint8_t* bct, const double* bvx, const double* bvy, const double* bvz,
+                       const uint8_t* const* ft, const uint8_t* const* id, const double* const* lam,
+                       const double* const* v, const double* const* mf, const double* const* muf, const double* mu,
+                       const double* rho_old, const double* p, const double* const* fb, const double* const* imp,
+                       const double* const* sf, double* const* vs) {
+  orc_predict_vstar2(Nx, Ny, Nz, dx, dy, dz, dt, gx, gy, gz, bct, bvx, bvy, bvz, ft, id, lam, v, mf, muf, mu, rho_old,
+                     p, fb, imp, sf, nullptr, nullptr, vs);
 }
 
 // The property update, G_SMACSolver::update_properties_by_alpha

@@ -69,6 +69,9 @@ MOMENTUM_CASES = [
     ("mom12x10x8_s1", dict(N=(12, 10, 8), seed=1, sides=("x+", "z-"))),
     ("mom16_s2_solid", dict(N=(16, 16, 16), seed=2, sides=("x-", "y+"), solid_fraction=0.3)),
     ("mom9x7x11_s3_noextras", dict(N=(9, 7, 11), seed=3, sides=("y-",), extras=False)),
+    # the two-way-coupled form (get_vof_vstar_rhouu_consistent_two_way)
+    ("mom2w12x10x8_s4", dict(N=(12, 10, 8), seed=4, sides=("x+", "z-"), two_way=True)),
+    ("mom2w16_s5_solid", dict(N=(16, 16, 16), seed=5, sides=("x-", "y+"), solid_fraction=0.3, two_way=True)),
 ]
 
 # The property update (update_properties_by_alpha): workloads.property_case kwargs.

@@ -313,9 +313,19 @@ def _momentum_fields(m):
     return f
 
 
+def _two_way_fields(m):
+    if m.eps_old is None:
+        return None
+    f = {"eps_old": _cuda(m.eps_old), "eps_new": _cuda(m.eps_new)}
+    for k, ax in enumerate("xyz"):
+        f["inv_rho" + ax] = _cuda(m.fir[k])
+    return f
+
+
 def run_predict(m):
     vs = [_cuda(a) for a in m.vs]
-    predict_vstar_device(m.N, m.h, BoundaryConditions(m.bc_type, *m.bc_v), _momentum_fields(m), m.dt, m.g, vs)
+    predict_vstar_device(m.N, m.h, BoundaryConditions(m.bc_type, *m.bc_v), _momentum_fields(m), m.dt, m.g, vs,
+                         two_way=_two_way_fields(m))
     torch.cuda.synchronize()
     return tuple(a.cpu().numpy() for a in vs)
 
@@ -325,6 +335,9 @@ def run_predict(m):
     dict(N=(16, 16, 16), seed=2, sides=("x-", "y+"), solid_fraction=0.3),
     dict(N=(9, 7, 11), seed=3, sides=("y-",), extras=False),
     dict(N=(33, 18, 20), seed=5, sides=("x-", "x+", "z+"), solid_fraction=0.2),
+    dict(N=(12, 10, 8), seed=4, sides=("x+", "z-"), two_way=True),
+    dict(N=(17, 14, 19), seed=6, sides=("y-", "z+"), solid_fraction=0.25, two_way=True),
+    dict(N=(9, 7, 11), seed=8, sides=("x-",), extras=False, two_way=True),
 ])
 def test_predict_vstar_bit_exact_against_oracle(spec):
     m = W.momentum_case(**spec)
@@ -514,3 +527,45 @@ def test_smac_step_update_properties_swaps_and_matches_oracle():
                     "rho" + ax: getattr(g, f"f_rho{ax}_"), "mu" + ax: getattr(g, f"f_mu{ax}_")})
     for k, v in got.items():
         assert np.array_equal(v.cpu().numpy(), want[k]), k
+
+
+@pytest.mark.skipif(not REF.available(), reason="reference build oracle/_ref not present")
+def test_predict_vstar_two_way_against_reference_library_128_and_time_256():
+    """The two-way-coupled predictor (get_vof_vstar_rhouu_consistent_two_way)
+    against the reference's own three kernels: bit for bit at 128^3, faster at
+    256^3."""
+    m = W.momentum_case((128, 128, 128), seed=16, sides=("x+", "z-"), solid_fraction=0.05, two_way=True)
+    *ref, _ = REF.predict_vstar(m)
+    for k, a, b in zip(("vxs", "vys", "vzs"), run_predict(m), ref):
+        assert np.array_equal(a, b), k
+    m = W.momentum_case((256, 256, 256), seed=17, sides=("x+",), solid_fraction=0.02, two_way=True)
+    REF.predict_vstar(m)  # loads the reference's kernels
+    *_, ref_ms = REF.predict_vstar(m)
+    fields, tw = _momentum_fields(m), _two_way_fields(m)
+    vs = [_cuda(a) for a in m.vs]
+    bc = BoundaryConditions(m.bc_type, *m.bc_v)
+    ms = _device_ms(lambda: predict_vstar_device(m.N, m.h, bc, fields, m.dt, m.g, vs, two_way=tw))
+    print(f"get_vof_vstar_rhouu_consistent_two_way 256^3: {ms * 1e3:.1f} us (reference {ref_ms * 1e3:.1f} us)")
+    assert ms < ref_ms
+
+
+def test_smac_step_two_way_predictor_matches_oracle():
+    """SMACStep.get_vof_vstar_rhouu_consistent_two_way on a DeviceGrid."""
+    m = W.momentum_case((14, 12, 10), seed=19, sides=("x+",), solid_fraction=0.2, two_way=True)
+    sh = W.shapes(m.N)
+    zc = lambda: torch.zeros(sh["cell"], dtype=torch.float64, device="cuda")  # noqa: E731
+    g = DeviceGrid(*m.N, *m.h, *(_cuda(a) for a in m.vs), *(_cuda(a) for a in m.fb), *(_cuda(a) for a in m.fir),
+                   _cuda(m.ct), *(_cuda(a) for a in m.ft), _cuda(m.p), zc(), zc(), *(_cuda(a) for a in m.v))
+    g.void_fraction_old_, g.void_fraction_ = _cuda(m.eps_old), _cuda(m.eps_new)
+    g.f_xbcid_, g.f_ybcid_, g.f_zbcid_ = (_cuda(a) for a in m.bcid)
+    g.f_ibm_area_solid_fraction_x_, g.f_ibm_area_solid_fraction_y_, g.f_ibm_area_solid_fraction_z_ = (
+        _cuda(a) for a in m.lam)
+    g.f_mfx_, g.f_mfy_, g.f_mfz_ = (_cuda(a) for a in m.mf)
+    g.f_mux_, g.f_muy_, g.f_muz_ = (_cuda(a) for a in m.muf)
+    g.mu_, g.rho_old_ = _cuda(m.mu), _cuda(m.rho_old)
+    g.f_coupling_impulse_x_, g.f_coupling_impulse_y_, g.f_coupling_impulse_z_ = (_cuda(a) for a in m.imp)
+    g.f_ibm_solid_fraction_x_, g.f_ibm_solid_fraction_y_, g.f_ibm_solid_fraction_z_ = (_cuda(a) for a in m.sf)
+    SMACStep(g, m.dt, g=m.g, bc=BoundaryConditions(m.bc_type, *m.bc_v)).get_vof_vstar_rhouu_consistent_two_way()
+    torch.cuda.synchronize()
+    for a, b in zip((g.f_vx_star_, g.f_vy_star_, g.f_vz_star_), O.predict_vstar(m)):
+        assert np.array_equal(a.cpu().numpy(), b)

@@ -600,3 +600,21 @@ def test_update_properties_oracle_matches_reference_golden(oracle_lib, name):
     for k in out:
         assert np.array_equal(out[k], arr[k]), k
     assert np.array_equal(arr["rho_old"], init["rho"])  # the swap keeps the previous rho
+
+
+def test_predict_vstar_two_way_with_unit_void_fraction_is_one_way(oracle_lib):
+    """eps_old = eps_new = 1 and f_inv_rho = f_b: every eps weight is exactly
+    1, so the two-way u* is the one-way u* up to the association of the last
+    update (inv_rho (eps rho u + dt tmp + imp/V) + dt g against
+    inv_rho (rho u + imp/V) + dt (inv_rho tmp + g))."""
+    import dataclasses
+    m = W.momentum_case((10, 9, 8), seed=7, sides=("x+", "y-"), solid_fraction=0.2)
+    ones = np.ones(W.shapes(m.N)["cell"])
+    m2 = dataclasses.replace(m, eps_old=ones, eps_new=ones, fir=m.fb)
+    for a, b in zip(oracle_lib.predict_vstar(m), oracle_lib.predict_vstar(m2)):
+        np.testing.assert_allclose(b, a, rtol=1e-12, atol=1e-12 * np.abs(a).max())
+    # and the weights do act: eps_new = 1/2 changes every predicted face
+    m3 = dataclasses.replace(m2, eps_new=0.5 * ones)
+    one, half = oracle_lib.predict_vstar(m2), oracle_lib.predict_vstar(m3)
+    inner = m.ft[0] == W.F_INTERIOR
+    assert np.all(one[0][inner] != half[0][inner])
