@@ -184,6 +184,16 @@ smac_status smac_update_properties(const smac_grid_desc* d, const smac_vof_param
                                    const uint8_t* celltype, const uint8_t* fxt, const uint8_t* fyt, const uint8_t* fzt,
                                    const smac_property_fields* out, void* stream);
 
+/* Poisson coefficients of the two-way-coupled step,
+ * G_CFDDEMCoupling::update_poisson_beta_two_way (Coupling/G_CFDDEMCoupling.cu:
+ * 419-460, called at Coupling/main.cu:533 after the property update):
+ * f_b = eps_f f_inv_rho, eps_f = (eps_L + eps_R)/2 of the face's two cells,
+ * on x-faces 1..Nx+1 x 1..Ny x 1..Nz (y and z alike); other faces keep their
+ * values.  eps: void_fraction_ (cells). */
+smac_status smac_poisson_beta_two_way(const smac_grid_desc* d, const double* eps, const double* firx,
+                                      const double* firy, const double* firz, double* fbx, double* fby, double* fbz,
+                                      void* stream);
+
 /* Outlet boundary faces: f_b = 2 f_b of the neighbouring face on the interior
  * side, where p = 0 is imposed.  G_SMACSolver::update_boundary_faces
  * (CFD/G_SMACSolver_VoF.cu:1798-1950), run after smac_assemble_vof.  The

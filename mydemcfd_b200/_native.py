@@ -96,7 +96,7 @@ EXPORTS = [
     "smac_selftest_sweep", "smac_apply_A_dot_noalloc", "smac_async_create", "smac_async_submit",
     "smac_async_wait", "smac_async_destroy", "smac_update_boundary_faces", "smac_update_pressure_ghost",
     "smac_update_velocity_ghost", "smac_face_gradp", "smac_update_vstar_boundary", "smac_surface_tension",
-    "smac_predict_vstar", "smac_predict_vstar_two_way", "smac_vti_block_bytes", "smac_vti_pack", "smac_vti_write", "smac_update_properties",
+    "smac_predict_vstar", "smac_predict_vstar_two_way", "smac_poisson_beta_two_way", "smac_vti_block_bytes", "smac_vti_pack", "smac_vti_write", "smac_update_properties",
 ]
 
 
@@ -144,6 +144,7 @@ def load(path: str = LIB_PATH):
         "smac_surface_tension": [ctypes.POINTER(GridDesc), dp, u8p, d, dp, dp, dp, dp, dp, dp, dp, dp, vp],
         "smac_predict_vstar": [ctypes.POINTER(GridDesc), ctypes.POINTER(BoundaryTable), ctypes.POINTER(MomentumFields),
                                d, d, d, d, dp, dp, dp, vp],
+        "smac_poisson_beta_two_way": [ctypes.POINTER(GridDesc), dp, dp, dp, dp, dp, dp, dp, vp],
         "smac_predict_vstar_two_way": [ctypes.POINTER(GridDesc), ctypes.POINTER(BoundaryTable),
                                        ctypes.POINTER(MomentumFields), ctypes.POINTER(TwoWayFields), d, d, d, d, dp,
                                        dp, dp, vp],

@@ -1132,6 +1132,34 @@ __global__ void __launch_bounds__(PR_TX* PR_TY) k_props(PropArgs A) {
   }
 }
 
+// ---------------------------------------------------------------------------
+// Two-way Poisson coefficients (G_CFDDEMCoupling::update_poisson_beta_two_way,
+// k_update_poisson_beta_two_way, Coupling/G_CFDDEMCoupling.cu:419-460):
+// f_b = eps_f f_inv_rho with eps_f the mean void fraction of the face's two
+// cells, on x-faces 1..Nx+1 x 1..Ny x 1..Nz and likewise for y and z.  One
+// thread per index (x, y, z) of the box 1..N+1 writes the faces there; the
+// void fractions of the cell and its three low neighbours come through L1.
+__global__ void __launch_bounds__(256) k_beta_two_way(RefDims R, const double* __restrict__ eps, const double* firx,
+                                                      const double* firy, const double* firz, double* fbx, double* fby,
+                                                      double* fbz) {
+  const int x = blockIdx.x * 32 + threadIdx.x + 1, y = blockIdx.y * 8 + threadIdx.y + 1, z = blockIdx.z + 1;
+  if (x > R.Nx + 1 || y > R.Ny + 1) return;
+  const long long c = R.cell(x, y, z), sx = R.Nx + 2, sxy = sx * (R.Ny + 2);
+  const double e = __ldg(eps + c);
+  if (y <= R.Ny && z <= R.Nz) {
+    const long long f = R.xf(x, y, z);
+    fbx[f] = DMUL(DMUL(0.5, DADD(__ldg(eps + c - 1), e)), firx[f]);
+  }
+  if (x <= R.Nx && z <= R.Nz) {
+    const long long f = R.yf(x, y, z);
+    fby[f] = DMUL(DMUL(0.5, DADD(__ldg(eps + c - sx), e)), firy[f]);
+  }
+  if (x <= R.Nx && y <= R.Ny) {
+    const long long f = R.zf(x, y, z);
+    fbz[f] = DMUL(DMUL(0.5, DADD(__ldg(eps + c - sxy), e)), firz[f]);
+  }
+}
+
 int sm_count() {
   static int n = 0;
   if (!n) {
@@ -1444,6 +1472,21 @@ smac_status smac_update_properties(const smac_grid_desc* d, const smac_vof_param
   const dim3 grid((unsigned)((d->nx + 3 + PR_TX - 1) / PR_TX), (unsigned)((d->ny + 3 + PR_TY - 1) / PR_TY),
                   (unsigned)(d->nz + 3));
   k_props<<<grid, dim3(PR_TX, PR_TY), 0, (cudaStream_t)stream>>>(A);
+  return launch_status(fn);
+}
+
+smac_status smac_poisson_beta_two_way(const smac_grid_desc* d, const double* eps, const double* firx,
+                                      const double* firy, const double* firz, double* fbx, double* fby, double* fbz,
+                                      void* stream) {
+  static const char* fn = "smac_poisson_beta_two_way";
+  if (!d || !eps || !firx || !firy || !firz || !fbx || !fby || !fbz) {
+    smac::set_error_text("%s: null argument", fn);
+    return SMAC_BAD_ARG;
+  }
+  if (bad_desc(d, fn, 1)) return SMAC_BAD_SHAPE;
+  const RefDims R{d->nx, d->ny, d->nz};
+  const dim3 grid((unsigned)((d->nx + 1 + 31) / 32), (unsigned)((d->ny + 1 + 7) / 8), (unsigned)(d->nz + 1));
+  k_beta_two_way<<<grid, dim3(32, 8), 0, (cudaStream_t)stream>>>(R, eps, firx, firy, firz, fbx, fby, fbz);
   return launch_status(fn);
 }
 

@@ -388,6 +388,16 @@ class SMACStep:
             "eps_old": g.void_fraction_old_, "eps_new": g.void_fraction_, "inv_rhox": g.f_inv_rhox_,
             "inv_rhoy": g.f_inv_rhoy_, "inv_rhoz": g.f_inv_rhoz_})
 
+    def update_poisson_beta_two_way(self):
+        """G_CFDDEMCoupling::update_poisson_beta_two_way
+        (Coupling/G_CFDDEMCoupling.cu:419-460): f_b*_ = eps_f f_inv_rho*_ from
+        void_fraction_ (smac_poisson_beta_two_way)."""
+        g = self.grid_
+        if g.void_fraction_ is None:
+            raise ValueError("update_poisson_beta_two_way needs the grid's void_fraction_")
+        poisson_beta_two_way_device(g.N, (g.dx_, g.dy_, g.dz_), g.void_fraction_,
+                                    (g.f_inv_rhox_, g.f_inv_rhoy_, g.f_inv_rhoz_), (g.f_bx_, g.f_by_, g.f_bz_))
+
     def update_properties_by_alpha(self, rho0: float, rho1: float, mu0: float, mu1: float):
         """G_SMACSolver::update_properties_by_alpha (CFD/G_SMACSolver_VoF.cu:1544-1566):
         rho_ and rho_old_ swap (the previous rho is kept as rho_old_), then
@@ -610,6 +620,15 @@ def predict_vstar_device(N, h, bc: BoundaryConditions, fields: dict, dt, g, vs, 
                                                         ctypes.byref(tw), dd(dt), dd(g[0]), dd(g[1]), dd(g[2]),
                                                         *map(_ptr, vs), ctypes.c_void_p(s)))
     del keep
+
+
+def poisson_beta_two_way_device(N, h, eps, fir, fb):
+    """smac_poisson_beta_two_way: fb = (fbx, fby, fbz) <- eps_f * fir on the
+    interior box faces (CUDA tensors, written in place)."""
+    d = nat.GridDesc(*N, *h)
+    s = torch.cuda.current_stream().cuda_stream
+    nat.check(nat.load().smac_poisson_beta_two_way(ctypes.byref(d), _ptr(eps), *map(_ptr, fir), *map(_ptr, fb),
+                                                   ctypes.c_void_p(s)))
 
 
 def update_properties_device(N, h, rho0, rho1, mu0, mu1, alpha, ct, ft, out: dict):

@@ -505,3 +505,20 @@ def property_case(N, seed, solid_fraction=0.0, rho=(1.0, 1000.0), mu=(1e-3, 1e-1
         kind = "cell" if key in ("rho", "rho_old", "inv_rho", "mu") else key[-1]
         init[key] = uniform_pm1(substream(seed, 310 + k), int(np.prod(sh[kind]))).reshape(sh[kind])
     return N, base.h, (rho[0], rho[1], mu[0], mu[1]), np.ascontiguousarray(alpha), base.ct, base.ft, init
+
+
+def beta_two_way_case(N, seed, h=(0.03125, 0.03125, 0.03125)):
+    """Inputs of the two-way Poisson coefficients: void fraction U[0.4, 1) on
+    the cells, f_inv_rho U[1e-3, 1) and f_b U[-1, 1) (its value before the
+    call) on the faces.  Returns (N, h, eps, fir, fb)."""
+    N = tuple(int(n) for n in N)
+    sh = shapes(N)
+
+    def rnd(tag, key, lo, hi):
+        n = int(np.prod(sh[key]))
+        return np.ascontiguousarray((lo + (hi - lo) * uniform01(substream(seed, tag), n)).reshape(sh[key]))
+
+    eps = rnd(400, "cell", 0.4, 1.0)
+    fir = tuple(rnd(401 + k, key, 1e-3, 1.0) for k, key in enumerate("xyz"))
+    fb = tuple(rnd(404 + k, key, -1.0, 1.0) for k, key in enumerate("xyz"))
+    return N, tuple(h), eps, fir, fb

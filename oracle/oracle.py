@@ -424,3 +424,15 @@ def update_properties(N, rho0, rho1, mu0, mu1, alpha, ct, ft, init):
                                 _p(out["inv_rho"]), _p(out["mu"]), p3(("fbx", "fby", "fbz")),
                                 p3(("firx", "firy", "firz")), p3(("rhox", "rhoy", "rhoz")), p3(("mux", "muy", "muz")))
     return out
+
+
+def poisson_beta_two_way(N, eps, fir, fb):
+    """G_CFDDEMCoupling::update_poisson_beta_two_way (Coupling/G_CFDDEMCoupling.cu:
+    419-460) on copies of fb: returns (fbx, fby, fbz) with f_b = eps_f f_inv_rho
+    on the interior box faces."""
+    out = [np.array(a, dtype=np.float64, order="C", copy=True) for a in fb]
+    firs = [np.ascontiguousarray(a, np.float64) for a in fir]
+    e = np.ascontiguousarray(eps, np.float64)
+    lib().orc_poisson_beta_two_way(*N, _p(e), (ctypes.c_void_p * 3)(*(a.ctypes.data for a in firs)),
+                                   (ctypes.c_void_p * 3)(*(a.ctypes.data for a in out)))
+    return tuple(out)

@@ -372,3 +372,32 @@ def update_properties(N, h, rho0, rho1, mu0, mu1, alpha, ct, ft, init):
     if rc != 0:
         raise RuntimeError(f"ref_update_properties returned {rc}")
     return out, io.ms
+
+
+class RefBetaIO(ctypes.Structure):
+    _fields_ = [("Nx", ctypes.c_int), ("Ny", ctypes.c_int), ("Nz", ctypes.c_int)] + \
+        [(k, ctypes.c_double) for k in ("Lx", "Ly", "Lz")] + \
+        [("eps", _dp), ("fir", ctypes.c_void_p * 3), ("fb", ctypes.c_void_p * 3), ("ms", ctypes.c_double)]
+
+
+def poisson_beta_two_way(N, h, eps, fir, fb):
+    """Run the reference's G_CFDDEMCoupling::update_poisson_beta_two_way:
+    returns (fbx, fby, fbz, ms), fb after the call."""
+    L = lib()
+    if not hasattr(L, "_beta_set"):
+        L.ref_poisson_beta_two_way.restype = ctypes.c_int
+        L.ref_poisson_beta_two_way.argtypes = [ctypes.POINTER(RefBetaIO)]
+        L._beta_set = True
+    e = np.ascontiguousarray(eps, np.float64)
+    firs = [np.ascontiguousarray(a, np.float64) for a in fir]
+    out = [np.array(a, dtype=np.float64, order="C", copy=True) for a in fb]
+    io = RefBetaIO()
+    io.Nx, io.Ny, io.Nz = N
+    io.Lx, io.Ly, io.Lz = (n * hh for n, hh in zip(N, h))
+    io.eps = _p(e)
+    io.fir = (ctypes.c_void_p * 3)(*(a.ctypes.data for a in firs))
+    io.fb = (ctypes.c_void_p * 3)(*(a.ctypes.data for a in out))
+    rc = L.ref_poisson_beta_two_way(ctypes.byref(io))
+    if rc != 0:
+        raise RuntimeError(f"ref_poisson_beta_two_way returned {rc}")
+    return (*out, io.ms)

@@ -28,6 +28,7 @@
 
 #include "G_SMACSolver.h"
 #include "SMACSolver.h"
+#include "../Coupling/G_CFDDEMCoupling.h"
 #include "pressure_solver/G_GMGSolver.h"
 #include "pressure_solver/G_PCGSolver.h"
 
@@ -509,3 +510,58 @@ int ref_update_properties(ref_props_io* io) {
 }
 
 }  // extern "C"
+
+struct ref_beta_io {
+  int Nx, Ny, Nz;
+  double Lx, Ly, Lz;
+  const double* eps;       // void_fraction_
+  const double* fir[3];    // f_inv_rho*_
+  double* fb[3];           // in: f_b*_ before the call; out: after it
+  double ms;               // out: device time
+};
+
+// G_CFDDEMCoupling::update_poisson_beta_two_way (Coupling/G_CFDDEMCoupling.cu:
+// 419-460) on host arrays, launched with the dimensions the coupled driver
+// gives it (those of G_SMACSolver::set_block_grid, Coupling/main.cu:484-485).
+// Returns 0 on success, -2 on a CUDA error.
+extern "C" int ref_poisson_beta_two_way(ref_beta_io* io) {
+  const int Nx = io->Nx, Ny = io->Ny, Nz = io->Nz;
+  SMACSolver solv;
+  solv.set_calc_properties(0., 0., 0., io->Lx, io->Ly, io->Lz, Nx, Ny, Nz);
+  solv.grid_.bc_.num_boundary_id_ = 1;  // sizes the boundary table solver_malloc allocates
+  solv.solver_malloc();
+  StaggeredGrid& hg = solv.grid_;
+  put(hg.void_fraction_, io->eps);
+  put(hg.f_inv_rhox_, io->fir[0]); put(hg.f_inv_rhoy_, io->fir[1]); put(hg.f_inv_rhoz_, io->fir[2]);
+  put(hg.f_bx_, (const double*)io->fb[0]); put(hg.f_by_, (const double*)io->fb[1]);
+  put(hg.f_bz_, (const double*)io->fb[2]);
+  G_SMACSolver g;
+  g.set_calc_properties(0., 0., 0., io->Lx, io->Ly, io->Lz, Nx, Ny, Nz);
+  g.grid_.bc_.num_boundary_id_ = 1;
+  g.solver_malloc();
+  g.cpuTogpu(solv.grid_);
+  g.set_block_grid(Nx, Ny, Nz);
+  G_CFDDEMCoupling cpl;
+  cpl.block_dim_ = g.block_dim_;
+  cpl.grid_dim_ = g.grid_dim_;
+  cudaDeviceSynchronize();
+  cudaEvent_t ev[2];
+  for (auto& x : ev) cudaEventCreate(&x);
+  cudaEventRecord(ev[0], 0);
+  cpl.update_poisson_beta_two_way(g.grid_);
+  cudaEventRecord(ev[1], 0);
+  cudaDeviceSynchronize();
+  float t = 0.f;
+  cudaEventElapsedTime(&t, ev[0], ev[1]);
+  io->ms = t;
+  for (auto& x : ev) cudaEventDestroy(x);
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) {
+    g.gpuTocpu(solv.grid_);
+    get(hg.f_bx_, io->fb[0]); get(hg.f_by_, io->fb[1]); get(hg.f_bz_, io->fb[2]);
+    e = cudaGetLastError();
+  }
+  g.solver_free();
+  solv.solver_free();
+  return e == cudaSuccess ? 0 : -2;
+}

@@ -1184,6 +1184,27 @@ void orc_predict_vstar(int Nx, int Ny, int Nz, double dx, double dy, double dz, 
                      p, fb, imp, sf, nullptr, nullptr, vs);
 }
 
+// The two-way Poisson coefficients, G_CFDDEMCoupling::update_poisson_beta_two_way
+// (Coupling/G_CFDDEMCoupling.cu:419-460): f_b = (eps_L + eps_R)/2 * f_inv_rho
+// on x-faces 1..Nx+1 x 1..Ny x 1..Nz, y-faces 1..Nx x 1..Ny+1 x 1..Nz, z-faces
+// 1..Nx x 1..Ny x 1..Nz+1.
+void orc_poisson_beta_two_way(int Nx, int Ny, int Nz, const double* eps, const double* const* fir,
+                              double* const* fb) {
+  const long long sx = Nx + 2, sxy = sx * (Ny + 2);
+  for (int a = 0; a < 3; ++a) {
+    const long long S0 = Nx + 2 + (a == 0), S1 = Ny + 2 + (a == 1);
+    const long long step = a == 0 ? 1 : a == 1 ? sx : sxy;
+    const int ex = Nx + (a == 0), ey = Ny + (a == 1), ez = Nz + (a == 2);
+    for (int z = 1; z <= ez; ++z)
+      for (int y = 1; y <= ey; ++y)
+        for (int x = 1; x <= ex; ++x) {
+          const long long c = z * sxy + y * sx + x, f = ((long long)z * S1 + y) * S0 + x;
+          const double epsf = 0.5 * (eps[c - step] + eps[c]);
+          fb[a][f] = epsf * fir[a][f];
+        }
+  }
+}
+
 // The property update, G_SMACSolver::update_properties_by_alpha
 // (CFD/G_SMACSolver_VoF.cu:1543-1566), after its swap of rho_ and rho_old_
 // (which the caller does by swapping arrays):

@@ -46,7 +46,7 @@ def golden_names():
     if not os.path.isdir(GOLDEN):
         return []
     return sorted(f[:-4] for f in os.listdir(GOLDEN)
-                  if f.endswith(".npz") and not f.startswith(("post", "vstar", "surface", "mom", "props")))
+                  if f.endswith(".npz") and not f.startswith(("post", "vstar", "surface", "mom", "props", "beta")))
 
 
 def surface_golden_names():
@@ -129,3 +129,16 @@ def property_case_from_spec(spec):
     spec = dict(spec)
     spec["N"] = tuple(spec["N"])
     return W.property_case(**spec)
+
+
+def beta_golden_names():
+    """Fixtures of the reference's update_poisson_beta_two_way."""
+    if not os.path.isdir(GOLDEN):
+        return []
+    return sorted(f[:-4] for f in os.listdir(GOLDEN) if f.endswith(".npz") and f.startswith("beta"))
+
+
+def beta_case_from_spec(spec):
+    spec = dict(spec)
+    spec["N"] = tuple(spec["N"])
+    return W.beta_two_way_case(**spec)

@@ -74,6 +74,12 @@ MOMENTUM_CASES = [
     ("mom2w16_s5_solid", dict(N=(16, 16, 16), seed=5, sides=("x-", "y+"), solid_fraction=0.3, two_way=True)),
 ]
 
+# The two-way Poisson coefficients (update_poisson_beta_two_way): workloads.beta_two_way_case kwargs.
+BETA_CASES = [
+    ("beta2w12x10x8_s1", dict(N=(12, 10, 8), seed=1)),
+    ("beta2w7x9x5_s2", dict(N=(7, 9, 5), seed=2)),
+]
+
 # The property update (update_properties_by_alpha): workloads.property_case kwargs.
 PROPERTY_CASES = [
     ("props12x10x8_s1", dict(N=(12, 10, 8), seed=1)),
@@ -140,6 +146,13 @@ def main():
         N, h, (r0, r1, m0, m1), alpha, ct, ft, init = W.property_case(**spec)
         out, _ = REF.update_properties(N, h, r0, r1, m0, m1, alpha, ct, ft, init)
         np.savez_compressed(os.path.join(args.out, name + ".npz"), meta=np.array(json.dumps(spec)), **out)
+        post_index[name] = spec
+        print(name, spec, flush=True)
+    for name, spec in BETA_CASES:
+        N, h, eps, fir, fb = W.beta_two_way_case(**spec)
+        fbx, fby, fbz, _ = REF.poisson_beta_two_way(N, h, eps, fir, fb)
+        np.savez_compressed(os.path.join(args.out, name + ".npz"), meta=np.array(json.dumps(spec)), fbx=fbx, fby=fby,
+                            fbz=fbz)
         post_index[name] = spec
         print(name, spec, flush=True)
     with open(os.path.join(args.out, "post_index.json"), "w") as f:

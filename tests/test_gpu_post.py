@@ -17,12 +17,13 @@ import torch
 from mydemcfd_b200 import _native as nat
 from mydemcfd_b200 import workloads as W
 from mydemcfd_b200.solver import (BoundaryConditions, DeviceGrid, SMACStep, face_gradp_device, predict_vstar_device,
-                                  surface_tension_device, update_pressure_ghost_device, update_properties_device,
+                                  poisson_beta_two_way_device, surface_tension_device,
+                                  update_pressure_ghost_device, update_properties_device,
                                   update_velocity_ghost_device, update_vstar_boundary_device)
 from oracle import oracle as O
 from oracle import ref as REF
 
-from _cases import (load_golden, momentum_case_from_spec, momentum_golden_names, post_case_from_spec,
+from _cases import (beta_case_from_spec, beta_golden_names, load_golden, momentum_case_from_spec, momentum_golden_names, post_case_from_spec,
                     post_golden_names, property_case_from_spec, property_golden_names, surface_case_from_spec,
                     surface_golden_names, vstar_golden_names)
 
@@ -569,3 +570,42 @@ def test_smac_step_two_way_predictor_matches_oracle():
     torch.cuda.synchronize()
     for a, b in zip((g.f_vx_star_, g.f_vy_star_, g.f_vz_star_), O.predict_vstar(m)):
         assert np.array_equal(a.cpu().numpy(), b)
+
+
+# ---------------------------------------------------------------------------
+# the two-way Poisson coefficients (update_poisson_beta_two_way)
+
+def run_beta(N, h, eps, fir, fb):
+    out = [_cuda(a) for a in fb]
+    poisson_beta_two_way_device(N, h, _cuda(eps), [_cuda(a) for a in fir], out)
+    torch.cuda.synchronize()
+    return tuple(a.cpu().numpy() for a in out)
+
+
+@pytest.mark.parametrize("N", [(12, 10, 8), (1, 6, 3), (33, 17, 9)])
+def test_poisson_beta_two_way_bit_exact_against_oracle(N):
+    N, h, eps, fir, fb = W.beta_two_way_case(N, seed=5)
+    for a, b in zip(run_beta(N, h, eps, fir, fb), O.poisson_beta_two_way(N, eps, fir, fb)):
+        assert np.array_equal(a, b)
+
+
+@pytest.mark.parametrize("name", beta_golden_names())
+def test_poisson_beta_two_way_bit_exact_against_reference_golden(name):
+    meta, arr = load_golden(name)
+    for k, a in zip(("fbx", "fby", "fbz"), run_beta(*beta_case_from_spec(meta))):
+        assert np.array_equal(a, arr[k]), k
+
+
+@pytest.mark.skipif(not REF.available(), reason="reference build oracle/_ref not present")
+def test_poisson_beta_two_way_against_reference_library_and_time_256():
+    case = W.beta_two_way_case((64, 48, 40), seed=6)
+    *ref, _ = REF.poisson_beta_two_way(*case)
+    for a, b in zip(run_beta(*case), ref):
+        assert np.array_equal(a, b)
+    N, h, eps, fir, fb = W.beta_two_way_case((256, 256, 256), seed=7)
+    REF.poisson_beta_two_way(N, h, eps, fir, fb)  # loads the reference's kernel
+    *_, ref_ms = REF.poisson_beta_two_way(N, h, eps, fir, fb)
+    e, fi, out = _cuda(eps), [_cuda(a) for a in fir], [_cuda(a) for a in fb]
+    ms = _device_ms(lambda: poisson_beta_two_way_device(N, h, e, fi, out))
+    print(f"update_poisson_beta_two_way 256^3: {ms * 1e3:.1f} us (reference {ref_ms * 1e3:.1f} us)")
+    assert ms < ref_ms

@@ -9,7 +9,7 @@ from mydemcfd_b200 import workloads as W
 from _cases import (build_case, fluid_demeaned, golden_names, load_golden, post_case_from_spec, post_golden_names,
                     ref_grid, rel_err, surface_case_from_spec, surface_golden_names, vstar_golden_names,
                     momentum_case_from_spec, momentum_golden_names, property_case_from_spec,
-                    property_golden_names)
+                    property_golden_names, beta_case_from_spec, beta_golden_names)
 
 
 def test_box_types_match_reference_setup(oracle_lib):
@@ -618,3 +618,35 @@ def test_predict_vstar_two_way_with_unit_void_fraction_is_one_way(oracle_lib):
     one, half = oracle_lib.predict_vstar(m2), oracle_lib.predict_vstar(m3)
     inner = m.ft[0] == W.F_INTERIOR
     assert np.all(one[0][inner] != half[0][inner])
+
+
+# ---------------------------------------------------------------------------
+# the two-way Poisson coefficients (update_poisson_beta_two_way)
+
+def test_poisson_beta_two_way_known_answer(oracle_lib):
+    """eps = 1: f_b = f_inv_rho on the interior box faces, untouched elsewhere;
+    eps = 1/2 on one side of a face: f_b = 3/4 f_inv_rho there."""
+    N, h, eps, fir, fb = W.beta_two_way_case((6, 5, 4), seed=3)
+    ones = np.ones_like(eps)
+    out = oracle_lib.poisson_beta_two_way(N, ones, fir, fb)
+    nx, ny, nz = N
+    box = [(slice(1, nz + 1), slice(1, ny + 1), slice(1, nx + 2)), (slice(1, nz + 1), slice(1, ny + 2), slice(1, nx + 1)),
+           (slice(1, nz + 2), slice(1, ny + 1), slice(1, nx + 1))]
+    for a in range(3):
+        assert np.array_equal(out[a][box[a]], fir[a][box[a]])
+        keep = np.ones(out[a].shape, bool)
+        keep[box[a]] = False
+        assert np.array_equal(out[a][keep], fb[a][keep])
+    half = ones.copy()
+    half[2, 2, 2] = 0.5   # cell (x, y, z) = (2, 2, 2)
+    out = oracle_lib.poisson_beta_two_way(N, half, fir, fb)
+    assert out[0][2, 2, 2] == 0.75 * fir[0][2, 2, 2] and out[0][2, 2, 3] == 0.75 * fir[0][2, 2, 3]
+
+
+@pytest.mark.skipif(not beta_golden_names(), reason="no two-way coefficient golden vectors")
+@pytest.mark.parametrize("name", beta_golden_names())
+def test_poisson_beta_two_way_oracle_matches_reference_golden(oracle_lib, name):
+    meta, arr = load_golden(name)
+    N, h, eps, fir, fb = beta_case_from_spec(meta)
+    for k, a in zip(("fbx", "fby", "fbz"), oracle_lib.poisson_beta_two_way(N, eps, fir, fb)):
+        assert np.array_equal(a, arr[k]), k
