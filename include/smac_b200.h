@@ -335,6 +335,30 @@ smac_status smac_predict_vstar_two_way(const smac_grid_desc* d, const smac_bound
                                        double gx, double gy, double gz, double* vxs, double* vys, double* vzs,
                                        void* stream);
 
+/* Inputs of the mass-flux update (device pointers, reference layout). */
+typedef struct {
+  const uint8_t *fxt, *fyt, *fzt;           /* f_*type_ */
+  const uint8_t *fxbcid, *fybcid, *fzbcid;  /* f_*bcid_ */
+  const double *lamx, *lamy, *lamz;         /* f_ibm_area_solid_fraction_*_ (NULL: 0) */
+  const double *vx, *vy, *vz;               /* f_v*_ */
+  const double *Fx, *Fy, *Fz;               /* f_F*_accum_: the accumulated volume-fraction flux */
+} smac_mass_flux_fields;
+
+/* The advecting mass flux the momentum predictor reads,
+ * G_SMACSolver::compute_mass_flux_from_alpha_flux (CFD/G_SMACSolver_VoF.cu:
+ * 1708-1795, called at CFD/main.cu:298): on every face of the three families
+ * mf = rho0 q + (rho1 - rho0) F_accum h / dt, q the face velocity by the
+ * boundary face rule (as smac_predict_vstar reads it).  With eps_half (the
+ * grid's void_fraction_half_, cells) the two-way form
+ * compute_mass_flux_from_alpha_flux_two_way (:2472-2687, Coupling/main.cu:531):
+ * q = eps_f u_f on faces 1..N+1 along their axis (eps_f the mean of the two
+ * cells, the one interior cell's at faces 1 and N+1), mf = 0 on faces 0 and
+ * N+2. */
+smac_status smac_mass_flux_from_alpha_flux(const smac_grid_desc* d, const smac_boundary_table* bc,
+                                           const smac_mass_flux_fields* in, double rho0, double rho1, double dt,
+                                           const double* eps_half, double* mfx, double* mfy, double* mfz,
+                                           void* stream);
+
 /* Wall-face u* before the projection, G_SMACSolver::update_vstar_boundary
  * (CFD/G_SMACSolver.cu:1044-1052, k_update_v*star_boundary,
  * CFD/G_BoundaryFunctions.cu:3-71, CFD/G_BoundaryFunctions.h:369-470), in

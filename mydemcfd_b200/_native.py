@@ -68,6 +68,13 @@ class TwoWayFields(ctypes.Structure):
     _fields_ = [(k, ctypes.c_void_p) for k in ("eps_old", "eps_new", "inv_rhox", "inv_rhoy", "inv_rhoz")]
 
 
+class MassFluxFields(ctypes.Structure):
+    """smac_mass_flux_fields: the inputs of the mass-flux update."""
+    _fields_ = [(k, ctypes.c_void_p) for k in (
+        "fxt", "fyt", "fzt", "fxbcid", "fybcid", "fzbcid", "lamx", "lamy", "lamz", "vx", "vy", "vz",
+        "Fx", "Fy", "Fz")]
+
+
 class VofParams(ctypes.Structure):
     _fields_ = [(k, ctypes.c_double) for k in ("rho0", "rho1", "mu0", "mu1")]
 
@@ -96,7 +103,8 @@ EXPORTS = [
     "smac_selftest_sweep", "smac_apply_A_dot_noalloc", "smac_async_create", "smac_async_submit",
     "smac_async_wait", "smac_async_destroy", "smac_update_boundary_faces", "smac_update_pressure_ghost",
     "smac_update_velocity_ghost", "smac_face_gradp", "smac_update_vstar_boundary", "smac_surface_tension",
-    "smac_predict_vstar", "smac_predict_vstar_two_way", "smac_poisson_beta_two_way", "smac_vti_block_bytes", "smac_vti_pack", "smac_vti_write", "smac_update_properties",
+    "smac_predict_vstar", "smac_predict_vstar_two_way", "smac_poisson_beta_two_way", "smac_mass_flux_from_alpha_flux",
+    "smac_vti_block_bytes", "smac_vti_pack", "smac_vti_write", "smac_update_properties",
 ]
 
 
@@ -145,6 +153,8 @@ def load(path: str = LIB_PATH):
         "smac_predict_vstar": [ctypes.POINTER(GridDesc), ctypes.POINTER(BoundaryTable), ctypes.POINTER(MomentumFields),
                                d, d, d, d, dp, dp, dp, vp],
         "smac_poisson_beta_two_way": [ctypes.POINTER(GridDesc), dp, dp, dp, dp, dp, dp, dp, vp],
+        "smac_mass_flux_from_alpha_flux": [ctypes.POINTER(GridDesc), ctypes.POINTER(BoundaryTable),
+                                           ctypes.POINTER(MassFluxFields), d, d, d, dp, dp, dp, dp, vp],
         "smac_predict_vstar_two_way": [ctypes.POINTER(GridDesc), ctypes.POINTER(BoundaryTable),
                                        ctypes.POINTER(MomentumFields), ctypes.POINTER(TwoWayFields), d, d, d, d, dp,
                                        dp, dp, vp],

@@ -1133,6 +1133,55 @@ __global__ void __launch_bounds__(PR_TX* PR_TY) k_props(PropArgs A) {
 }
 
 // ---------------------------------------------------------------------------
+// Advecting mass flux from the accumulated volume-fraction flux
+// (G_SMACSolver::compute_mass_flux_from_alpha_flux, k_compute_mass_flux_from_alpha_flux,
+// CFD/G_SMACSolver_VoF.cu:1708-1795; two-way form
+// k_compute_mass_flux_from_alpha_flux_two_way :2472-2687): on every face of
+// the three families mf = rho0 q + (rho1 - rho0) F_accum h / dt with q the
+// face velocity by the boundary face rule (m_face_val).  Two-way: q = eps_f
+// u_f with eps_f the mean void_fraction_half_ of the face's cells (the first
+// and last faces along the axis take their one interior cell's), and the
+// faces at 0 and N+2 along the axis get 0.
+
+struct FluxArgs {
+  MomArgs M;            // ft, id, lam, v and the boundary table of the face rule
+  const double* Fa[3];  // f_F*_accum_
+  const double* epsh;   // void_fraction_half_ (two-way); nullptr: the one-way form
+  double* mf[3];
+  double rho0, drho, hdt[3];  // h_d / dt as the reference forms it: h_d * (1 / dt)
+};
+
+template <int F, bool TW>
+__device__ __forceinline__ void flux_face(const FluxArgs& A, int x, int y, int z) {
+  const MomArgs& M = A.M;
+  const long long f = x * M.st[F][0] + y * M.st[F][1] + z * M.st[F][2];
+  const double aq = DMUL(A.Fa[F][f], A.hdt[F]);
+  double q = m_face_val<F>(M, f);
+  if (TW) {
+    const int along = F == 0 ? x : F == 1 ? y : z, n = M.N[F];
+    if (along < 1 || along > n + 1) {
+      A.mf[F][f] = 0.0;
+      return;
+    }
+    const long long c = x * M.st[3][0] + y * M.st[3][1] + z * M.st[3][2], s = M.st[3][F];
+    const double e = along == 1 ? A.epsh[c] : along == n + 1 ? A.epsh[c - s] : DMUL(0.5, DADD(A.epsh[c - s], A.epsh[c]));
+    q = DMUL(e, q);
+  }
+  A.mf[F][f] = DADD(DMUL(A.rho0, q), DMUL(A.drho, aq));
+}
+
+// One thread per index (x, y, z) of the box 0..N+2 writes the x-, y- and
+// z-face there (each family over its own extent).
+template <bool TW>
+__global__ void __launch_bounds__(256) k_mass_flux(FluxArgs A) {
+  const int x = blockIdx.x * 32 + threadIdx.x, y = blockIdx.y * 8 + threadIdx.y, z = blockIdx.z;
+  const int nx = A.M.N[0], ny = A.M.N[1], nz = A.M.N[2];
+  if (x <= nx + 2 && y <= ny + 1 && z <= nz + 1) flux_face<0, TW>(A, x, y, z);
+  if (x <= nx + 1 && y <= ny + 2 && z <= nz + 1) flux_face<1, TW>(A, x, y, z);
+  if (x <= nx + 1 && y <= ny + 1 && z <= nz + 2) flux_face<2, TW>(A, x, y, z);
+}
+
+// ---------------------------------------------------------------------------
 // Two-way Poisson coefficients (G_CFDDEMCoupling::update_poisson_beta_two_way,
 // k_update_poisson_beta_two_way, Coupling/G_CFDDEMCoupling.cu:419-460):
 // f_b = eps_f f_inv_rho with eps_f the mean void fraction of the face's two
@@ -1472,6 +1521,54 @@ smac_status smac_update_properties(const smac_grid_desc* d, const smac_vof_param
   const dim3 grid((unsigned)((d->nx + 3 + PR_TX - 1) / PR_TX), (unsigned)((d->ny + 3 + PR_TY - 1) / PR_TY),
                   (unsigned)(d->nz + 3));
   k_props<<<grid, dim3(PR_TX, PR_TY), 0, (cudaStream_t)stream>>>(A);
+  return launch_status(fn);
+}
+
+smac_status smac_mass_flux_from_alpha_flux(const smac_grid_desc* d, const smac_boundary_table* bc,
+                                           const smac_mass_flux_fields* in, double rho0, double rho1, double dt,
+                                           const double* eps_half, double* mfx, double* mfy, double* mfz,
+                                           void* stream) {
+  static const char* fn = "smac_mass_flux_from_alpha_flux";
+  if (!d || !bc || !in || !mfx || !mfy || !mfz) {
+    smac::set_error_text("%s: null argument", fn);
+    return SMAC_BAD_ARG;
+  }
+  const void* need[] = {in->fxt, in->fyt, in->fzt, in->fxbcid, in->fybcid, in->fzbcid,
+                        in->vx, in->vy, in->vz, in->Fx, in->Fy, in->Fz};
+  for (const void* q : need)
+    if (!q) {
+      smac::set_error_text("%s: a required field is null", fn);
+      return SMAC_BAD_ARG;
+    }
+  if (bad_table(bc, fn)) return SMAC_BAD_ARG;
+  if (bad_desc(d, fn, 1)) return SMAC_BAD_SHAPE;
+  FluxArgs A;
+  std::memset(&A, 0, sizeof(A));
+  MomArgs& M = A.M;
+  M.N[0] = d->nx; M.N[1] = d->ny; M.N[2] = d->nz;
+  M.ft[0] = in->fxt; M.ft[1] = in->fyt; M.ft[2] = in->fzt;
+  M.id[0] = in->fxbcid; M.id[1] = in->fybcid; M.id[2] = in->fzbcid;
+  M.lam[0] = in->lamx; M.lam[1] = in->lamy; M.lam[2] = in->lamz;
+  M.v[0] = in->vx; M.v[1] = in->vy; M.v[2] = in->vz;
+  for (int k = 0; k < 4; ++k) {
+    const long long S0 = d->nx + 2 + (k == 0), S1 = d->ny + 2 + (k == 1);
+    M.st[k][0] = 1;
+    M.st[k][1] = S0;
+    M.st[k][2] = S0 * S1;
+  }
+  fill_table(&M.bc, bc);
+  A.Fa[0] = in->Fx; A.Fa[1] = in->Fy; A.Fa[2] = in->Fz;
+  A.epsh = eps_half;
+  A.mf[0] = mfx; A.mf[1] = mfy; A.mf[2] = mfz;
+  A.rho0 = rho0;
+  A.drho = rho1 - rho0;
+  const double inv_dt = 1. / dt;
+  A.hdt[0] = d->dx * inv_dt; A.hdt[1] = d->dy * inv_dt; A.hdt[2] = d->dz * inv_dt;
+  const dim3 grid((unsigned)((d->nx + 3 + 31) / 32), (unsigned)((d->ny + 3 + 7) / 8), (unsigned)(d->nz + 3));
+  if (eps_half)
+    k_mass_flux<true><<<grid, dim3(32, 8), 0, (cudaStream_t)stream>>>(A);
+  else
+    k_mass_flux<false><<<grid, dim3(32, 8), 0, (cudaStream_t)stream>>>(A);
   return launch_status(fn);
 }
 

@@ -95,6 +95,11 @@ class DeviceGrid:
     f_muz_: torch.Tensor | None = None
     mu_: torch.Tensor | None = None
     rho_old_: torch.Tensor | None = None
+    # read by the mass-flux update (it writes f_mf*_)
+    f_Fx_accum_: torch.Tensor | None = None
+    f_Fy_accum_: torch.Tensor | None = None
+    f_Fz_accum_: torch.Tensor | None = None
+    void_fraction_half_: torch.Tensor | None = None
     # written by the property update (besides rho_, mu_, f_b*_, f_inv_rho*_, f_mu*_)
     inv_rho_: torch.Tensor | None = None
     f_rhox_: torch.Tensor | None = None
@@ -388,6 +393,30 @@ class SMACStep:
             "eps_old": g.void_fraction_old_, "eps_new": g.void_fraction_, "inv_rhox": g.f_inv_rhox_,
             "inv_rhoy": g.f_inv_rhoy_, "inv_rhoz": g.f_inv_rhoz_})
 
+    def compute_mass_flux_from_alpha_flux(self, rho0: float, rho1: float, two_way: bool = False):
+        """G_SMACSolver::compute_mass_flux_from_alpha_flux (CFD/G_SMACSolver_VoF.cu:
+        1792-1795), or with two_way compute_mass_flux_from_alpha_flux_two_way
+        (:2685-2687, reading void_fraction_half_): f_mf*_ from f_v*_ and
+        f_F*_accum_ (smac_mass_flux_from_alpha_flux).  Missing f_mf*_ are
+        allocated."""
+        g = self.grid_
+        need = ("f_Fx_accum_", "f_Fy_accum_", "f_Fz_accum_", "f_xbcid_") + (("void_fraction_half_",) if two_way else ())
+        if self.bc_ is None or any(getattr(g, k) is None for k in need):
+            raise ValueError("compute_mass_flux_from_alpha_flux needs bc_ and the grid's " + ", ".join(need))
+        sh = shapes(g.N)
+        for ax in "xyz":
+            if getattr(g, f"f_mf{ax}_") is None:
+                setattr(g, f"f_mf{ax}_", torch.zeros(sh[ax], dtype=torch.float64, device=g.p_.device))
+        f = {}
+        for ax in "xyz":
+            f["f" + ax + "t"] = getattr(g, f"f_{ax}type_")
+            f["f" + ax + "bcid"] = getattr(g, f"f_{ax}bcid_")
+            f["lam" + ax] = getattr(g, f"f_ibm_area_solid_fraction_{ax}_")
+            f["v" + ax] = getattr(g, f"f_v{ax}_")
+            f["F" + ax] = getattr(g, f"f_F{ax}_accum_")
+        mass_flux_device(g.N, (g.dx_, g.dy_, g.dz_), self.bc_, f, rho0, rho1, self.dt_,
+                         (g.f_mfx_, g.f_mfy_, g.f_mfz_), eps_half=g.void_fraction_half_ if two_way else None)
+
     def update_poisson_beta_two_way(self):
         """G_CFDDEMCoupling::update_poisson_beta_two_way
         (Coupling/G_CFDDEMCoupling.cu:419-460): f_b*_ = eps_f f_inv_rho*_ from
@@ -619,6 +648,24 @@ def predict_vstar_device(N, h, bc: BoundaryConditions, fields: dict, dt, g, vs, 
         nat.check(nat.load().smac_predict_vstar_two_way(ctypes.byref(d), ctypes.byref(table), ctypes.byref(mf),
                                                         ctypes.byref(tw), dd(dt), dd(g[0]), dd(g[1]), dd(g[2]),
                                                         *map(_ptr, vs), ctypes.c_void_p(s)))
+    del keep
+
+
+def mass_flux_device(N, h, bc: BoundaryConditions, fields: dict, rho0, rho1, dt, mf, eps_half=None):
+    """smac_mass_flux_from_alpha_flux: mf = (mfx, mfy, mfz) <- rho0 q + (rho1 -
+    rho0) F h / dt on every face.  fields maps the smac_mass_flux_fields names
+    to CUDA tensors (lam* may be missing); eps_half selects the two-way form."""
+    d = nat.GridDesc(*N, *h)
+    s = torch.cuda.current_stream().cuda_stream
+    table, keep = bc.table()
+    f = nat.MassFluxFields()
+    for name, _ in nat.MassFluxFields._fields_:
+        t = fields.get(name)
+        setattr(f, name, None if t is None else _ptr(t).value)
+    dd = ctypes.c_double
+    nat.check(nat.load().smac_mass_flux_from_alpha_flux(ctypes.byref(d), ctypes.byref(table), ctypes.byref(f),
+                                                        dd(rho0), dd(rho1), dd(dt), _ptr(eps_half), *map(_ptr, mf),
+                                                        ctypes.c_void_p(s)))
     del keep
 
 

@@ -522,3 +522,33 @@ def beta_two_way_case(N, seed, h=(0.03125, 0.03125, 0.03125)):
     fir = tuple(rnd(401 + k, key, 1e-3, 1.0) for k, key in enumerate("xyz"))
     fb = tuple(rnd(404 + k, key, -1.0, 1.0) for k, key in enumerate("xyz"))
     return N, tuple(h), eps, fir, fb
+
+
+@dataclass
+class MassFluxCase:
+    """Inputs of the mass-flux update (compute_mass_flux_from_alpha_flux):
+    the face rule's fields and dt of a MomentumCase, the accumulated
+    volume-fraction flux F, rho0 / rho1, the mass flux before the call, and
+    (two-way) void_fraction_half_."""
+    mom: MomentumCase
+    F: tuple
+    rho0: float
+    rho1: float
+    mf: tuple
+    eps_half: np.ndarray | None = None
+
+
+def mass_flux_case(N, seed, sides=("x+", "z-"), solid_fraction=0.0, extras=True, two_way=False, rho=(1.0, 1000.0)):
+    """Seeded mass-flux inputs: momentum_case's faces and velocities, F
+    U[-0.5, 0.5) on every face, the previous mf U[-1, 1), void_fraction_half_
+    U[0.4, 1) for the two-way form."""
+    m = momentum_case(N, seed, sides=sides, solid_fraction=solid_fraction, extras=extras)
+    sh = shapes(m.N)
+
+    def rnd(tag, key, lo, hi):
+        n = int(np.prod(sh[key]))
+        return np.ascontiguousarray((lo + (hi - lo) * uniform01(substream(seed, tag), n)).reshape(sh[key]))
+
+    return MassFluxCase(mom=m, F=tuple(rnd(500 + k, key, -0.5, 0.5) for k, key in enumerate("xyz")),
+                        rho0=rho[0], rho1=rho[1], mf=tuple(rnd(510 + k, key, -1.0, 1.0) for k, key in enumerate("xyz")),
+                        eps_half=rnd(520, "cell", 0.4, 1.0) if two_way else None)

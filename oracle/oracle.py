@@ -436,3 +436,32 @@ def poisson_beta_two_way(N, eps, fir, fb):
     lib().orc_poisson_beta_two_way(*N, _p(e), (ctypes.c_void_p * 3)(*(a.ctypes.data for a in firs)),
                                    (ctypes.c_void_p * 3)(*(a.ctypes.data for a in out)))
     return tuple(out)
+
+
+def mass_flux(c):
+    """G_SMACSolver::compute_mass_flux_from_alpha_flux (CFD/G_SMACSolver_VoF.cu:
+    1708-1795), or its two-way form (:2472-2687) when c.eps_half is set, on a
+    workloads.MassFluxCase: returns (mfx, mfy, mfz), copies of c.mf after the call."""
+    keep = []
+
+    def arr3(arrs, dtype=np.float64):
+        if arrs is None:
+            return (ctypes.c_void_p * 3)(None, None, None)
+        out = []
+        for a in arrs:
+            a = np.ascontiguousarray(a, dtype)
+            keep.append(a)
+            out.append(a.ctypes.data)
+        return (ctypes.c_void_p * 3)(*out)
+
+    m = c.mom
+    mf = [np.array(a, dtype=np.float64, order="C", copy=True) for a in c.mf]
+    bv = [np.ascontiguousarray(a, np.float64) for a in m.bc_v]
+    bct = np.ascontiguousarray(m.bc_type, np.uint8)
+    eh = None if c.eps_half is None else np.ascontiguousarray(c.eps_half, np.float64)
+    d = ctypes.c_double
+    lib().orc_mass_flux(*m.N, d(m.h[0]), d(m.h[1]), d(m.h[2]), d(m.dt), d(c.rho0), d(c.rho1), _u8(bct),
+                        *(_p(a) for a in bv), arr3(m.ft, np.uint8), arr3(m.bcid, np.uint8), arr3(m.lam), arr3(m.v),
+                        arr3(c.F), None if eh is None else _p(eh),
+                        (ctypes.c_void_p * 3)(*(a.ctypes.data for a in mf)))
+    return tuple(mf)

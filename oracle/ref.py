@@ -401,3 +401,52 @@ def poisson_beta_two_way(N, h, eps, fir, fb):
     if rc != 0:
         raise RuntimeError(f"ref_poisson_beta_two_way returned {rc}")
     return (*out, io.ms)
+
+
+class RefFluxIO(ctypes.Structure):
+    _fields_ = [("Nx", ctypes.c_int), ("Ny", ctypes.c_int), ("Nz", ctypes.c_int)] + \
+        [(k, ctypes.c_double) for k in ("Lx", "Ly", "Lz", "dt", "rho0", "rho1")] + \
+        [("num_ids", ctypes.c_int), ("bc_type", _u8p), ("bc_vx", _dp), ("bc_vy", _dp), ("bc_vz", _dp)] + \
+        [(k, ctypes.c_void_p * 3) for k in ("ft", "bcid", "lam", "v", "F")] + \
+        [("eps_half", _dp), ("mf", ctypes.c_void_p * 3), ("ms", ctypes.c_double)]
+
+
+def mass_flux(c):
+    """Run the reference's compute_mass_flux_from_alpha_flux (two-way form
+    when c.eps_half is set) on a mydemcfd_b200.workloads.MassFluxCase:
+    returns (mfx, mfy, mfz, ms)."""
+    L = lib()
+    if not hasattr(L, "_flux_set"):
+        L.ref_mass_flux.restype = ctypes.c_int
+        L.ref_mass_flux.argtypes = [ctypes.POINTER(RefFluxIO)]
+        L._flux_set = True
+    keep = []
+
+    def arr(a, dtype=np.float64):
+        a = np.ascontiguousarray(a, dtype)
+        keep.append(a)
+        return a
+
+    def three(arrs, dtype=np.float64, like=None):
+        if arrs is None:
+            arrs = tuple(np.zeros(x.shape) for x in like)
+        return (ctypes.c_void_p * 3)(*(arr(a, dtype).ctypes.data for a in arrs))
+
+    m = c.mom
+    io = RefFluxIO()
+    io.Nx, io.Ny, io.Nz = m.N
+    io.Lx, io.Ly, io.Lz = (n * hh for n, hh in zip(m.N, m.h))
+    io.dt, io.rho0, io.rho1 = m.dt, c.rho0, c.rho1
+    io.num_ids = len(m.bc_type)
+    io.bc_type = _p(arr(m.bc_type, np.uint8), ctypes.c_uint8)
+    io.bc_vx, io.bc_vy, io.bc_vz = (_p(arr(a)) for a in m.bc_v)
+    io.ft, io.bcid = three(m.ft, np.uint8), three(m.bcid, np.uint8)
+    io.lam, io.v, io.F = three(m.lam, like=m.v), three(m.v), three(c.F)
+    if c.eps_half is not None:
+        io.eps_half = _p(arr(c.eps_half))
+    out = [np.array(a, dtype=np.float64, order="C", copy=True) for a in c.mf]
+    io.mf = (ctypes.c_void_p * 3)(*(a.ctypes.data for a in out))
+    rc = L.ref_mass_flux(ctypes.byref(io))
+    if rc != 0:
+        raise RuntimeError(f"ref_mass_flux returned {rc}")
+    return (*out, io.ms)

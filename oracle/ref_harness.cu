@@ -565,3 +565,76 @@ extern "C" int ref_poisson_beta_two_way(ref_beta_io* io) {
   solv.solver_free();
   return e == cudaSuccess ? 0 : -2;
 }
+
+struct ref_flux_io {
+  int Nx, Ny, Nz;
+  double Lx, Ly, Lz, dt, rho0, rho1;
+  int num_ids;
+  const uint8_t* bc_type;
+  const double *bc_vx, *bc_vy, *bc_vz;
+  const uint8_t *ft[3], *bcid[3];
+  const double *lam[3], *v[3], *F[3];
+  const double* eps_half;  // set: the two-way form; NULL: the one-way form
+  double* mf[3];           // in: f_mf*_ before the call; out: after it
+  double ms;               // out: device time
+};
+
+// G_SMACSolver::compute_mass_flux_from_alpha_flux (CFD/G_SMACSolver_VoF.cu:
+// 1792-1795), or with io->eps_half set compute_mass_flux_from_alpha_flux_two_way
+// (:2685-2687), on host arrays.  Returns 0 on success, -2 on a CUDA error.
+extern "C" int ref_mass_flux(ref_flux_io* io) {
+  const int Nx = io->Nx, Ny = io->Ny, Nz = io->Nz;
+  SMACSolver solv;
+  solv.set_calc_properties(0., 0., 0., io->Lx, io->Ly, io->Lz, Nx, Ny, Nz);
+  solv.grid_.bc_.num_boundary_id_ = io->num_ids;
+  solv.solver_malloc();
+  solv.dt_ = io->dt;
+  solv.inv_dt_ = 1. / io->dt;
+  solv.rho0_ = io->rho0;
+  solv.rho1_ = io->rho1;
+  StaggeredGrid& hg = solv.grid_;
+  put(hg.f_xtype_, io->ft[0]); put(hg.f_ytype_, io->ft[1]); put(hg.f_ztype_, io->ft[2]);
+  put(hg.f_xbcid_, io->bcid[0]); put(hg.f_ybcid_, io->bcid[1]); put(hg.f_zbcid_, io->bcid[2]);
+  put(hg.f_ibm_area_solid_fraction_x_, io->lam[0]); put(hg.f_ibm_area_solid_fraction_y_, io->lam[1]);
+  put(hg.f_ibm_area_solid_fraction_z_, io->lam[2]);
+  put(hg.f_vx_, io->v[0]); put(hg.f_vy_, io->v[1]); put(hg.f_vz_, io->v[2]);
+  put(hg.f_Fx_accum_, io->F[0]); put(hg.f_Fy_accum_, io->F[1]); put(hg.f_Fz_accum_, io->F[2]);
+  put(hg.void_fraction_half_, io->eps_half);
+  put(hg.f_mfx_, (const double*)io->mf[0]); put(hg.f_mfy_, (const double*)io->mf[1]);
+  put(hg.f_mfz_, (const double*)io->mf[2]);
+  std::memcpy(hg.bc_.bcType_.data_, io->bc_type, (size_t)io->num_ids);
+  std::memcpy(hg.bc_.vx_.data_, io->bc_vx, sizeof(double) * (size_t)io->num_ids);
+  std::memcpy(hg.bc_.vy_.data_, io->bc_vy, sizeof(double) * (size_t)io->num_ids);
+  std::memcpy(hg.bc_.vz_.data_, io->bc_vz, sizeof(double) * (size_t)io->num_ids);
+  G_SMACSolver g;
+  g.set_calc_properties(0., 0., 0., io->Lx, io->Ly, io->Lz, Nx, Ny, Nz);
+  g.grid_.bc_.num_boundary_id_ = io->num_ids;
+  g.solver_malloc();
+  g.cpuTogpu(solv.grid_);
+  g.set_block_grid(Nx, Ny, Nz);
+  g.dt_ = io->dt;
+  g.inv_dt_ = 1. / io->dt;
+  cudaDeviceSynchronize();
+  cudaEvent_t ev[2];
+  for (auto& x : ev) cudaEventCreate(&x);
+  cudaEventRecord(ev[0], 0);
+  if (io->eps_half)
+    g.compute_mass_flux_from_alpha_flux_two_way(solv);
+  else
+    g.compute_mass_flux_from_alpha_flux(solv);
+  cudaEventRecord(ev[1], 0);
+  cudaDeviceSynchronize();
+  float t = 0.f;
+  cudaEventElapsedTime(&t, ev[0], ev[1]);
+  io->ms = t;
+  for (auto& x : ev) cudaEventDestroy(x);
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) {
+    g.gpuTocpu(solv.grid_);
+    get(hg.f_mfx_, io->mf[0]); get(hg.f_mfy_, io->mf[1]); get(hg.f_mfz_, io->mf[2]);
+    e = cudaGetLastError();
+  }
+  g.solver_free();
+  solv.solver_free();
+  return e == cudaSuccess ? 0 : -2;
+}

@@ -1136,6 +1136,49 @@ extern "C" {
 // convection - grad p) + g), scaled by 1 - IBM solid fraction.  Families in
 // the order x, y, z (independent: each reads only time-n fields).  Arrays
 // per family in the argument triples; lam/imp/sf may be NULL (0).
+// The advecting mass flux, G_SMACSolver::compute_mass_flux_from_alpha_flux
+// (CFD/G_SMACSolver_VoF.cu:1708-1795): on every face of family a,
+// mf = rho0 q + (rho1 - rho0) F_accum (h_a / dt), q = face_val.  With
+// eps_half given, the two-way form (:2472-2687): q = eps_f q on faces
+// 1..N+1 along a (eps_f the mean of eps_half of the face's two cells; at
+// faces 1 and N+1 the one interior cell's), mf = 0 at faces 0 and N+2.
+void orc_mass_flux(int Nx, int Ny, int Nz, double dx, double dy, double dz, double dt, double rho0, double rho1,
+                   const uint8_t* bct, const double* bvx, const double* bvy, const double* bvz,
+                   const uint8_t* const* ft, const uint8_t* const* id, const double* const* lam,
+                   const double* const* v, const double* const* Fa, const double* eps_half, double* const* mf) {
+  MomFields F{};
+  F.N[0] = Nx; F.N[1] = Ny; F.N[2] = Nz;
+  F.bct = bct;
+  F.bv[0] = bvx; F.bv[1] = bvy; F.bv[2] = bvz;
+  for (int a = 0; a < 3; ++a) {
+    F.ft[a] = ft[a]; F.id[a] = id[a]; F.lam[a] = lam[a]; F.v[a] = v[a];
+  }
+  const double inv_dt = 1. / dt, h[3] = {dx, dy, dz}, drho = rho1 - rho0;
+  for (int a = 0; a < 3; ++a) {
+    const double hdt = h[a] * inv_dt;
+    const int ex = Nx + 1 + (a == 0), ey = Ny + 1 + (a == 1), ez = Nz + 1 + (a == 2);
+    for (int z = 0; z <= ez; ++z)
+      for (int y = 0; y <= ey; ++y)
+        for (int x = 0; x <= ex; ++x) {
+          const Idx3 q{{x, y, z}};
+          const size_t f = face_off(F, a, q);
+          double u = face_val(F, a, q);
+          if (eps_half) {
+            const int along = q.i[a], n = F.N[a];
+            if (along < 1 || along > n + 1) {
+              mf[a][f] = 0.0;
+              continue;
+            }
+            const double e = along == 1       ? eps_half[cell_off(F, q)]
+                             : along == n + 1 ? eps_half[cell_off(F, shifted(q, a, -1))]
+                                              : 0.5 * (eps_half[cell_off(F, shifted(q, a, -1))] + eps_half[cell_off(F, q)]);
+            u = e * u;
+          }
+          mf[a][f] = rho0 * u + drho * (Fa[a][f] * hdt);
+        }
+  }
+}
+
 // With eps_old and eps_new given (not NULL): the two-way form,
 // G_SMACSolver::get_vof_vstar_rhouu_consistent_two_way (:2196-2203), with fb
 // the faces' f_inv_rho.

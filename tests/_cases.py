@@ -46,7 +46,7 @@ def golden_names():
     if not os.path.isdir(GOLDEN):
         return []
     return sorted(f[:-4] for f in os.listdir(GOLDEN)
-                  if f.endswith(".npz") and not f.startswith(("post", "vstar", "surface", "mom", "props", "beta")))
+                  if f.endswith(".npz") and not f.startswith(("post", "vstar", "surface", "mom", "props", "beta", "flux")))
 
 
 def surface_golden_names():
@@ -142,3 +142,18 @@ def beta_case_from_spec(spec):
     spec = dict(spec)
     spec["N"] = tuple(spec["N"])
     return W.beta_two_way_case(**spec)
+
+
+def flux_golden_names():
+    """Fixtures of the reference's compute_mass_flux_from_alpha_flux (one-way and two-way)."""
+    if not os.path.isdir(GOLDEN):
+        return []
+    return sorted(f[:-4] for f in os.listdir(GOLDEN) if f.endswith(".npz") and f.startswith("flux"))
+
+
+def flux_case_from_spec(spec):
+    spec = dict(spec)
+    for k in ("N", "sides"):
+        if k in spec:
+            spec[k] = tuple(spec[k])
+    return W.mass_flux_case(**spec)

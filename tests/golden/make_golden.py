@@ -74,6 +74,14 @@ MOMENTUM_CASES = [
     ("mom2w16_s5_solid", dict(N=(16, 16, 16), seed=5, sides=("x-", "y+"), solid_fraction=0.3, two_way=True)),
 ]
 
+# The mass-flux update (compute_mass_flux_from_alpha_flux, one-way and two-way):
+# workloads.mass_flux_case kwargs.
+FLUX_CASES = [
+    ("flux12x10x8_s1", dict(N=(12, 10, 8), seed=1, sides=("x+", "z-"))),
+    ("flux9x7x11_s2_solid", dict(N=(9, 7, 11), seed=2, sides=("y-",), solid_fraction=0.3)),
+    ("flux2w12x10x8_s3", dict(N=(12, 10, 8), seed=3, sides=("x-", "y+"), two_way=True)),
+]
+
 # The two-way Poisson coefficients (update_poisson_beta_two_way): workloads.beta_two_way_case kwargs.
 BETA_CASES = [
     ("beta2w12x10x8_s1", dict(N=(12, 10, 8), seed=1)),
@@ -146,6 +154,12 @@ def main():
         N, h, (r0, r1, m0, m1), alpha, ct, ft, init = W.property_case(**spec)
         out, _ = REF.update_properties(N, h, r0, r1, m0, m1, alpha, ct, ft, init)
         np.savez_compressed(os.path.join(args.out, name + ".npz"), meta=np.array(json.dumps(spec)), **out)
+        post_index[name] = spec
+        print(name, spec, flush=True)
+    for name, spec in FLUX_CASES:
+        mfx, mfy, mfz, _ = REF.mass_flux(W.mass_flux_case(**spec))
+        np.savez_compressed(os.path.join(args.out, name + ".npz"), meta=np.array(json.dumps(spec)), mfx=mfx, mfy=mfy,
+                            mfz=mfz)
         post_index[name] = spec
         print(name, spec, flush=True)
     for name, spec in BETA_CASES:

@@ -17,13 +17,13 @@ import torch
 from mydemcfd_b200 import _native as nat
 from mydemcfd_b200 import workloads as W
 from mydemcfd_b200.solver import (BoundaryConditions, DeviceGrid, SMACStep, face_gradp_device, predict_vstar_device,
-                                  poisson_beta_two_way_device, surface_tension_device,
+                                  mass_flux_device, poisson_beta_two_way_device, surface_tension_device,
                                   update_pressure_ghost_device, update_properties_device,
                                   update_velocity_ghost_device, update_vstar_boundary_device)
 from oracle import oracle as O
 from oracle import ref as REF
 
-from _cases import (beta_case_from_spec, beta_golden_names, load_golden, momentum_case_from_spec, momentum_golden_names, post_case_from_spec,
+from _cases import (beta_case_from_spec, beta_golden_names, flux_case_from_spec, flux_golden_names, load_golden, momentum_case_from_spec, momentum_golden_names, post_case_from_spec,
                     post_golden_names, property_case_from_spec, property_golden_names, surface_case_from_spec,
                     surface_golden_names, vstar_golden_names)
 
@@ -609,3 +609,91 @@ def test_poisson_beta_two_way_against_reference_library_and_time_256():
     ms = _device_ms(lambda: poisson_beta_two_way_device(N, h, e, fi, out))
     print(f"update_poisson_beta_two_way 256^3: {ms * 1e3:.1f} us (reference {ref_ms * 1e3:.1f} us)")
     assert ms < ref_ms
+
+
+# ---------------------------------------------------------------------------
+# the mass-flux update (compute_mass_flux_from_alpha_flux)
+
+def _flux_fields(c):
+    m = c.mom
+    f = {}
+    for k, ax in enumerate("xyz"):
+        f["f" + ax + "t"] = _cuda(m.ft[k])
+        f["f" + ax + "bcid"] = _cuda(m.bcid[k])
+        f["v" + ax] = _cuda(m.v[k])
+        f["F" + ax] = _cuda(c.F[k])
+        if m.lam is not None:
+            f["lam" + ax] = _cuda(m.lam[k])
+    return f
+
+
+def run_flux(c):
+    out = [_cuda(a) for a in c.mf]
+    m = c.mom
+    mass_flux_device(m.N, m.h, BoundaryConditions(m.bc_type, *m.bc_v), _flux_fields(c), c.rho0, c.rho1, m.dt, out,
+                     eps_half=None if c.eps_half is None else _cuda(c.eps_half))
+    torch.cuda.synchronize()
+    return tuple(a.cpu().numpy() for a in out)
+
+
+@pytest.mark.parametrize("spec", [
+    dict(N=(12, 10, 8), seed=1, sides=("x+", "z-")),
+    dict(N=(17, 9, 13), seed=2, sides=("y-",), solid_fraction=0.3),
+    dict(N=(9, 7, 11), seed=3, sides=("x-",), extras=False),
+    dict(N=(12, 10, 8), seed=4, sides=("x-", "y+"), two_way=True),
+    dict(N=(1, 6, 4), seed=5, sides=(), two_way=True),
+])
+def test_mass_flux_bit_exact_against_oracle(spec):
+    c = W.mass_flux_case(**spec)
+    for k, a, b in zip(("mfx", "mfy", "mfz"), run_flux(c), O.mass_flux(c)):
+        assert np.array_equal(a, b), k
+
+
+@pytest.mark.parametrize("name", flux_golden_names())
+def test_mass_flux_bit_exact_against_reference_golden(name):
+    meta, arr = load_golden(name)
+    for k, a in zip(("mfx", "mfy", "mfz"), run_flux(flux_case_from_spec(meta))):
+        assert np.array_equal(a, arr[k]), k
+
+
+@pytest.mark.skipif(not REF.available(), reason="reference build oracle/_ref not present")
+@pytest.mark.parametrize("two_way", [False, True])
+def test_mass_flux_against_reference_library_and_time_256(two_way):
+    c = W.mass_flux_case((64, 48, 40), seed=6, sides=("x+", "z-"), solid_fraction=0.05, two_way=two_way)
+    *ref, _ = REF.mass_flux(c)
+    for k, a, b in zip(("mfx", "mfy", "mfz"), run_flux(c), ref):
+        assert np.array_equal(a, b), k
+    c = W.mass_flux_case((256, 256, 256), seed=7, sides=("x+",), solid_fraction=0.02, two_way=two_way)
+    REF.mass_flux(c)  # loads the reference's kernel
+    *_, ref_ms = REF.mass_flux(c)
+    m = c.mom
+    fields, out = _flux_fields(c), [_cuda(a) for a in c.mf]
+    eh = None if c.eps_half is None else _cuda(c.eps_half)
+    bc = BoundaryConditions(m.bc_type, *m.bc_v)
+    ms = _device_ms(lambda: mass_flux_device(m.N, m.h, bc, fields, c.rho0, c.rho1, m.dt, out, eps_half=eh))
+    name = "compute_mass_flux_from_alpha_flux" + ("_two_way" if two_way else "")
+    print(f"{name} 256^3: {ms * 1e3:.1f} us (reference {ref_ms * 1e3:.1f} us)")
+    assert ms < ref_ms
+
+
+def test_smac_step_mass_flux_matches_oracle():
+    """SMACStep.compute_mass_flux_from_alpha_flux, one-way and two-way, on a DeviceGrid."""
+    c = W.mass_flux_case((14, 12, 10), seed=9, sides=("x+",), solid_fraction=0.2, two_way=True)
+    m = c.mom
+    sh = W.shapes(m.N)
+    zc = lambda: torch.zeros(sh["cell"], dtype=torch.float64, device="cuda")  # noqa: E731
+    g = DeviceGrid(*m.N, *m.h, *(_cuda(a) for a in m.vs), *(_cuda(a) for a in m.fb), *(_cuda(a) for a in m.fb),
+                   _cuda(m.ct), *(_cuda(a) for a in m.ft), _cuda(m.p), zc(), zc(), *(_cuda(a) for a in m.v))
+    g.f_xbcid_, g.f_ybcid_, g.f_zbcid_ = (_cuda(a) for a in m.bcid)
+    g.f_ibm_area_solid_fraction_x_, g.f_ibm_area_solid_fraction_y_, g.f_ibm_area_solid_fraction_z_ = (
+        _cuda(a) for a in m.lam)
+    g.f_Fx_accum_, g.f_Fy_accum_, g.f_Fz_accum_ = (_cuda(a) for a in c.F)
+    g.void_fraction_half_ = _cuda(c.eps_half)
+    g.f_mfx_, g.f_mfy_, g.f_mfz_ = (_cuda(a) for a in c.mf)
+    step = SMACStep(g, m.dt, g=m.g, bc=BoundaryConditions(m.bc_type, *m.bc_v))
+    import dataclasses
+    for two_way, case in ((True, c), (False, dataclasses.replace(c, eps_half=None))):
+        step.compute_mass_flux_from_alpha_flux(c.rho0, c.rho1, two_way=two_way)
+        torch.cuda.synchronize()
+        for a, b in zip((g.f_mfx_, g.f_mfy_, g.f_mfz_), O.mass_flux(case)):
+            assert np.array_equal(a.cpu().numpy(), b)

@@ -9,7 +9,8 @@ from mydemcfd_b200 import workloads as W
 from _cases import (build_case, fluid_demeaned, golden_names, load_golden, post_case_from_spec, post_golden_names,
                     ref_grid, rel_err, surface_case_from_spec, surface_golden_names, vstar_golden_names,
                     momentum_case_from_spec, momentum_golden_names, property_case_from_spec,
-                    property_golden_names, beta_case_from_spec, beta_golden_names)
+                    property_golden_names, beta_case_from_spec, beta_golden_names, flux_case_from_spec,
+                    flux_golden_names)
 
 
 def test_box_types_match_reference_setup(oracle_lib):
@@ -649,4 +650,37 @@ def test_poisson_beta_two_way_oracle_matches_reference_golden(oracle_lib, name):
     meta, arr = load_golden(name)
     N, h, eps, fir, fb = beta_case_from_spec(meta)
     for k, a in zip(("fbx", "fby", "fbz"), oracle_lib.poisson_beta_two_way(N, eps, fir, fb)):
+        assert np.array_equal(a, arr[k]), k
+
+
+# ---------------------------------------------------------------------------
+# the mass-flux update (compute_mass_flux_from_alpha_flux)
+
+def test_mass_flux_known_answers(oracle_lib):
+    """rho0 = rho1 = 1: mf is the face velocity (F drops out), equal to u on
+    F_INTERIOR faces; the two-way form with eps_half = 1 equals the one-way
+    form on faces 1..N+1 along each axis and is 0 on faces 0 and N+2."""
+    import dataclasses
+    c = W.mass_flux_case((7, 6, 5), seed=4, sides=("x+", "y-"), solid_fraction=0.2, rho=(1.0, 1.0))
+    mf = oracle_lib.mass_flux(c)
+    for a in range(3):
+        inner = c.mom.ft[a] == W.F_INTERIOR
+        assert np.array_equal(mf[a][inner], c.mom.v[a][inner])
+    c = W.mass_flux_case((7, 6, 5), seed=4, sides=("x+", "y-"), solid_fraction=0.2)
+    one = oracle_lib.mass_flux(c)
+    two = oracle_lib.mass_flux(dataclasses.replace(c, eps_half=np.ones(W.shapes(c.mom.N)["cell"])))
+    for a in range(3):
+        sl = [slice(None)] * 3
+        sl[2 - a] = slice(1, c.mom.N[a] + 2)
+        assert np.array_equal(two[a][tuple(sl)], one[a][tuple(sl)])
+        for edge in (0, c.mom.N[a] + 2):
+            sl[2 - a] = edge
+            assert np.all(two[a][tuple(sl)] == 0.0)
+
+
+@pytest.mark.skipif(not flux_golden_names(), reason="no mass-flux golden vectors")
+@pytest.mark.parametrize("name", flux_golden_names())
+def test_mass_flux_oracle_matches_reference_golden(oracle_lib, name):
+    meta, arr = load_golden(name)
+    for k, a in zip(("mfx", "mfy", "mfz"), oracle_lib.mass_flux(flux_case_from_spec(meta))):
         assert np.array_equal(a, arr[k]), k
