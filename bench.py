@@ -50,7 +50,8 @@ def parse():
                          "self-contained command for ncu captures")
     ap.add_argument("--around", default=None,
                     choices=["predict_vstar", "vstar_boundary", "pressure_ghost", "velocity_ghost", "face_gradp",
-                             "update_properties"],
+                             "update_properties", "predict_vstar_two_way", "mass_flux", "mass_flux_two_way",
+                             "poisson_beta_two_way"],
                     help="set up the workload and launch one of the calls around the projection --reps times "
                          "(for ncu captures)")
     ap.add_argument("--reps", type=int, default=3)
@@ -400,15 +401,19 @@ def around_calls(case, g, p, v, dev):
     """The calls either side of the projection on the bench grid, as
     closures, and the algorithmic bytes of each: before it the momentum
     predictor and update_vstar_boundary, after it update_boundary_ghost +
-    make_face_gradp, and the VoF property update.  Inputs: pressure p and
-    velocity v (device tensors), no-slip walls with an outlet on x+; the
-    property update takes alpha = (p + 1) / 2, rho 1 / 1000, mu 1e-3 / 1e-1."""
+    make_face_gradp, the VoF property update, the mass-flux update and the
+    two-way-coupled calls.  Inputs: pressure p and velocity v (device
+    tensors), no-slip walls with an outlet on x+; the property update takes
+    alpha = (p + 1) / 2, rho 1 / 1000, mu 1e-3 / 1e-1; the two-way calls take
+    the void fractions eps = 0.7 + 0.2 alpha and f_inv_rho = f_b; the mass
+    flux takes F_accum = 0.01 v."""
     import torch
 
     from mydemcfd_b200 import workloads as W
     from mydemcfd_b200.solver import (BoundaryConditions, face_gradp_device, predict_vstar_device,
-                                      update_pressure_ghost_device, update_properties_device,
-                                      update_velocity_ghost_device, update_vstar_boundary_device)
+                                      mass_flux_device, poisson_beta_two_way_device, update_pressure_ghost_device,
+                                      update_properties_device, update_velocity_ghost_device,
+                                      update_vstar_boundary_device)
     N, h = case.N, case.h
     sh = W.shapes(N)
     bcid = [torch.zeros(sh[k], dtype=torch.uint8, device=dev) for k in "xyz"]
@@ -436,6 +441,17 @@ def around_calls(case, g, p, v, dev):
         for k in ("fb", "fir", "rho", "mu"):
             props[k + ax] = torch.zeros(sh[ax], dtype=torch.float64, device=dev)
     ft = (g.f_xtype_, g.f_ytype_, g.f_ztype_)
+    eps = 0.7 + 0.2 * alpha
+    two_way = {"eps_old": eps, "eps_new": eps, "inv_rhox": fb[0], "inv_rhoy": fb[1], "inv_rhoz": fb[2]}
+    vs_pred2 = [t.clone() for t in vs]
+    flux_in = {}
+    for k, ax in enumerate("xyz"):
+        flux_in["f" + ax + "t"] = ft[k]
+        flux_in["f" + ax + "bcid"] = bcid[k]
+        flux_in["v" + ax] = v[k]
+        flux_in["F" + ax] = 0.01 * v[k]
+    mf_out = [torch.zeros_like(t) for t in v]
+    fb_out = [torch.zeros_like(t) for t in fb]
     calls = {
         "predict_vstar": lambda: predict_vstar_device(N, h, bc, mom, case.dt, (0.0, 0.0, -9.8), vs_pred),
         "vstar_boundary": lambda: update_vstar_boundary_device(N, h, bc, (g.f_xtype_, g.f_ytype_, g.f_ztype_), bcid,
@@ -445,6 +461,11 @@ def around_calls(case, g, p, v, dev):
         "face_gradp": lambda: face_gradp_device(N, h, p, gp),
         "update_properties": lambda: update_properties_device(N, h, 1.0, 1000.0, 1e-3, 1e-1, alpha, g.celltype_, ft,
                                                               props),
+        "predict_vstar_two_way": lambda: predict_vstar_device(N, h, bc, mom, case.dt, (0.0, 0.0, -9.8), vs_pred2,
+                                                              two_way=two_way),
+        "mass_flux": lambda: mass_flux_device(N, h, bc, flux_in, 1.0, 1000.0, case.dt, mf_out),
+        "mass_flux_two_way": lambda: mass_flux_device(N, h, bc, flux_in, 1.0, 1000.0, case.dt, mf_out, eps_half=eps),
+        "poisson_beta_two_way": lambda: poisson_beta_two_way_device(N, h, eps, fb, fb_out),
     }
     nx, ny, nz = N
     ncell = (nx + 2) * (ny + 2) * (nz + 2)
@@ -469,6 +490,13 @@ def around_calls(case, g, p, v, dev):
         # per cell its type and alpha read, rho, 1/rho and mu written; per face
         # its type read, 1/rho (f_b and f_inv_rho), rho and mu written
         "update_properties": ncell * (1 + 8 + 3 * 8) + nface * (1 + 4 * 8),
+        # as predict_vstar plus eps_old and eps_new per cell
+        "predict_vstar_two_way": ncell * (3 * (4 * 8 + 1) + 3 * 8 + 3 * 8 + 2 * 8),
+        # per face its type, u and F read, mf written (the ids of the few wall faces not counted)
+        "mass_flux": nface * (1 + 8 + 8 + 8),
+        "mass_flux_two_way": nface * (1 + 8 + 8 + 8) + ncell * 8,
+        # eps per cell; per face of the (N+1)^3 box f_inv_rho read and f_b written
+        "poisson_beta_two_way": ncell * 8 + 3 * (nx + 1) * (ny + 1) * (nz + 1) * 16,
     }
     return calls, alg
 
