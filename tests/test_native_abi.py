@@ -88,3 +88,64 @@ def test_post_pass_arguments_are_checked_before_any_device_work(lib):
     # outlet marks without p_delta
     bad = (fake,) * 3 + (fake,) * 3 + (None,) * 3 + (fake,) * 6 + (None, 1.0) + (fake,) * 3 + (None,)
     assert lib.smac_update_velocity_ghost(ctypes.byref(d), ctypes.byref(one), *bad) == nat.BAD_ARG
+
+
+def test_step_call_arguments_are_checked_before_any_device_work(lib):
+    """The property update, both predictors, the mass flux and the two-way
+    coefficients refuse null and mis-shaped arguments before any CUDA call
+    (so this runs without a GPU)."""
+    import numpy as np
+    fake = ctypes.c_void_p(256)  # never dereferenced
+    d = nat.GridDesc(8, 8, 8, 0.125, 0.125, 0.125)
+    flat = nat.GridDesc(8, 0, 8, 0.125, 0.125, 0.125)
+    thin = nat.GridDesc(8, 1, 8, 0.125, 0.125, 0.125)
+    neg = nat.GridDesc(8, 8, 8, 0.125, -0.125, 0.125)
+    vp = nat.VofParams(1.0, 1000.0, 1e-3, 1e-1)
+    out = nat.PropertyFields(*(256,) * 15)
+    assert lib.smac_update_properties(ctypes.byref(d), ctypes.byref(vp), None, fake, fake, fake, fake,
+                                      ctypes.byref(out), None) == nat.BAD_ARG
+    assert lib.smac_update_properties(ctypes.byref(flat), ctypes.byref(vp), fake, fake, fake, fake, fake,
+                                      ctypes.byref(out), None) == nat.BAD_SHAPE
+    no_mu = nat.PropertyFields(*(256,) * 12, None, 256, 256)   # f_mux missing
+    assert lib.smac_update_properties(ctypes.byref(d), ctypes.byref(vp), fake, fake, fake, fake, fake,
+                                      ctypes.byref(no_mu), None) == nat.BAD_ARG
+    optional = nat.PropertyFields(256, None, 256, 256, 256, 256, None, None, None, None, None, None, 256, 256, 256)
+    assert lib.smac_update_properties(ctypes.byref(neg), ctypes.byref(vp), fake, fake, fake, fake, fake,
+                                      ctypes.byref(optional), None) == nat.BAD_SHAPE
+
+    types = np.zeros(1, np.uint8)
+    vel = np.zeros(1)
+    one = nat.BoundaryTable(1, types.ctypes.data, vel.ctypes.data, vel.ctypes.data, vel.ctypes.data)
+    empty = nat.BoundaryTable(0, types.ctypes.data, vel.ctypes.data, vel.ctypes.data, vel.ctypes.data)
+    mf = nat.MomentumFields(*(256,) * 30)
+    tw = nat.TwoWayFields(*(256,) * 5)
+    vs = (fake,) * 3
+    assert lib.smac_predict_vstar(ctypes.byref(thin), ctypes.byref(one), ctypes.byref(mf), 0.01, 0.0, 0.0, -9.8,
+                                  *vs, None) == nat.BAD_SHAPE
+    assert lib.smac_predict_vstar(ctypes.byref(d), ctypes.byref(empty), ctypes.byref(mf), 0.01, 0.0, 0.0, -9.8,
+                                  *vs, None) == nat.BAD_ARG
+    assert lib.smac_predict_vstar_two_way(ctypes.byref(d), ctypes.byref(one), ctypes.byref(mf), None, 0.01, 0.0,
+                                          0.0, -9.8, *vs, None) == nat.BAD_ARG
+    no_eps = nat.TwoWayFields(256, None, 256, 256, 256)
+    assert lib.smac_predict_vstar_two_way(ctypes.byref(d), ctypes.byref(one), ctypes.byref(mf), ctypes.byref(no_eps),
+                                          0.01, 0.0, 0.0, -9.8, *vs, None) == nat.BAD_ARG
+    # the two-way form reads f_inv_rho from tw, so mf's f_b may be null there, not in the one-way form
+    mf_no_fb = nat.MomentumFields(*(256,) * 21, None, None, None, *(256,) * 6)
+    assert lib.smac_predict_vstar(ctypes.byref(d), ctypes.byref(one), ctypes.byref(mf_no_fb), 0.01, 0.0, 0.0, -9.8,
+                                  *vs, None) == nat.BAD_ARG
+    assert lib.smac_predict_vstar_two_way(ctypes.byref(thin), ctypes.byref(one), ctypes.byref(mf_no_fb),
+                                          ctypes.byref(tw), 0.01, 0.0, 0.0, -9.8, *vs, None) == nat.BAD_SHAPE
+
+    ff = nat.MassFluxFields(*(256,) * 15)
+    ff_no_F = nat.MassFluxFields(*(256,) * 12, None, 256, 256)
+    mfo = (fake,) * 3
+    assert lib.smac_mass_flux_from_alpha_flux(ctypes.byref(d), ctypes.byref(one), ctypes.byref(ff_no_F), 1.0, 1000.0,
+                                              0.01, None, *mfo, None) == nat.BAD_ARG
+    assert lib.smac_mass_flux_from_alpha_flux(ctypes.byref(flat), ctypes.byref(one), ctypes.byref(ff), 1.0, 1000.0,
+                                              0.01, None, *mfo, None) == nat.BAD_SHAPE
+    assert lib.smac_mass_flux_from_alpha_flux(ctypes.byref(d), ctypes.byref(empty), ctypes.byref(ff), 1.0, 1000.0,
+                                              0.01, fake, *mfo, None) == nat.BAD_ARG
+
+    assert lib.smac_poisson_beta_two_way(ctypes.byref(d), fake, fake, None, fake, fake, fake, fake, None) == nat.BAD_ARG
+    assert lib.smac_poisson_beta_two_way(ctypes.byref(flat), fake, fake, fake, fake, fake, fake, fake,
+                                         None) == nat.BAD_SHAPE
