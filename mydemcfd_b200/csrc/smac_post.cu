@@ -937,7 +937,10 @@ __device__ __forceinline__ double m_vstar(const MomArgs& A, const long long* b) 
 // on chains of dependent loads (a face type, then the value it selects), so
 // resident warps matter more than registers: 5 blocks per SM (48 registers,
 // a few spills to L1) measured 3.32 ms at 256^3, against 3.60 ms with 4
-// blocks, 4.27 ms with 3 and 3.43 ms with 6.
+// blocks, 4.27 ms with 3 and 3.43 ms with 6.  Family-major block order (all
+// planes of one family, then the next, so that resident warps share one
+// family's code) took 3.64 ms: the interleaved families' shared reads
+// through L2 are worth more than the instruction-cache locality.
 template <bool TW>
 __global__ void __launch_bounds__(256, 5) k_predict_vstar(MomArgs A) {
   const int fam = blockIdx.z % 3;
