@@ -309,7 +309,8 @@ typedef struct {
  * times (1 - IBM solid fraction); tau the Newtonian stress with the cell and
  * face viscosities, convection MUSCL with the minmod limiter, neighbours past
  * a wall mirrored about it (slip and outlet walls copied).  Other faces of
- * (vxs, vys, vzs) are not written.  Every grid extent must be >= 2. */
+ * (vxs, vys, vzs) are not written.  Every grid extent must be >= 2, and
+ * every face array below 2^31 entries (SMAC_BAD_SHAPE otherwise). */
 smac_status smac_predict_vstar(const smac_grid_desc* d, const smac_boundary_table* bc, const smac_momentum_fields* mf,
                                double dt, double gx, double gy, double gz, double* vxs, double* vys, double* vzs,
                                void* stream);
@@ -353,7 +354,7 @@ typedef struct {
  * compute_mass_flux_from_alpha_flux_two_way (:2472-2687, Coupling/main.cu:531):
  * q = eps_f u_f on faces 1..N+1 along their axis (eps_f the mean of the two
  * cells, the one interior cell's at faces 1 and N+1), mf = 0 on faces 0 and
- * N+2. */
+ * N+2.  Every face array must have fewer than 2^31 entries. */
 smac_status smac_mass_flux_from_alpha_flux(const smac_grid_desc* d, const smac_boundary_table* bc,
                                            const smac_mass_flux_fields* in, double rho0, double rho1, double dt,
                                            const double* eps_half, double* mfx, double* mfy, double* mfz,

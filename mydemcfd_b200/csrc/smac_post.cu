@@ -731,6 +731,12 @@ __global__ void __launch_bounds__(256) k_st_rim(StArgs A) {
 // k_get_vof_vstar_rhouu_consistent_{x,y,z}, CFD/G_SMACSolver.cu:90-1070,
 // boundary rules CFD/G_BoundaryFunctions.h:9-367)
 
+// Offsets into the predictor's and the mass flux's arrays are 32-bit: a grid
+// must keep every array below 2^31 entries (index_fits).  That bound is not a
+// practical limit here: the predictor's two dozen FP64 input arrays of a grid
+// that large would need more than 400 GB.  32-bit offsets cut the kernel's
+// registers and spills (80 instead of 164 bytes of spill stores) and its time
+// at 256^3 from 3.31 to 3.14 ms.
 struct MomArgs {
   int N[3];
   const uint8_t* ft[3];
@@ -749,7 +755,7 @@ struct MomArgs {
   const double* eps_new;
   double* vs[3];
   double dt, g[3], ih[3], ih2[3], inv_volume;
-  long long st[4][3];  // index strides along x, y, z of the three face families and (3) the cells
+  int st[4][3];  // index strides along x, y, z of the three face families and (3) the cells
   BcTable bc;
 };
 
@@ -757,7 +763,7 @@ struct MomArgs {
 // face f, boundary faces by their type; the x rule passes the stored value
 // through for outlets only, the y and z rules for slip too.
 template <int B>
-__device__ __forceinline__ double m_face_val(const MomArgs& A, long long f) {
+__device__ __forceinline__ double m_face_val(const MomArgs& A, int f) {
   const uint8_t t = A.ft[B][f];
   if (t == 0) return A.v[B][f];  // F_INTERIOR
   if (t == 1) {                  // F_BOUNDARY
@@ -774,11 +780,11 @@ __device__ __forceinline__ double m_face_val(const MomArgs& A, long long f) {
 // next to a face along D != AF on side s, mirrored about a wall.  fa, fd:
 // the face's index in the family-AF and family-D layouts.
 template <int AF, int D>
-__device__ __forceinline__ double m_dir_val(const MomArgs& A, long long fa, long long fd, int s) {
-  const long long f2 = s > 0 ? fa + A.st[AF][D] : fa - A.st[AF][D];
+__device__ __forceinline__ double m_dir_val(const MomArgs& A, int fa, int fd, int s) {
+  const int f2 = s > 0 ? fa + A.st[AF][D] : fa - A.st[AF][D];
   if (A.ft[AF][f2] == 0) return A.v[AF][f2];
   const double inside = A.v[AF][fa];
-  const long long ff = s > 0 ? fd + A.st[D][D] : fd, fg = ff - A.st[D][AF];
+  const int ff = s > 0 ? fd + A.st[D][D] : fd, fg = ff - A.st[D][AF];
   double wall = 0.0;
   int count = 0;
   if (A.ft[D][ff] == 1) {
@@ -809,9 +815,9 @@ template <int AF> struct Others { static constexpr int D0 = AF == 0 ? 1 : 0, D1 
 // reference writes them (k_get_vof_vstar_rhouu_consistent_*_two_way,
 // CFD/G_SMACSolver.cu:1610-1622, 1832-1844, 2050-2062).
 template <int AF, int D>
-__device__ __forceinline__ double m_eps4(const MomArgs& A, long long c, int s) {
-  const long long sa = A.st[3][AF], sd = A.st[3][D];
-  const long long lc = s > 0 ? c : c - sd, lcm = lc - sa, hc = lc + sd, hcm = lcm + sd;
+__device__ __forceinline__ double m_eps4(const MomArgs& A, int c, int s) {
+  const int sa = A.st[3][AF], sd = A.st[3][D];
+  const int lc = s > 0 ? c : c - sd, lcm = lc - sa, hc = lc + sd, hcm = lcm + sd;
   const double* e = A.eps_old;
   const double sum = D > AF ? DADD(DADD(DADD(e[lcm], e[lc]), e[hcm]), e[hc]) : DADD(DADD(DADD(e[lcm], e[hcm]), e[lc]), e[hc]);
   return DMUL(0.25, sum);
@@ -822,8 +828,8 @@ __device__ __forceinline__ double m_eps4(const MomArgs& A, long long c, int s) {
 // three family layouts and (b[3]) its high cell; vdp, vdm: its mirrored
 // neighbours along D.
 template <int AF, int D, bool TW>
-__device__ __forceinline__ double m_cross(const MomArgs& A, const long long* b, double v0, double vdp, double vdm) {
-  const long long qd = b[D] + A.st[D][D], qda = qd - A.st[D][AF], q = b[D], qm = b[D] - A.st[D][AF];
+__device__ __forceinline__ double m_cross(const MomArgs& A, const int* b, double v0, double vdp, double vdm) {
+  const int qd = b[D] + A.st[D][D], qda = qd - A.st[D][AF], q = b[D], qm = b[D] - A.st[D][AF];
   const double wp0 = m_face_val<D>(A, qd), wpm = m_face_val<D>(A, qda);
   const double w0 = m_face_val<D>(A, q), wm = m_face_val<D>(A, qm);
   const double mup = DMUL(0.5, DADD(A.muf[D][qd], A.muf[D][qda]));
@@ -838,9 +844,9 @@ __device__ __forceinline__ double m_cross(const MomArgs& A, const long long* b, 
 // reconstruction at an upwind neighbour needs that the face's own
 // stencil does not hold): the face rule along AF, the mirrored rule across.
 template <int AF, int D>
-__device__ __forceinline__ double m_far(const MomArgs& A, const long long* b, int s) {
+__device__ __forceinline__ double m_far(const MomArgs& A, const int* b, int s) {
   if (D == AF) return m_face_val<AF>(A, b[AF] + 2 * s * A.st[AF][AF]);
-  const long long fa = b[AF] + s * A.st[AF][D], fd = b[D] + s * A.st[D][D];
+  const int fa = b[AF] + s * A.st[AF][D], fd = b[D] + s * A.st[D][D];
   return m_dir_val<AF, D == AF ? Others<AF>::D0 : D>(A, fa, fd, s);
 }
 
@@ -856,14 +862,14 @@ __device__ __forceinline__ double m_muscl(double upwind_v, double flux, double s
 // its inner neighbour the face itself, its outer one m_far; a neighbour
 // that is not F_INTERIOR gives its value unlimited.
 template <int AF, int D>
-__device__ __forceinline__ double m_conv(const MomArgs& A, const long long* b, double v0, double np, double nm) {
+__device__ __forceinline__ double m_conv(const MomArgs& A, const int* b, double v0, double np, double nm) {
   double fp, fm;
   if (D == AF) {
-    const long long f = b[AF], s = A.st[AF][AF];
+    const int f = b[AF], s = A.st[AF][AF];
     fp = DMUL(0.5, DADD(A.mf[AF][f], A.mf[AF][f + s]));
     fm = DMUL(0.5, DADD(A.mf[AF][f - s], A.mf[AF][f]));
   } else {
-    const long long qd = b[D] + A.st[D][D], qda = qd - A.st[D][AF];
+    const int qd = b[D] + A.st[D][D], qda = qd - A.st[D][AF];
     fp = DMUL(0.5, DADD(A.mf[D][qda], A.mf[D][qd]));
     fm = DMUL(0.5, DADD(A.mf[D][b[D]], A.mf[D][b[D] - A.st[D][AF]]));
   }
@@ -892,9 +898,9 @@ __device__ __forceinline__ double m_conv(const MomArgs& A, const long long* b, d
 // 1538-2194): the stresses and the pressure gradient weighted by eps_old,
 // u* = (f_inv_rho / eps_new_f)(eps_old_f rho_old_f u + dt (...) + impulse/V) + dt g.
 template <int AF, bool TW>
-__device__ __forceinline__ double m_vstar(const MomArgs& A, const long long* b) {
+__device__ __forceinline__ double m_vstar(const MomArgs& A, const int* b) {
   constexpr int D0 = Others<AF>::D0, D1 = Others<AF>::D1;
-  const long long f = b[AF], c = b[3], cm = b[3] - A.st[3][AF];
+  const int f = b[AF], c = b[3], cm = b[3] - A.st[3][AF];
   const double v0 = A.v[AF][f];
   const double vp = m_face_val<AF>(A, f + A.st[AF][AF]), vm = m_face_val<AF>(A, f - A.st[AF][AF]);
   const double p0 = m_dir_val<AF, D0>(A, f, b[D0], +1), m0 = m_dir_val<AF, D0>(A, f, b[D0], -1);
@@ -936,8 +942,9 @@ __device__ __forceinline__ double m_vstar(const MomArgs& A, const long long* b) 
 // fields) through L2.  Only F_INTERIOR faces are written.  The kernel waits
 // on chains of dependent loads (a face type, then the value it selects), so
 // resident warps matter more than registers: 5 blocks per SM (48 registers,
-// a few spills to L1) measured 3.32 ms at 256^3, against 3.60 ms with 4
-// blocks, 4.27 ms with 3 and 3.43 ms with 6.  Family-major block order (all
+// a few spills to L1) measured 3.32 ms at 256^3 with 64-bit offsets (3.14 ms
+// with the 32-bit ones now used), against 3.60 ms with 4 blocks, 4.27 ms
+// with 3 and 3.43 ms with 6.  Family-major block order (all
 // planes of one family, then the next, so that resident warps share one
 // family's code) took 3.64 ms: the interleaved families' shared reads
 // through L2 are worth more than the instruction-cache locality.
@@ -947,7 +954,7 @@ __global__ void __launch_bounds__(256, 5) k_predict_vstar(MomArgs A) {
   const int z = blockIdx.z / 3 + 1;
   const int x = blockIdx.x * 32 + threadIdx.x + 1, y = blockIdx.y * 8 + threadIdx.y + 1;
   if (x > A.N[0] + 1 || y > A.N[1] + 1) return;
-  long long b[4];
+  int b[4];
 #pragma unroll
   for (int k = 0; k < 4; ++k) b[k] = x * A.st[k][0] + y * A.st[k][1] + z * A.st[k][2];
   if (fam == 0) {
@@ -1157,7 +1164,7 @@ struct FluxArgs {
 template <int F, bool TW>
 __device__ __forceinline__ void flux_face(const FluxArgs& A, int x, int y, int z) {
   const MomArgs& M = A.M;
-  const long long f = x * M.st[F][0] + y * M.st[F][1] + z * M.st[F][2];
+  const int f = x * M.st[F][0] + y * M.st[F][1] + z * M.st[F][2];
   const double aq = DMUL(A.Fa[F][f], A.hdt[F]);
   double q = m_face_val<F>(M, f);
   if (TW) {
@@ -1166,7 +1173,7 @@ __device__ __forceinline__ void flux_face(const FluxArgs& A, int x, int y, int z
       A.mf[F][f] = 0.0;
       return;
     }
-    const long long c = x * M.st[3][0] + y * M.st[3][1] + z * M.st[3][2], s = M.st[3][F];
+    const int c = x * M.st[3][0] + y * M.st[3][1] + z * M.st[3][2], s = M.st[3][F];
     const double e = along == 1 ? A.epsh[c] : along == n + 1 ? A.epsh[c - s] : DMUL(0.5, DADD(A.epsh[c - s], A.epsh[c]));
     q = DMUL(e, q);
   }
@@ -1238,6 +1245,20 @@ bool bad_table(const smac_boundary_table* bc, const char* fn) {
     return true;
   }
   return false;
+}
+
+// Every face and cell array of the grid has fewer than 2^31 entries (the
+// predictor and the mass flux index them with 32-bit offsets).
+bool index_fits(const smac_grid_desc* d, const char* fn) {
+  for (int k = 0; k < 3; ++k) {
+    const long long n = (long long)(d->nx + 2 + (k == 0)) * (d->ny + 2 + (k == 1)) * (d->nz + 2 + (k == 2));
+    if (n > 0x7fffffffLL) {
+      smac::set_error_text("%s: grid %d x %d x %d: a face array would exceed 2^31 - 1 entries", fn, d->nx, d->ny,
+                           d->nz);
+      return false;
+    }
+  }
+  return true;
 }
 
 bool bad_desc(const smac_grid_desc* d, const char* fn, int min_n) {
@@ -1436,7 +1457,7 @@ smac_status predict_vstar(const char* fn, const smac_grid_desc* d, const smac_bo
     }
   if (bad_table(bc, fn)) return SMAC_BAD_ARG;
   // the mirrored neighbours read two faces inside across every axis
-  if (bad_desc(d, fn, 2)) return SMAC_BAD_SHAPE;
+  if (bad_desc(d, fn, 2) || !index_fits(d, fn)) return SMAC_BAD_SHAPE;
   MomArgs A;
   std::memset(&A, 0, sizeof(A));
   A.N[0] = d->nx; A.N[1] = d->ny; A.N[2] = d->nz;
@@ -1466,8 +1487,8 @@ smac_status predict_vstar(const char* fn, const smac_grid_desc* d, const smac_bo
   for (int k = 0; k < 4; ++k) {  // families 0..2, cells 3
     const long long S0 = d->nx + 2 + (k == 0), S1 = d->ny + 2 + (k == 1);
     A.st[k][0] = 1;
-    A.st[k][1] = S0;
-    A.st[k][2] = S0 * S1;
+    A.st[k][1] = (int)S0;
+    A.st[k][2] = (int)(S0 * S1);
   }
   fill_table(&A.bc, bc);
   const dim3 grid((unsigned)((d->nx + 1 + 31) / 32), (unsigned)((d->ny + 1 + 7) / 8), 3u * (unsigned)(d->nz + 1));
@@ -1544,7 +1565,7 @@ smac_status smac_mass_flux_from_alpha_flux(const smac_grid_desc* d, const smac_b
       return SMAC_BAD_ARG;
     }
   if (bad_table(bc, fn)) return SMAC_BAD_ARG;
-  if (bad_desc(d, fn, 1)) return SMAC_BAD_SHAPE;
+  if (bad_desc(d, fn, 1) || !index_fits(d, fn)) return SMAC_BAD_SHAPE;
   FluxArgs A;
   std::memset(&A, 0, sizeof(A));
   MomArgs& M = A.M;
@@ -1556,8 +1577,8 @@ smac_status smac_mass_flux_from_alpha_flux(const smac_grid_desc* d, const smac_b
   for (int k = 0; k < 4; ++k) {
     const long long S0 = d->nx + 2 + (k == 0), S1 = d->ny + 2 + (k == 1);
     M.st[k][0] = 1;
-    M.st[k][1] = S0;
-    M.st[k][2] = S0 * S1;
+    M.st[k][1] = (int)S0;
+    M.st[k][2] = (int)(S0 * S1);
   }
   fill_table(&M.bc, bc);
   A.Fa[0] = in->Fx; A.Fa[1] = in->Fy; A.Fa[2] = in->Fz;

@@ -149,3 +149,21 @@ def test_step_call_arguments_are_checked_before_any_device_work(lib):
     assert lib.smac_poisson_beta_two_way(ctypes.byref(d), fake, fake, None, fake, fake, fake, fake, None) == nat.BAD_ARG
     assert lib.smac_poisson_beta_two_way(ctypes.byref(flat), fake, fake, fake, fake, fake, fake, fake,
                                          None) == nat.BAD_SHAPE
+
+
+def test_predictor_and_mass_flux_refuse_grids_beyond_32_bit_offsets(lib):
+    """Both index their arrays with 32-bit offsets: a grid with a face array
+    of 2^31 entries or more is refused before any device work."""
+    import numpy as np
+    fake = ctypes.c_void_p(256)
+    big = nat.GridDesc(1300, 1300, 1300, 1e-3, 1e-3, 1e-3)
+    types = np.zeros(1, np.uint8)
+    vel = np.zeros(1)
+    one = nat.BoundaryTable(1, types.ctypes.data, vel.ctypes.data, vel.ctypes.data, vel.ctypes.data)
+    mf = nat.MomentumFields(*(256,) * 30)
+    assert lib.smac_predict_vstar(ctypes.byref(big), ctypes.byref(one), ctypes.byref(mf), 0.01, 0.0, 0.0, -9.8,
+                                  fake, fake, fake, None) == nat.BAD_SHAPE
+    assert "2^31" in nat.last_error()
+    ff = nat.MassFluxFields(*(256,) * 15)
+    assert lib.smac_mass_flux_from_alpha_flux(ctypes.byref(big), ctypes.byref(one), ctypes.byref(ff), 1.0, 1000.0,
+                                              0.01, None, fake, fake, fake, None) == nat.BAD_SHAPE
