@@ -175,7 +175,8 @@ typedef struct {
  *  - F_INTERIOR faces: rho_f = the two cells' mean, f_b = f_inv_rho =
  *    1/rho_f, mu_f = the mean viscosity; other faces with indices 1..N+2
  *    along, 1..N+1 across: f_b = f_inv_rho = 0 (:1409-1535).
- * One launch computes every final value from alpha and the types.  The ghost
+ * One launch computes every final value from alpha and the types; every
+ * face array must have fewer than 2^31 entries (SMAC_BAD_SHAPE otherwise).  The ghost
  * layer must not hold C_INTERIOR cells next to C_SOLID interior cells (the
  * reference's set-up types it C_GHOST, CFD/SMACSolver.cpp:220; there the
  * reference's own passes would race).

@@ -152,8 +152,9 @@ def test_step_call_arguments_are_checked_before_any_device_work(lib):
 
 
 def test_predictor_and_mass_flux_refuse_grids_beyond_32_bit_offsets(lib):
-    """Both index their arrays with 32-bit offsets: a grid with a face array
-    of 2^31 entries or more is refused before any device work."""
+    """The predictor, the mass flux and the property update index their
+    arrays with 32-bit offsets: a grid with a face array of 2^31 entries or
+    more is refused before any device work."""
     import numpy as np
     fake = ctypes.c_void_p(256)
     big = nat.GridDesc(1300, 1300, 1300, 1e-3, 1e-3, 1e-3)
@@ -167,3 +168,7 @@ def test_predictor_and_mass_flux_refuse_grids_beyond_32_bit_offsets(lib):
     ff = nat.MassFluxFields(*(256,) * 15)
     assert lib.smac_mass_flux_from_alpha_flux(ctypes.byref(big), ctypes.byref(one), ctypes.byref(ff), 1.0, 1000.0,
                                               0.01, None, fake, fake, fake, None) == nat.BAD_SHAPE
+    vp = nat.VofParams(1.0, 1000.0, 1e-3, 1e-1)
+    out = nat.PropertyFields(*(256,) * 15)
+    assert lib.smac_update_properties(ctypes.byref(big), ctypes.byref(vp), fake, fake, fake, fake, fake,
+                                      ctypes.byref(out), None) == nat.BAD_SHAPE
