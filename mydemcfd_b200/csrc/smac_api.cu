@@ -1061,7 +1061,7 @@ smac_status run_solve(smac_handle* h, const double** xout) {
       if (h->hs->status == 2 && restarts < 3) {
         // Breakdown (p.Ap or r.z <= 0).  Near the rounding floor of a tight
         // tolerance it means the Krylov space is exhausted, not failure:
-        // judge by the FP64 true residual and restart PCG from it.
+        // decide by the FP64 true residual and restart PCG from it.
         const Scalars& hs0 = *h->hs;
         const int it_now = hs0.iter;
         auto S = stencil<double, double>(g, h->lv[0].bx64, h->lv[0].by64, h->lv[0].bz64);

@@ -7,7 +7,7 @@ Random numbers: SplitMix64(seed) -> u = (bits >> 11) * 2^-53 -> 2u - 1,
 uniform in [-1, 1); the i-th draw of a stream depends only on (seed, i), so
 the same arrays come out on any host.
 
-Workloads (BASELINE configurations; seeded synthetic fields with the stated
+Workloads (the benchmark configurations; seeded synthetic fields with the stated
 shapes stand in for simulation state):
   plain   - single phase, rho = 1 (f_b = 1 on interior faces), dt = 1,
             u* i.i.d. U[-1,1) on F_INTERIOR faces, 0 on the others

@@ -142,7 +142,7 @@ def _device_ms(fn, reps=8):
 
 @pytest.mark.skipif(not REF.available(), reason="reference build oracle/_ref not present")
 def test_post_pass_against_reference_time_256():
-    """update_boundary_ghost and make_face_gradp: this build's calls against
+    """update_boundary_ghost and make_face_gradp: this library's calls against
     the reference's own kernels on the same 256^3 inputs, device time."""
     c = W.post_case((256, 256, 256), seed=7, sides=("x+",), solid_fraction=0.05)
     REF.post(c)  # loads the reference's kernels

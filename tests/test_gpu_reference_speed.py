@@ -5,11 +5,11 @@ sources (oracle/_ref, test infrastructure).  Both run the 256³ plain input to
 a 1e-8 true relative residual:
 - the reference stops on its own rule, max|r|·dt < tol checked every 5
   iterations, so its tol is lowered until its output meets 1e-8 (measured
-  with this build's operator, which matches the reference's to 1e-13);
-- this build is called the way the reference's driver calls its solver
+  with this library's operator, which matches the reference's to 1e-13);
+- this library is called the way the reference's driver calls its solver
   (coefficients, RHS, solve: G_PressureSolverBase::solve).
 Both are timed with CUDA events around the call, host waits included (the
-reference copies its residual to the host every 5 iterations; this build
+reference copies its residual to the host every 5 iterations; this library
 reads its convergence flag once per two iterations).
 """
 import pytest
@@ -87,7 +87,7 @@ def test_faster_than_reference_gpu_solve_256():
     print(f"reference GPU solve 256^3: tol {tol:.3g} (max|r|*dt), {out['iterations']} iterations, "
           f"rel residual {rel:.2e}, {ref_ms:.2f} ms")
     for name, (ms, it, mine) in res.items():
-        print(f"this build {name}: {it} iterations, rel residual {mine:.2e}, {ms:.2f} ms, "
+        print(f"this library {name}: {it} iterations, rel residual {mine:.2e}, {ms:.2f} ms, "
               f"{ref_ms / ms:.1f}x the reference")
     assert res["fp64"][0] < ref_ms
     assert res["mixed"][0] < ref_ms
