@@ -417,6 +417,16 @@ class SMACStep:
         mass_flux_device(g.N, (g.dx_, g.dy_, g.dz_), self.bc_, f, rho0, rho1, self.dt_,
                          (g.f_mfx_, g.f_mfy_, g.f_mfz_), eps_half=g.void_fraction_half_ if two_way else None)
 
+    def update_boundary_faces(self):
+        """G_SMACSolver::update_boundary_faces (CFD/G_SMACSolver_VoF.cu:1798-1950):
+        f_b*_ of the outlet faces marked in f_*outlet_ become twice the f_b of
+        their interior neighbour (smac_update_boundary_faces)."""
+        g = self.grid_
+        if g.f_xoutlet_ is None:
+            raise ValueError("update_boundary_faces needs the grid's f_*outlet_ marks")
+        update_boundary_faces_device(g.N, (g.dx_, g.dy_, g.dz_), (g.f_xoutlet_, g.f_youtlet_, g.f_zoutlet_),
+                                     (g.f_bx_, g.f_by_, g.f_bz_))
+
     def update_poisson_beta_two_way(self):
         """G_CFDDEMCoupling::update_poisson_beta_two_way
         (Coupling/G_CFDDEMCoupling.cu:419-460): f_b*_ = eps_f f_inv_rho*_ from

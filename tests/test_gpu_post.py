@@ -697,3 +697,28 @@ def test_smac_step_mass_flux_matches_oracle():
         torch.cuda.synchronize()
         for a, b in zip((g.f_mfx_, g.f_mfy_, g.f_mfz_), O.mass_flux(case)):
             assert np.array_equal(a.cpu().numpy(), b)
+
+
+def test_smac_step_boundary_faces_and_two_way_coefficients_match_oracle():
+    """SMACStep.update_boundary_faces (outlet f_b) and, on the same grid,
+    SMACStep.update_poisson_beta_two_way (f_b = eps_f f_inv_rho)."""
+    c = W.post_case((16, 12, 10), seed=23, sides=("x+", "y-"), solid_fraction=0.1)
+    sh = W.shapes(c.N)
+    g = DeviceGrid(*c.N, *c.h, *(_cuda(a) for a in c.vs), *(_cuda(a) for a in c.fb), *(_cuda(a) for a in c.fb),
+                   _cuda(c.ct), *(_cuda(a) for a in c.ft), _cuda(c.p), _cuda(c.p_delta),
+                   torch.zeros(sh["cell"], dtype=torch.float64, device="cuda"), *(_cuda(a) for a in c.v))
+    g.f_xoutlet_, g.f_youtlet_, g.f_zoutlet_ = (_cuda(a) for a in c.marks)
+    step = SMACStep(g, c.dt, g=c.g, bc=BoundaryConditions(c.bc_type, *c.bc_v))
+    step.update_boundary_faces()
+    torch.cuda.synchronize()
+    want = O.update_boundary_faces(c.N, *c.marks, *c.fb)
+    for a, b in zip((g.f_bx_, g.f_by_, g.f_bz_), want):
+        assert np.array_equal(a.cpu().numpy(), b)
+    N, h, eps, fir, fb = W.beta_two_way_case(c.N, seed=23)
+    g.void_fraction_ = _cuda(eps)
+    g.f_inv_rhox_, g.f_inv_rhoy_, g.f_inv_rhoz_ = (_cuda(a) for a in fir)
+    g.f_bx_, g.f_by_, g.f_bz_ = (_cuda(a) for a in fb)
+    step.update_poisson_beta_two_way()
+    torch.cuda.synchronize()
+    for a, b in zip((g.f_bx_, g.f_by_, g.f_bz_), O.poisson_beta_two_way(N, eps, fir, fb)):
+        assert np.array_equal(a.cpu().numpy(), b)
