@@ -684,3 +684,31 @@ def test_mass_flux_oracle_matches_reference_golden(oracle_lib, name):
     meta, arr = load_golden(name)
     for k, a in zip(("mfx", "mfy", "mfz"), oracle_lib.mass_flux(flux_case_from_spec(meta))):
         assert np.array_equal(a, arr[k]), k
+
+
+def test_predict_vstar_two_way_fluid_at_rest_known_answer(oracle_lib):
+    """Known answer of the two-way form: with u = 0, no advecting flux and
+    zero boundary velocities every stress and flux term is 0, so on each
+    F_INTERIOR face u* = (1 - s)((f_inv_rho / eps_new_f)(eps_old_f rho_old_f 0
+    + dt (0 - eps_old_f (p - p_m) / h) + I/V) + dt g), with the operations in
+    the reference's order (CFD/G_SMACSolver.cu:1734-1757)."""
+    import dataclasses
+    m = W.momentum_case((8, 7, 6), seed=14, solid_fraction=0.3, two_way=True)
+    zero = lambda arrs: tuple(np.zeros_like(a) for a in arrs)  # noqa: E731
+    m = dataclasses.replace(m, v=zero(m.v), mf=zero(m.mf), bc_v=zero(m.bc_v))
+    got = oracle_lib.predict_vstar(m)
+    inv_vol = (1.0 / m.h[0]) * (1.0 / m.h[1]) * (1.0 / m.h[2])
+    for a in range(3):
+        t = m.ft[a]
+        z, y, x = np.nonzero(t == W.F_INTERIOR)
+        cz, cy, cx = z.copy(), y.copy(), x.copy()
+        (cx, cy, cz)[a][...] -= 1
+        eo = 0.5 * (m.eps_old[cz, cy, cx] + m.eps_old[z, y, x])
+        en = 0.5 * (m.eps_new[cz, cy, cx] + m.eps_new[z, y, x])
+        tmp = 0.0 - (eo * (m.p[z, y, x] - m.p[cz, cy, cx])) * (1.0 / m.h[a])
+        rho_f = 0.5 * (m.rho_old[z, y, x] + m.rho_old[cz, cy, cx])
+        coup = m.imp[a][z, y, x] * inv_vol
+        want = (m.fir[a][z, y, x] / en) * ((eo * rho_f) * 0.0 + m.dt * tmp + coup) + m.dt * m.g[a]
+        want = (1.0 - m.sf[a][z, y, x]) * want
+        np.testing.assert_array_equal(got[a][z, y, x], want)
+        np.testing.assert_array_equal(got[a][t != W.F_INTERIOR], m.vs[a][t != W.F_INTERIOR])
