@@ -712,3 +712,75 @@ def test_predict_vstar_two_way_fluid_at_rest_known_answer(oracle_lib):
         want = (1.0 - m.sf[a][z, y, x]) * want
         np.testing.assert_array_equal(got[a][z, y, x], want)
         np.testing.assert_array_equal(got[a][t != W.F_INTERIOR], m.vs[a][t != W.F_INTERIOR])
+
+
+def _props_passes_numpy(N, rho0, rho1, mu0, mu1, alpha, ct, ft, init):
+    """The reference's property passes one after another, in numpy
+    (CFD/G_SMACSolver_VoF.cu:1244-1535): mixing on C_INTERIOR /
+    C_NEAR_BOUNDARY cells 1..N+1, the solid rule on interior C_SOLID cells
+    (first C_INTERIOR neighbour x-, x+, y-, y+, z-, z+, else 0), ghost cells
+    from the nearest interior cell, then the faces."""
+    nx, ny, nz = N
+    out = {k: np.array(v, copy=True) for k, v in init.items()}
+    rho, inv, mu = out["rho"], out["inv_rho"], out["mu"]
+    box = (slice(1, nz + 2), slice(1, ny + 2), slice(1, nx + 2))
+    mix = (ct[box] == 0) | (ct[box] == 1)
+    a = alpha[box]
+    r = (1.0 - a) * rho0 + a * rho1
+    rho[box] = np.where(mix, r, rho[box])
+    inv[box] = np.where(mix, 1.0 / r, inv[box])
+    mu[box] = np.where(mix, (1.0 - a) * mu0 + a * mu1, mu[box])
+    r1, m1 = rho.copy(), mu.copy()
+    for z in range(1, nz + 1):
+        for y in range(1, ny + 1):
+            for x in range(1, nx + 1):
+                if ct[z, y, x] != 3:
+                    continue
+                rho[z, y, x] = mu[z, y, x] = 0.0
+                for dz, dy, dx in ((0, 0, -1), (0, 0, 1), (0, -1, 0), (0, 1, 0), (-1, 0, 0), (1, 0, 0)):
+                    if ct[z + dz, y + dy, x + dx] == 0:
+                        rho[z, y, x], mu[z, y, x] = r1[z + dz, y + dy, x + dx], m1[z + dz, y + dy, x + dx]
+                        break
+    for z in range(nz + 2):
+        for y in range(ny + 2):
+            for x in range(nx + 2):
+                if 0 < x <= nx and 0 < y <= ny and 0 < z <= nz:
+                    continue
+                s = (min(max(z, 1), nz), min(max(y, 1), ny), min(max(x, 1), nx))
+                rho[z, y, x], mu[z, y, x] = rho[s], mu[s]
+    for k, ax in enumerate("xyz"):
+        t = ft[k]
+        lo = [slice(1, nz + 2), slice(1, ny + 2), slice(1, nx + 2)]
+        lo[2 - k] = slice(1, (nz, ny, nx)[2 - k] + 3)
+        lo = tuple(lo)
+        hi = [slice(1, nz + 2), slice(1, ny + 2), slice(1, nx + 2)]
+        mlo = [slice(1, nz + 2), slice(1, ny + 2), slice(1, nx + 2)]
+        mlo[2 - k] = slice(0, (nz, ny, nx)[2 - k] + 1)
+        inner = t[tuple(hi)] == 0
+        fr = 0.5 * (rho[tuple(hi)] + rho[tuple(mlo)])
+        fm = 0.5 * (mu[tuple(hi)] + mu[tuple(mlo)])
+        for key in ("fb", "fir"):
+            out[key + ax][lo] = 0.0
+        out["fb" + ax][tuple(hi)] = np.where(inner, 1.0 / fr, 0.0)
+        out["fir" + ax][tuple(hi)] = np.where(inner, 1.0 / fr, 0.0)
+        out["rho" + ax][tuple(hi)] = np.where(inner, fr, out["rho" + ax][tuple(hi)])
+        out["mu" + ax][tuple(hi)] = np.where(inner, fm, out["mu" + ax][tuple(hi)])
+    return out
+
+
+def test_update_properties_oracle_matches_passes_with_near_boundary_cells(oracle_lib):
+    """Cells of all four types (C_NEAR_BOUNDARY and isolated C_SOLID cells
+    included): the oracle equals the reference's passes run in order."""
+    N, h, prm, alpha, ct, ft, init = W.property_case((7, 6, 5), seed=31, solid_fraction=0.25)
+    ct = ct.copy()
+    inside = ct[1:-1, 1:-1, 1:-1]
+    u = W.uniform01(W.substream(31, 900), inside.size).reshape(inside.shape)
+    inside[(inside == W.C_INTERIOR) & (u < 0.3)] = 1   # C_NEAR_BOUNDARY
+    inside[(inside == W.C_INTERIOR) & (u > 0.93)] = W.C_SOLID
+    assert (inside == 1).sum() > 20 and (inside == W.C_SOLID).sum() > 20
+    src = dict(init)
+    src["rho"] = init["rho_old"]
+    got = oracle_lib.update_properties(N, *prm, alpha, ct, ft, src)
+    want = _props_passes_numpy(N, *prm, alpha, ct, ft, {k: src[k] for k in got})
+    for k in got:
+        np.testing.assert_array_equal(got[k], want[k], err_msg=k)
