@@ -485,13 +485,22 @@ PROPERTY_KEYS = ("rho", "rho_old", "inv_rho", "mu", "fbx", "fby", "fbz", "firx",
                  "rhoz", "mux", "muy", "muz")
 
 
-def property_case(N, seed, solid_fraction=0.0, rho=(1.0, 1000.0), mu=(1e-3, 1e-1)):
+def property_case(N, seed, solid_fraction=0.0, rho=(1.0, 1000.0), mu=(1e-3, 1e-1), mixed_types=False):
     """Inputs of the property update: alpha of a seeded sphere (1.5-cell
     ramp) plus 20% of the cells U[0,1); box types with clustered solids
     (post_case's rule); every output array filled with U[-1,1) beforehand,
-    so that entries the update must not write are checked too.  Returns
+    so that entries the update must not write are checked too.  mixed_types:
+    30% of the C_INTERIOR cells become C_NEAR_BOUNDARY and 7% isolated
+    C_SOLID cells (faces unchanged).  Returns
     (N, h, (rho0, rho1, mu0, mu1), alpha, ct, ft, init)."""
     base = post_case(N, seed, sides=(), solid_fraction=solid_fraction)
+    if mixed_types:
+        ct = base.ct.copy()
+        inside = ct[1:-1, 1:-1, 1:-1]
+        u = uniform01(substream(seed, 900), inside.size).reshape(inside.shape)
+        inside[(inside == C_INTERIOR) & (u < 0.3)] = 1   # C_NEAR_BOUNDARY
+        inside[(inside == C_INTERIOR) & (u > 0.93)] = C_SOLID
+        base = PostCase(**{**base.__dict__, "ct": ct})
     N = base.N
     sh = shapes(N)
     n = int(np.prod(sh["cell"]))

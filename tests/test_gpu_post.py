@@ -455,6 +455,7 @@ def _oracle_props(N, prm, alpha, ct, ft, init):
     dict(N=(16, 16, 16), seed=2, solid_fraction=0.35),
     dict(N=(33, 18, 20), seed=5, solid_fraction=0.2),
     dict(N=(1, 7, 5), seed=8, solid_fraction=0.1),
+    dict(N=(19, 14, 11), seed=31, solid_fraction=0.25, mixed_types=True),
 ])
 def test_update_properties_bit_exact_against_oracle(spec):
     N, h, prm, alpha, ct, ft, init = W.property_case(**spec)

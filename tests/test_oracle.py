@@ -771,12 +771,8 @@ def _props_passes_numpy(N, rho0, rho1, mu0, mu1, alpha, ct, ft, init):
 def test_update_properties_oracle_matches_passes_with_near_boundary_cells(oracle_lib):
     """Cells of all four types (C_NEAR_BOUNDARY and isolated C_SOLID cells
     included): the oracle equals the reference's passes run in order."""
-    N, h, prm, alpha, ct, ft, init = W.property_case((7, 6, 5), seed=31, solid_fraction=0.25)
-    ct = ct.copy()
+    N, h, prm, alpha, ct, ft, init = W.property_case((7, 6, 5), seed=31, solid_fraction=0.25, mixed_types=True)
     inside = ct[1:-1, 1:-1, 1:-1]
-    u = W.uniform01(W.substream(31, 900), inside.size).reshape(inside.shape)
-    inside[(inside == W.C_INTERIOR) & (u < 0.3)] = 1   # C_NEAR_BOUNDARY
-    inside[(inside == W.C_INTERIOR) & (u > 0.93)] = W.C_SOLID
     assert (inside == 1).sum() > 20 and (inside == W.C_SOLID).sum() > 20
     src = dict(init)
     src["rho"] = init["rho_old"]
