@@ -91,7 +91,18 @@ typedef struct {
                              fallen by this factor since the last recomputation, default 1e-4 */
   int bf16_coarse_cells;  /* MIXED: grids with at most this many cells store BF16 coefficients
                              (default 4096, i.e. 16^3 and below); 0 disables BF16 */
+  int sweep_kernel;       /* smac_sweep_kernel: which kernel runs the fused red-black sweeps of the
+                             separately launched grids, default SMAC_SWEEP_AUTO; every choice gives
+                             the same result bit for bit */
 } smac_options;
+
+typedef enum {
+  SMAC_SWEEP_AUTO = 0,     /* the register z-march where the grid allows it, else the TMA ring */
+  SMAC_SWEEP_TMA = 1,      /* tiles staged in a shared-memory ring by the Tensor Memory Accelerator */
+  SMAC_SWEEP_ZMARCH = 2,   /* whole x-rows per warp, a register z-march (x extent <= 256 cells);
+                              other grids fall back to the TMA ring */
+  SMAC_SWEEP_SHARED = 3    /* tiles staged in shared memory by plain loads */
+} smac_sweep_kernel;
 
 typedef struct {
   int status;              /* smac_status of the solve */
@@ -472,7 +483,8 @@ smac_status smac_time_kernel(smac_handle* h, int kernel_id, int reps, float* ms_
  * grids need ceil(nx/32)*ceil(ny/4) <= 8192 (x-y planes up to 1024 x 1024),
  * larger ones are refused with SMAC_BAD_SHAPE.  The first call on a device
  * looks up the array's device address (cudaGetSymbolAddress), so make that
- * first call before any stream capture.  All calls share the one array:
+ * first call before any stream capture; a call after the device's context
+ * has changed (cudaDeviceReset) looks it up again.  All calls share the one array:
  * calls that overlap on the GPU (other streams, other threads) race; order
  * them on one stream.  All pointers are device pointers; x's ghost entries are
  * not read. */

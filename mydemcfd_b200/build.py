@@ -19,6 +19,7 @@ DEPS = SOURCES + [
     os.path.join(HERE, "csrc", "smac_kernels.cuh"),
     os.path.join(HERE, "csrc", "smac_rbgs.cuh"),
     os.path.join(HERE, "csrc", "smac_rbgs_tma.cuh"),
+    os.path.join(HERE, "csrc", "smac_rbgs_zm.cuh"),
     os.path.join(ROOT, "include", "smac_b200.h"),
 ]
 NVCC_FLAGS = [

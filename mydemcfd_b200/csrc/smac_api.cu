@@ -12,6 +12,7 @@
 #include "smac_kernels.cuh"
 #include "smac_rbgs.cuh"
 #include "smac_rbgs_tma.cuh"
+#include "smac_rbgs_zm.cuh"
 
 #include <cudaTypedefs.h>
 #include <type_traits>
@@ -111,6 +112,7 @@ struct smac_handle {
   int num_sms = 148;
   bool use_tma = true;     // fused sweeps stage their tiles with the copy engine
   int tma_ctas[2] = {1, 1};  // resident CTAs per SM of the TMA sweep: [0] FP32, [1] FP64
+  int zm_ctas[2][3] = {{0, 0, 0}, {0, 0, 0}};  // resident CTAs per SM of the z-march: [FP32, FP64][shape]
   Scalars* s = nullptr;    // device
   Scalars* hs = nullptr;   // pinned, mapped host mirror of the device scalars
   Scalars* hs_dev = nullptr;  // the mirror's device-side address
@@ -198,6 +200,7 @@ smac_status validate_options(const smac_options* o) {
   if (o->nu1 < 1 || o->nu2 < 1 || o->nu1 > 16 || o->nu2 > 16) { set_err("options: nu1, nu2 in [1,16]"); return SMAC_BAD_ARG; }
   if (o->coarse_sweeps < 1 || o->coarse_sweeps > 1024) { set_err("options: coarse_sweeps in [1,1024]"); return SMAC_BAD_ARG; }
   if (o->check_every < 1) { set_err("options: check_every >= 1"); return SMAC_BAD_ARG; }
+  if (o->sweep_kernel < 0 || o->sweep_kernel > 3) { set_err("options: sweep_kernel %d", o->sweep_kernel); return SMAC_BAD_ARG; }
   if (!(o->reliable_delta > 0.0 && o->reliable_delta < 1.0)) { set_err("options: reliable_delta in (0,1)"); return SMAC_BAD_ARG; }
   return SMAC_OK;
 }
@@ -258,15 +261,69 @@ void launch_tma_sweep(smac_handle* h, int l, const SweepMaps& maps, T* xout, con
                                                                     Lc.cz, h->s, h->red, zc);
 }
 
+// z-march shapes: the whole x extent in WX warps of 32 x NV cells, TY tile
+// rows.  Shape 0: one warp per row (x extent <= 32 NV), 14 rows; shape 1: two
+// warps (<= 64 NV), 6 rows; shape 2: four warps (<= 128 NV), 2 rows.
+template <class T> constexpr int zm_wx(int shape) { return shape == 0 ? 1 : shape == 1 ? 2 : 4; }
+template <class T> constexpr int zm_ty(int shape) { return shape == 0 ? 14 : shape == 1 ? 6 : 2; }
+template <class T>
+int zm_shape(const smac_handle* h, const Geom& g) {
+  constexpr int NV = Vec16<T>::n;
+  const int pt = sizeof(T) == 8 ? 1 : 0;
+  for (int sh = 0; sh < 3; ++sh)
+    if (g.nx <= 32 * NV * zm_wx<T>(sh) && h->zm_ctas[pt][sh] > 0) return sh;
+  return -1;
+}
+
+template <class T, int WX, int TY, int MODE, bool DOT>
+void launch_zm_shape(smac_handle* h, int l, const T* xin, T* xout, const T* rhs, const double* sh, const void* bx,
+                     const void* by, const void* bz, int c0, const T* xc, int ctas) {
+  typedef ZmTile<T, WX, TY> Z;
+  const Geom& g = h->lv[l].g;
+  const Level& Lc = h->lv[l + 1 < h->nlev ? l + 1 : l];
+  // z-chunk: the fewest planes per CTA, counting the two extra c0 planes of each item
+  const long long nty = (g.ny + TY - 1) / TY;
+  const long long slots = (long long)ctas * h->num_sms;
+  int zc = g.nz;
+  long long best = -1;
+  for (int cand = std::min(64, g.nz); cand >= std::min(4, g.nz); --cand) {
+    const long long items = nty * ((g.nz + cand - 1) / cand);
+    const long long cost = ((items + slots - 1) / slots) * (cand + 2);
+    if (best < 0 || cost < best) { best = cost; zc = cand; }
+  }
+  const long long items = nty * ((g.nz + zc - 1) / zc);
+  const int G = (int)std::max(1LL, std::min(slots, items));
+  Stencil<T, T> S{(const T*)bx, (const T*)by, (const T*)bz};
+  k_rbgs_zm<T, WX, TY, MODE, DOT><<<G, Z::NT, Z::SMEM, h->stream>>>(g, xin, xout, rhs, sh, S, c0, xc, Lc.g, Lc.cx,
+                                                                     Lc.cy, Lc.cz, h->s, h->red, zc);
+}
+
+template <class T, int MODE, bool DOT>
+void launch_zm(smac_handle* h, int l, int shape, const T* xin, T* xout, const T* rhs, const double* sh,
+               const void* bx, const void* by, const void* bz, int c0, const T* xc) {
+  const int n = h->zm_ctas[sizeof(T) == 8 ? 1 : 0][shape];
+  if (shape == 0) launch_zm_shape<T, zm_wx<T>(0), zm_ty<T>(0), MODE, DOT>(h, l, xin, xout, rhs, sh, bx, by, bz, c0, xc, n);
+  else if (shape == 1) launch_zm_shape<T, zm_wx<T>(1), zm_ty<T>(1), MODE, DOT>(h, l, xin, xout, rhs, sh, bx, by, bz, c0, xc, n);
+  else launch_zm_shape<T, zm_wx<T>(2), zm_ty<T>(2), MODE, DOT>(h, l, xin, xout, rhs, sh, bx, by, bz, c0, xc, n);
+}
+
 template <class T, class CS>
 void launch_sweep(smac_handle* h, int l, int mode, bool dot, const T* xin, T* xout, const T* rhs, const double* sh,
                   const void* bx, const void* by, const void* bz, int c0, const T* xc) {
   const Level& L = h->lv[l];
   const Geom& g = L.g;
   const Level& Lc = h->lv[l + 1 < h->nlev ? l + 1 : l];
+  const int sk = h->opts.sweep_kernel;
   if constexpr (std::is_same<T, CS>::value) {
+    const int zs = (sk == SMAC_SWEEP_ZMARCH) ? zm_shape<T>(h, g) : -1;
+    if (zs >= 0) {
+      if (mode == 0) { if (dot) launch_zm<T, 0, true>(h, l, zs, xin, xout, rhs, sh, bx, by, bz, c0, xc); else launch_zm<T, 0, false>(h, l, zs, xin, xout, rhs, sh, bx, by, bz, c0, xc); }
+      else if (mode == 1) { if (dot) launch_zm<T, 1, true>(h, l, zs, xin, xout, rhs, sh, bx, by, bz, c0, xc); else launch_zm<T, 1, false>(h, l, zs, xin, xout, rhs, sh, bx, by, bz, c0, xc); }
+      else { if (dot) launch_zm<T, 2, true>(h, l, zs, xin, xout, rhs, sh, bx, by, bz, c0, xc); else launch_zm<T, 2, false>(h, l, zs, xin, xout, rhs, sh, bx, by, bz, c0, xc); }
+      return;
+    }
     const bool ok = sizeof(T) == 8 ? L.tma64 : L.tma32;
-    if (h->use_tma && ok) {
+    if (h->use_tma && ok && sk != SMAC_SWEEP_SHARED) {
       // the maps bind the level's two iterate buffers, its rhs and coefficients
       const SweepMaps* mp = sizeof(T) == 8 ? L.mp64 : L.mp32;
       const void* xb = (l == 0) ? (sizeof(T) == 8 ? (const void*)h->z64b : (const void*)h->z32b)
@@ -589,6 +646,27 @@ cudaError_t tma_attr() {
                               TmaTile<T>::SMEM_BYTES);
 }
 
+// Resident CTAs per SM of each z-march shape (0: not usable).
+template <class T, int SH>
+int zm_occupancy() {
+  typedef ZmTile<T, zm_wx<T>(SH), zm_ty<T>(SH)> Z;
+  int n = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_rbgs_zm<T, zm_wx<T>(SH), zm_ty<T>(SH), 0, true>, Z::NT,
+                                                    Z::SMEM) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  return n;
+}
+void setup_zm(smac_handle* h) {
+  h->zm_ctas[0][0] = zm_occupancy<float, 0>();
+  h->zm_ctas[0][1] = zm_occupancy<float, 1>();
+  h->zm_ctas[0][2] = zm_occupancy<float, 2>();
+  h->zm_ctas[1][0] = zm_occupancy<double, 0>();
+  h->zm_ctas[1][1] = zm_occupancy<double, 1>();
+  h->zm_ctas[1][2] = zm_occupancy<double, 2>();
+}
+
 // Tensor maps for every separately launched grid, or use_tma = false.
 void setup_tma(smac_handle* h) {
   h->use_tma = false;
@@ -660,6 +738,7 @@ smac_status smac_default_options(smac_options* o) {
   o->check_every = 1;
   o->reliable_delta = 1e-4;
   o->bf16_coarse_cells = COARSE_CELLS;
+  o->sweep_kernel = SMAC_SWEEP_AUTO;
   return SMAC_OK;
 }
 
@@ -797,6 +876,7 @@ smac_status smac_create(const smac_grid_desc* desc, const smac_options* opts, vo
   }
   h->num_sms = prop.multiProcessorCount;
   setup_tma(h);
+  setup_zm(h);
   cudaError_t es = cudaStreamSynchronize(h->stream);
   if (es != cudaSuccess) { set_err("smac_create: %s", cudaGetErrorString(es)); return fail(SMAC_CUDA_ERROR); }
   *out = h;

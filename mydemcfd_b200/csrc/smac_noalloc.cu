@@ -17,6 +17,8 @@
 #include "smac_b200.h"
 #include "smac_common.cuh"
 
+#include <cudaTypedefs.h>
+
 using namespace smac;
 
 namespace smac {
@@ -43,9 +45,28 @@ static __device__ __align__(256) NoAllocScratch g_noalloc_scratch;
 // Device address of g_noalloc_scratch, per device ordinal.  In host code the
 // symbol is a host-side stand-in, not a device address, so it is looked up
 // once per device with cudaGetSymbolAddress while that device is current.
+// The address belongs to the device's current context: it is looked up again
+// when that context has changed (after cudaDeviceReset, for instance, the
+// module and its array are loaded anew).
 constexpr int NA_MAX_DEVICES = 128;
 std::mutex g_na_mutex;
 NoAllocScratch* g_na_addr[NA_MAX_DEVICES] = {};
+CUcontext g_na_ctx[NA_MAX_DEVICES] = {};
+PFN_cuCtxGetCurrent_v4000 g_ctx_current = nullptr;
+
+// The calling thread's current context (the driver's cuCtxGetCurrent, reached
+// through the runtime's entry-point query so the library needs no libcuda link).
+bool current_context(CUcontext* ctx) {
+  if (!g_ctx_current) {
+    void* fn = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &fn, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess || !fn)
+      return false;
+    g_ctx_current = reinterpret_cast<PFN_cuCtxGetCurrent_v4000>(fn);
+  }
+  return g_ctx_current(ctx) == CUDA_SUCCESS;
+}
 
 // Coefficient of the face between cells a (low) and b (high), reference
 // layout indices: the same masking as smac_set_coefficients.
@@ -136,7 +157,11 @@ extern "C" smac_status smac_apply_A_dot_noalloc(const smac_grid_desc* d, const d
   NoAllocScratch* scratch = nullptr;
   {
     std::lock_guard<std::mutex> lock(g_na_mutex);
-    if (!g_na_addr[dev]) {
+    CUcontext ctx = nullptr;
+    // cudaGetDevice does not create the context; the first runtime call that
+    // needs it does, so a missing context just means "look the address up"
+    const bool have_ctx = current_context(&ctx) && ctx != nullptr;
+    if (!g_na_addr[dev] || !have_ctx || ctx != g_na_ctx[dev]) {
       void* p = nullptr;
       e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
       if (e != cudaSuccess || !p) {
@@ -145,6 +170,8 @@ extern "C" smac_status smac_apply_A_dot_noalloc(const smac_grid_desc* d, const d
         return SMAC_CUDA_ERROR;
       }
       g_na_addr[dev] = (NoAllocScratch*)p;
+      CUcontext now = nullptr;
+      g_na_ctx[dev] = current_context(&now) ? now : nullptr;
     }
     scratch = g_na_addr[dev];
   }

@@ -248,16 +248,19 @@ def plain_case(n=64, seed=1, dt=1.0, N=None):
                 {"seed": seed})
 
 
-def vof_case(n=192, seed=3, ratio=1000.0, dt=1.0, width_cells=1.5):
-    N = (n, n, n)
-    h = (1.0 / n,) * 3
+def vof_case(n=192, seed=3, ratio=1000.0, dt=1.0, width_cells=1.5, N=None):
+    """The VoF sphere on the unit cube of n^3 cells, or of N = (nx, ny, nz)
+    cells (spacing 1/nx, 1/ny, 1/nz) when N is given."""
+    N = (n, n, n) if N is None else tuple(N)
+    h = tuple(1.0 / m for m in N)
     ct, fxt, fyt, fzt = box_types(N)
     u = uniform01(substream(seed, 11), 3)
     centre = 0.3 + 0.4 * u
     alpha = sphere_alpha(N, h, centre, 0.25, width_cells)
     rho, (fbx, fby, fbz) = face_coeffs_vof(N, alpha, 1.0, ratio, ct, fxt, fyt, fzt)
     vxs, vys, vzs = seeded_faces(N, seed, fxt, fyt, fzt)
-    return Case(f"vof{n}", N, h, dt, vxs, vys, vzs, fbx, fby, fbz, ct, fxt, fyt, fzt,
+    name = f"vof{n}" if N == (n, n, n) else "vof{}x{}x{}".format(*N)
+    return Case(name, N, h, dt, vxs, vys, vzs, fbx, fby, fbz, ct, fxt, fyt, fzt,
                 {"seed": seed, "alpha": alpha, "rho": rho, "centre": centre, "ratio": ratio})
 
 
