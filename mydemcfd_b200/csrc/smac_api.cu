@@ -109,6 +109,7 @@ struct smac_handle {
   float *r32 = nullptr, *z32 = nullptr, *z32b = nullptr, *d32 = nullptr, *d32b = nullptr, *q32 = nullptr,
         *e32 = nullptr;
   RedBuf red{};
+  long long red_blocks = 0;  // blocks a reducing launch may have (4 partials each)
   int num_sms = 148;
   bool use_tma = true;     // fused sweeps stage their tiles with the copy engine
   int tma_ctas[2] = {1, 1};  // resident CTAs per SM of the TMA sweep: [0] FP32, [1] FP64
@@ -256,7 +257,7 @@ void launch_tma_sweep(smac_handle* h, int l, const SweepMaps& maps, T* xout, con
     if (best < 0 || cost < best) { best = cost; zc = cand; }
   }
   const long long items = ncol * ((g.nz + zc - 1) / zc);
-  const int G = (int)std::max(1LL, std::min(slots, items));
+  const int G = (int)std::max(1LL, std::min(std::min(slots, items), h->red_blocks));
   k_rbgs_tma<T, MODE, DOT><<<G, Lt::NT, Lt::SMEM_BYTES, h->stream>>>(maps, g, xout, sh, c0, xc, Lc.g, Lc.cx, Lc.cy,
                                                                     Lc.cz, h->s, h->red, zc);
 }
@@ -292,7 +293,8 @@ void launch_zm_shape(smac_handle* h, int l, const T* xin, T* xout, const T* rhs,
     if (best < 0 || cost < best) { best = cost; zc = cand; }
   }
   const long long items = nty * ((g.nz + zc - 1) / zc);
-  const int G = (int)std::max(1LL, std::min(slots, items));
+  // persistent CTAs; one partial sum each in the reduction buffer
+  const int G = (int)std::max(1LL, std::min(std::min(slots, items), h->red_blocks));
   Stencil<T, T> S{(const T*)bx, (const T*)by, (const T*)bz};
   k_rbgs_zm<T, WX, TY, MODE, DOT><<<G, Z::NT, Z::SMEM, h->stream>>>(g, xin, xout, rhs, sh, S, c0, xc, Lc.g, Lc.cx,
                                                                      Lc.cy, Lc.cz, h->s, h->red, zc);
@@ -863,6 +865,7 @@ smac_status smac_create(const smac_grid_desc* desc, const smac_options* opts, vo
       maxb = std::max(maxb, (long long)gp.x * gp.y * gp.z);
     }
     if ((st = dalloc(h, &h->red.partials, maxb * 4 + 64))) return fail(st);
+    h->red_blocks = maxb;
     if ((st = dalloc(h, &h->red.ticket, 64))) return fail(st);
   }
   if ((st = dalloc(h, &h->s, 1))) return fail(st);
@@ -902,7 +905,9 @@ smac_status smac_set_options(smac_handle* h, const smac_options* opts) {
     set_err("smac_set_options: min_coarse, max_levels, bf16_coarse_cells and the GMG/Jacobi choice are fixed at creation");
     return SMAC_BAD_ARG;
   }
-  if (opts->nu1 != h->opts.nu1 || opts->nu2 != h->opts.nu2 || opts->coarse_sweeps != h->opts.coarse_sweeps) drop_graphs(h);
+  if (opts->nu1 != h->opts.nu1 || opts->nu2 != h->opts.nu2 || opts->coarse_sweeps != h->opts.coarse_sweeps ||
+      opts->sweep_kernel != h->opts.sweep_kernel)
+    drop_graphs(h);  // the captured iterations launch the old sweeps
   h->opts = *opts;
   return SMAC_OK;
 }
