@@ -97,10 +97,11 @@ typedef struct {
 } smac_options;
 
 typedef enum {
-  SMAC_SWEEP_AUTO = 0,     /* the register z-march where the grid allows it, else the TMA ring */
+  SMAC_SWEEP_AUTO = 0,     /* the z-march where the grid allows it and it measured faster, else the
+                              TMA ring */
   SMAC_SWEEP_TMA = 1,      /* tiles staged in a shared-memory ring by the Tensor Memory Accelerator */
-  SMAC_SWEEP_ZMARCH = 2,   /* whole x-rows per warp, a register z-march (x extent <= 256 cells);
-                              other grids fall back to the TMA ring */
+  SMAC_SWEEP_ZMARCH = 2,   /* whole x-rows per warp, a register z-march (x extent <= 256 cells FP64,
+                              512 FP32); other grids fall back to the TMA ring */
   SMAC_SWEEP_SHARED = 3    /* tiles staged in shared memory by plain loads */
 } smac_sweep_kernel;
 

@@ -113,7 +113,7 @@ struct smac_handle {
   int num_sms = 148;
   bool use_tma = true;     // fused sweeps stage their tiles with the copy engine
   int tma_ctas[2] = {1, 1};  // resident CTAs per SM of the TMA sweep: [0] FP32, [1] FP64
-  int zm_ctas[2][3] = {{0, 0, 0}, {0, 0, 0}};  // resident CTAs per SM of the z-march: [FP32, FP64][shape]
+  int zm_ctas[2][3] = {};  // resident CTAs per SM of the z-march: [FP32, FP64][shape]
   Scalars* s = nullptr;    // device
   Scalars* hs = nullptr;   // pinned, mapped host mirror of the device scalars
   Scalars* hs_dev = nullptr;  // the mirror's device-side address
@@ -267,19 +267,27 @@ void launch_tma_sweep(smac_handle* h, int l, const SweepMaps& maps, T* xout, con
 // warps (<= 64 NV), 6 rows; shape 2: four warps (<= 128 NV), 2 rows.
 template <class T> constexpr int zm_wx(int shape) { return shape == 0 ? 1 : shape == 1 ? 2 : 4; }
 template <class T> constexpr int zm_ty(int shape) { return shape == 0 ? 14 : shape == 1 ? 6 : 2; }
+// The narrowest shape that covers the x extent, or -1.  With `automatic`,
+// -1 also where the TMA ring measured faster: a two-row tile (four warps per
+// row) whose lanes are less than 80% busy.
 template <class T>
-int zm_shape(const smac_handle* h, const Geom& g) {
+int zm_shape(const smac_handle* h, const Geom& g, bool automatic) {
   constexpr int NV = Vec16<T>::n;
   const int pt = sizeof(T) == 8 ? 1 : 0;
-  for (int sh = 0; sh < 3; ++sh)
-    if (g.nx <= 32 * NV * zm_wx<T>(sh) && h->zm_ctas[pt][sh] > 0) return sh;
+  for (int sh = 0; sh < 3; ++sh) {
+    const int tw = 32 * NV * zm_wx<T>(sh);
+    if (g.nx <= tw && h->zm_ctas[pt][sh] > 0) {
+      if (automatic && zm_ty<T>(sh) < 6 && 5 * g.nx < 4 * tw) return -1;
+      return sh;
+    }
+  }
   return -1;
 }
 
 template <class T, int WX, int TY, int MODE, bool DOT>
 void launch_zm_shape(smac_handle* h, int l, const T* xin, T* xout, const T* rhs, const double* sh, const void* bx,
                      const void* by, const void* bz, int c0, const T* xc, int ctas) {
-  typedef ZmTile<T, WX, TY> Z;
+  constexpr int NT = ZmTile<T, WX, TY, MODE>::NT;
   const Geom& g = h->lv[l].g;
   const Level& Lc = h->lv[l + 1 < h->nlev ? l + 1 : l];
   // z-chunk: the fewest planes per CTA, counting the two extra c0 planes of each item
@@ -287,17 +295,19 @@ void launch_zm_shape(smac_handle* h, int l, const T* xin, T* xout, const T* rhs,
   const long long slots = (long long)ctas * h->num_sms;
   int zc = g.nz;
   long long best = -1;
+  // (an item costs about six steps beyond its planes: two extra c0 planes and
+  // the exposed latency of its first loads; measured at 192^3 and 256^3)
   for (int cand = std::min(64, g.nz); cand >= std::min(4, g.nz); --cand) {
     const long long items = nty * ((g.nz + cand - 1) / cand);
-    const long long cost = ((items + slots - 1) / slots) * (cand + 2);
+    const long long cost = ((items + slots - 1) / slots) * (cand + 6);
     if (best < 0 || cost < best) { best = cost; zc = cand; }
   }
   const long long items = nty * ((g.nz + zc - 1) / zc);
   // persistent CTAs; one partial sum each in the reduction buffer
   const int G = (int)std::max(1LL, std::min(std::min(slots, items), h->red_blocks));
   Stencil<T, T> S{(const T*)bx, (const T*)by, (const T*)bz};
-  k_rbgs_zm<T, WX, TY, MODE, DOT><<<G, Z::NT, Z::SMEM, h->stream>>>(g, xin, xout, rhs, sh, S, c0, xc, Lc.g, Lc.cx,
-                                                                     Lc.cy, Lc.cz, h->s, h->red, zc);
+  k_rbgs_zm<T, WX, TY, MODE, DOT><<<G, NT, ZmTile<T, WX, TY, MODE>::SMEM, h->stream>>>(
+      g, xin, xout, rhs, sh, S, c0, xc, Lc.g, Lc.cx, Lc.cy, Lc.cz, h->s, h->red, zc);
 }
 
 template <class T, int MODE, bool DOT>
@@ -309,6 +319,14 @@ void launch_zm(smac_handle* h, int l, int shape, const T* xin, T* xout, const T*
   else launch_zm_shape<T, zm_wx<T>(2), zm_ty<T>(2), MODE, DOT>(h, l, xin, xout, rhs, sh, bx, by, bz, c0, xc, n);
 }
 
+template <class T>
+void launch_zm_any(smac_handle* h, int l, int zs, int mode, bool dot, const T* xin, T* xout, const T* rhs,
+                   const double* sh, const void* bx, const void* by, const void* bz, int c0, const T* xc) {
+  if (mode == 0) { if (dot) launch_zm<T, 0, true>(h, l, zs, xin, xout, rhs, sh, bx, by, bz, c0, xc); else launch_zm<T, 0, false>(h, l, zs, xin, xout, rhs, sh, bx, by, bz, c0, xc); }
+  else if (mode == 1) { if (dot) launch_zm<T, 1, true>(h, l, zs, xin, xout, rhs, sh, bx, by, bz, c0, xc); else launch_zm<T, 1, false>(h, l, zs, xin, xout, rhs, sh, bx, by, bz, c0, xc); }
+  else { if (dot) launch_zm<T, 2, true>(h, l, zs, xin, xout, rhs, sh, bx, by, bz, c0, xc); else launch_zm<T, 2, false>(h, l, zs, xin, xout, rhs, sh, bx, by, bz, c0, xc); }
+}
+
 template <class T, class CS>
 void launch_sweep(smac_handle* h, int l, int mode, bool dot, const T* xin, T* xout, const T* rhs, const double* sh,
                   const void* bx, const void* by, const void* bz, int c0, const T* xc) {
@@ -317,11 +335,9 @@ void launch_sweep(smac_handle* h, int l, int mode, bool dot, const T* xin, T* xo
   const Level& Lc = h->lv[l + 1 < h->nlev ? l + 1 : l];
   const int sk = h->opts.sweep_kernel;
   if constexpr (std::is_same<T, CS>::value) {
-    const int zs = (sk == SMAC_SWEEP_ZMARCH) ? zm_shape<T>(h, g) : -1;
+    const int zs = (sk == SMAC_SWEEP_ZMARCH || sk == SMAC_SWEEP_AUTO) ? zm_shape<T>(h, g, sk == SMAC_SWEEP_AUTO) : -1;
     if (zs >= 0) {
-      if (mode == 0) { if (dot) launch_zm<T, 0, true>(h, l, zs, xin, xout, rhs, sh, bx, by, bz, c0, xc); else launch_zm<T, 0, false>(h, l, zs, xin, xout, rhs, sh, bx, by, bz, c0, xc); }
-      else if (mode == 1) { if (dot) launch_zm<T, 1, true>(h, l, zs, xin, xout, rhs, sh, bx, by, bz, c0, xc); else launch_zm<T, 1, false>(h, l, zs, xin, xout, rhs, sh, bx, by, bz, c0, xc); }
-      else { if (dot) launch_zm<T, 2, true>(h, l, zs, xin, xout, rhs, sh, bx, by, bz, c0, xc); else launch_zm<T, 2, false>(h, l, zs, xin, xout, rhs, sh, bx, by, bz, c0, xc); }
+      launch_zm_any<T>(h, l, zs, mode, dot, xin, xout, rhs, sh, bx, by, bz, c0, xc);
       return;
     }
     const bool ok = sizeof(T) == 8 ? L.tma64 : L.tma32;
@@ -648,17 +664,31 @@ cudaError_t tma_attr() {
                               TmaTile<T>::SMEM_BYTES);
 }
 
-// Resident CTAs per SM of each z-march shape (0: not usable).
-template <class T, int SH>
-int zm_occupancy() {
-  typedef ZmTile<T, zm_wx<T>(SH), zm_ty<T>(SH)> Z;
+// Resident CTAs per SM of each z-march shape (0: not usable): the kernels'
+// shared-memory limit raised to their needs, then the fewest resident CTAs
+// of the six forms.
+template <class T, int SH, int MODE, bool DOT>
+int zm_occupancy_one() {
+  constexpr int WX = zm_wx<T>(SH), TY = zm_ty<T>(SH);
+  constexpr int NT = ZmTile<T, WX, TY, MODE>::NT;
+  constexpr int SM = ZmTile<T, WX, TY, MODE>::SMEM;
+  auto fn = k_rbgs_zm<T, WX, TY, MODE, DOT>;
   int n = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_rbgs_zm<T, zm_wx<T>(SH), zm_ty<T>(SH), 0, true>, Z::NT,
-                                                    Z::SMEM) != cudaSuccess) {
+  if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, SM) != cudaSuccess ||
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fn, NT, SM) != cudaSuccess) {
     cudaGetLastError();
     return 0;
   }
   return n;
+}
+template <class T, int SH>
+int zm_occupancy() {
+  const int n[6] = {zm_occupancy_one<T, SH, 0, false>(), zm_occupancy_one<T, SH, 0, true>(),
+                    zm_occupancy_one<T, SH, 1, false>(), zm_occupancy_one<T, SH, 1, true>(),
+                    zm_occupancy_one<T, SH, 2, false>(), zm_occupancy_one<T, SH, 2, true>()};
+  int m = n[0];
+  for (int v : n) m = std::min(m, v);
+  return m;
 }
 void setup_zm(smac_handle* h) {
   h->zm_ctas[0][0] = zm_occupancy<float, 0>();
