@@ -211,6 +211,29 @@ def cpu_baseline(args, case, budget):
 REF_ITER_BYTES_PER_CELL = (72 + 24 + 8 + 48 + 24 + 8 + 8 * 80 + 80 + 9 + 17 + 32 + 24) * 8.0 / 7.0
 
 
+class _QuietStdout:
+    """Sends the process's C-level stdout to /dev/null for the duration (the
+    reference's driver prints its progress there), flushing the C buffers
+    before the descriptor is restored."""
+
+    def __enter__(self):
+        import ctypes
+        self._libc = ctypes.CDLL(None)
+        sys.stdout.flush()
+        self._libc.fflush(None)
+        self._saved = os.dup(1)
+        self._null = os.open(os.devnull, os.O_WRONLY)
+        os.dup2(self._null, 1)
+        return self
+
+    def __exit__(self, *exc):
+        self._libc.fflush(None)
+        os.dup2(self._saved, 1)
+        os.close(self._saved)
+        os.close(self._null)
+        return False
+
+
 def reference_gpu_baseline(case, peak):
     """The reference's own GPU projection (solve_poisson + correct_vof_velocity,
     built from its sources under oracle/_ref) on the same input, timed by CUDA
@@ -242,19 +265,20 @@ def reference_gpu_baseline(case, peak):
         return float(torch.linalg.norm(r) / torch.linalg.norm(b))
 
     tol, found = 1e-2, None
-    for _ in range(12):
-        out = REF.solve(case, solver_type=nat.PURENEUMANN_GMG_PCG, tol=tol, levels=6, do_correct=True)
-        r = rel(out["p_delta"], out["rhs"])
-        if r <= 1e-8:
-            found = (tol, out, r)
-            break
-        tol *= 0.25
-    probe.close()
-    if found is None:
-        return None
-    tol, out, r = found
-    runs = [out] + [REF.solve(case, solver_type=nat.PURENEUMANN_GMG_PCG, tol=tol, levels=6, do_correct=True)
-                    for _ in range(2)]
+    with _QuietStdout():
+        for _ in range(12):
+            out = REF.solve(case, solver_type=nat.PURENEUMANN_GMG_PCG, tol=tol, levels=6, do_correct=True)
+            r = rel(out["p_delta"], out["rhs"])
+            if r <= 1e-8:
+                found = (tol, out, r)
+                break
+            tol *= 0.25
+        probe.close()
+        if found is None:
+            return None
+        tol, out, r = found
+        runs = [out] + [REF.solve(case, solver_type=nat.PURENEUMANN_GMG_PCG, tol=tol, levels=6, do_correct=True)
+                        for _ in range(2)]
     ms = min(o["solve_ms"] + o["correct_ms"] for o in runs)
     cells = float(np.prod(case.N))
     alg = cells * (out["iterations"] * REF_ITER_BYTES_PER_CELL + 7 * 8 + 10 * 8)  # + RHS, correction

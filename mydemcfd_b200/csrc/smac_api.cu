@@ -327,8 +327,12 @@ void launch_zm_any(smac_handle* h, int l, int zs, int mode, bool dot, const T* x
   else { if (dot) launch_zm<T, 2, true>(h, l, zs, xin, xout, rhs, sh, bx, by, bz, c0, xc); else launch_zm<T, 2, false>(h, l, zs, xin, xout, rhs, sh, bx, by, bz, c0, xc); }
 }
 
+// One fused red-black sweep of grid l (mode 0 plain, 1 from zero, 2 with the
+// prolongation of the coarse correction xc added to the input).  Returns true
+// when mode 2 ran as a separate prolongation pass over xin (in place: the
+// input of that sweep is consumed) followed by the plain sweep.
 template <class T, class CS>
-void launch_sweep(smac_handle* h, int l, int mode, bool dot, const T* xin, T* xout, const T* rhs, const double* sh,
+bool launch_sweep(smac_handle* h, int l, int mode, bool dot, const T* xin, T* xout, const T* rhs, const double* sh,
                   const void* bx, const void* by, const void* bz, int c0, const T* xc) {
   const Level& L = h->lv[l];
   const Geom& g = L.g;
@@ -337,8 +341,16 @@ void launch_sweep(smac_handle* h, int l, int mode, bool dot, const T* xin, T* xo
   if constexpr (std::is_same<T, CS>::value) {
     const int zs = (sk == SMAC_SWEEP_ZMARCH || sk == SMAC_SWEEP_AUTO) ? zm_shape<T>(h, g, sk == SMAC_SWEEP_AUTO) : -1;
     if (zs >= 0) {
+      if (mode == 2) {
+        constexpr int NV = Vec16<T>::n;
+        const long long vecs = (long long)((g.nx + NV - 1) / NV) * g.ny * g.nz;
+        const int G = (int)std::max(1LL, std::min(8LL * h->num_sms, (vecs + 255) / 256));
+        k_prolong_add<T><<<G, 256, 0, h->stream>>>(g, const_cast<T*>(xin), xc, Lc.g, Lc.cx, Lc.cy, Lc.cz, h->s);
+        launch_zm_any<T>(h, l, zs, 0, dot, xin, xout, rhs, sh, bx, by, bz, c0, nullptr);
+        return true;
+      }
       launch_zm_any<T>(h, l, zs, mode, dot, xin, xout, rhs, sh, bx, by, bz, c0, xc);
-      return;
+      return false;
     }
     const bool ok = sizeof(T) == 8 ? L.tma64 : L.tma32;
     if (h->use_tma && ok && sk != SMAC_SWEEP_SHARED) {
@@ -351,7 +363,7 @@ void launch_sweep(smac_handle* h, int l, int mode, bool dot, const T* xin, T* xo
       else if (mode == 1) { if (dot) launch_tma_sweep<T, 1, true>(h, l, M, xout, sh, c0, xc); else launch_tma_sweep<T, 1, false>(h, l, M, xout, sh, c0, xc); }
       else { if (dot) launch_tma_sweep<T, 2, true>(h, l, M, xout, sh, c0, xc); else launch_tma_sweep<T, 2, false>(h, l, M, xout, sh, c0, xc); }
       (void)rhs; (void)bx; (void)by; (void)bz;
-      return;
+      return false;
     }
   }
   auto S = stencil<T, CS>(g, bx, by, bz);
@@ -364,6 +376,7 @@ void launch_sweep(smac_handle* h, int l, int mode, bool dot, const T* xin, T* xo
   else if (mode == 1) { if (dot) SW(1, true); else SW(1, false); }
   else { if (dot) SW(2, true); else SW(2, false); }
 #undef SW
+  return false;
 }
 
 // Mixed precision: the FP64 true residual and reliable update (k_reliable_vec).
@@ -464,9 +477,14 @@ smac_status launch_vcycle(smac_handle* h, T* r0, T* z0a, T* z0b, bool mixed, boo
     for (int it = 0; it < o.nu2; ++it) {
       T* out = other(l, in);
       const bool last_dot = dot && l == 0 && it == o.nu2 - 1;
-      launch_sweep<T, CS>(h, l, it == 0 ? 2 : 0, last_dot, in, out, B(l), sh, CF(l, 0), CF(l, 1), CF(l, 2), 1,
-                          it == 0 ? fin[l + 1] : nullptr);
-      account(h, g, 3.0 * s + 3 * sc + (it == 0 ? s / 8 : 0.0), 1);
+      const bool split = launch_sweep<T, CS>(h, l, it == 0 ? 2 : 0, last_dot, in, out, B(l), sh, CF(l, 0), CF(l, 1),
+                                             CF(l, 2), 1, it == 0 ? fin[l + 1] : nullptr);
+      if (split) {  // the prolongation pass (x read and written, coarse read), then the plain sweep
+        account(h, g, 2.0 * s + s / 8, 1);
+        account(h, g, 3.0 * s + 3 * sc, 1);
+      } else {
+        account(h, g, 3.0 * s + 3 * sc + (it == 0 ? s / 8 : 0.0), 1);
+      }
       in = out;
     }
     fin[l] = in;
@@ -595,7 +613,17 @@ double iteration_bytes(smac_handle* h, bool mixed, bool gmg, int* launches) {
       for (int it = 1; it < h->opts.nu1; ++it) { bytes += (3.0 * s + 3 * sc) * cells; n += 1; }
       bytes += (2 * s + 3 * sc + s / 8) * cells;
       n += 1;
-      for (int it = 0; it < h->opts.nu2; ++it) { bytes += (3.0 * s + 3 * sc + (it == 0 ? s / 8 : 0.0)) * cells; n += 1; }
+      // the first post-smoothing sweep: fused with the prolongation, or (the
+      // z-march) a prolongation pass followed by the plain sweep
+      const int sk = h->opts.sweep_kernel;
+      const bool zm_ok = sk == SMAC_SWEEP_ZMARCH || sk == SMAC_SWEEP_AUTO;
+      const bool split = zm_ok && (mixed ? zm_shape<float>(h, h->lv[l].g, sk == SMAC_SWEEP_AUTO)
+                                         : zm_shape<double>(h, h->lv[l].g, sk == SMAC_SWEEP_AUTO)) >= 0;
+      if (split) { bytes += (2.0 * s + s / 8) * cells; n += 1; }
+      for (int it = 0; it < h->opts.nu2; ++it) {
+        bytes += (3.0 * s + 3 * sc + (it == 0 && !split ? s / 8 : 0.0)) * cells;
+        n += 1;
+      }
     }
     n += 1;  // single-CTA coarse grids (their bytes are negligible)
     if (h->lc == 0) { bytes += 2 * s * (double)g.cells(); n += 1; }
@@ -1515,6 +1543,22 @@ smac_status smac_time_kernel(smac_handle* h, int kernel_id, int reps, float* ms,
       case 10: {
         launch_update<double>(h, g, h->tmp64, h->d64, h->r64, h->q64);
         per = 6 * 8.0;
+        break;
+      }
+      case 11: case 12: case 13: {  // FP32 sweep from zero / with the prolongation / with r.z
+        const int mode = kernel_id == 11 ? 1 : kernel_id == 12 ? 2 : 0;
+        launch_sweep<float, float>(h, 0, mode, kernel_id == 13, mode == 1 ? nullptr : h->z32, h->z32b, h->r32, nullptr,
+                                   h->lv[0].bxm, h->lv[0].bym, h->lv[0].bzm, mode == 2 ? 1 : 0,
+                                   mode == 2 ? h->lv[1].x32 : nullptr);
+        per = (mode == 1 ? 5 : 6) * 4.0 + (mode == 2 ? 4.0 / 8 : 0.0);
+        break;
+      }
+      case 14: case 15: case 16: {  // FP64 sweep from zero / with the prolongation / with r.z
+        const int mode = kernel_id == 14 ? 1 : kernel_id == 15 ? 2 : 0;
+        launch_sweep<double, double>(h, 0, mode, kernel_id == 16, mode == 1 ? nullptr : h->z64, h->z64b, h->r64,
+                                     nullptr, h->lv[0].bx64, h->lv[0].by64, h->lv[0].bz64, mode == 2 ? 1 : 0,
+                                     mode == 2 ? h->lv[1].x64 : nullptr);
+        per = (mode == 1 ? 5 : 6) * 8.0 + (mode == 2 ? 8.0 / 8 : 0.0);
         break;
       }
       case 4: {

@@ -38,6 +38,39 @@
 
 namespace smac {
 
+// x += P(xc) on the cells of the fine grid, in place: the prolongation of
+// the coarse-grid correction (the parent (i>>1, j>>1, k>>1) on the halved
+// directions), run ahead of the first post-smoothing sweep of the z-march,
+// which then takes its plain form.  Each cell's sum is the one the fused
+// forms compute, so the sweep's result is the same bit for bit.  (Fused into
+// the z-march, the coarse loads and sums cost 60% more than the sweep.)
+template <class T>
+__global__ void __launch_bounds__(256) k_prolong_add(Geom g, T* __restrict__ x, const T* __restrict__ xc, Geom gc,
+                                                     int cx, int cy, int cz, const Scalars* s) {
+  if (s && s->done) return;
+  typedef typename Vec16<T>::type V;
+  constexpr int NV = Vec16<T>::n;
+  const int nvr = (g.nx + NV - 1) / NV;  // vectors per row; the last one may reach into the zero pad
+  const long long total = (long long)nvr * g.ny * g.nz;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
+       t += (long long)gridDim.x * blockDim.x) {
+    const int v = (int)(t % nvr);
+    const long long r = t / nvr;
+    const int j = (int)(r % g.ny), k = (int)(r / g.ny);
+    const int ib = v * NV;
+    V* p = reinterpret_cast<V*>(x + g.idx(ib, j, k));
+    V a = *p;
+    T* pa = reinterpret_cast<T*>(&a);
+    const int jc = cy ? j >> 1 : j, kc = cz ? k >> 1 : k;
+#pragma unroll
+    for (int e = 0; e < NV; ++e) {
+      const int i = ib + e;
+      if (i < g.nx) pa[e] = (T)Ar<T>::add((T)pa[e], (T)xc[gc.idx(cx ? i >> 1 : i, jc, kc)]);
+    }
+    *p = a;
+  }
+}
+
 template <class T, int WX, int TY, int MODE>
 struct ZmTile {
   static constexpr int NV = Vec16<T>::n;          // cells per lane
@@ -59,14 +92,13 @@ template <class T>
 struct ZmOps {
   typename Vec16<T>::type rh, bx, by, byu, bzu, x1, xo;
   T bxe;
+  T c1[2];  // with the prolongation on a grid halved in every direction: the parents of x1
 };
 // Operands of the colour-(1-c0) pass on plane m, carried to the next step:
-// per cell of that colour its rhs and six weights, and the whole rhs vector
-// for the fused r.z.
+// per cell of that colour its rhs and six weights.
 template <class T, int H>
 struct ZmBlk {
   T rh[H], bxm[H], bxp[H], by[H], byu[H], bz[H], bzu[H];
-  typename Vec16<T>::type rhs_full;
 };
 
 template <class T, int WX, int TY, int MODE, bool DOT>
@@ -137,6 +169,32 @@ __global__ void __launch_bounds__(ZmTile<T, WX, TY, MODE>::NT)
       if (!ok || !col_ok) return zero();
       return *reinterpret_cast<const V*>(a + g.idx(ib, jj, m));
     };
+    // With the prolongation on a grid halved in every direction, the input
+    // vector of the lane's row is loaded as it is and its cells' parents
+    // (NV/2 coarse values) beside it; the sum is formed when the vector is
+    // used, a step later, so that no load is waited for where it is issued.
+    // (The ring rows' row beyond takes the immediate path: those warps wait
+    // at the step's barrier anyway.)
+    const bool pro4 = MODE == 2 && cx && cy && cz;
+    auto load_parents = [&](int m, int jj, bool ok, T (&c)[2]) {
+      c[0] = c[1] = (T)0;
+      if (!ok || !col_ok || m < 0 || m >= g.nz || ib >= g.nx) return;
+      const T* p = xc + gc.idx(ib >> 1, jj >> 1, m >> 1);
+      if constexpr (NV == 4) {
+        const typename Vec2<T>::type v = *reinterpret_cast<const typename Vec2<T>::type*>(p);
+        c[0] = v.x;
+        c[1] = v.y;
+      } else {
+        c[0] = p[0];
+      }
+    };
+    auto add_parents = [&](V v, const T (&c)[2]) -> V {
+      T* pv = reinterpret_cast<T*>(&v);
+#pragma unroll
+      for (int e = 0; e < NV; ++e)
+        if (ib + e < g.nx) pv[e] = (T)Ar<A>::add((A)pv[e], (A)c[e >> 1]);
+      return v;
+    };
     auto load_ops = [&](int m, Ops& o) {
       const bool ok = row_ok && m >= 0 && m < g.nz;
       o.rh = load_v(rhs, m, j, ok);
@@ -145,8 +203,15 @@ __global__ void __launch_bounds__(ZmTile<T, WX, TY, MODE>::NT)
       o.by = load_v(S.by, m, j, ok);
       o.byu = load_v(S.by, m, j + 1, ok);
       o.bzu = load_v(S.bz, m + 1, j, row_ok && m + 1 >= 0 && m + 1 <= g.nz);  // z-face m+1 (0..nz)
-      o.x1 = load_x(m + 1, j, row_ok);
-      o.xo = load_x(m, jo, jo_ok);
+      if (pro4) {
+        o.x1 = (row_ok && col_ok && m + 1 >= 0 && m + 1 < g.nz) ? *reinterpret_cast<const V*>(xin + g.idx(ib, j, m + 1))
+                                                                : zero();
+        o.xo = load_x(m, jo, jo_ok);
+        load_parents(m + 1, j, row_ok, o.c1);
+      } else {
+        o.x1 = load_x(m + 1, j, row_ok);
+        o.xo = load_x(m, jo, jo_ok);
+      }
     };
 
     // prologue: the inputs of planes kb-1 and kb, the shared plane kb, the
@@ -182,6 +247,7 @@ __global__ void __launch_bounds__(ZmTile<T, WX, TY, MODE>::NT)
       constexpr int P = decltype(Pc)::value;
       const V bz_c = nxt.bzu;  // z-faces k (the previous step's faces k-1+1), read before nxt is reloaded
       if (k + 1 <= z1) load_ops(k + 1, nxt);
+      if (pro4) cur.x1 = add_parents(cur.x1, cur.c1);  // the deferred prolongation of this step's input
       // --- the input of plane k+1 becomes visible to the rows above and below
       *reinterpret_cast<V*>(Mrow(k + 1, wr) + ib) = cur.x1;
       T xh_p[H];
@@ -221,6 +287,14 @@ __global__ void __launch_bounds__(ZmTile<T, WX, TY, MODE>::NT)
             }
           }
           red_k[q] = (T)v;
+          if constexpr (DOT) {
+            // r.z: the c0 cells of the chunk's planes (not the ring rows' nor the extra planes)
+            if (!ring && k >= z0 && k < z1 && row_ok && ib + e < g.nx) {
+              const double z = (double)red_k[q];
+              dv[0] += ((double)el(cur.rh, 2 * q + P) - shd) * z;
+              dv[1] += z;
+            }
+          }
         }
         // c0 results of plane k, H per lane side by side (0 outside the grid)
         {
@@ -243,7 +317,6 @@ __global__ void __launch_bounds__(ZmTile<T, WX, TY, MODE>::NT)
         bout.bz[q] = el(bz_c, 2 * q + Q);
         bout.bzu[q] = el(cur.bzu, 2 * q + Q);
       }
-      if constexpr (DOT) bout.rhs_full = cur.rh;
       __syncthreads();
       // --- colour 1-c0 on plane k-1 (tile rows only): cells 2q + P
       const int kk = k - 1;
@@ -283,11 +356,12 @@ __global__ void __launch_bounds__(ZmTile<T, WX, TY, MODE>::NT)
           }
           *reinterpret_cast<V*>(xout + g.idx(ib, j, kk)) = out;
           if constexpr (DOT) {
+            // r.z: the colour-(1-c0) cells of plane k-1
 #pragma unroll
-            for (int e = 0; e < NV; ++e) {
-              if (ib + e < g.nx) {
-                const double z = (double)o[e];
-                dv[0] += ((double)el(bin.rhs_full, e) - shd) * z;
+            for (int q = 0; q < H; ++q) {
+              if (ib + 2 * q + P < g.nx) {
+                const double z = (double)blk[q];
+                dv[0] += ((double)bin.rh[q] - shd) * z;
                 dv[1] += z;
               }
             }
