@@ -60,10 +60,42 @@ def _p(a, t=ctypes.c_double):
     return a.ctypes.data_as(ctypes.POINTER(t))
 
 
+SEAM_PATH = os.path.join(_HERE, "_ref", "libref_seam.so")
+_seam = None
+
+
+def seam_available() -> bool:
+    return os.path.exists(SEAM_PATH)
+
+
+def _seam_lib():
+    global _seam
+    if _seam is None:
+        if not seam_available():
+            raise ImportError(f"{SEAM_PATH} is not built (make -C oracle ref, where the reference sources exist)")
+        _seam = ctypes.CDLL(SEAM_PATH)
+        _seam.ref_solve_seam.restype = ctypes.c_int
+        _seam.ref_solve_seam.argtypes = [ctypes.POINTER(RefInputs), ctypes.POINTER(RefOutputs), ctypes.c_int]
+    return _seam
+
+
+def solve_seam(case, solver_type=3, tol=1e-11, precision=0, do_correct=True, eps=None, eps_old=None, fs=None):
+    """The reference's G_SMACSolver::solve_poisson() + correct_vof_velocity()
+    with this library's G_B200PressureSolver installed at its seam
+    (oracle/ref_seam.cu): the drop-in as a maintainer would install it.
+    tol is the reference's tol_ (max|r| dt); returns the same dict as solve."""
+    return _run(_seam_lib().ref_solve_seam, case, solver_type, tol, 4, do_correct, eps, eps_old, fs,
+                extra=(ctypes.c_int(precision),))
+
+
 def solve(case, solver_type=3, tol=1e-11, levels=4, do_correct=True, eps=None, eps_old=None, fs=None):
     """Run the reference's solve_poisson (+ correct_vof_velocity) on a
     mydemcfd_b200.workloads.Case.  eps defaults to 1 (the reference's
     standalone driver leaves it at 0, which zeroes the divergence term)."""
+    return _run(lib().ref_solve, case, solver_type, tol, levels, do_correct, eps, eps_old, fs)
+
+
+def _run(fn, case, solver_type, tol, levels, do_correct, eps, eps_old, fs, extra=()):
     N = case.N
     nx, ny, nz = N
     cell = (nz + 2, ny + 2, nx + 2)
@@ -95,9 +127,9 @@ def solve(case, solver_type=3, tol=1e-11, levels=4, do_correct=True, eps=None, e
     o = RefOutputs()
     for k in ("p_delta", "rhs", "p", "vx", "vy", "vz"):
         setattr(o, k, _p(out[k]))
-    rc = lib().ref_solve(ctypes.byref(i), ctypes.byref(o))
+    rc = fn(ctypes.byref(i), ctypes.byref(o), *extra)
     if rc != 0:
-        raise RuntimeError(f"ref_solve returned {rc}")
+        raise RuntimeError(f"{fn.__name__} returned {rc} (iterations field {o.iterations})")
     out["iterations"] = o.iterations
     out["num_levels"] = o.num_levels
     out["solve_ms"] = o.solve_ms
