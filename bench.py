@@ -57,6 +57,9 @@ def parse():
                     help="set up the workload and launch one of the calls around the projection --reps times "
                          "(for ncu captures)")
     ap.add_argument("--reps", type=int, default=3)
+    ap.add_argument("--breakdown", action="store_true",
+                    help="two warm-up and three timed projections per precision (mixed, FP64) of the workload, "
+                         "event-timed: a small, fixed launch list for ncu")
     ap.add_argument("--sweep-kernel", type=int, default=0,
                     help="smac_sweep_kernel of the solvers: 0 auto, 1 TMA ring, 2 z-march, 3 shared tiles")
     return ap.parse_args()
@@ -664,8 +667,40 @@ def run_kernel_only(args):
     s.close()
 
 
+def run_breakdown(args):
+    import torch
+
+    from mydemcfd_b200 import _native as nat
+    from mydemcfd_b200 import workloads as W
+    from mydemcfd_b200.solver import B200PressureSolver, DeviceGrid, ibm_solid_fraction_device
+    case = build_case(args, solid_fraction=lambda N, h, o, s: ibm_solid_fraction_device(N, h, o, s).cpu().numpy())
+    g = DeviceGrid.from_case(case)
+    sh = W.shapes(case.N)
+    ov = [torch.zeros(sh[k], dtype=torch.float64, device="cuda") for k in "xyz"]
+    pd = torch.zeros(sh["cell"], dtype=torch.float64, device="cuda")
+    for prec in (nat.PRECISION_MIXED, nat.PRECISION_FP64):
+        s = B200PressureSolver(case.N, case.h, precision=prec, tol=args.tol, sweep_kernel=args.sweep_kernel)
+        s.set_coefficients(g)
+        for _ in range(2):
+            s.project(g.f_vx_star_, g.f_vy_star_, g.f_vz_star_, case.dt, pd, *ov)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(3):
+            st = s.project(g.f_vx_star_, g.f_vy_star_, g.f_vz_star_, case.dt, pd, *ov)
+        e1.record()
+        torch.cuda.synchronize()
+        print(json.dumps({"precision": "mixed" if prec == nat.PRECISION_MIXED else "fp64",
+                          "ms_per_projection": e0.elapsed_time(e1) / 3, "launches": st["kernel_launches"],
+                          "iterations": st["iterations"]}), flush=True)
+        s.close()
+
+
 def main():
     args = parse()
+    if args.breakdown:
+        run_breakdown(args)
+        return
     if args.kernel_only is not None:
         run_kernel_only(args)
         return

@@ -113,7 +113,7 @@ struct smac_handle {
   int num_sms = 148;
   bool use_tma = true;     // fused sweeps stage their tiles with the copy engine
   int tma_ctas[2] = {1, 1};  // resident CTAs per SM of the TMA sweep: [0] FP32, [1] FP64
-  int zm_ctas[2][3] = {};  // resident CTAs per SM of the z-march: [FP32, FP64][shape]
+  int zm_ctas[2][4] = {};  // resident CTAs per SM of the z-march: [FP32, FP64][shape]
   Scalars* s = nullptr;    // device
   Scalars* hs = nullptr;   // pinned, mapped host mirror of the device scalars
   Scalars* hs_dev = nullptr;  // the mirror's device-side address
@@ -263,19 +263,31 @@ void launch_tma_sweep(smac_handle* h, int l, const SweepMaps& maps, T* xout, con
 }
 
 // z-march shapes: the whole x extent in WX warps of 32 x NV cells, TY tile
-// rows.  Shape 0: one warp per row (x extent <= 32 NV), 14 rows; shape 1: two
-// warps (<= 64 NV), 6 rows; shape 2: four warps (<= 128 NV), 2 rows.
+// rows.  FP64 (NV = 2): shape 0 one warp per row (x extent <= 64), 14 rows;
+// shape 1 two warps (<= 128), 6 rows; shape 2 four warps (<= 256), 2 rows.
+// FP32: shapes 0-2 the same with NV = 4 (extents 128, 256, 512), shape 3
+// four warps of float2 lanes (<= 256), 6 rows, 1024 threads.
+template <class T> constexpr int zm_nv(int shape) { return sizeof(T) == 8 ? 2 : shape == 3 ? 2 : 4; }
 template <class T> constexpr int zm_wx(int shape) { return shape == 0 ? 1 : shape == 1 ? 2 : 4; }
-template <class T> constexpr int zm_ty(int shape) { return shape == 0 ? 14 : shape == 1 ? 6 : 2; }
+template <class T> constexpr int zm_ty(int shape) { return shape == 0 ? 14 : shape == 2 ? 2 : 6; }
+constexpr int ZM_SHAPES = 4;
+#ifdef SMAC_ZM_F32_NARROW
+#define SMAC_ZM_F32_ORDER 0, 3, 1, 2
+#else
+#define SMAC_ZM_F32_ORDER 0, 1, 2, 3
+#endif
 // The narrowest shape that covers the x extent, or -1.  With `automatic`,
 // -1 also where the TMA ring measured faster: a two-row tile (four warps per
 // row) whose lanes are less than 80% busy.
 template <class T>
 int zm_shape(const smac_handle* h, const Geom& g, bool automatic) {
-  constexpr int NV = Vec16<T>::n;
   const int pt = sizeof(T) == 8 ? 1 : 0;
-  for (int sh = 0; sh < 3; ++sh) {
-    const int tw = 32 * NV * zm_wx<T>(sh);
+  const int order32[ZM_SHAPES] = {SMAC_ZM_F32_ORDER};
+  const int order64[ZM_SHAPES] = {0, 1, 2, -1};
+  for (int q = 0; q < ZM_SHAPES; ++q) {
+    const int sh = sizeof(T) == 8 ? order64[q] : order32[q];
+    if (sh < 0) continue;
+    const int tw = 32 * zm_nv<T>(sh) * zm_wx<T>(sh);
     if (g.nx <= tw && h->zm_ctas[pt][sh] > 0) {
       if (automatic && zm_ty<T>(sh) < 6 && 5 * g.nx < 4 * tw) return -1;
       return sh;
@@ -284,10 +296,10 @@ int zm_shape(const smac_handle* h, const Geom& g, bool automatic) {
   return -1;
 }
 
-template <class T, int WX, int TY, int MODE, bool DOT>
+template <class T, int NV, int WX, int TY, int MODE, bool DOT>
 void launch_zm_shape(smac_handle* h, int l, const T* xin, T* xout, const T* rhs, const double* sh, const void* bx,
                      const void* by, const void* bz, int c0, const T* xc, int ctas) {
-  constexpr int NT = ZmTile<T, WX, TY, MODE>::NT;
+  constexpr int NT = ZmTile<T, NV, WX, TY, MODE>::NT;
   const Geom& g = h->lv[l].g;
   const Level& Lc = h->lv[l + 1 < h->nlev ? l + 1 : l];
   // z-chunk: the fewest planes per CTA, counting the two extra c0 planes of each item
@@ -306,7 +318,7 @@ void launch_zm_shape(smac_handle* h, int l, const T* xin, T* xout, const T* rhs,
   // persistent CTAs; one partial sum each in the reduction buffer
   const int G = (int)std::max(1LL, std::min(std::min(slots, items), h->red_blocks));
   Stencil<T, T> S{(const T*)bx, (const T*)by, (const T*)bz};
-  k_rbgs_zm<T, WX, TY, MODE, DOT><<<G, NT, ZmTile<T, WX, TY, MODE>::SMEM, h->stream>>>(
+  k_rbgs_zm<T, NV, WX, TY, MODE, DOT><<<G, NT, ZmTile<T, NV, WX, TY, MODE>::SMEM, h->stream>>>(
       g, xin, xout, rhs, sh, S, c0, xc, Lc.g, Lc.cx, Lc.cy, Lc.cz, h->s, h->red, zc);
 }
 
@@ -314,9 +326,12 @@ template <class T, int MODE, bool DOT>
 void launch_zm(smac_handle* h, int l, int shape, const T* xin, T* xout, const T* rhs, const double* sh,
                const void* bx, const void* by, const void* bz, int c0, const T* xc) {
   const int n = h->zm_ctas[sizeof(T) == 8 ? 1 : 0][shape];
-  if (shape == 0) launch_zm_shape<T, zm_wx<T>(0), zm_ty<T>(0), MODE, DOT>(h, l, xin, xout, rhs, sh, bx, by, bz, c0, xc, n);
-  else if (shape == 1) launch_zm_shape<T, zm_wx<T>(1), zm_ty<T>(1), MODE, DOT>(h, l, xin, xout, rhs, sh, bx, by, bz, c0, xc, n);
-  else launch_zm_shape<T, zm_wx<T>(2), zm_ty<T>(2), MODE, DOT>(h, l, xin, xout, rhs, sh, bx, by, bz, c0, xc, n);
+#define ZM_SHAPE(S) launch_zm_shape<T, zm_nv<T>(S), zm_wx<T>(S), zm_ty<T>(S), MODE, DOT>(h, l, xin, xout, rhs, sh, bx, by, bz, c0, xc, n)
+  if (shape == 0) ZM_SHAPE(0);
+  else if (shape == 1) ZM_SHAPE(1);
+  else if (shape == 2) ZM_SHAPE(2);
+  else if constexpr (sizeof(T) == 4) ZM_SHAPE(3);
+#undef ZM_SHAPE
 }
 
 template <class T>
@@ -697,10 +712,10 @@ cudaError_t tma_attr() {
 // of the six forms.
 template <class T, int SH, int MODE, bool DOT>
 int zm_occupancy_one() {
-  constexpr int WX = zm_wx<T>(SH), TY = zm_ty<T>(SH);
-  constexpr int NT = ZmTile<T, WX, TY, MODE>::NT;
-  constexpr int SM = ZmTile<T, WX, TY, MODE>::SMEM;
-  auto fn = k_rbgs_zm<T, WX, TY, MODE, DOT>;
+  constexpr int NV = zm_nv<T>(SH), WX = zm_wx<T>(SH), TY = zm_ty<T>(SH);
+  constexpr int NT = ZmTile<T, NV, WX, TY, MODE>::NT;
+  constexpr int SM = ZmTile<T, NV, WX, TY, MODE>::SMEM;
+  auto fn = k_rbgs_zm<T, NV, WX, TY, MODE, DOT>;
   int n = 0;
   if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, SM) != cudaSuccess ||
       cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fn, NT, SM) != cudaSuccess) {
@@ -722,9 +737,11 @@ void setup_zm(smac_handle* h) {
   h->zm_ctas[0][0] = zm_occupancy<float, 0>();
   h->zm_ctas[0][1] = zm_occupancy<float, 1>();
   h->zm_ctas[0][2] = zm_occupancy<float, 2>();
+  h->zm_ctas[0][3] = zm_occupancy<float, 3>();
   h->zm_ctas[1][0] = zm_occupancy<double, 0>();
   h->zm_ctas[1][1] = zm_occupancy<double, 1>();
   h->zm_ctas[1][2] = zm_occupancy<double, 2>();
+  h->zm_ctas[1][3] = 0;
 }
 
 // Tensor maps for every separately launched grid, or use_tma = false.

@@ -5,8 +5,8 @@
 // half-sweep kernels (k_rbgs): xout = S(xin), colour c0 from xin, then colour
 // 1-c0 from the new c0 values.  The data movement is different:
 //
-//   - a warp owns 32 x NV consecutive cells of one row (NV = 4 FP32, 2 FP64,
-//     one 16-byte vector per lane and array), WX warps side by side cover the
+//   - a warp owns 32 x NV consecutive cells of one row (NV = 4 or 2 FP32, 2
+//     FP64: one 16- or 8-byte vector per lane and array), WX warps side by side cover the
 //     whole x extent, so the tile needs no ring in x;
 //   - a CTA stacks TY rows of such warps plus one ring row above and below
 //     (j0-1 and j0+TY), which compute colour c0 only: their values are the
@@ -71,9 +71,15 @@ __global__ void __launch_bounds__(256) k_prolong_add(Geom g, T* __restrict__ x, 
   }
 }
 
-template <class T, int WX, int TY, int MODE>
+// NV consecutive cells of one row as one register vector (8 or 16 bytes)
+template <class T, int N> struct VecN;
+template <> struct VecN<float, 2> { typedef float2 type; };
+template <> struct VecN<float, 4> { typedef float4 type; };
+template <> struct VecN<double, 2> { typedef double2 type; };
+
+template <class T, int NV_, int WX, int TY, int MODE>
 struct ZmTile {
-  static constexpr int NV = Vec16<T>::n;          // cells per lane
+  static constexpr int NV = NV_;                  // cells per lane
   static constexpr int H = NV / 2;                // cells of one colour per lane and plane
   static constexpr int TW = 32 * NV * WX;         // cells per row: the whole x extent
   static constexpr int ROWS = TY + 2;             // tile rows plus the two ring rows
@@ -88,9 +94,9 @@ struct ZmTile {
 // the x-faces (and the one past the lane's vector), the y-faces of rows j and
 // j+1, the z-faces m+1, the input of plane m+1 and, for the ring rows, the
 // input of the row beyond on plane m.
-template <class T>
+template <class T, int NV>
 struct ZmOps {
-  typename Vec16<T>::type rh, bx, by, byu, bzu, x1, xo;
+  typename VecN<T, NV>::type rh, bx, by, byu, bzu, x1, xo;
   T bxe;
   T c1[2];  // with the prolongation on a grid halved in every direction: the parents of x1
 };
@@ -101,15 +107,15 @@ struct ZmBlk {
   T rh[H], bxm[H], bxp[H], by[H], byu[H], bz[H], bzu[H];
 };
 
-template <class T, int WX, int TY, int MODE, bool DOT>
-__global__ void __launch_bounds__(ZmTile<T, WX, TY, MODE>::NT)
+template <class T, int NV_, int WX, int TY, int MODE, bool DOT>
+__global__ void __launch_bounds__(ZmTile<T, NV_, WX, TY, MODE>::NT)
     k_rbgs_zm(Geom g, const T* __restrict__ xin, T* __restrict__ xout, const T* __restrict__ rhs, const double* shift,
               Stencil<T, T> S, int c0, const T* __restrict__ xc, Geom gc, int cx, int cy, int cz, Scalars* s,
               RedBuf red, int zchunk) {
-  typedef ZmTile<T, WX, TY, MODE> L;
-  typedef typename Vec16<T>::type V;
+  typedef ZmTile<T, NV_, WX, TY, MODE> L;
+  typedef typename VecN<T, NV_>::type V;
   typedef T A;
-  typedef ZmOps<T> Ops;
+  typedef ZmOps<T, NV_> Ops;
   constexpr int NV = L::NV, H = L::H, TW = L::TW, ROWS = L::ROWS, NT = L::NT;
   typedef ZmBlk<T, H> Blk;
   extern __shared__ __align__(16) unsigned char zm_smem[];
