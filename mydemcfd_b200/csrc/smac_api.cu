@@ -68,6 +68,29 @@ namespace {
     if (st_ != SMAC_OK) return st_;     \
   } while (0)
 
+// Launch of an iteration kernel (one that starts with pdl_enter()) with
+// programmatic stream serialisation: its CTAs may be scheduled while the
+// previous kernel drains, and wait on the device for that kernel's writes.
+// SMAC_PDL=0 builds the plain stream order.  A launch error is left for
+// CKL() to report.
+#ifndef SMAC_PDL
+#define SMAC_PDL 1
+#endif
+template <class... KArgs, class... Args>
+void launch_pdl(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t stream, Args&&... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = SMAC_PDL;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  (void)cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
+}
+
 constexpr int MAXL = 16;
 constexpr int COARSE_CELLS = 4096;  // grids at or below this size run in the single-CTA kernel
 
@@ -258,8 +281,8 @@ void launch_tma_sweep(smac_handle* h, int l, const SweepMaps& maps, T* xout, con
   }
   const long long items = ncol * ((g.nz + zc - 1) / zc);
   const int G = (int)std::max(1LL, std::min(std::min(slots, items), h->red_blocks));
-  k_rbgs_tma<T, MODE, DOT><<<G, Lt::NT, Lt::SMEM_BYTES, h->stream>>>(maps, g, xout, sh, c0, xc, Lc.g, Lc.cx, Lc.cy,
-                                                                    Lc.cz, h->s, h->red, zc);
+  launch_pdl(k_rbgs_tma<T, MODE, DOT>, G, Lt::NT, Lt::SMEM_BYTES, h->stream, maps, g, xout, sh, c0, xc, Lc.g, Lc.cx,
+      Lc.cy, Lc.cz, h->s, h->red, zc);
 }
 
 // z-march shapes: the whole x extent in WX warps of 32 x NV cells, TY tile
@@ -318,8 +341,8 @@ void launch_zm_shape(smac_handle* h, int l, const T* xin, T* xout, const T* rhs,
   // persistent CTAs; one partial sum each in the reduction buffer
   const int G = (int)std::max(1LL, std::min(std::min(slots, items), h->red_blocks));
   Stencil<T, T> S{(const T*)bx, (const T*)by, (const T*)bz};
-  k_rbgs_zm<T, NV, WX, TY, MODE, DOT><<<G, NT, ZmTile<T, NV, WX, TY, MODE>::SMEM, h->stream>>>(
-      g, xin, xout, rhs, sh, S, c0, xc, Lc.g, Lc.cx, Lc.cy, Lc.cz, h->s, h->red, zc);
+  launch_pdl(k_rbgs_zm<T, NV, WX, TY, MODE, DOT>, G, NT, ZmTile<T, NV, WX, TY, MODE>::SMEM, h->stream, g, xin, xout,
+      rhs, sh, S, c0, xc, Lc.g, Lc.cx, Lc.cy, Lc.cz, h->s, h->red, zc);
 }
 
 template <class T, int MODE, bool DOT>
@@ -360,7 +383,8 @@ bool launch_sweep(smac_handle* h, int l, int mode, bool dot, const T* xin, T* xo
         constexpr int NV = Vec16<T>::n;
         const long long vecs = (long long)((g.nx + NV - 1) / NV) * g.ny * g.nz;
         const int G = (int)std::max(1LL, std::min(8LL * h->num_sms, (vecs + 255) / 256));
-        k_prolong_add<T><<<G, 256, 0, h->stream>>>(g, const_cast<T*>(xin), xc, Lc.g, Lc.cx, Lc.cy, Lc.cz, h->s);
+        launch_pdl(k_prolong_add<T>, G, 256, 0, h->stream, g, const_cast<T*>(xin), xc, Lc.g, Lc.cx, Lc.cy, Lc.cz,
+            h->s);
         launch_zm_any<T>(h, l, zs, 0, dot, xin, xout, rhs, sh, bx, by, bz, c0, nullptr);
         return true;
       }
@@ -385,8 +409,9 @@ bool launch_sweep(smac_handle* h, int l, int mode, bool dot, const T* xin, T* xo
   const int zc = sweep_zchunk<T>(g);
   const dim3 gr = grid_sweep<T>(g, zc);
   const dim3 bl(RB_NT, 1, 1);
-#define SW(M, D) k_rbgs_sweep<T, CS, M, D><<<gr, bl, 0, h->stream>>>(g, xin, xout, rhs, sh, S, c0, xc, Lc.g, Lc.cx, \
-                                                                      Lc.cy, Lc.cz, h->s, h->red, zc)
+#define SW(M, D)                                                                                           \
+  launch_pdl(k_rbgs_sweep<T, CS, M, D>, gr, bl, 0, h->stream, g, xin, xout, rhs, sh, S, c0, xc, Lc.g, Lc.cx, Lc.cy, \
+             Lc.cz, h->s, h->red, zc)
   if (mode == 0) { if (dot) SW(0, true); else SW(0, false); }
   else if (mode == 1) { if (dot) SW(1, true); else SW(1, false); }
   else { if (dot) SW(2, true); else SW(2, false); }
@@ -397,8 +422,8 @@ bool launch_sweep(smac_handle* h, int l, int mode, bool dot, const T* xin, T* xo
 // Mixed precision: the FP64 true residual and reliable update (k_reliable_vec).
 void launch_reliable(smac_handle* h, const Geom& g, const Stencil<double, double>& S64, int kz) {
   const dim3 gr((g.nx + 2 * REL_TX - 1) / (2 * REL_TX), (g.ny + REL_TY - 1) / REL_TY, (g.nz + kz - 1) / kz);
-  k_reliable_vec<float><<<gr, dim3(REL_TX, REL_TY, 1), 0, h->stream>>>(g, h->x64a, h->x64b, h->e32, h->b64, S64,
-                                                                       h->r32, h->red, h->s, kz);
+  launch_pdl(k_reliable_vec<float>, gr, dim3(REL_TX, REL_TY, 1), 0, h->stream, g, h->x64a, h->x64b, h->e32, h->b64, S64,
+      h->r32, h->red, h->s, kz);
 }
 
 // d = z - zshift + beta d, q = A d, p.Ap (k_dir_matvec_vec).
@@ -407,8 +432,8 @@ void launch_dir_matvec(smac_handle* h, const Geom& g, const T* z, const T* dold,
                        T* q, int kz) {
   constexpr int NV = Vec16<T>::n;
   const dim3 gr((g.nx + DMV_TX * NV - 1) / (DMV_TX * NV), (g.ny + DMV_TY - 1) / DMV_TY, (g.nz + kz - 1) / kz);
-  k_dir_matvec_vec<T><<<gr, dim3(DMV_TX, DMV_TY, 1), 0, h->stream>>>(g, z, dold, dnew, S, q, h->fluid, h->red, h->s,
-                                                                     kz);
+  launch_pdl(k_dir_matvec_vec<T>, gr, dim3(DMV_TX, DMV_TY, 1), 0, h->stream, g, z, dold, dnew, S, q, h->fluid, h->red,
+      h->s, kz);
 }
 
 // x += alpha d, r -= alpha q over whole padded arrays (k_update_flat).
@@ -417,8 +442,8 @@ void launch_update(smac_handle* h, const Geom& g, T* x, const T* d, T* r, const 
   const long long nvec = g.alloc / Vec16<T>::n;
   const long long blocks = (nvec + UPD_NT - 1) / UPD_NT;
   const int G = (int)std::max(1LL, std::min(4LL * h->num_sms, blocks));
-  k_update_flat<T><<<G, UPD_NT, 0, h->stream>>>(base_of(g, x), base_of(g, d), base_of(g, r), base_of(g, q), g.alloc,
-                                                h->red, h->s);
+  launch_pdl(k_update_flat<T>, G, UPD_NT, 0, h->stream, base_of(g, x), base_of(g, d), base_of(g, r), base_of(g, q),
+      g.alloc, h->red, h->s);
 }
 
 template <class T, class CS, class CC>
@@ -458,11 +483,11 @@ smac_status launch_vcycle(smac_handle* h, T* r0, T* z0a, T* z0b, bool mixed, boo
     const Level& Lc = h->lv[l + 1];
     auto S = stencil<T, CS>(g, CF(l, 0), CF(l, 1), CF(l, 2));
     if (std::is_same<T, CS>::value && Lc.cx && Lc.cy && Lc.cz)
-      k_resid_restrict2<T><<<grid_planes(Lc.g.nx, Lc.g.ny, Lc.g.nz), kBlock, 0, h->stream>>>(
-          g, cur[l], B(l), sh, stencil<T, T>(g, CF(l, 0), CF(l, 1), CF(l, 2)), Lc.g, B(l + 1), h->s);
+      launch_pdl(k_resid_restrict2<T>, grid_planes(Lc.g.nx, Lc.g.ny, Lc.g.nz), kBlock, 0, h->stream, g, cur[l], B(l),
+          sh, stencil<T, T>(g, CF(l, 0), CF(l, 1), CF(l, 2)), Lc.g, B(l + 1), h->s);
     else
-      k_resid_restrict<T, CS><<<grid_planes(Lc.g.nx, Lc.g.ny, Lc.g.nz), kBlock, 0, h->stream>>>(
-          g, cur[l], B(l), sh, S, Lc.g, Lc.cx, Lc.cy, Lc.cz, B(l + 1), h->s);
+      launch_pdl(k_resid_restrict<T, CS>, grid_planes(Lc.g.nx, Lc.g.ny, Lc.g.nz), kBlock, 0, h->stream, g, cur[l], B(l),
+          sh, S, Lc.g, Lc.cx, Lc.cy, Lc.cz, B(l + 1), h->s);
     account(h, g, 2 * s + 3 * sc + s / 8, 1);
     CKL();
   }
@@ -479,8 +504,8 @@ smac_status launch_vcycle(smac_handle* h, T* r0, T* z0a, T* z0b, bool mixed, boo
       C.x = XA(l);
       C.rhs = B(l);
     }
-    k_coarse_vcycle<T, CC><<<1, 1024, 0, h->stream>>>(set, o.nu1, o.nu2, o.coarse_sweeps, lc == 0 ? shift0 : nullptr,
-                                                       h->s);
+    launch_pdl(k_coarse_vcycle<T, CC>, 1, 1024, 0, h->stream, set, o.nu1, o.nu2, o.coarse_sweeps,
+        lc == 0 ? shift0 : nullptr, h->s);
     h->launches += 1;
     CKL();
     fin[lc] = XA(lc);
@@ -524,11 +549,12 @@ smac_status launch_iteration(smac_handle* h, bool mixed, bool gmg, int parity) {
       TRY((launch_vcycle<double, double, double>(h, h->r64, h->z64, h->z64b, false, fused_dot, &z)));
     } else {
       auto S = stencil<double, double>(g, h->lv[0].bx64, h->lv[0].by64, h->lv[0].bz64);
-      k_jacobi_precond<double, double><<<gr, kBlock, 0, h->stream>>>(g, h->r64, &h->s->rshift, S, h->z64, h->s, kz);
+      launch_pdl(k_jacobi_precond<double, double>, gr, kBlock, 0, h->stream, g, h->r64, &h->s->rshift, S, h->z64, h->s,
+          kz);
       account(h, g, 2 * 8 + 3 * 8);
     }
     if (!fused_dot) {
-      k_dot_rz<double><<<gr, kBlock, 0, h->stream>>>(g, h->r64, z, h->red, h->s, kz);
+      launch_pdl(k_dot_rz<double>, gr, kBlock, 0, h->stream, g, h->r64, z, h->red, h->s, kz);
       account(h, g, 16, 1);
     }
     double* dold = parity ? h->d64b : h->d64;
@@ -550,11 +576,12 @@ smac_status launch_iteration(smac_handle* h, bool mixed, bool gmg, int parity) {
       }
     } else {
       auto S = stencil<float, float>(g, h->lv[0].bxm, h->lv[0].bym, h->lv[0].bzm);
-      k_jacobi_precond<float, float><<<gr, kBlock, 0, h->stream>>>(g, h->r32, &h->s->rshift, S, h->z32, h->s, kz);
+      launch_pdl(k_jacobi_precond<float, float>, gr, kBlock, 0, h->stream, g, h->r32, &h->s->rshift, S, h->z32, h->s,
+          kz);
       account(h, g, 2 * 4 + 3 * 4);
     }
     if (!fused_dot) {
-      k_dot_rz<float><<<gr, kBlock, 0, h->stream>>>(g, h->r32, z, h->red, h->s, kz);
+      launch_pdl(k_dot_rz<float>, gr, kBlock, 0, h->stream, g, h->r32, z, h->red, h->s, kz);
       account(h, g, 8, 1);
     }
     float* dold = parity ? h->d32b : h->d32;
@@ -1235,8 +1262,8 @@ smac_status run_solve(smac_handle* h, const double** xout) {
           launch_reliable(h, g, S, kz);
           CKL();
         } else {
-          k_true_residual<<<grid_cells(g, kz), kBlock, 0, h->stream>>>(g, h->x64a, h->b64, S, h->r64, 1, h->red,
-                                                                        h->s, kz);
+          launch_pdl(k_true_residual, grid_cells(g, kz), kBlock, 0, h->stream, g, h->x64a, h->b64, S, h->r64, 1, h->red,
+              h->s, kz);
           CKL();
         }
         account(h, g, 6 * 8, 1);
@@ -1267,7 +1294,8 @@ smac_status run_solve(smac_handle* h, const double** xout) {
       if (!mixed && h->hs->status == 0) {
         // verify the recursive residual with the FP64 true residual
         auto S = stencil<double, double>(g, h->lv[0].bx64, h->lv[0].by64, h->lv[0].bz64);
-        k_true_residual<<<grid_cells(g, kz), kBlock, 0, h->stream>>>(g, h->x64a, h->b64, S, h->r64, 0, h->red, h->s, kz);
+        launch_pdl(k_true_residual, grid_cells(g, kz), kBlock, 0, h->stream, g, h->x64a, h->b64, S, h->r64, 0, h->red,
+            h->s, kz);
         CKL();
         account(h, g, 5 * 8, 1);
         TRY(scalars_to_host(h));
@@ -1277,8 +1305,8 @@ smac_status run_solve(smac_handle* h, const double** xout) {
         if (!ok && hs.iter < o.max_iter && restarts < 3) {
           // restart PCG from the true residual
           ++restarts;
-          k_true_residual<<<grid_cells(g, kz), kBlock, 0, h->stream>>>(g, h->x64a, h->b64, S, h->r64, 1, h->red, h->s,
-                                                                        kz);
+          launch_pdl(k_true_residual, grid_cells(g, kz), kBlock, 0, h->stream, g, h->x64a, h->b64, S, h->r64, 1, h->red,
+              h->s, kz);
           CKL();
           account(h, g, 6 * 8, 1);
           TRY(zero_async(h, base_of(g, h->d64), bytes));
@@ -1313,7 +1341,8 @@ smac_status run_solve(smac_handle* h, const double** xout) {
     // (a converged solve has just computed it: the FP64 check of the plain
     // form, the last reliable update of the mixed form)
     auto S = stencil<double, double>(g, h->lv[0].bx64, h->lv[0].by64, h->lv[0].bz64);
-    k_true_residual<<<grid_cells(g, kz), kBlock, 0, h->stream>>>(g, *xout, h->b64, S, h->r64, 0, h->red, h->s, kz);
+    launch_pdl(k_true_residual, grid_cells(g, kz), kBlock, 0, h->stream, g, *xout, h->b64, S, h->r64, 0, h->red, h->s,
+        kz);
     CKL();
     account(h, g, 5 * 8, 1);
     TRY(scalars_to_host(h));
@@ -1504,13 +1533,15 @@ smac_status smac_time_kernel(smac_handle* h, int kernel_id, int reps, float* ms,
     switch (kernel_id) {
       case 0: {
         auto S = stencil<double, double>(g, h->lv[0].bx64, h->lv[0].by64, h->lv[0].bz64);
-        k_matvec_pap<double, double><<<grid_cells(g, kz), kBlock, 0, h->stream>>>(g, h->d64, S, h->q64, h->red, h->s, kz);
+        launch_pdl(k_matvec_pap<double, double>, grid_cells(g, kz), kBlock, 0, h->stream, g, h->d64, S, h->q64, h->red,
+            h->s, kz);
         per = 5 * 8.0;
         break;
       }
       case 1: {
         auto S = stencil<float, float>(g, h->lv[0].bxm, h->lv[0].bym, h->lv[0].bzm);
-        k_matvec_pap<float, float><<<grid_cells(g, kz), kBlock, 0, h->stream>>>(g, h->d32, S, h->q32, h->red, h->s, kz);
+        launch_pdl(k_matvec_pap<float, float>, grid_cells(g, kz), kBlock, 0, h->stream, g, h->d32, S, h->q32, h->red,
+            h->s, kz);
         per = 5 * 4.0;
         break;
       }
@@ -1580,7 +1611,8 @@ smac_status smac_time_kernel(smac_handle* h, int kernel_id, int reps, float* ms,
       }
       case 4: {
         auto S = stencil<double, double>(g, h->lv[0].bx64, h->lv[0].by64, h->lv[0].bz64);
-        k_true_residual<<<grid_cells(g, kz), kBlock, 0, h->stream>>>(g, h->x64a, h->b64, S, h->r64, 0, h->red, h->s, kz);
+        launch_pdl(k_true_residual, grid_cells(g, kz), kBlock, 0, h->stream, g, h->x64a, h->b64, S, h->r64, 0, h->red,
+            h->s, kz);
         per = 5 * 8.0;
         break;
       }

@@ -108,6 +108,19 @@ struct Scalars {
 };
 
 // ---------------------------------------------------------------------------
+// Programmatic dependent launch.  The iteration's kernels are launched with
+// cudaLaunchAttributeProgrammaticStreamSerialization, so the next kernel's
+// CTAs may become resident while this one drains.  Every such kernel calls
+// pdl_enter() before its first global access: griddepcontrol.wait blocks
+// until the preceding grid has completed and its writes are visible, so the
+// ordering is that of a plain stream; launch_dependents then lets the next
+// grid be scheduled as soon as every CTA of this one has started.
+__device__ __forceinline__ void pdl_enter() {
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
+// ---------------------------------------------------------------------------
 // Deterministic grid reduction: every block reduces NV doubles in a fixed
 // tree, writes them to partials[block*NV + v], and the last block to arrive
 // (atomic ticket) sums the partials in a fixed order.  The result does not

@@ -314,6 +314,7 @@ __global__ void __launch_bounds__(TNT) k_setup_project(Geom g, double* b, const 
 template <class T, class C>
 __global__ void __launch_bounds__(TNT) k_matvec_pap(Geom g, const T* __restrict__ d, Stencil<T, C> S, T* q,
                                                     RedBuf red, Scalars* s, int kz) {
+  pdl_enter();
   if (s->done) return;
   typedef acc_t<T> A;
   const int i = blockIdx.x * TBX + threadIdx.x;
@@ -396,6 +397,7 @@ template <class T>
 __global__ void __launch_bounds__(UPD_NT) k_update_flat(T* x, const T* __restrict__ d, T* r,
                                                         const T* __restrict__ q, long long n, RedBuf red,
                                                         Scalars* s) {
+  pdl_enter();
   if (s->done) return;
   typedef typename Vec16<T>::type V;
   constexpr int NV = Vec16<T>::n;
@@ -448,6 +450,7 @@ __global__ void __launch_bounds__(REL_TX * REL_TY) k_reliable_vec(Geom g, double
                                                                   const double* __restrict__ b,
                                                                   Stencil<double, double> S, T* r, RedBuf red,
                                                                   Scalars* s, int kz) {
+  pdl_enter();
   if (s->done || !s->do_reliable) return;
   typedef typename Vec2<T>::type ET;
   const int lane = threadIdx.x;
@@ -550,6 +553,7 @@ __global__ void __launch_bounds__(REL_TX * REL_TY) k_reliable_vec(Geom g, double
 template <class T>
 __global__ void __launch_bounds__(TNT) k_dot_rz(Geom g, const T* __restrict__ r, const T* __restrict__ z, RedBuf red,
                                                 Scalars* s, int kz) {
+  pdl_enter();
   if (s->done) return;
   const int i = blockIdx.x * TBX + threadIdx.x;
   const int j = blockIdx.y * TBY + threadIdx.y;
@@ -604,6 +608,7 @@ __global__ void __launch_bounds__(TNT) k_dir(Geom g, const T* __restrict__ z, T*
 __global__ void __launch_bounds__(TNT) k_true_residual(Geom g, const double* __restrict__ x, const double* __restrict__ b,
                                                        Stencil<double, double> S, double* r, int write_r, RedBuf red,
                                                        Scalars* s, int kz) {
+  pdl_enter();
   const int i = blockIdx.x * TBX + threadIdx.x;
   const int j = blockIdx.y * TBY + threadIdx.y;
   const int k0 = blockIdx.z * kz;
@@ -727,6 +732,7 @@ template <class T, class C>
 __global__ void __launch_bounds__(TNT) k_resid_restrict(Geom g, const T* __restrict__ x, const T* __restrict__ rhs,
                                                         const double* shift, Stencil<T, C> S, Geom gc, int cx, int cy,
                                                         int cz, T* rhs_c, const Scalars* s) {
+  pdl_enter();
   if (s && s->done) return;
   typedef acc_t<T> A;
   const int I = blockIdx.x * TBX + threadIdx.x;
@@ -761,6 +767,7 @@ template <class T>
 __global__ void __launch_bounds__(TNT) k_resid_restrict2(Geom g, const T* __restrict__ x, const T* __restrict__ rhs,
                                                          const double* shift, Stencil<T, T> S, Geom gc, T* rhs_c,
                                                          const Scalars* s) {
+  pdl_enter();
   if (s && s->done) return;
   typedef acc_t<T> A;
   typedef typename Vec2<T>::type V2;
@@ -927,6 +934,7 @@ __device__ __forceinline__ void cta_resid_restrict(const CoarseLevel& L, const C
 template <class T, class C>
 __global__ void __launch_bounds__(1024) k_coarse_vcycle(CoarseSet set, int nu1, int nu2, int coarse_pairs,
                                                         const double* shift0, const Scalars* s) {
+  pdl_enter();
   if (s && s->done) return;
   const int n = set.n;
   // down
@@ -1115,6 +1123,7 @@ __global__ void k_adj_gradient(Geom g, RefDims R, double inv_dx, double inv_dy, 
 template <class T, class C>
 __global__ void __launch_bounds__(TNT) k_jacobi_precond(Geom g, const T* __restrict__ r, const double* shift,
                                                         Stencil<T, C> S, T* z, const Scalars* s, int kz) {
+  pdl_enter();
   if (s->done) return;
   typedef acc_t<T> A;
   const int i = blockIdx.x * TBX + threadIdx.x;

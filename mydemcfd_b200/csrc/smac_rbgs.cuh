@@ -41,6 +41,7 @@ __global__ void __launch_bounds__(RB_NT) k_rbgs_sweep(Geom g, const T* __restric
                                                       const T* __restrict__ rhs, const double* shift, Stencil<T, C> S,
                                                       int c0, const T* __restrict__ xc, Geom gc, int cx, int cy, int cz,
                                                       Scalars* s, RedBuf red, int zchunk) {
+  pdl_enter();
   typedef acc_t<T> A;
   constexpr int TX = RB_TX, TY = RbTile<T>::TY;
   constexpr int XW = TX + 8;  // staged xin columns i0-4 .. i0+TX+3
@@ -203,6 +204,7 @@ __global__ void __launch_bounds__(DMV_TX * DMV_TY) k_dir_matvec_vec(Geom g, cons
                                                                     Stencil<T, T> S, T* __restrict__ q,
                                                                     const uint8_t* __restrict__ fluid, RedBuf red,
                                                                     Scalars* s, int kz) {
+  pdl_enter();
   if (s->done) return;
   typedef acc_t<T> A;
   typedef typename Vec16<T>::type V;

@@ -115,6 +115,7 @@ template <class T, int MODE, bool DOT>
 __global__ void __launch_bounds__(TmaTile<T>::NT, 2)
     k_rbgs_tma(const __grid_constant__ SweepMaps maps, Geom g, T* __restrict__ xout, const double* shift, int c0,
                const T* __restrict__ xc, Geom gc, int cx, int cy, int cz, Scalars* s, RedBuf red, int zchunk) {
+  pdl_enter();
   typedef acc_t<T> A;
   typedef TmaTile<T> L;
   constexpr int TX = L::TX, TY = L::TY, XW = L::XW, RW = L::RW, RH = L::RH, NT = L::NT, HP = TX / 2;

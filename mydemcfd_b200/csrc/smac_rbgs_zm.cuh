@@ -47,6 +47,7 @@ namespace smac {
 template <class T>
 __global__ void __launch_bounds__(256) k_prolong_add(Geom g, T* __restrict__ x, const T* __restrict__ xc, Geom gc,
                                                      int cx, int cy, int cz, const Scalars* s) {
+  pdl_enter();
   if (s && s->done) return;
   typedef typename Vec16<T>::type V;
   constexpr int NV = Vec16<T>::n;
@@ -112,6 +113,7 @@ __global__ void __launch_bounds__(ZmTile<T, NV_, WX, TY, MODE>::NT)
     k_rbgs_zm(Geom g, const T* __restrict__ xin, T* __restrict__ xout, const T* __restrict__ rhs, const double* shift,
               Stencil<T, T> S, int c0, const T* __restrict__ xc, Geom gc, int cx, int cy, int cz, Scalars* s,
               RedBuf red, int zchunk) {
+  pdl_enter();
   typedef ZmTile<T, NV_, WX, TY, MODE> L;
   typedef typename VecN<T, NV_>::type V;
   typedef T A;

@@ -55,10 +55,12 @@ def test_noalloc_matches_apply_A_twice(kind):
         xAx = torch.zeros(1, dtype=torch.float64, device="cuda")
         torch.cuda.synchronize()
         free0 = torch.cuda.mem_get_info()[0]
+        alloc0 = torch.cuda.memory_allocated()
         assert _noalloc(case, g, x, y, xAx) == nat.OK, nat.last_error()
         torch.cuda.synchronize()
         if call == 1:  # the first call may load the library's module (and its static array)
             assert torch.cuda.mem_get_info()[0] == free0, "the call allocated device memory"
+            assert torch.cuda.memory_allocated() == alloc0
         yi, yri = W.interior(y.cpu().numpy()), W.interior(y_ref.cpu().numpy())
         scale = np.abs(yri).max()
         assert np.abs(yi - yri).max() <= 1e-13 * scale
@@ -69,6 +71,42 @@ def test_noalloc_matches_apply_A_twice(kind):
         assert abs(float(xAx.item()) - ref_dot) <= 1e-12 * abs(ref_dot)
         # ghost entries of y are not written
         assert float(y[0].abs().max()) == 0.0 and float(y[:, :, -1].abs().max()) == 0.0
+    solver.close()
+
+
+def test_noalloc_recorded_in_a_cuda_graph():
+    """The use the entry point exists for: one eager call (which may load the
+    module), then the call recorded in a stream capture (its memset node and
+    kernel) and replayed on new x."""
+    case = W.vof_case(40, seed=23, ratio=1000.0)
+    g = DeviceGrid.from_case(case)
+    solver = B200PressureSolver(case.N, case.h)
+    solver.set_coefficients(g)
+    sh = W.shapes(case.N)
+    n = int(np.prod(sh["cell"]))
+    x = torch.from_numpy(W.uniform_pm1(930, n).reshape(sh["cell"])).cuda()
+    y = torch.zeros_like(x)
+    xAx = torch.zeros(1, dtype=torch.float64, device="cuda")
+    assert _noalloc(case, g, x, y, xAx) == nat.OK, nat.last_error()
+    torch.cuda.synchronize()
+    graph = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(graph):
+        rc = _noalloc(case, g, x, y, xAx)
+    assert rc == nat.OK, nat.last_error()
+    for rep in range(2):
+        xh = W.uniform_pm1(931 + rep, n).reshape(sh["cell"])
+        x.copy_(torch.from_numpy(xh))
+        y.zero_()
+        xAx.fill_(12345.0)
+        graph.replay()
+        y_ref = torch.zeros_like(x)
+        solver.apply_A(x, y_ref)
+        torch.cuda.synchronize()
+        yi, yri = W.interior(y.cpu().numpy()), W.interior(y_ref.cpu().numpy())
+        assert np.abs(yi - yri).max() <= 1e-13 * np.abs(yri).max()
+        ref_dot = float((W.interior(xh) * yri).sum())
+        assert abs(float(xAx.item()) - ref_dot) <= 1e-12 * abs(ref_dot)
+    del graph
     solver.close()
 
 
