@@ -94,6 +94,8 @@ typedef struct {
   int sweep_kernel;       /* smac_sweep_kernel: which kernel runs the fused red-black sweeps of the
                              separately launched grids, default SMAC_SWEEP_AUTO; every choice gives
                              the same result bit for bit */
+  int coarse_kernel;      /* smac_coarse_kernel: how the lower part of the V-cycle runs, default
+                             SMAC_COARSE_AUTO; both choices give the same result bit for bit */
 } smac_options;
 
 typedef enum {
@@ -104,6 +106,14 @@ typedef enum {
                               512 FP32); other grids fall back to the TMA ring */
   SMAC_SWEEP_SHARED = 3    /* tiles staged in shared memory by plain loads */
 } smac_sweep_kernel;
+
+typedef enum {
+  SMAC_COARSE_AUTO = 0,    /* from the first grid of <= 32768 cells down, one cluster of 8 CTAs that
+                              holds the grids in distributed shared memory, where they fit (else as
+                              SMAC_COARSE_CTA) */
+  SMAC_COARSE_CTA = 1      /* the grids of <= 4096 cells in one CTA on global memory, the grids
+                              above them launched sweep by sweep */
+} smac_coarse_kernel;
 
 typedef struct {
   int status;              /* smac_status of the solve */

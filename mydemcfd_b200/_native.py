@@ -22,6 +22,7 @@ STANDARD_PCG, PURENEUMANN_STANDARD_PCG, GMG_PCG, PURENEUMANN_GMG_PCG = range(4)
 PRECISION_FP64, PRECISION_MIXED = 0, 1
 STOP_RELATIVE, STOP_REFERENCE = 0, 1
 SWEEP_AUTO, SWEEP_TMA, SWEEP_ZMARCH, SWEEP_SHARED = range(4)
+COARSE_AUTO, COARSE_CTA = range(2)
 
 
 class GridDesc(ctypes.Structure):
@@ -35,7 +36,7 @@ class Options(ctypes.Structure):
         ("tol", ctypes.c_double), ("max_iter", ctypes.c_int), ("min_coarse", ctypes.c_int),
         ("max_levels", ctypes.c_int), ("nu1", ctypes.c_int), ("nu2", ctypes.c_int),
         ("coarse_sweeps", ctypes.c_int), ("check_every", ctypes.c_int), ("reliable_delta", ctypes.c_double),
-        ("bf16_coarse_cells", ctypes.c_int), ("sweep_kernel", ctypes.c_int),
+        ("bf16_coarse_cells", ctypes.c_int), ("sweep_kernel", ctypes.c_int), ("coarse_kernel", ctypes.c_int),
     ]
 
 

@@ -20,6 +20,7 @@ DEPS = SOURCES + [
     os.path.join(HERE, "csrc", "smac_rbgs.cuh"),
     os.path.join(HERE, "csrc", "smac_rbgs_tma.cuh"),
     os.path.join(HERE, "csrc", "smac_rbgs_zm.cuh"),
+    os.path.join(HERE, "csrc", "smac_coarse_cluster.cuh"),
     os.path.join(ROOT, "include", "smac_b200.h"),
 ]
 NVCC_FLAGS = [

@@ -13,6 +13,7 @@
 #include "smac_rbgs.cuh"
 #include "smac_rbgs_tma.cuh"
 #include "smac_rbgs_zm.cuh"
+#include "smac_coarse_cluster.cuh"
 
 #include <cudaTypedefs.h>
 #include <type_traits>
@@ -103,6 +104,7 @@ struct Level {
   double *x64 = nullptr, *x64b = nullptr, *rhs64 = nullptr;  // levels >= 1 (two iterates: out-of-place sweeps)
   void *bxm = nullptr, *bym = nullptr, *bzm = nullptr;  // mixed-precision weights
   int ctm = CT_F32;
+  float *bxw = nullptr, *byw = nullptr, *bzw = nullptr;  // BF16 weights widened to FP32 (the cluster kernel's)
   float *x32 = nullptr, *x32b = nullptr, *rhs32 = nullptr;   // levels >= 1
   // TMA tensor maps of the fused sweep, indexed by the iterate buffer read
   SweepMaps mp64[2], mp32[2];
@@ -119,6 +121,12 @@ struct smac_handle {
   RefDims R{};
   int nlev = 0;
   int lc = 0;  // first grid of the single-CTA coarse set
+  // the cluster set (k_coarse_cluster): its first grid (-1: not used), grids
+  // spread over the ranks, and per grid its chunk and shared-memory offsets
+  int lk = -1, kc_nd = 0;
+  int kc_chunk[MAXL] = {}, kc_off[MAXL][5] = {};
+  int kc_elems = 0;
+  bool kc_ok[2] = {false, false};  // [FP32, FP64]: launchable
   Level lv[MAXL];
   uint8_t* fluid = nullptr;   // padded cell bits: 1 C_INTERIOR, 2 fluid unknown
   double *fbx = nullptr, *fby = nullptr, *fbz = nullptr;  // masked f_b, padded (divergence, correction, adjoint)
@@ -225,6 +233,7 @@ smac_status validate_options(const smac_options* o) {
   if (o->coarse_sweeps < 1 || o->coarse_sweeps > 1024) { set_err("options: coarse_sweeps in [1,1024]"); return SMAC_BAD_ARG; }
   if (o->check_every < 1) { set_err("options: check_every >= 1"); return SMAC_BAD_ARG; }
   if (o->sweep_kernel < 0 || o->sweep_kernel > 3) { set_err("options: sweep_kernel %d", o->sweep_kernel); return SMAC_BAD_ARG; }
+  if (o->coarse_kernel < 0 || o->coarse_kernel > 1) { set_err("options: coarse_kernel %d", o->coarse_kernel); return SMAC_BAD_ARG; }
   if (!(o->reliable_delta > 0.0 && o->reliable_delta < 1.0)) { set_err("options: reliable_delta in (0,1)"); return SMAC_BAD_ARG; }
   return SMAC_OK;
 }
@@ -376,8 +385,13 @@ bool launch_sweep(smac_handle* h, int l, int mode, bool dot, const T* xin, T* xo
   const Geom& g = L.g;
   const Level& Lc = h->lv[l + 1 < h->nlev ? l + 1 : l];
   const int sk = h->opts.sweep_kernel;
+  // FP64 sweeps from zero on rows wider than 128 cells take the shared-memory
+  // tiles, which stage no input then: measured 173 against 226 us (z-march)
+  // and 244 us (TMA ring) at 256^3, 68 against 119 and 104 us at 192^3.
+  const bool zero_shared = sk == SMAC_SWEEP_AUTO && sizeof(T) == 8 && mode == 1 && g.nx > 128;
   if constexpr (std::is_same<T, CS>::value) {
-    const int zs = (sk == SMAC_SWEEP_ZMARCH || sk == SMAC_SWEEP_AUTO) ? zm_shape<T>(h, g, sk == SMAC_SWEEP_AUTO) : -1;
+    const int zs = (!zero_shared && (sk == SMAC_SWEEP_ZMARCH || sk == SMAC_SWEEP_AUTO))
+                       ? zm_shape<T>(h, g, sk == SMAC_SWEEP_AUTO) : -1;
     if (zs >= 0) {
       if (mode == 2) {
         constexpr int NV = Vec16<T>::n;
@@ -392,7 +406,7 @@ bool launch_sweep(smac_handle* h, int l, int mode, bool dot, const T* xin, T* xo
       return false;
     }
     const bool ok = sizeof(T) == 8 ? L.tma64 : L.tma32;
-    if (h->use_tma && ok && sk != SMAC_SWEEP_SHARED) {
+    if (h->use_tma && ok && sk != SMAC_SWEEP_SHARED && !zero_shared) {
       // the maps bind the level's two iterate buffers, its rhs and coefficients
       const SweepMaps* mp = sizeof(T) == 8 ? L.mp64 : L.mp32;
       const void* xb = (l == 0) ? (sizeof(T) == 8 ? (const void*)h->z64b : (const void*)h->z32b)
@@ -446,10 +460,58 @@ void launch_update(smac_handle* h, const Geom& g, T* x, const T* d, T* r, const 
       g.alloc, h->red, h->s);
 }
 
+// Whether the lower part of the V-cycle runs in the cluster kernel, and the
+// first grid of the part that does not run sweep by sweep.
+bool use_cluster(const smac_handle* h, bool mixed) {
+  return h->lk >= 1 && h->opts.coarse_kernel == SMAC_COARSE_AUTO && h->kc_ok[mixed ? 0 : 1];
+}
+int coarse_start(const smac_handle* h, bool mixed) { return use_cluster(h, mixed) ? h->lk : h->lc; }
+
+// Global bytes of the cluster kernel per launch: the first grid's rhs in and
+// x out, every grid's three weight arrays in.
+double cluster_bytes(const smac_handle* h, bool mixed) {
+  const double s = mixed ? 4.0 : 8.0;
+  double b = 2.0 * s * (double)h->lv[h->lk].g.cells();
+  for (int l = h->lk; l < h->nlev; ++l) {
+    const double sc = mixed ? 4.0 : 8.0;  // (BF16 weights through their FP32 copies)
+    b += 3.0 * sc * (double)h->lv[l].g.cells();
+  }
+  return b;
+}
+
+template <class T>
+void launch_cluster(smac_handle* h, bool mixed, const T* rhs, T* x) {
+  ClusterSet set{};
+  set.n = h->nlev - h->lk;
+  set.nd = h->kc_nd;
+  for (int q = 0; q < set.n; ++q) {
+    const Level& L = h->lv[h->lk + q];
+    ClusterLevel& C = set.L[q];
+    C.g = L.g;
+    C.cx = L.cx; C.cy = L.cy; C.cz = L.cz;
+    C.chunk = h->kc_chunk[q];
+    C.ox = h->kc_off[q][0]; C.orhs = h->kc_off[q][1];
+    C.obx = h->kc_off[q][2]; C.oby = h->kc_off[q][3]; C.obz = h->kc_off[q][4];
+    // every array staged as T: BF16 weights through their exact FP32 copies
+    const bool wide = mixed && L.ctm == CT_BF16;
+    C.ctype = mixed ? CT_F32 : CT_F64;
+    C.bx = wide ? (const void*)L.bxw : mixed ? L.bxm : (const void*)L.bx64;
+    C.by = wide ? (const void*)L.byw : mixed ? L.bym : (const void*)L.by64;
+    C.bz = wide ? (const void*)L.bzw : mixed ? L.bzm : (const void*)L.bz64;
+  }
+  set.rhs0 = rhs;
+  set.x0 = x;
+  launch_pdl(k_coarse_cluster<T>, KCL, kcl_threads<T>(), (size_t)h->kc_elems * sizeof(T), h->stream, set, h->opts.nu1,
+      h->opts.nu2, h->opts.coarse_sweeps, (const Scalars*)h->s);
+  h->alg_bytes += cluster_bytes(h, mixed);
+  h->launches += 1;
+}
+
 template <class T, class CS, class CC>
 smac_status launch_vcycle(smac_handle* h, T* r0, T* z0a, T* z0b, bool mixed, bool dot, T** z_out) {
   const smac_options& o = h->opts;
-  const int lc = h->lc;
+  const bool clu = use_cluster(h, mixed);
+  const int lc = coarse_start(h, mixed);
   const double* shift0 = &h->s->rshift;
   const double s = sizeof(T);
   const double sc = mixed ? (double)sizeof(CS) : 8.0;
@@ -491,8 +553,12 @@ smac_status launch_vcycle(smac_handle* h, T* r0, T* z0a, T* z0b, bool mixed, boo
     account(h, g, 2 * s + 3 * sc + s / 8, 1);
     CKL();
   }
-  // single-CTA coarse set, in place on XA
-  {
+  if (clu) {
+    launch_cluster<T>(h, mixed, B(lc), XA(lc));
+    CKL();
+    fin[lc] = XA(lc);
+  } else {
+    // single-CTA coarse set, in place on XA
     CoarseSet set{};
     set.n = h->nlev - lc;
     for (int q = 0; q < set.n; ++q) {
@@ -647,7 +713,8 @@ double iteration_bytes(smac_handle* h, bool mixed, bool gmg, int* launches) {
   int n = 0;
   const double s = mixed ? 4.0 : 8.0;
   if (gmg) {
-    for (int l = 0; l < h->lc; ++l) {
+    const int lc = coarse_start(h, mixed);
+    for (int l = 0; l < lc; ++l) {
       const double cells = (double)h->lv[l].g.cells();
       const double sc = mixed ? 4.0 : 8.0;
       bytes += (4.0 * s + 3 * sc) * cells;
@@ -667,8 +734,9 @@ double iteration_bytes(smac_handle* h, bool mixed, bool gmg, int* launches) {
         n += 1;
       }
     }
-    n += 1;  // single-CTA coarse grids (their bytes are negligible)
-    if (h->lc == 0) { bytes += 2 * s * (double)g.cells(); n += 1; }
+    n += 1;  // the coarse grids' kernel (the single-CTA one's bytes are negligible)
+    if (use_cluster(h, mixed)) bytes += cluster_bytes(h, mixed);
+    if (lc == 0) { bytes += 2 * s * (double)g.cells(); n += 1; }
   } else {
     bytes += (2 * s + 3 * s) * (double)g.cells() + 2 * s * (double)g.cells();
     n += 2;
@@ -771,6 +839,69 @@ void setup_zm(smac_handle* h) {
   h->zm_ctas[1][3] = 0;
 }
 
+// The cluster set: from the first grid below the finest with <= KCL_TOP
+// cells down, where the coarsest grid has <= KCL_SOLO cells (rank 0 holds
+// those) and one rank's share fits in shared memory.  The spread grids'
+// chunks halve with every z-coarsening, so that a coarse plane is in the
+// rank of its two children: the first chunk is the planes per rank rounded
+// up to a multiple of 2^(z-coarsenings below it within the spread grids and
+// into the first held one).
+template <class T>
+bool cluster_attr(int bytes) {
+  if (cudaFuncSetAttribute(k_coarse_cluster<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(KCL, 1, 1);
+  cfg.blockDim = dim3(kcl_threads<T>(), 1, 1);
+  cfg.dynamicSmemBytes = (size_t)bytes;
+  int n = 0;
+  if (cudaOccupancyMaxActiveClusters(&n, k_coarse_cluster<T>, &cfg) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return n >= 1;
+}
+
+void setup_cluster(smac_handle* h, int smem_optin) {
+  h->lk = -1;
+  int lk = -1;
+  for (int l = 1; l < h->nlev; ++l)
+    if (h->lv[l].g.cells() <= KCL_TOP) { lk = l; break; }
+  if (lk < 1 || h->lv[h->nlev - 1].g.cells() > KCL_SOLO || h->nlev - lk > MAX_CLL) return;
+  const int n = h->nlev - lk;
+  int nd = 0;
+  while (nd < n && h->lv[lk + nd].g.cells() > KCL_SOLO) ++nd;
+  int pow2 = 1;
+  for (int q = 1; q <= nd && q < n; ++q)
+    if (h->lv[lk + q].cz) pow2 *= 2;
+  const int nz0 = h->lv[lk].g.nz;
+  int chunk = (nz0 + KCL - 1) / KCL;
+  chunk = (chunk + pow2 - 1) / pow2 * pow2;
+  long long tot = 0;
+  auto take = [&](long long e) { const long long o = tot; tot += (e + 3) / 4 * 4; return (int)o; };
+  for (int q = 0; q < n; ++q) {
+    const Geom& g = h->lv[lk + q].g;
+    if (q > 0 && q < nd && h->lv[lk + q].cz) chunk /= 2;
+    const int c = q < nd ? chunk : g.nz;
+    if (c < 1) return;
+    h->kc_chunk[q] = c;
+    const long long nx = g.nx, ny = g.ny;
+    h->kc_off[q][0] = take(c * nx * ny);            // x
+    h->kc_off[q][1] = take(c * nx * ny);            // rhs
+    h->kc_off[q][2] = take(c * ny * (nx + 1));      // bx
+    h->kc_off[q][3] = take(c * (ny + 1) * nx);      // by
+    h->kc_off[q][4] = take((c + 1) * ny * nx);      // bz
+  }
+  if (tot * 8 > (1LL << 30)) return;
+  h->kc_elems = (int)tot;
+  h->kc_nd = nd;
+  h->kc_ok[0] = tot * 4 <= smem_optin && cluster_attr<float>((int)(tot * 4));
+  h->kc_ok[1] = tot * 8 <= smem_optin && cluster_attr<double>((int)(tot * 8));
+  if (h->kc_ok[0] || h->kc_ok[1]) h->lk = lk;
+}
+
 // Tensor maps for every separately launched grid, or use_tma = false.
 void setup_tma(smac_handle* h) {
   h->use_tma = false;
@@ -843,6 +974,7 @@ smac_status smac_default_options(smac_options* o) {
   o->reliable_delta = 1e-4;
   o->bf16_coarse_cells = COARSE_CELLS;
   o->sweep_kernel = SMAC_SWEEP_AUTO;
+  o->coarse_kernel = SMAC_COARSE_AUTO;
   return SMAC_OK;
 }
 
@@ -949,6 +1081,7 @@ smac_status smac_create(const smac_grid_desc* desc, const smac_options* opts, vo
       if ((st = palloc(h, g, &p))) return fail(st); L.bym = p;
       if ((st = palloc(h, g, &p))) return fail(st); L.bzm = p;
       L.ctm = CT_BF16;
+      if ((st = palloc(h, g, &L.bxw)) || (st = palloc(h, g, &L.byw)) || (st = palloc(h, g, &L.bzw))) return fail(st);
     } else {
       float* p;
       if ((st = palloc(h, g, &p))) return fail(st); L.bxm = p;
@@ -982,6 +1115,7 @@ smac_status smac_create(const smac_grid_desc* desc, const smac_options* opts, vo
   h->num_sms = prop.multiProcessorCount;
   setup_tma(h);
   setup_zm(h);
+  setup_cluster(h, prop.sharedMemPerBlockOptin);
   cudaError_t es = cudaStreamSynchronize(h->stream);
   if (es != cudaSuccess) { set_err("smac_create: %s", cudaGetErrorString(es)); return fail(SMAC_CUDA_ERROR); }
   *out = h;
@@ -1008,7 +1142,7 @@ smac_status smac_set_options(smac_handle* h, const smac_options* opts) {
     return SMAC_BAD_ARG;
   }
   if (opts->nu1 != h->opts.nu1 || opts->nu2 != h->opts.nu2 || opts->coarse_sweeps != h->opts.coarse_sweeps ||
-      opts->sweep_kernel != h->opts.sweep_kernel)
+      opts->sweep_kernel != h->opts.sweep_kernel || opts->coarse_kernel != h->opts.coarse_kernel)
     drop_graphs(h);  // the captured iterations launch the old sweeps
   h->opts = *opts;
   return SMAC_OK;
@@ -1069,6 +1203,9 @@ smac_status smac_set_coefficients(smac_handle* h, const double* fbx, const doubl
       k_convert<__nv_bfloat16><<<256, 256, 0, h->stream>>>(base_of(L.g, L.bx64), base_of(L.g, (__nv_bfloat16*)L.bxm), n);
       k_convert<__nv_bfloat16><<<256, 256, 0, h->stream>>>(base_of(L.g, L.by64), base_of(L.g, (__nv_bfloat16*)L.bym), n);
       k_convert<__nv_bfloat16><<<256, 256, 0, h->stream>>>(base_of(L.g, L.bz64), base_of(L.g, (__nv_bfloat16*)L.bzm), n);
+      k_widen_bf16<<<256, 256, 0, h->stream>>>(base_of(L.g, (const __nv_bfloat16*)L.bxm), base_of(L.g, L.bxw), n);
+      k_widen_bf16<<<256, 256, 0, h->stream>>>(base_of(L.g, (const __nv_bfloat16*)L.bym), base_of(L.g, L.byw), n);
+      k_widen_bf16<<<256, 256, 0, h->stream>>>(base_of(L.g, (const __nv_bfloat16*)L.bzm), base_of(L.g, L.bzw), n);
     } else {
       k_convert<float><<<256, 256, 0, h->stream>>>(base_of(L.g, L.bx64), base_of(L.g, (float*)L.bxm), n);
       k_convert<float><<<256, 256, 0, h->stream>>>(base_of(L.g, L.by64), base_of(L.g, (float*)L.bym), n);

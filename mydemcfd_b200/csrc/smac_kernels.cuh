@@ -165,6 +165,13 @@ __global__ void k_convert(const double* __restrict__ a, C* b, long long n) {
   for (; t < n; t += (long long)gridDim.x * blockDim.x) b[t] = coef_from_double<C>(a[t]);
 }
 
+// BF16 -> FP32 copy of a whole padded array (exact): the cluster kernel's
+// copy of the BF16 coefficients, which it stages without conversion.
+__global__ void k_widen_bf16(const __nv_bfloat16* __restrict__ a, float* b, long long n) {
+  long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  for (; t < n; t += (long long)gridDim.x * blockDim.x) b[t] = __bfloat162float(a[t]);
+}
+
 // ------------------------------------------------------------------------
 // Right-hand side: base_k_make_poisson_rhs (G_PressureSolverBase.cu:49-118),
 // same operation order; eps == nullptr means eps == 1, fs == nullptr means

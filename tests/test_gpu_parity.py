@@ -168,6 +168,40 @@ def test_fused_sweep_equals_half_sweeps(precision, N, sweep):
         assert s.selftest_sweep(precision, mode) == 0, (mode, precision, sweep)
 
 
+def _coarse_cases():
+    from _cases import oracle_solid_fraction
+    return {
+        "plain64": lambda: W.plain_case(64, seed=1),
+        "plain128": lambda: W.plain_case(128, seed=2),
+        "vof40_r1000": lambda: W.vof_case(40, seed=3, ratio=1000.0),
+        "ibm48": lambda: W.ibm_case(48, seed=4, nsph=6, solid_fraction=oracle_solid_fraction, rmin_cells=3.0,
+                                    rmax_cells=6.0),
+        "vof_256x16x12": lambda: W.vof_case(256, seed=3, ratio=1000.0, N=(256, 16, 12)),
+        "vof_64x6x40": lambda: W.vof_case(64, seed=3, ratio=1000.0, N=(64, 6, 40)),
+    }
+
+
+@pytest.mark.parametrize("precision", [nat.PRECISION_FP64, nat.PRECISION_MIXED])
+@pytest.mark.parametrize("name", list(_coarse_cases()))
+def test_cluster_coarse_grids_equal_single_cta(name, precision):
+    """The lower V-cycle in one cluster (grids in distributed shared memory,
+    SMAC_COARSE_AUTO) gives the solve of the separately launched sweeps plus
+    the single-CTA kernel (SMAC_COARSE_CTA) bit for bit: the same iterations
+    and the same p_delta.  Cases: cubic grids whose cluster set starts at 32^3
+    or 20^3, a thin grid spread over six ranks one plane each, and one whose
+    set holds grids of five planes."""
+    case = _coarse_cases()[name]()
+    out = []
+    for ck in (nat.COARSE_AUTO, nat.COARSE_CTA):
+        g, s, st = solve_gpu(case, tol=1e-12, precision=precision, coarse_kernel=ck)
+        assert st["status"] == 0, st
+        out.append((st["iterations"], cpu(g.p_delta_).copy(), st["kernel_launches"]))
+        s.close()
+    assert out[0][0] == out[1][0]
+    assert np.array_equal(out[0][1], out[1][1])
+    print(f"{name}: {out[0][0]} iterations, {out[0][2]} launches with the cluster, {out[1][2]} without")
+
+
 # ---------------------------------------------------------------------------
 # solves
 def test_fp64_solve_matches_oracle_64(oracle_lib):

@@ -36,6 +36,7 @@ def test_default_options(lib):
     assert o.solver_type == nat.PURENEUMANN_GMG_PCG
     assert o.precision == nat.PRECISION_FP64
     assert o.tol == 1e-8 and o.max_iter == 2000 and o.nu1 == 2 and o.nu2 == 2
+    assert o.sweep_kernel == nat.SWEEP_AUTO and o.coarse_kernel == nat.COARSE_AUTO
 
 
 def test_null_arguments_are_refused(lib):
@@ -52,7 +53,8 @@ def test_null_arguments_are_refused(lib):
 def test_bad_options_are_refused(lib):
     d = nat.GridDesc(16, 16, 16, 1 / 16, 1 / 16, 1 / 16)
     h = ctypes.c_void_p()
-    for bad in (dict(tol=0.0), dict(solver_type=9), dict(nu1=0), dict(max_iter=0), dict(reliable_delta=1.5)):
+    for bad in (dict(tol=0.0), dict(solver_type=9), dict(nu1=0), dict(max_iter=0), dict(reliable_delta=1.5),
+                dict(sweep_kernel=4), dict(coarse_kernel=2)):
         o = nat.default_options(**bad)
         assert lib.smac_create(ctypes.byref(d), ctypes.byref(o), None, ctypes.byref(h)) == nat.BAD_ARG
     bad = nat.GridDesc(1, 16, 16, 1.0, 1.0, 1.0)
