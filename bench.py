@@ -414,7 +414,7 @@ def run_ours(args, ranks):
     achieved = bytes_k / (ms_k / 1e3) / 1e9
     traffic = ncu_traffic()
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                "traffic": traffic, "kernel": "k_rbgs_zm<float,2,6,0,false>: fused red-black sweep, register z-march "
+                "traffic": traffic, "kernel": "k_rbgs_zm<float,4,2,6,0,false>: fused red-black sweep, register z-march "
                                               "over whole rows, 256^3 grid",
                 "peak_kind": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else peak_kind,
                 "alg_bytes_per_launch": bytes_k, "ms_per_launch": ms_k}
