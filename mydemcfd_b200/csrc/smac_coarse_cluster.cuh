@@ -38,7 +38,7 @@ constexpr int KCL = 8;           // CTAs in the cluster (the portable maximum)
 #ifndef SMAC_KCL_NT32
 #define SMAC_KCL_NT32 512
 #endif
-template <class T> constexpr int kcl_threads() { return sizeof(T) == 8 ? 512 : SMAC_KCL_NT32; }
+template <class T> __host__ __device__ constexpr int kcl_threads() { return sizeof(T) == 8 ? 512 : SMAC_KCL_NT32; }
 constexpr int KCL_SOLO = 512;    // grids of at most this many cells are held and swept by rank 0
 constexpr int KCL_TOP = 32768;   // the set starts at the first grid of at most this many cells
 constexpr int MAX_CLL = 12;
@@ -140,6 +140,14 @@ __device__ __noinline__ void cl_stage(ClusterView<T> V, const ClusterLevel& Lp, 
   cl_copy_rows<T>(V.local + L.oby, Lp.by, Lp.ctype, b, np * (L.ny + 1), L.nx, L.ny + 1, g.px, g.ps);
   cl_copy_rows<T>(V.local + L.obz, Lp.bz, Lp.ctype, b, (np + 1) * L.ny, L.nx, L.ny, g.px, g.ps);  // z-faces k0..k0+np
   if (rhs0) cl_copy_rows<T>(V.local + L.orhs, rhs0, sizeof(T) == 8 ? 0 : 1, b, np * L.ny, L.nx, L.ny, g.px, g.ps);
+}
+template <class T>
+__device__ __noinline__ void cl_stage_rhs(ClusterView<T> V, const ClusterLevel& Lp, const T* rhs0) {
+  const ClGrid L = cl_grid(Lp);
+  const Geom& g = Lp.g;
+  const int k0 = V.p0(L), np = V.p1(L) - k0;
+  if (np <= 0) return;
+  cl_copy_rows<T>(V.local + L.orhs, rhs0, sizeof(T) == 8 ? 0 : 1, g.idx(0, 0, k0), np * L.ny, L.nx, L.ny, g.px, g.ps);
 }
 
 // The six neighbours (x-, x+, y-, y+, z-, z+) of the own cell (i, j, k) of
@@ -272,6 +280,62 @@ __device__ __noinline__ void cl_resid_restrict(ClusterView<T> V, ClGrid L, ClGri
   }
 }
 
+// nhalf half-sweeps of a grid held whole by rank 0 (nx*ny*nz <= KCL_SOLO <=
+// blockDim.x): thread t keeps cell t's weights and rhs in registers across
+// the half-sweeps, which read the neighbours' x from shared memory and end
+// at a CTA barrier.  Half-sweep h has colour c0 ^ (h & 1) before swap_at and
+// (1 - c0) ^ ((h - swap_at) & 1) from there (the coarsest grid's backward
+// pairs); the first starts from zero (zero_first) or adds the prolongation
+// of Lc's x to the neighbours (pro_first).  The operations are those of
+// cl_half_sweep.  Called by every thread of rank 0.
+template <class T>
+__device__ __noinline__ void cl_solo_run(ClusterView<T> V, ClGrid L, int nhalf, int c0, int swap_at, bool zero_first,
+                                         bool pro_first, ClGrid Lc) {
+  typedef acc_t<T> A;
+  const int nx = L.nx, ny = L.ny, nz = L.nz, pc = nx, pl = nx * ny;
+  const int t = threadIdx.x;
+  const bool own = t < nx * ny * nz;
+  int i = 0, j = 0, k = 0, c = 0;
+  T wxm = (T)0, wxp = (T)0, wym = (T)0, wyp = (T)0, wzm = (T)0, wzp = (T)0;
+  A bv = (A)0;
+  if (own) {
+    i = t % nx;
+    j = (t / nx) % ny;
+    k = t / pl;
+    c = (k * ny + j) * pc + i;
+    cl_weights(V, L, i, j, k, c, wxm, wxp, wym, wyp, wzm, wzp);
+    bv = (A)V.local[L.orhs + c];  // (no mean shift below the finest grid)
+  }
+  T* x = V.local + L.ox;
+  for (int h = 0; h < nhalf; ++h) {
+    const int colour = h < swap_at ? (c0 ^ (h & 1)) : ((1 - c0) ^ ((h - swap_at) & 1));
+    if (own && ((i + j + k + colour) & 1) == 0) {
+      A n[6] = {(A)0, (A)0, (A)0, (A)0, (A)0, (A)0};
+      if (!(h == 0 && zero_first)) {
+        n[0] = (A)(i > 0 ? x[c - 1] : (T)0);
+        n[1] = (A)(i + 1 < nx ? x[c + 1] : (T)0);
+        n[2] = (A)(j > 0 ? x[c - pc] : (T)0);
+        n[3] = (A)(j + 1 < ny ? x[c + pc] : (T)0);
+        n[4] = (A)(k > 0 ? x[c - pl] : (T)0);
+        n[5] = (A)(k + 1 < nz ? x[c + pl] : (T)0);
+        if (h == 0 && pro_first) {
+          const int ci[6][3] = {{i - 1, j, k}, {i + 1, j, k}, {i, j - 1, k}, {i, j + 1, k}, {i, j, k - 1},
+                                {i, j, k + 1}};
+#pragma unroll
+          for (int q = 0; q < 6; ++q) {
+            const int a = ci[q][0], b = ci[q][1], d = ci[q][2];
+            if (a >= 0 && b >= 0 && d >= 0 && a < nx && b < ny && d < nz)
+              n[q] = Ar<A>::add(n[q], (A)V.x(Lc, Lc.cx ? a >> 1 : a, Lc.cy ? b >> 1 : b, Lc.cz ? d >> 1 : d));
+          }
+        }
+      }
+      x[c] = (T)Stencil<T, T>::gs(bv, (A)wxm, (A)wxp, (A)wym, (A)wyp, (A)wzm, (A)wzp, n[0], n[1], n[2], n[3], n[4],
+                                  n[5]);
+    }
+    __syncthreads();
+  }
+}
+
 // Smoothing step helpers: the spread grids end each step at a cluster
 // barrier, the grids of rank 0 at a CTA barrier (rank 0 only).
 template <class T, class F>
@@ -289,8 +353,7 @@ __device__ __forceinline__ void cl_step(const ClusterView<T>& V, bool spread, F&
 template <class T>
 __global__ void __cluster_dims__(KCL, 1, 1) __launch_bounds__(kcl_threads<T>())
     k_coarse_cluster(const __grid_constant__ ClusterSet set, int nu1, int nu2, int coarse_pairs, const Scalars* s) {
-  pdl_enter();
-  if (s && s->done) return;  // the same flag for every rank: all return, or none
+  static_assert(KCL_SOLO <= kcl_threads<T>(), "a rank-0 grid needs a thread per cell");
   namespace cg = cooperative_groups;
   extern __shared__ __align__(16) unsigned char cl_smem[];
   cg::cluster_group cl = cg::this_cluster();
@@ -298,7 +361,16 @@ __global__ void __cluster_dims__(KCL, 1, 1) __launch_bounds__(kcl_threads<T>())
   V.me = (int)cl.block_rank();
   V.local = reinterpret_cast<T*>(cl_smem);
   const int n = set.n, nd = set.nd;
-  for (int q = 0; q < n; ++q) cl_stage<T>(V, set.L[q], q == 0 ? (const T*)set.rhs0 : nullptr);
+  // The weights, which no kernel of the solve writes, are staged while the
+  // previous kernel drains; the first grid's rhs, its output, after the wait.
+  for (int q = 0; q < n; ++q) cl_stage<T>(V, set.L[q], nullptr);
+  pdl_enter();
+  if (s && s->done) {  // the same flag for every rank: all return, or none
+    __pipeline_commit();
+    __pipeline_wait_prior(0);  // no copy into this CTA's shared memory outlives it
+    return;
+  }
+  cl_stage_rhs<T>(V, set.L[0], (const T*)set.rhs0);
   __pipeline_commit();
   __pipeline_wait_prior(0);
   cl.sync();
@@ -315,27 +387,14 @@ __global__ void __cluster_dims__(KCL, 1, 1) __launch_bounds__(kcl_threads<T>())
   if (V.me == 0) {
     for (int q = nd; q < n - 1; ++q) {
       const ClGrid L = cl_grid(set.L[q]);
-      for (int it = 0; it < nu1; ++it) {
-        cl_step(V, false, [&] { cl_half_sweep<T>(V, L, 0, it == 0, false, L); });
-        cl_step(V, false, [&] { cl_half_sweep<T>(V, L, 1, false, false, L); });
-      }
+      cl_solo_run<T>(V, L, 2 * nu1, 0, 2 * nu1, true, false, L);
       cl_step(V, false, [&] { cl_resid_restrict<T>(V, L, cl_grid(set.L[q + 1])); });
     }
     const ClGrid C = cl_grid(set.L[n - 1]);
-    for (int it = 0; it < coarse_pairs; ++it) {
-      cl_step(V, false, [&] { cl_half_sweep<T>(V, C, 0, it == 0, false, C); });
-      cl_step(V, false, [&] { cl_half_sweep<T>(V, C, 1, false, false, C); });
-    }
-    for (int it = 0; it < coarse_pairs; ++it) {
-      cl_step(V, false, [&] { cl_half_sweep<T>(V, C, 1, false, false, C); });
-      cl_step(V, false, [&] { cl_half_sweep<T>(V, C, 0, false, false, C); });
-    }
+    cl_solo_run<T>(V, C, 4 * coarse_pairs, 0, 2 * coarse_pairs, true, false, C);
     for (int q = n - 2; q >= nd; --q) {
       const ClGrid L = cl_grid(set.L[q]);
-      for (int it = 0; it < nu2; ++it) {
-        cl_step(V, false, [&] { cl_half_sweep<T>(V, L, 1, false, it == 0, cl_grid(set.L[q + 1])); });
-        cl_step(V, false, [&] { cl_half_sweep<T>(V, L, 0, false, false, L); });
-      }
+      cl_solo_run<T>(V, L, 2 * nu2, 1, 2 * nu2, false, true, cl_grid(set.L[q + 1]));
     }
   }
   cl.sync();
