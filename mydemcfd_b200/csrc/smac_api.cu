@@ -1303,9 +1303,16 @@ smac_status smac_divergence(smac_handle* h, const double* vxs, const double* vys
   if (!((fsx && fsy && fsz) || (!fsx && !fsy && !fsz))) { set_err("smac_divergence: fsx/fsy/fsz go together"); return SMAC_BAD_ARG; }
   if (!(dt > 0) || !std::isfinite(dt)) { set_err("smac_divergence: dt must be > 0"); return SMAC_BAD_ARG; }
   const Geom& g = h->lv[0].g;
-  k_divergence<<<grid_planes(g.nx, g.ny, g.nz), kBlock, 0, h->stream>>>(
-      g, h->R, 1.0 / h->desc.dx, 1.0 / h->desc.dy, 1.0 / h->desc.dz, 1.0 / dt, vxs, vys, vzs, eps, eps_old,
-      h->fbx, h->fby, h->fbz, fsx, fsy, fsz, h->fluid, h->b64, rhs_out);
+  if (!eps && !fsx) {
+    constexpr int KZ = 4;
+    k_divergence_z<KZ><<<dim3((g.nx + TBX - 1) / TBX, (g.ny + TBY - 1) / TBY, (g.nz + KZ - 1) / KZ), kBlock, 0,
+                         h->stream>>>(g, h->R, 1.0 / h->desc.dx, 1.0 / h->desc.dy, 1.0 / h->desc.dz, 1.0 / dt, vxs,
+                                      vys, vzs, h->fluid, h->b64, rhs_out);
+  } else {
+    k_divergence<<<grid_planes(g.nx, g.ny, g.nz), kBlock, 0, h->stream>>>(
+        g, h->R, 1.0 / h->desc.dx, 1.0 / h->desc.dy, 1.0 / h->desc.dz, 1.0 / dt, vxs, vys, vzs, eps, eps_old,
+        h->fbx, h->fby, h->fbz, fsx, fsy, fsz, h->fluid, h->b64, rhs_out);
+  }
   CKL();
   h->dt = dt;
   h->have_rhs = true;
@@ -1511,7 +1518,9 @@ smac_status export_solution(smac_handle* h, const double* x, double* p_delta) {
     k_sum_fluid<<<grid_cells(g, kz_for(g)), kBlock, 0, h->stream>>>(g, x, h->fluid, h->red, h->s, kz_for(g));
     CKL();
   }
-  k_export_cells<<<gp, kBlock, 0, h->stream>>>(g, h->R, x, h->fluid, pure ? &h->s->sum_tmp : nullptr, p_delta);
+  constexpr int KZ = 4;
+  k_export_cells_z<KZ><<<dim3(gp.x, gp.y, (g.nz + KZ - 1) / KZ), kBlock, 0, h->stream>>>(
+      g, h->R, x, h->fluid, pure ? &h->s->sum_tmp : nullptr, p_delta);
   CKL();
   account(h, g, pure ? 8 + 1 + 8 + 1 + 8 : 16, pure ? 2 : 1);
   return SMAC_OK;

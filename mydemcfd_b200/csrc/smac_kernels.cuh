@@ -224,6 +224,57 @@ __global__ void k_divergence(Geom g, RefDims R, double inv_dx, double inv_dy, do
   if (rhs_ref) rhs_ref[R.cell(ix, iy, iz)] = out;
 }
 
+// The same RHS without ε and f_s (ε = 1, f_s = 0: the same operations with
+// those constants), KZ planes per thread with every plane's loads issued
+// before the first result is formed; a z-face between two of the planes is
+// read once.
+template <int KZ>
+__global__ void __launch_bounds__(TNT) k_divergence_z(Geom g, RefDims R, double inv_dx, double inv_dy, double inv_dz,
+                                                      double inv_dt, const double* __restrict__ vx,
+                                                      const double* __restrict__ vy, const double* __restrict__ vz,
+                                                      const uint8_t* __restrict__ cellbits, double* rhs,
+                                                      double* rhs_ref) {
+  const int i = blockIdx.x * TBX + threadIdx.x;
+  const int j = blockIdx.y * TBY + threadIdx.y;
+  const int k0 = blockIdx.z * KZ;
+  if (i >= g.nx || j >= g.ny) return;
+  const int ix = i + 1, iy = j + 1;
+  double xp[KZ], xm[KZ], yp[KZ], ym[KZ], zf[KZ + 1];
+  uint8_t bits[KZ];
+#pragma unroll
+  for (int q = 0; q < KZ; ++q) {
+    const int k = k0 + q, iz = k + 1;
+    bits[q] = 0;
+    xp[q] = xm[q] = yp[q] = ym[q] = 0.0;
+    if (k < g.nz) {
+      bits[q] = cellbits[g.idx(i, j, k)];
+      xp[q] = vx[R.xf(ix + 1, iy, iz)];
+      xm[q] = vx[R.xf(ix, iy, iz)];
+      yp[q] = vy[R.yf(ix, iy + 1, iz)];
+      ym[q] = vy[R.yf(ix, iy, iz)];
+    }
+    zf[q] = k <= g.nz ? vz[R.zf(ix, iy, iz)] : 0.0;  // the low face of plane k, the top face of plane k-1
+  }
+  zf[KZ] = k0 + KZ <= g.nz ? vz[R.zf(ix, iy, k0 + KZ + 1)] : 0.0;
+#pragma unroll
+  for (int q = 0; q < KZ; ++q) {
+    const int k = k0 + q;
+    if (k >= g.nz) break;
+    const double ztop = zf[q + 1];
+    double out = 0.0;
+    if (bits[q] & 1) {
+      const double one = 1.0, deps = 0.0, f_st = 0.0;
+      const double tx = DMUL(DADD(DMUL(one, xp[q]), -DMUL(one, xm[q])), inv_dx);
+      const double ty = DMUL(DADD(DMUL(one, yp[q]), -DMUL(one, ym[q])), inv_dy);
+      const double tz = DMUL(DADD(DMUL(one, ztop), -DMUL(one, zf[q])), inv_dz);
+      const double div_eps = DADD(DADD(tx, ty), tz);
+      out = DADD(DADD(DMUL(-inv_dt, div_eps), -DMUL(DMUL(deps, inv_dt), inv_dt)), -f_st);
+    }
+    rhs[g.idx(i, j, k)] = out;
+    if (rhs_ref) rhs_ref[R.cell(ix, iy, k + 1)] = out;
+  }
+}
+
 // Reference-layout cell array (interior) -> padded array.
 template <class T>
 __global__ void k_import_cells(Geom g, RefDims R, const double* __restrict__ src, T* dst) {
@@ -236,6 +287,36 @@ __global__ void k_import_cells(Geom g, RefDims R, const double* __restrict__ src
 
 // Padded FP64 array -> reference-layout interior, minus `shift` on fluid cells
 // (the zero-mean projection of the solution).
+// KZ planes per thread, every plane's loads issued before the first store.
+template <int KZ>
+__global__ void __launch_bounds__(TNT) k_export_cells_z(Geom g, RefDims R, const double* __restrict__ src,
+                                                        const uint8_t* __restrict__ fluid, const double* shift,
+                                                        double* dst) {
+  const int i = blockIdx.x * TBX + threadIdx.x;
+  const int j = blockIdx.y * TBY + threadIdx.y;
+  const int k0 = blockIdx.z * KZ;
+  if (i >= g.nx || j >= g.ny) return;
+  const double sh = shift ? *shift : 0.0;
+  double v[KZ];
+  uint8_t f[KZ];
+#pragma unroll
+  for (int q = 0; q < KZ; ++q) {
+    v[q] = 0.0;
+    f[q] = 0;
+    if (k0 + q < g.nz) {
+      const int c = g.idx(i, j, k0 + q);
+      v[q] = src[c];
+      f[q] = fluid[c];
+    }
+  }
+#pragma unroll
+  for (int q = 0; q < KZ; ++q) {
+    if (k0 + q >= g.nz) break;
+    double w = v[q];
+    if (shift && (f[q] & 2)) w -= sh;
+    dst[R.cell(i + 1, j + 1, k0 + q + 1)] = w;
+  }
+}
 __global__ void k_export_cells(Geom g, RefDims R, const double* __restrict__ src, const uint8_t* __restrict__ fluid,
                                const double* shift, double* dst) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -278,15 +359,32 @@ __global__ void __launch_bounds__(TNT) k_setup_project(Geom g, double* b, const 
   const double m = s->sum_tmp;
   if (i < g.nx && j < g.ny) {
     const int k1 = min(k0 + kz, g.nz);
-    for (int k = k0; k < k1; ++k) {
-      const int c = g.idx(i, j, k);
-      double bv = b[c];
-      if (fluid[c] & 2) bv -= m;
-      else bv = 0.0;
-      b[c] = bv;
-      r[c] = (TR)bv;
-      v[0] += bv * bv;
-      v[1] = fmax(v[1], fabs(bv));
+    // four planes' loads ahead of their stores, the planes taken in order
+    for (int kb = k0; kb < k1; kb += 4) {
+      double bq[4];
+      uint8_t fq[4];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        bq[q] = 0.0;
+        fq[q] = 0;
+        if (kb + q < k1) {
+          const int c = g.idx(i, j, kb + q);
+          bq[q] = b[c];
+          fq[q] = fluid[c];
+        }
+      }
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        if (kb + q >= k1) break;
+        const int c = g.idx(i, j, kb + q);
+        double bv = bq[q];
+        if (fq[q] & 2) bv -= m;
+        else bv = 0.0;
+        b[c] = bv;
+        r[c] = (TR)bv;
+        v[0] += bv * bv;
+        v[1] = fmax(v[1], fabs(bv));
+      }
     }
   }
   const Op ops[2] = {Op::Sum, Op::Max};

@@ -7,7 +7,8 @@ oracle and the reference's own solve.
   oracle with the same solver type, both to a relative true residual of
   1e-13; the converged pressures agree to 1e-10 relative on the fluid cells
   after removing their mean (the pure-Neumann null space).  The grids are a
-  plain 32^3 box, a VoF sphere at 1000:1 and IBM spheres.
+  plain 32^3 box, a VoF sphere at 1000:1, IBM spheres and a ragged
+  40 x 24 x 22 VoF grid.
 - Every golden vector of the reference's own GPU solve (tests/golden/,
   made by tests/golden/make_golden.py) is solved on the GPU with the
   vector's solver type.  The GPU result agrees with the oracle's tight solve
@@ -59,6 +60,8 @@ def _cases():
         "vof32_r1000": lambda: W.vof_case(32, seed=3, ratio=1000.0),
         "ibm48": lambda: W.ibm_case(48, seed=4, nsph=6, solid_fraction=oracle_solid_fraction, rmin_cells=3.0,
                                     rmax_cells=6.0),
+        # ragged: depths and widths that fill no kernel's tiles or plane groups
+        "vof_40x24x22": lambda: W.vof_case(40, seed=5, ratio=100.0, N=(40, 24, 22)),
     }
 
 

@@ -51,9 +51,12 @@ def test_box_types_device():
         assert np.array_equal(cpu(a), b)
 
 
-def test_divergence_bit_exact(oracle_lib):
+@pytest.mark.parametrize("N", [(24, 24, 24), (37, 11, 18), (20, 9, 5)])
+def test_divergence_bit_exact(oracle_lib, N):
+    """The RHS is bit for bit the reference's; the grids' depths 18 and 5
+    leave the kernel's last group of four planes part full."""
     O = oracle_lib
-    case = W.plain_case(24, seed=3, dt=0.37)
+    case = W.vof_case(N[0], seed=3, ratio=10.0, N=N, dt=0.37) if N[1] != N[0] else W.plain_case(24, seed=3, dt=0.37)
     g = DeviceGrid.from_case(case)
     s = make_solver(case)
     s.set_coefficients(g)
