@@ -341,7 +341,15 @@ __global__ void __launch_bounds__(TNT) k_setup_sum(Geom g, const double* __restr
   double v[1] = {0.0};
   if (i < g.nx && j < g.ny) {
     const int k1 = min(k0 + kz, g.nz);
-    for (int k = k0; k < k1; ++k) v[0] += b[g.idx(i, j, k)];
+    // four planes' loads at once, summed in plane order
+    for (int kb = k0; kb < k1; kb += 4) {
+      double bq[4];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) bq[q] = kb + q < k1 ? b[g.idx(i, j, kb + q)] : 0.0;
+#pragma unroll
+      for (int q = 0; q < 4; ++q)
+        if (kb + q < k1) v[0] += bq[q];
+    }
   }
   const Op ops[1] = {Op::Sum};
   double out[1];
@@ -770,9 +778,23 @@ __global__ void __launch_bounds__(TNT) k_sum_fluid(Geom g, const double* __restr
   double v[1] = {0.0};
   if (i < g.nx && j < g.ny) {
     const int k1 = min(k0 + kz, g.nz);
-    for (int k = k0; k < k1; ++k) {
-      const int c = g.idx(i, j, k);
-      if (fluid[c] & 2) v[0] += x[c];
+    // four planes' values and masks loaded at once, summed in plane order
+    for (int kb = k0; kb < k1; kb += 4) {
+      double xq[4];
+      uint8_t fq[4];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        xq[q] = 0.0;
+        fq[q] = 0;
+        if (kb + q < k1) {
+          const int c = g.idx(i, j, kb + q);
+          xq[q] = x[c];
+          fq[q] = fluid[c];
+        }
+      }
+#pragma unroll
+      for (int q = 0; q < 4; ++q)
+        if (kb + q < k1 && (fq[q] & 2)) v[0] += xq[q];
     }
   }
   const Op ops[1] = {Op::Sum};

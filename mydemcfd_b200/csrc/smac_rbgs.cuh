@@ -26,6 +26,8 @@
 // residual, fused into the last sweep of the fine grid).
 #pragma once
 
+#include <type_traits>
+
 #include "smac_kernels.cuh"
 
 namespace smac {
@@ -252,9 +254,14 @@ __global__ void __launch_bounds__(DMV_TX * DMV_TY) k_dir_matvec_vec(Geom g, cons
       const T* byus = reinterpret_cast<const T*>(&byu);
       const T* bzs = reinterpret_cast<const T*>(&bzc);
       const T* bzus = reinterpret_cast<const T*>(&bzu);
+      // the vector's mask bytes in one load (c is a multiple of NV)
       uint8_t fl[NV];
+      {
+        typedef typename std::conditional<NV == 4, uint32_t, uint16_t>::type MW;
+        const MW mw = *reinterpret_cast<const MW*>(fluid + c);
 #pragma unroll
-      for (int e = 0; e < NV; ++e) fl[e] = fluid[c + e];
+        for (int e = 0; e < NV; ++e) fl[e] = (uint8_t)(mw >> (8 * e));
+      }
       // centre values with the fluid mask applied, as stored in d_new
       A xcm[NV];
 #pragma unroll
