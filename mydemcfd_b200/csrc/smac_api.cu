@@ -1580,10 +1580,9 @@ smac_status smac_project(smac_handle* h, const double* vxs, const double* vys, c
   TRY(export_solution(h, x, p_delta));
   const Geom& g = h->lv[0].g;
   const RefDims& R = h->R;
-  k_correct<<<grid_planes(R.Nx + 3, R.Ny + 3, R.Nz + 3), kBlock, 0, h->stream>>>(
-      R, g, 1.0 / h->desc.dx, 1.0 / h->desc.dy, 1.0 / h->desc.dz, dt, h->ct, h->fxt, h->fyt, h->fzt, p_delta, nullptr,
-      vxs, vys, vzs, nullptr, nullptr, nullptr, h->fbx, h->fby, h->fbz, nullptr, nullptr, nullptr,
-      vx, vy, vz, 1);
+  k_correct_project<<<grid_planes(R.Nx + 3, R.Ny + 3, R.Nz + 3), kBlock, 0, h->stream>>>(
+      R, g, 1.0 / h->desc.dx, 1.0 / h->desc.dy, 1.0 / h->desc.dz, dt, h->fxt, h->fyt, h->fzt, p_delta, vxs, vys, vzs,
+      h->fbx, h->fby, h->fbz, vx, vy, vz);
   CKL();
   account(h, g, 3 * 8 + 8 + 3 * 8 + 3 * 8 + 3, 1);
   if (stats) {

@@ -1172,6 +1172,98 @@ __global__ void k_correct(RefDims R, Geom g, double inv_dx, double inv_dy, doubl
   }
 }
 
+// The correction as smac_project runs it (f_s = 0, f_inv_rho from the padded
+// f_b, p untouched, faces that are not F_INTERIOR receive u*): the
+// operations of k_correct, with every value a face may need loaded together
+// with its type (the indices are valid for every face in the reference's
+// range), so an F_INTERIOR face costs one round trip instead of two.
+__global__ void k_correct_project(RefDims R, Geom g, double inv_dx, double inv_dy, double inv_dz, double dt,
+                                  const uint8_t* __restrict__ fxt, const uint8_t* __restrict__ fyt,
+                                  const uint8_t* __restrict__ fzt, const double* __restrict__ pd,
+                                  const double* __restrict__ vxs, const double* __restrict__ vys,
+                                  const double* __restrict__ vzs, const double* __restrict__ fbx,
+                                  const double* __restrict__ fby, const double* __restrict__ fbz, double* vx,
+                                  double* vy, double* vz) {
+  const int ix = blockIdx.x * blockDim.x + threadIdx.x;
+  const int iy = blockIdx.y * blockDim.y + threadIdx.y;
+  const int iz = blockIdx.z;
+  const int Nx = R.Nx, Ny = R.Ny, Nz = R.Nz;
+  auto padded = [&](const double* b, int i, int j, int k) -> double {
+    if (i < 0 || j < 0 || k < 0 || i > g.nx || j > g.ny || k > g.nz) return 0.0;
+    return b[g.idx(i, j, k)];
+  };
+  const bool cin = ix < Nx + 2 && iy < Ny + 2 && iz < Nz + 2;
+  const double p0 = cin ? pd[R.cell(ix, iy, iz)] : 0.0;
+  // x-faces
+  const bool xin = iy < Ny + 2 && ix < Nx + 3 && iz < Nz + 2, xr = ix >= 1 && ix <= Nx + 1;
+  uint8_t tx = 0;
+  double ux = 0.0, pxm = 0.0, irx = 0.0;
+  long long fx = 0;
+  if (xin) {
+    fx = R.xf(ix, iy, iz);
+    tx = fxt[fx];
+    ux = vxs[fx];
+    if (xr) {
+      pxm = pd[R.cell(ix - 1, iy, iz)];
+      irx = padded(fbx, ix - 1, iy - 1, iz - 1);
+    }
+  }
+  // y-faces
+  const bool yin = iy < Ny + 3 && ix < Nx + 2 && iz < Nz + 2, yr = iy >= 1 && iy <= Ny + 1;
+  uint8_t ty = 0;
+  double uy = 0.0, pym = 0.0, iry = 0.0;
+  long long fy = 0;
+  if (yin) {
+    fy = R.yf(ix, iy, iz);
+    ty = fyt[fy];
+    uy = vys[fy];
+    if (yr) {
+      pym = pd[R.cell(ix, iy - 1, iz)];
+      iry = padded(fby, ix - 1, iy - 1, iz - 1);
+    }
+  }
+  // z-faces
+  const bool zin = iy < Ny + 2 && ix < Nx + 2 && iz < Nz + 3, zr = iz >= 1 && iz <= Nz + 1;
+  uint8_t tz = 0;
+  double uz = 0.0, pzm = 0.0, irz = 0.0;
+  long long fz = 0;
+  if (zin) {
+    fz = R.zf(ix, iy, iz);
+    tz = fzt[fz];
+    uz = vzs[fz];
+    if (zr) {
+      pzm = pd[R.cell(ix, iy, iz - 1)];
+      irz = padded(fbz, ix - 1, iy - 1, iz - 1);
+    }
+  }
+  // (a face with xr, yr or zr has both of its cells, so p0 was loaded)
+  const double fs = 0.0;
+  if (xin) {
+    if (tx == F_INTERIOR && xr) {
+      const double gp = DMUL(DADD(p0, -pxm), inv_dx);
+      vx[fx] = DADD(ux, DMUL(DMUL(irx, dt), DADD(fs, -gp)));
+    } else {
+      vx[fx] = ux;
+    }
+  }
+  if (yin) {
+    if (ty == F_INTERIOR && yr) {
+      const double gp = DMUL(DADD(p0, -pym), inv_dy);
+      vy[fy] = DADD(uy, DMUL(DMUL(iry, dt), DADD(fs, -gp)));
+    } else {
+      vy[fy] = uy;
+    }
+  }
+  if (zin) {
+    if (tz == F_INTERIOR && zr) {
+      const double gp = DMUL(DADD(p0, -pzm), inv_dz);
+      vz[fz] = DADD(uz, DMUL(DMUL(irz, dt), DADD(fs, -gp)));
+    } else {
+      vz[fz] = uz;
+    }
+  }
+}
+
 // ------------------------------------------------------------------------
 // Adjoint pieces.  The projection on F_INTERIOR faces is
 //   u = u* + B G A^+ D u*     (B = diag f_b, G = face gradient, D = divergence)

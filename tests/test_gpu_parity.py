@@ -107,6 +107,28 @@ def test_correction_bit_exact(oracle_lib):
     assert float(g.p_delta_.abs().max()) == 0.0  # correct_vof_velocity zeroes p_delta_
 
 
+@pytest.mark.parametrize("N", [(24, 24, 24), (37, 11, 18)])
+def test_project_correction_bit_exact(oracle_lib, N):
+    """smac_project's correction is the reference's k_correct_vof_velocity of
+    the p_delta it exports, bit for bit, and every other face carries u*."""
+    O = oracle_lib
+    case = W.vof_case(N[0], seed=2, ratio=10.0, N=N)
+    g = DeviceGrid.from_case(case)
+    s = make_solver(case, tol=1e-10)
+    s.set_coefficients(g)
+    sh = W.shapes(case.N)
+    out = [torch.zeros(sh[k], dtype=torch.float64, device="cuda") for k in "xyz"]
+    pd = torch.zeros(sh["cell"], dtype=torch.float64, device="cuda")
+    s.project(g.f_vx_star_, g.f_vy_star_, g.f_vz_star_, case.dt, pd, *out)
+    torch.cuda.synchronize()
+    vx, vy, vz, _ = O.correct(ref_grid(case), cpu(pd))
+    for got, want, t, star in zip(out, (vx, vy, vz), (case.fxt, case.fyt, case.fzt), (case.vxs, case.vys, case.vzs)):
+        got = cpu(got)
+        m = t == W.F_INTERIOR
+        assert np.array_equal(got[m], want[m])
+        assert np.array_equal(got[~m], star[~m])
+
+
 def test_vof_assembly_bit_exact(oracle_lib):
     O = oracle_lib
     case = W.vof_case(20, seed=4, ratio=1000.0)
