@@ -35,6 +35,7 @@
 #include <type_traits>
 
 #include "smac_rbgs.cuh"
+#include "smac_rbgs_tma.cuh"
 
 namespace smac {
 
@@ -70,6 +71,10 @@ __global__ void __launch_bounds__(256) k_prolong_add(Geom g, T* __restrict__ x, 
     }
     *p = a;
   }
+}
+
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
 }
 
 // NV consecutive cells of one row as one register vector (8 or 16 bytes)
@@ -124,6 +129,28 @@ __global__ void __launch_bounds__(ZmTile<T, NV_, WX, TY, MODE>::NT)
   T* M = reinterpret_cast<T*>(zm_smem);                  // inputs [NB][ROWS][TW]
   T* R = reinterpret_cast<T*>(zm_smem + L::M_BYTES);     // c0 results [NB][ROWS][32 WX][H]
   if (s && s->done) return;
+  // One barrier phase per step, split: a warp arrives once its shared writes
+  // of step k are done and waits for the phase only before the first shared
+  // read of step k+1, so the colour-(1-c0) pass of step k (which reads step
+  // k-1's results) and the next step's loads overlap the slower warps.
+  // Waits are bounded; on expiry the status records the failure and the
+  // kernel runs on without waiting.
+  __shared__ uint64_t zm_bar;
+  if (threadIdx.x == 0) mbar_init(&zm_bar, ZmTile<T, NV_, WX, TY, MODE>::NT / 32);
+  __syncthreads();
+  uint32_t zm_phase = 0;
+  bool zm_bad = false;
+  auto zm_arrive = [&]() {
+    __syncwarp();
+    if ((threadIdx.x & 31) == 0) mbar_arrive(&zm_bar);
+  };
+  auto zm_wait = [&]() {
+    if (!zm_bad && !mbar_wait_bounded(&zm_bar, zm_phase & 1u)) {
+      zm_bad = true;
+      if (s) s->status = 6;
+    }
+    ++zm_phase;
+  };
   const int tid = threadIdx.x;
   const int lane = tid & 31, w = tid >> 5;
   const int wx = w % WX, wr = w / WX;
@@ -245,7 +272,7 @@ __global__ void __launch_bounds__(ZmTile<T, NV_, WX, TY, MODE>::NT)
     Blk blA, blB;
 #pragma unroll
     for (int q = 0; q < H; ++q) red_m2[q] = red_m1[q] = (T)0;
-    __syncthreads();
+    zm_arrive();  // the prologue's shared writes (waited for by the first step)
 
     // Step k with P = parity of plane k's c0 cells (a compile-time constant):
     // colour c0 on plane k from `cur`, the operands of plane k+1 loaded into
@@ -264,6 +291,7 @@ __global__ void __launch_bounds__(ZmTile<T, NV_, WX, TY, MODE>::NT)
       // --- colour c0 on plane k: cells 2q + P
       T red_k[H];
       const bool plane_ok = k >= 0 && k < g.nz;
+      zm_wait();  // every warp's shared writes of the previous step
       {
         const T* Mk = Mrow(k, 0);
         // x-neighbours across the vector edge: colour-(1-c0) inputs of plane k
@@ -325,7 +353,7 @@ __global__ void __launch_bounds__(ZmTile<T, NV_, WX, TY, MODE>::NT)
         bout.bz[q] = el(bz_c, 2 * q + Q);
         bout.bzu[q] = el(cur.bzu, 2 * q + Q);
       }
-      __syncthreads();
+      zm_arrive();
       // --- colour 1-c0 on plane k-1 (tile rows only): cells 2q + P
       const int kk = k - 1;
       if (!ring && kk >= z0 && kk < z1) {
@@ -397,6 +425,7 @@ __global__ void __launch_bounds__(ZmTile<T, NV_, WX, TY, MODE>::NT)
     };
     if (pk) march(std::integral_constant<int, 1>{});
     else march(std::integral_constant<int, 0>{});
+    zm_wait();        // the last step's phase
     __syncthreads();  // the shared planes are reused by the next item
   }
 
