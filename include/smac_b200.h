@@ -513,6 +513,15 @@ smac_status smac_apply_A_dot_noalloc(const smac_grid_desc* desc, const double* f
  * No counterpart in the reference (it has no Gauss-Seidel smoother). */
 smac_status smac_selftest_sweep(smac_handle* h, int precision, int mode, long long* mismatches);
 
+/* Self-test of the kernels' bounded waits: one warp waits on a shared-memory
+ * mbarrier that nothing arrives on, with the limit every device-side wait of
+ * this library uses (about one second of SM clock), and records the expiry
+ * as the kernels do (solver status SMAC_CUDA_ERROR).  Writes the status the
+ * device recorded (SMAC_CUDA_ERROR when the wait gave up) and the SM cycles it
+ * waited; the handle stays usable (the status is cleared after the read).
+ * No counterpart in the reference (its kernels do not wait on the device). */
+smac_status smac_selftest_wait(smac_handle* h, int* status, long long* cycles);
+
 /* ---------------------------------------------------------------------------
  * Projections with host buffers, queued.  A queue on a handle runs
  * smac_project on inputs and outputs in host memory (the reference layout, as

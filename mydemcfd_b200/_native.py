@@ -102,7 +102,7 @@ EXPORTS = [
     "smac_level_shape", "smac_set_coefficients", "smac_box_types", "smac_assemble_vof",
     "smac_ibm_solid_fraction_spheres", "smac_ibm_set_solid_cells", "smac_divergence", "smac_solve",
     "smac_set_rhs", "smac_correct", "smac_project", "smac_project_adjoint", "smac_apply_A", "smac_time_kernel",
-    "smac_selftest_sweep", "smac_apply_A_dot_noalloc", "smac_async_create", "smac_async_submit",
+    "smac_selftest_sweep", "smac_selftest_wait", "smac_apply_A_dot_noalloc", "smac_async_create", "smac_async_submit",
     "smac_async_wait", "smac_async_destroy", "smac_update_boundary_faces", "smac_update_pressure_ghost",
     "smac_update_velocity_ghost", "smac_face_gradp", "smac_update_vstar_boundary", "smac_surface_tension",
     "smac_predict_vstar", "smac_predict_vstar_two_way", "smac_poisson_beta_two_way", "smac_mass_flux_from_alpha_flux",
@@ -141,6 +141,7 @@ def load(path: str = LIB_PATH):
         "smac_apply_A": [vp, dp, dp],
         "smac_time_kernel": [vp, ip, ip, ctypes.POINTER(ctypes.c_float), ctypes.POINTER(d)],
         "smac_selftest_sweep": [vp, ip, ip, ctypes.POINTER(ctypes.c_longlong)],
+        "smac_selftest_wait": [vp, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_longlong)],
         "smac_apply_A_dot_noalloc": [ctypes.POINTER(GridDesc), dp, dp, dp, u8p, u8p, u8p, u8p, dp, dp, dp, vp],
         "smac_async_create": [vp, ctypes.POINTER(vp)],
         "smac_async_submit": [vp, dp, dp, dp, d, dp, dp, dp, dp, ctypes.POINTER(ctypes.c_ulonglong)],

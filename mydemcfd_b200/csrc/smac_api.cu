@@ -1821,6 +1821,27 @@ smac_status sweep_selftest(smac_handle* h, int mode, T* x, T* xa, T* xb, T* rhs,
 
 extern "C" {
 
+smac_status smac_selftest_wait(smac_handle* h, int* status, long long* cycles) {
+  if (!h || !status || !cycles) { set_err("smac_selftest_wait: null argument"); return SMAC_BAD_ARG; }
+  long long* dcyc = nullptr;
+  CK(cudaMalloc(&dcyc, sizeof(long long)));
+  h->hs->status = 0;
+  TRY(scalars_to_device(h));
+  k_wait_probe<<<1, 32, 0, h->stream>>>(h->s, dcyc);
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) e = cudaMemcpyAsync(cycles, dcyc, sizeof(long long), cudaMemcpyDeviceToHost, h->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+  cudaFree(dcyc);
+  if (e != cudaSuccess) { set_err("smac_selftest_wait: %s", cudaGetErrorString(e)); return SMAC_CUDA_ERROR; }
+  TRY(scalars_to_host(h));
+  CK(cudaStreamSynchronize(h->stream));
+  *status = h->hs->status;
+  h->hs->status = 0;  // the handle stays usable
+  TRY(scalars_to_device(h));
+  CK(cudaStreamSynchronize(h->stream));
+  return SMAC_OK;
+}
+
 smac_status smac_selftest_sweep(smac_handle* h, int precision, int mode, long long* mismatches) {
   if (!h || !mismatches || mode < 0 || mode > 2 || precision < 0 || precision > 1) {
     set_err("smac_selftest_sweep: bad argument");

@@ -77,6 +77,21 @@ __device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
   asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
 }
 
+// A bounded wait on an mbarrier that nothing arrives on (the self-test of the
+// kernels' wait limit): lane 0 records the expiry the way the sweeps do and
+// the cycles it waited.
+__global__ void k_wait_probe(Scalars* s, long long* cycles) {
+  __shared__ uint64_t bar;
+  if (threadIdx.x == 0) mbar_init(&bar, 1);
+  __syncthreads();
+  const long long t0 = clock64();
+  const bool ok = mbar_wait_bounded(&bar, 0u);
+  if (threadIdx.x == 0) {
+    cycles[0] = clock64() - t0;
+    if (!ok) s->status = 6;
+  }
+}
+
 // NV consecutive cells of one row as one register vector (8 or 16 bytes)
 template <class T, int N> struct VecN;
 template <> struct VecN<float, 2> { typedef float2 type; };

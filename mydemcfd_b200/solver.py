@@ -253,6 +253,14 @@ class B200PressureSolver:
         nat.check(self._lib.smac_time_kernel(self._h, kernel_id, reps, ctypes.byref(ms), ctypes.byref(b)))
         return ms.value, b.value
 
+    def selftest_wait(self):
+        """(status the device recorded, SM cycles waited) of a bounded wait that
+        nothing ends (smac_selftest_wait)."""
+        st = ctypes.c_int()
+        cyc = ctypes.c_longlong()
+        nat.check(self._lib.smac_selftest_wait(self._h, ctypes.byref(st), ctypes.byref(cyc)))
+        return st.value, cyc.value
+
     def selftest_sweep(self, precision: int, mode: int) -> int:
         n = ctypes.c_longlong()
         nat.check(self._lib.smac_selftest_sweep(self._h, precision, mode, ctypes.byref(n)))

@@ -193,6 +193,24 @@ def test_fused_sweep_equals_half_sweeps(precision, N, sweep):
         assert s.selftest_sweep(precision, mode) == 0, (mode, precision, sweep)
 
 
+def test_bounded_wait_expires_and_is_reported():
+    """A device-side wait that nothing ends gives up after its limit (about a
+    second of SM clock, the limit of every wait in the sweeps), the status
+    the host reads is SMAC_CUDA_ERROR, and the handle solves afterwards."""
+    case = W.plain_case(16, seed=1)
+    g = DeviceGrid.from_case(case)
+    s = make_solver(case, tol=1e-10)
+    s.set_coefficients(g)
+    status, cycles = s.selftest_wait()
+    assert status == nat.CUDA_ERROR
+    assert cycles >= 1_000_000_000
+    step = SMACStep(g, case.dt)
+    step.pressure_solver_ = s
+    st = step.solve_poisson()
+    assert st["status"] == nat.OK and st["rel_residual"] <= 1e-10, st
+    s.close()
+
+
 def _coarse_cases():
     from _cases import oracle_solid_fraction
     return {
