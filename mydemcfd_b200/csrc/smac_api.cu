@@ -142,9 +142,10 @@ struct smac_handle {
   RedBuf red{};
   long long red_blocks = 0;  // blocks a reducing launch may have (4 partials each)
   int num_sms = 148;
+  long long l2_bytes = 126LL << 20;
   bool use_tma = true;     // fused sweeps stage their tiles with the copy engine
   int tma_ctas[2] = {1, 1};  // resident CTAs per SM of the TMA sweep: [0] FP32, [1] FP64
-  int zm_ctas[2][4] = {};  // resident CTAs per SM of the z-march: [FP32, FP64][shape]
+  int zm_ctas[2][6] = {};  // resident CTAs per SM of the z-march: [FP32, FP64][shape]
   Scalars* s = nullptr;    // device
   Scalars* hs = nullptr;   // pinned, mapped host mirror of the device scalars
   Scalars* hs_dev = nullptr;  // the mirror's device-side address
@@ -296,17 +297,34 @@ void launch_tma_sweep(smac_handle* h, int l, const SweepMaps& maps, T* xout, con
 
 // z-march shapes: the whole x extent in WX warps of 32 x NV cells, TY tile
 // rows.  FP64 (NV = 2): shape 0 one warp per row (x extent <= 64), 14 rows;
-// shape 1 two warps (<= 128), 6 rows; shape 2 four warps (<= 256), 2 rows.
-// FP32: shapes 0-2 the same with NV = 4 (extents 128, 256, 512), shape 3
-// four warps of float2 lanes (<= 256), 6 rows, 1024 threads.
-template <class T> constexpr int zm_nv(int shape) { return sizeof(T) == 8 ? 2 : shape == 3 ? 2 : 4; }
-template <class T> constexpr int zm_wx(int shape) { return shape == 0 ? 1 : shape == 1 ? 2 : 4; }
+// shape 1 two warps (<= 128), 6 rows; shape 2 four warps (<= 256), 2 rows;
+// shape 4 one warp, 6 rows (256 threads, two or more CTAs per SM).  FP32:
+// shapes 0-2 and 4 the same with NV = 4 (extents 128, 256, 512 and 128),
+// shape 3 four warps of float2 lanes (<= 256), 6 rows, 1024 threads, shape 5
+// one warp of float2 lanes (<= 64), 6 rows.
+template <class T> constexpr int zm_nv(int shape) {
+  return sizeof(T) == 8 ? 2 : (shape == 3 || shape == 5) ? 2 : 4;
+}
+template <class T> constexpr int zm_wx(int shape) {
+  return (shape == 0 || shape == 4 || shape == 5) ? 1 : shape == 1 ? 2 : 4;
+}
 template <class T> constexpr int zm_ty(int shape) { return shape == 0 ? 14 : shape == 2 ? 2 : 6; }
-constexpr int ZM_SHAPES = 4;
-#ifdef SMAC_ZM_F32_NARROW
-#define SMAC_ZM_F32_ORDER 0, 3, 1, 2
-#else
-#define SMAC_ZM_F32_ORDER 0, 1, 2, 3
+constexpr int ZM_SHAPES = 6;
+// Rows of at most 128 (FP32) or 64 cells (FP64): SMAC_ZM_SMALL32 = 5 (the
+// default) takes shape 5 for FP32 rows of at most 64 cells and shape 4 up to
+// 128, 4 shape 4 for both, 0 the 14-row shape 0; SMAC_ZM_SMALL64 = 4 takes
+// shape 4 for FP64 rows of at most 64 cells.  Measured (FP32 sweep): 64^3
+// 5.6 us with shape 5, 7.0 with shape 4, 7.8 with shape 0; 128^3 12.4 with
+// shape 4, 13.6 with shape 0; FP64 64^3 shape 4 7.25, shape 0 7.31 (not
+// taken: the FP64 projection measured no faster).
+#ifndef SMAC_ZM_SMALL32
+#define SMAC_ZM_SMALL32 5
+#endif
+#ifndef SMAC_ZM_SMALL64
+#define SMAC_ZM_SMALL64 0
+#endif
+#ifndef SMAC_ZM_F32_ORDER
+#define SMAC_ZM_F32_ORDER 0, 1, 2, 3, -1, -1
 #endif
 // The narrowest shape that covers the x extent, or -1.  With `automatic`,
 // -1 also where the TMA ring measured faster: a two-row tile (four warps per
@@ -314,8 +332,14 @@ constexpr int ZM_SHAPES = 4;
 template <class T>
 int zm_shape(const smac_handle* h, const Geom& g, bool automatic) {
   const int pt = sizeof(T) == 8 ? 1 : 0;
+  if (sizeof(T) == 4) {
+    if (SMAC_ZM_SMALL32 == 5 && g.nx <= 64 && h->zm_ctas[0][5] > 0) return 5;
+    if (SMAC_ZM_SMALL32 >= 4 && g.nx <= 128 && h->zm_ctas[0][4] > 0) return 4;
+  } else if (SMAC_ZM_SMALL64 == 4 && g.nx <= 64 && h->zm_ctas[1][4] > 0) {
+    return 4;
+  }
   const int order32[ZM_SHAPES] = {SMAC_ZM_F32_ORDER};
-  const int order64[ZM_SHAPES] = {0, 1, 2, -1};
+  const int order64[ZM_SHAPES] = {0, 1, 2, -1, -1, -1};
   for (int q = 0; q < ZM_SHAPES; ++q) {
     const int sh = sizeof(T) == 8 ? order64[q] : order32[q];
     if (sh < 0) continue;
@@ -350,8 +374,10 @@ void launch_zm_shape(smac_handle* h, int l, const T* xin, T* xout, const T* rhs,
   // persistent CTAs; one partial sum each in the reduction buffer
   const int G = (int)std::max(1LL, std::min(std::min(slots, items), h->red_blocks));
   Stencil<T, T> S{(const T*)bx, (const T*)by, (const T*)bz};
+  // the L2 prefetch pays only where the sweep's five arrays do not stay in L2
+  const int pf = 5.0 * (double)g.alloc * sizeof(T) > (double)h->l2_bytes ? SMAC_ZM_PF : 0;
   launch_pdl(k_rbgs_zm<T, NV, WX, TY, MODE, DOT>, G, NT, ZmTile<T, NV, WX, TY, MODE>::SMEM, h->stream, g, xin, xout,
-      rhs, sh, S, c0, xc, Lc.g, Lc.cx, Lc.cy, Lc.cz, h->s, h->red, zc);
+      rhs, sh, S, c0, xc, Lc.g, Lc.cx, Lc.cy, Lc.cz, h->s, h->red, zc, pf);
 }
 
 template <class T, int MODE, bool DOT>
@@ -362,7 +388,11 @@ void launch_zm(smac_handle* h, int l, int shape, const T* xin, T* xout, const T*
   if (shape == 0) ZM_SHAPE(0);
   else if (shape == 1) ZM_SHAPE(1);
   else if (shape == 2) ZM_SHAPE(2);
-  else if constexpr (sizeof(T) == 4) ZM_SHAPE(3);
+  else if (shape == 4) ZM_SHAPE(4);
+  else if constexpr (sizeof(T) == 4) {
+    if (shape == 3) ZM_SHAPE(3);
+    else if (shape == 5) ZM_SHAPE(5);
+  }
 #undef ZM_SHAPE
 }
 
@@ -833,10 +863,14 @@ void setup_zm(smac_handle* h) {
   h->zm_ctas[0][1] = zm_occupancy<float, 1>();
   h->zm_ctas[0][2] = zm_occupancy<float, 2>();
   h->zm_ctas[0][3] = zm_occupancy<float, 3>();
+  h->zm_ctas[0][4] = zm_occupancy<float, 4>();
+  h->zm_ctas[0][5] = zm_occupancy<float, 5>();
   h->zm_ctas[1][0] = zm_occupancy<double, 0>();
   h->zm_ctas[1][1] = zm_occupancy<double, 1>();
   h->zm_ctas[1][2] = zm_occupancy<double, 2>();
   h->zm_ctas[1][3] = 0;
+  h->zm_ctas[1][4] = zm_occupancy<double, 4>();
+  h->zm_ctas[1][5] = 0;
 }
 
 // The cluster set: from the first grid below the finest with <= KCL_TOP
@@ -1113,6 +1147,7 @@ smac_status smac_create(const smac_grid_desc* desc, const smac_options* opts, vo
     memset(h->hs, 0, sizeof(Scalars));
   }
   h->num_sms = prop.multiProcessorCount;
+  h->l2_bytes = prop.l2CacheSize;
   setup_tma(h);
   setup_zm(h);
   setup_cluster(h, prop.sharedMemPerBlockOptin);

@@ -73,6 +73,20 @@ __global__ void __launch_bounds__(256) k_prolong_add(Geom g, T* __restrict__ x, 
   }
 }
 
+// Planes ahead of the one a step loads that one thread of the CTA asks the
+// L2 to fetch (one bulk prefetch per array and plane over the rows the tile
+// reads), on grids whose arrays do not fit in L2; 0 leaves the loads to find
+// their data in DRAM.
+#ifndef SMAC_ZM_PF
+#define SMAC_ZM_PF 0
+#endif
+
+// L2 prefetch of `bytes` (a multiple of 16) from a 16-byte aligned address
+__device__ __forceinline__ void bulk_prefetch_l2(const void* p, uint32_t bytes) {
+  if ((reinterpret_cast<uintptr_t>(p) & 15u) != 0 || (bytes & 15u) != 0) return;
+  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
+}
+
 __device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
   asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
 }
@@ -105,6 +119,9 @@ struct ZmTile {
   static constexpr int TW = 32 * NV * WX;         // cells per row: the whole x extent
   static constexpr int ROWS = TY + 2;             // tile rows plus the two ring rows
   static constexpr int NT = 32 * WX * ROWS;       // threads per CTA
+  // CTAs per SM the registers must allow: a 256-thread tile runs two (three
+  // with float2 lanes) per SM at 128 (85) registers a thread
+  static constexpr int MINB = NT <= 256 ? (NV == 2 && sizeof(T) == 4 ? 3 : 2) : 1;
   static constexpr int NB = 4;                    // shared planes in rotation
   static constexpr int M_BYTES = NB * ROWS * TW * (int)sizeof(T);           // inputs, whole vectors
   static constexpr int R_BYTES = NB * ROWS * 32 * WX * H * (int)sizeof(T);  // c0 results, H per lane
@@ -129,10 +146,10 @@ struct ZmBlk {
 };
 
 template <class T, int NV_, int WX, int TY, int MODE, bool DOT>
-__global__ void __launch_bounds__(ZmTile<T, NV_, WX, TY, MODE>::NT)
+__global__ void __launch_bounds__(ZmTile<T, NV_, WX, TY, MODE>::NT, ZmTile<T, NV_, WX, TY, MODE>::MINB)
     k_rbgs_zm(Geom g, const T* __restrict__ xin, T* __restrict__ xout, const T* __restrict__ rhs, const double* shift,
               Stencil<T, T> S, int c0, const T* __restrict__ xc, Geom gc, int cx, int cy, int cz, Scalars* s,
-              RedBuf red, int zchunk) {
+              RedBuf red, int zchunk, int pf) {
   pdl_enter();
   typedef ZmTile<T, NV_, WX, TY, MODE> L;
   typedef typename VecN<T, NV_>::type V;
@@ -264,9 +281,25 @@ __global__ void __launch_bounds__(ZmTile<T, NV_, WX, TY, MODE>::NT)
       }
     };
 
+    // The rows the tile reads on one plane (j0-2 .. j0+TY+1, clipped to the
+    // grid's ny+1 allocated rows) lie at consecutive addresses: one prefetch
+    // per array covers them.  Planes 0..nz are allocated in every array.
+    const int pf_j = max(0, j0 - 2);
+    const uint32_t pf_bytes = (uint32_t)((min(g.ny, j0 + TY + 1) - pf_j + 1) * g.px * (int)sizeof(T));
+    auto prefetch = [&](int m) {  // the operands of plane m (its z-faces m+1 and input m+1 with them)
+      if (tid != 0 || m < 0 || m + 1 > g.nz) return;
+      const int o = g.idx(0, pf_j, m), o1 = g.idx(0, pf_j, m + 1);
+      bulk_prefetch_l2(rhs + o, pf_bytes);
+      bulk_prefetch_l2(S.bx + o, pf_bytes);
+      bulk_prefetch_l2(S.by + o, pf_bytes);
+      bulk_prefetch_l2(S.bz + o1, pf_bytes);
+      if (MODE != 1) bulk_prefetch_l2(xin + o1, pf_bytes);
+    };
+
     // prologue: the inputs of planes kb-1 and kb, the shared plane kb, the
     // operands of the first c0 plane kb = z0 - 1
     const int kb = z0 - 1;
+    for (int d = 1; d <= pf; ++d) prefetch(kb + 1 + d);
     const int pk = (c0 + j + kb) & 1;  // parity of the c0 cells of plane kb in this row (warp-uniform)
     Ops opA, opB;
     load_ops(kb, opA);
@@ -297,6 +330,7 @@ __global__ void __launch_bounds__(ZmTile<T, NV_, WX, TY, MODE>::NT)
       constexpr int P = decltype(Pc)::value;
       const V bz_c = nxt.bzu;  // z-faces k (the previous step's faces k-1+1), read before nxt is reloaded
       if (k + 1 <= z1) load_ops(k + 1, nxt);
+      if (pf > 0 && k + 1 + pf <= z1) prefetch(k + 1 + pf);
       if (pro4) cur.x1 = add_parents(cur.x1, cur.c1);  // the deferred prolongation of this step's input
       // --- the input of plane k+1 becomes visible to the rows above and below
       *reinterpret_cast<V*>(Mrow(k + 1, wr) + ib) = cur.x1;
