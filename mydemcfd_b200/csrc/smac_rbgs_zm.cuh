@@ -78,7 +78,7 @@ __global__ void __launch_bounds__(256) k_prolong_add(Geom g, T* __restrict__ x, 
 // reads), on grids whose arrays do not fit in L2; 0 leaves the loads to find
 // their data in DRAM.
 #ifndef SMAC_ZM_PF
-#define SMAC_ZM_PF 0
+#define SMAC_ZM_PF 2
 #endif
 
 // L2 prefetch of `bytes` (a multiple of 16) from a 16-byte aligned address
