@@ -374,8 +374,11 @@ void launch_zm_shape(smac_handle* h, int l, const T* xin, T* xout, const T* rhs,
   // persistent CTAs; one partial sum each in the reduction buffer
   const int G = (int)std::max(1LL, std::min(std::min(slots, items), h->red_blocks));
   Stencil<T, T> S{(const T*)bx, (const T*)by, (const T*)bz};
-  // the L2 prefetch pays only where the sweep's five arrays do not stay in L2
-  const int pf = 5.0 * (double)g.alloc * sizeof(T) > (double)h->l2_bytes ? SMAC_ZM_PF : 0;
+  // the L2 prefetch pays only where the sweep's five arrays do not stay in
+  // L2; its bulk copies need 16-byte aligned arrays (rows and planes are
+  // multiples of 32 bytes)
+  const uintptr_t al = (uintptr_t)xin | (uintptr_t)rhs | (uintptr_t)bx | (uintptr_t)by | (uintptr_t)bz;
+  const int pf = ((al & 15u) == 0 && 5.0 * (double)g.alloc * sizeof(T) > (double)h->l2_bytes) ? SMAC_ZM_PF : 0;
   launch_pdl(k_rbgs_zm<T, NV, WX, TY, MODE, DOT>, G, NT, ZmTile<T, NV, WX, TY, MODE>::SMEM, h->stream, g, xin, xout,
       rhs, sh, S, c0, xc, Lc.g, Lc.cx, Lc.cy, Lc.cz, h->s, h->red, zc, pf);
 }

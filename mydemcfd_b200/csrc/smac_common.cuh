@@ -120,6 +120,12 @@ __device__ __forceinline__ void pdl_enter() {
   asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
 }
 
+// L2 prefetch of `bytes` (a multiple of 16) from a 16-byte aligned address
+// (a hint: nothing waits for it)
+__device__ __forceinline__ void bulk_prefetch_l2(const void* p, uint32_t bytes) {
+  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
+}
+
 // ---------------------------------------------------------------------------
 // Deterministic grid reduction: every block reduces NV doubles in a fixed
 // tree, writes them to partials[block*NV + v], and the last block to arrive

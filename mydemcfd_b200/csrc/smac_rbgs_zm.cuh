@@ -81,12 +81,6 @@ __global__ void __launch_bounds__(256) k_prolong_add(Geom g, T* __restrict__ x, 
 #define SMAC_ZM_PF 2
 #endif
 
-// L2 prefetch of `bytes` (a multiple of 16) from a 16-byte aligned address
-__device__ __forceinline__ void bulk_prefetch_l2(const void* p, uint32_t bytes) {
-  if ((reinterpret_cast<uintptr_t>(p) & 15u) != 0 || (bytes & 15u) != 0) return;
-  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
-}
-
 __device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
   asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
 }
@@ -283,17 +277,20 @@ __global__ void __launch_bounds__(ZmTile<T, NV_, WX, TY, MODE>::NT, ZmTile<T, NV
 
     // The rows the tile reads on one plane (j0-2 .. j0+TY+1, clipped to the
     // grid's ny+1 allocated rows) lie at consecutive addresses: one prefetch
-    // per array covers them.  Planes 0..nz are allocated in every array.
-    const int pf_j = max(0, j0 - 2);
-    const uint32_t pf_bytes = (uint32_t)((min(g.ny, j0 + TY + 1) - pf_j + 1) * g.px * (int)sizeof(T));
+    // per array covers them.  Planes 0..nz are allocated in every array, and
+    // the host passes pf = 0 unless every array is 16-byte aligned.  Thread 0
+    // (row j0-1) issues them from the kernel's parameters and its own row, so
+    // that no other thread keeps a value live for them.
     auto prefetch = [&](int m) {  // the operands of plane m (its z-faces m+1 and input m+1 with them)
-      if (tid != 0 || m < 0 || m + 1 > g.nz) return;
-      const int o = g.idx(0, pf_j, m), o1 = g.idx(0, pf_j, m + 1);
-      bulk_prefetch_l2(rhs + o, pf_bytes);
-      bulk_prefetch_l2(S.bx + o, pf_bytes);
-      bulk_prefetch_l2(S.by + o, pf_bytes);
-      bulk_prefetch_l2(S.bz + o1, pf_bytes);
-      if (MODE != 1) bulk_prefetch_l2(xin + o1, pf_bytes);
+      if (threadIdx.x != 0 || m < 0 || m + 1 > g.nz) return;
+      const int ja = max(0, j - 1);
+      const uint32_t bytes = (uint32_t)((min(g.ny, j + TY + 2) - ja + 1) * g.px * (int)sizeof(T));
+      const int o = g.idx(0, ja, m), o1 = o + g.ps;
+      bulk_prefetch_l2(rhs + o, bytes);
+      bulk_prefetch_l2(S.bx + o, bytes);
+      bulk_prefetch_l2(S.by + o, bytes);
+      bulk_prefetch_l2(S.bz + o1, bytes);
+      if (MODE != 1) bulk_prefetch_l2(xin + o1, bytes);
     };
 
     // prologue: the inputs of planes kb-1 and kb, the shared plane kb, the
