@@ -952,12 +952,19 @@ __device__ __forceinline__ double m_vstar(const MomArgs& A, const int* b) {
 // with 3 and 3.43 ms with 6.  Family-major block order (all
 // planes of one family, then the next, so that resident warps share one
 // family's code) took 3.64 ms: the interleaved families' shared reads
-// through L2 are worth more than the instruction-cache locality.
+// through L2 are worth more than the instruction-cache locality.  Block
+// shapes of 256 faces at 256^3: 32 x 8 2.28 ms, 64 x 4 2.32, 16 x 16 2.37,
+// 128 x 2 2.50 (two-way 2.56, 2.62, 2.65, 2.85).
+#ifndef SMAC_PV_BX
+#define SMAC_PV_BX 32  // predictor block: SMAC_PV_BX x (256 / SMAC_PV_BX) faces of one plane
+#endif
+constexpr int kPvBx = SMAC_PV_BX, kPvBy = 256 / SMAC_PV_BX;
+static_assert(kPvBx * kPvBy == 256, "the predictor's block has 256 threads");
 template <bool TW>
 __global__ void __launch_bounds__(256, 5) k_predict_vstar(MomArgs A) {
   const int fam = blockIdx.z % 3;
   const int z = blockIdx.z / 3 + 1;
-  const int x = blockIdx.x * 32 + threadIdx.x + 1, y = blockIdx.y * 8 + threadIdx.y + 1;
+  const int x = blockIdx.x * kPvBx + threadIdx.x + 1, y = blockIdx.y * kPvBy + threadIdx.y + 1;
   if (x > A.N[0] + 1 || y > A.N[1] + 1) return;
   int b[4];
 #pragma unroll
@@ -1498,11 +1505,12 @@ smac_status predict_vstar(const char* fn, const smac_grid_desc* d, const smac_bo
     A.st[k][2] = (int)(S0 * S1);
   }
   fill_table(&A.bc, bc);
-  const dim3 grid((unsigned)((d->nx + 1 + 31) / 32), (unsigned)((d->ny + 1 + 7) / 8), 3u * (unsigned)(d->nz + 1));
+  const dim3 grid((unsigned)((d->nx + 1 + kPvBx - 1) / kPvBx), (unsigned)((d->ny + 1 + kPvBy - 1) / kPvBy),
+                  3u * (unsigned)(d->nz + 1));
   if (tw)
-    k_predict_vstar<true><<<grid, dim3(32, 8), 0, (cudaStream_t)stream>>>(A);
+    k_predict_vstar<true><<<grid, dim3(kPvBx, kPvBy), 0, (cudaStream_t)stream>>>(A);
   else
-    k_predict_vstar<false><<<grid, dim3(32, 8), 0, (cudaStream_t)stream>>>(A);
+    k_predict_vstar<false><<<grid, dim3(kPvBx, kPvBy), 0, (cudaStream_t)stream>>>(A);
   return launch_status(fn);
 }
 
