@@ -942,11 +942,15 @@ __device__ __forceinline__ double m_vstar(const MomArgs& A, const int* b) {
 }
 
 // One thread per face index (x, y) of plane z of the box 1..N+1;
-// blockIdx.z = 3 (z - 1) + family, so the three families of a plane run
+// blockIdx.z takes SMAC_PV_ZG planes of family 0, the same planes of
+// family 1, then of family 2, so that the three families of a few planes run
 // together and share the arrays they all read (velocities, fluxes, cell
-// fields) through L2.  Only F_INTERIOR faces are written.  The kernel waits
-// on chains of dependent loads (a face type, then the value it selects), so
-// resident warps matter more than registers: 5 blocks per SM (48 registers,
+// fields) through L2, while an SM mostly runs one family's code at a time.
+// At 256^3, groups of 1, 2, 4, 8 and 16 planes: 2.268, 2.239, 2.244, 2.307
+// and 2.523 ms (two-way 2.540, 2.497, 2.507, 2.608, 2.839).  Only
+// F_INTERIOR faces are written.  The kernel waits on chains of dependent
+// loads (a face type, then the value it selects), so resident warps matter
+// more than registers: 5 blocks per SM (48 registers,
 // a few spills to L1) measured 3.32 ms at 256^3 with 64-bit offsets (3.14 ms
 // with the 32-bit ones now used), against 3.60 ms with 4 blocks, 4.27 ms
 // with 3 and 3.43 ms with 6.  Family-major block order (all
@@ -958,14 +962,18 @@ __device__ __forceinline__ double m_vstar(const MomArgs& A, const int* b) {
 #ifndef SMAC_PV_BX
 #define SMAC_PV_BX 32  // predictor block: SMAC_PV_BX x (256 / SMAC_PV_BX) faces of one plane
 #endif
-constexpr int kPvBx = SMAC_PV_BX, kPvBy = 256 / SMAC_PV_BX;
+#ifndef SMAC_PV_ZG
+#define SMAC_PV_ZG 2  // planes per family group: blockIdx.z runs G planes of family 0, then of 1, then of 2
+#endif
+constexpr int kPvBx = SMAC_PV_BX, kPvBy = 256 / SMAC_PV_BX, kPvZg = SMAC_PV_ZG;
 static_assert(kPvBx * kPvBy == 256, "the predictor's block has 256 threads");
 template <bool TW>
 __global__ void __launch_bounds__(256, 5) k_predict_vstar(MomArgs A) {
-  const int fam = blockIdx.z % 3;
-  const int z = blockIdx.z / 3 + 1;
+  const int q = blockIdx.z % (3 * kPvZg);
+  const int fam = q / kPvZg;
+  const int z = blockIdx.z / (3 * kPvZg) * kPvZg + q % kPvZg + 1;
   const int x = blockIdx.x * kPvBx + threadIdx.x + 1, y = blockIdx.y * kPvBy + threadIdx.y + 1;
-  if (x > A.N[0] + 1 || y > A.N[1] + 1) return;
+  if (x > A.N[0] + 1 || y > A.N[1] + 1 || z > A.N[2] + 1) return;
   int b[4];
 #pragma unroll
   for (int k = 0; k < 4; ++k) b[k] = x * A.st[k][0] + y * A.st[k][1] + z * A.st[k][2];
@@ -1506,7 +1514,7 @@ smac_status predict_vstar(const char* fn, const smac_grid_desc* d, const smac_bo
   }
   fill_table(&A.bc, bc);
   const dim3 grid((unsigned)((d->nx + 1 + kPvBx - 1) / kPvBx), (unsigned)((d->ny + 1 + kPvBy - 1) / kPvBy),
-                  3u * (unsigned)(d->nz + 1));
+                  3u * (unsigned)((d->nz + 1 + kPvZg - 1) / kPvZg * kPvZg));
   if (tw)
     k_predict_vstar<true><<<grid, dim3(kPvBx, kPvBy), 0, (cudaStream_t)stream>>>(A);
   else
